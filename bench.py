@@ -1,0 +1,364 @@
+"""Throughput of the OpenMULTI3D LTE output pass on B200.
+
+Workload (the 3D LTE synthesis configuration): a 240^3 seeded synthetic cube in 10
+depth slabs of 24 planes, 500 lines in 5000-5020 A, 4000 frequencies uniform in
+ln(lambda) split into windows of --nf frequencies, 13 output rays (Lobatto 4x4),
+rotate_array + long_char_quadratic.  One step is one frequency window for every
+ray: line opacity, transfer units, the slab-by-slab sweep, emergent intensity and
+flux.  Metric: Gpt*nu*ray/s = 1e-9 * rays * cells * frequencies / s.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--nf NF] [--impl reference]
+
+Ranks (torchrun) each take their own frequency windows: the windows are
+independent (weak scaling, no data-path collective).  --impl reference times the
+CPU restatement of the reference on this host's cores on a bounded sample.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "formal-solve Gpt*nu*ray/s on 1 B200, FP32 vs FP64 path at <=1e-4 flux error"
+UNIT = "Gpt*nu*ray/s"
+NFREQ_TOTAL = 4000
+
+
+def _args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=8)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--nf", type=int, default=32)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-fp64", action="store_true")
+    return p.parse_args()
+
+
+def _workload(nf):
+    return {"workload": "c1 3D LTE synthesis: 240^3 cube in 10 slabs of 24 planes, 500 lines 5000-5020 A, "
+                        f"4000 frequencies in windows of {nf}, 13 rays (Lobatto 4x4), rotate_array + "
+                        "long_char_quadratic; one step = one frequency window, all rays",
+            "cells": 240 ** 3, "rays": 13, "nf_window": nf, "nf_total": NFREQ_TOTAL, "slabs": 10,
+            "l2": "inputs larger than L2 (0.7 GB atmosphere + 3.5 GB transfer units per window)"}
+
+
+def _make_inputs(nf):
+    from dispatch_b200 import synth
+    atm, _, _, vec, wmu = synth.lte_config("c1", nf=nf, window=0)
+    llam_all, nu_all = synth.frequency_grid(5000.0, 5020.0, NFREQ_TOTAL)
+    return atm, llam_all, nu_all, vec, wmu
+
+
+def _window(llam_all, nu_all, nf, w):
+    nwin = NFREQ_TOTAL // nf
+    w = w % nwin
+    sl = slice(w * nf, (w + 1) * nf)
+    return np.ascontiguousarray(nu_all[sl]), np.ascontiguousarray(llam_all[sl])
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.f = None
+
+    def __enter__(self):
+        try:
+            self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.gpu)], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if self.proc is None or self.f is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.f.flush()
+        rows = [r.split(",") for r in open(self.f.name).read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [x.strip() for x in r]
+            if len(r) < 9:
+                continue
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, r[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def _peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        return None
+
+
+def _traffic_from_profiles(nf):
+    """dram bytes per k_quad_rot_column launch from the committed ncu summary, scaled to nf."""
+    path = os.path.join(ROOT, "profiles", "k_quad_rot_column_c1.md")
+    try:
+        for line in open(path):
+            if line.startswith("dram_bytes_per_launch_per_frequency:"):
+                return float(line.split(":")[1]) * nf
+    except OSError:
+        pass
+    return None
+
+
+def _cpu_baseline(atm, nu, llam, vec, wmu, ncols=2):
+    """The oracle (single thread) on a bounded sample: an ncols x ncols column block
+    of the cube, full depth and all slabs, this window, all rays."""
+    from oracle import pipeline as P
+    sub = _subcube(atm, ncols)
+    t0 = time.perf_counter()
+    P.lte_synthesis(sub, nu, llam, vec, wmu)
+    dt = time.perf_counter() - t0
+    work = wmu.size * sub["nx"] * sub["ny"] * sub["nz"] * nu.size
+    return {"value": work / dt / 1e9, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"{ncols}x{ncols} columns x 240 planes (10 slabs) x {nu.size} frequencies x {wmu.size} rays "
+                      f"of the same cube and window, C restatement of the reference, {dt:.1f} s"}
+
+
+def _subcube(atm, n):
+    nx, ny, nz = atm["nx"], atm["ny"], atm["nz"]
+
+    def cut(a):
+        return np.ascontiguousarray(a.reshape(nz, ny, nx)[:, :n, :n]).ravel()
+
+    sub = dict(atm)
+    sub["nx"] = sub["ny"] = n
+    for k in ("temp", "chi_c", "vx", "vy", "vz", "e_kT", "ne", "tothi", "stark_pe"):
+        sub[k] = cut(atm[k])
+    sub["species"] = [{k: (cut(v) if k in ("inv_df", "vbar2", "lnbase") else v) for k, v in sp.items()}
+                      for sp in atm["species"]]
+    return sub
+
+
+def _ref_task(args):
+    sub, nu, llam, vec, wmu = args
+    from oracle import pipeline as P
+    return P.lte_synthesis(sub, nu, llam, vec, wmu)[1]
+
+
+def run_reference(a):
+    """The reference arm: the CPU restatement on all host cores, bounded sample per step."""
+    ws, rank, _ = _dist()
+    if rank != 0:
+        return
+    import multiprocessing as mp
+    atm, llam_all, nu_all, vec, wmu = _make_inputs(a.nf)
+    nu, llam = _window(llam_all, nu_all, a.nf, NFREQ_TOTAL // a.nf // 2)
+    cores = os.cpu_count() or 1
+    ncols = 4
+    sub = _subcube(atm, ncols)
+    tasks = [(sub, nu, llam, vec[r:r + 1], wmu[r:r + 1]) for r in range(wmu.size)]
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(min(cores, len(tasks))) as pool:
+        for _ in range(a.warmup):
+            pool.map(_ref_task, tasks[:1])
+        t0 = time.perf_counter()
+        for _ in range(a.steps):
+            pool.map(_ref_task, tasks)
+        dt = (time.perf_counter() - t0) / a.steps
+    work = wmu.size * ncols * ncols * atm["nz"] * a.nf
+    value = work / dt / 1e9
+    sample = (f"{ncols}x{ncols} columns x 240 planes x {a.nf} frequencies x {wmu.size} rays per step, "
+              f"rays spread over {min(cores, len(tasks))} processes")
+    cfg = _workload(a.nf)
+    cfg["sample"] = sample
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": cfg,
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_b200(a):
+    import torch
+    import torch.distributed as dist
+
+    ws, rank, local = _dist()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+    import dispatch_b200 as m
+
+    m.init(local)
+    stream = torch.cuda.current_stream()
+    m.set_stream(stream.cuda_stream)
+    nf = a.nf
+    atm, llam_all, nu_all, vec, wmu = _make_inputs(nf)
+    ncell = atm["nx"] * atm["ny"] * atm["nz"]
+    nray = wmu.size
+    work_per_step = nray * ncell * nf
+
+    def to_dev(x):
+        return torch.from_numpy(np.ascontiguousarray(x)).to(f"cuda:{local}")
+
+    datm = {k: (to_dev(v) if isinstance(v, np.ndarray) else v) for k, v in atm.items()}
+    datm["species"] = [{k: to_dev(v) for k, v in sp.items()} for sp in atm["species"]]
+    nwin = NFREQ_TOTAL // nf
+    steps_total = a.warmup + a.steps
+    wins = [(rank * steps_total + i) % nwin for i in range(steps_total)]
+    dwin = [tuple(to_dev(x) for x in _window(llam_all, nu_all, nf, w)) for w in wins]
+
+    def step(i):
+        nu_d, llam_d = dwin[i]
+        return m.lte_synthesis(datm, nu_d, llam_d, vec, wmu, device=True)
+
+    for i in range(a.warmup):
+        step(i)
+    torch.cuda.synchronize()
+    if ws > 1:
+        dist.barrier()
+    n0 = m.launch_count()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for i in range(a.warmup, steps_total):
+            step(i)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    launches = m.launch_count() - n0
+    ms = ev0.elapsed_time(ev1)
+    if ws > 1:
+        t = torch.tensor([ms], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    value = ws * a.steps * work_per_step / (ms / 1e3) / 1e9
+    clocks = clk.summary()
+
+    # stage times and the sweep kernel's roofline (library CUDA events on its stream)
+    m.profile_enable(True)
+    step(a.warmup)
+    op_ms, op_n = m.profile_read(m.STAGE_OPACITY)
+    sv_ms, sv_n = m.profile_read(m.STAGE_SOLVE)
+    rd_ms, rd_n = m.profile_read(m.STAGE_REDUCE)
+    m.profile_enable(False)
+    peaks = _peaks()
+    peak = peaks["hbm_gbs"] if peaks else 6650.0
+    bytes_launch = 8.0 * ncell * nf                          # chi and Snu read once per ray point frequency
+    achieved = bytes_launch / (sv_ms / sv_n / 1e3) / 1e9 if sv_n else None
+    traffic = _traffic_from_profiles(nf)
+    roofline = {"kernel": "k_quad_rot_column (rotate_array + long_char_quadratic, all slabs)", "bound": "hbm",
+                "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak if achieved else None,
+                "traffic": traffic, "peak_source": "measured" if peaks else "fallback",
+                "algorithmic_bytes_per_launch": bytes_launch}
+    stages = {"opacity_ms_per_step": op_ms, "opacity_launches": op_n, "solve_ms_per_step": sv_ms,
+              "solve_launches": sv_n, "reduce_ms_per_step": rd_ms,
+              "solve_gpt_per_s": work_per_step / (sv_ms / 1e3) / 1e9 if sv_ms else None}
+
+    # end to end through the C ABI with pinned host buffers (copies inside the timed region)
+    def pin(x):
+        t = torch.from_numpy(np.ascontiguousarray(x)).pin_memory()
+        return t.numpy()
+
+    hatm = {k: (pin(v) if isinstance(v, np.ndarray) else v) for k, v in atm.items()}
+    hatm["species"] = [{k: pin(v) for k, v in sp.items()} for sp in atm["species"]]
+    hwin = [tuple(pin(x) for x in _window(llam_all, nu_all, nf, w)) for w in wins]
+    h2d = sum(v.nbytes for k, v in hatm.items() if isinstance(v, np.ndarray))
+    h2d += sum(v.nbytes for sp in hatm["species"] for v in sp.values()) + 2 * nf * 8
+    d2h = (nray + 1) * nf * 4
+    m.lte_synthesis(hatm, hwin[0][0], hwin[0][1], vec, wmu)
+    e2e_steps = max(1, min(a.steps, 4))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for i in range(e2e_steps):
+        nu_h, llam_h = hwin[a.warmup + i % a.steps]
+        ie, flux, _ = m.lte_synthesis(hatm, nu_h, llam_h, vec, wmu)
+        float(flux[0])
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    e2e = {"value": ws * work_per_step / e2e_s / 1e9, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+           "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_s * 1e3}
+
+    # the plain FP64 path on the same window, and the FP32 flux error against it
+    fp64 = None
+    if not a.no_fp64:
+        nu_d, llam_d = dwin[a.warmup]
+        _, f32, _ = m.lte_synthesis(datm, nu_d, llam_d, vec, wmu, device=True)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        _, f64, _ = m.lte_synthesis(datm, nu_d, llam_d, vec, wmu, device=True, fp64=True)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t64 = e0.elapsed_time(e1)
+        err = float(torch.max(torch.abs(f32 - f64) / torch.abs(f64)).item())
+        fp64 = {"value": work_per_step / (t64 / 1e3) / 1e9, "unit": UNIT, "ms_per_step": t64,
+                "fp32_over_fp64": value / ws / (work_per_step / (t64 / 1e3) / 1e9),
+                "max_rel_flux_err_fp32_vs_fp64": err,
+                "path": "same kernels in FP64 for units, rotation and solver, one launch per ray and slab"}
+
+    cpu = None
+    if rank == 0 and not a.no_cpu_baseline:
+        nu, llam = _window(llam_all, nu_all, nf, wins[a.warmup])
+        cpu = _cpu_baseline(atm, nu, llam, vec, wmu)
+
+    if ws > 1:
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (seeded grey cube, random line list)", "config": _workload(nf),
+            "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline, "cpu_baseline": cpu,
+            "clocks": clocks, "stages": stages, "fp64_plain": fp64}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    a = _args()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_b200(a)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,1038 @@
+// libm3dgpu.so: the C ABI of include/m3dgpu.h over the sm_100a kernels.
+//
+// Host pointers are staged through device buffers for the duration of a call;
+// with M3D_DEVICE_PTRS the caller's device pointers are used directly and the
+// call only enqueues work on the library stream.
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/m3dgpu.h"
+#include "m3d_pipeline.cuh"
+
+using namespace m3d;
+
+namespace {
+
+struct Ctx {
+  bool init = false;
+  int device = 0;
+  cudaStream_t own = nullptr, stream = nullptr;
+  float *d_tgx = nullptr, *d_th2x = nullptr;
+  std::vector<float> h_tgx, h_th2x;
+  long long launches = 0;
+  std::string err;
+  // scratch buffers kept between calls, grown on demand
+  std::vector<void *> scratch;
+  std::vector<size_t> scratch_bytes;
+  // staging buffers of host-pointer calls, reused from call to call
+  std::vector<void *> stage_buf;
+  std::vector<size_t> stage_bytes;
+  // stage timing (m3d_profile_enable)
+  bool profile = false;
+  std::vector<cudaEvent_t> ev_free;
+  struct Rec { int stage; cudaEvent_t a, b; };
+  std::vector<Rec> recs;
+  double stage_ms[4] = {0, 0, 0, 0};
+  long long stage_n[4] = {0, 0, 0, 0};
+};
+
+Ctx g_ctx;
+
+int fail(int code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_ctx.err = buf;
+  return code;
+}
+
+#define CUDA_TRY(expr)                                                                   \
+  do {                                                                                   \
+    cudaError_t e_ = (expr);                                                             \
+    if (e_ != cudaSuccess) return fail(M3D_ECUDA, "%s: %s", #expr, cudaGetErrorString(e_)); \
+  } while (0)
+
+cudaEvent_t take_event() {
+  if (!g_ctx.ev_free.empty()) {
+    cudaEvent_t e = g_ctx.ev_free.back();
+    g_ctx.ev_free.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+#define LAUNCH_S(stage_, kernel, grid, block, smem, ...)                                           \
+  do {                                                                                             \
+    cudaEvent_t ea_ = nullptr, eb_ = nullptr;                                                      \
+    if (g_ctx.profile) {                                                                           \
+      ea_ = take_event();                                                                          \
+      eb_ = take_event();                                                                          \
+      cudaEventRecord(ea_, g_ctx.stream);                                                          \
+    }                                                                                              \
+    kernel<<<(grid), (block), (smem), g_ctx.stream>>>(__VA_ARGS__);                                \
+    g_ctx.launches++;                                                                              \
+    cudaError_t e_ = cudaGetLastError();                                                           \
+    if (e_ != cudaSuccess) return fail(M3D_ECUDA, "launch %s: %s", #kernel, cudaGetErrorString(e_)); \
+    if (g_ctx.profile) {                                                                           \
+      cudaEventRecord(eb_, g_ctx.stream);                                                          \
+      g_ctx.recs.push_back(Ctx::Rec{(stage_), ea_, eb_});                                          \
+    }                                                                                              \
+  } while (0)
+#define LAUNCH(kernel, grid, block, smem, ...) LAUNCH_S(M3D_STAGE_OTHER, kernel, grid, block, smem, __VA_ARGS__)
+
+int need_init() {
+  if (!g_ctx.init) return fail(M3D_ENOINIT, "m3d_init has not been called");
+  return M3D_OK;
+}
+
+// scratch slot: a device buffer of at least `bytes`, kept for later calls
+int scratch(int slot, size_t bytes, void **out) {
+  if ((int)g_ctx.scratch.size() <= slot) {
+    g_ctx.scratch.resize(slot + 1, nullptr);
+    g_ctx.scratch_bytes.resize(slot + 1, 0);
+  }
+  if (g_ctx.scratch_bytes[slot] < bytes) {
+    if (g_ctx.scratch[slot]) {
+      CUDA_TRY(cudaStreamSynchronize(g_ctx.stream));
+      CUDA_TRY(cudaFree(g_ctx.scratch[slot]));
+      g_ctx.scratch[slot] = nullptr;
+      g_ctx.scratch_bytes[slot] = 0;
+    }
+    CUDA_TRY(cudaMalloc(&g_ctx.scratch[slot], bytes));
+    g_ctx.scratch_bytes[slot] = bytes;
+  }
+  *out = g_ctx.scratch[slot];
+  return M3D_OK;
+}
+
+// Host-pointer staging for one call: device copies of the arguments, copied
+// back on finish() for the ones marked out.
+class Staging {
+ public:
+  explicit Staging(unsigned flags) : dev_(flags & M3D_DEVICE_PTRS) {}
+  // in: copied to the device; out: copied back; both: both
+  template <typename T>
+  int map(T *host, size_t count, bool in, bool out, T **dptr) {
+    if (host == nullptr || count == 0) { *dptr = nullptr; return M3D_OK; }
+    if (dev_) { *dptr = host; return M3D_OK; }
+    Buf b;
+    b.host = (void *)host;
+    b.bytes = count * sizeof(T);
+    b.out = out;
+    const size_t slot = bufs_.size();
+    if (g_ctx.stage_buf.size() <= slot) {
+      g_ctx.stage_buf.resize(slot + 1, nullptr);
+      g_ctx.stage_bytes.resize(slot + 1, 0);
+    }
+    if (g_ctx.stage_bytes[slot] < b.bytes) {
+      if (g_ctx.stage_buf[slot]) {
+        CUDA_TRY(cudaStreamSynchronize(g_ctx.stream));
+        CUDA_TRY(cudaFree(g_ctx.stage_buf[slot]));
+      }
+      g_ctx.stage_buf[slot] = nullptr;
+      g_ctx.stage_bytes[slot] = 0;
+      CUDA_TRY(cudaMalloc(&g_ctx.stage_buf[slot], b.bytes));
+      g_ctx.stage_bytes[slot] = b.bytes;
+    }
+    b.dptr = g_ctx.stage_buf[slot];
+    if (in) CUDA_TRY(cudaMemcpyAsync(b.dptr, host, b.bytes, cudaMemcpyHostToDevice, g_ctx.stream));
+    else CUDA_TRY(cudaMemsetAsync(b.dptr, 0, b.bytes, g_ctx.stream));
+    bufs_.push_back(b);
+    *dptr = (T *)b.dptr;
+    return M3D_OK;
+  }
+  template <typename T>
+  int in(const T *host, size_t count, const T **dptr) {
+    T *d;
+    int rc = map(const_cast<T *>(host), count, true, false, &d);
+    *dptr = d;
+    return rc;
+  }
+  int finish() {
+    if (dev_) return M3D_OK;
+    for (auto &b : bufs_)
+      if (b.out) CUDA_TRY(cudaMemcpyAsync(b.host, b.dptr, b.bytes, cudaMemcpyDeviceToHost, g_ctx.stream));
+    CUDA_TRY(cudaStreamSynchronize(g_ctx.stream));
+    return M3D_OK;
+  }
+  bool device() const { return dev_; }
+
+ private:
+  struct Buf { void *dptr = nullptr; void *host = nullptr; size_t bytes = 0; bool out = false; };
+  bool dev_;
+  std::vector<Buf> bufs_;
+};
+
+#define TRY(expr)                  \
+  do {                             \
+    int rc_ = (expr);              \
+    if (rc_ != M3D_OK) return rc_; \
+  } while (0)
+
+int grid_for(size_t n, int block = 256) {
+  size_t g = (n + block - 1) / block;
+  const size_t cap = (size_t)148 * 32;
+  return (int)(g > cap ? cap : (g < 1 ? 1 : g));
+}
+
+// ---- QLG tables: qlg_init (qlg_mod.f90:364-375) with the Weideman-32 /
+// Humlicek-w4 fp64 reference (qlg_mod.f90:411-447) and Z_0.2 (qlg_mod.f90:384-399)
+const double W32_LD = 4.75682846001088411e+00;
+const double W32_AD[32] = {
+    -1.30317978630500875e-12, +3.74107755472269789e-12, +8.03033538228436012e-12, -2.15435373143760700e-11,
+    -5.54423561143486540e-11, +1.16582546820233235e-10, +4.15374271614691897e-10, -5.23102143724924582e-10,
+    -3.20801514078875819e-09, +8.12488896568210460e-10, +2.37975567593842971e-08, +2.29304391194392872e-08,
+    -1.48130789124396946e-07, -4.18407637053084035e-07, +4.25583313792292626e-07, +4.40153173159092505e-06,
+    +6.82103194402497841e-06, -2.14096192018698432e-05, -1.30754492546239731e-04, -2.45329802700202065e-04,
+    +3.92591360700705167e-04, +4.51954110534923473e-03, +1.90061557848454077e-02, +5.73044035298371918e-02,
+    +1.40607162268937713e-01, +2.95444510715087261e-01, +5.46013972063934205e-01, +9.01925489364799993e-01,
+    +1.34554416923454490e+00, +1.82566962963248147e+00, +2.26353729990026764e+00, +2.57225340812456960e+00};
+
+double voigt_ref_f64(double a, double v) {
+  const double ISQPI8 = 0.564189583547756287;
+  const double av = fabs(v);
+  if (av + a >= 15.0) {
+    const double tr = a * a - av * av + 0.5, ti = -2.0 * a * av;
+    const double q = 1.0 / (tr * tr + ti * ti);
+    return ISQPI8 * ((a * tr + (-av) * ti) * q);
+  }
+  const double dr = W32_LD + a, nr0 = W32_LD - a, di = -v;
+  const double q = 1.0 / (dr * dr + di * di);
+  const double zr = (nr0 * dr + v * di) * q, zi = (v * dr - nr0 * di) * q;
+  double pr = W32_AD[0], pim = 0.0;
+  for (int j = 1; j < 32; j++) {
+    const double t = pr * zr - pim * zi + W32_AD[j];
+    pim = pr * zi + pim * zr;
+    pr = t;
+  }
+  const double ir = dr * q, ii = -di * q;
+  const double sr = ir * ir - ii * ii, si = 2.0 * ir * ii;
+  return 2.0 * (pr * sr - pim * si) + ISQPI8 * ir;
+}
+
+double z02_over_l2(double u) {
+  const double A2 = 0.18741813853432507, GAM = 0.93709069267162530, KP = 0.81924853602069690;
+  const double ETA = 0.14697983683153040, QRS = 0.16, DLN2 = 0.69314718055994531;
+  const double v = GAM * sqrt(u), L = 1.0 / (1.0 + u), G = exp(-DLN2 * u);
+  const double Kv = voigt_ref_f64(A2, v);
+  const double P = KP * (ETA * L + (1.0 - ETA) * G);
+  return (Kv - P) / (QRS * KP) * (1.0 + u) * (1.0 + u);
+}
+
+int ensure_tables() {
+  if (g_ctx.d_tgx) return M3D_OK;
+  g_ctx.h_tgx.resize(QLG_NTAB);
+  g_ctx.h_th2x.resize(QLG_NTAB);
+  for (int i = 0; i < QLG_NTAB; i++) {
+    const double x = (double)i / 800.0;
+    g_ctx.h_tgx[i] = (float)pow(2.0, -x * x);
+    g_ctx.h_th2x[i] = (float)z02_over_l2(x * x);
+  }
+  CUDA_TRY(cudaMalloc(&g_ctx.d_tgx, 2 * QLG_NTAB * sizeof(float)));
+  g_ctx.d_th2x = g_ctx.d_tgx + QLG_NTAB;
+  CUDA_TRY(cudaMemcpy(g_ctx.d_tgx, g_ctx.h_tgx.data(), QLG_NTAB * sizeof(float), cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(g_ctx.d_th2x, g_ctx.h_th2x.data(), QLG_NTAB * sizeof(float), cudaMemcpyHostToDevice));
+  return M3D_OK;
+}
+
+SlabArgs slab_args(const m3d_slab_t *s, unsigned flags) {
+  SlabArgs a;
+  a.nf = s->nf; a.nx = s->nx; a.ny = s->ny; a.nz = s->nz; a.dir = s->dir;
+  a.get_psi = s->get_psi || (flags & M3D_GET_PSI);
+  a.split_rates = s->split_rates || (flags & M3D_SPLIT_RATES);
+  for (int i = 0; i < 3; i++) { a.ds[i] = s->ds[i]; a.vec[i] = s->vec[i]; }
+  a.maser_dtau_max = s->maser_dtau_max;
+  a.maser_Inu_max = s->maser_Inu_max;
+  return a;
+}
+
+int check_slab(const m3d_slab_t *s) {
+  if (!s) return fail(M3D_EINVAL, "slab is NULL");
+  if (s->nf < 1 || s->nx < 1 || s->ny < 1 || s->nz < 2) return fail(M3D_EINVAL, "slab needs nf,nx,ny >= 1 and nz >= 2");
+  if (s->dir != 1 && s->dir != -1) return fail(M3D_EINVAL, "slab dir must be +1 or -1");
+  if (s->vec[2] == 0.0) return fail(M3D_EINVAL, "ray direction with vec(3) = 0");
+  return M3D_OK;
+}
+
+// set_stencil (ray_mod.f90:493-512) and the Keys kernel (ray_mod.f90:581-597)
+void cc_kernel(double s, double k[4]) {
+  const double s2 = s * s, s3 = s2 * s;
+  k[0] = 0.5 * (-s3 + 2 * s2 - s);
+  k[1] = 0.5 * (3 * s3 - 5 * s2 + 2);
+  k[2] = 0.5 * (-3 * s3 + 4 * s2 + s);
+  k[3] = 0.5 * (s3 - s2);
+}
+void set_stencil(const double ds[3], const double vec[3], double xk[4], double yk[4], int *upo1, int *upo2,
+                 double *dsup) {
+  *dsup = ds[2] / fabs(vec[2]);
+  const double wt1 = -vec[0] / ds[0] * *dsup, wt2 = -vec[1] / ds[1] * *dsup;
+  const double h1 = wt1 > 0 ? wt1 : wt1 + 1, h2 = wt2 > 0 ? wt2 : wt2 + 1;
+  *upo1 = wt1 > 0 ? -1 : -2;
+  *upo2 = wt2 > 0 ? -1 : -2;
+  cc_kernel(h1, xk);
+  cc_kernel(h2, yk);
+}
+
+// quadratic solver constants (rt_solvers_mod.f90:908-912)
+QuadConst quad_const(double ds_cm3, double vec3) {
+  QuadConst q;
+  const float ds = (float)ds_cm3;
+  const float dsup = (float)((double)ds / fabs(vec3));
+  q.rdsup = 1.0f / dsup;
+  q.dsup1 = 0.5f * dsup;
+  q.dsup2 = ((1.0f / 12.0f) * dsup) * dsup;
+  return q;
+}
+
+// pchip_mono extrapolation constants for the bottom ghost (interpol_mod.f90:289-365
+// with xx = (1,2,3)*ds, newx = 0)
+PchipConst pchip_const(float ds3_code) {
+  PchipConst c;
+  const float xx1 = (float)(1.0 * (double)ds3_code), xx2 = (float)(2.0 * (double)ds3_code);
+  c.dx1 = xx2 - xx1;
+  const float t1 = (0.0f - xx1) / c.dx1;
+  const float t2 = t1 * t1, t3 = t2 * t1;
+  c.p = 3.0f * t2 - 2.0f * t3;
+  c.c0 = 1.0f - c.p;
+  c.cm0 = (t3 - 2.0f * t2) + t1;
+  c.cm1 = t3 - t2;
+  return c;
+}
+
+// rotate_array coefficients of local planes 1..nz of a slab (rt_patch_mod.f90:3821-3841)
+void rot_planes(const double vec[3], const double ds_code[3], double bot2pivot, const double ray_offset[2], int nz,
+                RotPlane *out) {
+  const float delta0 = (float)(vec[0] / (vec[2] * ds_code[0]));
+  const float delta1 = (float)(vec[1] / (vec[2] * ds_code[1]));
+  const float b2p = (float)bot2pivot;
+  for (int z = 1; z <= nz; z++) {
+    const float height = (float)((double)z * ds_code[2]);
+    const float dk0 = (float)((double)((b2p - height) * delta0) + ray_offset[0]);
+    const float dk1 = (float)((double)((b2p - height) * delta1) + ray_offset[1]);
+    const int up1 = (int)floorf(dk0), up2 = (int)floorf(dk1);
+    const float f1 = dk0 - (float)up1, f2 = dk1 - (float)up2;
+    RotPlane r;
+    r.up1 = up1;
+    r.up2 = up2;
+    r.a = (1.0f - f1) * (1.0f - f2);
+    r.b = f1 * (1.0f - f2);
+    r.c = (1.0f - f1) * f2;
+    r.d = f1 * f2;
+    out[z - 1] = r;
+  }
+}
+
+LineArgs line_args(const m3d_linelist_t *ll) {
+  LineArgs L;
+  L.nline = ll->nline;
+  L.llam0 = ll->llam0;
+  L.lower_ev = ll->lower_ev; L.gpref = ll->gpref; L.grad = ll->grad;
+  L.gw1 = ll->gw1; L.gw2 = ll->gw2; L.gstk = ll->gstk;
+  L.unsold = ll->unsold;
+  L.lev_i = ll->lev_i; L.lev_j = ll->lev_j;
+  L.active = ll->active;
+  return L;
+}
+
+// stage a line list's arrays
+int stage_linelist(Staging &st, const m3d_linelist_t *ll, LineArgs *L) {
+  const size_t n = (size_t)ll->nline;
+  *L = line_args(ll);
+  TRY(st.in(ll->llam0, n, &L->llam0));
+  TRY(st.in(ll->lower_ev, n, &L->lower_ev));
+  TRY(st.in(ll->gpref, n, &L->gpref));
+  TRY(st.in(ll->grad, n, &L->grad));
+  TRY(st.in(ll->gw1, n, &L->gw1));
+  TRY(st.in(ll->gw2, n, &L->gw2));
+  TRY(st.in(ll->gstk, n, &L->gstk));
+  TRY(st.in(ll->unsold, n, &L->unsold));
+  TRY(st.in(ll->lev_i, n, &L->lev_i));
+  TRY(st.in(ll->lev_j, n, &L->lev_j));
+  TRY(st.in(ll->active, n, &L->active));
+  if (!L->llam0 || !L->lower_ev || !L->gpref || !L->grad || !L->gw1 || !L->gw2 || !L->gstk || !L->unsold)
+    return fail(M3D_EINVAL, "line list with a NULL array");
+  return M3D_OK;
+}
+
+GridArgs grid_args(int nf, const double *llam_host_or_dev, const double *d_llam, bool dev, float tol,
+                   float line_reject_frac) {
+  GridArgs G;
+  double l0, l1;
+  if (dev) {
+    cudaMemcpy(&l0, llam_host_or_dev, sizeof(double), cudaMemcpyDeviceToHost);
+    cudaMemcpy(&l1, llam_host_or_dev + nf - 1, sizeof(double), cudaMemcpyDeviceToHost);
+  } else {
+    l0 = llam_host_or_dev[0];
+    l1 = llam_host_or_dev[nf - 1];
+  }
+  G.nf = nf;
+  G.llam = d_llam;
+  G.llam1 = l0;
+  G.dllam = (l1 - l0) / (double)(nf - 1);
+  G.inv_dllam = 1.0 / G.dllam;
+  G.sdl = (float)G.inv_dllam;
+  G.tol = tol;
+  G.flo_scale = fmaxf(tol, line_reject_frac) * tol;
+  return G;
+}
+
+}  // namespace
+
+// ============================================================================
+extern "C" {
+
+int m3d_init(int device, unsigned flags) {
+  (void)flags;
+  if (g_ctx.init) {
+    if (device != g_ctx.device) return fail(M3D_EINVAL, "already initialised on device %d", g_ctx.device);
+    return M3D_OK;
+  }
+  int n = 0;
+  CUDA_TRY(cudaGetDeviceCount(&n));
+  if (device < 0 || device >= n) return fail(M3D_EINVAL, "device %d not present (%d devices)", device, n);
+  CUDA_TRY(cudaSetDevice(device));
+  CUDA_TRY(cudaStreamCreateWithFlags(&g_ctx.own, cudaStreamNonBlocking));
+  g_ctx.stream = g_ctx.own;
+  g_ctx.device = device;
+  g_ctx.init = true;
+  return ensure_tables();
+}
+
+int m3d_free(void) {
+  if (!g_ctx.init) return M3D_OK;
+  cudaStreamSynchronize(g_ctx.stream);
+  for (void *p : g_ctx.scratch) if (p) cudaFree(p);
+  g_ctx.scratch.clear();
+  g_ctx.scratch_bytes.clear();
+  for (void *p : g_ctx.stage_buf) if (p) cudaFree(p);
+  g_ctx.stage_buf.clear();
+  g_ctx.stage_bytes.clear();
+  for (auto &r : g_ctx.recs) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
+  g_ctx.recs.clear();
+  for (auto e : g_ctx.ev_free) cudaEventDestroy(e);
+  g_ctx.ev_free.clear();
+  if (g_ctx.d_tgx) cudaFree(g_ctx.d_tgx);
+  g_ctx.d_tgx = g_ctx.d_th2x = nullptr;
+  if (g_ctx.own) cudaStreamDestroy(g_ctx.own);
+  g_ctx.own = g_ctx.stream = nullptr;
+  g_ctx.init = false;
+  return M3D_OK;
+}
+
+int m3d_last_error(char *buf, int buflen) {
+  if (!buf || buflen < 1) return M3D_EINVAL;
+  snprintf(buf, (size_t)buflen, "%s", g_ctx.err.c_str());
+  return M3D_OK;
+}
+
+int m3d_version(int *major, int *minor, int *patch) {
+  if (major) *major = 0;
+  if (minor) *minor = 1;
+  if (patch) *patch = 0;
+  return M3D_OK;
+}
+
+int m3d_set_stream(void *s) {
+  TRY(need_init());
+  g_ctx.stream = s ? (cudaStream_t)s : g_ctx.own;
+  return M3D_OK;
+}
+
+int m3d_synchronize(void) {
+  TRY(need_init());
+  CUDA_TRY(cudaStreamSynchronize(g_ctx.stream));
+  return M3D_OK;
+}
+
+long long m3d_launch_count(void) { return g_ctx.launches; }
+
+int m3d_profile_enable(int on) {
+  TRY(need_init());
+  g_ctx.profile = on != 0;
+  for (int i = 0; i < 4; i++) { g_ctx.stage_ms[i] = 0; g_ctx.stage_n[i] = 0; }
+  return M3D_OK;
+}
+
+int m3d_profile_read(int stage, double *ms, long long *launches) {
+  TRY(need_init());
+  if (stage < 0 || stage > 3) return fail(M3D_EINVAL, "m3d_profile_read: stage %d", stage);
+  CUDA_TRY(cudaStreamSynchronize(g_ctx.stream));
+  for (auto &r : g_ctx.recs) {
+    float t = 0;
+    CUDA_TRY(cudaEventElapsedTime(&t, r.a, r.b));
+    g_ctx.stage_ms[r.stage] += t;
+    g_ctx.stage_n[r.stage] += 1;
+    g_ctx.ev_free.push_back(r.a);
+    g_ctx.ev_free.push_back(r.b);
+  }
+  g_ctx.recs.clear();
+  if (ms) *ms = g_ctx.stage_ms[stage];
+  if (launches) *launches = g_ctx.stage_n[stage];
+  return M3D_OK;
+}
+
+int m3d_weights(int which, int n, const void *t, void *o1, void *o2, void *o3, void *o4, unsigned flags) {
+  TRY(need_init());
+  if (n < 0 || which < 0 || which > 4) return fail(M3D_EINVAL, "m3d_weights: bad which/n");
+  if (n == 0) return M3D_OK;
+  const bool f64 = flags & M3D_FP64;
+  if (f64 && which != 1 && which != 2) return fail(M3D_EUNSUPPORTED, "m3d_weights: FP64 has which = 1, 2 only");
+  const int nout = which == 0 ? 2 : (which >= 3 ? 1 : 4);
+  Staging st(flags);
+  if (f64) {
+    const double *dt; double *d[4] = {nullptr, nullptr, nullptr, nullptr};
+    TRY(st.in((const double *)t, n, &dt));
+    void *outs[4] = {o1, o2, o3, o4};
+    for (int i = 0; i < nout; i++) TRY(st.map((double *)outs[i], n, false, true, &d[i]));
+    LAUNCH(k_weights_f64, grid_for(n), 256, 0, which, n, dt, d[0], d[1], d[2], d[3]);
+  } else {
+    const float *dt; float *d[4] = {nullptr, nullptr, nullptr, nullptr};
+    TRY(st.in((const float *)t, n, &dt));
+    void *outs[4] = {o1, o2, o3, o4};
+    for (int i = 0; i < nout; i++) TRY(st.map((float *)outs[i], n, false, true, &d[i]));
+    LAUNCH(k_weights_f32, grid_for(n), 256, 0, which, n, dt, d[0], d[1], d[2], d[3]);
+  }
+  return st.finish();
+}
+
+int m3d_qlg_init(void) {
+  TRY(need_init());
+  return ensure_tables();
+}
+
+int m3d_qlg_tables(float *tgx, float *th2x) {
+  TRY(need_init());
+  TRY(ensure_tables());
+  if (tgx) memcpy(tgx, g_ctx.h_tgx.data(), QLG_NTAB * sizeof(float));
+  if (th2x) memcpy(th2x, g_ctx.h_th2x.data(), QLG_NTAB * sizeof(float));
+  return M3D_OK;
+}
+
+int m3d_qlg_bot_profile(int n, const float *a, const float *q, const float *vpr, const float *idf, float *h,
+                        unsigned flags) {
+  TRY(need_init());
+  if (n < 0) return fail(M3D_EINVAL, "n < 0");
+  if (n == 0) return M3D_OK;
+  Staging st(flags);
+  const float *da, *dq, *dv, *di;
+  float *dh;
+  TRY(st.in(a, n, &da)); TRY(st.in(q, n, &dq)); TRY(st.in(vpr, n, &dv)); TRY(st.in(idf, n, &di));
+  TRY(st.map(h, n, false, true, &dh));
+  LAUNCH(k_qlg_profile, grid_for(n), 256, 0, n, g_ctx.d_tgx, g_ctx.d_th2x, da, dq, dv, di, dh);
+  return st.finish();
+}
+
+int m3d_line_opacity(const m3d_linelist_t *ll, int nf, const double *llam, int ncell, float *chi, float *eta,
+                     const float *cont, const float *logref, const float *vproj, const float *inv_df,
+                     const float *vbar2, const float *e_kT, const float *lnbase, const float *ne,
+                     const float *tothi, const float *stark_pe, const float *dep_mem, int nlevel, int do_nlte,
+                     float tol, float line_reject_frac, unsigned char *used, float *strength, float *reach,
+                     unsigned flags) {
+  TRY(need_init());
+  if (!ll || !llam) return fail(M3D_EINVAL, "m3d_line_opacity: NULL line list or grid");
+  if (ll->nline == 0 || nf < 2 || ncell == 0) return M3D_OK;
+  if (ncell < 0 || ll->nline < 0) return fail(M3D_EINVAL, "m3d_line_opacity: negative size");
+  const bool diag = flags & M3D_LINE_DIAG;
+  if (diag && (!used || !strength || !reach)) return fail(M3D_EINVAL, "M3D_LINE_DIAG needs used, strength, reach");
+  if (do_nlte && (!dep_mem || nlevel < 1)) return fail(M3D_EINVAL, "do_nlte needs dep_mem and nlevel");
+  Staging st(flags);
+  LineArgs L;
+  TRY(stage_linelist(st, ll, &L));
+  const double *dllam;
+  TRY(st.in(llam, nf, &dllam));
+  const size_t nfc = (size_t)nf * ncell;
+  float *dchi, *deta;
+  const float *dcont, *dlr, *dvp, *didf, *dvb, *dek, *dlb, *dne, *dth, *dsp, *ddep = nullptr;
+  TRY(st.map(chi, nfc, true, true, &dchi));
+  TRY(st.map(eta, nfc, true, true, &deta));
+  TRY(st.in(cont, nfc, &dcont)); TRY(st.in(logref, nfc, &dlr));
+  TRY(st.in(vproj, ncell, &dvp)); TRY(st.in(inv_df, ncell, &didf)); TRY(st.in(vbar2, ncell, &dvb));
+  TRY(st.in(e_kT, ncell, &dek)); TRY(st.in(lnbase, ncell, &dlb)); TRY(st.in(ne, ncell, &dne));
+  TRY(st.in(tothi, ncell, &dth)); TRY(st.in(stark_pe, ncell, &dsp));
+  if (do_nlte) TRY(st.in(dep_mem, (size_t)ncell * nlevel, &ddep));
+  unsigned char *dused = nullptr;
+  float *dstr = nullptr, *dreach = nullptr;
+  if (diag) {
+    TRY(st.map(used, ll->nline, true, true, &dused));
+    TRY(st.map(strength, ll->nline, true, true, &dstr));
+    TRY(st.map(reach, ll->nline, true, true, &dreach));
+  }
+  GridArgs G = grid_args(nf, llam, dllam, st.device(), tol, line_reject_frac);
+  if (!(G.dllam > 0)) return fail(M3D_EINVAL, "m3d_line_opacity: log(lambda) grid must be ascending");
+  const int block = 256, warps = block / 32;
+  const size_t smem = 2 * QLG_NTAB * sizeof(float);
+  static bool attr = false;
+  if (!attr) {
+    CUDA_TRY(cudaFuncSetAttribute(k_line_opacity, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    attr = true;
+  }
+  int grid = (ncell + warps - 1) / warps;
+  if (grid > 148 * 8) grid = 148 * 8;
+  LAUNCH_S(M3D_STAGE_OPACITY, k_line_opacity, grid, block, smem, L, G, ncell, dchi, deta, dcont, dlr, dvp, didf, dvb, dek, dlb, dne, dth,
+         dsp, ddep, do_nlte, diag ? 1 : 0, dused, dstr, dreach, g_ctx.d_tgx, g_ctx.d_th2x);
+  return st.finish();
+}
+
+int m3d_lte_background(int nf, int ncell, const double *nu, const float *temp, float *beta, float *Bnu,
+                       unsigned flags) {
+  TRY(need_init());
+  if (nf < 1 || ncell < 1) return fail(M3D_EINVAL, "m3d_lte_background: empty");
+  Staging st(flags);
+  const double *dnu;
+  const float *dt;
+  float *db, *dB;
+  const size_t n = (size_t)nf * ncell;
+  TRY(st.in(nu, nf, &dnu)); TRY(st.in(temp, ncell, &dt));
+  TRY(st.map(beta, n, false, true, &db)); TRY(st.map(Bnu, n, false, true, &dB));
+  LAUNCH(k_lte_background, grid_for(n), 256, 0, nf, ncell, dnu, dt, db, dB);
+  return st.finish();
+}
+
+int m3d_work_to_transfer_units(int nf, int ncell, float *w1, float *w2, const float *beta, double maser_chi_floor,
+                               int suppress_masers, int *n_floored, unsigned flags) {
+  TRY(need_init());
+  if (nf < 1 || ncell < 1) return fail(M3D_EINVAL, "m3d_work_to_transfer_units: empty");
+  Staging st(flags);
+  const size_t n = (size_t)nf * ncell;
+  float *d1, *d2;
+  const float *db;
+  int *dcnt;
+  TRY(st.map(w1, n, true, true, &d1)); TRY(st.map(w2, n, true, true, &d2)); TRY(st.in(beta, n, &db));
+  void *cnt;
+  TRY(scratch(0, sizeof(int), &cnt));
+  dcnt = (int *)cnt;
+  CUDA_TRY(cudaMemsetAsync(dcnt, 0, sizeof(int), g_ctx.stream));
+  LAUNCH(k_transfer_units, grid_for(n), 256, 0, n, d1, d2, db, (float)maser_chi_floor, suppress_masers, dcnt);
+  if (n_floored) {
+    if (st.device()) {
+      CUDA_TRY(cudaMemcpyAsync(n_floored, dcnt, sizeof(int), cudaMemcpyDeviceToDevice, g_ctx.stream));
+    } else {
+      CUDA_TRY(cudaMemcpyAsync(n_floored, dcnt, sizeof(int), cudaMemcpyDeviceToHost, g_ctx.stream));
+    }
+  }
+  return st.finish();
+}
+
+int m3d_integrate_intensity(int n, float wmu, const float *inu, const float *psi, float *Jnu, float *PsiJ,
+                            unsigned flags) {
+  TRY(need_init());
+  if (n < 1) return M3D_OK;
+  Staging st(flags);
+  const float *di, *dp = nullptr;
+  float *dJ, *dPJ = nullptr;
+  TRY(st.in(inu, n, &di));
+  TRY(st.map(Jnu, n, true, true, &dJ));
+  if (psi && PsiJ) {
+    TRY(st.in(psi, n, &dp));
+    TRY(st.map(PsiJ, n, true, true, &dPJ));
+  }
+  LAUNCH(k_integrate_intensity, grid_for(n), 256, 0, (size_t)n, wmu, di, dp, dJ, dPJ);
+  return st.finish();
+}
+
+}  // extern "C"
+
+namespace {
+
+template <typename T>
+int rotate_impl(const m3d_slab_t *s, T *dwork, const double *ds_code, double bot2pivot, const double *ray_offset) {
+  const int nf = s->nf, nx = s->nx, ny = s->ny, nz = s->nz;
+  std::vector<RotPlane> h(nz);
+  const double off0[2] = {0.0, 0.0};
+  rot_planes(s->vec, ds_code, bot2pivot, ray_offset ? ray_offset : off0, nz, h.data());
+  void *drot, *tmp;
+  TRY(scratch(1, sizeof(RotPlane) * nz, &drot));
+  const size_t plane = (size_t)nf * nx * ny;
+  TRY(scratch(2, sizeof(T) * plane * nz * 2, &tmp));
+  CUDA_TRY(cudaMemcpyAsync(drot, h.data(), sizeof(RotPlane) * nz, cudaMemcpyHostToDevice, g_ctx.stream));
+  // rotate slot 0 planes 1..nz and slot 1 planes 1..nz: both views are contiguous
+  for (int k = 0; k < 2; k++) {
+    T *src = dwork + plane * (1 + (size_t)k * (nz + 2));
+    LAUNCH_S(M3D_STAGE_SOLVE, k_rotate_planes<T>, grid_for(plane * nz), 256, 0, nf, nx, ny, nz, (const T *)src,
+           (T *)tmp + plane * nz * k, (const RotPlane *)drot);
+  }
+  for (int k = 0; k < 2; k++)
+    CUDA_TRY(cudaMemcpyAsync(dwork + plane * (1 + (size_t)k * (nz + 2)), (T *)tmp + plane * nz * k,
+                             sizeof(T) * plane * nz, cudaMemcpyDeviceToDevice, g_ctx.stream));
+  CUDA_TRY(cudaStreamSynchronize(g_ctx.stream));
+  return M3D_OK;
+}
+
+template <typename T>
+int solve_impl(int solver, const m3d_slab_t *s, unsigned flags, T *work, T *psi, T *irem, T *esc,
+               const float *chi500, const float *chi500_up, const float *g500, const int *eta_row,
+               const unsigned char *eta_mask) {
+  const SlabArgs a = slab_args(s, flags);
+  const size_t ncol = (size_t)a.nf * a.nx * a.ny;
+  if (a.get_psi && !psi) return fail(M3D_EINVAL, "get_psi without psi");
+  if (a.split_rates && (!irem || !esc)) return fail(M3D_EINVAL, "split_rates without irem/escape");
+  const int block = 256;
+  const int grid = (int)((ncol + block - 1) / block);
+  switch (solver) {
+    case M3D_SOLVER_LINEAR: {
+      const float ds = (float)s->ds[2];
+      const T dsup05 = (T)(float)((double)(0.5f * ds) / fabs(s->vec[2]));
+      LAUNCH_S(M3D_STAGE_SOLVE, k_long_char_linear<T>, grid, block, 0, a, work, psi, irem, esc, dsup05);
+      return M3D_OK;
+    }
+    case M3D_SOLVER_LINEAR2: {
+      if (!chi500 || !g500) return fail(M3D_EINVAL, "linear2 needs chi500 and g500");
+      LAUNCH_S(M3D_STAGE_SOLVE, k_long_char2<T>, grid, block, 0, a, work, psi, irem, esc, chi500, g500, eta_row,
+             (const uint8_t *)eta_mask, s->ds[2] / fabs(s->vec[2]));
+      return M3D_OK;
+    }
+    case M3D_SOLVER_QUADRATIC: {
+      LAUNCH_S(M3D_STAGE_SOLVE, k_long_char_quadratic<T>, grid, block, 0, a, work, psi, quad_const(s->ds[2], s->vec[2]));
+      return M3D_OK;
+    }
+    case M3D_SOLVER_SHORT_LINEAR:
+    case M3D_SOLVER_SHORT_LINEAR2: {
+      double xk[4], yk[4], dsup;
+      int upo1, upo2;
+      set_stencil(s->ds, s->vec, xk, yk, &upo1, &upo2, &dsup);
+      std::vector<int> tab(4 * (a.nx + a.ny));
+      for (int x = 0; x < a.nx; x++)
+        for (int ii = 0; ii < 4; ii++) {
+          int v = ((ii + 1) + (x + 1) + (upo1 - 2)) % a.nx;
+          tab[4 * x + ii] = v < 0 ? v + a.nx : v;
+        }
+      for (int y = 0; y < a.ny; y++)
+        for (int jj = 0; jj < 4; jj++) {
+          int v = ((jj + 1) + (y + 1) + (upo2 - 2)) % a.ny;
+          tab[4 * a.nx + 4 * y + jj] = v < 0 ? v + a.ny : v;
+        }
+      void *dtab;
+      TRY(scratch(3, sizeof(int) * tab.size(), &dtab));
+      CUDA_TRY(cudaMemcpyAsync(dtab, tab.data(), sizeof(int) * tab.size(), cudaMemcpyHostToDevice, g_ctx.stream));
+      const int *xt = (const int *)dtab, *yt = xt + 4 * a.nx;
+      const float4 kx = make_float4((float)xk[0], (float)xk[1], (float)xk[2], (float)xk[3]);
+      const float4 ky = make_float4((float)yk[0], (float)yk[1], (float)yk[2], (float)yk[3]);
+      const int zs = a.dir > 0 ? 1 : a.nz;
+      if (solver == M3D_SOLVER_SHORT_LINEAR) {
+        const T dsup05 = (T)(0.5f * (float)dsup);
+        for (int i = 0, z = zs; i < a.nz; i++, z += a.dir)
+          LAUNCH_S(M3D_STAGE_SOLVE, k_short_char_plane<T>, grid, block, 0, a, z, work, psi, irem, esc, xt, yt, kx, ky, dsup05);
+      } else {
+        if (!chi500 || !chi500_up || !g500) return fail(M3D_EINVAL, "linear2 needs chi500, chi500_up and g500");
+        const float hx = 2.0f * kx.w + (-kx.x + kx.z), hy = 2.0f * ky.w + (-ky.x + ky.z);
+        for (int i = 0, z = zs; i < a.nz; i++, z += a.dir)
+          LAUNCH_S(M3D_STAGE_SOLVE, k_short_char2_plane<T>, grid, block, 0, a, z, work, psi, irem, esc, xt, yt, kx, ky, hx, hy, chi500,
+                 chi500_up, g500, eta_row, (const uint8_t *)eta_mask, dsup);
+      }
+      CUDA_TRY(cudaStreamSynchronize(g_ctx.stream));
+      return M3D_OK;
+    }
+  }
+  return fail(M3D_EINVAL, "unknown solver %d", solver);
+}
+
+template <typename T>
+int formal_solve_t(int solver, const m3d_slab_t *s, void *work, void *psi, void *irem, void *escape,
+                   const float *chi500, const float *chi500_up, const float *g500, const int *eta_row,
+                   const unsigned char *eta_mask, const double *rot_ds_code, double rot_bot2pivot,
+                   const double *rot_offset, unsigned flags) {
+  Staging st(flags);
+  const size_t nw = (size_t)s->nf * s->nx * s->ny * (s->nz + 2) * 3;
+  const size_t np = (size_t)s->nf * s->nx * s->ny * s->nz;
+  const size_t nc = (size_t)s->nx * s->ny * s->nz;
+  const SlabArgs a = slab_args(s, flags);
+  T *dw, *dp = nullptr, *dir_ = nullptr, *de = nullptr;
+  TRY(st.map((T *)work, nw, true, true, &dw));
+  if (a.get_psi) TRY(st.map((T *)psi, np, true, true, &dp));
+  if (a.split_rates) {
+    TRY(st.map((T *)irem, np, true, true, &dir_));
+    TRY(st.map((T *)escape, np, true, true, &de));
+  }
+  const float *c5 = nullptr, *c5u = nullptr, *g5 = nullptr;
+  const int *er = nullptr;
+  const unsigned char *em = nullptr;
+  if (solver == M3D_SOLVER_LINEAR2 || solver == M3D_SOLVER_SHORT_LINEAR2) {
+    TRY(st.in(chi500, nc, &c5));
+    TRY(st.in(g500, (size_t)s->nx * s->ny, &g5));
+    if (solver == M3D_SOLVER_SHORT_LINEAR2) TRY(st.in(chi500_up, nc, &c5u));
+    if (eta_row) {
+      TRY(st.in(eta_row, nc, &er));
+      if (!eta_mask) return fail(M3D_EINVAL, "eta_row without eta_mask");
+      int nrows = 0;
+      if (st.device()) {
+        return fail(M3D_EUNSUPPORTED, "eta flags with device pointers: pass host buffers");
+      }
+      for (size_t i = 0; i < nc; i++) nrows = eta_row[i] > nrows ? eta_row[i] : nrows;
+      TRY(st.in(eta_mask, (size_t)s->nf * (nrows > 0 ? nrows : 1), &em));
+    }
+  }
+  if ((flags & M3D_ROTATE) && solver == M3D_SOLVER_QUADRATIC) {
+    if (!rot_ds_code) return fail(M3D_EINVAL, "M3D_ROTATE needs rot_ds_code");
+    TRY(rotate_impl<T>(s, dw, rot_ds_code, rot_bot2pivot, rot_offset));
+  }
+  TRY(solve_impl<T>(solver, s, flags, dw, dp, dir_, de, c5, c5u, g5, er, em));
+  return st.finish();
+}
+
+template <typename T>
+int boundary_t(const m3d_slab_t *s, void *work, int mode, const void *mem, float ds3_code, const float *ghost_r500,
+               const float *ghost_temp, const double *nu, unsigned flags) {
+  Staging st(flags);
+  const size_t plane = (size_t)s->nf * s->nx * s->ny;
+  const size_t nw = plane * (s->nz + 2) * 3;
+  T *dw;
+  const T *dm = nullptr;
+  const float *dr = nullptr, *dt = nullptr;
+  const double *dnu = nullptr;
+  TRY(st.map((T *)work, nw, true, true, &dw));
+  if (mode == M3D_BND_MEM) {
+    if (!mem) return fail(M3D_EINVAL, "M3D_BND_MEM needs mem");
+    TRY(st.in((const T *)mem, plane * 3, &dm));
+  } else if (mode == M3D_BND_LTE) {
+    if (!ghost_r500 || !ghost_temp || !nu) return fail(M3D_EINVAL, "M3D_BND_LTE needs ghost_r500, ghost_temp, nu");
+    TRY(st.in(ghost_r500, (size_t)s->nx * s->ny, &dr));
+    TRY(st.in(ghost_temp, (size_t)s->nx * s->ny, &dt));
+    TRY(st.in(nu, s->nf, &dnu));
+  } else if (mode != M3D_BND_ZERO && mode != M3D_BND_PCHIP) {
+    return fail(M3D_EINVAL, "unknown boundary mode %d", mode);
+  }
+  LAUNCH(k_upstream_boundary<T>, grid_for(plane), 256, 0, s->nf, s->nx, s->ny, s->nz, s->dir, dw, mode, dm,
+         pchip_const(ds3_code), dr, dt, dnu);
+  return st.finish();
+}
+
+}  // namespace
+
+extern "C" {
+
+int m3d_formal_solve(int solver, const m3d_slab_t *slab, void *work, void *psi, void *irem, void *escape,
+                     const float *chi500, const float *chi500_up, const float *g500, const int *eta_row,
+                     const unsigned char *eta_mask, const double *rot_ds_code, double rot_bot2pivot,
+                     const double *rot_offset, unsigned flags) {
+  TRY(need_init());
+  TRY(check_slab(slab));
+  if (!work) return fail(M3D_EINVAL, "work is NULL");
+  if (flags & M3D_FP64)
+    return formal_solve_t<double>(solver, slab, work, psi, irem, escape, chi500, chi500_up, g500, eta_row, eta_mask,
+                                  rot_ds_code, rot_bot2pivot, rot_offset, flags);
+  return formal_solve_t<float>(solver, slab, work, psi, irem, escape, chi500, chi500_up, g500, eta_row, eta_mask,
+                               rot_ds_code, rot_bot2pivot, rot_offset, flags);
+}
+
+int m3d_rotate_array(const m3d_slab_t *slab, void *work, const double *ds_code, double bot2pivot,
+                     const double *ray_offset, unsigned flags) {
+  TRY(need_init());
+  TRY(check_slab(slab));
+  if (!work || !ds_code) return fail(M3D_EINVAL, "m3d_rotate_array: NULL work or ds_code");
+  const size_t nw = (size_t)slab->nf * slab->nx * slab->ny * (slab->nz + 2) * 3;
+  Staging st(flags);
+  if (flags & M3D_FP64) {
+    double *dw;
+    TRY(st.map((double *)work, nw, true, true, &dw));
+    TRY(rotate_impl<double>(slab, dw, ds_code, bot2pivot, ray_offset));
+  } else {
+    float *dw;
+    TRY(st.map((float *)work, nw, true, true, &dw));
+    TRY(rotate_impl<float>(slab, dw, ds_code, bot2pivot, ray_offset));
+  }
+  return st.finish();
+}
+
+int m3d_upstream_boundary(const m3d_slab_t *slab, void *work, int mode, const void *mem, float ds3_code,
+                          const float *ghost_r500, const float *ghost_temp, const double *nu, unsigned flags) {
+  TRY(need_init());
+  TRY(check_slab(slab));
+  if (!work) return fail(M3D_EINVAL, "work is NULL");
+  if (flags & M3D_FP64) return boundary_t<double>(slab, work, mode, mem, ds3_code, ghost_r500, ghost_temp, nu, flags);
+  return boundary_t<float>(slab, work, mode, mem, ds3_code, ghost_r500, ghost_temp, nu, flags);
+}
+
+// ---------------------------------------------------------------------------
+// LTE synthesis output pass of one window
+// ---------------------------------------------------------------------------
+int m3d_lte_synthesis(const m3d_atmos_t *atm, int nf, const double *nu, const double *llam, int nray,
+                      const double *vec, const double *wmu, void *i_top, float *ie, float *flux, unsigned flags) {
+  TRY(need_init());
+  if (!atm || !nu || !llam || !vec || !wmu || !ie || !flux) return fail(M3D_EINVAL, "m3d_lte_synthesis: NULL argument");
+  if (nf < 2 || nray < 1) return fail(M3D_EINVAL, "m3d_lte_synthesis: need nf >= 2 and nray >= 1");
+  if (nf > 1024) return fail(M3D_EUNSUPPORTED, "m3d_lte_synthesis: nf = %d > 1024 per window", nf);
+  const int nx = atm->nx, ny = atm->ny, nz = atm->nz;
+  if (nx < 1 || ny < 1 || nz < 2 || atm->nslab < 1 || !atm->slab_nz) return fail(M3D_EINVAL, "m3d_lte_synthesis: bad atmosphere shape");
+  std::vector<int> z0(atm->nslab + 1, 0);
+  for (int s = 0; s < atm->nslab; s++) {
+    if (atm->slab_nz[s] < 2) return fail(M3D_EINVAL, "slab %d has %d < 2 planes", s, atm->slab_nz[s]);
+    z0[s + 1] = z0[s] + atm->slab_nz[s];
+  }
+  if (z0[atm->nslab] != nz) return fail(M3D_EINVAL, "slab planes sum to %d, not nz = %d", z0[atm->nslab], nz);
+  for (int r = 0; r < nray; r++)
+    if (!(vec[3 * r + 2] > 0)) return fail(M3D_EINVAL, "ray %d is not upward (vec(3) <= 0)", r);
+  const bool fp64 = flags & M3D_FP64;
+  const size_t ncell = (size_t)nx * ny * nz;
+  const size_t ncol = (size_t)nx * ny;
+  const size_t plane = (size_t)nf * ncol;
+
+  Staging st(flags);
+  AtmosDev A;
+  A.ncell = (int)ncell;
+  TRY(st.in(atm->temp, ncell, &A.temp)); TRY(st.in(atm->chi_c, ncell, &A.chi_c));
+  TRY(st.in(atm->vx, ncell, &A.vx)); TRY(st.in(atm->vy, ncell, &A.vy)); TRY(st.in(atm->vz, ncell, &A.vz));
+  TRY(st.in(atm->e_kT, ncell, &A.e_kT)); TRY(st.in(atm->ne, ncell, &A.ne));
+  TRY(st.in(atm->tothi, ncell, &A.tothi)); TRY(st.in(atm->stark_pe, ncell, &A.stark_pe));
+  if (!A.temp || !A.chi_c || !A.vx || !A.vy || !A.vz || !A.e_kT || !A.ne || !A.tothi || !A.stark_pe)
+    return fail(M3D_EINVAL, "m3d_lte_synthesis: NULL atmosphere field");
+  A.maser_chi_floor = (float)atm->maser_chi_floor;
+  A.nspecies = atm->nspecies;
+  std::vector<SpeciesDev> sp(atm->nspecies > 0 ? atm->nspecies : 1);
+  for (int k = 0; k < atm->nspecies; k++) {
+    TRY(stage_linelist(st, &atm->species[k].ll, &sp[k].L));
+    TRY(st.in(atm->species[k].inv_df, ncell, &sp[k].inv_df));
+    TRY(st.in(atm->species[k].vbar2, ncell, &sp[k].vbar2));
+    TRY(st.in(atm->species[k].lnbase, ncell, &sp[k].lnbase));
+  }
+  void *dsp;
+  TRY(scratch(4, sizeof(SpeciesDev) * sp.size(), &dsp));
+  CUDA_TRY(cudaMemcpyAsync(dsp, sp.data(), sizeof(SpeciesDev) * sp.size(), cudaMemcpyHostToDevice, g_ctx.stream));
+  A.species = (const SpeciesDev *)dsp;
+  const double *dnu, *dllam;
+  TRY(st.in(nu, nf, &dnu));
+  TRY(st.in(llam, nf, &dllam));
+  GridArgs G = grid_args(nf, llam, dllam, st.device(), (float)atm->tol, 0.0f);
+  if (!(G.dllam > 0)) return fail(M3D_EINVAL, "m3d_lte_synthesis: log(lambda) grid must be ascending");
+
+  // rotation table of every global plane, per ray; slab starts
+  // A single column is a plane-parallel atmosphere: radiative_transfer applies no
+  // rotate_array there (rt_patch_mod.f90:1670), so its planes keep identity weights.
+  const bool one_d = nx == 1 && ny == 1;
+  std::vector<RotPlane> rot((size_t)nray * nz);
+  for (int r = 0; r < nray; r++)
+    for (int s = 0; s < atm->nslab; s++) {
+      const float bottom = (float)((double)z0[s] * atm->ds_code[2]);
+      const double b2p = atm->pivot_z - (double)bottom;
+      RotPlane *out = rot.data() + (size_t)r * nz + z0[s];
+      if (one_d) {
+        for (int z = 0; z < atm->slab_nz[s]; z++) out[z] = RotPlane{0, 0, 1.0f, 0.0f, 0.0f, 0.0f};
+      } else {
+        rot_planes(vec + 3 * r, atm->ds_code, b2p, atm->ray_offset, atm->slab_nz[s], out);
+      }
+    }
+  void *drot, *dz0;
+  TRY(scratch(5, sizeof(RotPlane) * rot.size(), &drot));
+  TRY(scratch(6, sizeof(int) * z0.size(), &dz0));
+  CUDA_TRY(cudaMemcpyAsync(drot, rot.data(), sizeof(RotPlane) * rot.size(), cudaMemcpyHostToDevice, g_ctx.stream));
+  CUDA_TRY(cudaMemcpyAsync(dz0, z0.data(), sizeof(int) * z0.size(), cudaMemcpyHostToDevice, g_ctx.stream));
+
+  // transfer units of the whole column (one ray at a time) and the emergent planes
+  const size_t esz = fp64 ? sizeof(double) : sizeof(float);
+  void *dchi, *dS, *dtop;
+  TRY(scratch(7, esz * plane * nz, &dchi));
+  TRY(scratch(8, esz * plane * nz, &dS));
+  void *dtop_user = nullptr;
+  if (i_top) {
+    if (fp64) { double *p; TRY(st.map((double *)i_top, plane * nray, false, true, &p)); dtop_user = p; }
+    else { float *p; TRY(st.map((float *)i_top, plane * nray, false, true, &p)); dtop_user = p; }
+    dtop = dtop_user;
+  } else {
+    TRY(scratch(9, esz * plane * nray, &dtop));
+  }
+  float *die;
+  TRY(st.map(ie, (size_t)nf * nray, false, true, &die));
+
+  const int block = 256, warps = block / 32;
+  const size_t smem_op = (2 * QLG_NTAB + (size_t)warps * 4 * nf) * sizeof(float);
+  {
+    static size_t attr32 = 0, attr64 = 0;
+    if (!fp64 && attr32 < smem_op) {
+      CUDA_TRY(cudaFuncSetAttribute(k_lte_opacity_units<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_op));
+      attr32 = smem_op;
+    }
+    if (fp64 && attr64 < smem_op) {
+      CUDA_TRY(cudaFuncSetAttribute(k_lte_opacity_units<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_op));
+      attr64 = smem_op;
+    }
+  }
+  int ogrid = (int)((ncell + warps - 1) / warps);
+  if (ogrid > 148 * 16) ogrid = 148 * 16;
+  const float dtmax = -(float)atm->maser_dtau_max, Imax = (float)atm->maser_Inu_max;
+  const PchipConst pc = pchip_const((float)atm->ds_code[2]);
+
+  // FP64 plain path buffers
+  void *dwork = nullptr, *dmem = nullptr;
+  int maxn = 0;
+  for (int s = 0; s < atm->nslab; s++) maxn = atm->slab_nz[s] > maxn ? atm->slab_nz[s] : maxn;
+  if (fp64) {
+    TRY(scratch(10, sizeof(double) * plane * (maxn + 2) * 3, &dwork));
+    TRY(scratch(11, sizeof(double) * plane * 3, &dmem));
+  }
+
+  for (int r = 0; r < nray; r++) {
+    const double *v = vec + 3 * r;
+    if (!fp64) {
+      LAUNCH_S(M3D_STAGE_OPACITY, k_lte_opacity_units<float>, ogrid, block, smem_op, A, G, dnu, v[0], v[1], v[2], (float *)dchi, (float *)dS,
+             g_ctx.d_tgx, g_ctx.d_th2x);
+      const QuadConst qc = quad_const(atm->ds_cm[2], v[2]);
+      LAUNCH_S(M3D_STAGE_SOLVE, k_quad_rot_column, (int)((plane + 255) / 256), 256, 0, nf, nx, ny, nz, (const float *)dchi, (const float *)dS, (const RotPlane *)drot + (size_t)r * nz,
+             (const int *)dz0, atm->nslab, qc, pc, dtmax, Imax, (float *)dtop + plane * r);
+      dim3 sb(32, 8);
+      LAUNCH_S(M3D_STAGE_REDUCE, k_save_intensity<float>, (nf + 31) / 32, sb, 0, nf, (int)ncol, dnu, (const float *)dtop + plane * r,
+             die + (size_t)nf * r);
+    } else {
+      LAUNCH_S(M3D_STAGE_OPACITY, k_lte_opacity_units<double>, ogrid, block, smem_op, A, G, dnu, v[0], v[1], v[2], (double *)dchi,
+             (double *)dS, g_ctx.d_tgx, g_ctx.d_th2x);
+      for (int s = 0; s < atm->nslab; s++) {
+        const int n = atm->slab_nz[s];
+        m3d_slab_t sl;
+        memset(&sl, 0, sizeof sl);
+        sl.nf = nf; sl.nx = nx; sl.ny = ny; sl.nz = n; sl.dir = 1;
+        for (int i = 0; i < 3; i++) { sl.ds[i] = atm->ds_cm[i]; sl.vec[i] = v[i]; }
+        sl.maser_dtau_max = atm->maser_dtau_max;
+        sl.maser_Inu_max = atm->maser_Inu_max;
+        double *w = (double *)dwork;
+        LAUNCH(k_slab_in, grid_for(plane * n), 256, 0, plane, n, (const double *)dchi + plane * z0[s],
+               (const double *)dS + plane * z0[s], w, n);
+        LAUNCH(k_upstream_boundary<double>, grid_for(plane), 256, 0, nf, nx, ny, n, 1, w, s == 0 ? M3D_BND_PCHIP : M3D_BND_MEM,
+               (const double *)dmem, pc, (const float *)nullptr, (const float *)nullptr, (const double *)nullptr);
+        const float bottom = (float)((double)z0[s] * atm->ds_code[2]);
+        if (!one_d) TRY(rotate_impl<double>(&sl, w, atm->ds_code, atm->pivot_z - (double)bottom, atm->ray_offset));
+        TRY(solve_impl<double>(M3D_SOLVER_QUADRATIC, &sl, 0, w, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
+                               nullptr, nullptr));
+        // exit plane -> mem (chi, S, I at plane n)
+        for (int k = 0; k < 3; k++)
+          CUDA_TRY(cudaMemcpyAsync((double *)dmem + plane * k, w + plane * ((size_t)n + (size_t)k * (n + 2)),
+                                   sizeof(double) * plane, cudaMemcpyDeviceToDevice, g_ctx.stream));
+      }
+      CUDA_TRY(cudaMemcpyAsync((double *)dtop + plane * r, (double *)dmem + 2 * plane, sizeof(double) * plane,
+                               cudaMemcpyDeviceToDevice, g_ctx.stream));
+      dim3 sb(32, 8);
+      LAUNCH_S(M3D_STAGE_REDUCE, k_save_intensity<double>, (nf + 31) / 32, sb, 0, nf, (int)ncol, dnu, (const double *)dtop + plane * r,
+             die + (size_t)nf * r);
+    }
+  }
+  TRY(st.finish());
+  // flux = 2 pi sum_mu wmu ie (rt_patch_mod.f90:4193-4200), ie now on the host or device
+  std::vector<float> hie((size_t)nf * nray);
+  if (st.device()) {
+    CUDA_TRY(cudaMemcpyAsync(hie.data(), ie, sizeof(float) * hie.size(), cudaMemcpyDeviceToHost, g_ctx.stream));
+    CUDA_TRY(cudaStreamSynchronize(g_ctx.stream));
+  } else {
+    memcpy(hie.data(), ie, sizeof(float) * hie.size());
+  }
+  std::vector<float> hflux(nf, 0.0f);
+  for (int r = 0; r < nray; r++) {
+    const float w = (float)(2.0 * 3.14159265359 * wmu[r]);
+    for (int f = 0; f < nf; f++) hflux[f] = fmaf(w, hie[(size_t)f + (size_t)nf * r], hflux[f]);
+  }
+  if (st.device()) {
+    CUDA_TRY(cudaMemcpyAsync(flux, hflux.data(), sizeof(float) * nf, cudaMemcpyHostToDevice, g_ctx.stream));
+    CUDA_TRY(cudaStreamSynchronize(g_ctx.stream));
+  } else {
+    memcpy(flux, hflux.data(), sizeof(float) * nf);
+  }
+  return M3D_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,693 @@
+// sm_100a kernels of the radiative-transfer hot path.  Every array uses the
+// reference's layout, frequency fastest, so consecutive threads own consecutive
+// frequencies of one (x, y) column and every access along a sweep is coalesced.
+#pragma once
+#include <cstdint>
+
+#include "m3d_math.cuh"
+#include "m3d_qlg.cuh"
+
+namespace m3d {
+
+__device__ __forceinline__ size_t iw(int f, int x, int y, int z, int k, int nf, int nx, int ny, int nz) {
+  return (size_t)f + (size_t)nf * ((size_t)x + (size_t)nx * ((size_t)y + (size_t)ny * ((size_t)z + (size_t)(nz + 2) * (size_t)k)));
+}
+__device__ __forceinline__ size_t ip(int f, int x, int y, int z, int nf, int nx, int ny) {
+  return (size_t)f + (size_t)nf * ((size_t)x + (size_t)nx * ((size_t)y + (size_t)ny * (size_t)(z - 1)));
+}
+__device__ __forceinline__ size_t ic3(int x, int y, int z, int nx, int ny) {
+  return (size_t)x + (size_t)nx * ((size_t)y + (size_t)ny * (size_t)(z - 1));
+}
+__device__ __forceinline__ int wrap(int v, int n) { v %= n; return v < 0 ? v + n : v; }
+
+constexpr double M3D_H_K = 6.626176e-27 / 1.380662e-16;  // h/k (const_mod.f90:39,43,71)
+
+template <typename T> __device__ __forceinline__ T tmin(T a, T b) { return a < b ? a : b; }
+template <typename T> __device__ __forceinline__ T tmax(T a, T b) { return a > b ? a : b; }
+__device__ __forceinline__ float tmin(float a, float b) { return fminf(a, b); }
+__device__ __forceinline__ float tmax(float a, float b) { return fmaxf(a, b); }
+__device__ __forceinline__ double tmin(double a, double b) { return fmin(a, b); }
+__device__ __forceinline__ double tmax(double a, double b) { return fmax(a, b); }
+__device__ __forceinline__ float tabs(float a) { return fabsf(a); }
+__device__ __forceinline__ double tabs(double a) { return fabs(a); }
+__device__ __forceinline__ float tcopysign(float a, float b) { return copysignf(a, b); }
+__device__ __forceinline__ double tcopysign(double a, double b) { return copysign(a, b); }
+
+
+// ----------------------------------------------------------------------------
+// K0 diagnostics: the weights elementwise
+// ----------------------------------------------------------------------------
+__global__ void k_weights_f32(int which, int n, const float *t, float *o1, float *o2, float *o3, float *o4) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float x = t[i];
+    switch (which) {
+      case 0: { float E, u; exp_neg(x, E, u); o1[i] = E; o2[i] = u; } break;
+      case 1: { float E, W, P, S; linear_weights(x, E, W, P, S); o1[i] = E; o2[i] = W; o3[i] = P; o4[i] = S; } break;
+      case 2: { float E, U0, U1, q; parab_moments(x, E, U0, U1, q); o1[i] = E; o2[i] = U0; o3[i] = U1; o4[i] = q; } break;
+      case 3: o1[i] = exp4(x); break;
+      default: o1[i] = logf_m3d(x); break;
+    }
+  }
+}
+
+__global__ void k_weights_f64(int which, int n, const double *t, double *o1, double *o2, double *o3, double *o4) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double x = t[i];
+    if (which == 1) { double E, W, P, S; linear_weights(x, E, W, P, S); o1[i] = E; o2[i] = W; o3[i] = P; o4[i] = S; }
+    else { double E, U0, U1, q; parab_moments(x, E, U0, U1, q); o1[i] = E; o2[i] = U0; o3[i] = U1; o4[i] = q; }
+  }
+}
+
+// qlg_bot_profile (qlg_mod.f90:682-689)
+__global__ void k_qlg_profile(int n, const float *tgx, const float *th2x, const float *a, const float *q,
+                              const float *vpr, const float *idf, float *h) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float v = fabsf(q[i] - vpr[i]) * idf[i];
+    const QlgCoef c = qlg_setup(a[i], 1.0f, 0.8325546112f, 1.7724538509f);
+    const float K1 = qlg_eval(tgx, th2x, c, v);
+    h[i] = ((K1 * 0.5641895835f) * idf[i]) * (q[i] + 1.0f);
+  }
+}
+
+// ----------------------------------------------------------------------------
+// Line opacity of one cell by one warp (add_opacity_equi, linelist_mod.f90:729-960)
+// ----------------------------------------------------------------------------
+struct LineArgs {
+  int nline;
+  const double *llam0;
+  const float *lower_ev, *gpref, *grad, *gw1, *gw2, *gstk;
+  const uint8_t *unsold;
+  const int *lev_i, *lev_j;
+  const uint8_t *active;
+};
+
+struct GridArgs {
+  int nf;
+  const double *llam;
+  double llam1, inv_dllam, dllam;
+  float sdl, tol, flo_scale;
+};
+
+struct CellArgs {
+  float idf, vbar2, ekt, ne, tothi, starkpe, vproj, base;
+};
+
+__device__ __forceinline__ float line_damping_a(const LineArgs &L, int l, float unsold_c, float lvb2,
+                                                float tothi, float ne, float starkpe) {
+  float a = L.grad[l];
+  if (L.unsold[l]) a = fmaf(L.gw1[l], unsold_c, a);
+  else a = fmaf(L.gw1[l] * exp4(L.gw2[l] * lvb2), tothi, a);
+  const float gs = L.gstk[l];
+  if (gs >= 0.0f) a = fmaf(gs, ne, a);
+  else a = fmaf(-gs, starkpe, a);
+  return a;
+}
+
+// chi, eta, cont, logref point at this cell's nf values (shared or global memory).
+// dep(level) returns the departure coefficient of a 1-based level of this cell.
+// diag: strength/reach/used as the reference updates them.  Lanes of the warp
+// first screen 32 lines at a time against the unfloored tolerance reference and
+// window (a superset of the lines the exact test keeps, since the floor only
+// raises the reference), then the candidates go through the exact test in line
+// order, so chi accumulates in exactly the reference's order.
+template <class DepFn>
+__device__ void warp_cell_lines(const LineArgs &L, const GridArgs &G, const CellArgs &c, float *chi, float *eta,
+                                const float *cont, const float *logref, DepFn dep, bool do_nlte, bool diag,
+                                uint8_t *used, float *strength, float *reach, const float *tgx,
+                                const float *th2x, int lane) {
+  const float ex_cutoff = -85.0f, voigt_peak = 0.5641895835f, sqrt_pi = 1.7724538509f;
+  const int nf = G.nf;
+  const QlgCell qw = qlg_cell(G.sdl / c.idf);
+  const float lvb2 = logf_m3d(c.vbar2);
+  const float unsold_c = exp4(0.3f * lvb2) * c.tothi;
+  for (int l0 = 0; l0 < L.nline; l0 += 32) {
+    const int l = l0 + lane;
+    bool cand = false;
+    if (l < L.nline && (L.active == nullptr || L.active[l])) {
+      const double llc = L.llam0[l] - (double)c.vproj;
+      const double pos = (llc - G.llam1) * G.inv_dllam;
+      const int ic = (int)lround(pos) + 1;
+      const int f0 = ic < 1 ? 1 : (ic > nf ? nf : ic);
+      const float ex = L.lower_ev[l] * c.ekt;
+      const float arg = (c.base + L.gpref[l]) - ex;
+      if (!(arg < ex_cutoff)) {
+        const float lr = logref[f0 - 1];
+        if (arg > lr - 1e-3f) {
+          const float Rij = exp4(arg);
+          const float ref0 = G.tol * cont[f0 - 1];
+          if (voigt_peak * Rij > ref0) {
+            if (diag) {
+              cand = true;
+            } else {
+              const float a = line_damping_a(L, l, unsold_c, lvb2, c.tothi, c.ne, c.starkpe) * G.sdl;
+              const float hw = qlg_halfwidth(qw, a, Rij * qw.D, ref0, (arg - lr) + 1e-3f);
+              const int noff = (int)lroundf(fminf(fmaf(hw, 1.001f, 1.0f), (float)(nf + abs(ic))));
+              cand = (ic - noff <= nf) && (ic + noff >= 1);
+            }
+          }
+        }
+      }
+    }
+    unsigned m = __ballot_sync(0xffffffffu, cand);
+    while (m) {
+      const int j = __ffs(m) - 1;
+      m &= m - 1;
+      const int ln = l0 + j;
+      const double llc = L.llam0[ln] - (double)c.vproj;
+      const double pos = (llc - G.llam1) * G.inv_dllam;
+      const int ic = (int)lround(pos) + 1;
+      const int f0 = ic < 1 ? 1 : (ic > nf ? nf : ic);
+      const float ex = L.lower_ev[ln] * c.ekt;
+      const float arg = (c.base + L.gpref[ln]) - ex;
+      float refl = G.tol * cont[f0 - 1];
+      const float flo = G.flo_scale * chi[f0 - 1];
+      float lref;
+      if (flo > refl) { refl = flo; lref = logf_m3d(flo * sqrt_pi); }
+      else lref = logref[f0 - 1];
+      if (arg <= lref) continue;
+      const float Rij = exp4(arg);
+      if (voigt_peak * Rij <= refl) continue;
+      float bi = 1.0f, bj = 1.0f;
+      if (do_nlte && L.lev_i && L.lev_j && L.lev_i[ln] > 0 && L.lev_j[ln] > 0) {
+        bi = dep(L.lev_i[ln]);
+        bj = dep(L.lev_j[ln]);
+      }
+      const float a = line_damping_a(L, ln, unsold_c, lvb2, c.tothi, c.ne, c.starkpe) * G.sdl;
+      if (diag && lane == 0) {
+        const float st = (voigt_peak * Rij) / cont[f0 - 1];
+        atomicMax(reinterpret_cast<int *>(strength + ln), __float_as_int(st));
+      }
+      const float lnq = arg - lref;
+      // qlg_bot_line_sweep (qlg_mod.f90:646-671)
+      const float S = Rij * qw.D;
+      const int i1 = f0;
+      const float x1 = (float)((G.llam[i1 - 1] - llc) * G.inv_dllam);
+      const QlgCoef cf = qlg_setup(a, qw.D, qw.SQ, S);
+      const float hw = qlg_halfwidth(qw, a, S, refl, lnq);
+      const int noff = (int)lroundf(fminf(fminf(hw, FLT_MAX), (float)(nf + abs(ic))));
+      const int fa = ic - noff > 1 ? ic - noff : 1;
+      const int fb = ic + noff < nf ? ic + noff : nf;
+      if (diag && lane == 0) {
+        const float rch = (float)((double)hw * G.dllam);
+        atomicMax(reinterpret_cast<int *>(reach + ln), __float_as_int(rch));
+      }
+      if (fa > fb) continue;
+      if (diag && lane == 0) used[ln] = 1;
+      const float x0 = x1 - (float)(i1 - fa);
+      for (int f = fa + lane; f <= fb; f += 32) {
+        const float K = qlg_eval(tgx, th2x, cf, x0 + (float)(f - fa));
+        chi[f - 1] = fmaf(K, bi, chi[f - 1]);
+        eta[f - 1] = fmaf(K, bj, eta[f - 1]);
+      }
+      __syncwarp();
+    }
+  }
+}
+
+__device__ __forceinline__ void stage_tables(float *s_tgx, float *s_th2x, const float *tgx, const float *th2x) {
+  for (int i = threadIdx.x; i < QLG_NTAB; i += blockDim.x) {
+    s_tgx[i] = tgx[i];
+    s_th2x[i] = th2x[i];
+  }
+  __syncthreads();
+}
+
+// m3d_line_opacity: warp per cell, arrays in global memory
+__global__ void __launch_bounds__(256) k_line_opacity(LineArgs L, GridArgs G, int ncell, float *chi, float *eta,
+                                                      const float *cont, const float *logref, const float *vproj,
+                                                      const float *inv_df, const float *vbar2, const float *e_kT,
+                                                      const float *lnbase, const float *ne, const float *tothi,
+                                                      const float *stark_pe, const float *dep_mem, int do_nlte,
+                                                      int diag, uint8_t *used, float *strength, float *reach,
+                                                      const float *tgx, const float *th2x) {
+  extern __shared__ float smem[];
+  float *s_tgx = smem, *s_th2x = smem + QLG_NTAB;
+  stage_tables(s_tgx, s_th2x, tgx, th2x);
+  const int lane = threadIdx.x & 31;
+  const int warps = blockDim.x >> 5;
+  for (int cell = blockIdx.x * warps + (threadIdx.x >> 5); cell < ncell; cell += gridDim.x * warps) {
+    CellArgs c;
+    c.idf = inv_df[cell]; c.vbar2 = vbar2[cell]; c.ekt = e_kT[cell]; c.ne = ne[cell];
+    c.tothi = tothi[cell]; c.starkpe = stark_pe[cell]; c.vproj = vproj[cell]; c.base = lnbase[cell];
+    const size_t o = (size_t)G.nf * cell;
+    auto dep = [&](int lev) { return dep_mem[(size_t)cell + (size_t)ncell * (size_t)(lev - 1)]; };
+    warp_cell_lines(L, G, c, chi + o, eta + o, cont + o, logref + o, dep, do_nlte != 0, diag != 0, used, strength,
+                    reach, s_tgx, s_th2x, lane);
+  }
+}
+
+// lte_background_opacities: beta, Bnu (rt_patch_mod.f90:2004-2023)
+__global__ void k_lte_background(int nf, int ncell, const double *nu, const float *temp, float *beta, float *Bnu) {
+  const size_t n = (size_t)nf * ncell;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+    const int f = (int)(k % nf);
+    const size_t i = k / nf;
+    const float h_kT = (float)(M3D_H_K / (double)temp[i]);
+    const float hv = (float)(nu[f] * (double)h_kT);
+    float E, u0;
+    exp_neg(hv, E, u0);
+    const float b = fmaxf(E, FLT_MIN);
+    beta[k] = b;
+    Bnu[k] = b / (1.0f - b);
+  }
+}
+
+// work_to_transfer_units without split rates or line scattering (rt_patch_mod.f90:3571-3651)
+__global__ void k_transfer_units(size_t n, float *w1, float *w2, const float *beta, float fl, int suppress,
+                                 int *n_floored) {
+  int cnt = 0;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+    const float xhat = w1[k];
+    const float etav = w2[k] * beta[k];
+    float chi = xhat - etav;
+    const float floor_ = fmaxf(fl * fabsf(xhat), FLT_MIN);
+    if (suppress) chi = fmaxf(chi, floor_);
+    else if (fabsf(chi) < floor_) { chi = copysignf(floor_, chi); cnt++; }
+    w1[k] = chi;
+    w2[k] = etav / chi;
+  }
+  if (n_floored && cnt) atomicAdd(n_floored, cnt);
+}
+
+// integrate_intensity (rt_patch_mod.f90:3399-3431)
+__global__ void k_integrate_intensity(size_t n, float wmu, const float *inu, const float *psi, float *Jnu,
+                                      float *PsiJ) {
+  const float w2 = 2.0f * wmu;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+    Jnu[k] = fmaf(w2, inu[k], Jnu[k]);
+    if (psi && PsiJ) PsiJ[k] = fmaf(w2, psi[k], PsiJ[k]);
+  }
+}
+
+// ----------------------------------------------------------------------------
+// Formal solvers
+// ----------------------------------------------------------------------------
+struct SlabArgs {
+  int nf, nx, ny, nz, dir, get_psi, split_rates;
+  double ds[3], vec[3];
+  double maser_dtau_max, maser_Inu_max;
+};
+
+// long_char_linear (rt_solvers_mod.f90:666-757): thread per (f, x, y), z sequential
+template <typename T>
+__global__ void k_long_char_linear(SlabArgs s, T *work, T *psi, T *irem, T *esc, T dsup05) {
+  const size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  const int nf = s.nf, nx = s.nx, ny = s.ny, nz = s.nz, dir = s.dir;
+  if (g >= (size_t)nf * nx * ny) return;
+  const int f = (int)(g % nf), x = (int)((g / nf) % nx), y = (int)(g / ((size_t)nf * nx));
+  const T dtmax = -(T)s.maser_dtau_max, Imax = (T)s.maser_Inu_max;
+  const int zs = dir > 0 ? 1 : nz;
+  const size_t zstride = (size_t)nf * nx * ny;
+  const size_t k1 = zstride * (nz + 2);
+  const size_t b = g;
+  T xxup = work[b + zstride * (zs - dir)], ssup = work[b + zstride * (zs - dir) + k1];
+  T Inuup = work[b + zstride * (zs - dir) + 2 * k1];
+  for (int i = 0, z = zs; i < nz; i++, z += dir) {
+    const size_t o = b + zstride * z;
+    const T xx = work[o], ss = work[o + k1];
+    T dt = dsup05 * (xxup + xx);
+    dt = tmax(dt, dtmax);
+    T E, W, Psi, Esc;
+    linear_weights(dt, E, W, Psi, Esc);
+    T Inu = fma_t(Psi, ss, fma_t(W, ssup, Inuup * E));
+    if (s.split_rates) {
+      const bool off = dt <= 0 || xx <= 0 || tabs(Inu) > Imax;
+      const T Irem = fma_t(W, ssup, Inuup * E);
+      Inu = tmax(-Imax, tmin(Imax, Inu));
+      Psi = off ? (T)0 : Psi;
+      const size_t p = ip(f, x, y, z, nf, nx, ny);
+      irem[p] = off ? Inu : Irem;
+      esc[p] = off ? (T)1 : Esc;
+    } else {
+      Inu = tmax(-Imax, tmin(Imax, Inu));
+    }
+    work[o + 2 * k1] = Inu;
+    if (s.get_psi) psi[ip(f, x, y, z, nf, nx, ny)] = (dt > 0 && xx > 0) ? Psi / xx : (T)0;
+    xxup = xx; ssup = ss; Inuup = Inu;
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ T dt500_of(double dsup, double c, double cu) {
+  const double r = cu / c;
+  if (fabs(r - 1.0) < 1e-3) return (T)(dsup * c * (1.0 + (r - 1.0) * (0.5 - (r - 1.0) / 12.0)));
+  return (T)(dsup * c * (r - 1.0) / log(r));
+}
+
+// The update of one point shared by long_char2 and short_char2 once the upwind
+// values are known (rt_solvers_mod.f90:404-491 and :606-657).
+template <typename T>
+__device__ __forceinline__ void linear2_point(bool split, int row, bool special, T xxup, T eup, T Inuup, T ssup,
+                                              T chi, T ss, T xx, T dt, T d5, T rc, T Imax, T &Inu_out,
+                                              T &psi_out, T &irem_out, T &esc_out) {
+  T E, W, Psi, Esc;
+  linear_weights(dt, E, W, Psi, Esc);
+  const T pl = Psi / tcopysign(tmax(tabs(chi), tiny_of<T>()), chi);
+  if (split && row == 0) {
+    const T Irem = fma_t(W, ssup, Inuup * E);
+    T Inu = fma_t(Psi, ss, Irem);
+    const bool off = tmin(tmin(dt, chi), Imax - tabs(Inu)) <= 0;
+    Inu = tmax(-Imax, tmin(Imax, Inu));
+    irem_out = off ? Inu : Irem;
+    esc_out = off ? (T)1 : Esc;
+    Inu_out = Inu;
+    psi_out = off ? (T)0 : pl;
+  } else if (split) {
+    const T ee = xx * ss;
+    const T rxb = d5 / (dt != 0 ? dt : (T)1);
+    const T Irem = special ? fma_t(W * eup, rxb, Inuup * E) : fma_t(W, ssup, Inuup * E);
+    T Inu = special ? fma_t(Psi * ee, rxb, Irem) : fma_t(Psi, ss, Irem);
+    T mm = tmin(tmin(dt, chi), Imax - tabs(Inu));
+    mm = tmin(mm, special ? xxup : (T)1);
+    const bool off = mm <= 0;
+    Esc = special ? fma_t(((T)0.5 * Psi) * (xxup - xx), rxb, Esc) : Esc;
+    Inu = tmax(-Imax, tmin(Imax, Inu));
+    irem_out = off ? Inu : Irem;
+    esc_out = off ? (T)1 : Esc;
+    Inu_out = Inu;
+    psi_out = off ? (T)0 : (special ? (Psi * rxb) * rc : pl);
+  } else if (row == 0) {
+    const T Inu = fma_t(Psi, ss, fma_t(W, ssup, Inuup * E));
+    Inu_out = tmax(-Imax, tmin(Imax, Inu));
+    const bool off = tmin(dt, chi) <= 0;
+    psi_out = off ? (T)0 : pl;
+  } else {
+    const T ee = xx * ss;
+    const T rxb = d5 / (dt != 0 ? dt : (T)1);
+    const T Inu = special ? fma_t(fma_t(Psi, ee, W * eup), rxb, Inuup * E) : fma_t(Psi, ss, fma_t(W, ssup, Inuup * E));
+    Inu_out = tmax(-Imax, tmin(Imax, Inu));
+    T mm = tmin(dt, chi);
+    mm = tmin(mm, special ? xxup : (T)1);
+    const bool off = mm <= 0;
+    psi_out = off ? (T)0 : (special ? (Psi * rxb) * rc : pl);
+  }
+}
+
+// long_char2 (rt_solvers_mod.f90:527-663)
+template <typename T>
+__global__ void k_long_char2(SlabArgs s, T *work, T *psi, T *irem, T *esc, const float *chi500, const float *g500,
+                             const int *eta_row, const uint8_t *eta_mask, double dsup) {
+  const size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  const int nf = s.nf, nx = s.nx, ny = s.ny, nz = s.nz, dir = s.dir;
+  if (g >= (size_t)nf * nx * ny) return;
+  const int f = (int)(g % nf), x = (int)((g / nf) % nx), y = (int)(g / ((size_t)nf * nx));
+  const T dtmax = -(T)s.maser_dtau_max, Imax = (T)s.maser_Inu_max;
+  const int zs = dir > 0 ? 1 : nz;
+  const size_t zstride = (size_t)nf * nx * ny;
+  const size_t k1 = zstride * (nz + 2);
+  for (int i = 0, z = zs; i < nz; i++, z += dir) {
+    const int zup = z - dir;
+    const double c = chi500[ic3(x, y, z, nx, ny)];
+    const double cu = (zup < 1 || zup > nz) ? (double)g500[x + nx * y] : (double)chi500[ic3(x, y, zup, nx, ny)];
+    const T d5 = dt500_of<T>(dsup, c, cu);
+    const T rc = (T)(1.0 / c), rcu = (T)(1.0 / cu);
+    const int row = eta_row ? eta_row[ic3(x, y, z, nx, ny)] : 0;
+    const bool special = row > 0 ? eta_mask[(size_t)f + (size_t)nf * (size_t)(row - 1)] != 0 : false;
+    const size_t ou = g + zstride * zup, o = g + zstride * z;
+    const T xxup = work[ou] * rcu, ssup = work[ou + k1], Inuup = work[ou + 2 * k1];
+    const T eup = xxup * ssup;
+    const T chi = work[o], ss = work[o + k1];
+    const T xx = chi * rc;
+    const T dt = tmax(((T)0.5 * (xxup + xx)) * d5, dtmax);
+    T Inu, ps, ir = 0, es = 0;
+    linear2_point<T>(s.split_rates != 0, row, special, xxup, eup, Inuup, ssup, chi, ss, xx, dt, d5, rc, Imax, Inu,
+                     ps, ir, es);
+    work[o + 2 * k1] = Inu;
+    const size_t p = ip(f, x, y, z, nf, nx, ny);
+    if (s.split_rates) { irem[p] = ir; esc[p] = es; }
+    if (s.get_psi) psi[p] = ps;
+  }
+}
+
+// quad_step of long_char_quadratic (rt_solvers_mod.f90:966-1019)
+template <typename T>
+__device__ __forceinline__ void quad_step(T xxup, T xxc, T xxdn, T ssup, T ssc, T ssdn, T Inuup, bool at_target,
+                                          T rdsup, T dsup1, T dsup2, T dtmax, T Imax, bool get_psi, T &Inu_out,
+                                          T &plam_out) {
+  const T dtmin = (T)1e-20f;
+  T t1 = (xxc - xxup) * rdsup;
+  T t3 = (xxdn - xxc) * rdsup;
+  T t2 = (T)0.5 * (t1 + t3);
+  t2 = (tcopysign((T)1, t1) + tcopysign((T)1, t3)) * tmin(tmin(tabs(t1), tabs(t3)), tabs((T)0.5 * t2));
+  T dtup = fma_t(dsup2, t1 - t2, dsup1 * (xxup + xxc));
+  T dtdn = fma_t(dsup2, t2 - t3, dsup1 * (xxdn + xxc));
+  dtup = tmax(tcopysign(tmax(tabs(dtup), dtmin), dtup), dtmax);
+  dtdn = tmax(tcopysign(tmax(tabs(dtdn), dtmin), dtdn), dtmax);
+  const T dt = at_target ? dtup : dtdn;
+  const T rdt = (T)1 / dt;
+  T ex, U0, U1, q;
+  parab_moments(dt, ex, U0, U1, q);
+  if (at_target) {
+    t1 = (ssc - ssup) * rdt;
+    t3 = (ssdn - ssc) / dtdn;
+  } else {
+    t1 = (ssc - ssup) / dtup;
+    t3 = (ssdn - ssc) * rdt;
+  }
+  t2 = (T)0.5 * (t1 + t3);
+  const T dsdtau = (tcopysign((T)1, t1) + tcopysign((T)1, t3)) * tmin(tmin(tabs(t1), tabs(t3)), tabs((T)0.5 * t2));
+  T plam = 0, Inu;
+  if (at_target) {
+    const T B = ((T)2 * U1 - q) * rdt;
+    const T A = U0 - B;
+    const T C = q - U1;
+    Inu = fma_t(C, dsdtau, fma_t(B, ssc, fma_t(A, ssup, Inuup * ex)));
+    if (get_psi && dt > 0 && xxc > 0) plam = B / xxc;
+  } else {
+    const T A = q * rdt;
+    const T B = U0 - A;
+    const T C = U1 - q;
+    Inu = fma_t(C, dsdtau, fma_t(B, ssc, fma_t(A, ssdn, Inuup * ex)));
+    if (get_psi && dt > 0 && xxdn > 0) plam = A / xxdn;
+  }
+  Inu_out = tmax(-Imax, tmin(Imax, Inu));
+  plam_out = plam;
+}
+
+struct QuadConst { float rdsup, dsup1, dsup2; };
+
+// long_char_quadratic (rt_solvers_mod.f90:891-1020) on a slab's work array
+template <typename T>
+__global__ void k_long_char_quadratic(SlabArgs s, T *work, T *psi, QuadConst qc) {
+  const size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  const int nf = s.nf, nx = s.nx, ny = s.ny, nz = s.nz, dir = s.dir;
+  if (g >= (size_t)nf * nx * ny) return;
+  const int f = (int)(g % nf), x = (int)((g / nf) % nx), y = (int)(g / ((size_t)nf * nx));
+  const T dtmax = -(T)s.maser_dtau_max, Imax = (T)s.maser_Inu_max;
+  const T rdsup = (T)qc.rdsup, dsup1 = (T)qc.dsup1, dsup2 = (T)qc.dsup2;
+  const bool gp = s.get_psi != 0;
+  const int zs = dir > 0 ? 1 : nz, ze = dir > 0 ? nz : 1;
+  const size_t zstride = (size_t)nf * nx * ny;
+  const size_t k1 = zstride * (nz + 2);
+  T xu = work[g + zstride * (zs - dir)], su = work[g + zstride * (zs - dir) + k1];
+  T Iu = work[g + zstride * (zs - dir) + 2 * k1];
+  T xc = work[g + zstride * zs], sc = work[g + zstride * zs + k1];
+  T xd = work[g + zstride * (zs + dir)], sd = work[g + zstride * (zs + dir) + k1];
+  int z = zs;
+  for (; z != ze; z += dir) {
+    T Inu, pl;
+    quad_step<T>(xu, xc, xd, su, sc, sd, Iu, true, rdsup, dsup1, dsup2, dtmax, Imax, gp, Inu, pl);
+    work[g + zstride * z + 2 * k1] = Inu;
+    if (gp) psi[ip(f, x, y, z, nf, nx, ny)] = pl;
+    Iu = Inu;
+    if (z + dir != ze) {
+      xu = xc; su = sc; xc = xd; sc = sd;
+      xd = work[g + zstride * (z + 2 * dir)];
+      sd = work[g + zstride * (z + 2 * dir) + k1];
+    }
+  }
+  // last plane: the interval z0 -> ze with dS/dtau at its upwind end z0; the
+  // planes (ze-2dir, ze-dir, ze) are the ones held after the final interior step
+  {
+    T Inu, pl;
+    quad_step<T>(xu, xc, xd, su, sc, sd, Iu, false, rdsup, dsup1, dsup2, dtmax, Imax, gp, Inu, pl);
+    work[g + zstride * ze + 2 * k1] = Inu;
+    if (gp) psi[ip(f, x, y, ze, nf, nx, ny)] = pl;
+  }
+}
+
+// rotate_array (rt_patch_mod.f90:3809-3866) of plane z of slot k, out of place
+struct RotPlane { int up1, up2; float a, b, c, d; };
+
+template <typename T>
+__global__ void k_rotate_planes(int nf, int nx, int ny, int nz, const T *src, T *dst, const RotPlane *rot) {
+  // src, dst: (nf, nx, ny, 1:nz, 2) views starting at plane 1 of slot k (stride between slots sk)
+  const size_t plane = (size_t)nf * nx * ny;
+  const size_t n = plane * nz * 2;
+  for (size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x; g < n; g += (size_t)gridDim.x * blockDim.x) {
+    const size_t inplane = g % plane;
+    const int zk = (int)(g / plane);
+    const int z = zk % nz, k = zk / nz;
+    const int f = (int)(inplane % nf), x = (int)((inplane / nf) % nx), y = (int)(inplane / ((size_t)nf * nx));
+    const RotPlane r = rot[z];
+    const int x1 = wrap(x + r.up1, nx), x2 = wrap(x + r.up1 + 1, nx);
+    const int y1 = wrap(y + r.up2, ny), y2 = wrap(y + r.up2 + 1, ny);
+    const T *p = src + plane * ((size_t)k * nz + z);
+    T v = (T)r.a * p[(size_t)f + (size_t)nf * ((size_t)x1 + (size_t)nx * y1)];
+    v = fma_t((T)r.b, p[(size_t)f + (size_t)nf * ((size_t)x2 + (size_t)nx * y1)], v);
+    v = fma_t((T)r.c, p[(size_t)f + (size_t)nf * ((size_t)x1 + (size_t)nx * y2)], v);
+    v = fma_t((T)r.d, p[(size_t)f + (size_t)nf * ((size_t)x2 + (size_t)nx * y2)], v);
+    dst[g] = v;
+  }
+}
+
+// set_upstream_boundary (rt_patch_mod.f90:3270-3393) on the ghost plane of work
+struct PchipConst { float c0, p, cm0, cm1, dx1; };
+
+template <typename T>
+__global__ void k_upstream_boundary(int nf, int nx, int ny, int nz, int dir, T *work, int mode, const T *mem,
+                                    PchipConst pc, const float *ghost_r500, const float *ghost_temp,
+                                    const double *nu) {
+  const size_t plane = (size_t)nf * nx * ny;
+  const size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (g >= plane) return;
+  const int z = dir > 0 ? 0 : nz + 1, zi = dir > 0 ? 1 : -1;
+  const size_t k1 = plane * (nz + 2);
+  const size_t o = g + plane * z;
+  if (mode == 1) {
+    work[o] = 0; work[o + k1] = 0; work[o + 2 * k1] = 0;
+  } else if (mode == 2) {
+    for (int k = 0; k < 2; k++) {
+      const float y1 = (float)work[g + plane * (z + zi) + k * k1], y2 = (float)work[g + plane * (z + 2 * zi) + k * k1];
+      const float dy1 = y2 - y1;
+      const float dydx1 = (2.0f * dy1) / pc.dx1 - 0.0f;
+      const float v = (pc.c0 * y1 + pc.p * y2) + pc.dx1 * (pc.cm0 * dydx1 + pc.cm1 * 0.0f);
+      work[o + k * k1] = (T)fmaxf(v, 0.0f);
+    }
+    work[o + 2 * k1] = work[o + k1];
+  } else if (mode == 3) {
+    const int f = (int)(g % nf);
+    const size_t xy = g / nf;
+    const float r500 = ghost_r500[xy];
+    const float h_kT = (float)(M3D_H_K / (double)ghost_temp[xy]);
+    const float hv = (float)(nu[f] * (double)h_kT);
+    float E, u0;
+    exp_neg(hv, E, u0);
+    const float beta = fmaxf(E, FLT_MIN);
+    work[o] = work[g + plane * (z + zi)] * (T)r500;
+    work[o + k1] = (T)(beta / (1.0f - beta));
+    work[o + 2 * k1] = work[o + k1];
+  } else {
+    work[o] = mem[g]; work[o + k1] = mem[g + plane]; work[o + 2 * k1] = mem[g + 2 * plane];
+  }
+}
+
+// short_char / short_char2 on plane z: each thread forms the row sums of its
+// four upwind rows itself, in the reference's order (row pass, then column)
+template <typename T>
+__global__ void k_short_char_plane(SlabArgs s, int z, T *work, T *psi, T *irem, T *esc, const int *xt, const int *yt,
+                                   float4 kx, float4 ky, T dsup05) {
+  const size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  const int nf = s.nf, nx = s.nx, ny = s.ny, nz = s.nz, dir = s.dir;
+  if (g >= (size_t)nf * nx * ny) return;
+  const int f = (int)(g % nf), x = (int)((g / nf) % nx), y = (int)(g / ((size_t)nf * nx));
+  const int zup = z - dir;
+  const T dtmax = -(T)s.maser_dtau_max, Imax = (T)s.maser_Inu_max;
+  const T k_x[4] = {(T)kx.x, (T)kx.y, (T)kx.z, (T)kx.w};
+  const T k_y[4] = {(T)ky.x, (T)ky.y, (T)ky.z, (T)ky.w};
+  T up[3], mn[3];
+  for (int i = 0; i < 3; i++) {
+    T r = 0;
+    for (int jj = 0; jj < 4; jj++) {
+      const int yu = yt[4 * y + jj];
+      T rr = 0;
+      for (int ii = 0; ii < 4; ii++) rr = fma_t(k_x[ii], work[iw(f, xt[4 * x + ii], yu, zup, i, nf, nx, ny, nz)], rr);
+      r = fma_t(k_y[jj], rr, r);
+    }
+    T m = (T)FLT_MAX;
+    if (sizeof(T) == 8) m = (T)DBL_MAX;
+    for (int jj = 1; jj <= 2; jj++)
+      for (int ii = 1; ii <= 2; ii++) m = tmin(m, work[iw(f, xt[4 * x + ii], yt[4 * y + jj], zup, i, nf, nx, ny, nz)]);
+    up[i] = r;
+    mn[i] = m;
+  }
+  const T xxup = tmax(up[0], mn[0]), ssup = tmax(up[1], mn[1]), Inuup = tmax(up[2], mn[2]);
+  const size_t o = iw(f, x, y, z, 0, nf, nx, ny, nz);
+  const size_t k1 = (size_t)nf * nx * ny * (nz + 2);
+  const T xx = work[o], ss = work[o + k1];
+  T dt = dsup05 * (xxup + xx);
+  dt = tmax(dt, dtmax);
+  T E, W, Psi, Esc;
+  linear_weights(dt, E, W, Psi, Esc);
+  T Inu = fma_t(Psi, ss, fma_t(W, ssup, Inuup * E));
+  const size_t p = ip(f, x, y, z, nf, nx, ny);
+  if (s.split_rates) {
+    const bool off = dt <= 0 || xx <= 0 || tabs(Inu) > Imax;
+    const T Irem = fma_t(W, ssup, Inuup * E);
+    Inu = tmax(-Imax, tmin(Imax, Inu));
+    Psi = off ? (T)0 : Psi;
+    irem[p] = off ? Inu : Irem;
+    esc[p] = off ? (T)1 : Esc;
+  } else {
+    Inu = tmax(-Imax, tmin(Imax, Inu));
+  }
+  work[o + 2 * k1] = Inu;
+  if (s.get_psi) psi[p] = (dt > 0 && xx > 0) ? Psi / xx : (T)0;
+}
+
+template <typename T>
+__global__ void k_short_char2_plane(SlabArgs s, int z, T *work, T *psi, T *irem, T *esc, const int *xt, const int *yt,
+                                    float4 kx, float4 ky, float hx, float hy, const float *chi500,
+                                    const float *chi500_up, const float *g500, const int *eta_row,
+                                    const uint8_t *eta_mask, double dsup) {
+  const size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  const int nf = s.nf, nx = s.nx, ny = s.ny, nz = s.nz, dir = s.dir;
+  if (g >= (size_t)nf * nx * ny) return;
+  const int f = (int)(g % nf), x = (int)((g / nf) % nx), y = (int)(g / ((size_t)nf * nx));
+  const int zup = z - dir;
+  const T dtmax = -(T)s.maser_dtau_max, Imax = (T)s.maser_Inu_max;
+  const size_t k1 = (size_t)nf * nx * ny * (nz + 2);
+  const bool ghost = zup < 1 || zup > nz;
+  const int x1 = xt[4 * x], x2 = xt[4 * x + 1], x3 = xt[4 * x + 2], x4 = xt[4 * x + 3];
+  const int yy[4] = {yt[4 * y], yt[4 * y + 1], yt[4 * y + 2], yt[4 * y + 3]};
+  const T hxr = (T)hx, hx1 = (T)(1.0f - hx), hyr = (T)hy, hy1 = (T)(1.0f - hy);
+  // row sums at the four upwind rows (row_red slots 1..4, rt_solvers_mod.f90:334-348)
+  T r0[4], r1[4], r2[4], r3[4];
+  for (int jj = 0; jj < 4; jj++) {
+    const int yu = yy[jj];
+    const float c2 = ghost ? g500[x2 + nx * yu] : chi500[ic3(x2, yu, zup, nx, ny)];
+    const float c3 = ghost ? g500[x3 + nx * yu] : chi500[ic3(x3, yu, zup, nx, ny)];
+    const T w2 = (T)((1.0f - hx) * (1.0f / c2));
+    const T w3 = (T)(hx * (1.0f / c3));
+    const T a21 = work[iw(f, x2, yu, zup, 0, nf, nx, ny, nz)], a31 = work[iw(f, x3, yu, zup, 0, nf, nx, ny, nz)];
+    const T a22 = work[iw(f, x2, yu, zup, 1, nf, nx, ny, nz)], a32 = work[iw(f, x3, yu, zup, 1, nf, nx, ny, nz)];
+    r0[jj] = fma_t(w3, a31, w2 * a21);
+    r1[jj] = fma_t(w3 * a31, a32, (w2 * a21) * a22);
+    T t = (T)kx.x * work[iw(f, x1, yu, zup, 2, nf, nx, ny, nz)];
+    t = fma_t((T)kx.y, work[iw(f, x2, yu, zup, 2, nf, nx, ny, nz)], t);
+    t = fma_t((T)kx.z, work[iw(f, x3, yu, zup, 2, nf, nx, ny, nz)], t);
+    t = fma_t((T)kx.w, work[iw(f, x4, yu, zup, 2, nf, nx, ny, nz)], t);
+    r2[jj] = t;
+    r3[jj] = fma_t(hxr, a32, hx1 * a22);
+  }
+  const double c = chi500[ic3(x, y, z, nx, ny)];
+  const double cu = chi500_up[ic3(x, y, z, nx, ny)];
+  const T d5 = dt500_of<T>(dsup, c, cu);
+  const T rc = (T)(1.0 / c);
+  const T xxup = fma_t(hyr, r0[2], hy1 * r0[1]);
+  const T eup = fma_t(hyr, r1[2], hy1 * r1[1]);
+  T Inuup = (T)ky.x * r2[0];
+  Inuup = fma_t((T)ky.y, r2[1], Inuup);
+  Inuup = fma_t((T)ky.z, r2[2], Inuup);
+  Inuup = fma_t((T)ky.w, r2[3], Inuup);
+  const T m = tmin(tmin(tmin(work[iw(f, x2, yy[1], zup, 2, nf, nx, ny, nz)], work[iw(f, x3, yy[1], zup, 2, nf, nx, ny, nz)]),
+                        work[iw(f, x2, yy[2], zup, 2, nf, nx, ny, nz)]),
+                   work[iw(f, x3, yy[2], zup, 2, nf, nx, ny, nz)]);
+  Inuup = tmax(Inuup, m);
+  const size_t o = iw(f, x, y, z, 0, nf, nx, ny, nz);
+  const T chi = work[o], ss = work[o + k1];
+  const T xx = chi * rc;
+  const T dt = tmax(((T)0.5 * (xxup + xx)) * d5, dtmax);
+  const T ssup = fma_t(hyr, r3[2], hy1 * r3[1]);
+  const int row = eta_row ? eta_row[ic3(x, y, z, nx, ny)] : 0;
+  const bool special = row > 0 ? eta_mask[(size_t)f + (size_t)nf * (size_t)(row - 1)] != 0 : false;
+  T Inu, ps, ir = 0, es = 0;
+  linear2_point<T>(s.split_rates != 0, row, special, xxup, eup, Inuup, ssup, chi, ss, xx, dt, d5, rc, Imax, Inu, ps,
+                   ir, es);
+  work[o + 2 * k1] = Inu;
+  const size_t p = ip(f, x, y, z, nf, nx, ny);
+  if (s.split_rates) { irem[p] = ir; esc[p] = es; }
+  if (s.get_psi) psi[p] = ps;
+}
+
+}  // namespace m3d

@@ -1,0 +1,65 @@
+// QLG-bot Voigt profile on the device (HOP/qlg_mod.f90, OpenMULTI3D's additions
+// bot_setup :538, qlg_bot_line_eval :556, qlg_bot_cell :576, qlg_bot_line :616,
+// qlg_bot_line_sweep :646).  The two tables TGX = 2^-u and TH2X = Z_0.2(u)(1+u)^2
+// (qlg_init :364) live in global memory and are staged into shared memory by the
+// kernels that sweep line windows.  The fitted constants are the published QLG-bot
+// coefficients; they have to be the same numbers for the profile to be QLG-bot.
+#pragma once
+#include "m3d_math.cuh"
+
+namespace m3d {
+
+constexpr int QLG_NTAB = 9020;  // indices 0..9019 on xi = sqrt(u) at 800 per unit
+
+struct QlgCoef { float ih, bL, gG, cZH, cL2; };
+struct QlgCell { float D, D2, SQ, D2h, D2G, D2L; };
+
+__device__ __forceinline__ QlgCell qlg_cell(float D) {
+  QlgCell w;
+  w.D = D;
+  w.D2 = D * D;
+  w.SQ = 0.8325546112f * w.D2;
+  w.D2h = 0.5f * w.D2;
+  w.D2G = 1.5f * w.D2;
+  w.D2L = 5.0f * w.D2;
+  return w;
+}
+
+// per-line setup on the caller's abscissa: gL Lorentz width, D Doppler width,
+// SQ = sqrt(ln2) D^2, S the strength folded in
+__device__ __forceinline__ QlgCoef qlg_setup(float gL, float D, float SQ, float S) {
+  QlgCoef c;
+  const float e = fmaf(gL, 0.60602209212341318f, D);
+  c.ih = e / fmaf(gL, e, SQ);
+  const float r = gL * c.ih;
+  const float q = r * (1.0f - r);
+  const float sc = S * c.ih;
+  const float qs = q * sc;
+  const float x = 2.0f * r - 1.0f;
+  c.bL = (0.3183098862f * r) * sc;
+  c.gG = fmaf(qs, fmaf(x, -0.11019326278794868f, -0.064924393191013452f), (0.4697186f * (1.0f - r)) * sc);
+  c.cZH = qs * fmaf(x, -0.10567135279610407f, 0.38494195930078284f);
+  c.cL2 = qs * fmaf(x, 0.16241029253712097f, 0.04054415746208978f);
+  return c;
+}
+
+__device__ __forceinline__ float qlg_eval(const float *tgx, const float *th2x, const QlgCoef &c, float x) {
+  const float xs = fabsf(x) * c.ih;
+  const float u = xs * xs;
+  const float L = 1.0f / (1.0f + u);
+  const int ig = (int)lroundf(fminf(xs * 800.0f, 9019.0f));
+  const float G = tgx[ig], W = th2x[ig];
+  float p = fmaf(c.cZH, W, c.cL2);
+  p = fmaf(L, p, c.bL);
+  return fmaf(L, p, G * c.gG);
+}
+
+// analytic half-width where the line falls to ref (qlg_bot_line, qlg_mod.f90:616-627)
+__device__ __forceinline__ float qlg_halfwidth(const QlgCell &w, float gL, float S, float ref, float lnq) {
+  const float AL = ((0.3183098862f * gL) * S) / ref;
+  const float h1 = fmaf(w.D2, lnq, fminf(AL, w.D2G));
+  const float h2 = (AL - fmaxf(fmaf(gL, gL, -w.D2h), 0.0f)) + fminf(AL, w.D2L);
+  return sqrtf(fmaxf(fmaxf(h1, h2), 0.0f));
+}
+
+}  // namespace m3d

@@ -1,0 +1,260 @@
+"""Array-level wrappers of the libm3dgpu.so entry points.
+
+numpy arguments are host buffers; torch CUDA tensors are passed as device
+pointers (M3D_DEVICE_PTRS).  All arrays keep the reference's Fortran layout,
+frequency fastest; in numpy C order that is the reversed shape, e.g. work is
+(3, nz+2, ny, nx, nf).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import (DEVICE_PTRS, FP64, LINE_DIAG, ROTATE, Atmos, LineList, Species, check, init, lib, ptr)
+
+_F32 = np.float32
+
+
+def _is_dev(*arrays) -> bool:
+    for a in arrays:
+        if a is not None and not isinstance(a, np.ndarray):
+            return True
+    return False
+
+
+def _flags(arrays, extra=0) -> int:
+    f = extra
+    if _is_dev(*arrays):
+        f |= DEVICE_PTRS
+    for a in arrays:
+        if a is None:
+            continue
+        if str(getattr(a, "dtype", "")) in ("float64", "torch.float64"):
+            f |= FP64
+            break
+    return f
+
+
+def weights(which: int, t, fp64: bool = False):
+    """K0 elementwise: 0 exp_neg (E, u0), 1 linear_weights (E, W, Psi, Esc),
+    2 parab_moments (E, U0, U1, q), 3 exp4, 4 the library's fp32 log."""
+    init()
+    dt = np.float64 if fp64 else np.float32
+    t = np.ascontiguousarray(t, dt)
+    nout = 2 if which == 0 else (1 if which >= 3 else 4)
+    outs = [np.empty_like(t) for _ in range(nout)] + [None] * (4 - nout)
+    check(lib().m3d_weights(C.c_int(which), C.c_int(t.size), ptr(t), *[ptr(o) for o in outs],
+                            C.c_uint(FP64 if fp64 else 0)), "m3d_weights")
+    return outs[:nout] if nout > 1 else outs[0]
+
+
+def qlg_tables():
+    init()
+    tgx = np.empty(9020, _F32)
+    th2x = np.empty(9020, _F32)
+    check(lib().m3d_qlg_tables(ptr(tgx), ptr(th2x)), "m3d_qlg_tables")
+    return tgx, th2x
+
+
+def qlg_bot_profile(a, q, vpr, idf):
+    init()
+    a, q, vpr, idf = (np.ascontiguousarray(x, _F32) for x in (a, q, vpr, idf))
+    h = np.empty_like(a)
+    check(lib().m3d_qlg_bot_profile(C.c_int(a.size), ptr(a), ptr(q), ptr(vpr), ptr(idf), ptr(h), C.c_uint(0)),
+          "m3d_qlg_bot_profile")
+    return h
+
+
+def make_linelist(ll: dict, keep: list) -> LineList:
+    """Build an m3d_linelist_t from a dict of arrays (numpy or torch); arrays
+    are appended to keep so that they outlive the call."""
+
+    def arr(name, dt):
+        if name not in ll or ll[name] is None:
+            return None
+        a = ll[name]
+        if isinstance(a, np.ndarray) or not hasattr(a, "data_ptr"):
+            a = np.ascontiguousarray(a, dt)
+        keep.append(a)
+        return ptr(a)
+
+    s = LineList()
+    s.nline = int(len(ll["llam0"]))
+    s.llam0 = arr("llam0", np.float64)
+    for k in ("lower_ev", "gpref", "grad", "gw1", "gw2", "gstk"):
+        setattr(s, k, arr(k, _F32))
+    s.unsold = arr("unsold", np.uint8)
+    s.lev_i = arr("lev_i", np.int32)
+    s.lev_j = arr("lev_j", np.int32)
+    s.active = arr("active", np.uint8)
+    return s
+
+
+def line_opacity(ll: dict, llam, chi, eta, cont, logref, cells: dict, dep_mem=None, nlevel=0, do_nlte=False,
+                 tol=1e-4, line_reject_frac=0.0, diag=False):
+    """add_opacity_equi over ncell cells, in place on chi/eta ((ncell, nf) in C order).
+    Returns (used, strength, reach) with diag, else None."""
+    init()
+    keep = []
+    s = make_linelist(ll, keep)
+    nl = s.nline
+    dev = _is_dev(chi)
+    if dev:
+        import torch
+        used = torch.zeros(nl, dtype=torch.uint8, device=chi.device) if diag else None
+        strength = torch.zeros(nl, dtype=torch.float32, device=chi.device) if diag else None
+        reach = torch.zeros(nl, dtype=torch.float32, device=chi.device) if diag else None
+    else:
+        used = np.zeros(nl, np.uint8) if diag else None
+        strength = np.zeros(nl, _F32) if diag else None
+        reach = np.zeros(nl, _F32) if diag else None
+        llam = np.ascontiguousarray(llam, np.float64)
+    nf = int(llam.shape[0])
+    ncell = int(chi.shape[0])
+    flags = (DEVICE_PTRS if dev else 0) | (LINE_DIAG if diag else 0)
+    cf = [cells[k] for k in ("vproj", "inv_df", "vbar2", "e_kT", "lnbase", "ne", "tothi", "stark_pe")]
+    if not dev:
+        cf = [np.ascontiguousarray(c, _F32) for c in cf]
+        cont = np.ascontiguousarray(cont, _F32)
+        logref = np.ascontiguousarray(logref, _F32)
+        if dep_mem is not None:
+            dep_mem = np.ascontiguousarray(dep_mem, _F32)
+    check(lib().m3d_line_opacity(C.byref(s), C.c_int(nf), ptr(llam), C.c_int(ncell), ptr(chi), ptr(eta), ptr(cont),
+                                 ptr(logref), *[ptr(c) for c in cf], ptr(dep_mem), C.c_int(nlevel),
+                                 C.c_int(int(do_nlte)), C.c_float(tol), C.c_float(line_reject_frac), ptr(used),
+                                 ptr(strength), ptr(reach), C.c_uint(flags)), "m3d_line_opacity")
+    del keep
+    return (used, strength, reach) if diag else None
+
+
+def lte_background(nu, temp):
+    init()
+    nu = np.ascontiguousarray(nu, np.float64)
+    temp = np.ascontiguousarray(temp, _F32)
+    beta = np.empty((temp.size, nu.size), _F32)
+    Bnu = np.empty_like(beta)
+    check(lib().m3d_lte_background(C.c_int(nu.size), C.c_int(temp.size), ptr(nu), ptr(temp), ptr(beta), ptr(Bnu),
+                                   C.c_uint(0)), "m3d_lte_background")
+    return beta, Bnu
+
+
+def work_to_transfer_units(w1, w2, beta, maser_chi_floor=1e-4, suppress_masers=False) -> int:
+    init()
+    nc, nf = beta.shape
+    nfl = C.c_int(0)
+    flags = DEVICE_PTRS if _is_dev(w1) else 0
+    if flags:
+        import torch
+        cnt = torch.zeros(1, dtype=torch.int32, device=w1.device)
+        check(lib().m3d_work_to_transfer_units(C.c_int(nf), C.c_int(nc), ptr(w1), ptr(w2), ptr(beta),
+                                               C.c_double(maser_chi_floor), C.c_int(int(suppress_masers)), ptr(cnt),
+                                               C.c_uint(flags)), "m3d_work_to_transfer_units")
+        return int(cnt.item())
+    check(lib().m3d_work_to_transfer_units(C.c_int(nf), C.c_int(nc), ptr(w1), ptr(w2), ptr(beta),
+                                           C.c_double(maser_chi_floor), C.c_int(int(suppress_masers)), C.byref(nfl),
+                                           C.c_uint(0)), "m3d_work_to_transfer_units")
+    return nfl.value
+
+
+def formal_solve(solver, slab, work, psi=None, irem=None, escape=None, chi500=None, chi500_up=None, g500=None,
+                 eta_row=None, eta_mask=None, rotate=None, extra_flags=0):
+    """radiative_transfer of one slab.  rotate = (ds_code(3), bot2pivot, ray_offset(2))
+    applies rotate_array first (quadratic solver)."""
+    init()
+    flags = _flags([work], extra_flags)
+    if rotate is not None:
+        flags |= ROTATE
+        ds_code = (C.c_double * 3)(*rotate[0])
+        b2p = float(rotate[1])
+        off = (C.c_double * 2)(*(rotate[2] if len(rotate) > 2 else (0.0, 0.0)))
+    else:
+        ds_code, b2p, off = None, 0.0, None
+    check(lib().m3d_formal_solve(C.c_int(solver), C.byref(slab), ptr(work), ptr(psi), ptr(irem), ptr(escape),
+                                 ptr(chi500), ptr(chi500_up), ptr(g500), ptr(eta_row), ptr(eta_mask), ds_code,
+                                 C.c_double(b2p), off, C.c_uint(flags)), "m3d_formal_solve")
+
+
+def rotate_array(slab, work, ds_code, bot2pivot, ray_offset=(0.0, 0.0)):
+    init()
+    check(lib().m3d_rotate_array(C.byref(slab), ptr(work), (C.c_double * 3)(*ds_code), C.c_double(bot2pivot),
+                                 (C.c_double * 2)(*ray_offset), C.c_uint(_flags([work]))), "m3d_rotate_array")
+
+
+def upstream_boundary(slab, work, mode, mem=None, ds3_code=1.0, ghost_r500=None, ghost_temp=None, nu=None):
+    init()
+    check(lib().m3d_upstream_boundary(C.byref(slab), ptr(work), C.c_int(mode), ptr(mem), C.c_float(ds3_code),
+                                      ptr(ghost_r500), ptr(ghost_temp), ptr(nu), C.c_uint(_flags([work]))),
+          "m3d_upstream_boundary")
+
+
+def integrate_intensity(wmu, inu, psi, Jnu, PsiJ):
+    init()
+    check(lib().m3d_integrate_intensity(C.c_int(int(np.prod(inu.shape))), C.c_float(wmu), ptr(inu), ptr(psi),
+                                        ptr(Jnu), ptr(PsiJ), C.c_uint(_flags([inu]))), "m3d_integrate_intensity")
+
+
+def lte_synthesis(atm: dict, nu, llam, vec, wmu, fp64=False, return_itop=False, device=False):
+    """The LTE output pass of one frequency window for every ray (m3d_lte_synthesis).
+
+    atm: dict with nx, ny, nz, slab_nz, ds_cm, ds_code, pivot_z, ray_offset and the
+    per-cell fields (numpy for host buffers, torch CUDA tensors with device=True),
+    species: list of dicts (linelist arrays + inv_df, vbar2, lnbase).
+    Returns (ie (nray, nf), flux (nf,), i_top or None)."""
+    init()
+    keep = []
+    a = Atmos()
+    a.nx, a.ny, a.nz = atm["nx"], atm["ny"], atm["nz"]
+    slab_nz = np.ascontiguousarray(atm["slab_nz"], np.int32)
+    keep.append(slab_nz)
+    a.nslab = slab_nz.size
+    a.slab_nz = ptr(slab_nz)
+    a.ds_cm[:] = list(atm["ds_cm"])
+    a.ds_code[:] = list(atm["ds_code"])
+    a.pivot_z = float(atm["pivot_z"])
+    a.ray_offset[:] = list(atm.get("ray_offset", (0.0, 0.0)))
+
+    def fld(x):
+        if isinstance(x, np.ndarray):
+            x = np.ascontiguousarray(x, _F32)
+        keep.append(x)
+        return ptr(x)
+
+    for k in ("temp", "chi_c", "vx", "vy", "vz", "e_kT", "ne", "tothi", "stark_pe"):
+        setattr(a, k, fld(atm[k]))
+    sp_list = atm["species"]
+    sarr = (Species * max(1, len(sp_list)))()
+    for i, sp in enumerate(sp_list):
+        sarr[i].ll = make_linelist(sp, keep)
+        sarr[i].inv_df = fld(sp["inv_df"])
+        sarr[i].vbar2 = fld(sp["vbar2"])
+        sarr[i].lnbase = fld(sp["lnbase"])
+    keep.append(sarr)
+    a.nspecies = len(sp_list)
+    a.species = C.cast(sarr, C.c_void_p)
+    a.tol = atm.get("tol", 1e-4)
+    a.maser_chi_floor = atm.get("maser_chi_floor", 1e-4)
+    a.maser_dtau_max = atm.get("maser_dtau_max", 2.0)
+    a.maser_Inu_max = atm.get("maser_Inu_max", 1e30)
+    vec = np.ascontiguousarray(vec, np.float64)
+    wmu = np.ascontiguousarray(wmu, np.float64)
+    nray = wmu.size
+    nf = int(nu.shape[0])
+    flags = (FP64 if fp64 else 0) | (DEVICE_PTRS if device else 0)
+    if device:
+        import torch
+        dev = atm["temp"].device
+        ie = torch.empty((nray, nf), dtype=torch.float32, device=dev)
+        flux = torch.empty(nf, dtype=torch.float32, device=dev)
+        itop = torch.empty((nray, a.ny, a.nx, nf), dtype=torch.float64 if fp64 else torch.float32,
+                           device=dev) if return_itop else None
+    else:
+        nu = np.ascontiguousarray(nu, np.float64)
+        llam = np.ascontiguousarray(llam, np.float64)
+        ie = np.empty((nray, nf), _F32)
+        flux = np.empty(nf, _F32)
+        itop = np.empty((nray, a.ny, a.nx, nf), np.float64 if fp64 else _F32) if return_itop else None
+    check(lib().m3d_lte_synthesis(C.byref(a), C.c_int(nf), ptr(nu), ptr(llam), C.c_int(nray), ptr(vec), ptr(wmu),
+                                  ptr(itop), ptr(ie), ptr(flux), C.c_uint(flags)), "m3d_lte_synthesis")
+    del keep
+    return ie, flux, itop

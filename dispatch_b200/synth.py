@@ -1,0 +1,279 @@
+"""Seeded synthetic atmospheres, line lists and frequency grids of the
+benchmark configurations (stand-ins for real model atmospheres and line lists).
+
+Grey atmosphere T^4 = 3/4 Teff^4 (tau + 2/3), Teff = 5800 K, log g = 4.4, a grey
+continuum kappa500 = 0.2 cm^2/g of pure absorption, hydrostatic equilibrium with
+mean molecular weight 1.26, n_H = rho/(1.4 m_H), n_e = 1e-4 n_H.  One line
+absorber per species (mass 56 u, A = 7.50, U = 25, vmic = 1 km/s by default).
+Random numbers: numpy PCG64 (default_rng(seed)).  3D cubes: a Gaussian random
+temperature field (periodic, correlation exp(-r^2/2l^2)) on the grey model,
+vertical velocities, density re-integrated hydrostatically per column.
+
+The per-cell quantities the line kernel takes are formed exactly as
+add_particle_opacity forms them (HOP/linelist_mod.f90:1000-1047,
+HOP/ion_mod.f90:198-225).
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+# const_mod.f90:38-73
+EE = 1.602189e-12
+HH = 6.626176e-27
+CC = 2.99792458e10
+EM = 9.109534e-28
+UU = 1.6605655e-24
+BK = 1.380662e-16
+ECH = 4.80325e-10
+MH = 1.6726e-24
+PI = 3.14159265359
+HZ_TO_AA = CC / 1e-8
+F_CONV = 8.0 * PI**2 * ECH**2 / EM / CC**3      # bbtrans_mod.f90:47
+C2_2H = CC**2 / 2.0 / HH
+H_4PI = HH * (1.0 / (4.0 * PI))
+BIJ_CONST = C2_2H * F_CONV * H_4PI               # linelist_mod.f90:53
+
+TEFF, LOGG, KAPPA500, MU_MOL = 5800.0, 4.4, 0.2, 1.26
+
+
+def grey_temperature(tau):
+    return (0.75 * TEFF**4 * (tau + 2.0 / 3.0)) ** 0.25
+
+
+def grey_model(log_tau):
+    """T, P, rho, n_H, n_e of the grey model at log10 tau500 (any shape)."""
+    tau = 10.0 ** np.asarray(log_tau, np.float64)
+    g = 10.0**LOGG
+    T = grey_temperature(tau)
+    P = g * tau / KAPPA500
+    rho = P * MU_MOL * MH / (BK * T)
+    nH = rho / (1.4 * MH)
+    return T, P, rho, nH, 1e-4 * nH
+
+
+def random_linelist(rng, n, lam0, lam1, loggf=(-3.0, 0.0), elow=(0.0, 5.0), adamp=(1e-3, 1e-1)):
+    """Lines uniform in [lam0, lam1] AA, sorted; returns raw parameters."""
+    lam = np.sort(rng.uniform(lam0, lam1, n))
+    return {"lam": lam, "loggf": rng.uniform(*loggf, n), "elow": rng.uniform(*elow, n),
+            "adamp": 10.0 ** rng.uniform(math.log10(adamp[0]), math.log10(adamp[1]), n)}
+
+
+def inverse_doppler_factor(temp, awgt, vmic_kms):
+    """ion_mod.f90:198-211, in real(4)."""
+    const = np.float32(2.0 * BK / UU)
+    temp = np.asarray(temp, np.float32)
+    dop = (const * temp) / np.float32(awgt)
+    if vmic_kms > 0:
+        dop = dop + np.float32((vmic_kms * 1e5) ** 2)
+    return (np.float32(CC) / np.sqrt(dop)).astype(np.float32)
+
+
+def compute_vbar2(temp, awgt):
+    """ion_mod.f90:214-225, in real(4)."""
+    const = np.float32(8.0 * BK / (PI * UU))
+    inv_mh = np.float32(UU / MH)
+    temp = np.asarray(temp, np.float32)
+    return ((const * temp) * (inv_mh + np.float32(1.0) / np.float32(awgt))).astype(np.float32)
+
+
+def species_arrays(raw, temp, n_x, awgt=56.0, part=25.0, vmic_kms=1.0):
+    """Line-list SoA and per-cell fields of one species (one isotope).
+
+    gpref = loggf ln10 + ln(bij_const/nu0) (line_types_mod.f90:30-35); the damping
+    drawn in Doppler widths is folded in as grad = a/idf at Teff, with no van der
+    Waals or Stark term (gw1 = gstk = 0)."""
+    lam = raw["lam"]
+    nu0 = HZ_TO_AA / lam
+    idf_ref = float(inverse_doppler_factor(np.float32(TEFF), awgt, vmic_kms))
+    n = lam.size
+    ll = {
+        "llam0": np.log(lam).astype(np.float64),
+        "lower_ev": raw["elow"].astype(np.float32),
+        "gpref": (raw["loggf"] * math.log(10.0) + np.log(BIJ_CONST / nu0)).astype(np.float32),
+        "grad": (raw["adamp"] / idf_ref).astype(np.float32),
+        "gw1": np.zeros(n, np.float32),
+        "gw2": np.zeros(n, np.float32),
+        "gstk": np.zeros(n, np.float32),
+        "unsold": np.zeros(n, np.uint8),
+    }
+    idf = inverse_doppler_factor(temp, awgt, vmic_kms)
+    vb2 = compute_vbar2(temp, awgt)
+    lnb = (np.log(np.maximum(np.asarray(n_x, np.float64), np.finfo(np.float64).tiny)).astype(np.float32)
+           - np.float32(math.log(part)) + np.log(idf).astype(np.float32))
+    ll.update({"inv_df": idf, "vbar2": vb2, "lnbase": lnb.astype(np.float32)})
+    return ll
+
+
+def cell_fields(temp, nH, ne):
+    """e_kT, ne, tothi, stark_pe per cell (composition_mod.f90:1719-1724)."""
+    temp = np.asarray(temp, np.float32)
+    return {"e_kT": (np.float32(EE / BK) / temp).astype(np.float32),
+            "ne": np.asarray(ne, np.float32),
+            "tothi": np.asarray(nH, np.float32),
+            "stark_pe": (np.asarray(ne, np.float32) * temp ** np.float32(1.0 / 6.0)).astype(np.float32)}
+
+
+def frequency_grid(lam0, lam1, nf):
+    """Uniform in ln(lambda): returns (llam, nu) ascending in llam."""
+    llam = np.linspace(math.log(lam0), math.log(lam1), nf)
+    return llam, HZ_TO_AA / np.exp(llam)
+
+
+def gaussian_field(rng, shape, ell, sigma):
+    """Periodic Gaussian random field with correlation exp(-r^2/2 ell^2), scaled to sigma."""
+    white = rng.standard_normal(shape)
+    if sigma == 0.0:
+        return np.zeros(shape)
+    k = [np.fft.fftfreq(n) * 2 * np.pi for n in shape]
+    kk = np.zeros(shape)
+    for i, ki in enumerate(k):
+        s = [1] * len(shape)
+        s[i] = -1
+        kk = kk + ki.reshape(s) ** 2
+    sk = ell / math.sqrt(2.0)
+    filt = np.exp(-0.5 * kk * sk**2)
+    f = np.real(np.fft.ifftn(np.fft.fftn(white) * filt))
+    f -= f.mean()
+    return f * (sigma / f.std())
+
+
+def cube_atmosphere(seed, nx, ny, nz, sigma_t=300.0, ell=8.0, sigma_vz_kms=2.0, log_tau=(-6.0, 2.0)):
+    """3D cube, z index 0 = bottom (deepest).  Returns dict of (nz, ny, nx) arrays
+    plus the cell size [cm]."""
+    rng = np.random.default_rng(seed)
+    # mean model on a fine tau grid -> geometric depth
+    lt = np.linspace(log_tau[1], log_tau[0], 4001)
+    T, P, rho, nH, _ = grey_model(lt)
+    tau = 10.0**lt
+    dz = np.concatenate([[0.0], -np.diff(tau) / (KAPPA500 * 0.5 * (rho[1:] + rho[:-1]))])
+    height = np.cumsum(dz)                      # 0 at the bottom (tau = 100), increasing upwards
+    zc = np.linspace(0.0, height[-1], nz + 1)
+    zc = 0.5 * (zc[1:] + zc[:-1])
+    ds_z = zc[1] - zc[0]
+    ltz = np.interp(zc, height, lt)
+    T0 = grey_temperature(10.0**ltz)
+    dT = gaussian_field(rng, (nz, ny, nx), ell, sigma_t)
+    temp = np.maximum(T0[:, None, None] + dT, 2500.0)
+    vz = gaussian_field(rng, (nz, ny, nx), ell, sigma_vz_kms) * 1e5
+    # hydrostatic per column from the top down: dP/dz = -rho g, rho = P mu m_H/(kT)
+    g = 10.0**LOGG
+    P = np.empty_like(temp)
+    _, Ptop, _, _, _ = grey_model(ltz[-1])
+    P[-1] = Ptop
+    for k in range(nz - 2, -1, -1):
+        Tm = 0.5 * (temp[k] + temp[k + 1])
+        P[k] = P[k + 1] * np.exp(g * MU_MOL * MH / (BK * Tm) * ds_z)
+    rho = P * MU_MOL * MH / (BK * temp)
+    nH = rho / (1.4 * MH)
+    ds_xy = ds_z * 2.0
+    return {"temp": temp.astype(np.float32), "rho": rho, "nH": nH, "ne": 1e-4 * nH,
+            "chi_c": (KAPPA500 * rho).astype(np.float32), "vz": (vz / CC).astype(np.float32),
+            "ds_cm": (ds_xy, ds_xy, ds_z)}
+
+
+def column_1d(ndep=80, log_tau=(-6.0, 2.0)):
+    """The 1D grey model on log tau uniform, z index 0 = bottom."""
+    lt = np.linspace(log_tau[1], log_tau[0], ndep)
+    T, P, rho, nH, ne = grey_model(lt)
+    tau = 10.0**lt
+    dz = -np.diff(tau) / (KAPPA500 * 0.5 * (rho[1:] + rho[:-1]))
+    return {"temp": T.astype(np.float32), "rho": rho, "nH": nH, "ne": ne,
+            "chi_c": (KAPPA500 * rho).astype(np.float32), "dz": dz}
+
+
+def lobatto_rays(ntheta=4, nphi=4):
+    """Output rays of set_lobatto_quadratures + nphi_copies with flux weights
+    (SRC/ray_mod.f90:224-262, 392-490): mu = 1 once, every other mu with nphi
+    azimuths; weights wmu/nphi times mu."""
+    tab = {4: ([1.0, 0.87174015, 0.59170018, 0.20929922], [0.03571428, 0.21070422, 0.34112270, 0.41245880]),
+           3: ([1.0, 0.76505532, 0.28523152], [0.06666667, 0.37847496, 0.55485838]),
+           2: ([1.0, 0.44721360], [0.16666667, 0.83333333])}
+    mu, wmu = tab[ntheta]
+    return _nphi_copies(nphi, np.array(mu), np.array(wmu))
+
+
+def gauss_rays(ntheta=5):
+    """Gauss-Legendre mu on (0, 1), plane parallel (one azimuth), flux weights."""
+    x, w = np.polynomial.legendre.leggauss(ntheta)
+    mu = 0.5 * (x + 1.0)
+    wmu = 0.5 * w
+    order = np.argsort(-mu)
+    return _nphi_copies(1, mu[order], wmu[order])
+
+
+def _nphi_copies(nphi, mu, wmu):
+    vec, wts = [], []
+    for m, w in zip(mu, wmu):
+        if m == 1.0:
+            vec.append([0.0, 0.0, 1.0])
+            wts.append(w)
+            continue
+        th = math.acos(m)
+        for p in range(nphi):
+            ph = 2.0 * math.pi / nphi * p
+            v = [math.sin(th) * math.cos(ph), math.sin(th) * math.sin(ph), m]
+            v = [0.0 if abs(c) < 1e-3 else c for c in v]
+            vec.append(v)
+            wts.append(w / nphi)
+    vec = np.array(vec, np.float64)
+    wts = np.array(wts, np.float64) * vec[:, 2]
+    return vec, wts
+
+
+def lte_config(kind: str, seed: int | None = None, nf: int | None = None, window: int = 0,
+               cube=None, lines=None):
+    """Inputs of one frequency window of a configuration, ready for
+    m3d_lte_synthesis.
+
+    kind: 'c0' (1D, 80 depths, 2000 lines in 5000-5100 AA, 20000 freq, 5 Gauss mu),
+          'c1' (3D 240^3 in 10 slabs, 500 lines in 5000-5020 AA, 4000 freq, 13 rays),
+          'mini' (a small 3D case for tests: 16x12x10, 2 slabs, 60 lines).
+    nf: frequencies per window (the run's n_windows split); window: which one."""
+    if kind == "c0":
+        seed = 0 if seed is None else seed
+        nxyz, nfree, lam = (1, 1, 80), 20000, (5000.0, 5100.0)
+        nline, nslab = 2000, 1
+    elif kind == "c1":
+        seed = 1 if seed is None else seed
+        nxyz, nfree, lam = (240, 240, 240), 4000, (5000.0, 5020.0)
+        nline, nslab = 500, 10
+    elif kind == "mini":
+        seed = 7 if seed is None else seed
+        nxyz, nfree, lam = (16, 12, 10), 400, (5000.0, 5004.0)
+        nline, nslab = 60, 2
+    else:
+        raise ValueError(kind)
+    nf = nfree if nf is None else nf
+    rng = np.random.default_rng(seed + 1000)
+    if lines is None:
+        lines = random_linelist(rng, nline, *lam)
+    nx, ny, nz = nxyz
+    if cube is None:
+        if kind == "c0":
+            # the grey column on 80 planes uniform in height over log tau500 in [-6, 2]
+            cube = cube_atmosphere(seed, 1, 1, nz, sigma_t=0.0, sigma_vz_kms=0.0, log_tau=(-6.0, 2.0))
+        else:
+            cube = cube_atmosphere(seed, nx, ny, nz)
+    temp, rho, nH, ne, chi_c, vz = (cube[k] for k in ("temp", "rho", "nH", "ne", "chi_c", "vz"))
+    ds_cm = cube["ds_cm"]
+    n_x = 10.0 ** (7.5 - 12.0) * nH
+    sp = species_arrays(lines, temp, n_x)
+    cf = cell_fields(temp, nH, ne)
+    llam_all, nu_all = frequency_grid(lam[0], lam[1], nfree)
+    sl = slice(window * nf, (window + 1) * nf)
+    ds_code = tuple(d / 1e8 for d in ds_cm)
+    slab_nz = [nz // nslab] * nslab
+    slab_nz[-1] += nz - sum(slab_nz)
+    atm = {"nx": nx, "ny": ny, "nz": nz, "slab_nz": slab_nz, "ds_cm": ds_cm, "ds_code": ds_code,
+           "pivot_z": nz * ds_code[2], "ray_offset": (0.0, 0.0),
+           "temp": np.ascontiguousarray(temp, np.float32).ravel(),
+           "chi_c": np.ascontiguousarray(chi_c, np.float32).ravel(),
+           "vx": np.zeros(temp.size, np.float32), "vy": np.zeros(temp.size, np.float32),
+           "vz": np.ascontiguousarray(vz, np.float32).ravel(),
+           "species": [{k: (np.ascontiguousarray(v).ravel() if k in ("inv_df", "vbar2", "lnbase") else v)
+                        for k, v in sp.items()}]}
+    atm.update({k: np.ascontiguousarray(v, np.float32).ravel() for k, v in cf.items()})
+    vec, wmu = gauss_rays(5) if kind == "c0" else lobatto_rays(4, 4)
+    return atm, np.ascontiguousarray(nu_all[sl]), np.ascontiguousarray(llam_all[sl]), vec, wmu

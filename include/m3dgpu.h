@@ -1,0 +1,223 @@
+/*
+ * m3dgpu.h -- C ABI of libm3dgpu.so, the B200 (sm_100a) radiative-transfer hot
+ * path of OpenMULTI3D: QLG-bot line opacity, the short- and long-characteristics
+ * formal solvers, the ALI accumulation and the LTE synthesis output pass.
+ *
+ * Conventions follow HOP's libhop.h (experiments/OpenMULTI3D/HOP/standalone/
+ * hop_c_api.f90:1-60):
+ *   - every function returns an int status, 0 = ok, > 0 = error, and
+ *     m3d_last_error(buf, len) gives the message;
+ *   - arrays belong to the caller; nothing is retained after a call returns,
+ *     except device buffers the library caches for its own scratch;
+ *   - floating arrays are float32 (float64 with M3D_FP64), integer arrays int32;
+ *   - multi-dimensional arrays use the reference's Fortran layout, first index
+ *     fastest: work(f, x, y, z, k), frequency fastest.
+ *
+ * Host or device pointers: without M3D_DEVICE_PTRS every array is a host buffer
+ * and the call copies it in and out synchronously; with M3D_DEVICE_PTRS every
+ * array is a device pointer on the current device and the call is ordered on the
+ * library stream (m3d_set_stream) and returns without synchronising.
+ *
+ * Thread safety: one process-wide context, not re-entrant, as libhop.
+ */
+#ifndef M3DGPU_H
+#define M3DGPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define M3D_OK 0
+#define M3D_EINVAL 1      /* invalid argument */
+#define M3D_ECUDA 2       /* CUDA runtime error */
+#define M3D_ENOINIT 3     /* m3d_init has not been called */
+#define M3D_EUNSUPPORTED 4
+#define M3D_ENONFINITE 5  /* a non-finite value where the reference stops */
+
+/* ---- flags ---- */
+#define M3D_DEVICE_PTRS 0x1u  /* array arguments are device pointers */
+#define M3D_FP64 0x2u         /* work/psi/irem/escape/mem are float64 (the plain FP64 path) */
+#define M3D_GET_PSI 0x4u      /* compute the Lambda diagonal (rt_patch_t%compute_psi) */
+#define M3D_SPLIT_RATES 0x8u  /* rate_formulation='largest': also Irem and escape */
+#define M3D_LINE_DIAG 0x10u   /* accumulate the line diagnostics used/strength/reach */
+#define M3D_ROTATE 0x20u      /* quadratic solver: apply rotate_array first (3D output pass) */
+
+/* ---- formal solvers (rt_patch_mod.f90:1649-1721, rt_params_mod.f90 solver names) ---- */
+#define M3D_SOLVER_LINEAR 0        /* long_char_linear, rt_solvers_mod.f90:666 ('linear', 1D) */
+#define M3D_SOLVER_LINEAR2 1       /* long_char2, rt_solvers_mod.f90:527 ('linear2', 1D) */
+#define M3D_SOLVER_QUADRATIC 2     /* long_char_quadratic, rt_solvers_mod.f90:891 ('quadratic') */
+#define M3D_SOLVER_SHORT_LINEAR 3  /* short_char, rt_solvers_mod.f90:19 ('linear', 3D) */
+#define M3D_SOLVER_SHORT_LINEAR2 4 /* short_char2, rt_solvers_mod.f90:224 ('linear2', 3D) */
+
+/* ---- upstream boundary (set_upstream_boundary, rt_patch_mod.f90:3270-3393) ---- */
+#define M3D_BND_MEM 0    /* the upstream slab's exit plane, mem(f,x,y,1:3) */
+#define M3D_BND_ZERO 1   /* top of the domain: no incoming radiation */
+#define M3D_BND_PCHIP 2  /* bottom: pchip_mono extrapolation of planes 1..3, Inu = Snu */
+#define M3D_BND_LTE 3    /* bottom: LTE ghost plane (lte_ghost) */
+
+/* One depth slab of one ray direction: the state rt_patch_t carries into a sweep.
+ * work is (nf, nx, ny, 0:nz+1, 3) with one ghost plane at each end. */
+typedef struct m3d_slab {
+  int nf, nx, ny, nz;
+  int dir;            /* +1: sweep towards increasing z (upward rays), -1: downward */
+  int get_psi;        /* also set by M3D_GET_PSI */
+  int split_rates;    /* also set by M3D_SPLIT_RATES */
+  int pad;
+  double ds[3];       /* cell size [cm] (ds * scaling%l) */
+  double vec[3];      /* ray direction, unit vector */
+  double maser_dtau_max; /* nlte_params maser_dtau_max, default 2 (m3d_patch_mod.f90:319) */
+  double maser_Inu_max;  /* nlte_params maser_Inu_max, default 1e30 (m3d_patch_mod.f90:320) */
+} m3d_slab_t;
+
+/* Line list of one isotope in structure-of-arrays form (line_types_mod.f90:22-75),
+ * sorted ascending in llam0. */
+typedef struct m3d_linelist {
+  int nline;
+  const double *llam0;          /* ln(lambda0 / AA) */
+  const float *lower_ev;        /* lower level energy [eV] */
+  const float *gpref;           /* loggf*ln10 + ln(bij_const/nu0) */
+  const float *grad, *gw1, *gw2, *gstk; /* damping coefficients (bbtrans_mod.f90:78-106) */
+  const unsigned char *unsold;  /* 1: Unsold van der Waals, 0: Barklem */
+  const int *lev_i, *lev_j;     /* NLTE level indices, 1-based, 0 = LTE; may be NULL */
+  const unsigned char *active;  /* may be NULL: every line active */
+} m3d_linelist_t;
+
+/* ---- context (hop_init / hop_free / hop_last_error counterparts) ---- */
+int m3d_init(int device, unsigned flags);
+int m3d_free(void);
+int m3d_last_error(char *buf, int buflen);
+int m3d_version(int *major, int *minor, int *patch);
+int m3d_set_stream(void *cuda_stream);        /* NULL: the library's own stream */
+int m3d_synchronize(void);
+/* Number of kernel launches the library has issued since m3d_init. */
+long long m3d_launch_count(void);
+/* Stage timing with CUDA events on the library stream (off by default).
+ * Stages: 0 line opacity + transfer units, 1 formal solution (sweep), 2 intensity
+ * reduction, 3 everything else.  m3d_profile_read synchronises and returns the
+ * accumulated milliseconds and launch count of one stage since it was enabled. */
+#define M3D_STAGE_OPACITY 0
+#define M3D_STAGE_SOLVE 1
+#define M3D_STAGE_REDUCE 2
+#define M3D_STAGE_OTHER 3
+int m3d_profile_enable(int on);
+int m3d_profile_read(int stage, double *ms, long long *launches);
+
+/* ---- K0: the transfer weights, elementwise over n points (diagnostics) ----
+ * which: 0 exp_neg (E, u0), 1 linear_weights (E, W, Psi, Esc), 2 parab_moments
+ * (E, U0, U1, q), 3 exp4 (y), 4 the library's fp32 log (y).
+ * Replaces exp_neg.inc:20-74 and rt_solvers_mod.f90:785-877. */
+int m3d_weights(int which, int n, const void *t, void *o1, void *o2, void *o3, void *o4, unsigned flags);
+
+/* ---- QLG-bot Voigt (qlg_mod.f90) ---- */
+/* qlg_init (qlg_mod.f90:364-375): copies the two 9020-entry tables to the device. */
+int m3d_qlg_init(void);
+/* The tables as built, for inspection (host buffers of 9020 floats). */
+int m3d_qlg_tables(float *tgx, float *th2x);
+/* qlg_bot_profile (qlg_mod.f90:682-689), elementwise over n points. */
+int m3d_qlg_bot_profile(int n, const float *a, const float *q, const float *vpr, const float *idf,
+                        float *h, unsigned flags);
+
+/* ---- line opacity: add_opacity_equi (linelist_mod.f90:729-960) ----
+ * chi, eta, cont, logref are (nf, ncell); the per-cell fields are (ncell); dep_mem
+ * is (ncell, nlevel).  chi and eta are accumulated in place.  used/strength/reach
+ * (nline each) are updated with M3D_LINE_DIAG, else may be NULL.
+ * Lines without a per-line reach (has_reach = .false.); no LTE scattering split. */
+int m3d_line_opacity(const m3d_linelist_t *ll, int nf, const double *llam, int ncell,
+                     float *chi, float *eta, const float *cont, const float *logref,
+                     const float *vproj, const float *inv_df, const float *vbar2, const float *e_kT,
+                     const float *lnbase, const float *ne, const float *tothi, const float *stark_pe,
+                     const float *dep_mem, int nlevel, int do_nlte, float tol, float line_reject_frac,
+                     unsigned char *used, float *strength, float *reach, unsigned flags);
+
+/* ---- background and work units ---- */
+/* beta = max(exp(-h nu/kT), tiny), Bnu = beta/(1-beta): (nf, ncell)
+ * (lte_background_opacities, rt_patch_mod.f90:2004-2023) */
+int m3d_lte_background(int nf, int ncell, const double *nu, const float *temp, float *beta,
+                       float *Bnu, unsigned flags);
+/* (xhat, ehat) -> (chi, Snu) in place, maser floor (work_to_transfer_units,
+ * rt_patch_mod.f90:3571-3651, without split rates or line scattering).
+ * n_floored (may be NULL) receives the number of floored points. */
+int m3d_work_to_transfer_units(int nf, int ncell, float *w1, float *w2, const float *beta,
+                               double maser_chi_floor, int suppress_masers, int *n_floored,
+                               unsigned flags);
+
+/* ---- formal solution of one slab (radiative_transfer, rt_patch_mod.f90:1649) ----
+ * psi, irem, escape are (nf, nx, ny, nz); chi500, chi500_up (this direction) are
+ * (nx, ny, nz) and g500 the ghost plane's chi500 (nx, ny) -- the linear2 solvers
+ * only.  eta_row (nx, ny, nz; 0 = no flags) and eta_mask (nf, nrows) are the
+ * update_eta_mask flags, may be NULL.  With M3D_ROTATE the quadratic solver first
+ * applies rotate_array to work(:,:,:,1:nz,1:2), which then holds the sheared
+ * chi and Snu as in the reference; rot_ds_code, rot_bot2pivot, rot_offset are
+ * rotate_array's cell size [code units], pivot height above the slab bottom and
+ * ray_offset [cells]. */
+int m3d_formal_solve(int solver, const m3d_slab_t *slab, void *work, void *psi, void *irem,
+                     void *escape, const float *chi500, const float *chi500_up, const float *g500,
+                     const int *eta_row, const unsigned char *eta_mask, const double *rot_ds_code,
+                     double rot_bot2pivot, const double *rot_offset, unsigned flags);
+
+/* rotate_array (rt_patch_mod.f90:3809-3866) on work(:,:,:,1:nz,1:2), in place. */
+int m3d_rotate_array(const m3d_slab_t *slab, void *work, const double *ds_code, double bot2pivot,
+                     const double *ray_offset, unsigned flags);
+
+/* set_upstream_boundary (rt_patch_mod.f90:3270-3393): fills the ghost plane of work.
+ * mem is (nf, nx, ny, 3) for M3D_BND_MEM; ghost_r500 = chi500_ghost/chi500(:,:,1)
+ * and ghost_temp (nx, ny) plus nu (nf) for M3D_BND_LTE; ds3_code is ds(3) in code
+ * units for M3D_BND_PCHIP. */
+int m3d_upstream_boundary(const m3d_slab_t *slab, void *work, int mode, const void *mem,
+                          float ds3_code, const float *ghost_r500, const float *ghost_temp,
+                          const double *nu, unsigned flags);
+
+/* ---- ALI accumulation: integrate_intensity (rt_patch_mod.f90:3399-3431) ----
+ * Jnu += 2 wmu I, PsiJ += 2 wmu Psi over n points (PsiJ, psi may be NULL). */
+int m3d_integrate_intensity(int n, float wmu, const float *inu, const float *psi, float *Jnu,
+                            float *PsiJ, unsigned flags);
+
+/* ---- LTE synthesis output pass of one frequency window ----
+ * The whole do_final branch of rt_patch_t%execute (rt_patch_mod.f90:1014-1030)
+ * for every direction and every depth slab of the column, bottom slab first:
+ * LTE background, line opacity of every species (add_linelist_opacities,
+ * composition_mod.f90:1663-1954), work_to_transfer_units, the bottom PCHIP ghost,
+ * rotate_array and long_char_quadratic with the exit plane handed from slab to
+ * slab, then save_intensity (rt_patch_mod.f90:4151-4208).
+ */
+typedef struct m3d_species {
+  m3d_linelist_t ll;
+  const float *inv_df;  /* (ncell) inverse Doppler factor c/v (ion_mod.f90:198) */
+  const float *vbar2;   /* (ncell) compute_vbar2 (ion_mod.f90:214) */
+  const float *lnbase;  /* (ncell) ln n - ln U + ln inv_df (linelist_mod.f90:1042-1047) */
+} m3d_species_t;
+
+typedef struct m3d_atmos {
+  int nx, ny, nz;          /* cells; plane z = 1 is the bottom of the domain */
+  int nslab;               /* depth slabs, bottom first */
+  const int *slab_nz;      /* planes per slab (nslab), each >= 2, summing to nz (host memory) */
+  double ds_cm[3];         /* cell size [cm] */
+  double ds_code[3];       /* cell size [code units], for rotate_array */
+  double pivot_z;          /* pivot height above the bottom of the domain [code units] */
+  double ray_offset[2];    /* [cells] */
+  const float *temp;       /* (ncell) [K] */
+  const float *chi_c;      /* (ncell) grey continuum extinction [1/cm], pure absorption */
+  const float *vx, *vy, *vz; /* (ncell) velocity [c] */
+  const float *e_kT, *ne, *tothi, *stark_pe; /* (ncell) */
+  int nspecies;
+  const m3d_species_t *species; /* host memory; the arrays inside follow M3D_DEVICE_PTRS */
+  double tol;              /* linelist_params tolerance, 1e-4 */
+  double maser_chi_floor;  /* 1e-4 */
+  double maser_dtau_max;   /* 2 */
+  double maser_Inu_max;    /* 1e30 */
+} m3d_atmos_t;
+
+/* nu (nf) [Hz], llam (nf) = ln(lambda/AA), uniform; vec (3, nray) (host), wmu (nray)
+ * flux weights (host).  Outputs: i_top (nf, nx, ny, nray) the emergent intensity in
+ * transfer units (may be NULL), ie (nf, nray) and flux (nf) as save_intensity writes
+ * them.  With M3D_FP64 the transfer units, rotation and solver run in FP64, one
+ * launch per ray and slab (the plain FP64 path); i_top is then float64. */
+int m3d_lte_synthesis(const m3d_atmos_t *atm, int nf, const double *nu, const double *llam,
+                      int nray, const double *vec, const double *wmu, void *i_top, float *ie,
+                      float *flux, unsigned flags);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* M3DGPU_H */

@@ -1,0 +1,648 @@
+/*
+ * m3d_oracle.c -- CPU restatement of OpenMULTI3D's radiative-transfer hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY: the checker of the CUDA library, loaded by tests/,
+ * __graft_entry__.smoke() and bench.py's CPU-baseline leg.  Nothing in the
+ * product links or calls it.  Build: oracle/Makefile (gcc -O2 -ffp-contract=off).
+ *
+ * Each routine cites the reference routine (file:line, paths relative to
+ * experiments/OpenMULTI3D/) whose arithmetic it restates.  Where the reference
+ * calls the platform libm exp/log on a path that decides an integer (a line's
+ * window), this file uses the reference's own fp32 exponential (exp_neg.inc)
+ * and an fp32 logarithm from the atanh series, written out op by op, so that
+ * the CUDA kernels can reproduce window indices bit for bit.
+ */
+#include <float.h>
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "m3d_oracle.h"
+
+/* const_mod.f90:38-73 */
+#define OR_HH 6.626176e-27
+#define OR_BK 1.380662e-16
+#define OR_CC 2.99792458e10
+#define OR_PI 3.14159265359
+#define OR_H_K (OR_HH / OR_BK)
+#define OR_CM_TO_AA 1e8
+
+static inline float f32_from_bits(uint32_t u) { float f; memcpy(&f, &u, 4); return f; }
+static inline uint32_t bits_from_f32(float f) { uint32_t u; memcpy(&u, &f, 4); return u; }
+
+/* =========================================================================
+ * K0: exp_neg, exp_neg0, exp4 (HOP/exp_neg.inc:20-74)
+ * ========================================================================= */
+static const float EXP_LOG2E = 1.44269504f, EXP_C1 = 0.693359375f, EXP_C2 = -2.12194440e-4f;
+static const float EXP_Q[6] = {+1.000000000e+00f, -5.000000000e-01f, +1.666666716e-01f,
+                               -4.167019576e-02f, +8.353385143e-03f, -1.351550105e-03f};
+
+/* exp(-t) and 1-exp(-t), neither formed from the other; t clamped at 87 */
+static inline void or_exp_neg1(float t, float *E, float *u0)
+{
+  float tc = fminf(t, 87.0f);
+  float n = roundf(tc * EXP_LOG2E);
+  float r = fmaf(-n, EXP_C2, fmaf(-n, EXP_C1, tc));
+  float p = fmaf(r, EXP_Q[5], EXP_Q[4]);
+  p = fmaf(r, p, EXP_Q[3]);
+  p = fmaf(r, p, EXP_Q[2]);
+  p = fmaf(r, p, EXP_Q[1]);
+  p = fmaf(r, p, EXP_Q[0]);
+  float m = r * p;
+  float s = f32_from_bits((uint32_t)(127 - (int)n) << 23);
+  *E = s * (1.0f - m);
+  *u0 = fmaf(s, m, 1.0f - s);
+}
+
+/* exp_neg0: E = 0 above t = 87, t clamped at -87 below */
+static inline void or_exp_neg0(float t, float *E, float *u0)
+{
+  or_exp_neg1(fmaxf(t, -87.0f), E, u0);
+  if (!(t <= 87.0f)) *E = 0.0f;
+}
+
+/* exp4(x) = exp_neg0(-x) */
+static inline float or_exp4(float x)
+{
+  float E, u0;
+  or_exp_neg0(-x, &E, &u0);
+  return E;
+}
+
+/* fp32 natural log for x > 0: x = 2^e m, m in [sqrt(1/2), sqrt(2)), log m =
+ * 2 atanh(s), s = (m-1)/(m+1), by its Taylor series to s^11 (|s| <= 0.1716);
+ * e ln2 with ln2 split so that e*LN2_HI is exact.  Used wherever the
+ * reference's libm log feeds a window index (logref, the floored reference,
+ * the van der Waals power). */
+static inline float or_logf1(float x)
+{
+  if (!(x > 0.0f)) return x == 0.0f ? -INFINITY : NAN;
+  if (x == INFINITY) return x;
+  int e = 0;
+  if (x < FLT_MIN) { x *= 8388608.0f; e = -23; }
+  uint32_t u = bits_from_f32(x);
+  e += (int)((u >> 23) & 0xff) - 127;
+  float m = f32_from_bits((u & 0x7fffffu) | 0x3f800000u);
+  if (m > 1.41421356f) { m *= 0.5f; e += 1; }
+  float f = m - 1.0f;
+  float s = f / (2.0f + f);
+  float s2 = s * s;
+  float p = fmaf(s2, 0.0909090936f, 0.111111112f);   /* 1/11, 1/9 */
+  p = fmaf(s2, p, 0.142857143f);                       /* 1/7 */
+  p = fmaf(s2, p, 0.200000003f);                       /* 1/5 */
+  p = fmaf(s2, p, 0.333333343f);                       /* 1/3 */
+  p = fmaf(s2, p, 1.0f);
+  float lm = (2.0f * s) * p;
+  float fe = (float)e;
+  float r = fmaf(fe, 1.42860677e-06f, lm);             /* ln2 - LN2_HI */
+  return fmaf(fe, 0.693145752f, r);                    /* LN2_HI = 0x3f317200 */
+}
+
+void or_exp_neg_f32(int n, const float *t, float *E, float *u0)
+{
+  for (int i = 0; i < n; i++) or_exp_neg1(t[i], &E[i], &u0[i]);
+}
+void or_exp4_f32(int n, const float *x, float *y)
+{
+  for (int i = 0; i < n; i++) y[i] = or_exp4(x[i]);
+}
+void or_log_f32(int n, const float *x, float *y)
+{
+  for (int i = 0; i < n; i++) y[i] = or_logf1(x[i]);
+}
+
+/* =========================================================================
+ * linear_weights / lw_series / parab_moments (rt_solvers_mod.f90:785-877)
+ * ========================================================================= */
+static const float LW_P[8] = {+5.000000000e-01f, -1.666666716e-01f, +4.166666791e-02f, -8.333330974e-03f,
+                              +1.388740959e-03f, -1.983609400e-04f, +2.522676368e-05f, -2.834696488e-06f};
+static const float PM_R[9] = {+3.333333433e-01f, -8.333329856e-02f, +1.666668802e-02f, -2.777901944e-03f,
+                              +3.968053206e-04f, -4.948913192e-05f, +5.514686109e-06f, -5.894584660e-07f,
+                              +5.153443894e-08f};
+
+static inline float or_lw_series(float t)
+{
+  float p = fmaf(t, LW_P[7], LW_P[6]);
+  for (int k = 5; k >= 0; k--) p = fmaf(t, p, LW_P[k]);
+  return t * p;
+}
+
+static inline void lw32(float t, float *E, float *W, float *Psi, float *Esc)
+{
+  float u0;
+  or_exp_neg1(t, E, &u0);
+  float ut = u0 / t;
+  float ps = or_lw_series(t);
+  int thin = fabsf(t) <= 1.0f;
+  *Psi = thin ? ps : 1.0f - ut;
+  *Esc = thin ? 1.0f - ps : ut;
+  *W = thin ? u0 - ps : ut - *E;
+}
+
+static inline void pm32(float t, float *E, float *U0, float *U1, float *q)
+{
+  or_exp_neg1(t, E, U0);
+  *U1 = fabsf(t) <= 1.0f ? t * or_lw_series(t) : t - *U0;
+  float p = fmaf(t, PM_R[8], PM_R[7]);
+  for (int k = 6; k >= 0; k--) p = fmaf(t, p, PM_R[k]);
+  float qs = (t * t) * p;
+  *q = fabsf(t) <= 2.0f ? qs : t - 2.0f * (*U1 / t);
+}
+
+/* plain FP64 weights: exact exp/expm1, Taylor series where the forms cancel */
+/* Taylor sums of the FP64 forms below |t| = 0.1, where the closed forms cancel:
+ * Psi = sum_{k>=1} (-1)^(k+1) t^k/(k+1)!, U1 = sum_{k>=2} (-1)^k t^k/k!,
+ * q = sum_{k>=3} 2 (-1)^(k+1) t^(k-1)/k!, each to 12 terms (truncation < 1e-17). */
+static inline double series64(double t, int k0, int shift, double scale)
+{
+  /* sum_{k=k0}^{k0+11} scale (-1)^k t^(k-shift)/k!, Horner from the top */
+  double fact = 1.0;
+  for (int k = 2; k <= k0 + 11; k++) fact *= k;
+  double p = 0.0;
+  for (int k = k0 + 11; k >= k0; k--) {
+    p = p * t + ((k & 1) ? -1.0 : 1.0) / fact;
+    fact /= (k > 1 ? k : 1);
+  }
+  double tp = 1.0;
+  for (int k = 0; k < k0 - shift; k++) tp *= t;
+  return scale * p * tp;
+}
+
+static inline void lw64(double t, double *E, double *W, double *Psi, double *Esc)
+{
+  double tc = fmin(t, 700.0);
+  *E = exp(-tc);
+  double u0 = -expm1(-tc);
+  if (fabs(t) < 0.1) {
+    /* Psi = sum_{k>=2} (-1)^k t^(k-1)/k! */
+    double ps = series64(t, 2, 1, 1.0);
+    *Psi = ps;
+    *Esc = 1.0 - ps;
+    *W = u0 - ps;
+  } else {
+    double ut = u0 / t;
+    *Psi = 1.0 - ut;
+    *Esc = ut;
+    *W = ut - *E;
+  }
+}
+
+static inline void pm64(double t, double *E, double *U0, double *U1, double *q)
+{
+  double tc = fmin(t, 700.0);
+  *E = exp(-tc);
+  *U0 = -expm1(-tc);
+  if (fabs(t) < 0.1) {
+    *U1 = series64(t, 2, 0, 1.0);
+    *q = series64(t, 3, 1, -2.0);
+  } else {
+    *U1 = t - *U0;
+    *q = t - 2.0 * (*U1 / t);
+  }
+}
+
+void or_linear_weights_f32(int n, const float *t, float *E, float *W, float *Psi, float *Esc)
+{
+  for (int i = 0; i < n; i++) lw32(t[i], &E[i], &W[i], &Psi[i], &Esc[i]);
+}
+void or_linear_weights_f64(int n, const double *t, double *E, double *W, double *Psi, double *Esc)
+{
+  for (int i = 0; i < n; i++) lw64(t[i], &E[i], &W[i], &Psi[i], &Esc[i]);
+}
+void or_parab_moments_f32(int n, const float *t, float *E, float *U0, float *U1, float *q)
+{
+  for (int i = 0; i < n; i++) pm32(t[i], &E[i], &U0[i], &U1[i], &q[i]);
+}
+void or_parab_moments_f64(int n, const double *t, double *E, double *U0, double *U1, double *q)
+{
+  for (int i = 0; i < n; i++) pm64(t[i], &E[i], &U0[i], &U1[i], &q[i]);
+}
+
+/* =========================================================================
+ * Stencil (ray_mod.f90:493-512) and Keys cubic kernel (ray_mod.f90:581-597)
+ * ========================================================================= */
+static void cc_kernel(double s, double k[4])
+{
+  double s2 = s * s, s3 = s2 * s;
+  k[0] = 0.5 * (-s3 + 2 * s2 - s);
+  k[1] = 0.5 * (3 * s3 - 5 * s2 + 2);
+  k[2] = 0.5 * (-3 * s3 + 4 * s2 + s);
+  k[3] = 0.5 * (s3 - s2);
+}
+
+void or_set_stencil(const double ds[3], const double vec[3], double xkern[4], double ykern[4],
+                    int *upo1, int *upo2, double *dsup)
+{
+  *dsup = ds[2] / fabs(vec[2]);
+  double wt1 = -vec[0] / ds[0] * *dsup;
+  double wt2 = -vec[1] / ds[1] * *dsup;
+  double h1 = wt1 > 0 ? wt1 : wt1 + 1;
+  double h2 = wt2 > 0 ? wt2 : wt2 + 1;
+  *upo1 = wt1 > 0 ? -1 : -2;
+  *upo2 = wt2 > 0 ? -1 : -2;
+  cc_kernel(h1, xkern);
+  cc_kernel(h2, ykern);
+}
+
+/* =========================================================================
+ * QLG (HOP/qlg_mod.f90)
+ * ========================================================================= */
+#define QLG_NX 9019
+static const float QLG_XSCL = 800.0f, QLG_RNX = 9019.0f;
+static const float QLG_OVERPI = 0.3183098862f, QLG_GNORM = 0.4697186f, QLG_SQL2 = 0.8325546112f;
+static const float QLG_RPI = 1.7724538509f, QLG_ISQPI = 0.5641895835f;
+
+/* Weideman (1994) N = 32 rational coefficients, qlg_mod.f90:134-151 */
+static const double W32_LD = 4.75682846001088411e+00;
+static const double W32_AD[32] = {
+    -1.30317978630500875e-12, +3.74107755472269789e-12, +8.03033538228436012e-12, -2.15435373143760700e-11,
+    -5.54423561143486540e-11, +1.16582546820233235e-10, +4.15374271614691897e-10, -5.23102143724924582e-10,
+    -3.20801514078875819e-09, +8.12488896568210460e-10, +2.37975567593842971e-08, +2.29304391194392872e-08,
+    -1.48130789124396946e-07, -4.18407637053084035e-07, +4.25583313792292626e-07, +4.40153173159092505e-06,
+    +6.82103194402497841e-06, -2.14096192018698432e-05, -1.30754492546239731e-04, -2.45329802700202065e-04,
+    +3.92591360700705167e-04, +4.51954110534923473e-03, +1.90061557848454077e-02, +5.73044035298371918e-02,
+    +1.40607162268937713e-01, +2.95444510715087261e-01, +5.46013972063934205e-01, +9.01925489364799993e-01,
+    +1.34554416923454490e+00, +1.82566962963248147e+00, +2.26353729990026764e+00, +2.57225340812456960e+00};
+
+/* Humlicek-Weideman fp64 hybrid, qlg_mod.f90:411-447 */
+void or_qlg_ref_f64(double a, double v0, double dv, int n, double *K)
+{
+  const double ISQPI8 = 0.564189583547756287;
+  double dr = W32_LD + a, nr0 = W32_LD - a;
+  for (int f = 0; f < n; f++) {
+    double v = v0 + (double)f * dv, av = fabs(v);
+    if (av + a >= 15.0) {
+      double tr = a * a - av * av + 0.5, ti = -2.0 * a * av;
+      double q = 1.0 / (tr * tr + ti * ti);
+      double ur = (a * tr + (-av) * ti) * q;
+      K[f] = ISQPI8 * ur;
+    } else {
+      double di = -v;
+      double q = 1.0 / (dr * dr + di * di);
+      double zr = (nr0 * dr + v * di) * q, zi = (v * dr - nr0 * di) * q;
+      double pr = W32_AD[0], pi_ = 0.0;
+      for (int j = 1; j < 32; j++) {
+        double t = pr * zr - pi_ * zi + W32_AD[j];
+        pi_ = pr * zi + pi_ * zr;
+        pr = t;
+      }
+      double ir = dr * q, ii = -di * q;
+      double sr = ir * ir - ii * ii, si = 2.0 * ir * ii;
+      K[f] = 2.0 * (pr * sr - pi_ * si) + ISQPI8 * ir;
+    }
+  }
+}
+
+/* Z_0.2(u)(1+u)^2, qlg_mod.f90:384-399 */
+static double qlg_wr02(double u)
+{
+  const double A2 = 0.18741813853432507, GAM = 0.93709069267162530, KP = 0.81924853602069690;
+  const double ETA = 0.14697983683153040, QRS = 0.16, DLN2 = 0.69314718055994531;
+  double v = GAM * sqrt(u), L = 1.0 / (1.0 + u), G = exp(-DLN2 * u), Kv;
+  or_qlg_ref_f64(A2, v, 0.0, 1, &Kv);
+  double P = KP * (ETA * L + (1.0 - ETA) * G);
+  return (Kv - P) / (QRS * KP) * (1.0 + u) * (1.0 + u);
+}
+
+/* qlg_init, qlg_mod.f90:364-375 */
+void or_qlg_tables(float *tgx, float *th2x)
+{
+  for (int i = 0; i <= QLG_NX; i++) {
+    double x = (double)i / 800.0;
+    tgx[i] = (float)pow(2.0, -x * x);
+    th2x[i] = (float)qlg_wr02(x * x);
+  }
+}
+
+typedef struct { float ih, bL, gG, cZH, cL2; } qlg_coef_t;
+
+/* bot_setup, qlg_mod.f90:538-554 */
+static inline qlg_coef_t bot_setup(float gL, float D, float SQ, float S)
+{
+  qlg_coef_t c;
+  float e = fmaf(gL, 0.60602209212341318f, D);
+  c.ih = e / fmaf(gL, e, SQ);
+  float r = gL * c.ih;
+  float q = r * (1.0f - r);
+  float sc = S * c.ih;
+  float qs = q * sc;
+  float x = 2.0f * r - 1.0f;
+  c.bL = (QLG_OVERPI * r) * sc;
+  c.gG = fmaf(qs, fmaf(x, -0.11019326278794868f, -0.064924393191013452f), (QLG_GNORM * (1.0f - r)) * sc);
+  c.cZH = qs * fmaf(x, -0.10567135279610407f, 0.38494195930078284f);
+  c.cL2 = qs * fmaf(x, 0.16241029253712097f, 0.04054415746208978f);
+  return c;
+}
+
+/* qlg_bot_line_eval, qlg_mod.f90:556-571 */
+static inline float bot_eval(const float *tgx, const float *th2x, const qlg_coef_t *c, float x)
+{
+  float xs = fabsf(x) * c->ih;
+  float u = xs * xs;
+  float L = 1.0f / (1.0f + u);
+  int ig = (int)lroundf(fminf(xs * QLG_XSCL, QLG_RNX));
+  float G = tgx[ig], W = th2x[ig];
+  float p = fmaf(c->cZH, W, c->cL2);
+  p = fmaf(L, p, c->bL);
+  return fmaf(L, p, G * c->gG);
+}
+
+/* qlg_bot_sweep (qlg_mod.f90:222-257) = bot_setup(a, 1, SQL2, RPI) + eval */
+void or_qlg_bot_sweep(const float *tgx, const float *th2x, float a, float v0, float dv, int n, float *K)
+{
+  qlg_coef_t c = bot_setup(a, 1.0f, QLG_SQL2, QLG_RPI);
+  for (int f = 0; f < n; f++) K[f] = bot_eval(tgx, th2x, &c, fmaf((float)f, dv, v0));
+}
+
+/* qlg_bot_profile, qlg_mod.f90:682-689 */
+void or_qlg_bot_profile(const float *tgx, const float *th2x, int n, const float *a, const float *q,
+                        const float *vpr, const float *idf, float *h)
+{
+  for (int i = 0; i < n; i++) {
+    float v = fabsf(q[i] - vpr[i]) * idf[i], K1;
+    or_qlg_bot_sweep(tgx, th2x, a[i], v, 0.0f, 1, &K1);
+    h[i] = ((K1 * QLG_ISQPI) * idf[i]) * (q[i] + 1.0f);
+  }
+}
+
+/* qlg_bot_line (qlg_mod.f90:616-627): setup plus half-width */
+typedef struct { float D, D2, SQ, D2h, D2G, D2L; } qlg_cell_t;
+static inline qlg_cell_t bot_cell(float D)
+{
+  qlg_cell_t w;
+  w.D = D;
+  w.D2 = D * D;
+  w.SQ = QLG_SQL2 * w.D2;
+  w.D2h = 0.5f * w.D2;
+  w.D2G = 1.5f * w.D2;
+  w.D2L = 5.0f * w.D2;
+  return w;
+}
+
+static inline float bot_halfwidth(const qlg_cell_t *w, float gL, float S, float ref, float lnq)
+{
+  float AL = ((QLG_OVERPI * gL) * S) / ref;
+  float h1 = fmaf(w->D2, lnq, fminf(AL, w->D2G));
+  float h2 = (AL - fmaxf(fmaf(gL, gL, -w->D2h), 0.0f)) + fminf(AL, w->D2L);
+  return sqrtf(fmaxf(fmaxf(h1, h2), 0.0f));
+}
+
+/* qlg_bot_line_sweep, qlg_mod.f90:646-671; returns the number of K values */
+static int line_sweep(const float *tgx, const float *th2x, const qlg_cell_t *w, float gL, float S,
+                      float ref, float lnq, int nf, const double *llam, double llc, double pos,
+                      double idl, float cap, int *fa, int *fb, float *hw, float *K)
+{
+  int ic = (int)lround(pos) + 1;
+  int i1 = ic < 1 ? 1 : (ic > nf ? nf : ic);
+  float x1 = (float)((llam[i1 - 1] - llc) * idl);
+  qlg_coef_t c = bot_setup(gL, w->D, w->SQ, S);
+  *hw = bot_halfwidth(w, gL, S, ref, lnq);
+  int noff = (int)lroundf(fminf(fminf(*hw, cap), (float)(nf + abs(ic))));
+  *fa = ic - noff > 1 ? ic - noff : 1;
+  *fb = ic + noff < nf ? ic + noff : nf;
+  if (*fa > *fb) return 0;
+  float x0 = x1 - (float)(i1 - *fa);
+  for (int f = 0; f <= *fb - *fa; f++) K[f] = bot_eval(tgx, th2x, &c, x0 + (float)f);
+  return *fb - *fa + 1;
+}
+
+int or_qlg_bot_line_sweep(const float *tgx, const float *th2x, float D, float gL, float S, float ref,
+                          float lnq, int nf, const double *llam, double llc, double pos, double idl,
+                          float cap, int *fa, int *fb, float *hw, float *K)
+{
+  qlg_cell_t w = bot_cell(D);
+  return line_sweep(tgx, th2x, &w, gL, S, ref, lnq, nf, llam, llc, pos, idl, cap, fa, fb, hw, K);
+}
+
+/* =========================================================================
+ * add_opacity_equi (HOP/linelist_mod.f90:729-960), without per-line reach
+ * (has_reach = .false.) and without the LTE scattering split (do_scat)
+ * ========================================================================= */
+int or_add_opacity_equi(const float *tgx, const float *th2x, const or_linelist_t *ll,
+                        int nf, const double *llam, int ncell,
+                        float *chi, float *eta, const float *cont, const float *logref,
+                        const float *vproj, const float *inv_df, const float *vbar2, const float *e_kT,
+                        const float *lnbase, const float *ne, const float *tothi, const float *stark_pe,
+                        const float *dep_mem, int nlevel, int do_nlte, float tol, float line_reject_frac,
+                        uint8_t *used, float *strength, float *reach)
+{
+  const float ex_cutoff = -85.0f, voigt_peak = 0.5641895835f, sqrt_pi = 1.7724538509f;
+  if (ll->nline == 0 || nf < 2) return 0;
+  if (llam[nf - 1] < llam[0]) return 1;
+  const double llam1 = llam[0];
+  const double dllam = (llam[nf - 1] - llam[0]) / (double)(nf - 1);
+  const double inv_dllam = 1.0 / dllam;
+  const float sdl = (float)inv_dllam;
+  const float flo_scale = fmaxf(tol, line_reject_frac) * tol;
+  float *Kbuf = (float *)malloc(sizeof(float) * (size_t)nf);
+  for (int i = 0; i < ncell; i++) {
+    float *ch = chi + (size_t)nf * i, *et = eta + (size_t)nf * i;
+    const float *co = cont + (size_t)nf * i, *lr = logref + (size_t)nf * i;
+    int f0_prev = -1;
+    float refl_c = 0, lref_c = 0;
+    const float idf = inv_df[i];
+    qlg_cell_t qw = bot_cell(sdl / idf);
+    const float lvb2 = or_logf1(vbar2[i]);
+    const float unsold_c = or_exp4(0.3f * lvb2) * tothi[i];
+    const float ekt = e_kT[i], ne_c = ne[i], tothi_c = tothi[i], starkpe = stark_pe[i];
+    const float vproj_c = vproj[i];
+    const float base = lnbase[i];
+    for (int l = 0; l < ll->nline; l++) {
+      if (ll->active && !ll->active[l]) continue;
+      double llc = ll->llam0[l] - (double)vproj_c;
+      double pos = (llc - llam1) * inv_dllam;
+      int f0 = (int)lround(pos) + 1;
+      f0 = f0 < 1 ? 1 : (f0 > nf ? nf : f0);
+      float ex = ll->lower_ev[l] * ekt;
+      float arg = (base + ll->gpref[l]) - ex;
+      if (arg < ex_cutoff) continue;
+      if (f0 != f0_prev) {
+        f0_prev = f0;
+        refl_c = tol * co[f0 - 1];
+        float flo = flo_scale * ch[f0 - 1];
+        if (flo > refl_c) {
+          refl_c = flo;
+          lref_c = or_logf1(flo * sqrt_pi);
+        } else {
+          lref_c = lr[f0 - 1];
+        }
+      }
+      if (arg <= lref_c) continue;
+      float Rij = or_exp4(arg);
+      float ref = refl_c;
+      if (voigt_peak * Rij <= ref) continue;
+      int nlte = do_nlte && ll->lev_i && ll->lev_j && ll->lev_i[l] > 0 && ll->lev_j[l] > 0;
+      float bi = 1.0f, bj = 1.0f;
+      if (nlte) {
+        bi = dep_mem[(size_t)i + (size_t)ncell * (ll->lev_i[l] - 1)];
+        bj = dep_mem[(size_t)i + (size_t)ncell * (ll->lev_j[l] - 1)];
+      }
+      float a = ll->grad[l];
+      if (ll->unsold[l]) a = fmaf(ll->gw1[l], unsold_c, a);
+      else a = fmaf(ll->gw1[l] * or_exp4(ll->gw2[l] * lvb2), tothi_c, a);
+      if (ll->gstk[l] >= 0.0f) a = fmaf(ll->gstk[l], ne_c, a);
+      else a = fmaf(-ll->gstk[l], starkpe, a);
+      a = a * sdl;
+      if (strength) {
+        float st = (voigt_peak * Rij) / co[f0 - 1];
+        if (st > strength[l]) strength[l] = st;
+      }
+      float lnq = arg - lref_c;
+      int fa, fb;
+      float hw;
+      int nk = line_sweep(tgx, th2x, &qw, a, Rij * qw.D, ref, lnq, nf, llam, llc, pos, inv_dllam,
+                          FLT_MAX, &fa, &fb, &hw, Kbuf);
+      if (reach) {
+        float rch = (float)((double)hw * dllam);
+        if (rch > reach[l]) reach[l] = rch;
+      }
+      if (nk == 0) continue;
+      if (used) used[l] = 1;
+      for (int f = fa; f <= fb; f++) {
+        float lte = Kbuf[f - fa];
+        ch[f - 1] = fmaf(lte, bi, ch[f - 1]);
+        et[f - 1] = fmaf(lte, bj, et[f - 1]);
+      }
+      f0_prev = -1;
+    }
+  }
+  free(Kbuf);
+  return 0;
+}
+
+/* =========================================================================
+ * Background and work units
+ * ========================================================================= */
+/* lte_background_opacities (rt_patch_mod.f90:2004-2023): beta, Bnu */
+void or_lte_background(int nf, int ncell, const double *nu, const float *temp, float *beta, float *Bnu)
+{
+  for (int i = 0; i < ncell; i++) {
+    float h_kT = (float)(OR_H_K / (double)temp[i]);
+    for (int f = 0; f < nf; f++) {
+      float hv = (float)(nu[f] * (double)h_kT), E, u0;
+      or_exp_neg1(hv, &E, &u0);
+      float b = fmaxf(E, FLT_MIN);
+      beta[(size_t)f + (size_t)nf * i] = b;
+      Bnu[(size_t)f + (size_t)nf * i] = b / (1.0f - b);
+    }
+  }
+}
+
+/* lte_background_emission with sigma = 0 (eta = chi_c Bnu, rt_patch_mod.f90:2309-2326)
+ * then convert_to_work_units (rt_patch_mod.f90:3518-3536): xhat = chi + eta,
+ * ehat = eta/beta.  chi_c is per cell (frequency independent grey continuum). */
+void or_lte_work(int nf, int ncell, const float *chi_c, const float *beta, const float *Bnu,
+                 float *xhat, float *ehat)
+{
+  for (int i = 0; i < ncell; i++)
+    for (int f = 0; f < nf; f++) {
+      size_t k = (size_t)f + (size_t)nf * i;
+      float etav = chi_c[i] * Bnu[k];
+      xhat[k] = chi_c[i] + etav;
+      ehat[k] = etav / beta[k];
+    }
+}
+
+/* logref of add_linelist_opacities (composition_mod.f90:1766-1772) */
+void or_logref(int n, const float *xhat, float tol, float *logref)
+{
+  const float voigt_peak = 0.5641895835f;
+  const float lt = or_logf1(tol / voigt_peak);
+  for (int i = 0; i < n; i++) logref[i] = xhat[i] > 0.0f ? lt + or_logf1(xhat[i]) : -FLT_MAX;
+}
+
+/* work_to_transfer_units without split rates or line scattering
+ * (rt_patch_mod.f90:3571-3651); returns the number of floored points */
+int or_work_to_transfer_units(int nf, int ncell, float *w1, float *w2, const float *beta,
+                              double maser_chi_floor, int suppress_masers)
+{
+  int nfl = 0;
+  const float fl = (float)maser_chi_floor;
+  for (size_t k = 0; k < (size_t)nf * ncell; k++) {
+    float xhat = w1[k];
+    float etav = w2[k] * beta[k];
+    float chi = xhat - etav;
+    float floor_ = fmaxf(fl * fabsf(xhat), FLT_MIN);
+    if (suppress_masers) chi = fmaxf(chi, floor_);
+    else if (fabsf(chi) < floor_) { chi = copysignf(floor_, chi); nfl++; }
+    w1[k] = chi;
+    w2[k] = etav / chi;
+  }
+  return nfl;
+}
+
+/* integrate_intensity (rt_patch_mod.f90:3399-3431) */
+void or_integrate_intensity(int nf, int ncell, float wmu, const float *work3, const float *psi,
+                            float *Jnu, float *PsiJ)
+{
+  float w2 = 2.0f * wmu;
+  for (size_t k = 0; k < (size_t)nf * ncell; k++) {
+    Jnu[k] = fmaf(w2, work3[k], Jnu[k]);
+    if (psi && PsiJ) PsiJ[k] = fmaf(w2, psi[k], PsiJ[k]);
+  }
+}
+
+/* save_intensity (rt_patch_mod.f90:4151-4208): ie = <I>_xy 2h nu^5/(c^3 AA),
+ * flux = 2 pi sum_mu wmu ie.  I_top is (nf, nx, ny, nmu). */
+void or_save_intensity(int nf, int nx, int ny, int nmu, const double *nu, const float *I_top,
+                       const double *wmu, float *ie, float *flux)
+{
+  const double conversion = 2.0 * OR_HH / (OR_CC * OR_CC * OR_CC * OR_CM_TO_AA);
+  for (int f = 0; f < nf; f++) flux[f] = 0.0f;
+  for (int mu = 0; mu < nmu; mu++) {
+    for (int f = 0; f < nf; f++) {
+      double n5 = nu[f] * nu[f] * nu[f] * nu[f] * nu[f];
+      float acc = 0.0f;
+      for (int y = 0; y < ny; y++)
+        for (int x = 0; x < nx; x++) {
+          float i3 = (float)(conversion * n5 * (double)I_top[(size_t)f + (size_t)nf * ((size_t)x + (size_t)nx * ((size_t)y + (size_t)ny * mu))]);
+          acc += i3;
+        }
+      ie[(size_t)f + (size_t)nf * mu] = acc / (float)(nx * ny);
+    }
+  }
+  for (int mu = 0; mu < nmu; mu++) {
+    float w = (float)(2.0 * OR_PI * wmu[mu]);
+    for (int f = 0; f < nf; f++) flux[f] = fmaf(w, ie[(size_t)f + (size_t)nf * mu], flux[f]);
+  }
+}
+
+/* =========================================================================
+ * Formal solvers, rotate_array and boundaries for REAL = float and double
+ * ========================================================================= */
+static inline float tiny_f32(void) { return FLT_MIN; }
+static inline float huge_f32(void) { return FLT_MAX; }
+static inline double tiny_f64(void) { return DBL_MIN; }
+static inline double huge_f64(void) { return DBL_MAX; }
+
+#define REAL float
+#define SFX(n) n##_f32
+#define FMA fmaf
+#define RABS fabsf
+#define RMAX fmaxf
+#define RMIN fminf
+#define RCOPYSIGN copysignf
+#define LW lw32
+#define PM pm32
+#include "or_solvers.inc"
+#undef REAL
+#undef SFX
+#undef FMA
+#undef RABS
+#undef RMAX
+#undef RMIN
+#undef RCOPYSIGN
+#undef LW
+#undef PM
+
+#define REAL double
+#define SFX(n) n##_f64
+#define FMA fma
+#define RABS fabs
+#define RMAX fmax
+#define RMIN fmin
+#define RCOPYSIGN copysign
+#define LW lw64
+#define PM pm64
+#include "or_solvers.inc"

@@ -1,0 +1,224 @@
+"""The oracle against the reference's in-source accuracy contracts and against
+analytic known answers (CPU only).
+
+Pins (the reference's own stated guarantees, cited):
+  * linear_weights: every output within 4 fp32 ulp of exact over -2 <= t <= 90
+    (SRC/rt_solvers_mod.f90:772-775); E is clamped at t = 87 by design (:774-775).
+  * parab_moments: within 4 ulp over -2 <= t <= 87 (SRC/rt_solvers_mod.f90:858-860).
+  * QLG-bot fit: 5.6923e-3 max relative error against qlg_ref_f64
+    (HOP/qlg_mod.f90:218-221); the tabulated fp32 form adds the nearest-node error.
+  * The window extent never ends inside the true tolerance crossing
+    (HOP/qlg_mod.f90:612-614).
+"""
+import math
+
+import numpy as np
+import pytest
+
+mpmath = pytest.importorskip("mpmath")
+mpmath.mp.dps = 40
+
+
+def _ulp_err(got, exact):
+    exact = np.asarray(exact, np.float64)
+    sp = np.spacing(np.abs(exact).astype(np.float32)).astype(np.float64)
+    return np.abs(np.asarray(got, np.float64) - exact) / sp
+
+
+def _sample_t(lo, hi, n, seed):
+    rng = np.random.default_rng(seed)
+    t = np.concatenate([rng.uniform(lo, hi, n), np.logspace(-7, 0, n // 4), -np.logspace(-7, math.log10(-lo), n // 4)])
+    return t.astype(np.float32)
+
+
+def test_linear_weights_within_4_ulp(oracle):
+    t = _sample_t(-2.0, 90.0, 1600, 1)
+    t = t[t != 0]
+    E, W, Psi, Esc = oracle.linear_weights(t)
+    ex = {k: [] for k in "EWPS"}
+    for tt in t.astype(np.float64):
+        x = mpmath.mpf(tt)
+        e = mpmath.e ** (-x)
+        u0 = -mpmath.expm1(-x)
+        ex["E"].append(float(e))
+        ex["W"].append(float(u0 / x - e))
+        ex["P"].append(float(1 - u0 / x))
+        ex["S"].append(float(u0 / x))
+    ok87 = t <= 87.0
+    assert _ulp_err(E[ok87], np.array(ex["E"])[ok87]).max() <= 4
+    assert _ulp_err(W, ex["W"]).max() <= 4
+    assert _ulp_err(Psi, ex["P"]).max() <= 4
+    assert _ulp_err(Esc, ex["S"]).max() <= 4
+
+
+def test_parab_moments_within_4_ulp(oracle):
+    t = _sample_t(-2.0, 87.0, 1600, 2)
+    t = t[t != 0]
+    E, U0, U1, q = oracle.parab_moments(t)
+    exE, exU0, exU1, exq = [], [], [], []
+    for tt in t.astype(np.float64):
+        x = mpmath.mpf(tt)
+        e = mpmath.e ** (-x)
+        u0 = -mpmath.expm1(-x)
+        u1 = x - u0
+        exE.append(float(e)); exU0.append(float(u0)); exU1.append(float(u1)); exq.append(float((x * x - 2 * u1) / x))
+    for got, ex in ((E, exE), (U0, exU0), (U1, exU1), (q, exq)):
+        assert _ulp_err(got, ex).max() <= 4
+
+
+def test_fp64_weights_exact(oracle):
+    t = np.concatenate([np.logspace(-9, 2, 300), -np.logspace(-9, 0.3, 100)])
+    E, W, Psi, Esc = oracle.linear_weights(t, fp64=True)
+    for i in range(0, t.size, 7):
+        x = mpmath.mpf(t[i])
+        u0 = -mpmath.expm1(-x)
+        assert abs(Psi[i] - float(1 - u0 / x)) <= 1e-14 * max(1.0, abs(float(1 - u0 / x)))
+        assert abs(W[i] - float(u0 / x - mpmath.e ** (-x))) <= 1e-14
+    E, U0, U1, q = oracle.parab_moments(t, fp64=True)
+    for i in range(0, t.size, 7):
+        x = mpmath.mpf(t[i])
+        u1 = x + mpmath.expm1(-x)
+        assert abs(U1[i] - float(u1)) <= 1e-13 * abs(float(u1)) + 1e-300
+        assert abs(q[i] - float((x * x - 2 * u1) / x)) <= 1e-12 * abs(float((x * x - 2 * u1) / x)) + 1e-300
+
+
+def test_exp4_and_log_accuracy(oracle):
+    x = np.linspace(-85.0, 85.0, 20001).astype(np.float32)
+    y = oracle.exp4(x)
+    assert _ulp_err(y, np.exp(x.astype(np.float64))).max() <= 2
+    assert oracle.exp4(np.array([-88.0, -100.0], np.float32)).tolist() == [0.0, 0.0]
+    x = np.float32(np.logspace(-37, 37, 20001))
+    y = oracle.logf(x)
+    assert _ulp_err(y, np.log(x.astype(np.float64))).max() <= 2
+    assert oracle.logf(np.array([1.0], np.float32))[0] == 0.0
+
+
+def _bot_exact_u(a, v):
+    """QLG-bot with G and Z_0.2 at the exact u (no table snap), fp64 -- the fit."""
+    from oracle import oracle as O
+    A2, GAM, KP, ETA, QRS = 0.18741813853432507, 0.93709069267162530, 0.81924853602069690, 0.14697983683153040, 0.16
+    d = 1 + a * 0.60602209212341318
+    ih = d / (a * d + 0.8325546112)
+    r = a * ih
+    q = r * (1 - r)
+    sc = 1.7724538509 * ih
+    qs = q * sc
+    x = 2 * r - 1
+    bL = (0.3183098862 * r) * sc
+    gG = (0.4697186 * (1 - r)) * sc + qs * (-0.064924393191013452 + x * (-0.11019326278794868))
+    cZH = qs * (0.38494195930078284 + x * (-0.10567135279610407))
+    cL2 = qs * (0.04054415746208978 + x * 0.16241029253712097)
+    u = (np.abs(v) * ih) ** 2
+    L = 1 / (1 + u)
+    G = 2.0 ** (-u)
+    vv = GAM * np.sqrt(u)
+    W = (O.qlg_ref_f64(A2, vv) - KP * (ETA * L + (1 - ETA) * np.exp(-math.log(2) * u))) / (QRS * KP) * (1 + u) ** 2
+    return G * gG + L * (bL + L * (cL2 + cZH * W))
+
+
+def test_qlg_bot_fit_error_matches_published(oracle):
+    worst_fit, worst_tab = 0.0, 0.0
+    v = np.concatenate([np.linspace(0, 12, 241), np.logspace(1.1, 3, 30)])
+    for a in np.logspace(-4, 3, 29):
+        ref = oracle.qlg_ref_f64(a, v)
+        worst_fit = max(worst_fit, (np.abs(_bot_exact_u(a, v) - ref) / ref).max())
+        K = np.array([oracle.qlg_bot_sweep(np.float32(a), np.float32(vi), 0.0, 1)[0] for vi in v])
+        worst_tab = max(worst_tab, (np.abs(K - ref) / ref).max())
+    # the published 5.6923e-3 is the fit's maximum; this sampling reaches within 1%
+    assert 5.0e-3 < worst_fit < 5.70e-3
+    # the nearest-node table lookup adds at most the snap of xi by 1/1600
+    assert worst_tab < 6.6e-3
+
+
+def test_qlg_tables(oracle):
+    tgx, th2x = oracle.qlg_tables()
+    i = np.arange(9020)
+    np.testing.assert_array_equal(tgx, (2.0 ** (-(i / 800.0) ** 2)).astype(np.float32))
+    assert th2x[0] == pytest.approx(((oracle.qlg_ref_f64(0.18741813853432507, np.array([0.0]))[0]
+                                      - 0.81924853602069690) / (0.16 * 0.81924853602069690)), rel=1e-6)
+    assert np.all(np.isfinite(th2x))
+
+
+def test_window_never_inside_tolerance_crossing(oracle):
+    """qlg_bot_line_sweep's half-width against the exact profile: beyond the
+    window the true opacity is below ref (HOP/qlg_mod.f90:612-614)."""
+    rng = np.random.default_rng(5)
+    nf = 4001
+    llam = np.arange(nf, dtype=np.float64)        # grid steps as the abscissa
+    for _ in range(60):
+        D = float(10 ** rng.uniform(-0.5, 1.5))       # Doppler width in grid steps
+        a = float(10 ** rng.uniform(-4, 2))           # damping in Doppler widths
+        lnq = float(rng.uniform(0.5, 25.0))
+        ref = 1.0
+        R = ref * math.sqrt(math.pi) * math.exp(lnq)  # peak R/sqrt(pi) = ref*q
+        pos = 2000.0 + float(rng.uniform(-0.5, 0.5))
+        fa, fb, hw, K = oracle.qlg_bot_line_sweep(np.float32(D), np.float32(a * D), np.float32(R * D),
+                                                   np.float32(ref), np.float32(lnq), llam, pos, pos, 1.0)
+        if fb >= nf or fa <= 1:
+            continue
+        # exact opacity just outside the window
+        for f in (fa - 2, fb):
+            v = (llam[f] - pos) / D
+            Kex = R * oracle.qlg_ref_f64(a, np.array([v]))[0] / math.sqrt(math.pi)
+            assert Kex <= ref * 1.0001, (D, a, lnq, f, fa, fb, Kex)
+
+
+def test_stencil_kernel_properties(oracle):
+    for vec in ([0.3, 0.2, math.sqrt(1 - 0.13)], [-0.5, 0.1, math.sqrt(1 - 0.26)], [0.0, 0.0, 1.0]):
+        xk, yk, u1, u2, dsup = oracle.set_stencil([1.0, 1.0, 1.0], vec)
+        assert xk.sum() == pytest.approx(1.0)
+        assert yk.sum() == pytest.approx(1.0)
+        assert dsup == pytest.approx(1.0 / abs(vec[2]))
+        # the kernel reproduces linear functions: first moment -k1 + k3 + 2k4 in [0, 1)
+        h = -xk[0] + xk[2] + 2 * xk[3]
+        assert 0.0 <= h <= 1.0
+        assert u1 in (-1, -2) and u2 in (-1, -2)
+
+
+def test_pchip_ghost_is_linear_extrapolation(oracle):
+    """With one ghost plane the reference's pchip_mono call reduces to 4 y1 - 3 y2,
+    clamped at 0 (interpol_mod.f90:289-365 with imin = imax = 1)."""
+    nf, nx, ny, nz = 3, 2, 2, 4
+    slab = oracle.make_slab(nf, nx, ny, nz, 1, [1e7, 1e7, 1e7], [0, 0, 1])
+    rng = np.random.default_rng(3)
+    work = rng.uniform(1.0, 2.0, (3, nz + 2, ny, nx, nf)).astype(np.float32)
+    work[:, 2] = work[:, 1] * 1.1
+    oracle.upstream_boundary(slab, work, oracle.BND_PCHIP, ds3_code=np.float32(0.1))
+    exp = np.maximum(4 * work[:2, 1].astype(np.float64) - 3 * work[:2, 2], 0)
+    np.testing.assert_allclose(work[:2, 0], exp, rtol=2e-6, atol=1e-6)
+    np.testing.assert_array_equal(work[2, 0], work[1, 0])
+
+
+def _column(nf=3, nz=40, S_of_tau=lambda t: 1.0 + 0 * t, chi=1e-7, ds=1e6):
+    tau = np.arange(nz + 2) * chi * ds
+    work = np.zeros((3, nz + 2, 1, 1, nf), np.float64)
+    work[0] = chi
+    for k in range(nz + 2):
+        work[1, k] = S_of_tau(tau[-1] - tau[k])
+    return work, tau
+
+
+@pytest.mark.parametrize("solver", ["linear", "quadratic"])
+def test_formal_solvers_reproduce_linear_source(oracle, solver):
+    """A source function linear in optical depth is integrated exactly by the
+    linear and (unlimited, monotone slope) quadratic steps: I(top) = S(tau=0) +
+    S'(tau) for a semi-infinite slab seen through tau >> 1 (here e^-tau ~ 0)."""
+    nz = 200
+    work, tau = _column(nz=nz, S_of_tau=lambda t: 2.0 + 0.5 * t, chi=3e-7, ds=1e6)
+    slab = oracle.make_slab(3, 1, 1, nz, 1, [1e6, 1e6, 1e6], [0, 0, 1])
+    work[2, 0] = work[1, 0] + 0.5   # incoming I at depth equals S + S' there
+    oracle.formal_solve(oracle.LINEAR if solver == "linear" else oracle.QUADRATIC, slab, work)
+    top = work[2, nz]
+    S0 = work[1, nz]
+    np.testing.assert_allclose(top, S0 + 0.5, rtol=1e-10)
+
+
+def test_quadrature_weights():
+    from dispatch_b200 import synth
+    vec, w = synth.lobatto_rays(4, 4)
+    assert vec.shape == (13, 3)
+    assert np.allclose(np.linalg.norm(vec, axis=1), 1.0)
+    assert w.sum() == pytest.approx(0.5, abs=0.01)     # flux weights integrate mu over mu in [0,1]
+    vec, w = synth.gauss_rays(5)
+    assert vec.shape == (5, 3)
+    assert w.sum() == pytest.approx(0.5, abs=1e-12)
