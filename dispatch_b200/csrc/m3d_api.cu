@@ -681,7 +681,7 @@ int solve_impl(int solver, const m3d_slab_t *s, unsigned flags, T *work, T *psi,
   switch (solver) {
     case M3D_SOLVER_LINEAR: {
       const float ds = (float)s->ds[2];
-      const T dsup05 = (T)(float)((double)(0.5f * ds) / fabs(s->vec[2]));
+      const T dsup05 = (T)((double)(0.5f * ds) / fabs(s->vec[2]));
       LAUNCH_S(M3D_STAGE_SOLVE, k_long_char_linear<T>, grid, block, 0, a, work, psi, irem, esc, dsup05);
       return M3D_OK;
     }
@@ -943,20 +943,26 @@ int m3d_lte_synthesis(const m3d_atmos_t *atm, int nf, const double *nu, const do
   TRY(st.map(ie, (size_t)nf * nray, false, true, &die));
 
   const int block = 256, warps = block / 32;
-  const size_t smem_op = (2 * QLG_NTAB + (size_t)warps * 4 * nf) * sizeof(float);
+  // windows of 32 frequencies take the lane-per-cell kernel, others the warp-per-cell one
+  const bool lane32 = nf == 32;
+  const size_t smem_op = lane32 ? 2 * QLG_NTAB * sizeof(float) + (size_t)warps * 32 * 33 * esz
+                                : (2 * QLG_NTAB + (size_t)warps * 4 * nf) * sizeof(float);
   {
-    static size_t attr32 = 0, attr64 = 0;
-    if (!fp64 && attr32 < smem_op) {
-      CUDA_TRY(cudaFuncSetAttribute(k_lte_opacity_units<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_op));
-      attr32 = smem_op;
-    }
-    if (fp64 && attr64 < smem_op) {
-      CUDA_TRY(cudaFuncSetAttribute(k_lte_opacity_units<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_op));
-      attr64 = smem_op;
+    static size_t attr[4] = {0, 0, 0, 0};
+    const int which = (lane32 ? 2 : 0) + (fp64 ? 1 : 0);
+    if (attr[which] < smem_op) {
+      const void *fn = lane32 ? (fp64 ? (const void *)k_lte_opacity_units_lane<32, double>
+                                      : (const void *)k_lte_opacity_units_lane<32, float>)
+                              : (fp64 ? (const void *)k_lte_opacity_units<double> : (const void *)k_lte_opacity_units<float>);
+      CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_op));
+      attr[which] = smem_op;
     }
   }
   int ogrid = (int)((ncell + warps - 1) / warps);
   if (ogrid > 148 * 16) ogrid = 148 * 16;
+  // lane kernel: one warp per 32 cells, grid-stride over warps
+  int lgrid = (int)((ncell + block - 1) / block);
+  if (lgrid > 148 * 2 * 8) lgrid = 148 * 2 * 8;
   const float dtmax = -(float)atm->maser_dtau_max, Imax = (float)atm->maser_Inu_max;
   const PchipConst pc = pchip_const((float)atm->ds_code[2]);
 
@@ -972,8 +978,12 @@ int m3d_lte_synthesis(const m3d_atmos_t *atm, int nf, const double *nu, const do
   for (int r = 0; r < nray; r++) {
     const double *v = vec + 3 * r;
     if (!fp64) {
-      LAUNCH_S(M3D_STAGE_OPACITY, k_lte_opacity_units<float>, ogrid, block, smem_op, A, G, dnu, v[0], v[1], v[2], (float *)dchi, (float *)dS,
-             g_ctx.d_tgx, g_ctx.d_th2x);
+      if (lane32)
+        LAUNCH_S(M3D_STAGE_OPACITY, (k_lte_opacity_units_lane<32, float>), lgrid, block, smem_op, A, G, dnu, v[0], v[1],
+                 v[2], (float *)dchi, (float *)dS, g_ctx.d_tgx, g_ctx.d_th2x);
+      else
+        LAUNCH_S(M3D_STAGE_OPACITY, k_lte_opacity_units<float>, ogrid, block, smem_op, A, G, dnu, v[0], v[1], v[2],
+                 (float *)dchi, (float *)dS, g_ctx.d_tgx, g_ctx.d_th2x);
       const QuadConst qc = quad_const(atm->ds_cm[2], v[2]);
       LAUNCH_S(M3D_STAGE_SOLVE, k_quad_rot_column, (int)((plane + 255) / 256), 256, 0, nf, nx, ny, nz, (const float *)dchi, (const float *)dS, (const RotPlane *)drot + (size_t)r * nz,
              (const int *)dz0, atm->nslab, qc, pc, dtmax, Imax, (float *)dtop + plane * r);
@@ -981,8 +991,12 @@ int m3d_lte_synthesis(const m3d_atmos_t *atm, int nf, const double *nu, const do
       LAUNCH_S(M3D_STAGE_REDUCE, k_save_intensity<float>, (nf + 31) / 32, sb, 0, nf, (int)ncol, dnu, (const float *)dtop + plane * r,
              die + (size_t)nf * r);
     } else {
-      LAUNCH_S(M3D_STAGE_OPACITY, k_lte_opacity_units<double>, ogrid, block, smem_op, A, G, dnu, v[0], v[1], v[2], (double *)dchi,
-             (double *)dS, g_ctx.d_tgx, g_ctx.d_th2x);
+      if (lane32)
+        LAUNCH_S(M3D_STAGE_OPACITY, (k_lte_opacity_units_lane<32, double>), lgrid, block, smem_op, A, G, dnu, v[0], v[1],
+                 v[2], (double *)dchi, (double *)dS, g_ctx.d_tgx, g_ctx.d_th2x);
+      else
+        LAUNCH_S(M3D_STAGE_OPACITY, k_lte_opacity_units<double>, ogrid, block, smem_op, A, G, dnu, v[0], v[1], v[2],
+                 (double *)dchi, (double *)dS, g_ctx.d_tgx, g_ctx.d_th2x);
       for (int s = 0; s < atm->nslab; s++) {
         const int n = atm->slab_nz[s];
         m3d_slab_t sl;

@@ -511,18 +511,17 @@ struct RotPlane { int up1, up2; float a, b, c, d; };
 
 template <typename T>
 __global__ void k_rotate_planes(int nf, int nx, int ny, int nz, const T *src, T *dst, const RotPlane *rot) {
-  // src, dst: (nf, nx, ny, 1:nz, 2) views starting at plane 1 of slot k (stride between slots sk)
+  // src, dst: (nf, nx, ny, nz) views of planes 1..nz of one slot of work
   const size_t plane = (size_t)nf * nx * ny;
-  const size_t n = plane * nz * 2;
+  const size_t n = plane * nz;
   for (size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x; g < n; g += (size_t)gridDim.x * blockDim.x) {
     const size_t inplane = g % plane;
-    const int zk = (int)(g / plane);
-    const int z = zk % nz, k = zk / nz;
+    const int z = (int)(g / plane);
     const int f = (int)(inplane % nf), x = (int)((inplane / nf) % nx), y = (int)(inplane / ((size_t)nf * nx));
     const RotPlane r = rot[z];
     const int x1 = wrap(x + r.up1, nx), x2 = wrap(x + r.up1 + 1, nx);
     const int y1 = wrap(y + r.up2, ny), y2 = wrap(y + r.up2 + 1, ny);
-    const T *p = src + plane * ((size_t)k * nz + z);
+    const T *p = src + plane * (size_t)z;
     T v = (T)r.a * p[(size_t)f + (size_t)nf * ((size_t)x1 + (size_t)nx * y1)];
     v = fma_t((T)r.b, p[(size_t)f + (size_t)nf * ((size_t)x2 + (size_t)nx * y1)], v);
     v = fma_t((T)r.c, p[(size_t)f + (size_t)nf * ((size_t)x1 + (size_t)nx * y2)], v);
@@ -539,10 +538,9 @@ __global__ void k_upstream_boundary(int nf, int nx, int ny, int nz, int dir, T *
                                     PchipConst pc, const float *ghost_r500, const float *ghost_temp,
                                     const double *nu) {
   const size_t plane = (size_t)nf * nx * ny;
-  const size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-  if (g >= plane) return;
   const int z = dir > 0 ? 0 : nz + 1, zi = dir > 0 ? 1 : -1;
   const size_t k1 = plane * (nz + 2);
+  for (size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x; g < plane; g += (size_t)gridDim.x * blockDim.x) {
   const size_t o = g + plane * z;
   if (mode == 1) {
     work[o] = 0; work[o + k1] = 0; work[o + 2 * k1] = 0;
@@ -569,6 +567,7 @@ __global__ void k_upstream_boundary(int nf, int nx, int ny, int nz, int dir, T *
     work[o + 2 * k1] = work[o + k1];
   } else {
     work[o] = mem[g]; work[o + k1] = mem[g + plane]; work[o + 2 * k1] = mem[g + 2 * plane];
+  }
   }
 }
 

@@ -129,6 +129,119 @@ __global__ void __launch_bounds__(256) k_lte_opacity_units(AtmosDev A, GridArgs 
   }
 }
 
+// ---------------------------------------------------------------------------
+// The same pass with one LANE per cell, for windows of NF frequencies: each lane
+// runs its own cell's line loop in line order and keeps chi_l, eta_l of the window
+// in registers, so no lane idles on the per-line scalar work and every line's window
+// is evaluated with one point per unrolled step.  The tolerance reference at a
+// line's nearest node f0 is formed on the spot (xhat and its log), and the
+// accumulated line opacity there is picked out of the register array.  The
+// results are bit-identical to k_lte_opacity_units.
+// ---------------------------------------------------------------------------
+template <int NF>
+__device__ __forceinline__ float pick(const float (&a)[NF], int i) {
+  float v = a[0];
+#pragma unroll
+  for (int k = 1; k < NF; k++) v = (k == i) ? a[k] : v;
+  return v;
+}
+
+template <int NF, typename TO>
+__global__ void __launch_bounds__(256, 2) k_lte_opacity_units_lane(AtmosDev A, GridArgs G, const double *nu, double v0,
+                                                                   double v1, double v2, TO *chi_out, TO *S_out,
+                                                                   const float *tgx, const float *th2x) {
+  extern __shared__ float smem[];
+  float *s_tgx = smem, *s_th2x = smem + QLG_NTAB;
+  stage_tables(s_tgx, s_th2x, tgx, th2x);
+  // per-warp transpose buffer for coalesced stores: 32 cells x (NF + 1) values of TO
+  TO *s_out = reinterpret_cast<TO *>(smem + 2 * QLG_NTAB) + (size_t)(threadIdx.x >> 5) * 32 * (NF + 1);
+  const int lane = threadIdx.x & 31;
+  const float ex_cutoff = -85.0f, voigt_peak = 0.5641895835f, sqrt_pi = 1.7724538509f;
+  const float lt = logf_m3d(G.tol / voigt_peak);
+  const int ncell = A.ncell;
+  const int nwarp_total = (gridDim.x * blockDim.x) >> 5;
+  const int ncell32 = (ncell + 31) / 32;
+  for (int cb = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; cb < ncell32; cb += nwarp_total) {
+    const int cell = cb * 32 + lane;
+    const bool live = cell < ncell;
+    const int cs = live ? cell : ncell - 1;
+    const float T = A.temp[cs], chi_c = A.chi_c[cs];
+    const float h_kT = (float)(M3D_H_K / (double)T);
+    float chl[NF], etl[NF];
+#pragma unroll
+    for (int f = 0; f < NF; f++) { chl[f] = 0.0f; etl[f] = 0.0f; }
+    const float vproj = (float)((v0 * (double)A.vx[cs] + v1 * (double)A.vy[cs]) + v2 * (double)A.vz[cs]);
+    const float ekt = A.e_kT[cs], ne = A.ne[cs], tothi = A.tothi[cs], starkpe = A.stark_pe[cs];
+    for (int sp = 0; sp < A.nspecies; sp++) {
+      const SpeciesDev &Sd = A.species[sp];
+      const LineArgs &L = Sd.L;
+      const float idf = Sd.inv_df[cs], base = Sd.lnbase[cs];
+      const QlgCell qw = qlg_cell(G.sdl / idf);
+      const float lvb2 = logf_m3d(Sd.vbar2[cs]);
+      const float unsold_c = exp4(0.3f * lvb2) * tothi;
+      for (int l = 0; l < L.nline; l++) {
+        if (L.active && !L.active[l]) continue;
+        const double llc = L.llam0[l] - (double)vproj;
+        const double pos = (llc - G.llam1) * G.inv_dllam;
+        const int ic = (int)lround(pos) + 1;
+        const int f0 = ic < 1 ? 1 : (ic > NF ? NF : ic);
+        const float ex = L.lower_ev[l] * ekt;
+        const float arg = (base + L.gpref[l]) - ex;
+        if (arg < ex_cutoff) continue;
+        const float cont0 = point_xhat(chi_c, h_kT, nu[f0 - 1]);
+        float refl = G.tol * cont0;
+        const float flo = G.flo_scale * pick<NF>(chl, f0 - 1);
+        float lref;
+        if (flo > refl) { refl = flo; lref = logf_m3d(flo * sqrt_pi); }
+        else lref = cont0 > 0.0f ? lt + logf_m3d(cont0) : -FLT_MAX;
+        if (arg <= lref) continue;
+        const float Rij = exp4(arg);
+        if (voigt_peak * Rij <= refl) continue;
+        const float a = line_damping_a(L, l, unsold_c, lvb2, tothi, ne, starkpe) * G.sdl;
+        const float S = Rij * qw.D;
+        const float x1 = (float)((G.llam[f0 - 1] - llc) * G.inv_dllam);
+        const QlgCoef cf = qlg_setup(a, qw.D, qw.SQ, S);
+        const float hw = qlg_halfwidth(qw, a, S, refl, arg - lref);
+        const int noff = (int)lroundf(fminf(fminf(hw, FLT_MAX), (float)(NF + abs(ic))));
+        const int fa = ic - noff > 1 ? ic - noff : 1;
+        const int fb = ic + noff < NF ? ic + noff : NF;
+        if (fa > fb) continue;
+        const float x0 = x1 - (float)(f0 - fa);
+#pragma unroll
+        for (int f = 0; f < NF; f++) {
+          if (f + 1 >= fa && f + 1 <= fb) {
+            const float K = qlg_eval(s_tgx, s_th2x, cf, x0 + (float)(f + 1 - fa));
+            chl[f] = fmaf(K, 1.0f, chl[f]);
+            etl[f] = fmaf(K, 1.0f, etl[f]);
+          }
+        }
+      }
+    }
+    // epilogue: transfer units, staged through shared memory for coalesced stores
+    for (int half = 0; half < 2; half++) {
+#pragma unroll
+      for (int f = 0; f < NF; f++) {
+        TO co, so;
+        if constexpr (sizeof(TO) == 4) {
+          point_units(chi_c, h_kT, nu[f], chl[f], etl[f], A.maser_chi_floor, co, so);
+        } else {
+          point_units((double)chi_c, (double)T, nu[f], (double)chl[f], (double)etl[f], (double)A.maser_chi_floor, co, so);
+        }
+        s_out[lane * (NF + 1) + f] = half == 0 ? co : so;
+      }
+      __syncwarp();
+      TO *dst = half == 0 ? chi_out : S_out;
+      for (int c = 0; c < 32; c++) {
+        const int cc = cb * 32 + c;
+        if (cc < ncell)
+          for (int f = lane; f < NF; f += 32) dst[(size_t)NF * cc + f] = s_out[c * (NF + 1) + f];
+      }
+      __syncwarp();
+    }
+    (void)live;
+  }
+}
+
 __device__ __forceinline__ void rot_load(const float *chi, const float *S, size_t plane, int zg, const RotPlane &r, int f,
                                          int x, int y, int nf, int nx, int ny, float &xv, float &sv) {
   const int x1 = wrap(x + r.up1, nx), x2 = x1 + 1 == nx ? 0 : x1 + 1;

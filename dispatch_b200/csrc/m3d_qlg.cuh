@@ -47,7 +47,7 @@ __device__ __forceinline__ float qlg_eval(const float *tgx, const float *th2x, c
   const float xs = fabsf(x) * c.ih;
   const float u = xs * xs;
   const float L = 1.0f / (1.0f + u);
-  const int ig = (int)lroundf(fminf(xs * 800.0f, 9019.0f));
+  const int ig = max((int)lroundf(fminf(xs * 800.0f, 9019.0f)), 0);
   const float G = tgx[ig], W = th2x[ig];
   float p = fmaf(c.cZH, W, c.cL2);
   p = fmaf(L, p, c.bL);

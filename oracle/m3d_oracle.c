@@ -342,6 +342,7 @@ static inline float bot_eval(const float *tgx, const float *th2x, const qlg_coef
   float u = xs * xs;
   float L = 1.0f / (1.0f + u);
   int ig = (int)lroundf(fminf(xs * QLG_XSCL, QLG_RNX));
+  if (ig < 0) ig = 0;
   float G = tgx[ig], W = th2x[ig];
   float p = fmaf(c->cZH, W, c->cL2);
   p = fmaf(L, p, c->bL);

@@ -67,10 +67,13 @@ def _line_case(seed, nline=150, nf=300, ncell=48, nlevel=4, recipes=True):
     _, _, _, nH, ne = synth.grey_model(lt)
     sp = synth.species_arrays(raw, temp, 10 ** -4.5 * nH)
     if recipes:
-        sp["gw1"] = (10 ** rng.uniform(-9, -7, nline)).astype(np.float32)
+        # damping constants already scaled by 1/(4 pi nu0), as the line list stores them
+        # (line_types_mod.f90:36): gamma6 ~ 1e-8 cm^3/s, gamma4 ~ 1e-5 cm^3/s
+        s4 = 1.0 / (4.0 * np.pi * (synth.HZ_TO_AA / raw["lam"]))
+        sp["gw1"] = (10 ** rng.uniform(-9, -7.5, nline) * s4).astype(np.float32)
         sp["gw2"] = rng.uniform(0.3, 0.45, nline).astype(np.float32)
         sp["unsold"] = (rng.uniform(size=nline) < 0.5).astype(np.uint8)
-        sp["gstk"] = (rng.choice([-1, 1], nline) * 10 ** rng.uniform(-7, -5, nline)).astype(np.float32)
+        sp["gstk"] = (rng.choice([-1, 1], nline) * 10 ** rng.uniform(-6, -5, nline) * s4).astype(np.float32)
     sp["lev_i"] = rng.integers(0, nlevel + 1, nline).astype(np.int32)
     sp["lev_j"] = rng.integers(0, nlevel + 1, nline).astype(np.int32)
     cf = synth.cell_fields(temp, nH, ne)
@@ -268,7 +271,7 @@ def test_integrate_intensity(m3d, oracle):
     np.testing.assert_array_equal(gP, oP)
 
 
-@pytest.mark.parametrize("kind,nf,window", [("mini", 64, 2), ("c0", 256, 31)])
+@pytest.mark.parametrize("kind,nf,window", [("mini", 64, 2), ("c0", 256, 31), ("mini", 32, 5), ("c0", 32, 200)])
 def test_lte_synthesis_matches_oracle(m3d, oracle, kind, nf, window):
     from dispatch_b200 import synth
     from oracle import pipeline as P
@@ -304,3 +307,24 @@ def test_lte_synthesis_device_pointers_match_host(m3d):
     np.testing.assert_array_equal(itop_d.cpu().numpy(), itop_h)
     np.testing.assert_array_equal(ie_d.cpu().numpy(), ie_h)
     np.testing.assert_array_equal(flux_d.cpu().numpy(), flux_h)
+
+
+def test_full_size_window_properties(m3d):
+    """The 240^3, 10-slab cube of the 3D LTE configuration, one window, two rays:
+    sizes where every launch needs many waves of blocks.  Size-independent
+    properties: the FP32 path is within 1e-4 of the plain FP64 path, intensities
+    are positive and finite, and lines only remove flux from the continuum."""
+    from dispatch_b200 import synth
+    cube = synth.cube_atmosphere(1, 240, 240, 240)
+    atm, nu, llam, vec, wmu = synth.lte_config("c1", nf=32, window=62, cube=cube)
+    vec, wmu = vec[[0, 12]], wmu[[0, 12]]
+    ie, flux, itop = m3d.lte_synthesis(atm, nu, llam, vec, wmu, return_itop=True)
+    ie64, flux64, _ = m3d.lte_synthesis(atm, nu, llam, vec, wmu, fp64=True)
+    assert np.all(np.isfinite(itop)) and np.all(itop > 0)
+    assert np.max(np.abs(flux - flux64) / flux64) <= 1e-4
+    assert np.max(np.abs(ie - ie64) / ie64) <= 1e-4
+    cont = dict(atm)
+    cont["species"] = []
+    _, fc, _ = m3d.lte_synthesis(cont, nu, llam, vec, wmu)
+    assert np.all(flux <= fc * (1 + 1e-6))
+    assert np.min(flux / fc) < 0.9
