@@ -42,20 +42,21 @@ def _args():
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-fp64", action="store_true")
+    p.add_argument("--cube", type=int, default=240, help="cube edge (240 = the configuration; smaller for profiling)")
     return p.parse_args()
 
 
-def _workload(nf):
-    return {"workload": "c1 3D LTE synthesis: 240^3 cube in 10 slabs of 24 planes, 500 lines 5000-5020 A, "
+def _workload(nf, n=240):
+    return {"workload": f"c1 3D LTE synthesis: {n}^3 cube in 10 slabs of {n // 10} planes, 500 lines 5000-5020 A, "
                         f"4000 frequencies in windows of {nf}, 13 rays (Lobatto 4x4), rotate_array + "
                         "long_char_quadratic; one step = one frequency window, all rays",
-            "cells": 240 ** 3, "rays": 13, "nf_window": nf, "nf_total": NFREQ_TOTAL, "slabs": 10,
+            "cells": n ** 3, "rays": 13, "nf_window": nf, "nf_total": NFREQ_TOTAL, "slabs": 10,
             "l2": "inputs larger than L2 (0.7 GB atmosphere + 3.5 GB transfer units per window)"}
 
 
-def _make_inputs(nf):
+def _make_inputs(nf, n=240):
     from dispatch_b200 import synth
-    atm, _, _, vec, wmu = synth.lte_config("c1", nf=nf, window=0)
+    atm, _, _, vec, wmu = synth.lte_config("c1", nf=nf, window=0, size=None if n == 240 else n)
     llam_all, nu_all = synth.frequency_grid(5000.0, 5020.0, NFREQ_TOTAL)
     return atm, llam_all, nu_all, vec, wmu
 
@@ -135,13 +136,14 @@ def _peaks():
         return None
 
 
-def _traffic_from_profiles(nf):
-    """dram bytes per k_quad_rot_column launch from the committed ncu summary, scaled to nf."""
-    path = os.path.join(ROOT, "profiles", "k_quad_rot_column_c1.md")
+def _traffic_from_profiles(ncell, nf):
+    """dram bytes per k_quad_rot_column launch: the committed ncu figure per cell and
+    frequency (a small case of the same kernel) times this launch's cells and frequencies."""
+    path = os.path.join(ROOT, "profiles", "k_quad_rot_column_c1_48.md")
     try:
         for line in open(path):
-            if line.startswith("dram_bytes_per_launch_per_frequency:"):
-                return float(line.split(":")[1]) * nf
+            if line.startswith("dram_bytes_per_cell_frequency:"):
+                return float(line.split(":")[1]) * ncell * nf
     except OSError:
         pass
     return None
@@ -231,7 +233,7 @@ def run_b200(a):
     stream = torch.cuda.current_stream()
     m.set_stream(stream.cuda_stream)
     nf = a.nf
-    atm, llam_all, nu_all, vec, wmu = _make_inputs(nf)
+    atm, llam_all, nu_all, vec, wmu = _make_inputs(nf, a.cube)
     ncell = atm["nx"] * atm["ny"] * atm["nz"]
     nray = wmu.size
     work_per_step = nray * ncell * nf
@@ -285,7 +287,7 @@ def run_b200(a):
     peak = peaks["hbm_gbs"] if peaks else 6650.0
     bytes_launch = 8.0 * ncell * nf                          # chi and Snu read once per ray point frequency
     achieved = bytes_launch / (sv_ms / sv_n / 1e3) / 1e9 if sv_n else None
-    traffic = _traffic_from_profiles(nf)
+    traffic = _traffic_from_profiles(ncell, nf)
     roofline = {"kernel": "k_quad_rot_column (rotate_array + long_char_quadratic, all slabs)", "bound": "hbm",
                 "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak if achieved else None,
                 "traffic": traffic, "peak_source": "measured" if peaks else "fallback",
@@ -330,9 +332,15 @@ def run_b200(a):
         torch.cuda.synchronize()
         t64 = e0.elapsed_time(e1)
         err = float(torch.max(torch.abs(f32 - f64) / torch.abs(f64)).item())
+        m.profile_enable(True)
+        m.lte_synthesis(datm, nu_d, llam_d, vec, wmu, device=True, fp64=True)
+        sv64_ms, sv64_n = m.profile_read(m.STAGE_SOLVE)
+        m.profile_enable(False)
         fp64 = {"value": work_per_step / (t64 / 1e3) / 1e9, "unit": UNIT, "ms_per_step": t64,
                 "fp32_over_fp64": value / ws / (work_per_step / (t64 / 1e3) / 1e9),
                 "max_rel_flux_err_fp32_vs_fp64": err,
+                "solve_ms_per_step": sv64_ms, "solve_launches": sv64_n,
+                "solve_fp32_over_fp64": sv64_ms / sv_ms if sv_ms else None,
                 "path": "same kernels in FP64 for units, rotation and solver, one launch per ray and slab"}
 
     cpu = None
@@ -346,7 +354,7 @@ def run_b200(a):
         return
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32", "data": "synthetic (seeded grey cube, random line list)", "config": _workload(nf),
+            "dtype": "f32", "data": "synthetic (seeded grey cube, random line list)", "config": _workload(nf, a.cube),
             "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline, "cpu_baseline": cpu,
             "clocks": clocks, "stages": stages, "fp64_plain": fp64}
     print(json.dumps(line), flush=True)

@@ -223,13 +223,14 @@ def _nphi_copies(nphi, mu, wmu):
 
 
 def lte_config(kind: str, seed: int | None = None, nf: int | None = None, window: int = 0,
-               cube=None, lines=None):
+               cube=None, lines=None, size: int | None = None):
     """Inputs of one frequency window of a configuration, ready for
     m3d_lte_synthesis.
 
     kind: 'c0' (1D, 80 depths, 2000 lines in 5000-5100 AA, 20000 freq, 5 Gauss mu),
           'c1' (3D 240^3 in 10 slabs, 500 lines in 5000-5020 AA, 4000 freq, 13 rays),
           'mini' (a small 3D case for tests: 16x12x10, 2 slabs, 60 lines).
+    size: an n^3 cube in place of the configuration's own (same lines, slabs, rays).
     nf: frequencies per window (the run's n_windows split); window: which one."""
     if kind == "c0":
         seed = 0 if seed is None else seed
@@ -245,6 +246,8 @@ def lte_config(kind: str, seed: int | None = None, nf: int | None = None, window
         nline, nslab = 60, 2
     else:
         raise ValueError(kind)
+    if size is not None:
+        nxyz = (size, size, size)
     nf = nfree if nf is None else nf
     rng = np.random.default_rng(seed + 1000)
     if lines is None:
