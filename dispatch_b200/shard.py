@@ -1,0 +1,52 @@
+"""Frequency windows across ranks (one process per GPU).
+
+The reference splits the spectrum into n_windows frequency windows whose
+opacities and sweeps are independent for all rays (E/SRC/ray_patch_mod.f90:97-127).
+A rank takes every world-th window; the spectra of the windows a rank computed
+are gathered to every rank only for output, and the step time reported is the
+maximum over ranks.  Nothing on the data path is exchanged.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def windows_for_rank(rank: int, world: int, nwin: int) -> list[int]:
+    """Round-robin: rank r takes windows r, r + world, r + 2 world, ..."""
+    if not (0 <= rank < world):
+        raise ValueError(f"rank {rank} outside world {world}")
+    return list(range(rank, nwin, world))
+
+
+def gather_spectrum(local: dict[int, np.ndarray], nwin: int, nf: int) -> np.ndarray:
+    """Assemble the full spectrum (nwin * nf) from every rank's {window: flux(nf)}
+    with torch.distributed (any backend); ranks must call it together."""
+    import torch
+    import torch.distributed as dist
+
+    world = dist.get_world_size()
+    rank = dist.get_rank()
+    mine = windows_for_rank(rank, world, nwin)
+    if sorted(local) != mine:
+        raise ValueError(f"rank {rank} holds windows {sorted(local)}, expected {mine}")
+    nmax = len(windows_for_rank(0, world, nwin))
+    buf = torch.zeros((nmax, nf), dtype=torch.float64)
+    for i, w in enumerate(mine):
+        buf[i] = torch.as_tensor(np.asarray(local[w], np.float64))
+    parts = [torch.zeros_like(buf) for _ in range(world)]
+    dist.all_gather(parts, buf)
+    out = np.zeros((nwin, nf))
+    for r in range(world):
+        for i, w in enumerate(windows_for_rank(r, world, nwin)):
+            out[w] = parts[r][i].numpy()
+    return out.ravel()
+
+
+def max_over_ranks(ms: float) -> float:
+    """The slowest rank's time, the figure a weak-scaling step reports."""
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([ms], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())

@@ -1,0 +1,51 @@
+"""Window sharding across ranks: world-size-2 gloo processes on CPU."""
+import os
+
+import numpy as np
+import pytest
+
+
+def test_windows_partition():
+    from dispatch_b200.shard import windows_for_rank
+    for world in (1, 2, 3, 8):
+        got = sorted(w for r in range(world) for w in windows_for_rank(r, world, 125))
+        assert got == list(range(125))
+    with pytest.raises(ValueError):
+        windows_for_rank(2, 2, 10)
+
+
+def _worker(rank, world, port, q):
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        from dispatch_b200.shard import gather_spectrum, max_over_ranks, windows_for_rank
+        nwin, nf = 7, 4
+        local = {w: np.arange(nf) + 100.0 * w for w in windows_for_rank(rank, world, nwin)}
+        full = gather_spectrum(local, nwin, nf)
+        t = max_over_ranks(10.0 + rank)
+        q.put((rank, full.tolist(), t))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_gather_and_max_over_two_gloo_ranks():
+    import multiprocessing as mp
+    import socket
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=120) for _ in procs]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    exp = (np.arange(4)[None, :] + 100.0 * np.arange(7)[:, None]).ravel()
+    for rank, full, t in res:
+        np.testing.assert_array_equal(full, exp)
+        assert t == 11.0
