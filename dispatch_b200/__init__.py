@@ -32,7 +32,7 @@ EXPORTS = ("m3d_init", "m3d_free", "m3d_last_error", "m3d_version", "m3d_set_str
            "m3d_launch_count", "m3d_weights", "m3d_qlg_init", "m3d_qlg_tables", "m3d_qlg_bot_profile",
            "m3d_line_opacity", "m3d_lte_background", "m3d_work_to_transfer_units", "m3d_formal_solve",
            "m3d_rotate_array", "m3d_upstream_boundary", "m3d_integrate_intensity", "m3d_lte_synthesis",
-           "m3d_profile_enable", "m3d_profile_read")
+           "m3d_profile_enable", "m3d_profile_read", "m3d_rotate_array_noalloc")
 
 
 class M3DError(RuntimeError):

@@ -1050,3 +1050,108 @@ int m3d_lte_synthesis(const m3d_atmos_t *atm, int nf, const double *nu, const do
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// rotate_array without any allocation.
+//
+// Some callers cannot let the library allocate device memory: a host program
+// that hands all device memory to its own pool (PyTorch's caching allocator, a
+// preallocated arena) leaves nothing for cudaMalloc, and a program that drives
+// the device from several host threads at once cannot afford the device-wide
+// synchronisation that cudaMalloc/cudaFree imply.  This entry point therefore
+// takes its scratch from a fixed array in the library's own device image,
+// M3D_NOALLOC_SCRATCH_BYTES (8 MiB) large, which every GPU that loads the
+// library holds until the process exits.  It rotates one plane at a time
+// through that array, so the limit is one plane, nf*nx*ny values.
+// ===========================================================================
+namespace {
+
+constexpr size_t M3D_NOALLOC_SCRATCH_BYTES = (size_t)8 << 20;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[M3D_NOALLOC_SCRATCH_BYTES];
+// device address of g_noalloc_scratch, looked up once per device
+void *g_noalloc_addr[64] = {};
+
+int noalloc_scratch(void **out) {
+  int dev = 0;
+  CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return fail(M3D_EUNSUPPORTED, "device %d: no-alloc scratch supports devices 0..63", dev);
+  if (!g_noalloc_addr[dev]) {
+    void *p = nullptr;
+    CUDA_TRY(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    g_noalloc_addr[dev] = p;
+  }
+  *out = g_noalloc_addr[dev];
+  return M3D_OK;
+}
+
+// the rotate_array weights of local plane z, formed as rot_planes forms them
+RotPlane rot_plane_at(const double vec[3], const double ds_code[3], double bot2pivot, const double ray_offset[2],
+                      int z) {
+  const float delta0 = (float)(vec[0] / (vec[2] * ds_code[0]));
+  const float delta1 = (float)(vec[1] / (vec[2] * ds_code[1]));
+  const float b2p = (float)bot2pivot;
+  const float height = (float)((double)z * ds_code[2]);
+  const float dk0 = (float)((double)((b2p - height) * delta0) + ray_offset[0]);
+  const float dk1 = (float)((double)((b2p - height) * delta1) + ray_offset[1]);
+  const int up1 = (int)floorf(dk0), up2 = (int)floorf(dk1);
+  const float f1 = dk0 - (float)up1, f2 = dk1 - (float)up2;
+  RotPlane r;
+  r.up1 = up1;
+  r.up2 = up2;
+  r.a = (1.0f - f1) * (1.0f - f2);
+  r.b = f1 * (1.0f - f2);
+  r.c = (1.0f - f1) * f2;
+  r.d = f1 * f2;
+  return r;
+}
+
+// one plane of rotate_array into dst, the weights passed by value
+template <typename T>
+__global__ void k_rotate_one_plane(int nf, int nx, int ny, const T *src, T *dst, RotPlane r) {
+  const size_t plane = (size_t)nf * nx * ny;
+  for (size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x; g < plane; g += (size_t)gridDim.x * blockDim.x) {
+    const int f = (int)(g % nf), x = (int)((g / nf) % nx), y = (int)(g / ((size_t)nf * nx));
+    const int x1 = wrap(x + r.up1, nx), x2 = wrap(x + r.up1 + 1, nx);
+    const int y1 = wrap(y + r.up2, ny), y2 = wrap(y + r.up2 + 1, ny);
+    T v = (T)r.a * src[(size_t)f + (size_t)nf * ((size_t)x1 + (size_t)nx * y1)];
+    v = fma_t((T)r.b, src[(size_t)f + (size_t)nf * ((size_t)x2 + (size_t)nx * y1)], v);
+    v = fma_t((T)r.c, src[(size_t)f + (size_t)nf * ((size_t)x1 + (size_t)nx * y2)], v);
+    v = fma_t((T)r.d, src[(size_t)f + (size_t)nf * ((size_t)x2 + (size_t)nx * y2)], v);
+    dst[g] = v;
+  }
+}
+
+template <typename T>
+int rotate_noalloc_t(const m3d_slab_t *s, T *dwork, const double *ds_code, double bot2pivot,
+                     const double *ray_offset) {
+  const size_t plane = (size_t)s->nf * s->nx * s->ny;
+  if (plane * sizeof(T) > M3D_NOALLOC_SCRATCH_BYTES)
+    return fail(M3D_EINVAL, "m3d_rotate_array_noalloc: a plane of %zu values (%zu bytes) exceeds the %zu-byte scratch",
+                plane, plane * sizeof(T), M3D_NOALLOC_SCRATCH_BYTES);
+  void *tmp = nullptr;
+  TRY(noalloc_scratch(&tmp));
+  const double off0[2] = {0.0, 0.0};
+  const double *off = ray_offset ? ray_offset : off0;
+  for (int k = 0; k < 2; k++)
+    for (int z = 1; z <= s->nz; z++) {
+      T *p = dwork + plane * ((size_t)z + (size_t)k * (s->nz + 2));
+      LAUNCH(k_rotate_one_plane<T>, grid_for(plane), 256, 0, s->nf, s->nx, s->ny, (const T *)p, (T *)tmp,
+             rot_plane_at(s->vec, ds_code, bot2pivot, off, z));
+      CUDA_TRY(cudaMemcpyAsync(p, tmp, sizeof(T) * plane, cudaMemcpyDeviceToDevice, g_ctx.stream));
+    }
+  return M3D_OK;
+}
+
+}  // namespace
+
+extern "C" int m3d_rotate_array_noalloc(const m3d_slab_t *slab, void *work, const double *ds_code, double bot2pivot,
+                                        const double *ray_offset, unsigned flags) {
+  TRY(need_init());
+  TRY(check_slab(slab));
+  if (!work || !ds_code) return fail(M3D_EINVAL, "m3d_rotate_array_noalloc: NULL work or ds_code");
+  if (!(flags & M3D_DEVICE_PTRS))
+    return fail(M3D_EINVAL, "m3d_rotate_array_noalloc: work must be a device pointer (M3D_DEVICE_PTRS); "
+                            "staging host buffers would allocate");
+  if (flags & M3D_FP64) return rotate_noalloc_t<double>(slab, (double *)work, ds_code, bot2pivot, ray_offset);
+  return rotate_noalloc_t<float>(slab, (float *)work, ds_code, bot2pivot, ray_offset);
+}

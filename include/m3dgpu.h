@@ -160,6 +160,22 @@ int m3d_formal_solve(int solver, const m3d_slab_t *slab, void *work, void *psi, 
 int m3d_rotate_array(const m3d_slab_t *slab, void *work, const double *ds_code, double bot2pivot,
                      const double *ray_offset, unsigned flags);
 
+/* m3d_rotate_array for callers that cannot let the library allocate device memory
+ * (programs whose own pool holds all device memory, or that drive the device from
+ * several host threads where cudaMalloc/cudaFree would stall the other streams).
+ * It has no counterpart in the reference.  It allocates nothing: its scratch is one
+ * fixed 8 MiB array inside the library's device image, held by every GPU that loads
+ * the library until the process exits, so one plane (nf*nx*ny values of the chosen
+ * precision) may use at most 8 MiB; larger slabs are rejected with M3D_EINVAL.
+ * work must be a device pointer (M3D_DEVICE_PTRS is required; M3D_FP64 optional).
+ * The first call on a device looks up the array's device address on that device
+ * (cudaGetSymbolAddress); make that first call before any stream capture.  All
+ * calls share the one array, so calls that overlap on the GPU (on different streams
+ * at the same time) race; each call overwrites the scratch before reading it, so
+ * nothing in it has to start at zero.  Results are bit-identical to m3d_rotate_array. */
+int m3d_rotate_array_noalloc(const m3d_slab_t *slab, void *work, const double *ds_code, double bot2pivot,
+                             const double *ray_offset, unsigned flags);
+
 /* set_upstream_boundary (rt_patch_mod.f90:3270-3393): fills the ghost plane of work.
  * mem is (nf, nx, ny, 3) for M3D_BND_MEM; ghost_r500 = chi500_ghost/chi500(:,:,1)
  * and ghost_temp (nx, ny) plus nu (nf) for M3D_BND_LTE; ds3_code is ds(3) in code
