@@ -24,6 +24,7 @@ struct Ctx {
   int device = 0;
   cudaStream_t own = nullptr, stream = nullptr;
   float *d_tgx = nullptr, *d_th2x = nullptr;
+  float2 *d_tab = nullptr;  // (TGX(i), TH2X(i)) interleaved, read by the kernels
   std::vector<float> h_tgx, h_th2x;
   long long launches = 0;
   std::string err;
@@ -242,6 +243,10 @@ int ensure_tables() {
   g_ctx.d_th2x = g_ctx.d_tgx + QLG_NTAB;
   CUDA_TRY(cudaMemcpy(g_ctx.d_tgx, g_ctx.h_tgx.data(), QLG_NTAB * sizeof(float), cudaMemcpyHostToDevice));
   CUDA_TRY(cudaMemcpy(g_ctx.d_th2x, g_ctx.h_th2x.data(), QLG_NTAB * sizeof(float), cudaMemcpyHostToDevice));
+  std::vector<float2> tab(QLG_NTAB);
+  for (int i = 0; i < QLG_NTAB; i++) tab[i] = make_float2(g_ctx.h_tgx[i], g_ctx.h_th2x[i]);
+  CUDA_TRY(cudaMalloc(&g_ctx.d_tab, QLG_NTAB * sizeof(float2)));
+  CUDA_TRY(cudaMemcpy(g_ctx.d_tab, tab.data(), QLG_NTAB * sizeof(float2), cudaMemcpyHostToDevice));
   return M3D_OK;
 }
 
@@ -423,6 +428,8 @@ int m3d_free(void) {
   g_ctx.ev_free.clear();
   if (g_ctx.d_tgx) cudaFree(g_ctx.d_tgx);
   g_ctx.d_tgx = g_ctx.d_th2x = nullptr;
+  if (g_ctx.d_tab) cudaFree(g_ctx.d_tab);
+  g_ctx.d_tab = nullptr;
   if (g_ctx.own) cudaStreamDestroy(g_ctx.own);
   g_ctx.own = g_ctx.stream = nullptr;
   g_ctx.init = false;
@@ -528,7 +535,7 @@ int m3d_qlg_bot_profile(int n, const float *a, const float *q, const float *vpr,
   float *dh;
   TRY(st.in(a, n, &da)); TRY(st.in(q, n, &dq)); TRY(st.in(vpr, n, &dv)); TRY(st.in(idf, n, &di));
   TRY(st.map(h, n, false, true, &dh));
-  LAUNCH(k_qlg_profile, grid_for(n), 256, 0, n, g_ctx.d_tgx, g_ctx.d_th2x, da, dq, dv, di, dh);
+  LAUNCH(k_qlg_profile, grid_for(n), 256, 0, n, g_ctx.d_tab, da, dq, dv, di, dh);
   return st.finish();
 }
 
@@ -579,7 +586,7 @@ int m3d_line_opacity(const m3d_linelist_t *ll, int nf, const double *llam, int n
   int grid = (ncell + warps - 1) / warps;
   if (grid > 148 * 8) grid = 148 * 8;
   LAUNCH_S(M3D_STAGE_OPACITY, k_line_opacity, grid, block, smem, L, G, ncell, dchi, deta, dcont, dlr, dvp, didf, dvb, dek, dlb, dne, dth,
-         dsp, ddep, do_nlte, diag ? 1 : 0, dused, dstr, dreach, g_ctx.d_tgx, g_ctx.d_th2x);
+         dsp, ddep, do_nlte, diag ? 1 : 0, dused, dstr, dreach, g_ctx.d_tab);
   return st.finish();
 }
 
@@ -920,10 +927,16 @@ int m3d_lte_synthesis(const m3d_atmos_t *atm, int nf, const double *nu, const do
         rot_planes(vec + 3 * r, atm->ds_code, b2p, atm->ray_offset, atm->slab_nz[s], out);
       }
     }
+  // the fused sweep takes the periodic offsets reduced to [0, n)
+  std::vector<RotCol> rotc(rot.size());
+  for (size_t i = 0; i < rot.size(); i++) {
+    int ux = rot[i].up1 % nx, uy = rot[i].up2 % ny;
+    rotc[i] = RotCol{ux < 0 ? ux + nx : ux, uy < 0 ? uy + ny : uy, rot[i].a, rot[i].b, rot[i].c, rot[i].d};
+  }
   void *drot, *dz0;
-  TRY(scratch(5, sizeof(RotPlane) * rot.size(), &drot));
+  TRY(scratch(5, sizeof(RotCol) * rotc.size(), &drot));
   TRY(scratch(6, sizeof(int) * z0.size(), &dz0));
-  CUDA_TRY(cudaMemcpyAsync(drot, rot.data(), sizeof(RotPlane) * rot.size(), cudaMemcpyHostToDevice, g_ctx.stream));
+  CUDA_TRY(cudaMemcpyAsync(drot, rotc.data(), sizeof(RotCol) * rotc.size(), cudaMemcpyHostToDevice, g_ctx.stream));
   CUDA_TRY(cudaMemcpyAsync(dz0, z0.data(), sizeof(int) * z0.size(), cudaMemcpyHostToDevice, g_ctx.stream));
 
   // transfer units of the whole column (one ray at a time) and the emergent planes
@@ -945,7 +958,7 @@ int m3d_lte_synthesis(const m3d_atmos_t *atm, int nf, const double *nu, const do
   const int block = 256, warps = block / 32;
   // windows of 32 frequencies take the lane-per-cell kernel, others the warp-per-cell one
   const bool lane32 = nf == 32;
-  const size_t smem_op = lane32 ? 2 * QLG_NTAB * sizeof(float) + (size_t)warps * 32 * 33 * esz
+  const size_t smem_op = lane32 ? 2 * QLG_NTAB * sizeof(float)
                                 : (2 * QLG_NTAB + (size_t)warps * 4 * nf) * sizeof(float);
   {
     static size_t attr[4] = {0, 0, 0, 0};
@@ -962,9 +975,14 @@ int m3d_lte_synthesis(const m3d_atmos_t *atm, int nf, const double *nu, const do
   if (ogrid > 148 * 16) ogrid = 148 * 16;
   // lane kernel: one warp per 32 cells, grid-stride over warps
   int lgrid = (int)((ncell + block - 1) / block);
-  if (lgrid > 148 * 2 * 8) lgrid = 148 * 2 * 8;
+  if (lgrid > 148 * 3 * 8) lgrid = 148 * 3 * 8;
   const float dtmax = -(float)atm->maser_dtau_max, Imax = (float)atm->maser_Inu_max;
   const PchipConst pc = pchip_const((float)atm->ds_code[2]);
+
+  // partial sums of the intensity reduction
+  const int kParts = 148;
+  void *dpart;
+  TRY(scratch(12, sizeof(double) * kParts * nf, &dpart));
 
   // FP64 plain path buffers
   void *dwork = nullptr, *dmem = nullptr;
@@ -980,23 +998,24 @@ int m3d_lte_synthesis(const m3d_atmos_t *atm, int nf, const double *nu, const do
     if (!fp64) {
       if (lane32)
         LAUNCH_S(M3D_STAGE_OPACITY, (k_lte_opacity_units_lane<32, float>), lgrid, block, smem_op, A, G, dnu, v[0], v[1],
-                 v[2], (float *)dchi, (float *)dS, g_ctx.d_tgx, g_ctx.d_th2x);
+                 v[2], (float *)dchi, (float *)dS, g_ctx.d_tab);
       else
         LAUNCH_S(M3D_STAGE_OPACITY, k_lte_opacity_units<float>, ogrid, block, smem_op, A, G, dnu, v[0], v[1], v[2],
-                 (float *)dchi, (float *)dS, g_ctx.d_tgx, g_ctx.d_th2x);
+                 (float *)dchi, (float *)dS, g_ctx.d_tab);
       const QuadConst qc = quad_const(atm->ds_cm[2], v[2]);
-      LAUNCH_S(M3D_STAGE_SOLVE, k_quad_rot_column, (int)((plane + 255) / 256), 256, 0, nf, nx, ny, nz, (const float *)dchi, (const float *)dS, (const RotPlane *)drot + (size_t)r * nz,
+      LAUNCH_S(M3D_STAGE_SOLVE, k_quad_rot_column, (int)((plane + 255) / 256), 256, 0, nf, nx, ny, nz, (const float *)dchi, (const float *)dS, (const RotCol *)drot + (size_t)r * nz,
              (const int *)dz0, atm->nslab, qc, pc, dtmax, Imax, (float *)dtop + plane * r);
-      dim3 sb(32, 8);
-      LAUNCH_S(M3D_STAGE_REDUCE, k_save_intensity<float>, (nf + 31) / 32, sb, 0, nf, (int)ncol, dnu, (const float *)dtop + plane * r,
-             die + (size_t)nf * r);
+      LAUNCH_S(M3D_STAGE_REDUCE, k_save_partial<float>, dim3((nf + 31) / 32, kParts), dim3(32, 8), 0, nf, (int)ncol,
+               dnu, (const float *)dtop + plane * r, (double *)dpart);
+      LAUNCH_S(M3D_STAGE_REDUCE, k_save_final, (nf + 127) / 128, 128, 0, nf, (int)ncol, kParts, (const double *)dpart,
+               die + (size_t)nf * r);
     } else {
       if (lane32)
         LAUNCH_S(M3D_STAGE_OPACITY, (k_lte_opacity_units_lane<32, double>), lgrid, block, smem_op, A, G, dnu, v[0], v[1],
-                 v[2], (double *)dchi, (double *)dS, g_ctx.d_tgx, g_ctx.d_th2x);
+                 v[2], (double *)dchi, (double *)dS, g_ctx.d_tab);
       else
         LAUNCH_S(M3D_STAGE_OPACITY, k_lte_opacity_units<double>, ogrid, block, smem_op, A, G, dnu, v[0], v[1], v[2],
-                 (double *)dchi, (double *)dS, g_ctx.d_tgx, g_ctx.d_th2x);
+                 (double *)dchi, (double *)dS, g_ctx.d_tab);
       for (int s = 0; s < atm->nslab; s++) {
         const int n = atm->slab_nz[s];
         m3d_slab_t sl;
@@ -1021,9 +1040,10 @@ int m3d_lte_synthesis(const m3d_atmos_t *atm, int nf, const double *nu, const do
       }
       CUDA_TRY(cudaMemcpyAsync((double *)dtop + plane * r, (double *)dmem + 2 * plane, sizeof(double) * plane,
                                cudaMemcpyDeviceToDevice, g_ctx.stream));
-      dim3 sb(32, 8);
-      LAUNCH_S(M3D_STAGE_REDUCE, k_save_intensity<double>, (nf + 31) / 32, sb, 0, nf, (int)ncol, dnu, (const double *)dtop + plane * r,
-             die + (size_t)nf * r);
+      LAUNCH_S(M3D_STAGE_REDUCE, k_save_partial<double>, dim3((nf + 31) / 32, kParts), dim3(32, 8), 0, nf,
+               (int)ncol, dnu, (const double *)dtop + plane * r, (double *)dpart);
+      LAUNCH_S(M3D_STAGE_REDUCE, k_save_final, (nf + 127) / 128, 128, 0, nf, (int)ncol, kParts, (const double *)dpart,
+               die + (size_t)nf * r);
     }
   }
   TRY(st.finish());

@@ -22,6 +22,10 @@ __device__ __forceinline__ int wrap(int v, int n) { v %= n; return v < 0 ? v + n
 
 constexpr double M3D_H_K = 6.626176e-27 / 1.380662e-16;  // h/k (const_mod.f90:39,43,71)
 
+// correctly rounded reciprocal: the same value as the IEEE quotient 1/x
+__device__ __forceinline__ float recip(float x) { return __frcp_rn(x); }
+__device__ __forceinline__ double recip(double x) { return __drcp_rn(x); }
+
 template <typename T> __device__ __forceinline__ T tmin(T a, T b) { return a < b ? a : b; }
 template <typename T> __device__ __forceinline__ T tmax(T a, T b) { return a > b ? a : b; }
 __device__ __forceinline__ float tmin(float a, float b) { return fminf(a, b); }
@@ -59,12 +63,12 @@ __global__ void k_weights_f64(int which, int n, const double *t, double *o1, dou
 }
 
 // qlg_bot_profile (qlg_mod.f90:682-689)
-__global__ void k_qlg_profile(int n, const float *tgx, const float *th2x, const float *a, const float *q,
+__global__ void k_qlg_profile(int n, const float2 *tab, const float *a, const float *q,
                               const float *vpr, const float *idf, float *h) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const float v = fabsf(q[i] - vpr[i]) * idf[i];
     const QlgCoef c = qlg_setup(a[i], 1.0f, 0.8325546112f, 1.7724538509f);
-    const float K1 = qlg_eval(tgx, th2x, c, v);
+    const float K1 = qlg_eval(tab, c, v);
     h[i] = ((K1 * 0.5641895835f) * idf[i]) * (q[i] + 1.0f);
   }
 }
@@ -95,8 +99,11 @@ struct CellArgs {
 __device__ __forceinline__ float line_damping_a(const LineArgs &L, int l, float unsold_c, float lvb2,
                                                 float tothi, float ne, float starkpe) {
   float a = L.grad[l];
-  if (L.unsold[l]) a = fmaf(L.gw1[l], unsold_c, a);
-  else a = fmaf(L.gw1[l] * exp4(L.gw2[l] * lvb2), tothi, a);
+  const float gw1 = L.gw1[l];
+  // a line without van der Waals broadening adds fmaf(0*w, tothi, a) = a exactly
+  // (grad >= 0, finite tothi), so the power is skipped for it
+  if (L.unsold[l]) a = fmaf(gw1, unsold_c, a);
+  else if (gw1 != 0.0f) a = fmaf(gw1 * exp4(L.gw2[l] * lvb2), tothi, a);
   const float gs = L.gstk[l];
   if (gs >= 0.0f) a = fmaf(gs, ne, a);
   else a = fmaf(-gs, starkpe, a);
@@ -113,8 +120,7 @@ __device__ __forceinline__ float line_damping_a(const LineArgs &L, int l, float 
 template <class DepFn>
 __device__ void warp_cell_lines(const LineArgs &L, const GridArgs &G, const CellArgs &c, float *chi, float *eta,
                                 const float *cont, const float *logref, DepFn dep, bool do_nlte, bool diag,
-                                uint8_t *used, float *strength, float *reach, const float *tgx,
-                                const float *th2x, int lane) {
+                                uint8_t *used, float *strength, float *reach, const float2 *tab, int lane) {
   const float ex_cutoff = -85.0f, voigt_peak = 0.5641895835f, sqrt_pi = 1.7724538509f;
   const int nf = G.nf;
   const QlgCell qw = qlg_cell(G.sdl / c.idf);
@@ -195,7 +201,7 @@ __device__ void warp_cell_lines(const LineArgs &L, const GridArgs &G, const Cell
       if (diag && lane == 0) used[ln] = 1;
       const float x0 = x1 - (float)(i1 - fa);
       for (int f = fa + lane; f <= fb; f += 32) {
-        const float K = qlg_eval(tgx, th2x, cf, x0 + (float)(f - fa));
+        const float K = qlg_eval(tab, cf, x0 + (float)(f - fa));
         chi[f - 1] = fmaf(K, bi, chi[f - 1]);
         eta[f - 1] = fmaf(K, bj, eta[f - 1]);
       }
@@ -204,11 +210,8 @@ __device__ void warp_cell_lines(const LineArgs &L, const GridArgs &G, const Cell
   }
 }
 
-__device__ __forceinline__ void stage_tables(float *s_tgx, float *s_th2x, const float *tgx, const float *th2x) {
-  for (int i = threadIdx.x; i < QLG_NTAB; i += blockDim.x) {
-    s_tgx[i] = tgx[i];
-    s_th2x[i] = th2x[i];
-  }
+__device__ __forceinline__ void stage_tables(float2 *s_tab, const float2 *tab) {
+  for (int i = threadIdx.x; i < QLG_NTAB; i += blockDim.x) s_tab[i] = tab[i];
   __syncthreads();
 }
 
@@ -219,10 +222,10 @@ __global__ void __launch_bounds__(256) k_line_opacity(LineArgs L, GridArgs G, in
                                                       const float *lnbase, const float *ne, const float *tothi,
                                                       const float *stark_pe, const float *dep_mem, int do_nlte,
                                                       int diag, uint8_t *used, float *strength, float *reach,
-                                                      const float *tgx, const float *th2x) {
+                                                      const float2 *tab) {
   extern __shared__ float smem[];
-  float *s_tgx = smem, *s_th2x = smem + QLG_NTAB;
-  stage_tables(s_tgx, s_th2x, tgx, th2x);
+  float2 *s_tab = reinterpret_cast<float2 *>(smem);
+  stage_tables(s_tab, tab);
   const int lane = threadIdx.x & 31;
   const int warps = blockDim.x >> 5;
   for (int cell = blockIdx.x * warps + (threadIdx.x >> 5); cell < ncell; cell += gridDim.x * warps) {
@@ -232,7 +235,7 @@ __global__ void __launch_bounds__(256) k_line_opacity(LineArgs L, GridArgs G, in
     const size_t o = (size_t)G.nf * cell;
     auto dep = [&](int lev) { return dep_mem[(size_t)cell + (size_t)ncell * (size_t)(lev - 1)]; };
     warp_cell_lines(L, G, c, chi + o, eta + o, cont + o, logref + o, dep, do_nlte != 0, diag != 0, used, strength,
-                    reach, s_tgx, s_th2x, lane);
+                    reach, s_tab, lane);
   }
 }
 
@@ -434,7 +437,7 @@ __device__ __forceinline__ void quad_step(T xxup, T xxc, T xxdn, T ssup, T ssc, 
   dtup = tmax(tcopysign(tmax(tabs(dtup), dtmin), dtup), dtmax);
   dtdn = tmax(tcopysign(tmax(tabs(dtdn), dtmin), dtdn), dtmax);
   const T dt = at_target ? dtup : dtdn;
-  const T rdt = (T)1 / dt;
+  const T rdt = recip(dt);
   T ex, U0, U1, q;
   parab_moments(dt, ex, U0, U1, q);
   if (at_target) {

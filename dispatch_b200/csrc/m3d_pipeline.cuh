@@ -83,10 +83,10 @@ __device__ __forceinline__ float point_xhat(float chi_c, float h_kT, double nu) 
 template <typename TO>
 __global__ void __launch_bounds__(256) k_lte_opacity_units(AtmosDev A, GridArgs G, const double *nu, double v0,
                                                            double v1, double v2, TO *chi_out, TO *S_out,
-                                                           const float *tgx, const float *th2x) {
+                                                           const float2 *tab) {
   extern __shared__ float smem[];
-  float *s_tgx = smem, *s_th2x = smem + QLG_NTAB;
-  stage_tables(s_tgx, s_th2x, tgx, th2x);
+  float2 *s_tab = reinterpret_cast<float2 *>(smem);
+  stage_tables(s_tab, tab);
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int warps = blockDim.x >> 5;
   const int nf = G.nf;
@@ -111,8 +111,8 @@ __global__ void __launch_bounds__(256) k_lte_opacity_units(AtmosDev A, GridArgs 
       const SpeciesDev &S = A.species[sp];
       c.idf = S.inv_df[cell]; c.vbar2 = S.vbar2[cell]; c.base = S.lnbase[cell];
       auto dep = [](int) { return 1.0f; };
-      warp_cell_lines(S.L, G, c, s_chi, s_eta, s_x, s_lr, dep, false, false, nullptr, nullptr, nullptr, s_tgx,
-                      s_th2x, lane);
+      warp_cell_lines(S.L, G, c, s_chi, s_eta, s_x, s_lr, dep, false, false, nullptr, nullptr, nullptr, s_tab,
+                      lane);
     }
     __syncwarp();
     for (int f = lane; f < nf; f += 32) {
@@ -131,12 +131,15 @@ __global__ void __launch_bounds__(256) k_lte_opacity_units(AtmosDev A, GridArgs 
 
 // ---------------------------------------------------------------------------
 // The same pass with one LANE per cell, for windows of NF frequencies: each lane
-// runs its own cell's line loop in line order and keeps chi_l, eta_l of the window
-// in registers, so no lane idles on the per-line scalar work and every line's window
-// is evaluated with one point per unrolled step.  The tolerance reference at a
-// line's nearest node f0 is formed on the spot (xhat and its log), and the
-// accumulated line opacity there is picked out of the register array.  The
-// results are bit-identical to k_lte_opacity_units.
+// runs its own cell's line loop in line order and keeps chi_l of the window in
+// registers, so no lane idles on the per-line scalar work and every line's window
+// is evaluated with one point per unrolled step.  In this LTE pass every line
+// deposits the same profile into chi_l and eta_l (b_i = b_j = 1, both start at
+// zero), so eta_l is chi_l and is not carried separately.  The tolerance
+// reference at a line's nearest node f0 -- xhat and its log -- is kept for the two
+// window edges, where every line centred outside the window lands, and formed on
+// the spot otherwise; the accumulated line opacity there is picked out of the
+// register array.  Results are bit-identical to k_lte_opacity_units.
 // ---------------------------------------------------------------------------
 template <int NF>
 __device__ __forceinline__ float pick(const float (&a)[NF], int i) {
@@ -147,31 +150,32 @@ __device__ __forceinline__ float pick(const float (&a)[NF], int i) {
 }
 
 template <int NF, typename TO>
-__global__ void __launch_bounds__(256, 2) k_lte_opacity_units_lane(AtmosDev A, GridArgs G, const double *nu, double v0,
+__global__ void __launch_bounds__(256, 3) k_lte_opacity_units_lane(AtmosDev A, GridArgs G, const double *nu, double v0,
                                                                    double v1, double v2, TO *chi_out, TO *S_out,
-                                                                   const float *tgx, const float *th2x) {
+                                                                   const float2 *tab) {
   extern __shared__ float smem[];
-  float *s_tgx = smem, *s_th2x = smem + QLG_NTAB;
-  stage_tables(s_tgx, s_th2x, tgx, th2x);
-  // per-warp transpose buffer for coalesced stores: 32 cells x (NF + 1) values of TO
-  TO *s_out = reinterpret_cast<TO *>(smem + 2 * QLG_NTAB) + (size_t)(threadIdx.x >> 5) * 32 * (NF + 1);
+  float2 *s_tab = reinterpret_cast<float2 *>(smem);
+  stage_tables(s_tab, tab);
   const int lane = threadIdx.x & 31;
   const float ex_cutoff = -85.0f, voigt_peak = 0.5641895835f, sqrt_pi = 1.7724538509f;
   const float lt = logf_m3d(G.tol / voigt_peak);
   const int ncell = A.ncell;
-  const int nwarp_total = (gridDim.x * blockDim.x) >> 5;
-  const int ncell32 = (ncell + 31) / 32;
-  for (int cb = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; cb < ncell32; cb += nwarp_total) {
-    const int cell = cb * 32 + lane;
+  const int nthreads = gridDim.x * blockDim.x;
+  const int ncell_pad = (ncell + 31) / 32 * 32;
+  for (int cell = blockIdx.x * blockDim.x + threadIdx.x; cell < ncell_pad; cell += nthreads) {
     const bool live = cell < ncell;
     const int cs = live ? cell : ncell - 1;
     const float T = A.temp[cs], chi_c = A.chi_c[cs];
     const float h_kT = (float)(M3D_H_K / (double)T);
-    float chl[NF], etl[NF];
+    float chl[NF];
 #pragma unroll
-    for (int f = 0; f < NF; f++) { chl[f] = 0.0f; etl[f] = 0.0f; }
+    for (int f = 0; f < NF; f++) chl[f] = 0.0f;
     const float vproj = (float)((v0 * (double)A.vx[cs] + v1 * (double)A.vy[cs]) + v2 * (double)A.vz[cs]);
     const float ekt = A.e_kT[cs], ne = A.ne[cs], tothi = A.tothi[cs], starkpe = A.stark_pe[cs];
+    // xhat and logref at the window edges
+    const float x_lo = point_xhat(chi_c, h_kT, nu[0]), x_hi = point_xhat(chi_c, h_kT, nu[NF - 1]);
+    const float lr_lo = x_lo > 0.0f ? lt + logf_m3d(x_lo) : -FLT_MAX;
+    const float lr_hi = x_hi > 0.0f ? lt + logf_m3d(x_hi) : -FLT_MAX;
     for (int sp = 0; sp < A.nspecies; sp++) {
       const SpeciesDev &Sd = A.species[sp];
       const LineArgs &L = Sd.L;
@@ -188,12 +192,18 @@ __global__ void __launch_bounds__(256, 2) k_lte_opacity_units_lane(AtmosDev A, G
         const float ex = L.lower_ev[l] * ekt;
         const float arg = (base + L.gpref[l]) - ex;
         if (arg < ex_cutoff) continue;
-        const float cont0 = point_xhat(chi_c, h_kT, nu[f0 - 1]);
+        float cont0, lr0;
+        if (f0 == 1) { cont0 = x_lo; lr0 = lr_lo; }
+        else if (f0 == NF) { cont0 = x_hi; lr0 = lr_hi; }
+        else {
+          cont0 = point_xhat(chi_c, h_kT, nu[f0 - 1]);
+          lr0 = cont0 > 0.0f ? lt + logf_m3d(cont0) : -FLT_MAX;
+        }
         float refl = G.tol * cont0;
         const float flo = G.flo_scale * pick<NF>(chl, f0 - 1);
         float lref;
         if (flo > refl) { refl = flo; lref = logf_m3d(flo * sqrt_pi); }
-        else lref = cont0 > 0.0f ? lt + logf_m3d(cont0) : -FLT_MAX;
+        else lref = lr0;
         if (arg <= lref) continue;
         const float Rij = exp4(arg);
         if (voigt_peak * Rij <= refl) continue;
@@ -207,62 +217,108 @@ __global__ void __launch_bounds__(256, 2) k_lte_opacity_units_lane(AtmosDev A, G
         const int fb = ic + noff < NF ? ic + noff : NF;
         if (fa > fb) continue;
         const float x0 = x1 - (float)(f0 - fa);
+        const float kfa = (float)(1 - fa);    // (float)(f + 1 - fa) = (float)f + kfa, exactly
+        // Far wing: when even the window point nearest the line centre snaps to the
+        // last table node, G and W are the same two constants at every point, and the
+        // evaluation is qlg_eval's with them folded in.  The snapped index is monotone
+        // in |x| (rounded products are monotone), so the nearer window end decides.
+        const float xe = x0 + (float)(fb - fa);
+        const float xnear = (x0 > 0.0f) ? x0 : ((xe < 0.0f) ? -xe : 0.0f);
+        if (fminf((xnear * cf.ih) * 800.0f, 9019.0f) >= 9018.5f) {
+          const float2 gw = s_tab[QLG_NTAB - 1];
+          const float p1 = fmaf(cf.cZH, gw.y, cf.cL2);
+          const float gg = gw.x * cf.gG;
 #pragma unroll
-        for (int f = 0; f < NF; f++) {
-          if (f + 1 >= fa && f + 1 <= fb) {
-            const float K = qlg_eval(s_tgx, s_th2x, cf, x0 + (float)(f + 1 - fa));
-            chl[f] = fmaf(K, 1.0f, chl[f]);
-            etl[f] = fmaf(K, 1.0f, etl[f]);
+          for (int f = 0; f < NF; f++) {
+            if (f + 1 >= fa && f + 1 <= fb) {
+              const float xs = fabsf(x0 + ((float)f + kfa)) * cf.ih;
+              const float L = __frcp_rn(1.0f + xs * xs);
+              const float K = fmaf(L, fmaf(L, p1, cf.bL), gg);
+              chl[f] = fmaf(K, 1.0f, chl[f]);
+            }
+          }
+        } else {
+#pragma unroll
+          for (int f = 0; f < NF; f++) {
+            if (f + 1 >= fa && f + 1 <= fb) {
+              const float K = qlg_eval(s_tab, cf, x0 + ((float)f + kfa));
+              chl[f] = fmaf(K, 1.0f, chl[f]);
+            }
           }
         }
       }
     }
-    // epilogue: transfer units, staged through shared memory for coalesced stores
-    for (int half = 0; half < 2; half++) {
+    // epilogue: transfer units, written as 16-byte stores of this cell's row
+    if (live) {
+      TO *co = chi_out + (size_t)NF * cell, *so = S_out + (size_t)NF * cell;
 #pragma unroll
-      for (int f = 0; f < NF; f++) {
-        TO co, so;
-        if constexpr (sizeof(TO) == 4) {
-          point_units(chi_c, h_kT, nu[f], chl[f], etl[f], A.maser_chi_floor, co, so);
-        } else {
-          point_units((double)chi_c, (double)T, nu[f], (double)chl[f], (double)etl[f], (double)A.maser_chi_floor, co, so);
+      for (int f = 0; f < NF; f += 4) {
+        TO c4[4], s4[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+          if constexpr (sizeof(TO) == 4) {
+            point_units(chi_c, h_kT, nu[f + k], chl[f + k], chl[f + k], A.maser_chi_floor, c4[k], s4[k]);
+          } else {
+            point_units((double)chi_c, (double)T, nu[f + k], (double)chl[f + k], (double)chl[f + k],
+                        (double)A.maser_chi_floor, c4[k], s4[k]);
+          }
         }
-        s_out[lane * (NF + 1) + f] = half == 0 ? co : so;
+        if constexpr (sizeof(TO) == 4) {
+          *reinterpret_cast<float4 *>(co + f) = make_float4(c4[0], c4[1], c4[2], c4[3]);
+          *reinterpret_cast<float4 *>(so + f) = make_float4(s4[0], s4[1], s4[2], s4[3]);
+        } else {
+          reinterpret_cast<double2 *>(co + f)[0] = make_double2(c4[0], c4[1]);
+          reinterpret_cast<double2 *>(co + f)[1] = make_double2(c4[2], c4[3]);
+          reinterpret_cast<double2 *>(so + f)[0] = make_double2(s4[0], s4[1]);
+          reinterpret_cast<double2 *>(so + f)[1] = make_double2(s4[2], s4[3]);
+        }
       }
-      __syncwarp();
-      TO *dst = half == 0 ? chi_out : S_out;
-      for (int c = 0; c < 32; c++) {
-        const int cc = cb * 32 + c;
-        if (cc < ncell)
-          for (int f = lane; f < NF; f += 32) dst[(size_t)NF * cc + f] = s_out[c * (NF + 1) + f];
-      }
-      __syncwarp();
     }
-    (void)live;
   }
 }
 
-__device__ __forceinline__ void rot_load(const float *chi, const float *S, size_t plane, int zg, const RotPlane &r, int f,
-                                         int x, int y, int nf, int nx, int ny, float &xv, float &sv) {
-  const int x1 = wrap(x + r.up1, nx), x2 = x1 + 1 == nx ? 0 : x1 + 1;
-  const int y1 = wrap(y + r.up2, ny), y2 = y1 + 1 == ny ? 0 : y1 + 1;
-  const size_t o = plane * (size_t)zg + (size_t)f;
-  const size_t i11 = o + (size_t)nf * ((size_t)x1 + (size_t)nx * y1), i21 = o + (size_t)nf * ((size_t)x2 + (size_t)nx * y1);
-  const size_t i12 = o + (size_t)nf * ((size_t)x1 + (size_t)nx * y2), i22 = o + (size_t)nf * ((size_t)x2 + (size_t)nx * y2);
-  float v = r.a * __ldg(chi + i11);
-  v = fmaf(r.b, __ldg(chi + i21), v);
-  v = fmaf(r.c, __ldg(chi + i12), v);
-  xv = fmaf(r.d, __ldg(chi + i22), v);
-  float w = r.a * __ldg(S + i11);
-  w = fmaf(r.b, __ldg(S + i21), w);
-  w = fmaf(r.c, __ldg(S + i12), w);
-  sv = fmaf(r.d, __ldg(S + i22), w);
+// rotate_array's weights of one plane for the fused sweep, with the periodic
+// offsets already reduced to [0, n): ux = modulo(up1, nx), uy = modulo(up2, ny)
+struct RotCol { int ux, uy; float a, b, c, d; };
+
+// The four raw taps of one plane (chi and Snu), loaded ahead of their use
+struct Taps { float c11, c21, c12, c22, s11, s21, s12, s22; };
+
+__device__ __forceinline__ Taps load_taps(const float *chi, const float *S, size_t plane_off, const RotCol &r, int f,
+                                          int x, int y, int nf, int nx, int ny) {
+  int x1 = x + r.ux;
+  x1 = x1 >= nx ? x1 - nx : x1;
+  const int x2 = x1 + 1 == nx ? 0 : x1 + 1;
+  int y1 = y + r.uy;
+  y1 = y1 >= ny ? y1 - ny : y1;
+  const int y2 = y1 + 1 == ny ? 0 : y1 + 1;
+  const unsigned rx1 = (unsigned)nf * x1, rx2 = (unsigned)nf * x2;
+  const unsigned ry1 = (unsigned)nf * nx * y1, ry2 = (unsigned)nf * nx * y2;
+  const float *pc = chi + plane_off + f, *ps = S + plane_off + f;
+  Taps t;
+  t.c11 = __ldg(pc + rx1 + ry1); t.c21 = __ldg(pc + rx2 + ry1);
+  t.c12 = __ldg(pc + rx1 + ry2); t.c22 = __ldg(pc + rx2 + ry2);
+  t.s11 = __ldg(ps + rx1 + ry1); t.s21 = __ldg(ps + rx2 + ry1);
+  t.s12 = __ldg(ps + rx1 + ry2); t.s22 = __ldg(ps + rx2 + ry2);
+  return t;
+}
+
+// shifted = a p11; then b p21, c p12, d p22 added in that order (rt_patch_mod.f90:3850-3853)
+__device__ __forceinline__ void combine(const Taps &t, const RotCol &r, float &xv, float &sv) {
+  float v = r.a * t.c11;
+  v = fmaf(r.b, t.c21, v);
+  v = fmaf(r.c, t.c12, v);
+  xv = fmaf(r.d, t.c22, v);
+  float w = r.a * t.s11;
+  w = fmaf(r.b, t.s21, w);
+  w = fmaf(r.c, t.s12, w);
+  sv = fmaf(r.d, t.s22, w);
 }
 
 // chi, S: (nf, nx, ny, nz) unrotated transfer units of the whole column; rot: per
 // global plane; slab_z0: first global plane of each slab (nslab + 1 entries).
 __global__ void __launch_bounds__(256) k_quad_rot_column(int nf, int nx, int ny, int nz, const float *chi,
-                                                         const float *S, const RotPlane *rot, const int *slab_z0,
+                                                         const float *S, const RotCol *rot, const int *slab_z0,
                                                          int nslab, QuadConst qc, PchipConst pc, float dtmax,
                                                          float Imax, float *I_top) {
   const size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
@@ -283,15 +339,26 @@ __global__ void __launch_bounds__(256) k_quad_rot_column(int nf, int nx, int ny,
   for (int s = 0; s < nslab; s++) {
     const int z0 = slab_z0[s], n = slab_z0[s + 1] - z0;
     float xu = gx, su = gs, Iu = gI, xc, sc, xd, sd;
-    rot_load(chi, S, plane, z0, rot[z0], f, x, y, nf, nx, ny, xc, sc);
-    rot_load(chi, S, plane, z0 + 1, rot[z0 + 1], f, x, y, nf, nx, ny, xd, sd);
+    RotCol r0 = rot[z0], r1 = rot[z0 + 1];
+    Taps t0 = load_taps(chi, S, plane * z0, r0, f, x, y, nf, nx, ny);
+    Taps t1 = load_taps(chi, S, plane * (z0 + 1), r1, f, x, y, nf, nx, ny);
+    combine(t0, r0, xc, sc);
+    combine(t1, r1, xd, sd);
     for (int zl = 1; zl < n; zl++) {
+      // the plane after next, loaded while this step computes
+      const bool more = zl + 1 < n;
+      RotCol rn;
+      Taps tn;
+      if (more) {
+        rn = rot[z0 + zl + 1];
+        tn = load_taps(chi, S, plane * (z0 + zl + 1), rn, f, x, y, nf, nx, ny);
+      }
       float Inu, pl;
       quad_step<float>(xu, xc, xd, su, sc, sd, Iu, true, qc.rdsup, qc.dsup1, qc.dsup2, dtmax, Imax, false, Inu, pl);
       Iu = Inu;
-      if (zl + 1 < n) {
+      if (more) {
         xu = xc; su = sc; xc = xd; sc = sd;
-        rot_load(chi, S, plane, z0 + zl + 1, rot[z0 + zl + 1], f, x, y, nf, nx, ny, xd, sd);
+        combine(tn, rn, xd, sd);
       }
     }
     float In, pl;
@@ -301,25 +368,36 @@ __global__ void __launch_bounds__(256) k_quad_rot_column(int nf, int nx, int ny,
   I_top[g] = gI;
 }
 
-// save_intensity (rt_patch_mod.f90:4151-4208): ie(f) = <2h nu^5/(c^3 AA) I>_xy
+// save_intensity (rt_patch_mod.f90:4151-4208): ie(f) = <2h nu^5/(c^3 AA) I>_xy, in
+// two deterministic stages: blocks (32 frequencies x 8 rows) sum a fixed stride of
+// columns into partials, then one thread per frequency adds the partials in order.
 template <typename TI>
-__global__ void k_save_intensity(int nf, int ncol, const double *nu, const TI *I_top, float *ie) {
-  __shared__ double part[8][33];
+__global__ void k_save_partial(int nf, int ncol, const double *nu, const TI *I_top, double *part) {
+  __shared__ double acc[8][33];
   const int f = blockIdx.x * 32 + threadIdx.x;
-  double acc = 0.0;
+  const int nparts = gridDim.y;
+  double s = 0.0;
   if (f < nf) {
     const double conv = 2.0 * 6.626176e-27 / (2.99792458e10 * 2.99792458e10 * 2.99792458e10 * 1e8);
     const double n5 = nu[f] * nu[f] * nu[f] * nu[f] * nu[f];
-    for (int c = threadIdx.y; c < ncol; c += blockDim.y)
-      acc += (double)(float)(conv * n5 * (double)I_top[(size_t)f + (size_t)nf * c]);
+    for (int c = blockIdx.y * blockDim.y + threadIdx.y; c < ncol; c += nparts * blockDim.y)
+      s += (double)(float)(conv * n5 * (double)I_top[(size_t)f + (size_t)nf * c]);
   }
-  part[threadIdx.y][threadIdx.x] = acc;
+  acc[threadIdx.y][threadIdx.x] = s;
   __syncthreads();
   if (threadIdx.y == 0 && f < nf) {
-    double s = 0.0;
-    for (int k = 0; k < (int)blockDim.y; k++) s += part[k][threadIdx.x];
-    ie[f] = (float)s / (float)ncol;
+    double t = 0.0;
+    for (int k = 0; k < (int)blockDim.y; k++) t += acc[k][threadIdx.x];
+    part[(size_t)blockIdx.y * nf + f] = t;
   }
+}
+
+__global__ void k_save_final(int nf, int ncol, int nparts, const double *part, float *ie) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= nf) return;
+  double t = 0.0;
+  for (int p = 0; p < nparts; p++) t += part[(size_t)p * nf + f];
+  ie[f] = (float)t / (float)ncol;
 }
 
 // copy the transfer units of a slab's planes into its FP64 work array (plain path)

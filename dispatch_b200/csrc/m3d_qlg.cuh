@@ -4,6 +4,14 @@
 // (qlg_init :364) live in global memory and are staged into shared memory by the
 // kernels that sweep line windows.  The fitted constants are the published QLG-bot
 // coefficients; they have to be the same numbers for the profile to be QLG-bot.
+//
+// The tables are read interleaved, tab[i] = (TGX(i), TH2X(i)), one 8-byte load per
+// point.  Two exact rewrites keep the point cost down: 1/(1+u) is the correctly
+// rounded reciprocal (__frcp_rn equals the IEEE quotient 1.0f/(1+u)), and the
+// snapped index nint(min(xs*800, 9019)) is formed as (int)(y + 0.5f) for y >= 0.5
+// and 0 below -- for y in [0.5, 9019] the sum y + 0.5f rounds across no integer, so
+// the truncation equals round-half-away-from-zero, and y < 0.5 (including the one
+// float just below 0.5, whose sum rounds up to 1) snaps to node 0.
 #pragma once
 #include "m3d_math.cuh"
 
@@ -43,12 +51,14 @@ __device__ __forceinline__ QlgCoef qlg_setup(float gL, float D, float SQ, float 
   return c;
 }
 
-__device__ __forceinline__ float qlg_eval(const float *tgx, const float *th2x, const QlgCoef &c, float x) {
+__device__ __forceinline__ float qlg_eval(const float2 *tab, const QlgCoef &c, float x) {
   const float xs = fabsf(x) * c.ih;
   const float u = xs * xs;
-  const float L = 1.0f / (1.0f + u);
-  const int ig = max((int)lroundf(fminf(xs * 800.0f, 9019.0f)), 0);
-  const float G = tgx[ig], W = th2x[ig];
+  const float L = __frcp_rn(1.0f + u);
+  const float y = fminf(xs * 800.0f, 9019.0f);
+  const int ig = y < 0.5f ? 0 : (int)(y + 0.5f);
+  const float2 gw = tab[ig];
+  const float G = gw.x, W = gw.y;
   float p = fmaf(c.cZH, W, c.cL2);
   p = fmaf(L, p, c.bL);
   return fmaf(L, p, G * c.gG);
