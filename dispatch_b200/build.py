@@ -17,7 +17,8 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libm3dgpu.so")
 SOURCES = ["m3d_api.cu"]
-HEADERS = ["m3d_math.cuh", "m3d_qlg.cuh", "m3d_kernels.cuh", "m3d_pipeline.cuh"]
+HEADERS = ["m3d_math.cuh", "m3d_qlg.cuh", "m3d_kernels.cuh", "m3d_pipeline.cuh", "m3d_stateq.cuh",
+           "m3d_stateq_api.inc"]
 
 
 def nvcc() -> str:

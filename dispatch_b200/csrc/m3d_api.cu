@@ -3,6 +3,8 @@
 // Host pointers are staged through device buffers for the duration of a call;
 // with M3D_DEVICE_PTRS the caller's device pointers are used directly and the
 // call only enqueues work on the library stream.
+#include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -14,6 +16,7 @@
 
 #include "../../include/m3dgpu.h"
 #include "m3d_pipeline.cuh"
+#include "m3d_stateq.cuh"
 
 using namespace m3d;
 
@@ -1070,6 +1073,8 @@ int m3d_lte_synthesis(const m3d_atmos_t *atm, int nf, const double *nu, const do
 }
 
 }  // extern "C"
+
+#include "m3d_stateq_api.inc"
 
 // ===========================================================================
 // rotate_array without any allocation.

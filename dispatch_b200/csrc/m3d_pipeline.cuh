@@ -156,7 +156,6 @@ __global__ void __launch_bounds__(256, 3) k_lte_opacity_units_lane(AtmosDev A, G
   extern __shared__ float smem[];
   float2 *s_tab = reinterpret_cast<float2 *>(smem);
   stage_tables(s_tab, tab);
-  const int lane = threadIdx.x & 31;
   const float ex_cutoff = -85.0f, voigt_peak = 0.5641895835f, sqrt_pi = 1.7724538509f;
   const float lt = logf_m3d(G.tol / voigt_peak);
   const int ncell = A.ncell;

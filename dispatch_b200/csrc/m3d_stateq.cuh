@@ -1,0 +1,705 @@
+// Statistical equilibrium on the device, FP64: the rate matrix of every cell
+// (setup_transition_matrix, SRC/atom_mod.f90:740-841, with line_rate_coefficients
+// :862-884 and the electron branches of classic_col :1758-1850), its dense solve
+// (lineq_no_pivot / lineq, HOP/op_math_mod.f90:263-356, 420-449, or LU with
+// partial pivoting) and the population update (update_populations :439-732);
+// then Ng's accumulation and extrapolation in ln b (SRC/ng_mod.f90:241-390).
+//
+// One warp owns one cell at a time and keeps the cell's rate matrix (column
+// major, n <= 64) and its vectors in shared memory.  Every elimination step
+// updates each matrix element once, so spreading a step's elements over the
+// lanes performs exactly the roundings of the sequential loops; the
+// substitutions that a row-wise loop orders differently from a column-wise one
+// run column by column where the orders agree and on one lane where they do
+// not (the back substitution of lineq_no_pivot).  The library is compiled with
+// -fmad=false, so no product is fused into a sum.
+#pragma once
+#include <cfloat>
+#include <cstdint>
+
+namespace m3d {
+
+constexpr int SE_NMAX = 64;
+constexpr int SE_COL_REGEMORTER = 1, SE_COL_SEATON = 2;
+
+// Atom tables in device memory.  Transitions are listed by round: the
+// transitions of one round touch pairwise different matrix elements, and a
+// pair's transitions fall in successive rounds in their original order, so
+// the additions into each element keep the reference's transition order.
+struct SeAtomDev {
+  int n, nline, nround, ncol;
+  const int *order;      // transition index, grouped by round (active ones only)
+  const int *round_off;  // [nround + 1]
+  const int *ti, *tj;    // [nrad]
+  const double *Aji;     // [nrad]
+  const double *g, *ev;  // [n]
+  const int *ion;        // [n]
+  const int *ci, *cj, *ckind;  // [ncol]
+  const float *cfac;           // [ncol]
+  double fmin, cbbesc, cbfesc, colscale, upsilon_floor, cut_x, bf_cut_rate;
+};
+
+struct SeParams {
+  double max_update, sor_w, min_pop_frac, conv_pop_floor, tmax_update, cswitch;
+  int solver;
+};
+
+struct SeCells {
+  int ncell;
+  double *b;
+  const double *nstar, *totn, *temp, *ne, *e_kT, *dxi;
+  const float *gij, *gji;
+  const double *cup;  // precomputed collision rates, or null to form them here
+};
+
+// per-warp partial results of the convergence measures
+struct SeWarpBest {
+  double maxerr_abs, maxerr;  // weighted |e| and the signed value
+  long long cell;             // -1: none
+  int level, pad;
+};
+
+// ---- classic_col helpers (atom_mod.f90:2362-2467) ------------------------------
+// The Fortran tables are default-real literals: their single-precision values
+// enter the double arithmetic.
+__device__ __forceinline__ double se_expin(double x) {
+  const float a0 = -44178.5471728217f, a1 = 57721.7247139444f, a2 = 9938.31388962037f, a3 = 1842.11088668000f,
+              a4 = 101.093806161906f, a5 = 5.03416184097568f;
+  const float b0 = 76537.3323337614f, b1 = 32597.1881290275f, b2 = 6106.10794245759f, b3 = 635.419418378382f,
+              b4 = 37.2298352833327f;
+  const float c0 = 4.65627107975096e-7f, c1 = .999979577051595f, c2 = 9.04161556946329f, c3 = 24.3784088791317f,
+              c4 = 23.0192559391333f, c5 = 6.90522522784444f, c6 = .430967839469389f;
+  const float d0 = 10.0411643829054f, d1 = 32.4264210695138f, d2 = 41.2807841891424f, d3 = 20.4494785013794f,
+              d4 = 3.31909213593302f, d5 = .103400130404874f;
+  const float e0 = -.999999999998447f, e1 = -26.6271060431811f, e2 = -241.055827097015f, e3 = -895.927957772937f,
+              e4 = -1298.85688746484f, e5 = -545.374158883133f, e6 = -5.66575206533869f;
+  const float f0 = 28.6271060422192f, f1 = 292.310039388533f, f2 = 1332.78537748257f, f3 = 2777.61949509163f,
+              f4 = 2404.01713225909f, f5 = 631.657483280800f;
+  const double ex = exp(-x);
+  if (x > 4) {
+    return (ex + ex * ((double)e0 + ((double)e1 + ((double)e2 + ((double)e3 + ((double)e4 + ((double)e5 + (double)e6 / x) / x) / x) / x) / x) / x) /
+                     (x + (double)f0 + ((double)f1 + ((double)f2 + ((double)f3 + ((double)f4 + (double)f5 / x) / x) / x) / x) / x)) /
+           x;
+  } else if (x > 1) {
+    return ex * ((double)c6 + ((double)c5 + ((double)c4 + ((double)c3 + ((double)c2 + ((double)c1 + (double)c0 * x) * x) * x) * x) * x) * x) /
+           ((double)d5 + ((double)d4 + ((double)d3 + ((double)d2 + ((double)d1 + ((double)d0 + x) * x) * x) * x) * x) * x);
+  } else if (x > 0) {
+    return ((double)a0 + ((double)a1 + ((double)a2 + ((double)a3 + ((double)a4 + (double)a5 * x) * x) * x) * x) * x) /
+               ((double)b0 + ((double)b1 + ((double)b2 + ((double)b3 + ((double)b4 + x) * x) * x) * x) * x) -
+           log(x);
+  }
+  return 0.0;
+}
+
+__constant__ float se_gaunt_a1[6] = {1.078e00f, 1.0926e0f, 1.0983e0f, 1.0954e0f, 1.0912e0f, 1.0925e0f};
+__constant__ float se_gaunt_b1[6] = {-8.754e14f, -2.019e14f, -9.45e13f, -5.188e13f, -3.2e13f, -2.331e13f};
+__constant__ float se_gaunt_c1[6] = {-1.791e29f, 1.836e28f, 9.177e27f, 3.552e27f, 1.576e27f, 9.325e26f};
+__constant__ float se_gaunt_a2[6] = {0.798e00f, 0.768e00f, 0.793e00f, 0.831e00f, 0.758e00f, 0.79e00f};
+__constant__ float se_gaunt_b2[6] = {5.358e15f, 6.242e15f, 5.48e15f, 4.094e15f, 6.633e15f, 5.808e15f};
+__constant__ float se_gaunt_c2[6] = {-3.484e31f, -3.208e31f, -2.318e31f, -1.43e31f, -3.32e31f, -2.844e31f};
+
+__device__ __forceinline__ double se_gaunt(double lam, int n) {
+  const float *a1 = se_gaunt_a1, *b1 = se_gaunt_b1, *c1 = se_gaunt_c1;
+  const float *a2 = se_gaunt_a2, *b2 = se_gaunt_b2, *c2 = se_gaunt_c2;
+  const double inv_nu = lam * (1e-8 / 2.99792458e10);
+  if (n > 6) return 1.0;
+  if (inv_nu >= (double)1e-16f) return (double)a1[n - 1] + ((double)b1[n - 1] + (double)c1[n - 1] * inv_nu) * inv_nu;
+  return (double)a2[n - 1] + ((double)b2[n - 1] + (double)c2[n - 1] * inv_nu) * inv_nu;
+}
+
+// Kramers' cross section; kramer_const = 64 PI^4 EC^10 EM / (3 sqrt(3) CC HH^6)
+// with each power and product rounded to double once
+__device__ __forceinline__ double se_kramer(double lam, double dev) {
+  const double nu = (2.99792458e10 / 1e-8) / lam;
+  if (dev > 0) {
+    const double nl = sqrt(13.605 / dev);
+    const double nl2 = nl * nl, nl5 = nl * (nl2 * nl2), nu3 = nu * (nu * nu);
+    return 0x1.c6dc1aa1038f0p+97 * se_gaunt(lam, (int)ceil(nl)) / (nl5 * nu3);
+  }
+  return 0.0;
+}
+
+struct SeColCell { double allen, regemorter, seaton, ekt, dxi; };
+
+__device__ __forceinline__ SeColCell se_col_cell(double temp, double ne, double ekt, double dxi) {
+  const double PI = 3.14159265359, BK = 1.380662e-16, EM = 9.109534e-28, RB = 5.29177349e-9;
+  const double E_K = 1.602189e-12 / BK, RYDK = 13.605 * E_K;
+  const double sq8bmp = sqrt(8 * BK / EM / PI);
+  const double c0 = PI * (RB * RB) * sq8bmp;
+  const double sqt = sqrt(temp);
+  SeColCell w;
+  w.allen = c0 * RYDK * ne / sqt;
+  w.regemorter = 14.5 * w.allen * RYDK / E_K;
+  w.seaton = (double)1.55e13f * ne / sqt;
+  w.ekt = ekt;
+  w.dxi = dxi;
+  return w;
+}
+
+// upward electron-collision rate of pair p [1/s], colscale applied
+__device__ __forceinline__ double se_col_rate(const SeAtomDev &A, const SeColCell &w, int p) {
+  const double sqr3_2pi = (sqrt(3.0) / 2.0) / 3.14159265359;
+  const int i = A.ci[p], j = A.cj[p], kind = A.ckind[p];
+  const int ioni = A.ion[i], ionj = A.ion[j];
+  const bool cont = ionj > ioni;
+  double fac = (double)A.cfac[p], f = 0;
+  double dev = A.ev[j] - A.ev[i];
+  dev = fmax(dev, 1e-8);
+  if (cont) {
+    const int jj = ionj * (ionj - 1), ii = ioni * (ioni - 1);
+    dev = dev - w.dxi * 0.5 * (double)(jj - ii);
+  } else {
+    f = fmax(fac, A.fmin * A.g[j]);
+  }
+  const double u0 = dev * w.ekt;
+  const double ex = exp(-u0);
+  double v = 0;
+  if (cont && kind == SE_COL_SEATON) {
+    if (fac == 0) {
+      const double lam0 = (2.99792458e10 / 1e-8) * (6.626176e-27 / 1.602189e-12) / dev;
+      fac = se_kramer(lam0, dev);
+    }
+    const double tmp = (double)fminf(0.1f * (float)ioni, 0.3f);
+    v = w.seaton * fac * tmp / u0 * ex;
+    v = v * A.cbfesc;
+  } else if (!cont && kind == SE_COL_REGEMORTER) {
+    const double tmp = fmax((double)0.2f * ex, sqr3_2pi * se_expin(u0));
+    v = w.regemorter * f * tmp / dev;
+    v = fmax(v, w.allen * A.upsilon_floor * ex / A.g[i]);
+    v = v * A.cbbesc;
+  }
+  if (v != 0) v = v * A.colscale;
+  return v;
+}
+
+// cup[cell + ncell*p], one thread per cell
+__global__ void k_collision_rates(SeAtomDev A, int ncell, const double *__restrict__ temp,
+                                  const double *__restrict__ ne, const double *__restrict__ ekt,
+                                  const double *__restrict__ dxi, double *__restrict__ cup) {
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += gridDim.x * blockDim.x) {
+    const SeColCell w = se_col_cell(temp[c], ne[c], ekt[c], dxi ? dxi[c] : 0.0);
+    for (int p = 0; p < A.ncol; p++) cup[(size_t)c + (size_t)ncell * p] = se_col_rate(A, w, p);
+  }
+}
+
+// ---- the per-warp dense solvers ------------------------------------------------
+// a(i,j) = W[i + n*j]; e is the right-hand side, the solution on return.
+
+// lineq_no_pivot (op_math_mod.f90:420-449)
+__device__ __forceinline__ void se_solve_no_pivot(double *W, double *e, int n, int lane) {
+  for (int k = 0; k < n - 1; k++) {
+    const double pk = W[k + n * k];
+    for (int i = k + 1 + lane; i < n; i += 32) W[i + n * k] = W[i + n * k] / pk;
+    __syncwarp();
+    const int m = n - k - 1;
+    int ii = lane % m, jj = lane / m;
+    for (int idx = lane; idx < m * m; idx += 32) {
+      const int i = k + 1 + ii, j = k + 1 + jj;
+      const double akj = W[k + n * j];
+      if (akj != 0) W[i + n * j] = W[i + n * j] - W[i + n * k] * akj;
+      ii += 32;
+      while (ii >= m) { ii -= m; jj++; }
+    }
+    __syncwarp();
+  }
+  // forward substitution: per row the terms arrive in ascending j, as in the row loop
+  for (int j = 0; j < n - 1; j++) {
+    const double ej = e[j];
+    for (int i = j + 1 + lane; i < n; i += 32) e[i] = e[i] - W[i + n * j] * ej;
+    __syncwarp();
+  }
+  // back substitution: the row loop adds its terms in ascending j, an order no
+  // column sweep reproduces, so one lane runs it
+  if (lane == 0) {
+    for (int i = n - 1; i >= 0; i--) {
+      double t = e[i];
+      for (int j = i + 1; j < n; j++) t = t - W[i + n * j] * e[j];
+      e[i] = t / W[i + n * i];
+    }
+  }
+  __syncwarp();
+}
+
+// warp arg-max: largest v, ties to the smallest idx; idx < 0 never wins
+__device__ __forceinline__ void warp_argmax(double &v, int &idx) {
+  for (int o = 16; o > 0; o >>= 1) {
+    const double ov = __shfl_xor_sync(0xffffffffu, v, o);
+    const int oi = __shfl_xor_sync(0xffffffffu, idx, o);
+    const bool take = oi >= 0 && (idx < 0 || ov > v || (ov == v && oi < idx));
+    if (take) { v = ov; idx = oi; }
+  }
+}
+
+// lineq: Gaussian elimination with full pivoting (op_math_mod.f90:263-356)
+__device__ __forceinline__ void se_solve_lineq(double *W, double *e, double *q, int *icol, int n, int lane) {
+  for (int i = lane; i < n; i += 32) icol[i] = i;
+  __syncwarp();
+  for (int s = 0; s < n - 1; s++) {
+    // pivot: the first element in row-major order of the largest |a|; the
+    // sequential scan starts from |a(s,s)| and moves only on a strict increase
+    const int m = n - s;
+    double bv = -1.0;
+    int bi = -1;
+    for (int idx = lane; idx < m * m; idx += 32) {
+      const int i = s + idx / m, j = s + idx % m;
+      const double a = fabs(W[i + n * j]);
+      const double v = a == a ? a : INFINITY;  // a NaN pivot, taken alike by every lane
+      if (bi < 0 || v > bv) { bv = v; bi = idx; }
+    }
+    warp_argmax(bv, bi);
+    const int ima = s + bi / m, jma = s + bi % m;
+    for (int i = lane; i < n; i += 32) {
+      const double t = W[i + n * jma];
+      W[i + n * jma] = W[i + n * s];
+      W[i + n * s] = t;
+    }
+    __syncwarp();
+    for (int j = s + lane; j < n; j += 32) {
+      const double t = W[ima + n * j];
+      W[ima + n * j] = W[s + n * j];
+      W[s + n * j] = t;
+    }
+    if (lane == 0) {
+      const double t = e[ima];
+      e[ima] = e[s];
+      e[s] = t;
+      const int it = icol[s];
+      icol[s] = icol[jma];
+      icol[jma] = it;
+    }
+    __syncwarp();
+    const double piv = W[s + n * s];
+    for (int i = s + 1 + lane; i < n; i += 32) q[i] = W[i + n * s] / piv;
+    __syncwarp();
+    const int mm = n - s - 1;
+    int ii = mm > 0 ? lane % mm : 0, jj = mm > 0 ? lane / mm : 0;
+    for (int idx = lane; idx < mm * mm; idx += 32) {
+      const int i = s + 1 + ii, j = s + 1 + jj;
+      W[i + n * j] = W[i + n * j] - q[i] * W[s + n * j];
+      ii += 32;
+      while (ii >= mm) { ii -= mm; jj++; }
+    }
+    const double es = e[s];
+    for (int i = s + 1 + lane; i < n; i += 32) e[i] = e[i] - q[i] * es;
+    __syncwarp();
+  }
+  // back substitution: the row loop runs j downwards, as a column sweep does
+  if (lane == 0) e[n - 1] = e[n - 1] / W[(n - 1) + n * (n - 1)];
+  __syncwarp();
+  for (int j = n - 1; j >= 1; j--) {
+    const double ej = e[j];
+    for (int i = lane; i < j; i += 32) e[i] = e[i] - W[i + n * j] * ej;
+    __syncwarp();
+    if (lane == 0) e[j - 1] = e[j - 1] / W[(j - 1) + n * (j - 1)];
+    __syncwarp();
+  }
+  // reorder: c(icol(i)) = b(i)
+  for (int i = lane; i < n; i += 32) q[icol[i]] = e[i];
+  __syncwarp();
+  for (int i = lane; i < n; i += 32) e[i] = q[i];
+  __syncwarp();
+}
+
+// LU with partial (row) pivoting: pivot of column k the first row of largest
+// |a(i,k)|, i >= k; forward substitution by columns ascending, back
+// substitution by columns descending
+__device__ __forceinline__ void se_solve_partial(double *W, double *e, int n, int lane) {
+  for (int k = 0; k < n - 1; k++) {
+    double bv = -1.0;
+    int bi = -1;
+    for (int i = k + lane; i < n; i += 32) {
+      const double a = fabs(W[i + n * k]);
+      const double v = a == a ? a : INFINITY;
+      if (bi < 0 || v > bv) { bv = v; bi = i; }
+    }
+    warp_argmax(bv, bi);
+    const int p = bi;
+    if (p != k) {
+      for (int j = lane; j < n; j += 32) {
+        const double t = W[k + n * j];
+        W[k + n * j] = W[p + n * j];
+        W[p + n * j] = t;
+      }
+      if (lane == 0) {
+        const double t = e[k];
+        e[k] = e[p];
+        e[p] = t;
+      }
+    }
+    __syncwarp();
+    const double pk = W[k + n * k];
+    for (int i = k + 1 + lane; i < n; i += 32) W[i + n * k] = W[i + n * k] / pk;
+    __syncwarp();
+    const int m = n - k - 1;
+    int ii = lane % m, jj = lane / m;
+    for (int idx = lane; idx < m * m; idx += 32) {
+      const int i = k + 1 + ii, j = k + 1 + jj;
+      W[i + n * j] = W[i + n * j] - W[i + n * k] * W[k + n * j];
+      ii += 32;
+      while (ii >= m) { ii -= m; jj++; }
+    }
+    __syncwarp();
+  }
+  for (int j = 0; j < n - 1; j++) {
+    const double ej = e[j];
+    for (int i = j + 1 + lane; i < n; i += 32) e[i] = e[i] - W[i + n * j] * ej;
+    __syncwarp();
+  }
+  for (int j = n - 1; j >= 0; j--) {
+    if (lane == 0) e[j] = e[j] / W[j + n * j];
+    __syncwarp();
+    const double ej = e[j];
+    for (int i = lane; i < j; i += 32) e[i] = e[i] - W[i + n * j] * ej;
+    __syncwarp();
+  }
+}
+
+// shared memory of one warp, in doubles (plus n ints for lineq's column order)
+__host__ __device__ inline size_t se_warp_doubles(int n) { return (size_t)n * n + 4 * (size_t)n + (size_t)(n + 1) / 2; }
+
+// update_populations over all cells: warps stride over the cells in ascending order
+__global__ void k_stateq_update(SeAtomDev A, SeParams P, SeCells C, SeWarpBest *__restrict__ wbest,
+                                double *__restrict__ lvl_val, long long *__restrict__ lvl_cell,
+                                unsigned long long *__restrict__ counts, long long *__restrict__ nonfinite) {
+  extern __shared__ double se_smem[];
+  const int n = A.n, lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  double *W = se_smem + se_warp_doubles(n) * wib;
+  double *bl = W + n * n, *ns = bl + n, *e = ns + n, *q = e + n;
+  int *icol = (int *)(q + n);
+  const int nwarp = gridDim.x * (blockDim.x >> 5);
+  const int gw = blockIdx.x * (blockDim.x >> 5) + wib;
+  const int ncell = C.ncell;
+  const double eup = fmax(P.max_update, 1.0), elo = 1.0 / eup;
+
+  SeWarpBest best;
+  best.maxerr_abs = 0;
+  best.maxerr = 0;
+  best.cell = -1;
+  best.level = -1;
+  best.pad = 0;
+  double lv[2] = {0, 0};
+  long long lc[2] = {-1, -1};
+  unsigned long long nclamp = 0, ntot = 0;
+
+  for (int c = gw; c < ncell; c += nwarp) {
+    const double totn = C.totn[c];
+    if (!(totn > 0)) continue;
+    if (C.temp && !(C.temp[c] < P.tmax_update)) continue;
+    const double ekt = C.e_kT[c];
+    for (int k = lane; k < n; k += 32) {
+      bl[k] = C.b[(size_t)c + (size_t)ncell * k];
+      ns[k] = C.nstar[(size_t)c + (size_t)ncell * k];
+      e[k] = 0;
+    }
+    for (int idx = lane; idx < n * n; idx += 32) W[idx] = 0;
+    __syncwarp();
+    // radiative rates, round by round
+    for (int r = 0; r < A.nround; r++) {
+      for (int t = A.round_off[r] + lane; t < A.round_off[r + 1]; t += 32) {
+        const int kr = A.order[t];
+        const int i = A.ti[kr], j = A.tj[kr];
+        if ((A.ev[j] - A.ev[i]) * ekt > A.cut_x) {
+          const double cut_rate = kr < A.nline ? A.Aji[kr] : A.bf_cut_rate;
+          W[i + n * j] = W[i + n * j] + cut_rate;
+          W[j + n * i] = W[j + n * i] + cut_rate * ns[j] / ns[i];
+          continue;
+        }
+        const double th = (double)C.gij[(size_t)c + (size_t)ncell * kr];
+        const double dv = (double)C.gji[(size_t)c + (size_t)ncell * kr];
+        double r_up, r_down;
+        if (kr < A.nline) {
+          const double g_ij = A.g[i] / A.g[j];
+          if (ns[i] > 0 && ns[j] > 0) {
+            const double beta_ref = ns[j] * g_ij / ns[i];
+            r_up = th * (beta_ref / (1.0 - beta_ref)) + dv;
+            r_down = g_ij * (th / (1.0 - beta_ref) + dv);
+          } else {
+            r_up = 0;
+            r_down = 0;
+          }
+        } else {
+          r_up = th;
+          r_down = dv;
+        }
+        W[j + n * i] = W[j + n * i] + r_up;
+        W[i + n * j] = W[i + n * j] + r_down;
+      }
+      __syncwarp();
+    }
+    // collisions times cswitch; the pairs are distinct
+    if (P.cswitch > 0 && A.ncol > 0) {
+      SeColCell cw{0, 0, 0, 0, 0};
+      if (!C.cup) cw = se_col_cell(C.temp[c], C.ne[c], ekt, C.dxi ? C.dxi[c] : 0.0);
+      for (int p = lane; p < A.ncol; p += 32) {
+        const double u = C.cup ? C.cup[(size_t)c + (size_t)ncell * p] : se_col_rate(A, cw, p);
+        if (u == 0) continue;
+        const int i = A.ci[p], j = A.cj[p];
+        const double nij = ns[i] / ns[j];
+        W[j + n * i] = W[j + n * i] + u * P.cswitch;
+        W[i + n * j] = W[i + n * j] + (u * nij) * P.cswitch;
+      }
+      __syncwarp();
+    }
+    // diagonal = -(column sum), each lane one column
+    for (int i = lane; i < n; i += 32) {
+      double s = 0;
+      for (int k = 0; k < n; k++) s = s + W[k + n * i];
+      W[i + n * i] = -s;
+    }
+    // the conservation row: the first level of largest b n*
+    int pos = 0;
+    {
+      double bst = bl[0] * ns[0];
+      for (int k = 1; k < n; k++) {
+        const double v = bl[k] * ns[k];
+        if (v > bst) { bst = v; pos = k; }
+      }
+    }
+    __syncwarp();
+    for (int idx = lane; idx < n * n; idx += 32) {
+      const int i = idx % n, j = idx / n;
+      W[idx] = (i == pos) ? bl[j] * ns[j] : (W[idx] * bl[j]) * ns[j];
+    }
+    if (lane == 0) e[pos] = totn;
+    __syncwarp();
+
+    if (P.solver == 1) se_solve_lineq(W, e, q, icol, n, lane);
+    else if (P.solver == 2) se_solve_partial(W, e, n, lane);
+    else se_solve_no_pivot(W, e, n, lane);
+
+    bool finite = true;
+    for (int k = lane; k < n; k += 32) finite = finite && (fabs(e[k]) <= DBL_MAX);
+    if (!__all_sync(0xffffffffu, finite)) {
+      if (lane == 0) atomicMin((unsigned long long *)nonfinite, (unsigned long long)c);
+      __syncwarp();
+      continue;
+    }
+    // limiter, under-relaxation, the update
+    for (int k = lane; k < n; k += 32) {
+      double x = e[k];
+      if (x < elo || x > eup) nclamp++;
+      ntot++;
+      if (x < elo) x = elo * exp(fmax(x, 0.0) / elo - 1.0);
+      else if (x > eup) x = eup * (2.0 - eup / x);
+      if (P.sor_w != 1.0) x = pow(x, P.sor_w);
+      q[k] = bl[k];          // bold
+      bl[k] = bl[k] * x;
+    }
+    __syncwarp();
+    double sum = 0;
+    for (int k = 0; k < n; k++) sum = sum + bl[k] * ns[k];
+    const double norm = totn / sum;
+    double wv = -1.0;
+    int wk = -1;
+    for (int k = lane, slot = 0; k < n; k += 32, slot++) {
+      double x = bl[k] * norm;
+      if (ns[k] > 0) x = fmax(x, fmin(1.0, P.min_pop_frac * totn / ns[k]));
+      const double bold = q[k];
+      const double ek = bold > 0 ? x / bold - 1.0 : 0.0;
+      if (fabs(ek) > fabs(lv[slot])) { lv[slot] = ek; lc[slot] = c; }
+      double ew = fabs(ek);
+      if (P.conv_pop_floor > 0) ew = ew * fmin(1.0, x * ns[k] / (P.conv_pop_floor * totn));
+      if (ew > wv) { wv = ew; wk = k; }  // a NaN never wins, as in the sequential scan
+      e[k] = ek;
+      C.b[(size_t)c + (size_t)ncell * k] = x;
+    }
+    warp_argmax(wv, wk);
+    __syncwarp();
+    if (wk >= 0 && wv > best.maxerr_abs) {
+      best.maxerr_abs = wv;
+      best.maxerr = copysign(wv, e[wk]);
+      best.cell = c;
+      best.level = wk;
+    }
+    __syncwarp();
+  }
+  // per-warp partials
+  if (lane == 0) wbest[gw] = best;
+  for (int k = lane, slot = 0; k < n; k += 32, slot++) {
+    lvl_val[(size_t)gw * n + k] = lv[slot];
+    lvl_cell[(size_t)gw * n + k] = lc[slot];
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    nclamp += __shfl_xor_sync(0xffffffffu, nclamp, o);
+    ntot += __shfl_xor_sync(0xffffffffu, ntot, o);
+  }
+  if (lane == 0 && ntot) {
+    atomicAdd(&counts[0], nclamp);
+    atomicAdd(&counts[1], ntot);
+  }
+}
+
+// one block: the largest change over the warps' partials, ties to the first cell
+__global__ void k_stateq_finish(int nwarp, int n, const SeWarpBest *__restrict__ wbest,
+                                const double *__restrict__ lvl_val, const long long *__restrict__ lvl_cell,
+                                SeWarpBest *__restrict__ out_best, double *__restrict__ out_lvl) {
+  __shared__ SeWarpBest sb[256];
+  SeWarpBest b;
+  b.maxerr_abs = 0;
+  b.maxerr = 0;
+  b.cell = -1;
+  b.level = -1;
+  b.pad = 0;
+  for (int w = threadIdx.x; w < nwarp; w += blockDim.x) {
+    const SeWarpBest o = wbest[w];
+    if (o.cell >= 0 && (b.cell < 0 || o.maxerr_abs > b.maxerr_abs || (o.maxerr_abs == b.maxerr_abs && o.cell < b.cell)))
+      b = o;
+  }
+  sb[threadIdx.x] = b;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    SeWarpBest r = sb[0];
+    for (int t = 1; t < (int)blockDim.x; t++) {
+      const SeWarpBest o = sb[t];
+      if (o.cell >= 0 && (r.cell < 0 || o.maxerr_abs > r.maxerr_abs || (o.maxerr_abs == r.maxerr_abs && o.cell < r.cell)))
+        r = o;
+    }
+    *out_best = r;
+  }
+  for (int k = threadIdx.x; k < n; k += blockDim.x) {
+    double v = 0;
+    long long cc = -1;
+    for (int w = 0; w < nwarp; w++) {
+      const long long oc = lvl_cell[(size_t)w * n + k];
+      const double ov = lvl_val[(size_t)w * n + k];
+      if (oc >= 0 && (cc < 0 || fabs(ov) > fabs(v) || (fabs(ov) == fabs(v) && oc < cc))) { v = ov; cc = oc; }
+    }
+    out_lvl[k] = v;
+  }
+}
+
+// ---- Ng acceleration (ng_mod.f90:241-390) ---------------------------------------
+// oldb holds n1, n2, n3 as three consecutive (cell, level) blocks of nv values.
+
+// per-block partial sums of d01, d02, d11, d12, d22, |d0|^2
+__global__ void k_ng_accumulate(long long nv, const double *__restrict__ b, const double *__restrict__ oldb,
+                                double *__restrict__ part) {
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nv; i += (long long)gridDim.x * blockDim.x) {
+    const double n1 = log(oldb[i]), n2 = log(oldb[i + nv]), n3 = log(oldb[i + 2 * nv]), n4 = log(b[i]);
+    const double d0 = n4 - n3, d1 = d0 - (n3 - n2), d2 = d0 - (n2 - n1);
+    acc[0] += d0 * d1;
+    acc[1] += d0 * d2;
+    acc[2] += d1 * d1;
+    acc[3] += d1 * d2;
+    acc[4] += d2 * d2;
+    acc[5] += d0 * d0;
+  }
+  __shared__ double red[6][32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int q = 0; q < 6; q++) {
+    double v = acc[q];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) red[q][w] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 6) {
+    double v = 0;
+    for (int t = 0; t < (int)(blockDim.x >> 5); t++) v += red[threadIdx.x][t];
+    part[(size_t)blockIdx.x * 6 + threadIdx.x] = v;
+  }
+}
+
+__global__ void k_ng_accumulate_finish(int nblk, const double *__restrict__ part, double *__restrict__ gram) {
+  if (threadIdx.x < 6) {
+    double v = 0;
+    for (int t = 0; t < nblk; t++) v += part[(size_t)t * 6 + threadIdx.x];
+    const int q = threadIdx.x;
+    // gram: d01, d02, d11, d12, d21, d22, |d0|^2
+    if (q == 0) gram[0] = v;
+    if (q == 1) gram[1] = v;
+    if (q == 2) gram[2] = v;
+    if (q == 3) { gram[3] = v; gram[4] = v; }
+    if (q == 4) gram[5] = v;
+    if (q == 5) gram[6] = v;
+  }
+}
+
+// pass 1: the largest |ln step| per block
+__global__ void k_ng_worst(long long nv, const double *__restrict__ b, const double *__restrict__ oldb, double a,
+                           double bc, double *__restrict__ part) {
+  double worst = 0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nv; i += (long long)gridDim.x * blockDim.x) {
+    const double n2 = log(oldb[i + nv]), n3 = log(oldb[i + 2 * nv]), n4 = log(b[i]);
+    const double e = (1.0 - a - bc) * n4 + a * n3 + bc * n2;
+    worst = fmax(worst, fabs(e - n4));
+  }
+  for (int o = 16; o > 0; o >>= 1) worst = fmax(worst, __shfl_xor_sync(0xffffffffu, worst, o));
+  __shared__ double red[32];
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = worst;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double v = 0;
+    for (int t = 0; t < (int)(blockDim.x >> 5); t++) v = fmax(v, red[t]);
+    part[blockIdx.x] = v;
+  }
+}
+
+// the veto (ng_mod.f90:345), written so that a NaN step is vetoed too
+__global__ void k_ng_decide(int nblk, const double *__restrict__ part, double a, double bc, double max_change,
+                            int *__restrict__ applied) {
+  if (threadIdx.x == 0) {
+    double worst = 0;
+    for (int t = 0; t < nblk; t++) worst = fmax(worst, part[t]);
+    *applied = (exp(worst) - 1.0 <= max_change && fabs(a) <= DBL_MAX && fabs(bc) <= DBL_MAX) ? 1 : 0;
+  }
+}
+
+struct NgBest { double v; long long pos; };  // pos = cell * nlevel + level; -1 none
+
+// pass 2, one thread per cell: the extrapolated b, renormalised
+__global__ void k_ng_apply(int ncell, int nlevel, double *__restrict__ b, const double *__restrict__ oldb,
+                           const double *__restrict__ nstar, const double *__restrict__ totn, double a, double bc,
+                           const int *__restrict__ applied, NgBest *__restrict__ part) {
+  NgBest best{0.0, -1};
+  if (*applied) {
+    const long long nv = (long long)ncell * nlevel;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += gridDim.x * blockDim.x) {
+      for (int k = 0; k < nlevel; k++) {
+        const long long i = c + (long long)ncell * k;
+        const double n2 = log(oldb[i + nv]), n3 = log(oldb[i + 2 * nv]), n4 = log(b[i]);
+        const double e = (1.0 - a - bc) * n4 + a * n3 + bc * n2;
+        b[i] = exp(e);
+        const double enew = exp(e - n4) - 1.0;
+        if (fabs(enew) > fabs(best.v)) { best.v = enew; best.pos = (long long)c * nlevel + k; }
+      }
+      double s = 0;
+      for (int k = 0; k < nlevel; k++) s = s + b[c + (long long)ncell * k] * nstar[c + (long long)ncell * k];
+      const double f = totn[c] / s;
+      for (int k = 0; k < nlevel; k++) b[c + (long long)ncell * k] = b[c + (long long)ncell * k] * f;
+    }
+  }
+  // block arg-max of |enew|, ties to the first (cell, level)
+  for (int o = 16; o > 0; o >>= 1) {
+    const double ov = __shfl_xor_sync(0xffffffffu, best.v, o);
+    const long long op = __shfl_xor_sync(0xffffffffu, best.pos, o);
+    if (op >= 0 && (best.pos < 0 || fabs(ov) > fabs(best.v) || (fabs(ov) == fabs(best.v) && op < best.pos))) {
+      best.v = ov;
+      best.pos = op;
+    }
+  }
+  __shared__ NgBest red[32];
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = best;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    NgBest r = red[0];
+    for (int t = 1; t < (int)(blockDim.x >> 5); t++) {
+      const NgBest o = red[t];
+      if (o.pos >= 0 && (r.pos < 0 || fabs(o.v) > fabs(r.v) || (fabs(o.v) == fabs(r.v) && o.pos < r.pos))) r = o;
+    }
+    part[blockIdx.x] = r;
+  }
+}
+
+__global__ void k_ng_apply_finish(int nblk, const NgBest *__restrict__ part, NgBest *__restrict__ out) {
+  if (threadIdx.x == 0) {
+    NgBest r{0.0, -1};
+    for (int t = 0; t < nblk; t++) {
+      const NgBest o = part[t];
+      if (o.pos >= 0 && (r.pos < 0 || fabs(o.v) > fabs(r.v) || (fabs(o.v) == fabs(r.v) && o.pos < r.pos))) r = o;
+    }
+    *out = r;
+  }
+}
+
+}  // namespace m3d

@@ -280,3 +280,139 @@ def lte_config(kind: str, seed: int | None = None, nf: int | None = None, window
     atm.update({k: np.ascontiguousarray(v, np.float32).ravel() for k, v in cf.items()})
     vec, wmu = gauss_rays(5) if kind == "c0" else lobatto_rays(4, 4)
     return atm, np.ascontiguousarray(nu_all[sl]), np.ascontiguousarray(llam_all[sl]), vec, wmu
+
+
+# ---- NLTE: a seeded model atom and the per-cell inputs of its SE update ---------------
+RYDV = 13.605
+
+
+def model_atom(seed: int = 2, nbound: int = 20, nline: int = 60, e_max: float = 7.0, e_ion: float = 7.9,
+               logf=(-4.0, 0.0)) -> dict:
+    """A seeded model atom: nbound levels of the neutral (ground at 0 eV, the rest
+    uniform in [0, e_max]) plus the ground level of the ion at e_ion; nline lines
+    between distinct random bound pairs with log f uniform in logf; one continuum
+    from every bound level to the ion; classic_col pairs as the reference fills
+    them for an atom without collision data: van Regemorter for every bound pair
+    (f of the pair's line, or 0) and Seaton for every continuum, whose alpha0 is
+    the hydrogenic 7.91e-18 n_eff cm^2 for even levels and 0 (Kramers inside
+    the collision recipe) for odd ones.  Indices are 0-based."""
+    rng = np.random.default_rng(seed + 2000)
+    ev = np.concatenate([[0.0], np.sort(rng.uniform(0.0, e_max, nbound - 1)), [e_ion]])
+    g = np.concatenate([rng.choice([1.0, 3.0, 5.0, 7.0, 9.0], nbound), [1.0]])
+    ion = np.concatenate([np.ones(nbound, np.int32), [2]]).astype(np.int32)
+    n = nbound + 1
+    pairs = [(i, j) for i in range(nbound) for j in range(i + 1, nbound)]
+    pick = np.sort(rng.choice(len(pairs), size=min(nline, len(pairs)), replace=False))
+    lines = [pairs[p] for p in pick]
+    f = 10.0 ** rng.uniform(*logf, len(lines))
+    ti = [i for i, _ in lines] + list(range(nbound))
+    tj = [j for _, j in lines] + [nbound] * nbound
+    lam_aa = np.array([HH * CC / ((ev[j] - ev[i]) * EE) * 1e8 for i, j in lines])
+    # A_ji = 6.670e15 g_i/g_j f / lambda[AA]^2
+    aji = np.concatenate([6.670e15 * g[[i for i, _ in lines]] / g[[j for _, j in lines]] * f / lam_aa**2,
+                          np.zeros(nbound)])
+    fpair = {p: fv for p, fv in zip(lines, f)}
+    col_i, col_j, col_kind, col_fac = [], [], [], []
+    for i in range(nbound):
+        for j in range(i + 1, n):
+            if ion[j] > ion[i]:
+                col_i.append(i)
+                col_j.append(j)
+                col_kind.append(2)
+                col_fac.append(7.91e-18 * math.sqrt(RYDV / (e_ion - ev[i])) if i % 2 == 0 else 0.0)
+            else:
+                col_i.append(i)
+                col_j.append(j)
+                col_kind.append(1)
+                col_fac.append(fpair.get((i, j), 0.0))
+    return {"nlevel": n, "g": g, "ev": ev, "ion": ion,
+            "ti": np.array(ti, np.int32), "tj": np.array(tj, np.int32), "nline": len(lines),
+            "Aji": aji, "active": None, "line_f": f,
+            "col_i": np.array(col_i, np.int32), "col_j": np.array(col_j, np.int32),
+            "col_kind": np.array(col_kind, np.int32), "col_fac": np.array(col_fac, np.float32),
+            "fmin": float(np.float32(1e-6)), "cbbesc": 1.0, "cbfesc": 1.0, "colscale": 1.0,
+            "upsilon_floor": 0.0, "cut_x": 70.0, "bf_cut_rate": 1.0}
+
+
+def lte_populations(atom: dict, temp, ne, totn, dxi=None):
+    """compute_lte_populations with the atom's own levels as partition function
+    (level_partf, atom_mod.f90:1041-1140) and lte_pop (:1132-1150), in float64:
+    returns nstar (nlevel, ncell) and totn = sum of nstar."""
+    temp = np.asarray(temp, np.float64)
+    ne = np.asarray(ne, np.float64)
+    e_kT = (EE / BK) / temp
+    lsaha = np.log(2.0 * (2.0 * PI * EM * BK * temp / HH**2) ** 1.5 / ne)
+    dxi = np.zeros_like(temp) if dxi is None else np.asarray(dxi, np.float64)
+    ion0 = atom["ion"][0]
+    ns = np.empty((atom["nlevel"], temp.size))
+    for i in range(atom["nlevel"]):
+        j = atom["ion"][i]
+        evi = atom["ev"][i] - dxi * 0.5 * (j - 1) * j
+        tns = math.log(atom["g"][i]) - e_kT * evi + (j - ion0) * lsaha
+        ns[i] = np.exp(tns)
+    ns *= np.asarray(totn, np.float64) / ns.sum(axis=0)
+    return ns, ns.sum(axis=0)
+
+
+def se_inputs(atom: dict, temp, ne, nH, seed: int = 2, dilution=None, perturb: float = 0.3,
+              abundance: float = 7.5) -> dict:
+    """Per-cell inputs of one SE update (all (level or transition, cell), cell fastest):
+    temp, ne, e_kT, nstar, totn, b (LTE times exp(N(0, perturb))), and the rates a
+    diluted Planck field J = W B(T) gives: for a line th = g_j/g_i A_ji and
+    dev = th n_ref (W - 1) (so R_ij = B_ij J, R_ji = A_ji + B_ji J in the
+    (th, dev) form of line_rate_coefficients), for a continuum gamma_ij = W R0
+    and gamma_ji = R0 n*_i/n*_j with R0 = 1e3/s.  W = 1 is LTE: detailed balance
+    holds for every transition and b = 1 solves the rate equations."""
+    rng = np.random.default_rng(seed + 3000)
+    temp = np.ascontiguousarray(temp, np.float64).ravel()
+    ne = np.ascontiguousarray(ne, np.float64).ravel()
+    nH = np.ascontiguousarray(nH, np.float64).ravel()
+    ncell = temp.size
+    totn0 = 10.0 ** (abundance - 12.0) * nH
+    nstar, totn = lte_populations(atom, temp, ne, totn0)
+    e_kT = (EE / BK) / temp
+    W = np.ones(ncell) if dilution is None else np.broadcast_to(np.asarray(dilution, np.float64), (ncell,))
+    nrad, nline = len(atom["ti"]), atom["nline"]
+    gij = np.zeros((nrad, ncell), np.float32)
+    gji = np.zeros((nrad, ncell), np.float32)
+    for kr in range(nrad):
+        i, j = atom["ti"][kr], atom["tj"][kr]
+        if kr < nline:
+            hnu_kt = (atom["ev"][j] - atom["ev"][i]) * e_kT
+            nref = 1.0 / np.expm1(hnu_kt)
+            th = atom["g"][j] / atom["g"][i] * atom["Aji"][kr]
+            gij[kr] = th
+            gji[kr] = th * nref * (W - 1.0)
+        else:
+            gij[kr] = 1e3 * W
+            gji[kr] = 1e3 * nstar[i] / nstar[j]
+    b = np.exp(perturb * rng.standard_normal((atom["nlevel"], ncell))) if perturb > 0 else np.ones((atom["nlevel"], ncell))
+    return {"temp": temp, "ne": ne, "e_kT": e_kT, "nstar": np.ascontiguousarray(nstar),
+            "totn": np.ascontiguousarray(totn), "b": np.ascontiguousarray(b), "gamma_ij": gij, "gamma_ji": gji}
+
+
+def se_config(kind: str = "small", seed: int | None = None, ncell: int | None = None, lte: bool = False,
+              nbound: int = 20, nline: int = 60) -> tuple:
+    """(atom, inputs) of an SE case.  'c2': the 120^3 cube of seed 2 and the
+    20-level atom (a radiation field diluted upwards, W = exp(-3 z/nz));
+    'small': ncell cells (default 2048) drawn from a 16^3 cube with W uniform
+    in [0.05, 1]; lte: W = 1.  nbound/nline: the atom's bound levels and lines
+    (60/180 for the larger atom of the batched configuration)."""
+    if kind == "c2":
+        seed = 2 if seed is None else seed
+        cube = cube_atmosphere(seed, 120, 120, 120)
+        nz = 120
+        W = np.exp(-3.0 * (np.arange(nz) + 0.5) / nz)[:, None, None] * np.ones((1, 120, 120))
+    elif kind == "small":
+        seed = 5 if seed is None else seed
+        cube = cube_atmosphere(seed, 16, 16, 16)
+        W = np.random.default_rng(seed + 4000).uniform(0.05, 1.0, 16**3)
+    else:
+        raise ValueError(kind)
+    atom = model_atom(seed, nbound=nbound, nline=nline)
+    temp, ne, nH = cube["temp"].ravel(), cube["ne"].ravel(), cube["nH"].ravel()
+    W = np.asarray(W).ravel()
+    if ncell is not None:
+        idx = np.arange(ncell) % temp.size
+        temp, ne, nH, W = temp[idx], ne[idx], nH[idx], W[idx]
+    return atom, se_inputs(atom, temp, ne, nH, seed=seed, dilution=None if lte else W)

@@ -233,6 +233,91 @@ int m3d_lte_synthesis(const m3d_atmos_t *atm, int nf, const double *nu, const do
                       int nray, const double *vec, const double *wmu, void *i_top, float *ie,
                       float *flux, unsigned flags);
 
+/* ---- statistical equilibrium (FP64) ----
+ * Level and transition indices are 0-based (the reference's minus one).  Per-cell
+ * arrays keep the cell index fastest: b(cell, level) at b[cell + ncell*level], as
+ * adata%b(x,y,z,level) with cell = x + nx*(y + ny*z).  The atom tables are host
+ * memory whatever the flags; M3D_DEVICE_PTRS applies to the per-cell arrays. */
+#define M3D_SE_LINEQ_NO_PIVOT 0 /* lse_solver='lineq_no_pivot' (default; 'eqsyst' rounds identically) */
+#define M3D_SE_LINEQ 1          /* lse_solver='lineq': full pivoting */
+#define M3D_SE_LU_PARTIAL 2     /* LU with partial (row) pivoting */
+#define M3D_COL_REGEMORTER 1    /* e_excitation='regemorter' (atom_mod.f90:1825-1832) */
+#define M3D_COL_SEATON 2        /* e_ionisation='seaton' (atom_mod.f90:1814-1822) */
+
+/* The model atom (atom_type, atom_mod.f90:120-160).  Transitions 0..nline-1 are the
+ * lines, nline..nrad-1 the continua.  Collision pairs are the (i < j) pairs that
+ * classic_col fills with an electron recipe, each pair at most once. */
+typedef struct m3d_atom {
+  int nlevel;                  /* 1..64 */
+  int nrad, nline;             /* transitions, of which lines */
+  int ncol;                    /* electron-collision pairs */
+  const int *trans_i, *trans_j;   /* (nrad) lower, upper level */
+  const unsigned char *active;    /* (nrad) trans%active, or NULL for all */
+  const double *Aji;              /* (nrad) line Einstein A [1/s]; the cut rate of a line */
+  const double *g, *ev;           /* (nlevel) statistical weight, energy [eV] */
+  const int *ion;                 /* (nlevel) ion stage, 1 = neutral */
+  const int *col_i, *col_j, *col_kind; /* (ncol) pair and M3D_COL_* */
+  const float *col_fac;           /* (ncol) cdata(tri): f of a line, alpha0 of a continuum, 0 */
+  double fmin;                    /* atom_params fmin, (double)1e-6f */
+  double cbbesc, cbfesc, colscale, upsilon_floor; /* 1, 1, 1, 0 */
+  double cut_x, bf_cut_rate;      /* radiative cut, 70 and 1 [1/s] (atom_mod.f90:256-257) */
+} m3d_atom_t;
+
+typedef struct m3d_se_params {
+  double max_update;     /* 100 */
+  double sor_w;          /* 1 */
+  double min_pop_frac;   /* 1e-30 */
+  double conv_pop_floor; /* 0 */
+  double tmax_update;    /* 1e7 K; needs temp */
+  double cswitch;        /* factor on the collision matrix, 0 leaves collisions out */
+  int solver;            /* M3D_SE_* */
+  int pad;
+} m3d_se_params_t;
+
+typedef struct m3d_se_result {
+  double maxerr;         /* adata%maxerr: signed largest (conv_pop_floor-weighted) relative change */
+  long long epos_cell;   /* its cell, -1 if nothing changed */
+  int epos_level;        /* its level, -1 if nothing changed */
+  int pad;
+  long long nclamp, ntot; /* corrections cut by the limiter, all corrections (ng_count_clamped) */
+  long long nonfinite_cell; /* first cell whose solution was not finite, -1 if none */
+} m3d_se_result_t;
+
+/* classic_col's electron rates (atom_mod.f90:1758-1850): cup (ncell, ncol) [1/s],
+ * upward, colscale applied; the downward rate is cup * n*_i/n*_j.  dxi may be NULL (0). */
+int m3d_collision_rates(const m3d_atom_t *atom, int ncell, const double *temp, const double *ne,
+                        const double *e_kT, const double *dxi, double *cup, unsigned flags);
+
+/* update_populations (atom_mod.f90:439-732) with setup_transition_matrix (:740-841):
+ * for every cell with totn > 0 (and temp < tmax_update when temp is given) the rate
+ * matrix from gamma_ij/gamma_ji (ncell, nrad) float32 -- a line's thermal and
+ * deviation integrals, a continuum's upward and downward rates -- plus
+ * collisions x cswitch, the solve, the limiter, e^sor_w, renormalisation to totn and
+ * the population floor; b (ncell, nlevel) is updated in place.  Collisions come from
+ * cup (ncell, ncol) when given, else from temp, ne, e_kT, dxi as m3d_collision_rates
+ * forms them.  lvlerr (nlevel, host) and res (host) receive the convergence record.
+ * A cell whose solution is not finite keeps its b, and the call returns
+ * M3D_ENONFINITE with res->nonfinite_cell set (the reference stops the run there). */
+int m3d_stateq_update(const m3d_atom_t *atom, const m3d_se_params_t *par, int ncell, double *b,
+                      const double *nstar, const double *totn, const double *temp, const double *ne,
+                      const double *e_kT, const double *dxi, const float *gamma_ij,
+                      const float *gamma_ji, const double *cup, double *lvlerr,
+                      m3d_se_result_t *res, unsigned flags);
+
+/* ng_accumulate (ng_mod.f90:241-287): gram (host, 7) = d01, d02, d11, d12, d21, d22
+ * and |d0|^2 over all cells and levels of ln b; oldb is (ncell, nlevel, 3), the
+ * iterates n1, n2, n3. */
+int m3d_ng_accumulate(int ncell, int nlevel, const double *b, const double *oldb, double *gram,
+                      unsigned flags);
+
+/* ng_extrapolate (ng_mod.f90:314-390): b = exp((1-a-bc) n4 + a n3 + bc n2), renormalised
+ * per cell to totn, unless some level would move by more than max_change (or a, bc
+ * are not finite): then b is untouched and *applied = 0.  emax, epos_cell, epos_level
+ * (host) give the largest relative change. */
+int m3d_ng_extrapolate(int ncell, int nlevel, double *b, const double *oldb, const double *nstar,
+                       const double *totn, double a, double bc, double max_change, int *applied,
+                       double *emax, long long *epos_cell, int *epos_level, unsigned flags);
+
 #ifdef __cplusplus
 }
 #endif
