@@ -17,6 +17,7 @@
 #include "../../include/m3dgpu.h"
 #include "m3d_pipeline.cuh"
 #include "m3d_stateq.cuh"
+#include "m3d_nlte.cuh"
 
 using namespace m3d;
 
@@ -1075,6 +1076,7 @@ int m3d_lte_synthesis(const m3d_atmos_t *atm, int nf, const double *nu, const do
 }  // extern "C"
 
 #include "m3d_stateq_api.inc"
+#include "m3d_nlte_api.inc"
 
 // ===========================================================================
 // rotate_array without any allocation.

@@ -1,0 +1,415 @@
+// Model-atom opacities and ALI rate integrals of one frequency window
+// (non-hydrogen lines), FP32 with the reference's real(8) constants:
+//   bound_bound_damping / line_damping    SRC/rt_patch_mod.f90:2649-2681, HOP/bbtrans_mod.f90:78-106
+//   add_bound_free_opacities              SRC/rt_patch_mod.f90:2581-2643
+//   foreground's split start              SRC/rt_patch_mod.f90:1474-1487
+//   add_bound_bound_opacities             SRC/rt_patch_mod.f90:2689-2831
+//   add_largest / other_contribution      SRC/rt_patch_mod.f90:3150-3187
+//   work_to_transfer_units (split form)   SRC/rt_patch_mod.f90:3571-3651
+//   bound_bound_rates                     SRC/rt_patch_mod.f90:2852-3142
+//   bound_free_rates                      SRC/rt_patch_mod.f90:3193-3259
+//   integrate_rates                       SRC/rt_patch_mod.f90:3437-3465
+//   normalize_profiles                    SRC/atom_mod.f90:377-430
+//   combine_twin_hemispheres' average     SRC/rt_patch_mod.f90:1812-1887
+//
+// The opacity kernels give one thread one (f, cell) point, which walks the
+// transitions that cover f in their window order, so every point accumulates
+// in the reference's order.  The rate kernels give one thread one
+// (transition, cell) pair, which sums over the transition's points in f
+// order.  A real(4) local assigned from a real(8) expression is rounded where
+// the Fortran assigns it.
+#pragma once
+#include "m3d_qlg.cuh"
+
+namespace m3d {
+
+struct NlWinDev {
+  int nf, nline, ncont;
+  const int *li, *lj, *lntrans, *lindex, *lblue, *lred, *loff;
+  const float *q;
+  const double *wnu, *wq, *Bij, *Aij, *lower_ev, *grad, *gw1, *gw2, *gstk;
+  const unsigned char *lactive, *lsums, *unsold;
+  const int *ci, *cj, *cntrans, *cblue, *cred, *coff;
+  const float *alpha;
+  const double *cwnu;
+  const unsigned char *cactive;
+  const double *g, *ev;
+  double cut_x;
+  // per frequency: the active lines / continua whose window holds f, ascending
+  const int *lf_ptr, *lf_idx, *cf_ptr, *cf_idx;
+};
+
+// qlg_bot_profile (qlg_mod.f90:682-689)
+__device__ __forceinline__ float nl_profile(const float2 *tab, float a, float q, float vpr, float idf) {
+  const float v = fabsf(q - vpr) * idf;
+  const QlgCoef c = qlg_setup(a, 1.0f, 0.8325546112f, 1.7724538509f);
+  const float K1 = qlg_eval(tab, c, v);
+  return ((K1 * 0.5641895835f) * idf) * (q + 1.0f);
+}
+
+__global__ void k_bb_damping(NlWinDev W, int ncell, const float *__restrict__ ne, const float *__restrict__ tothi,
+                             const float *__restrict__ vbar2, const float *__restrict__ stark_pe,
+                             const float *__restrict__ unsold, const float *__restrict__ inv_df,
+                             float *__restrict__ adamp) {
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += gridDim.x * blockDim.x) {
+    for (int i = 0; i < W.nline; i++) {
+      if (W.lactive && !W.lactive[i]) continue;
+      float a = 0.0f;
+      if (W.unsold[i]) a = (float)((double)a + W.gw1[i] * (double)unsold[c]);
+      else a = (float)((double)a + (W.gw1[i] == 0.0 ? 0.0 : W.gw1[i] * pow((double)vbar2[c], W.gw2[i]) * (double)tothi[c]));
+      if (W.gstk[i] >= 0.0) a = (float)((double)a + W.gstk[i] * (double)ne[c]);
+      else a = (float)((double)a - W.gstk[i] * (double)stark_pe[c]);
+      a = (float)((double)a + W.grad[i]);
+      adamp[(size_t)c + (size_t)ncell * i] = a * inv_df[c];
+    }
+  }
+}
+
+__global__ void k_bf_opacity(NlWinDev W, int ncell, const double *__restrict__ b, const double *__restrict__ nstar,
+                             const double *__restrict__ pop_ratio, const double *__restrict__ e_kT,
+                             float *__restrict__ xhat, float *__restrict__ ehat) {
+  const size_t nf = (size_t)W.nf, n = nf * ncell;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+    const int f = (int)(k % nf), c = (int)(k / nf);
+    const int p0 = W.cf_ptr[f], p1 = W.cf_ptr[f + 1];
+    if (p0 == p1) continue;
+    float xh = xhat[k], eh = ehat[k];
+    for (int p = p0; p < p1; p++) {
+      const int i = W.cf_idx[p];
+      const int li = W.ci[i], lj = W.cj[i];
+      const double ns = nstar[(size_t)c + (size_t)ncell * li];
+      float ni, tmp;
+      if (b) {
+        ni = (float)(ns * b[(size_t)c + (size_t)ncell * li] * pop_ratio[c]);
+        tmp = (float)(ns * b[(size_t)c + (size_t)ncell * lj] * pop_ratio[c]);
+        if ((W.ev[lj] - W.ev[li]) * e_kT[c] > W.cut_x) tmp = 0.0f;
+      } else {
+        ni = (float)(ns * pop_ratio[c]);
+        tmp = ni;
+      }
+      const float alpha = W.alpha[W.coff[i] + f - W.cblue[i]];
+      xh = xh + alpha * ni;
+      eh = eh + alpha * tmp;
+    }
+    xhat[k] = xh;
+    ehat[k] = eh;
+  }
+}
+
+__device__ __forceinline__ void add_largest(float value, int index, float &largest, float &rest, int &largest_index) {
+  if (fabsf(value) > fabsf(largest)) {
+    rest = rest + largest;
+    largest = value;
+    largest_index = index;
+  } else {
+    rest = rest + value;
+  }
+}
+
+__device__ __forceinline__ float other_contribution(float value, int index, float largest, float rest,
+                                                    int largest_index) {
+  return index == largest_index ? rest : largest + (rest - value);
+}
+
+struct NlSplit {
+  float *sopL, *sopR, *schL, *schR;
+  int *sid, *schid;
+};
+
+__global__ void k_bb_opacity(NlWinDev W, int ncell, const double *__restrict__ b, const double *__restrict__ nstar,
+                             const double *__restrict__ pop_ratio, const double *__restrict__ e_kT,
+                             const float *__restrict__ inv_df, const float *__restrict__ vproj,
+                             const float *__restrict__ adamp, const float2 *__restrict__ tab, int lte,
+                             float *__restrict__ xhat, float *__restrict__ ehat, NlSplit S) {
+  const size_t nf = (size_t)W.nf, n = nf * ncell;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+    const int f = (int)(k % nf), c = (int)(k / nf);
+    float xh = xhat[k], eh = ehat[k];
+    float oL = eh, oR = 0.0f, cL = xh, cR = 0.0f;
+    int oid = 0, cid = 0;
+    const int p0 = W.lf_ptr[f], p1 = W.lf_ptr[f + 1];
+    if (p0 < p1) {
+      const float idf = inv_df[c], vpr = vproj[c], ekt = (float)e_kT[c];
+      for (int p = p0; p < p1; p++) {
+        const int i = W.lf_idx[p];
+        const int li = W.li[i], lj = W.lj[i];
+        const float ni = (float)(nstar[(size_t)c + (size_t)ncell * li] * pop_ratio[c]);
+        float bi = 1.0f, bj = 1.0f;
+        if (!lte && b) {
+          bi = (float)b[(size_t)c + (size_t)ncell * li];
+          bj = (float)b[(size_t)c + (size_t)ncell * lj];
+        }
+        const float lower_off = (float)(W.lower_ev[i] - W.ev[li]);
+        if (lower_off != 0.0f) {
+          bi = bi * expf(-lower_off * ekt);
+          bj = bj * expf(-lower_off * ekt);
+        }
+        const float phi = nl_profile(tab, adamp[(size_t)c + (size_t)ncell * i], W.q[W.loff[i] + f - W.lblue[i]], vpr, idf);
+        const float Rij = (float)((double)ni * W.Bij[i]);
+        const float eta_fac = Rij * bj, chi_fac = Rij * bi;
+        xh = xh + phi * chi_fac;
+        eh = eh + phi * eta_fac;
+        if (S.sopL) {
+          add_largest(phi * eta_fac, W.lindex[i], oL, oR, oid);
+          add_largest(phi * chi_fac, W.lindex[i], cL, cR, cid);
+        }
+      }
+      xhat[k] = xh;
+      ehat[k] = eh;
+    }
+    if (S.sopL) {
+      S.sopL[k] = oL;
+      S.sopR[k] = oR;
+      S.sid[k] = oid;
+      S.schL[k] = cL;
+      S.schR[k] = cR;
+      S.schid[k] = cid;
+    }
+  }
+}
+
+// the direction's profile integral of the lines that sum over windows, one
+// thread per (line, cell): wphi(cell, ntrans) += wmu * sum(phi * wq)
+__global__ void k_bb_wphi(NlWinDev W, int ncell, const float *__restrict__ inv_df, const float *__restrict__ vproj,
+                          const float *__restrict__ adamp, const float2 *__restrict__ tab, float wmu,
+                          float *__restrict__ wphi) {
+  const size_t n = (size_t)ncell * W.nline;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+    const int c = (int)(k % ncell), i = (int)(k / ncell);
+    if ((W.lactive && !W.lactive[i]) || !W.lsums[i]) continue;
+    const float idf = inv_df[c], vpr = vproj[c], a = adamp[k];
+    double s = 0.0;
+    for (int f = W.lblue[i]; f <= W.lred[i]; f++) {
+      const int o = W.loff[i] + f - W.lblue[i];
+      s = s + (double)nl_profile(tab, a, W.q[o], vpr, idf) * W.wq[o];
+    }
+    const size_t kw = (size_t)c + (size_t)ncell * W.lntrans[i];
+    wphi[kw] = wphi[kw] + wmu * (float)s;
+  }
+}
+
+__global__ void k_transfer_units_split(size_t n, float *__restrict__ w1, float *__restrict__ w2,
+                                       const float *__restrict__ beta, const float *__restrict__ sopL,
+                                       const float *__restrict__ sopR, const float *__restrict__ scat, float fl,
+                                       int suppress, int *n_floored) {
+  int cnt = 0;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+    const float be = beta[k];
+    const float eta_rest = be * sopR[k];
+    float eta = be * sopL[k] + eta_rest;
+    const float xhat = w1[k];
+    float chi = xhat - eta;
+    if (scat) eta = be * sopL[k] + (eta_rest + scat[k]);
+    const float floor_ = fmaxf(fl * fabsf(xhat), FLT_MIN);
+    if (suppress) chi = fmaxf(chi, floor_);
+    else if (fabsf(chi) < floor_) { chi = copysignf(floor_, chi); cnt++; }
+    w1[k] = chi;
+    w2[k] = eta / chi;
+  }
+  if (n_floored && cnt) atomicAdd(n_floored, cnt);
+}
+
+struct NlRateOpts { int split, precond, per_direction, use_flags, do_scat; float wmu, wtot; };
+
+struct NlRadField {
+  const float *work1, *inu, *psi, *irem, *escape, *beta, *Bnu, *scat;
+  const float *sopL, *sopR, *schL, *schR;
+  const int *sid, *schid;
+};
+
+__global__ void k_bb_rates(NlWinDev W, NlRateOpts O, int ncell, const double *__restrict__ b,
+                           const double *__restrict__ nstar, const double *__restrict__ pop_ratio,
+                           const double *__restrict__ e_kT, const float *__restrict__ inv_df,
+                           const float *__restrict__ vproj, const float *__restrict__ adamp,
+                           const float2 *__restrict__ tab, NlRadField R, const unsigned *__restrict__ flags_in,
+                           unsigned *__restrict__ flags_raise, float *__restrict__ gamma_ij,
+                           float *__restrict__ gamma_ji) {
+  const size_t nf = (size_t)W.nf, n = (size_t)ncell * W.nline;
+  for (size_t kk = blockIdx.x * (size_t)blockDim.x + threadIdx.x; kk < n; kk += (size_t)gridDim.x * blockDim.x) {
+    const int c = (int)(kk % ncell), i = (int)(kk / ncell);
+    if (W.lactive && !W.lactive[i]) continue;
+    const int li = W.li[i], lj = W.lj[i], fs = W.lblue[i], fe = W.lred[i], off = W.loff[i];
+    const bool own_norm = O.per_direction && !W.lsums[i];
+    const int index = W.lindex[i];
+    const double Aij = W.Aij[i];
+    const double nsi = nstar[(size_t)c + (size_t)ncell * li], nsj = nstar[(size_t)c + (size_t)ncell * lj];
+    const double bbi = b[(size_t)c + (size_t)ncell * li], bbj = b[(size_t)c + (size_t)ncell * lj];
+    float ni = (float)(bbi * nsi), nj = (float)(bbj * nsj);
+    const float idf = inv_df[c], vpr = vproj[c], a = adamp[kk], ekt = (float)e_kT[c];
+    const float lower_off = (float)(W.lower_ev[i] - W.ev[li]);
+    float inv_nref = 0.0f;
+    if (nsi > 0 && nsj > 0) {
+      const double beta_ref = nsj * W.g[li] / (nsi * W.g[lj]);
+      inv_nref = (float)fmin((1.0 - beta_ref) / beta_ref, 1e35);
+    }
+    if (lower_off != 0.0f) {
+      ni = ni * expf(-lower_off * ekt);
+      nj = nj * expf(-lower_off * ekt);
+    }
+    float eta_coef = 0.0f, abs_coef = 0.0f, g_ratio = 0.0f;
+    if (O.precond) {
+      float split_bj = (float)bbj;
+      if (lower_off != 0.0f) split_bj = split_bj * expf(-lower_off * ekt);
+      float split_Rij = (float)(nsi * pop_ratio[c]);
+      split_Rij = (float)((double)split_Rij * W.Bij[i]);
+      eta_coef = split_Rij * split_bj;
+      float split_bi = (float)bbi;
+      if (lower_off != 0.0f) split_bi = split_bi * expf(-lower_off * ekt);
+      abs_coef = split_Rij * split_bi;
+      if (nj > 0.0f) g_ratio = (float)((double)(ni / nj) * (W.g[lj] / W.g[li]));
+    }
+    float sum_A = 0, sum_I = 0, sum_P = 0, sum_T = 0, sum_U = 0, sum_w = 0;
+    int in_force = 0, raise = 0;
+    const int t = W.lntrans[i], pw = t >> 5, pb = t & 31;
+    if (O.split && O.precond && O.use_flags) in_force = (flags_in[(size_t)c + (size_t)ncell * pw] >> pb) & 1u;
+    for (int f = fs; f <= fe; f++) {
+      const size_t k = (size_t)f + nf * c;
+      const int o = off + f - fs;
+      const float phi = nl_profile(tab, a, W.q[o], vpr, idf);
+      const float wmunu = (float)((double)O.wmu * W.wnu[o] * Aij);
+      const float wqf = (float)W.wq[o];
+      if (!O.split) {
+        const float vvv = phi * wmunu;
+        if (own_norm) sum_w = sum_w + phi * wqf;
+        sum_A = sum_A + vvv * (R.Bnu[k] * inv_nref);
+        sum_I = sum_I + vvv * R.inu[k];
+        sum_P = sum_P + vvv * phi * R.psi[k] * R.beta[k];
+      } else {
+        if (own_norm) sum_w = sum_w + phi * wqf;  // sum(vph * wqf), in the same f order
+        const float nb = R.Bnu[k];
+        const float vvv = phi * wmunu;
+        if (O.precond) {
+          const float be = R.beta[k];
+          float psi = R.psi[k];
+          const float eta_u = phi * eta_coef;
+          const float eta_t = eta_u * be;
+          const float chi_t = phi * abs_coef - eta_t;
+          const float eta_other = be * other_contribution(eta_u, index, R.sopL[k], R.sopR[k], R.sid[k]);
+          const float chi_other = other_contribution(phi * abs_coef, index, R.schL[k], R.schR[k], R.schid[k]) - eta_other;
+          float other = eta_other;
+          if (O.do_scat) other = other + R.scat[k];
+          if (chi_t < 0.0f || in_force) psi = 0.0f;
+          raise = raise || psi == 0.0f;
+          const float up = psi == 0.0f ? R.inu[k] : R.irem[k] + psi * other;
+          const float spont = psi == 0.0f ? 1.0f : (chi_other + R.escape[k] * chi_t) / R.work1[k];
+          sum_T = sum_T + vvv * spont * (nb * inv_nref);
+          sum_U = sum_U + vvv * (up - nb * spont);
+        } else {
+          sum_T = sum_T + vvv * (nb * inv_nref);
+          sum_U = sum_U + vvv * (R.inu[k] - nb);
+        }
+      }
+    }
+    if (O.split && O.precond && O.use_flags && raise && !in_force)
+      atomicOr(&flags_raise[(size_t)c + (size_t)ncell * pw], 1u << pb);
+    float g_th, g_dev;
+    if (O.split) {
+      g_th = sum_T;
+      g_dev = sum_U;
+    } else {
+      g_th = sum_A;
+      g_dev = sum_I;
+      if (O.precond) {
+        g_th = g_th - sum_P * eta_coef * (g_ratio - 1.0f);
+        g_dev = g_dev - sum_P * eta_coef;
+      }
+      if (inv_nref > 0.0f) g_dev = g_dev - g_th / inv_nref;
+    }
+    if (own_norm && sum_w > 0.0f) {
+      g_th = g_th / (sum_w * O.wtot);
+      g_dev = g_dev / (sum_w * O.wtot);
+    }
+    gamma_ij[kk] = gamma_ij[kk] + g_th;
+    gamma_ji[kk] = gamma_ji[kk] + g_dev;
+  }
+}
+
+__global__ void k_bf_rates(NlWinDev W, int ncell, int precond, const double *__restrict__ b,
+                           const double *__restrict__ nstar, const double *__restrict__ e_kT,
+                           const float *__restrict__ twohnu3_c2, const float *__restrict__ Jnu,
+                           const float *__restrict__ PsiJ, const float *__restrict__ beta,
+                           float *__restrict__ gamma_ij, float *__restrict__ gamma_ji) {
+  const size_t nf = (size_t)W.nf, n = (size_t)ncell * W.ncont;
+  for (size_t kk = blockIdx.x * (size_t)blockDim.x + threadIdx.x; kk < n; kk += (size_t)gridDim.x * blockDim.x) {
+    const int c = (int)(kk % ncell), j = (int)(kk / ncell);
+    if (W.cactive && !W.cactive[j]) continue;
+    const int li = W.ci[j], lj = W.cj[j], fs = W.cblue[j], fe = W.cred[j], off = W.coff[j];
+    if ((W.ev[lj] - W.ev[li]) * e_kT[c] > W.cut_x) continue;
+    float sum_abs = 0, sum_ems = 0, sum_pre = 0;
+    for (int f = fs; f <= fe; f++) {
+      const size_t k = (size_t)f + nf * c;
+      const int o = off + f - fs;
+      const float wmunu = (float)(0.5 * W.cwnu[o]);
+      const float vij = twohnu3_c2[f] * W.alpha[o] * wmunu;
+      const float vji = vij * beta[k];
+      const float phi = PsiJ[k] * W.alpha[o];
+      sum_abs = sum_abs + vij * Jnu[k];
+      sum_ems = sum_ems + vji * (Jnu[k] + 1.0f);
+      sum_pre = sum_pre + vji * phi;
+    }
+    float g_ij = sum_abs, g_ji = sum_ems;
+    if (precond) {
+      const double nsi = nstar[(size_t)c + (size_t)ncell * li];
+      g_ij = (float)((double)g_ij - (double)sum_pre * nsi * b[(size_t)c + (size_t)ncell * lj]);
+      g_ji = (float)((double)g_ji - (double)sum_pre * nsi * b[(size_t)c + (size_t)ncell * li]);
+    }
+    const size_t kg = (size_t)c + (size_t)ncell * (W.nline + j);
+    gamma_ij[kg] = gamma_ij[kg] + g_ij;
+    gamma_ji[kg] = gamma_ji[kg] + g_ji;
+  }
+}
+
+// integrate_rates: the window's sums into the atom's rates by transition index
+__global__ void k_integrate_rates(NlWinDev W, int ncell, const float *__restrict__ gw_ij,
+                                  const float *__restrict__ gw_ji, float *__restrict__ g_ij,
+                                  float *__restrict__ g_ji) {
+  const int ntr = W.nline + W.ncont;
+  const size_t n = (size_t)ncell * ntr;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+    const int c = (int)(k % ncell), i = (int)(k / ncell);
+    const int t = i < W.nline ? W.lntrans[i] : W.cntrans[i - W.nline];
+    const size_t ka = (size_t)c + (size_t)ncell * t;
+    g_ij[ka] = g_ij[ka] + gw_ij[k];
+    g_ji[ka] = g_ji[ka] + gw_ji[k];
+  }
+}
+
+struct NlNormArgs {
+  int nline, nrad, first_iter;
+  const int *ti, *tj;
+  const unsigned char *active, *has_wphi;
+};
+
+__global__ void k_normalize_profiles(NlNormArgs A, int ncell, const double *__restrict__ nstar,
+                                     float *__restrict__ wphi, float *__restrict__ gamma_ij,
+                                     float *__restrict__ gamma_ji) {
+  const size_t n = (size_t)ncell * A.nrad;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+    const int c = (int)(k % ncell), i = (int)(k / ncell);
+    if (A.active && !A.active[i]) continue;
+    if (i < A.nline) {
+      if (!A.has_wphi[i]) continue;
+      float w = wphi[k];
+      if (A.first_iter) {
+        w = w > 0.0f ? 1.0f / w : 1.0f;
+        wphi[k] = w;
+      }
+      gamma_ij[k] = gamma_ij[k] * w;
+      gamma_ji[k] = gamma_ji[k] * w;
+    } else {
+      gamma_ji[k] = (float)((double)gamma_ji[k] *
+                            (nstar[(size_t)c + (size_t)ncell * A.ti[i]] / nstar[(size_t)c + (size_t)ncell * A.tj[i]]));
+    }
+  }
+}
+
+// the average of two hemispheres' J (and PsiJ), stored in both
+__global__ void k_combine_twins(size_t n, float *__restrict__ a, float *__restrict__ b) {
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+    const float v = 0.5f * (a[k] + b[k]);
+    a[k] = v;
+    b[k] = v;
+  }
+}
+
+}  // namespace m3d

@@ -416,3 +416,89 @@ def se_config(kind: str = "small", seed: int | None = None, ncell: int | None = 
         idx = np.arange(ncell) % temp.size
         temp, ne, nH, W = temp[idx], ne[idx], nH[idx], W[idx]
     return atom, se_inputs(atom, temp, ne, nH, seed=seed, dilution=None if lte else W)
+
+
+def _set_weights(x):
+    """set_weights (HOP/spectrum_mod.f90:491-513): trapezoid weights, positive."""
+    x = np.asarray(x, np.float64)
+    w = np.empty_like(x)
+    if x.size == 1:
+        return np.ones(1)
+    w[0] = 0.5 * (x[1] - x[0])
+    w[1:-1] = 0.5 * (x[2:] - x[:-2])
+    w[-1] = 0.5 * (x[-1] - x[-2])
+    return np.abs(w)
+
+
+def atom_window(atom: dict, nper: int = 25, seed: int = 2, qmax_doppler: float = 5.0, idf_ref: float = 1.8e5,
+                adamp=(1e-3, 1e-1), sums=None) -> dict:
+    """The atom's transitions on one frequency window holding every transition:
+    nper points per line on q = 1 - lam/lam0 in +-qmax_doppler/idf_ref, nper
+    points per continuum from 0.3 of its edge wavelength to the edge, merged
+    into one grid ascending in wavelength.  A transition's window is every grid
+    point inside its own range (the reference's get_interval), with q, the rate
+    weights wnu (set_weights in nu, / nu for a line, / (h/4pi nu) for a
+    continuum) and the profile weights wq over all of them.  Lines: Einstein
+    coefficients of init_einstein_coefficients (bbtrans_mod.f90:55-67) from the
+    atom's f values, damping a log-uniform in adamp (grad = a/idf_ref), no van der
+    Waals or Stark terms; continua: Kramers-shaped alpha0 (lam/lam_edge)^3.
+    sums: per line sums_over_windows (default none)."""
+    rng = np.random.default_rng(seed + 5000)
+    nline = atom["nline"]
+    ti, tj, ev, g = atom["ti"], atom["tj"], atom["ev"], atom["g"]
+    nrad = len(ti)
+    lam_pts = []
+    q0 = np.linspace(-qmax_doppler / idf_ref, qmax_doppler / idf_ref, nper)
+    lam0 = np.array([HH * CC / ((ev[tj[k]] - ev[ti[k]]) * EE) * 1e8 for k in range(nrad)])
+    for k in range(nrad):
+        if k < nline:
+            lam_pts.append(lam0[k] * (1.0 - q0))
+        else:
+            lam_pts.append(np.geomspace(0.3 * lam0[k], lam0[k] * (1.0 - 1e-7), nper))
+    grid = np.unique(np.concatenate(lam_pts))
+    nu = HZ_TO_AA / grid
+    nf = grid.size
+    li, lj, lb, lr, lo, q, wnu, wq = [], [], [], [], [], [], [], []
+    ci, cj, cb, cr, co, alpha, cwnu = [], [], [], [], [], [], []
+    off_l = off_c = 0
+    f_osc = atom.get("line_f", np.full(nline, 0.1))
+    Aij = np.empty(nline)
+    Bij = np.empty(nline)
+    for k in range(nrad):
+        lo_lam, hi_lam = lam_pts[k].min(), lam_pts[k].max()
+        blue = int(np.searchsorted(grid, lo_lam, "left"))
+        red = int(np.searchsorted(grid, hi_lam, "right")) - 1
+        sl = slice(blue, red + 1)
+        if k < nline:
+            nu0 = CC / (lam0[k] * 1e-8)
+            Aij[k] = F_CONV * f_osc[k] * nu0**2
+            Bij[k] = C2_2H / nu0**3 * (Aij[k] * H_4PI)
+            qq = (1.0 - grid[sl] / lam0[k]).astype(np.float32)
+            li.append(ti[k]); lj.append(tj[k]); lb.append(blue); lr.append(red); lo.append(off_l)
+            q.append(qq)
+            wnu.append(_set_weights(nu[sl]) / nu[sl])
+            wq.append(_set_weights(qq.astype(np.float64)))
+            off_l += red - blue + 1
+        else:
+            a0 = 7.91e-18 * math.sqrt(RYDV / (ev[tj[k]] - ev[ti[k]]))
+            ci.append(ti[k]); cj.append(tj[k]); cb.append(blue); cr.append(red); co.append(off_c)
+            alpha.append((a0 * (grid[sl] / lam0[k]) ** 3).astype(np.float32))
+            cwnu.append(_set_weights(nu[sl]) / (H_4PI * nu[sl]))
+            off_c += red - blue + 1
+    a = 10.0 ** rng.uniform(math.log10(adamp[0]), math.log10(adamp[1]), nline)
+    sums = np.zeros(nline, np.uint8) if sums is None else np.asarray(sums, np.uint8)
+    i32 = lambda v: np.asarray(v, np.int32)
+    return {"nf": nf, "lam": grid, "nu": nu, "nline": nline, "ncont": nrad - nline, "nlevel": atom["nlevel"],
+            "line_i": i32(li), "line_j": i32(lj), "line_ntrans": i32(np.arange(nline)),
+            "line_index": i32(np.arange(nline) + 1), "line_blue": i32(lb), "line_red": i32(lr), "line_off": i32(lo),
+            "q": np.concatenate(q).astype(np.float32), "wnu": np.concatenate(wnu), "wq": np.concatenate(wq),
+            "Bij": Bij, "Aij": Aij, "lower_ev": np.asarray(ev[ti[:nline]], np.float64),
+            "line_active": None, "sums_over_windows": sums,
+            "grad": a / idf_ref, "gw1": np.zeros(nline), "gw2": np.zeros(nline), "gstk": np.zeros(nline),
+            "unsold": np.zeros(nline, np.uint8),
+            "cont_i": i32(ci), "cont_j": i32(cj), "cont_ntrans": i32(np.arange(nline, nrad)),
+            "cont_blue": i32(cb), "cont_red": i32(cr), "cont_off": i32(co),
+            "alpha": np.concatenate(alpha).astype(np.float32) if alpha else np.zeros(0, np.float32),
+            "cwnu": np.concatenate(cwnu) if cwnu else np.zeros(0),
+            "cont_active": None, "g": np.asarray(g, np.float64), "ev": np.asarray(ev, np.float64), "cut_x": 70.0,
+            "twohnu3_c2": (2.0 * HH * nu**3 / CC**2).astype(np.float32)}

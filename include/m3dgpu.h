@@ -318,6 +318,115 @@ int m3d_ng_extrapolate(int ncell, int nlevel, double *b, const double *oldb, con
                        const double *totn, double a, double bc, double max_change, int *applied,
                        double *emax, long long *epos_cell, int *epos_level, unsigned flags);
 
+/* ---- model-atom opacities and ALI rate integrals of one frequency window ----
+ * The transitions of the atom in the window (atom_trans_t, hydrogen lines
+ * excluded), 0-based.  A line's points f = blue..red of the window (0-based, within
+ * 0..nf-1) sit at q[off + f - blue] (likewise wnu, wq); a continuum's at
+ * alpha[off + f - blue].  Kinds follow the reference's declarations
+ * (trans_mod.f90:20-80, bbtrans_mod.f90:15-25): q and alpha real(4), the rest real(8).
+ * The window tables are host memory whatever the flags. */
+typedef struct m3d_atom_window {
+  int nf, nline, ncont, nlevel;
+  const int *line_i, *line_j;       /* (nline) levels */
+  const int *line_ntrans;           /* (nline) transition index in the atom: gamma, wphi, psi flag bit */
+  const int *line_index;            /* (nline) contribution index of the split tracking, >= 1 */
+  const int *line_blue, *line_red, *line_off;
+  const float *q;                   /* per line point: 1 - lam/lam0 [Doppler units of idf] */
+  const double *wnu, *wq;           /* per line point: rate and profile quadrature weights */
+  const double *Bij, *Aij, *lower_ev;       /* (nline) */
+  const unsigned char *line_active;         /* (nline) or NULL */
+  const unsigned char *sums_over_windows;   /* (nline) */
+  const double *grad, *gw1, *gw2, *gstk;    /* (nline) damping constants */
+  const unsigned char *unsold;              /* (nline) */
+  const int *cont_i, *cont_j, *cont_ntrans, *cont_blue, *cont_red, *cont_off;
+  const float *alpha;               /* per continuum point [cm^2] */
+  const double *cwnu;               /* per continuum point */
+  const unsigned char *cont_active; /* (ncont) or NULL */
+  const double *g, *ev;             /* (nlevel) */
+  double cut_x;                     /* 70 */
+} m3d_atom_window_t;
+
+/* bound_bound_damping (rt_patch_mod.f90:2649-2681): adamp (ncell, nline) */
+int m3d_bb_damping(const m3d_atom_window_t *w, int ncell, const float *ne, const float *tothi,
+                   const float *vbar2, const float *stark_pe, const float *unsold, const float *inv_df,
+                   float *adamp, unsigned flags);
+
+/* add_bound_free_opacities (rt_patch_mod.f90:2581-2643): xhat, ehat (nf, ncell) += ;
+ * b (ncell, nlevel) NULL for b = 1; nstar (ncell, nlevel) and pop_ratio, e_kT (ncell)
+ * float64 */
+int m3d_bf_opacity(const m3d_atom_window_t *w, int ncell, const double *b, const double *nstar,
+                   const double *pop_ratio, const double *e_kT, float *xhat, float *ehat,
+                   unsigned flags);
+
+/* add_bound_bound_opacities for one direction (rt_patch_mod.f90:2689-2831) into
+ * work(:, :, 1:2) = (xhat, ehat), (nf, ncell) each.  With split arrays (all six
+ * non-NULL, (nf, ncell)) the tracking starts from (ehat, xhat) as foreground does
+ * (:1474-1487) and takes every line's contribution through add_largest.  wphi
+ * (ncell, nline of the atom, indexed by line_ntrans) or NULL: the direction's profile
+ * integral times wmu is added for the lines that sum over windows (iteration 0). */
+int m3d_bb_opacity(const m3d_atom_window_t *w, int ncell, const double *b, const double *nstar,
+                   const double *pop_ratio, const double *e_kT, const float *inv_df,
+                   const float *vproj, const float *adamp, int lte, float wmu, float *xhat,
+                   float *ehat, float *split_opac_L, float *split_opac_R, int *split_id,
+                   float *split_chi_L, float *split_chi_R, int *split_chi_id, float *wphi,
+                   unsigned flags);
+
+/* work_to_transfer_units with split rates (rt_patch_mod.f90:3591-3604, 3614-3632):
+ * scat = chi_scat*dJnu (nf, ncell) or NULL */
+int m3d_work_to_transfer_units_split(int nf, int ncell, float *w1, float *w2, const float *beta,
+                                     const float *split_opac_L, const float *split_opac_R,
+                                     const float *scat, double maser_chi_floor, int suppress_masers,
+                                     int *n_floored, unsigned flags);
+
+/* bound_bound_rates for one direction (rt_patch_mod.f90:2852-3142); gamma_ij/ji
+ * (ncell, nline + ncont) of the window, accumulated.  work1 = chi after
+ * work_to_transfer_units; inu = work(:,:,3); psi, irem, escape from the formal solver
+ * (M3D_GET_PSI, M3D_SPLIT_RATES); the split arrays of m3d_bb_opacity.  psi_flags
+ * (ncell, nwords) uint32, bit ntrans%32 of word ntrans/32: flags_in the pairs in
+ * force, flags_raise receives the raised ones (atom_data_t psi_flags(:,:,:,:,1:2)). */
+typedef struct m3d_rate_opts {
+  int split_rates;    /* rate_formulation = 'largest' */
+  int preconditioning;
+  int per_direction;  /* .not. (do_full_sp .and. fixed_Jnu > 0) */
+  int use_flags;
+  int do_scat;        /* line scattering: scat given */
+  int nwords;
+  float wmu, wtot;    /* the direction's weight and the sum of all directions' weights */
+} m3d_rate_opts_t;
+
+int m3d_bb_rates(const m3d_atom_window_t *w, const m3d_rate_opts_t *o, int ncell, const double *b,
+                 const double *nstar, const double *pop_ratio, const double *e_kT,
+                 const float *inv_df, const float *vproj, const float *adamp, const float *work1,
+                 const float *inu, const float *psi, const float *irem, const float *escape,
+                 const float *beta, const float *Bnu, const float *split_opac_L,
+                 const float *split_opac_R, const int *split_id, const float *split_chi_L,
+                 const float *split_chi_R, const int *split_chi_id, const float *scat,
+                 const unsigned *flags_in, unsigned *flags_raise, float *gamma_ij, float *gamma_ji,
+                 unsigned flags);
+
+/* bound_free_rates (rt_patch_mod.f90:3193-3259) from the angle-integrated Jnu and
+ * PsiJ (nf, ncell); twohnu3_c2 (nf) */
+int m3d_bf_rates(const m3d_atom_window_t *w, int ncell, int preconditioning, const double *b,
+                 const double *nstar, const double *e_kT, const float *twohnu3_c2, const float *Jnu,
+                 const float *PsiJ, const float *beta, float *gamma_ij, float *gamma_ji,
+                 unsigned flags);
+
+/* integrate_rates (rt_patch_mod.f90:3437-3465): the window's (ncell, nline + ncont)
+ * sums into the atom's (ncell, nrad) rates by transition index */
+int m3d_integrate_rates(const m3d_atom_window_t *w, int ncell, const float *gw_ij, const float *gw_ji,
+                        float *gamma_ij, float *gamma_ji, unsigned flags);
+
+/* normalize_profiles (atom_mod.f90:377-430) on the atom's rates (ncell, nrad): in the
+ * first iteration wphi -> 1/wphi (1 where wphi = 0); lines with has_wphi scale by
+ * wphi; continua scale gamma_ji by n*_i/n*_j.  ti, tj, active, has_wphi host memory. */
+int m3d_normalize_profiles(int ncell, int nline, int nrad, const int *ti, const int *tj,
+                           const unsigned char *active, const unsigned char *has_wphi,
+                           int first_iter, const double *nstar, float *wphi, float *gamma_ij,
+                           float *gamma_ji, unsigned flags);
+
+/* combine_twin_hemispheres' average (rt_patch_mod.f90:1812-1887): a = b = (a + b)/2 over n */
+int m3d_combine_twins(long long n, float *a, float *b, unsigned flags);
+
 #ifdef __cplusplus
 }
 #endif
