@@ -199,7 +199,10 @@ __global__ void __launch_bounds__(256, 3) k_lte_opacity_units_lane(AtmosDev A, G
           lr0 = cont0 > 0.0f ? lt + logf_m3d(cont0) : -FLT_MAX;
         }
         float refl = G.tol * cont0;
-        const float flo = G.flo_scale * pick<NF>(chl, f0 - 1);
+        // chi_l at f0: a line centred outside the window -- nearly all of them --
+        // lands on an edge, read directly instead of through the select chain
+        const float chl0 = f0 == 1 ? chl[0] : (f0 == NF ? chl[NF - 1] : pick<NF>(chl, f0 - 1));
+        const float flo = G.flo_scale * chl0;
         float lref;
         if (flo > refl) { refl = flo; lref = logf_m3d(flo * sqrt_pi); }
         else lref = lr0;
@@ -223,18 +226,37 @@ __global__ void __launch_bounds__(256, 3) k_lte_opacity_units_lane(AtmosDev A, G
         // in |x| (rounded products are monotone), so the nearer window end decides.
         const float xe = x0 + (float)(fb - fa);
         const float xnear = (x0 > 0.0f) ? x0 : ((xe < 0.0f) ? -xe : 0.0f);
+        // A window over the whole frequency range -- most lines -- runs without
+        // per-point predicates, and with fa = 1 the offset (float)f + kfa is (float)f.
+        const bool full = fa == 1 && fb == NF;
         if (fminf((xnear * cf.ih) * 800.0f, 9019.0f) >= 9018.5f) {
           const float2 gw = s_tab[QLG_NTAB - 1];
           const float p1 = fmaf(cf.cZH, gw.y, cf.cL2);
           const float gg = gw.x * cf.gG;
+          if (full) {
 #pragma unroll
-          for (int f = 0; f < NF; f++) {
-            if (f + 1 >= fa && f + 1 <= fb) {
-              const float xs = fabsf(x0 + ((float)f + kfa)) * cf.ih;
+            for (int f = 0; f < NF; f++) {
+              const float xs = fabsf(x0 + (float)f) * cf.ih;
               const float L = __frcp_rn(1.0f + xs * xs);
               const float K = fmaf(L, fmaf(L, p1, cf.bL), gg);
               chl[f] = fmaf(K, 1.0f, chl[f]);
             }
+          } else {
+#pragma unroll
+            for (int f = 0; f < NF; f++) {
+              if (f + 1 >= fa && f + 1 <= fb) {
+                const float xs = fabsf(x0 + ((float)f + kfa)) * cf.ih;
+                const float L = __frcp_rn(1.0f + xs * xs);
+                const float K = fmaf(L, fmaf(L, p1, cf.bL), gg);
+                chl[f] = fmaf(K, 1.0f, chl[f]);
+              }
+            }
+          }
+        } else if (full) {
+#pragma unroll
+          for (int f = 0; f < NF; f++) {
+            const float K = qlg_eval(s_tab, cf, x0 + (float)f);
+            chl[f] = fmaf(K, 1.0f, chl[f]);
           }
         } else {
 #pragma unroll
