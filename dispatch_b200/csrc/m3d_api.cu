@@ -18,6 +18,7 @@
 #include "m3d_pipeline.cuh"
 #include "m3d_stateq.cuh"
 #include "m3d_nlte.cuh"
+#include "m3d_aux.cuh"
 
 using namespace m3d;
 
@@ -1077,6 +1078,7 @@ int m3d_lte_synthesis(const m3d_atmos_t *atm, int nf, const double *nu, const do
 
 #include "m3d_stateq_api.inc"
 #include "m3d_nlte_api.inc"
+#include "m3d_aux_api.inc"
 
 // ===========================================================================
 // rotate_array without any allocation.

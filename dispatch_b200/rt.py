@@ -258,3 +258,50 @@ def lte_synthesis(atm: dict, nu, llam, vec, wmu, fp64=False, return_itop=False, 
                                   ptr(itop), ptr(ie), ptr(flux), C.c_uint(flags)), "m3d_lte_synthesis")
     del keep
     return ie, flux, itop
+
+
+def eta_spread(vecs, ds, dz_upstream=None, one_dimensional=False) -> tuple[int, int]:
+    """eta_rx, eta_ry of update_eta_mask (rt_patch_mod.f90:3683-3700): the horizontal
+    reach of an upwind point over the slab's directions, plus the cell beyond it."""
+    if one_dimensional:
+        return 0, 0
+    dz = ds[2] if dz_upstream is None else max(ds[2], dz_upstream)
+    sx = max(abs(v[0] / v[2]) for v in vecs)
+    sy = max(abs(v[1] / v[2]) for v in vecs)
+    return int(np.floor(sx * dz / ds[0])) + 1, int(np.floor(sy * dz / ds[1])) + 1
+
+
+def update_eta_mask(slab, work, beta, eta_src, eta_mask, rx, ry, eta_gsrc=None):
+    """update_eta_mask with dense flags (uint8), in place; eta_gsrc given = test the ghost plane."""
+    init()
+    ghost = eta_gsrc is not None
+    check(lib().m3d_update_eta_mask(C.byref(slab), ptr(work), ptr(beta), ptr(eta_src), ptr(eta_gsrc), ptr(eta_mask),
+                                    C.c_int(rx), C.c_int(ry), C.c_int(int(ghost)),
+                                    C.c_uint(_flags([work, beta, eta_src]) & DEVICE_PTRS)), "m3d_update_eta_mask")
+
+
+def lte_populations(atom: dict, temp, lsaha, totn, dxi=None):
+    """compute_lte_populations (level partition function): returns nstar (nlevel, ncell); totn updated in place."""
+    init()
+    from .stateq import make_atom
+    st, keep = make_atom(atom)
+    temp, lsaha = np.ascontiguousarray(temp, _F32), np.ascontiguousarray(lsaha, _F32)
+    dxi = None if dxi is None else np.ascontiguousarray(dxi, _F32)
+    if totn.dtype != np.float64 or not totn.flags.c_contiguous:
+        raise ValueError("totn must be a C-contiguous float64 array (updated in place)")
+    nstar = np.zeros((st.nlevel, temp.size), np.float64)
+    check(lib().m3d_lte_populations(C.byref(st), C.c_int(temp.size), ptr(temp), ptr(lsaha), ptr(dxi), ptr(nstar),
+                                    ptr(totn), C.c_uint(0)), "m3d_lte_populations")
+    return nstar
+
+
+def particle_fields(awgt, vmic, iso_frac, temp, n, part, population_scale=0.0):
+    """inverse_doppler_factor, compute_vbar2 and lnbase of one isotope: (inv_df, vbar2, lnbase)."""
+    init()
+    temp = np.ascontiguousarray(temp, _F32)
+    n, part = np.ascontiguousarray(n, np.float64), np.ascontiguousarray(part, np.float64)
+    idf, vb, lb = (np.zeros(temp.size, _F32) for _ in range(3))
+    check(lib().m3d_particle_fields(C.c_int(temp.size), C.c_double(awgt), C.c_float(vmic), C.c_double(iso_frac),
+                                    C.c_double(population_scale), ptr(temp), ptr(n), ptr(part), ptr(idf), ptr(vb),
+                                    ptr(lb), C.c_uint(0)), "m3d_particle_fields")
+    return idf, vb, lb

@@ -427,6 +427,33 @@ int m3d_normalize_profiles(int ncell, int nline, int nrad, const int *ti, const 
 /* combine_twin_hemispheres' average (rt_patch_mod.f90:1812-1887): a = b = (a + b)/2 over n */
 int m3d_combine_twins(long long n, float *a, float *b, unsigned flags);
 
+/* ---- inputs and bookkeeping around the solvers ----
+ * update_eta_mask (rt_patch_mod.f90:3671-3807) for one slab and set, with the flags
+ * kept dense: eta_src and eta_mask (nf, nx, ny, nz), eta_gsrc (nf, nx, ny) of the
+ * upstream ghost plane, one byte per point.  work (nf, nx, ny, 0:nz+1, 3) holds
+ * (chi, Snu) after work_to_transfer_units and the boundary; beta (nf, nx, ny, nz).
+ * rx, ry: the spread eta_rx, eta_ry (floor(max|vx/vz| dz/dx) + 1, 0 for columns);
+ * ghost: test the ghost plane (the slab is not at the top of the domain).  The
+ * solvers take the dense mask as eta_row(cell) = cell + 1 with eta_mask. */
+int m3d_update_eta_mask(const m3d_slab_t *slab, const float *work, const float *beta, unsigned char *eta_src,
+                        unsigned char *eta_gsrc, unsigned char *eta_mask, int rx, int ry, int ghost,
+                        unsigned flags);
+
+/* compute_lte_populations with the atom's own levels as partition function
+ * (level_partf, atom_mod.f90:1041-1140) and lte_pop (:1132-1150): nstar (ncell, nlevel)
+ * out, totn (ncell) in (the species' atoms) and out (the sum of nstar).  temp, lsaha =
+ * ln(2 (2 pi m_e kT/h^2)^1.5 / ne) and dxi (may be NULL) are float32. */
+int m3d_lte_populations(const m3d_atom_t *atom, int ncell, const float *temp, const float *lsaha, const float *dxi,
+                        double *nstar, double *totn, unsigned flags);
+
+/* add_particle_opacity's per-cell fields of one isotope (linelist_mod.f90:1023-1042,
+ * ion_mod.f90:198-221): inv_df, vbar2 and lnbase = ln max(n, tiny) [+ ln scale] - part
+ * + ln inv_df + ln iso_frac; n and part (the log partition function) float64.
+ * population_scale 0 = none. */
+int m3d_particle_fields(int ncell, double awgt, float vmic, double iso_frac, double population_scale,
+                        const float *temp, const double *n, const double *part, float *inv_df, float *vbar2,
+                        float *lnbase, unsigned flags);
+
 #ifdef __cplusplus
 }
 #endif
