@@ -231,7 +231,9 @@ def run_b200(a):
 
     m.init(local)
     stream = torch.cuda.current_stream()
-    m.set_stream(stream.cuda_stream)
+    # the library's work on the stream the timing events are recorded on (torch's
+    # default stream is the legacy one, named by cudaStreamLegacy = 0x1)
+    m.set_stream(stream.cuda_stream or 1)
     nf = a.nf
     atm, llam_all, nu_all, vec, wmu = _make_inputs(nf, a.cube)
     ncell = atm["nx"] * atm["ny"] * atm["nz"]

@@ -58,7 +58,8 @@ class LineList(C.Structure):
     _fields_ = [("nline", C.c_int), ("llam0", C.c_void_p), ("lower_ev", C.c_void_p),
                 ("gpref", C.c_void_p), ("grad", C.c_void_p), ("gw1", C.c_void_p),
                 ("gw2", C.c_void_p), ("gstk", C.c_void_p), ("unsold", C.c_void_p),
-                ("lev_i", C.c_void_p), ("lev_j", C.c_void_p), ("active", C.c_void_p)]
+                ("lev_i", C.c_void_p), ("lev_j", C.c_void_p), ("active", C.c_void_p),
+                ("reach_in", C.c_void_p)]
 
 
 class Species(C.Structure):
@@ -135,8 +136,30 @@ def synchronize() -> None:
     check(lib().m3d_synchronize(), "m3d_synchronize")
 
 
+_lib_stream = 0
+
+
 def set_stream(stream_ptr: int | None) -> None:
+    """Order the library's work on this CUDA stream (None: its own stream)."""
+    global _lib_stream
     check(lib().m3d_set_stream(C.c_void_p(stream_ptr or 0)), "m3d_set_stream")
+    _lib_stream = stream_ptr or 0
+
+
+def order_after_torch(*arrays) -> None:
+    """Device pointers are read and written on the library stream: when torch
+    tensors come in, the library moves onto torch's current stream, so that the
+    tensors' pending writes come first and torch's later reads see the results."""
+    for a in arrays:
+        if a is not None and not isinstance(a, np.ndarray) and hasattr(a, "is_cuda") and a.is_cuda:
+            import torch
+            cur = torch.cuda.current_stream().cuda_stream
+            # torch's default stream is the legacy one (handle 0), which the
+            # library names by cudaStreamLegacy (0x1); 0 would select its own
+            cur = cur if cur != 0 else 1
+            if cur != _lib_stream:
+                set_stream(cur)
+            return
 
 
 def ptr(a) -> C.c_void_p | None:

@@ -351,6 +351,9 @@ LineArgs line_args(const m3d_linelist_t *ll) {
   L.unsold = ll->unsold;
   L.lev_i = ll->lev_i; L.lev_j = ll->lev_j;
   L.active = ll->active;
+  L.reach_in = ll->reach_in;
+  L.sel = nullptr;
+  L.nsel = nullptr;
   return L;
 }
 
@@ -369,6 +372,7 @@ int stage_linelist(Staging &st, const m3d_linelist_t *ll, LineArgs *L) {
   TRY(st.in(ll->lev_i, n, &L->lev_i));
   TRY(st.in(ll->lev_j, n, &L->lev_j));
   TRY(st.in(ll->active, n, &L->active));
+  TRY(st.in(ll->reach_in, n, &L->reach_in));
   if (!L->llam0 || !L->lower_ev || !L->gpref || !L->grad || !L->gw1 || !L->gw2 || !L->gstk || !L->unsold)
     return fail(M3D_EINVAL, "line list with a NULL array");
   return M3D_OK;
@@ -587,6 +591,18 @@ int m3d_line_opacity(const m3d_linelist_t *ll, int nf, const double *llam, int n
   if (!attr) {
     CUDA_TRY(cudaFuncSetAttribute(k_line_opacity, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     attr = true;
+  }
+  if (L.reach_in) {
+    // select_lines: max |vproj| over the cells, then the kept lines
+    void *sp = nullptr;
+    TRY(scratch(20, sizeof(int) * ((size_t)ll->nline + 8), &sp));
+    unsigned *vmax = (unsigned *)sp;
+    int *dnsel = (int *)sp + 1, *dsel = (int *)sp + 4;
+    CUDA_TRY(cudaMemsetAsync(vmax, 0, sizeof(unsigned), g_ctx.stream));
+    LAUNCH(k_absmax, grid_for(ncell), 256, 0, ncell, dvp, vmax);
+    LAUNCH(k_select_lines, 1, 32, 0, L, dllam, nf, (const unsigned *)vmax, dsel, dnsel);
+    L.sel = dsel;
+    L.nsel = dnsel;
   }
   int grid = (ncell + warps - 1) / warps;
   if (grid > 148 * 8) grid = 148 * 8;
@@ -900,11 +916,34 @@ int m3d_lte_synthesis(const m3d_atmos_t *atm, int nf, const double *nu, const do
   A.maser_chi_floor = (float)atm->maser_chi_floor;
   A.nspecies = atm->nspecies;
   std::vector<SpeciesDev> sp(atm->nspecies > 0 ? atm->nspecies : 1);
+  bool reach = false;
+  size_t nsel_all = 0;
   for (int k = 0; k < atm->nspecies; k++) {
     TRY(stage_linelist(st, &atm->species[k].ll, &sp[k].L));
     TRY(st.in(atm->species[k].inv_df, ncell, &sp[k].inv_df));
     TRY(st.in(atm->species[k].vbar2, ncell, &sp[k].vbar2));
     TRY(st.in(atm->species[k].lnbase, ncell, &sp[k].lnbase));
+    if (sp[k].L.reach_in) reach = true;
+    nsel_all += (size_t)sp[k].L.nline + 8;
+  }
+  if (reach && fp64) return fail(M3D_EUNSUPPORTED, "m3d_lte_synthesis: reach_in with the FP64 path");
+  // select_lines per ray: a vmax word, then per species its count and its list
+  unsigned *d_vmax = nullptr;
+  std::vector<int *> d_sel(sp.size(), nullptr), d_nsel(sp.size(), nullptr);
+  if (reach) {
+    for (int k = 0; k < atm->nspecies; k++)
+      if (!sp[k].L.reach_in) return fail(M3D_EINVAL, "m3d_lte_synthesis: reach_in given for some species only");
+    void *sbuf = nullptr;
+    TRY(scratch(21, sizeof(int) * (nsel_all + 8), &sbuf));
+    d_vmax = (unsigned *)sbuf;
+    int *p = (int *)sbuf + 8;
+    for (int k = 0; k < atm->nspecies; k++) {
+      d_nsel[k] = p;
+      d_sel[k] = p + 8;
+      p += sp[k].L.nline + 8;
+      sp[k].L.sel = d_sel[k];
+      sp[k].L.nsel = d_nsel[k];
+    }
   }
   void *dsp;
   TRY(scratch(4, sizeof(SpeciesDev) * sp.size(), &dsp));
@@ -969,10 +1008,13 @@ int m3d_lte_synthesis(const m3d_atmos_t *atm, int nf, const double *nu, const do
     static size_t attr[4] = {0, 0, 0, 0};
     const int which = (lane32 ? 2 : 0) + (fp64 ? 1 : 0);
     if (attr[which] < smem_op) {
-      const void *fn = lane32 ? (fp64 ? (const void *)k_lte_opacity_units_lane<32, double>
-                                      : (const void *)k_lte_opacity_units_lane<32, float>)
+      const void *fn = lane32 ? (fp64 ? (const void *)k_lte_opacity_units_lane<32, double, false>
+                                      : (const void *)k_lte_opacity_units_lane<32, float, false>)
                               : (fp64 ? (const void *)k_lte_opacity_units<double> : (const void *)k_lte_opacity_units<float>);
       CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_op));
+      if (lane32 && !fp64)
+        CUDA_TRY(cudaFuncSetAttribute((const void *)k_lte_opacity_units_lane<32, float, true>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_op));
       attr[which] = smem_op;
     }
   }
@@ -1001,9 +1043,18 @@ int m3d_lte_synthesis(const m3d_atmos_t *atm, int nf, const double *nu, const do
   for (int r = 0; r < nray; r++) {
     const double *v = vec + 3 * r;
     if (!fp64) {
-      if (lane32)
-        LAUNCH_S(M3D_STAGE_OPACITY, (k_lte_opacity_units_lane<32, float>), lgrid, block, smem_op, A, G, dnu, v[0], v[1],
-                 v[2], (float *)dchi, (float *)dS, g_ctx.d_tab);
+      if (reach) {
+        CUDA_TRY(cudaMemsetAsync(d_vmax, 0, sizeof(unsigned), g_ctx.stream));
+        LAUNCH(k_vproj_absmax, grid_for(ncell), 256, 0, A, v[0], v[1], v[2], d_vmax);
+        for (int k = 0; k < atm->nspecies; k++)
+          LAUNCH(k_select_lines, 1, 32, 0, sp[k].L, dllam, nf, (const unsigned *)d_vmax, d_sel[k], d_nsel[k]);
+      }
+      if (reach && lane32)
+        LAUNCH_S(M3D_STAGE_OPACITY, (k_lte_opacity_units_lane<32, float, true>), lgrid, block, smem_op, A, G, dnu, v[0],
+                 v[1], v[2], (float *)dchi, (float *)dS, g_ctx.d_tab);
+      else if (lane32)
+        LAUNCH_S(M3D_STAGE_OPACITY, (k_lte_opacity_units_lane<32, float, false>), lgrid, block, smem_op, A, G, dnu, v[0],
+                 v[1], v[2], (float *)dchi, (float *)dS, g_ctx.d_tab);
       else
         LAUNCH_S(M3D_STAGE_OPACITY, k_lte_opacity_units<float>, ogrid, block, smem_op, A, G, dnu, v[0], v[1], v[2],
                  (float *)dchi, (float *)dS, g_ctx.d_tab);
@@ -1016,8 +1067,8 @@ int m3d_lte_synthesis(const m3d_atmos_t *atm, int nf, const double *nu, const do
                die + (size_t)nf * r);
     } else {
       if (lane32)
-        LAUNCH_S(M3D_STAGE_OPACITY, (k_lte_opacity_units_lane<32, double>), lgrid, block, smem_op, A, G, dnu, v[0], v[1],
-                 v[2], (double *)dchi, (double *)dS, g_ctx.d_tab);
+        LAUNCH_S(M3D_STAGE_OPACITY, (k_lte_opacity_units_lane<32, double, false>), lgrid, block, smem_op, A, G, dnu,
+                 v[0], v[1], v[2], (double *)dchi, (double *)dS, g_ctx.d_tab);
       else
         LAUNCH_S(M3D_STAGE_OPACITY, k_lte_opacity_units<double>, ogrid, block, smem_op, A, G, dnu, v[0], v[1], v[2],
                  (double *)dchi, (double *)dS, g_ctx.d_tab);

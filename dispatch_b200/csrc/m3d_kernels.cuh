@@ -83,6 +83,10 @@ struct LineArgs {
   const uint8_t *unsold;
   const int *lev_i, *lev_j;
   const uint8_t *active;
+  // has_reach: the per-line reach of a previous run, and the lines select_lines
+  // kept for this call (0-based, ascending; *nsel of them); null without reach
+  const float *reach_in;
+  const int *sel, *nsel;
 };
 
 struct GridArgs {
@@ -126,17 +130,23 @@ __device__ void warp_cell_lines(const LineArgs &L, const GridArgs &G, const Cell
   const QlgCell qw = qlg_cell(G.sdl / c.idf);
   const float lvb2 = logf_m3d(c.vbar2);
   const float unsold_c = exp4(0.3f * lvb2) * c.tothi;
-  for (int l0 = 0; l0 < L.nline; l0 += 32) {
-    const int l = l0 + lane;
+  const int nline = L.sel ? *L.nsel : L.nline;
+  const double lam_lo = G.llam[0], lam_hi = G.llam[nf - 1];
+  for (int l0 = 0; l0 < nline; l0 += 32) {
+    const int l = l0 + lane < nline ? (L.sel ? L.sel[l0 + lane] : l0 + lane) : -1;
     bool cand = false;
-    if (l < L.nline && (L.active == nullptr || L.active[l])) {
+    if (l >= 0 && (L.active == nullptr || L.active[l])) {
       const double llc = L.llam0[l] - (double)c.vproj;
       const double pos = (llc - G.llam1) * G.inv_dllam;
       const int ic = (int)lround(pos) + 1;
       const int f0 = ic < 1 ? 1 : (ic > nf ? nf : ic);
       const float ex = L.lower_ev[l] * c.ekt;
       const float arg = (c.base + L.gpref[l]) - ex;
-      if (!(arg < ex_cutoff)) {
+      const bool outside = L.reach_in && (llc < lam_lo || llc > lam_hi);
+      if (!(arg < ex_cutoff) && outside) {
+        // centred beyond the chunk: its exact test is arg > logref at the nearer end
+        cand = arg > logref[f0 - 1] - 1e-3f;
+      } else if (!(arg < ex_cutoff)) {
         const float lr = logref[f0 - 1];
         if (arg > lr - 1e-3f) {
           const float Rij = exp4(arg);
@@ -158,28 +168,37 @@ __device__ void warp_cell_lines(const LineArgs &L, const GridArgs &G, const Cell
     while (m) {
       const int j = __ffs(m) - 1;
       m &= m - 1;
-      const int ln = l0 + j;
+      const int ln = L.sel ? L.sel[l0 + j] : l0 + j;
       const double llc = L.llam0[ln] - (double)c.vproj;
       const double pos = (llc - G.llam1) * G.inv_dllam;
       const int ic = (int)lround(pos) + 1;
       const int f0 = ic < 1 ? 1 : (ic > nf ? nf : ic);
       const float ex = L.lower_ev[ln] * c.ekt;
       const float arg = (c.base + L.gpref[ln]) - ex;
-      float refl = G.tol * cont[f0 - 1];
-      const float flo = G.flo_scale * chi[f0 - 1];
-      float lref;
-      if (flo > refl) { refl = flo; lref = logf_m3d(flo * sqrt_pi); }
-      else lref = logref[f0 - 1];
-      if (arg <= lref) continue;
+      const bool outside = L.reach_in && (llc < lam_lo || llc > lam_hi);
+      float refl, lref, cap = FLT_MAX;
+      if (outside) {
+        // f0 is the nearer chunk end here; no floor, no peak test, window capped by the reach
+        lref = logref[f0 - 1];
+        if (arg <= lref) continue;
+        refl = G.tol * cont[f0 - 1];
+        cap = (float)((double)L.reach_in[ln] * G.inv_dllam);
+      } else {
+        refl = G.tol * cont[f0 - 1];
+        const float flo = G.flo_scale * chi[f0 - 1];
+        if (flo > refl) { refl = flo; lref = logf_m3d(flo * sqrt_pi); }
+        else lref = logref[f0 - 1];
+        if (arg <= lref) continue;
+      }
       const float Rij = exp4(arg);
-      if (voigt_peak * Rij <= refl) continue;
+      if (!outside && voigt_peak * Rij <= refl) continue;
       float bi = 1.0f, bj = 1.0f;
       if (do_nlte && L.lev_i && L.lev_j && L.lev_i[ln] > 0 && L.lev_j[ln] > 0) {
         bi = dep(L.lev_i[ln]);
         bj = dep(L.lev_j[ln]);
       }
       const float a = line_damping_a(L, ln, unsold_c, lvb2, c.tothi, c.ne, c.starkpe) * G.sdl;
-      if (diag && lane == 0) {
+      if (diag && lane == 0 && !outside) {
         const float st = (voigt_peak * Rij) / cont[f0 - 1];
         atomicMax(reinterpret_cast<int *>(strength + ln), __float_as_int(st));
       }
@@ -190,7 +209,7 @@ __device__ void warp_cell_lines(const LineArgs &L, const GridArgs &G, const Cell
       const float x1 = (float)((G.llam[i1 - 1] - llc) * G.inv_dllam);
       const QlgCoef cf = qlg_setup(a, qw.D, qw.SQ, S);
       const float hw = qlg_halfwidth(qw, a, S, refl, lnq);
-      const int noff = (int)lroundf(fminf(fminf(hw, FLT_MAX), (float)(nf + abs(ic))));
+      const int noff = (int)lroundf(fminf(fminf(hw, cap), (float)(nf + abs(ic))));
       const int fa = ic - noff > 1 ? ic - noff : 1;
       const int fb = ic + noff < nf ? ic + noff : nf;
       if (diag && lane == 0) {
@@ -208,6 +227,63 @@ __device__ void warp_cell_lines(const LineArgs &L, const GridArgs &G, const Cell
       __syncwarp();
     }
   }
+}
+
+// max |vproj| over the cells (select_lines' vmax), as the bits of a non-negative
+// float: their unsigned order is the float order, so atomicMax is exact
+__global__ void k_absmax(int n, const float *v, unsigned *out) {
+  unsigned m = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    m = max(m, __float_as_uint(fabsf(v[i])));
+  for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
+
+__device__ __forceinline__ int lower_bound8(const double *a, int n, double x) {
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    const int mid = (lo + hi) / 2;
+    if (a[mid] >= x) hi = mid;
+    else lo = mid + 1;
+  }
+  return lo;
+}
+__device__ __forceinline__ int upper_bound8(const double *a, int n, double x) {
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    const int mid = (lo + hi) / 2;
+    if (a[mid] > x) hi = mid;
+    else lo = mid + 1;
+  }
+  return lo - 1;
+}
+
+// select_lines (linelist_mod.f90:1110-1142) with one warp: the slice by bisection on
+// the centres with the largest reach as margin, then each line against its own
+// reach; the ballot keeps the selected lines in ascending order
+__global__ void k_select_lines(LineArgs L, const double *llam, int nf, const unsigned *vmax_bits, int *sel,
+                               int *nsel) {
+  const int lane = threadIdx.x & 31;
+  float r = 0.0f;
+  for (int l = lane; l < L.nline; l += 32) r = fmaxf(r, L.reach_in[l]);
+  for (int o = 16; o > 0; o >>= 1) r = fmaxf(r, __shfl_xor_sync(0xffffffffu, r, o));
+  const double rmax = (double)r;
+  const double vmax = (double)__uint_as_float(*vmax_bits);
+  const double hb1 = nf > 1 ? 0.5 * (llam[1] - llam[0]) : 0.0;
+  const double hb2 = nf > 1 ? 0.5 * (llam[nf - 1] - llam[nf - 2]) : 0.0;
+  const double blue = llam[0] - hb1 - vmax, red = llam[nf - 1] + hb2 + vmax;
+  const int l0 = max(0, lower_bound8(L.llam0, L.nline, blue - rmax));
+  const int l1 = min(L.nline - 1, upper_bound8(L.llam0, L.nline, red + rmax));
+  int count = 0;
+  for (int b = l0; b <= l1; b += 32) {
+    const int l = b + lane;
+    bool ok = l <= l1 && (L.active == nullptr || L.active[l]);
+    if (ok) ok = !(L.llam0[l] + (double)L.reach_in[l] < blue || L.llam0[l] - (double)L.reach_in[l] > red);
+    const unsigned m = __ballot_sync(0xffffffffu, ok);
+    if (ok) sel[count + __popc(m & ((1u << lane) - 1u))] = l;
+    count += __popc(m);
+  }
+  if (lane == 0) *nsel = count;
 }
 
 __device__ __forceinline__ void stage_tables(float2 *s_tab, const float2 *tab) {

@@ -149,7 +149,10 @@ __device__ __forceinline__ float pick(const float (&a)[NF], int i) {
   return v;
 }
 
-template <int NF, typename TO>
+// REACH: the line list carries reach_in (has_reach): the lines select_lines kept,
+// and lines centred beyond the window take the unfloored reference at the nearer
+// end, no peak test and a window capped by their reach (linelist_mod.f90:844-854, 914-921)
+template <int NF, typename TO, bool REACH>
 __global__ void __launch_bounds__(256, 3) k_lte_opacity_units_lane(AtmosDev A, GridArgs G, const double *nu, double v0,
                                                                    double v1, double v2, TO *chi_out, TO *S_out,
                                                                    const float2 *tab) {
@@ -182,7 +185,9 @@ __global__ void __launch_bounds__(256, 3) k_lte_opacity_units_lane(AtmosDev A, G
       const QlgCell qw = qlg_cell(G.sdl / idf);
       const float lvb2 = logf_m3d(Sd.vbar2[cs]);
       const float unsold_c = exp4(0.3f * lvb2) * tothi;
-      for (int l = 0; l < L.nline; l++) {
+      const int nline = REACH ? *L.nsel : L.nline;
+      for (int s = 0; s < nline; s++) {
+        const int l = REACH ? L.sel[s] : s;
         if (L.active && !L.active[l]) continue;
         const double llc = L.llam0[l] - (double)vproj;
         const double pos = (llc - G.llam1) * G.inv_dllam;
@@ -199,22 +204,29 @@ __global__ void __launch_bounds__(256, 3) k_lte_opacity_units_lane(AtmosDev A, G
           lr0 = cont0 > 0.0f ? lt + logf_m3d(cont0) : -FLT_MAX;
         }
         float refl = G.tol * cont0;
-        // chi_l at f0: a line centred outside the window -- nearly all of them --
-        // lands on an edge, read directly instead of through the select chain
-        const float chl0 = f0 == 1 ? chl[0] : (f0 == NF ? chl[NF - 1] : pick<NF>(chl, f0 - 1));
-        const float flo = G.flo_scale * chl0;
-        float lref;
-        if (flo > refl) { refl = flo; lref = logf_m3d(flo * sqrt_pi); }
-        else lref = lr0;
-        if (arg <= lref) continue;
+        float lref, cap = FLT_MAX;
+        const bool outside = REACH && (llc < G.llam[0] || llc > G.llam[NF - 1]);
+        if (outside) {
+          lref = lr0;
+          if (arg <= lref) continue;
+          cap = (float)((double)L.reach_in[l] * G.inv_dllam);
+        } else {
+          // chi_l at f0: a line centred outside the window -- nearly all of them --
+          // lands on an edge, read directly instead of through the select chain
+          const float chl0 = f0 == 1 ? chl[0] : (f0 == NF ? chl[NF - 1] : pick<NF>(chl, f0 - 1));
+          const float flo = G.flo_scale * chl0;
+          if (flo > refl) { refl = flo; lref = logf_m3d(flo * sqrt_pi); }
+          else lref = lr0;
+          if (arg <= lref) continue;
+        }
         const float Rij = exp4(arg);
-        if (voigt_peak * Rij <= refl) continue;
+        if (!outside && voigt_peak * Rij <= refl) continue;
         const float a = line_damping_a(L, l, unsold_c, lvb2, tothi, ne, starkpe) * G.sdl;
         const float S = Rij * qw.D;
         const float x1 = (float)((G.llam[f0 - 1] - llc) * G.inv_dllam);
         const QlgCoef cf = qlg_setup(a, qw.D, qw.SQ, S);
         const float hw = qlg_halfwidth(qw, a, S, refl, arg - lref);
-        const int noff = (int)lroundf(fminf(fminf(hw, FLT_MAX), (float)(NF + abs(ic))));
+        const int noff = (int)lroundf(fminf(fminf(hw, cap), (float)(NF + abs(ic))));
         const int fa = ic - noff > 1 ? ic - noff : 1;
         const int fb = ic + noff < NF ? ic + noff : NF;
         if (fa > fb) continue;
@@ -296,6 +308,17 @@ __global__ void __launch_bounds__(256, 3) k_lte_opacity_units_lane(AtmosDev A, G
       }
     }
   }
+}
+
+// max |vproj| of one ray over the cells, vproj formed as the opacity kernels form it
+__global__ void k_vproj_absmax(AtmosDev A, double v0, double v1, double v2, unsigned *out) {
+  unsigned m = 0;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < A.ncell; c += gridDim.x * blockDim.x) {
+    const float vp = (float)((v0 * (double)A.vx[c] + v1 * (double)A.vy[c]) + v2 * (double)A.vz[c]);
+    m = max(m, __float_as_uint(fabsf(vp)));
+  }
+  for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, m);
 }
 
 // rotate_array's weights of one plane for the fused sweep, with the periodic

@@ -12,7 +12,7 @@ import ctypes as C
 
 import numpy as np
 
-from . import DEVICE_PTRS, M3DError, check, init, lib, ptr
+from . import DEVICE_PTRS, M3DError, check, init, lib, order_after_torch, ptr
 
 _P = C.c_void_p
 
@@ -68,6 +68,7 @@ def make_window(win: dict) -> tuple[AtomWindow, list]:
 def _flags(*arrays) -> int:
     for a in arrays:
         if a is not None and not isinstance(a, np.ndarray):
+            order_after_torch(a)
             return DEVICE_PTRS
     return 0
 

@@ -11,7 +11,8 @@ import ctypes as C
 
 import numpy as np
 
-from . import (DEVICE_PTRS, FP64, LINE_DIAG, ROTATE, Atmos, LineList, Species, check, init, lib, ptr)
+from . import (DEVICE_PTRS, FP64, LINE_DIAG, ROTATE, Atmos, LineList, Species, check, init, lib, order_after_torch,
+               ptr)
 
 _F32 = np.float32
 
@@ -19,6 +20,7 @@ _F32 = np.float32
 def _is_dev(*arrays) -> bool:
     for a in arrays:
         if a is not None and not isinstance(a, np.ndarray):
+            order_after_torch(a)
             return True
     return False
 
@@ -88,6 +90,7 @@ def make_linelist(ll: dict, keep: list) -> LineList:
     s.lev_i = arr("lev_i", np.int32)
     s.lev_j = arr("lev_j", np.int32)
     s.active = arr("active", np.uint8)
+    s.reach_in = arr("reach_in", _F32)
     return s
 
 

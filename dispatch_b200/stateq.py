@@ -23,7 +23,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from . import DEVICE_PTRS, M3DError, check, init, lib, ptr
+from . import DEVICE_PTRS, M3DError, check, init, lib, order_after_torch, ptr
 
 LINEQ_NO_PIVOT, LINEQ, LU_PARTIAL = 0, 1, 2
 COL_REGEMORTER, COL_SEATON = 1, 2
@@ -101,6 +101,7 @@ def make_atom(atom: dict) -> tuple[Atom, list]:
 def _flags(*arrays) -> int:
     for a in arrays:
         if a is not None and not isinstance(a, np.ndarray):
+            order_after_torch(a)
             return DEVICE_PTRS
     return 0
 

@@ -81,6 +81,8 @@ typedef struct m3d_linelist {
   const unsigned char *unsold;  /* 1: Unsold van der Waals, 0: Barklem */
   const int *lev_i, *lev_j;     /* NLTE level indices, 1-based, 0 = LTE; may be NULL */
   const unsigned char *active;  /* may be NULL: every line active */
+  const float *reach_in;        /* reach of a previous run [log(lambda)] (line_types_mod.f90:48-53),
+                                   or NULL: has_reach = .false. */
 } m3d_linelist_t;
 
 /* ---- context (hop_init / hop_free / hop_last_error counterparts) ---- */
@@ -88,7 +90,8 @@ int m3d_init(int device, unsigned flags);
 int m3d_free(void);
 int m3d_last_error(char *buf, int buflen);
 int m3d_version(int *major, int *minor, int *patch);
-int m3d_set_stream(void *cuda_stream);        /* NULL: the library's own stream */
+int m3d_set_stream(void *cuda_stream);        /* NULL: the library's own (non-blocking) stream;
+                                                 cudaStreamLegacy: the legacy default stream */
 int m3d_synchronize(void);
 /* Number of kernel launches the library has issued since m3d_init. */
 long long m3d_launch_count(void);
@@ -122,7 +125,11 @@ int m3d_qlg_bot_profile(int n, const float *a, const float *q, const float *vpr,
  * chi, eta, cont, logref are (nf, ncell); the per-cell fields are (ncell); dep_mem
  * is (ncell, nlevel).  chi and eta are accumulated in place.  used/strength/reach
  * (nline each) are updated with M3D_LINE_DIAG, else may be NULL.
- * Lines without a per-line reach (has_reach = .false.); no LTE scattering split. */
+ * With reach_in the lines are those select_lines keeps (linelist_mod.f90:1110-1142:
+ * centres within the chunk widened by half a grid step, max |vproj| and each line's
+ * reach), and lines centred beyond the chunk take the unfloored reference at the
+ * nearer end and a window capped by their reach (:844-854, 914-921).  No LTE
+ * scattering split. */
 int m3d_line_opacity(const m3d_linelist_t *ll, int nf, const double *llam, int ncell,
                      float *chi, float *eta, const float *cont, const float *logref,
                      const float *vproj, const float *inv_df, const float *vbar2, const float *e_kT,

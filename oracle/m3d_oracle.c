@@ -416,9 +416,62 @@ int or_qlg_bot_line_sweep(const float *tgx, const float *th2x, float D, float gL
   return line_sweep(tgx, th2x, &w, gL, S, ref, lnq, nf, llam, llc, pos, idl, cap, fa, fb, hw, K);
 }
 
+/* lower_bound8 / upper_bound8 (linelist_mod.f90:1807-1844), 0-based: the first
+ * index with a[i] >= x (n if none), the last index with a[i] <= x (-1 if none) */
+static int lower_bound8(const double *a, int n, double x)
+{
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    const int mid = (lo + hi) / 2;
+    if (a[mid] >= x) hi = mid;
+    else lo = mid + 1;
+  }
+  return lo;
+}
+static int upper_bound8(const double *a, int n, double x)
+{
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    const int mid = (lo + hi) / 2;
+    if (a[mid] > x) hi = mid;
+    else lo = mid + 1;
+  }
+  return lo - 1;
+}
+
+int or_select_lines(const or_linelist_t *ll, int nf, const double *llam, float vmax, int *sel)
+{
+  int l0 = 0, l1 = ll->nline - 1, nsel = 0;
+  double blue = 0, red = 0;
+  if (ll->reach_in) {
+    double hb1 = 0, hb2 = 0, rmax = 0;
+    if (nf > 1) {
+      hb1 = 0.5 * (llam[1] - llam[0]);
+      hb2 = 0.5 * (llam[nf - 1] - llam[nf - 2]);
+    }
+    for (int l = 0; l < ll->nline; l++)
+      if ((double)ll->reach_in[l] > rmax) rmax = ll->reach_in[l];
+    blue = llam[0] - hb1 - (double)vmax;
+    red = llam[nf - 1] + hb2 + (double)vmax;
+    const int a = lower_bound8(ll->llam0, ll->nline, blue - rmax);
+    const int b = upper_bound8(ll->llam0, ll->nline, red + rmax);
+    l0 = a > l0 ? a : l0;
+    l1 = b < l1 ? b : l1;
+  }
+  for (int l = l0; l <= l1; l++) {
+    if (ll->active && !ll->active[l]) continue;
+    if (ll->reach_in && (ll->llam0[l] + (double)ll->reach_in[l] < blue || ll->llam0[l] - (double)ll->reach_in[l] > red))
+      continue;
+    sel[nsel++] = l;
+  }
+  return nsel;
+}
+
 /* =========================================================================
- * add_opacity_equi (HOP/linelist_mod.f90:729-960), without per-line reach
- * (has_reach = .false.) and without the LTE scattering split (do_scat)
+ * add_opacity_equi (HOP/linelist_mod.f90:729-960), with or without per-line
+ * reach (has_reach: select_lines, and lines centred beyond the chunk take the
+ * unfloored reference at the nearer end and a window capped by their reach);
+ * without the LTE scattering split (do_scat)
  * ========================================================================= */
 int or_add_opacity_equi(const float *tgx, const float *th2x, const or_linelist_t *ll,
                         int nf, const double *llam, int ncell,
@@ -437,6 +490,11 @@ int or_add_opacity_equi(const float *tgx, const float *th2x, const or_linelist_t
   const float sdl = (float)inv_dllam;
   const float flo_scale = fmaxf(tol, line_reject_frac) * tol;
   float *Kbuf = (float *)malloc(sizeof(float) * (size_t)nf);
+  int *sel = (int *)malloc(sizeof(int) * (size_t)(ll->nline > 0 ? ll->nline : 1));
+  float vmax = 0.0f;
+  if (ll->reach_in)
+    for (int i = 0; i < ncell; i++) vmax = fmaxf(vmax, fabsf(vproj[i]));
+  const int nsel = or_select_lines(ll, nf, llam, vmax, sel);
   for (int i = 0; i < ncell; i++) {
     float *ch = chi + (size_t)nf * i, *et = eta + (size_t)nf * i;
     const float *co = cont + (size_t)nf * i, *lr = logref + (size_t)nf * i;
@@ -449,8 +507,8 @@ int or_add_opacity_equi(const float *tgx, const float *th2x, const or_linelist_t
     const float ekt = e_kT[i], ne_c = ne[i], tothi_c = tothi[i], starkpe = stark_pe[i];
     const float vproj_c = vproj[i];
     const float base = lnbase[i];
-    for (int l = 0; l < ll->nline; l++) {
-      if (ll->active && !ll->active[l]) continue;
+    for (int isel = 0; isel < nsel; isel++) {
+      const int l = sel[isel];
       double llc = ll->llam0[l] - (double)vproj_c;
       double pos = (llc - llam1) * inv_dllam;
       int f0 = (int)lround(pos) + 1;
@@ -458,21 +516,33 @@ int or_add_opacity_equi(const float *tgx, const float *th2x, const or_linelist_t
       float ex = ll->lower_ev[l] * ekt;
       float arg = (base + ll->gpref[l]) - ex;
       if (arg < ex_cutoff) continue;
-      if (f0 != f0_prev) {
-        f0_prev = f0;
-        refl_c = tol * co[f0 - 1];
-        float flo = flo_scale * ch[f0 - 1];
-        if (flo > refl_c) {
-          refl_c = flo;
-          lref_c = or_logf1(flo * sqrt_pi);
-        } else {
-          lref_c = lr[f0 - 1];
+      const int outside = ll->reach_in && (llc < llam[0] || llc > llam[nf - 1]);
+      float Rij, ref, lref_o = 0.0f;
+      int fe = 0;
+      if (outside) {
+        /* centred beyond the chunk: the reference at the nearer end, unfloored */
+        fe = llc < llam[0] ? 1 : nf;
+        lref_o = lr[fe - 1];
+        if (arg <= lref_o) continue;
+        Rij = or_exp4(arg);
+        ref = tol * co[fe - 1];
+      } else {
+        if (f0 != f0_prev) {
+          f0_prev = f0;
+          refl_c = tol * co[f0 - 1];
+          float flo = flo_scale * ch[f0 - 1];
+          if (flo > refl_c) {
+            refl_c = flo;
+            lref_c = or_logf1(flo * sqrt_pi);
+          } else {
+            lref_c = lr[f0 - 1];
+          }
         }
+        if (arg <= lref_c) continue;
+        Rij = or_exp4(arg);
+        ref = refl_c;
+        if (voigt_peak * Rij <= ref) continue;
       }
-      if (arg <= lref_c) continue;
-      float Rij = or_exp4(arg);
-      float ref = refl_c;
-      if (voigt_peak * Rij <= ref) continue;
       int nlte = do_nlte && ll->lev_i && ll->lev_j && ll->lev_i[l] > 0 && ll->lev_j[l] > 0;
       float bi = 1.0f, bj = 1.0f;
       if (nlte) {
@@ -485,15 +555,21 @@ int or_add_opacity_equi(const float *tgx, const float *th2x, const or_linelist_t
       if (ll->gstk[l] >= 0.0f) a = fmaf(ll->gstk[l], ne_c, a);
       else a = fmaf(-ll->gstk[l], starkpe, a);
       a = a * sdl;
-      if (strength) {
-        float st = (voigt_peak * Rij) / co[f0 - 1];
-        if (st > strength[l]) strength[l] = st;
+      float cap = FLT_MAX, lnq;
+      if (outside) {
+        cap = (float)((double)ll->reach_in[l] * inv_dllam);
+        lnq = arg - lref_o;
+      } else {
+        if (strength) {
+          float st = (voigt_peak * Rij) / co[f0 - 1];
+          if (st > strength[l]) strength[l] = st;
+        }
+        lnq = arg - lref_c;
       }
-      float lnq = arg - lref_c;
       int fa, fb;
       float hw;
       int nk = line_sweep(tgx, th2x, &qw, a, Rij * qw.D, ref, lnq, nf, llam, llc, pos, inv_dllam,
-                          FLT_MAX, &fa, &fb, &hw, Kbuf);
+                          cap, &fa, &fb, &hw, Kbuf);
       if (reach) {
         float rch = (float)((double)hw * dllam);
         if (rch > reach[l]) reach[l] = rch;
@@ -509,6 +585,7 @@ int or_add_opacity_equi(const float *tgx, const float *th2x, const or_linelist_t
     }
   }
   free(Kbuf);
+  free(sel);
   return 0;
 }
 

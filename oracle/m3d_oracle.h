@@ -76,7 +76,13 @@ typedef struct {
   const uint8_t *unsold;    /* 1 -> Unsold van der Waals */
   const int *lev_i, *lev_j; /* NLTE levels (1-based, 0 = none), may be NULL */
   const uint8_t *active;    /* may be NULL (all active) */
+  const float *reach_in;    /* per-line reach [log(lambda)] from a previous run, or NULL (has_reach = .false.) */
 } or_linelist_t;
+
+/* select_lines (linelist_mod.f90:1110-1142): the active lines whose reach window can
+ * touch llam(1:nf) given the largest |vproj|; sel receives 0-based line indices in
+ * ascending order, the return value is their number.  Without reach_in every active line. */
+int or_select_lines(const or_linelist_t *ll, int nf, const double *llam, float vmax, int *sel);
 
 /* per-cell fields (m1*m2*m3 cells, x fastest); cont, logref, chi, eta are (nf, cells) */
 int or_add_opacity_equi(const float *tgx, const float *th2x, const or_linelist_t *ll,

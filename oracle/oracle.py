@@ -34,7 +34,8 @@ class LineList(C.Structure):
     _fields_ = [("nline", C.c_int), ("llam0", C.c_void_p), ("lower_ev", C.c_void_p),
                 ("gpref", C.c_void_p), ("grad", C.c_void_p), ("gw1", C.c_void_p),
                 ("gw2", C.c_void_p), ("gstk", C.c_void_p), ("unsold", C.c_void_p),
-                ("lev_i", C.c_void_p), ("lev_j", C.c_void_p), ("active", C.c_void_p)]
+                ("lev_i", C.c_void_p), ("lev_j", C.c_void_p), ("active", C.c_void_p),
+                ("reach_in", C.c_void_p)]
 
 
 def build() -> str:
@@ -189,7 +190,17 @@ def make_linelist(ll: dict) -> tuple[LineList, list]:
     s.lev_i = arr("lev_i", np.int32)
     s.lev_j = arr("lev_j", np.int32)
     s.active = arr("active", np.uint8)
+    s.reach_in = arr("reach_in", np.float32)
     return s, keep
+
+
+def select_lines(ll: dict, llam, vmax: float):
+    """select_lines: the selected 0-based line indices."""
+    s, keep = make_linelist(ll)
+    llam = np.ascontiguousarray(llam, np.float64)
+    sel = np.zeros(max(s.nline, 1), np.int32)
+    n = lib().or_select_lines(C.byref(s), C.c_int(llam.size), _p(llam), C.c_float(vmax), _p(sel))
+    return sel[:n]
 
 
 def add_opacity_equi(ll: dict, llam, chi, eta, cont, logref, cells: dict, dep_mem=None,
