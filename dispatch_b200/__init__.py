@@ -36,7 +36,7 @@ EXPORTS = ("m3d_init", "m3d_free", "m3d_last_error", "m3d_version", "m3d_set_str
            "m3d_stateq_update", "m3d_ng_accumulate", "m3d_ng_extrapolate", "m3d_bb_damping", "m3d_bf_opacity",
            "m3d_bb_opacity", "m3d_work_to_transfer_units_split", "m3d_bb_rates", "m3d_bf_rates",
            "m3d_integrate_rates", "m3d_normalize_profiles", "m3d_combine_twins", "m3d_update_eta_mask",
-           "m3d_lte_populations", "m3d_particle_fields")
+           "m3d_lte_populations", "m3d_particle_fields", "m3d_lte_emission")
 
 
 class M3DError(RuntimeError):

@@ -138,3 +138,44 @@ __global__ void k_particle_fields(int ncell, ParticleArgs P, const float *__rest
 }
 
 }  // namespace m3d
+
+namespace m3d {
+
+// lte_background_emission (rt_patch_mod.f90:2127-2328) with convert_to_work_units
+// (:3518-3536), per point: J from the previous iteration (jmode 0), Bnu (1, the
+// Planck start) or 0 (2); with PsiJ, the OAB step of scattering preconditioning
+// Jali = (J - op Jali_old)/(1 - op), op = sigma PsiJ clamped to [0, op_max], in
+// real(8), kept for the next iteration; then eta = chi Bnu + sigma (J - Bnu),
+// dJnu = J - Bnu, xhat = chi + eta, ehat = eta/beta.
+struct EmissionArgs { int jmode, scat_precond, jali_valid; double op_max; };
+
+__global__ void k_lte_emission(size_t n, EmissionArgs E, const float *__restrict__ chi, const float *__restrict__ sigma,
+                               const float *__restrict__ Bnu, const float *__restrict__ beta, const float *__restrict__ J,
+                               const float *__restrict__ PsiJ, float *__restrict__ Jali, float *__restrict__ xhat,
+                               float *__restrict__ ehat, float *__restrict__ dJnu, unsigned *__restrict__ nneg) {
+  unsigned neg = 0;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+    const float B = Bnu[k];
+    float j = E.jmode == 1 ? B : (E.jmode == 2 ? 0.0f : J[k]);
+    if (E.jmode == 0 && E.scat_precond) {
+      const float sg = sigma ? sigma[k] : 0.0f;
+      double op = (double)sg * (double)PsiJ[k];
+      op = fmax(0.0, fmin(op, E.op_max));
+      const double jfs = (double)j;
+      const double jold = E.jali_valid ? (double)Jali[k] : jfs;
+      double jn = (jfs - op * jold) / (1.0 - op);
+      if (jn < 0.0) { jn = jfs; neg++; }
+      j = (float)jn;
+      Jali[k] = j;
+    }
+    const float dj = j - B;
+    const float s = sigma ? sigma[k] : 0.0f;
+    const float eta = chi[k] * B + s * dj;
+    if (dJnu) dJnu[k] = dj;
+    xhat[k] = chi[k] + eta;
+    ehat[k] = eta / beta[k];
+  }
+  if (nneg && neg) atomicAdd(nneg, neg);
+}
+
+}  // namespace m3d

@@ -308,3 +308,30 @@ def particle_fields(awgt, vmic, iso_frac, temp, n, part, population_scale=0.0):
                                     C.c_double(population_scale), ptr(temp), ptr(n), ptr(part), ptr(idf), ptr(vb),
                                     ptr(lb), C.c_uint(0)), "m3d_particle_fields")
     return idf, vb, lb
+
+
+def lte_emission(chi_cont, Bnu, beta, sigma=None, Jnu=None, jnu_init=0, PsiJ=None, Jali=None, jali_valid=False,
+                 scat_op_max=0.9, out=None):
+    """lte_background_emission + convert_to_work_units: (xhat, ehat, dJnu, n_negative).
+
+    jnu_init: 0 Jnu given, 1 Jnu = Bnu (the Planck start), 2 Jnu = 0; PsiJ given:
+    the OAB step with Jali (in/out).  out: optional (xhat, ehat, dJnu) arrays."""
+    init()
+    dev = _is_dev(Bnu)
+    if out is None:
+        if dev:
+            import torch
+            out = tuple(torch.empty_like(Bnu) for _ in range(3))
+        else:
+            out = tuple(np.empty(np.shape(Bnu), _F32) for _ in range(3))
+    xhat, ehat, dj = out
+    if not dev:
+        chi_cont, Bnu, beta, sigma, Jnu, PsiJ = (None if a is None else np.ascontiguousarray(a, _F32)
+                                                 for a in (chi_cont, Bnu, beta, sigma, Jnu, PsiJ))
+    nf, ncell = int(Bnu.shape[-1]), int(np.prod(Bnu.shape[:-1]))
+    neg = C.c_longlong()
+    check(lib().m3d_lte_emission(C.c_int(nf), C.c_int(ncell), ptr(chi_cont), ptr(sigma), ptr(Bnu), ptr(beta),
+                                 ptr(Jnu), C.c_int(jnu_init), ptr(PsiJ), ptr(Jali), C.c_int(int(jali_valid)),
+                                 C.c_double(scat_op_max), ptr(xhat), ptr(ehat), ptr(dj), C.byref(neg),
+                                 C.c_uint(DEVICE_PTRS if dev else 0)), "m3d_lte_emission")
+    return xhat, ehat, dj, neg.value

@@ -453,6 +453,18 @@ int m3d_update_eta_mask(const m3d_slab_t *slab, const float *work, const float *
 int m3d_lte_populations(const m3d_atom_t *atom, int ncell, const float *temp, const float *lsaha, const float *dxi,
                         double *nstar, double *totn, unsigned flags);
 
+/* lte_background_emission (rt_patch_mod.f90:2127-2328) with convert_to_work_units
+ * (:3518-3536), all (nf, ncell): J is Jnu (jnu_init 0, a later iteration), Bnu (1,
+ * initial_Jnu='Planck') or 0 (2, 'zero'); with PsiJ the OAB step of scattering
+ * preconditioning, Jali = (J - op Jali_old)/(1 - op), op = sigma PsiJ clamped to
+ * [0, scat_op_max], in float64 (Jali in/out, jali_valid 0 seeds it with J; negative
+ * results fall back to J and are counted in n_negative); then eta = chi_cont Bnu +
+ * sigma (J - Bnu), dJnu = J - Bnu (may be NULL), xhat = chi_cont + eta, ehat = eta/beta.
+ * sigma NULL: no continuum scattering.  Jnu itself is not modified. */
+int m3d_lte_emission(int nf, int ncell, const float *chi_cont, const float *sigma, const float *Bnu, const float *beta,
+                     const float *Jnu, int jnu_init, const float *PsiJ, float *Jali, int jali_valid, double scat_op_max,
+                     float *xhat, float *ehat, float *dJnu, long long *n_negative, unsigned flags);
+
 /* add_particle_opacity's per-cell fields of one isotope (linelist_mod.f90:1023-1042,
  * ion_mod.f90:198-221): inv_df, vbar2 and lnbase = ln max(n, tiny) [+ ln scale] - part
  * + ln inv_df + ln iso_frac; n and part (the log partition function) float64.

@@ -147,3 +147,14 @@ def normalize_profiles(atom, nstar, wphi, gamma_ij, gamma_ji, has_wphi, first_it
     lib().or_normalize_profiles(C.c_int(gamma_ij.shape[1]), C.c_int(int(atom["nline"])), C.c_int(len(ti)), _vp(ti),
                                 _vp(tj), _vp(act), _vp(hw), C.c_int(int(first_iter)), _vp(nstar), _vp(wphi),
                                 _vp(gamma_ij), _vp(gamma_ji))
+
+
+def lte_emission(chi, sigma, Bnu, beta, J=None, jmode=0, PsiJ=None, Jali=None, jali_valid=False, op_max=0.9):
+    """Returns xhat, ehat, dJnu, n_negative; Jali updated in place."""
+    chi, sigma, Bnu, beta, J, PsiJ = (_c(x, np.float32) for x in (chi, sigma, Bnu, beta, J, PsiJ))
+    xhat, ehat, dj = np.empty_like(Bnu), np.empty_like(Bnu), np.empty_like(Bnu)
+    f = lib().or_lte_emission
+    f.restype = C.c_longlong
+    neg = f(C.c_size_t(Bnu.size), _vp(chi), _vp(sigma), _vp(Bnu), _vp(beta), _vp(J), C.c_int(jmode), _vp(PsiJ),
+            _vp(Jali), C.c_int(int(jali_valid)), C.c_double(op_max), _vp(xhat), _vp(ehat), _vp(dj))
+    return xhat, ehat, dj, neg

@@ -368,3 +368,36 @@ void or_normalize_profiles(int ncell, int nline, int nrad, const int *ti, const 
     }
   }
 }
+
+/* lte_background_emission (rt_patch_mod.f90:2127-2328) with convert_to_work_units
+ * (:3518-3536); jmode 0: Jnu given, 1: Jnu = Bnu, 2: Jnu = 0; PsiJ non-NULL: the OAB
+ * step (:2225-2252); returns the number of negative OAB results */
+long long or_lte_emission(size_t n, const float *chi, const float *sigma, const float *Bnu, const float *beta,
+                          const float *J, int jmode, const float *PsiJ, float *Jali, int jali_valid, double op_max,
+                          float *xhat, float *ehat, float *dJnu)
+{
+  long long neg = 0;
+  for (size_t k = 0; k < n; k++) {
+    const float B = Bnu[k];
+    float j = jmode == 1 ? B : (jmode == 2 ? 0.0f : J[k]);
+    if (jmode == 0 && PsiJ) {
+      double op = (double)(sigma ? sigma[k] : 0.0f) * (double)PsiJ[k];
+      op = fmax(0.0, fmin(op, op_max));
+      const double jfs = (double)j;
+      const double jold = jali_valid ? (double)Jali[k] : jfs;
+      double jn = (jfs - op * jold) / (1.0 - op);
+      if (jn < 0.0) {
+        jn = jfs;
+        neg++;
+      }
+      j = (float)jn;
+      Jali[k] = j;
+    }
+    const float dj = j - B;
+    const float eta = chi[k] * B + (sigma ? sigma[k] : 0.0f) * dj;
+    if (dJnu) dJnu[k] = dj;
+    xhat[k] = chi[k] + eta;
+    ehat[k] = eta / beta[k];
+  }
+  return neg;
+}

@@ -9,6 +9,7 @@
  */
 #ifndef OR_NLTE_H
 #define OR_NLTE_H
+#include <stddef.h>
 
 #ifdef __cplusplus
 extern "C" {
@@ -84,6 +85,11 @@ void or_bf_rates(const nl_window_t *w, int ncell, int precond, const double *b, 
 void or_normalize_profiles(int ncell, int nline, int nrad, const int *ti, const int *tj,
                            const unsigned char *active, const unsigned char *has_wphi, int first_iter,
                            const double *nstar, float *wphi, float *gamma_ij, float *gamma_ji);
+
+/* lte_background_emission with convert_to_work_units (rt_patch_mod.f90:2127-2328, 3518-3536) */
+long long or_lte_emission(size_t n, const float *chi, const float *sigma, const float *Bnu, const float *beta,
+                          const float *J, int jmode, const float *PsiJ, float *Jali, int jali_valid, double op_max,
+                          float *xhat, float *ehat, float *dJnu);
 
 #ifdef __cplusplus
 }

@@ -103,3 +103,30 @@ def test_particle_fields_gpu(m3d, ax):
         ig, vg, lg = m3d.rt.particle_fields(55.847, vmic, frac, temp, n, part, population_scale=scale)
         assert np.array_equal(ig, io) and np.array_equal(vg, vo)
         np.testing.assert_allclose(lg, lo, rtol=0, atol=4 * np.spacing(np.abs(lo)).max())   # log / logf ulps
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("jmode,precond,valid", [(1, False, False), (2, False, False), (0, False, False),
+                                                   (0, True, False), (0, True, True)])
+def test_lte_emission_gpu(m3d, jmode, precond, valid):
+    from oracle import nlte as onl
+    rng = np.random.default_rng(jmode + 3 * precond + 7 * valid)
+    shape = (500, 64)
+    chi = rng.uniform(1e-9, 1e-6, shape).astype(np.float32)
+    sigma = (chi * rng.uniform(0, 3, shape)).astype(np.float32)
+    beta = rng.uniform(1e-6, 0.9, shape).astype(np.float32)
+    Bnu = (beta / (1 - beta)).astype(np.float32)
+    J = (Bnu * rng.uniform(0.2, 1.5, shape)).astype(np.float32)
+    PsiJ = (rng.uniform(0, 2, shape) / chi).astype(np.float32) if precond else None
+    Jali0 = (J * rng.uniform(0.5, 1.5, shape)).astype(np.float32)
+    ja_o, ja_g = Jali0.copy(), Jali0.copy()
+    xo, eo, do, no = onl.lte_emission(chi, sigma, Bnu, beta, J if jmode == 0 else None, jmode, PsiJ,
+                                      ja_o if precond else None, valid, 0.9)
+    xg, eg, dg, ng = m3d.rt.lte_emission(chi, Bnu, beta, sigma=sigma, Jnu=J if jmode == 0 else None,
+                                         jnu_init=jmode, PsiJ=PsiJ, Jali=ja_g if precond else None,
+                                         jali_valid=valid, scat_op_max=0.9)
+    for a, b in ((xg, xo), (eg, eo), (dg, do), (ja_g, ja_o)):
+        assert np.array_equal(a, b)
+    assert ng == no
+    if precond:
+        assert no > 0 or not np.array_equal(ja_o, Jali0)
