@@ -1,0 +1,276 @@
+"""The 3D NLTE ALI iteration of one frequency window, composed from the library's
+entry points over device-resident arrays.
+
+One iteration is the ALI branch of rt_patch_t%execute (SRC/rt_patch_mod.f90:1038-1060)
+for the two hemisphere twins of a periodic cube held as one patch, then the
+atom update of nlte_patch_t%execute (SRC/nlte_patch_mod.f90:590-660):
+
+* per twin: background (lte_background_emission + convert_to_work_units,
+  add_bound_free_opacities, :1297-1351); per direction back_to_work, foreground
+  (the split start and add_bound_bound_opacities, :1462-1500),
+  work_to_transfer_units, set_upstream_boundary, radiative_transfer,
+  aniso_integrations (integrate_intensity, bound_bound_rates, :1728-1758); then
+  iso_integrations (bound_free_rates, integrate_rates, :1765-1777);
+* combine_twin_hemispheres (:1812-1887);
+* the update: normalize_profiles (SRC/atom_mod.f90:377-431), update_populations
+  with the fused classic_col rates (:439-732), the convergence bookkeeping of
+  nlte_patch_t%execute (:711-765) and ng_acceleration (:2469-2548).
+
+Everything per point stays on the GPU between the calls; the host keeps the
+scalars of the convergence test and the Ng gate.  Arrays follow the library's
+layout: per-point (ncell, nf) frequency fastest with cell = x + nx (y + ny z),
+z = 0 the bottom plane; per-level (nlevel, ncell).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import (BND_PCHIP, BND_ZERO, SHORT_LINEAR, M3DError, init, make_slab, nlte, rt, stateq, synth)
+
+
+@dataclass
+class AliParams:
+    """The run parameters the iteration reads (the reference's &rt_params and
+    &nlte_params defaults where they exist)."""
+
+    solver: int = SHORT_LINEAR          # rt_iter%solver: short_char ('linear' in 3D)
+    bottom: int = BND_PCHIP             # upstream ghost of upward rays at the bottom
+    preconditioning: bool = True        # Rybicki-Hummer preconditioning of the rates
+    split_rates: bool = True            # rate_formulation = 'largest'
+    maser_chi_floor: float = 1e-4
+    maser_dtau_max: float = 2.0
+    maser_Inu_max: float = 1e30
+    se_solver: int = stateq.LINEQ_NO_PIVOT
+    max_update: float = 1e2
+    sor_w: float = 1.0
+    min_pop_frac: float = 1e-30
+    convlim: float = 1e-3
+    ng_step: int = 0                    # < 0 off, 0 the automatic gate, > 0 fixed schedule
+    ng_start: int = 0
+    ng: stateq.NgParams = field(default_factory=stateq.NgParams)
+
+
+class AliWindow:
+    """One frequency window of a model atom on a periodic cube, device resident.
+
+    cube: temp, ne, nH (ncell,), chi_c (ncell,) grey continuum [1/cm], vz (ncell,)
+    vertical velocity [c], the shape (nx, ny, nz) and ds (3,) [cm].  atom: a
+    model atom (synth.model_atom); win: its transitions on one frequency window
+    (synth.atom_window); vec, wts: the directions of both hemispheres with
+    mean-intensity weights (synth.lobatto_rays(..., jnu_weights=True)), the
+    upward half first.
+    """
+
+    def __init__(self, cube: dict, atom: dict, win: dict, vec, wts, params: AliParams | None = None,
+                 abundance: float = 7.5, awgt: float = 56.0, vmic_kms: float = 1.0, device: str = "cuda"):
+        import torch
+
+        init()
+        self.p = params or AliParams()
+        self.atom, self.win = atom, win
+        self.nx, self.ny, self.nz = (int(v) for v in cube["shape"])
+        self.ds = [float(v) for v in cube["ds"]]
+        nc = self.nx * self.ny * self.nz
+        self.ncell, self.nf = nc, int(win["nf"])
+        vec = np.asarray(vec, np.float64)
+        wts = np.asarray(wts, np.float64)
+        nd = vec.shape[0]
+        if nd % 2 or not np.allclose(vec[nd // 2:], -vec[:nd // 2]) or np.any(vec[:nd // 2, 2] <= 0):
+            raise M3DError("AliWindow: vec must hold the upward directions, then the same mirrored")
+        self.vec, self.wts = vec, wts
+        self.wmu = wts.astype(np.float32)
+        # wtot = sum(rt_iter%wmu) in real(4), in the order the directions come
+        wt = np.float32(0.0)
+        for w in self.wmu:
+            wt = np.float32(wt + w)
+        self.wtot = float(wt)
+        dev = torch.device(device)
+        self.dev = dev
+        f32 = lambda a: torch.as_tensor(np.ascontiguousarray(a, np.float32), device=dev)
+        f64 = lambda a: torch.as_tensor(np.ascontiguousarray(a, np.float64), device=dev)
+
+        temp = np.ascontiguousarray(cube["temp"], np.float32).ravel()
+        ne = np.asarray(cube["ne"], np.float64).ravel()
+        nH = np.asarray(cube["nH"], np.float64).ravel()
+        totn0 = 10.0 ** (abundance - 12.0) * nH
+        nstar, totn = synth.lte_populations(atom, temp, ne, totn0)
+        self.temp, self.ne = f64(temp), f64(ne)
+        self.e_kT = f64(synth.EE / synth.BK / temp.astype(np.float64))
+        self.nstar, self.totn = f64(nstar), f64(totn)
+        self.pop_ratio = torch.ones(nc, dtype=torch.float64, device=dev)
+        idf = synth.inverse_doppler_factor(temp, awgt, vmic_kms).astype(np.float32)
+        self.inv_df = f32(idf)
+        vbar2 = synth.compute_vbar2(temp, awgt).astype(np.float32)
+        ne32, nh32 = ne.astype(np.float32), nH.astype(np.float32)
+        stark = (ne32 * temp ** np.float32(1.0 / 6.0)).astype(np.float32)
+        uns = (vbar2.astype(np.float64) ** 0.3 * nH).astype(np.float32)
+        self.adamp = f32(nlte.bb_damping(win, ne32, nh32, vbar2, stark, uns, idf))
+        vz = np.ascontiguousarray(cube["vz"], np.float32).ravel()
+        self.vproj = [f32(vz * np.float32(v[2])) for v in vec]
+        self.beta, self.Bnu = rt.lte_background(f64(win["nu"]), f32(temp))
+        self.chi_c = f32(np.asarray(cube["chi_c"], np.float32).ravel())[:, None].expand(nc, self.nf).contiguous()
+
+        nl = self.nlevel = int(atom["nlevel"])
+        self.nrad = len(atom["ti"])
+        self.b = torch.ones((nl, nc), dtype=torch.float64, device=dev)
+        self.oldb = torch.zeros((3, nl, nc), dtype=torch.float64, device=dev)
+        self.gamma_ij = torch.zeros((self.nrad, nc), dtype=torch.float32, device=dev)
+        self.gamma_ji = torch.zeros_like(self.gamma_ij)
+        nw = int(win["nline"]) + int(win["ncont"])
+        self.gw_ij = torch.zeros((max(nw, 1), nc), dtype=torch.float32, device=dev)
+        self.gw_ji = torch.zeros_like(self.gw_ij)
+        sums = np.zeros(int(atom["nline"]), np.uint8)
+        sums[np.asarray(win["line_ntrans"], np.int64)] = np.asarray(win["sums_over_windows"], np.uint8)
+        self.has_wphi = sums
+        # profile integrals of the lines whose windows are summed (rows of the others stay 0)
+        self.wphi = torch.zeros((max(int(atom["nline"]), 1), nc), dtype=torch.float32, device=dev)
+
+        shp = (nc, self.nf)
+        self.work = torch.zeros((3, self.nz + 2, self.ny, self.nx, self.nf), dtype=torch.float32, device=dev)
+        self.w1 = self.work[0, 1:self.nz + 1].view(shp)
+        self.w2 = self.work[1, 1:self.nz + 1].view(shp)
+        self.inu = self.work[2, 1:self.nz + 1].view(shp)
+        z = lambda dt=torch.float32: torch.zeros(shp, dtype=dt, device=dev)
+        self.psi, self.irem, self.escape = z(), z(), z()
+        self.xhat, self.ehat, self.dj = z(), z(), z()
+        self.split = {"opac_L": z(), "opac_R": z(), "id": z(torch.int32), "chi_L": z(), "chi_R": z(),
+                      "chi_id": z(torch.int32)}
+        self.J = torch.zeros((2,) + shp, dtype=torch.float32, device=dev)
+        self.PsiJ = torch.zeros_like(self.J)
+        self.slabs = [make_slab(self.nf, self.nx, self.ny, self.nz, 1 if v[2] > 0 else -1, self.ds, v, get_psi=True,
+                                split_rates=self.p.split_rates, maser_dtau_max=self.p.maser_dtau_max,
+                                maser_Inu_max=self.p.maser_Inu_max) for v in vec]
+        self.ng = stateq.NgState(params=self.p.ng)
+        self.iter = 0
+        self.history: list[dict] = []
+        self._sweep_maxerr = 0.0
+        self._last_maxerr = 0.0
+        self._global = 0.0
+        self.converged = False
+
+    # ---- rt_patch_t%execute, ALI branch -------------------------------------------------
+    def sweep(self) -> None:
+        """The formal solutions of every direction of both twins, with J, PsiJ and the
+        rates of this iteration accumulated into gamma_ij/ji."""
+        p, win = self.p, self.win
+        nd = len(self.slabs)
+        first = self.iter == 0
+        for h in range(2):
+            dirs = range(h * nd // 2, (h + 1) * nd // 2)
+            # background: the LTE continuum (pure absorption, Jnu = Bnu) in work units,
+            # then the bound-free opacities of the current populations
+            rt.lte_emission(self.chi_c, self.Bnu, self.beta, jnu_init=1, out=(self.xhat, self.ehat, self.dj))
+            nlte.bf_opacity(win, self.b, self.nstar, self.pop_ratio, self.e_kT, self.xhat, self.ehat)
+            self.J[h].zero_()
+            self.PsiJ[h].zero_()
+            self.gw_ij.zero_()
+            self.gw_ji.zero_()
+            for d in dirs:
+                slab, wmu, vp = self.slabs[d], float(self.wmu[d]), self.vproj[d]
+                self.w1.copy_(self.xhat)
+                self.w2.copy_(self.ehat)
+                nlte.bb_opacity(win, self.b, self.nstar, self.pop_ratio, self.e_kT, self.inv_df, vp, self.adamp,
+                                self.w1, self.w2, lte=False, wmu=wmu, split=self.split if p.split_rates else None,
+                                wphi=self.wphi if first else None)
+                if p.split_rates:
+                    nlte.transfer_units_split(self.w1, self.w2, self.beta, self.split,
+                                              maser_chi_floor=p.maser_chi_floor)
+                else:
+                    rt.work_to_transfer_units(self.w1, self.w2, self.beta, maser_chi_floor=p.maser_chi_floor)
+                mode = p.bottom if slab.dir > 0 else BND_ZERO
+                rt.upstream_boundary(slab, self.work, mode)
+                rt.formal_solve(p.solver, slab, self.work, psi=self.psi,
+                                irem=self.irem if p.split_rates else None,
+                                escape=self.escape if p.split_rates else None)
+                rt.integrate_intensity(wmu, self.inu, self.psi, self.J[h], self.PsiJ[h])
+                nlte.bb_rates(win, self.b, self.nstar, self.pop_ratio, self.e_kT, self.inv_df, vp, self.adamp,
+                              self.inu, self.beta, self.Bnu, self.gw_ij, self.gw_ji, work1=self.w1, psi=self.psi,
+                              irem=self.irem if p.split_rates else None,
+                              escape=self.escape if p.split_rates else None,
+                              split=self.split if p.split_rates else None, split_rates=p.split_rates,
+                              preconditioning=p.preconditioning, per_direction=True, wmu=wmu, wtot=self.wtot)
+            if int(win["ncont"]) > 0:
+                nlte.bf_rates(win, self.b, self.nstar, self.e_kT, self.J[h], self.PsiJ[h], self.beta, self.gw_ij,
+                              self.gw_ji, preconditioning=p.preconditioning)
+            nlte.integrate_rates(win, self.gw_ij, self.gw_ji, self.gamma_ij, self.gamma_ji)
+        nlte.combine_twins(self.J[0], self.J[1])
+        nlte.combine_twins(self.PsiJ[0], self.PsiJ[1])
+
+    # ---- nlte_patch_t%execute ----------------------------------------------------------
+    def update(self) -> dict:
+        """The atom update of iteration self.iter (>= 1): returns its record."""
+        p, it = self.p, self.iter
+        nlte.normalize_profiles(self.atom, self.nstar, self.wphi, self.gamma_ij, self.gamma_ji, self.has_wphi,
+                                first_iter=it == 1)
+        stateq.shift_oldb(self.oldb, self.b)
+        res, _ = stateq.stateq_update(self.atom, self.b, self.nstar, self.totn, self.e_kT, self.gamma_ij,
+                                      self.gamma_ji, temp=self.temp, ne=self.ne, solver=p.se_solver,
+                                      max_update=p.max_update, sor_w=p.sor_w, min_pop_frac=p.min_pop_frac)
+        maxerr = float(res["maxerr"])
+        self.ng.count_clamped(res["nclamp"], res["ntot"])
+        rec = {"iter": it, "maxerr": maxerr, "epos_cell": int(res["epos_cell"]), "epos_level": int(res["epos_level"]),
+               "ng": None}
+        convmax = 0.1 * max(p.convlim, 0.0)
+        atom_converged = abs(maxerr) < convmax
+        if p.ng_step >= 0 and not atom_converged:
+            ng = stateq.ng_acceleration(self.ng, it, self._global, p.convlim, self.b, self.oldb, self.nstar,
+                                        self.totn, extrapolate=abs(maxerr) >= p.convlim, ng_step=p.ng_step,
+                                        ng_start=p.ng_start)
+            rec["ng"] = ng
+        # the sweep bookkeeping of one patch: the Ng gate reads the change of the
+        # iteration before the last (self%global = last_maxerr)
+        self._last_maxerr = self._sweep_maxerr
+        self._sweep_maxerr = maxerr
+        self._global = self._last_maxerr
+        applied = bool(rec["ng"] and rec["ng"].get("applied"))
+        self.converged = atom_converged or (0.0 < abs(maxerr) < p.convlim and not applied)
+        self.gamma_ij.zero_()
+        self.gamma_ji.zero_()
+        self.history.append(rec)
+        return rec
+
+    def run(self, maxiter: int) -> list[dict]:
+        """Iteration 0 (LTE start, b = 1) and up to maxiter updates, each followed by
+        the next iteration's formal solutions unless it converged."""
+        if self.iter == 0:
+            self.sweep()
+        while self.iter < maxiter and not self.converged:
+            self.iter += 1
+            self.update()
+            if not self.converged and self.iter < maxiter:
+                self.sweep()
+        return self.history
+
+    def points(self) -> int:
+        """Ray-point-frequency visits of one sweep (both twins)."""
+        return len(self.slabs) * self.ncell * self.nf
+
+
+def cube_problem(kind: str = "small", seed: int = 2, nx: int = 8, ny: int = 8, nz: int = 12, nbound: int = 6,
+                 nline: int = 8, nper: int = 25, transitions=None, ntheta: int = 2, nphi: int = 4,
+                 sums=None) -> tuple[dict, dict, dict, np.ndarray, np.ndarray]:
+    """(cube, atom, win, vec, wts) of a seeded NLTE window: the grey cube with its
+    temperature and velocity fields, a model atom with nbound bound levels and
+    nline lines, its transitions on one window, and Lobatto directions with
+    mean-intensity weights.  kind 'c2': the 120^3 cube and the 20-level atom.
+    The horizontal cell size is the vertical one times the largest |tan theta| of
+    the directions (rounded up to a half), so that every upwind point of the
+    short characteristics lies within one cell (the stencil of set_stencil)."""
+    if kind == "c2":
+        nx = ny = nz = 120
+        nbound, nline = 20, 60
+        ntheta, nphi = 4, 4
+    vec, wts = synth.lobatto_rays(ntheta, nphi, jnu_weights=True)
+    tan_max = float(np.max(np.hypot(vec[:, 0], vec[:, 1]) / np.abs(vec[:, 2])))
+    aspect = max(2.0, float(np.ceil(2.0 * tan_max * (1.0 + 1e-6)) / 2.0))
+    c = synth.cube_atmosphere(seed, nx, ny, nz, aspect=aspect)
+    cube = {"temp": c["temp"].ravel(), "ne": c["ne"].ravel(), "nH": c["nH"].ravel(), "chi_c": c["chi_c"].ravel(),
+            "vz": c["vz"].ravel(), "shape": (nx, ny, nz), "ds": c["ds_cm"]}
+    atom = synth.model_atom(seed, nbound=nbound, nline=nline)
+    win = synth.atom_window(atom, nper=nper, seed=seed, transitions=transitions, sums=sums)
+    return cube, atom, win, vec, wts
+
+
+__all__ = ["AliParams", "AliWindow", "cube_problem"]

@@ -728,6 +728,17 @@ int solve_impl(int solver, const m3d_slab_t *s, unsigned flags, T *work, T *psi,
       double xk[4], yk[4], dsup;
       int upo1, upo2;
       set_stencil(s->ds, s->vec, xk, yk, &upo1, &upo2, &dsup);
+      {
+        // set_stencil places the upwind point between the two inner nodes of the
+        // 4x4 stencil only when it lies within one cell horizontally; beyond
+        // that the cubic kernel extrapolates and the sweep diverges
+        const double wt1 = -s->vec[0] / s->ds[0] * dsup, wt2 = -s->vec[1] / s->ds[1] * dsup;
+        if (fabs(wt1) > 1.0 || fabs(wt2) > 1.0)
+          return fail(M3D_EINVAL,
+                      "short characteristics: the upwind point of direction (%g, %g, %g) lies (%g, %g) cells away; "
+                      "the stencil reaches one cell (ds_x >= |v_x/v_z| ds_z)",
+                      s->vec[0], s->vec[1], s->vec[2], wt1, wt2);
+      }
       std::vector<int> tab(4 * (a.nx + a.ny));
       for (int x = 0; x < a.nx; x++)
         for (int ii = 0; ii < 4; ii++) {

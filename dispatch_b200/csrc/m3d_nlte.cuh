@@ -217,15 +217,33 @@ struct NlRadField {
   const int *sid, *schid;
 };
 
-__global__ void k_bb_rates(NlWinDev W, NlRateOpts O, int ncell, const double *__restrict__ b,
-                           const double *__restrict__ nstar, const double *__restrict__ pop_ratio,
-                           const double *__restrict__ e_kT, const float *__restrict__ inv_df,
-                           const float *__restrict__ vproj, const float *__restrict__ adamp,
-                           const float2 *__restrict__ tab, NlRadField R, const unsigned *__restrict__ flags_in,
-                           unsigned *__restrict__ flags_raise, float *__restrict__ gamma_ij,
-                           float *__restrict__ gamma_ji) {
+// Both rate kernels give one warp to one (cell, transition): its lanes evaluate
+// the window's frequencies 32 at a time, reading the per-point arrays along f
+// (coalesced), and lanes 0..3 then add the terms in ascending f out of shared
+// memory, so that every sum keeps the reference's left-to-right order.
+constexpr int kRateWarps = 8;
+
+__device__ __forceinline__ void rate_chunk_sum(float (*T)[33], int lane, int cnt, float &acc) {
+  __syncwarp();
+  if (lane < 4)
+    for (int j = 0; j < cnt; j++) acc = acc + T[lane][j];
+  __syncwarp();
+}
+
+__global__ void __launch_bounds__(kRateWarps * 32)
+k_bb_rates(NlWinDev W, NlRateOpts O, int ncell, const double *__restrict__ b,
+           const double *__restrict__ nstar, const double *__restrict__ pop_ratio,
+           const double *__restrict__ e_kT, const float *__restrict__ inv_df,
+           const float *__restrict__ vproj, const float *__restrict__ adamp,
+           const float2 *__restrict__ tab, NlRadField R, const unsigned *__restrict__ flags_in,
+           unsigned *__restrict__ flags_raise, float *__restrict__ gamma_ij,
+           float *__restrict__ gamma_ji) {
+  __shared__ float sh[kRateWarps][4][33];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  float (*T)[33] = sh[wib];
   const size_t nf = (size_t)W.nf, n = (size_t)ncell * W.nline;
-  for (size_t kk = blockIdx.x * (size_t)blockDim.x + threadIdx.x; kk < n; kk += (size_t)gridDim.x * blockDim.x) {
+  const size_t stride = (size_t)gridDim.x * kRateWarps;
+  for (size_t kk = (size_t)blockIdx.x * kRateWarps + wib; kk < n; kk += stride) {
     const int c = (int)(kk % ncell), i = (int)(kk / ncell);
     if (W.lactive && !W.lactive[i]) continue;
     const int li = W.li[i], lj = W.lj[i], fs = W.lblue[i], fe = W.lred[i], off = W.loff[i];
@@ -258,104 +276,132 @@ __global__ void k_bb_rates(NlWinDev W, NlRateOpts O, int ncell, const double *__
       abs_coef = split_Rij * split_bi;
       if (nj > 0.0f) g_ratio = (float)((double)(ni / nj) * (W.g[lj] / W.g[li]));
     }
-    float sum_A = 0, sum_I = 0, sum_P = 0, sum_T = 0, sum_U = 0, sum_w = 0;
+    // lane j < 4 accumulates sum j: (A, I, P, w) without the split, (T, U, -, w) with it
+    float acc = 0.0f;
     int in_force = 0, raise = 0;
     const int t = W.lntrans[i], pw = t >> 5, pb = t & 31;
     if (O.split && O.precond && O.use_flags) in_force = (flags_in[(size_t)c + (size_t)ncell * pw] >> pb) & 1u;
-    for (int f = fs; f <= fe; f++) {
-      const size_t k = (size_t)f + nf * c;
-      const int o = off + f - fs;
-      const float phi = nl_profile(tab, a, W.q[o], vpr, idf);
-      const float wmunu = (float)((double)O.wmu * W.wnu[o] * Aij);
-      const float wqf = (float)W.wq[o];
-      if (!O.split) {
-        const float vvv = phi * wmunu;
-        if (own_norm) sum_w = sum_w + phi * wqf;
-        sum_A = sum_A + vvv * (R.Bnu[k] * inv_nref);
-        sum_I = sum_I + vvv * R.inu[k];
-        sum_P = sum_P + vvv * phi * R.psi[k] * R.beta[k];
-      } else {
-        if (own_norm) sum_w = sum_w + phi * wqf;  // sum(vph * wqf), in the same f order
-        const float nb = R.Bnu[k];
-        const float vvv = phi * wmunu;
-        if (O.precond) {
-          const float be = R.beta[k];
-          float psi = R.psi[k];
-          const float eta_u = phi * eta_coef;
-          const float eta_t = eta_u * be;
-          const float chi_t = phi * abs_coef - eta_t;
-          const float eta_other = be * other_contribution(eta_u, index, R.sopL[k], R.sopR[k], R.sid[k]);
-          const float chi_other = other_contribution(phi * abs_coef, index, R.schL[k], R.schR[k], R.schid[k]) - eta_other;
-          float other = eta_other;
-          if (O.do_scat) other = other + R.scat[k];
-          if (chi_t < 0.0f || in_force) psi = 0.0f;
-          raise = raise || psi == 0.0f;
-          const float up = psi == 0.0f ? R.inu[k] : R.irem[k] + psi * other;
-          const float spont = psi == 0.0f ? 1.0f : (chi_other + R.escape[k] * chi_t) / R.work1[k];
-          sum_T = sum_T + vvv * spont * (nb * inv_nref);
-          sum_U = sum_U + vvv * (up - nb * spont);
+    for (int f0 = fs; f0 <= fe; f0 += 32) {
+      const int f = f0 + lane;
+      float t0 = 0.0f, t1 = 0.0f, t2 = 0.0f, t3 = 0.0f;
+      if (f <= fe) {
+        const size_t k = (size_t)f + nf * c;
+        const int o = off + f - fs;
+        const float phi = nl_profile(tab, a, W.q[o], vpr, idf);
+        const float wmunu = (float)((double)O.wmu * W.wnu[o] * Aij);
+        const float wqf = (float)W.wq[o];
+        t3 = phi * wqf;
+        if (!O.split) {
+          const float vvv = phi * wmunu;
+          t0 = vvv * (R.Bnu[k] * inv_nref);
+          t1 = vvv * R.inu[k];
+          t2 = vvv * phi * R.psi[k] * R.beta[k];
         } else {
-          sum_T = sum_T + vvv * (nb * inv_nref);
-          sum_U = sum_U + vvv * (R.inu[k] - nb);
+          const float nb = R.Bnu[k];
+          const float vvv = phi * wmunu;
+          if (O.precond) {
+            const float be = R.beta[k];
+            float psi = R.psi[k];
+            const float eta_u = phi * eta_coef;
+            const float eta_t = eta_u * be;
+            const float chi_t = phi * abs_coef - eta_t;
+            const float eta_other = be * other_contribution(eta_u, index, R.sopL[k], R.sopR[k], R.sid[k]);
+            const float chi_other = other_contribution(phi * abs_coef, index, R.schL[k], R.schR[k], R.schid[k]) - eta_other;
+            float other = eta_other;
+            if (O.do_scat) other = other + R.scat[k];
+            if (chi_t < 0.0f || in_force) psi = 0.0f;
+            raise = raise || psi == 0.0f;
+            const float up = psi == 0.0f ? R.inu[k] : R.irem[k] + psi * other;
+            const float spont = psi == 0.0f ? 1.0f : (chi_other + R.escape[k] * chi_t) / R.work1[k];
+            t0 = vvv * spont * (nb * inv_nref);
+            t1 = vvv * (up - nb * spont);
+          } else {
+            t0 = vvv * (nb * inv_nref);
+            t1 = vvv * (R.inu[k] - nb);
+          }
         }
       }
+      T[0][lane] = t0;
+      T[1][lane] = t1;
+      T[2][lane] = t2;
+      T[3][lane] = t3;
+      rate_chunk_sum(T, lane, min(32, fe - f0 + 1), acc);
     }
-    if (O.split && O.precond && O.use_flags && raise && !in_force)
-      atomicOr(&flags_raise[(size_t)c + (size_t)ncell * pw], 1u << pb);
-    float g_th, g_dev;
-    if (O.split) {
-      g_th = sum_T;
-      g_dev = sum_U;
-    } else {
-      g_th = sum_A;
-      g_dev = sum_I;
-      if (O.precond) {
-        g_th = g_th - sum_P * eta_coef * (g_ratio - 1.0f);
-        g_dev = g_dev - sum_P * eta_coef;
+    raise = __any_sync(0xffffffffu, raise);
+    const float s0 = __shfl_sync(0xffffffffu, acc, 0), s1 = __shfl_sync(0xffffffffu, acc, 1);
+    const float s2 = __shfl_sync(0xffffffffu, acc, 2), sum_w = __shfl_sync(0xffffffffu, acc, 3);
+    if (lane == 0) {
+      if (O.split && O.precond && O.use_flags && raise && !in_force)
+        atomicOr(&flags_raise[(size_t)c + (size_t)ncell * pw], 1u << pb);
+      float g_th = s0, g_dev = s1;
+      if (!O.split) {
+        if (O.precond) {
+          g_th = g_th - s2 * eta_coef * (g_ratio - 1.0f);
+          g_dev = g_dev - s2 * eta_coef;
+        }
+        if (inv_nref > 0.0f) g_dev = g_dev - g_th / inv_nref;
       }
-      if (inv_nref > 0.0f) g_dev = g_dev - g_th / inv_nref;
+      if (own_norm && sum_w > 0.0f) {
+        g_th = g_th / (sum_w * O.wtot);
+        g_dev = g_dev / (sum_w * O.wtot);
+      }
+      gamma_ij[kk] = gamma_ij[kk] + g_th;
+      gamma_ji[kk] = gamma_ji[kk] + g_dev;
     }
-    if (own_norm && sum_w > 0.0f) {
-      g_th = g_th / (sum_w * O.wtot);
-      g_dev = g_dev / (sum_w * O.wtot);
-    }
-    gamma_ij[kk] = gamma_ij[kk] + g_th;
-    gamma_ji[kk] = gamma_ji[kk] + g_dev;
   }
 }
 
-__global__ void k_bf_rates(NlWinDev W, int ncell, int precond, const double *__restrict__ b,
-                           const double *__restrict__ nstar, const double *__restrict__ e_kT,
-                           const float *__restrict__ twohnu3_c2, const float *__restrict__ Jnu,
-                           const float *__restrict__ PsiJ, const float *__restrict__ beta,
-                           float *__restrict__ gamma_ij, float *__restrict__ gamma_ji) {
+__global__ void __launch_bounds__(kRateWarps * 32)
+k_bf_rates(NlWinDev W, int ncell, int precond, const double *__restrict__ b,
+           const double *__restrict__ nstar, const double *__restrict__ e_kT,
+           const float *__restrict__ twohnu3_c2, const float *__restrict__ Jnu,
+           const float *__restrict__ PsiJ, const float *__restrict__ beta,
+           float *__restrict__ gamma_ij, float *__restrict__ gamma_ji) {
+  __shared__ float sh[kRateWarps][4][33];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  float (*T)[33] = sh[wib];
   const size_t nf = (size_t)W.nf, n = (size_t)ncell * W.ncont;
-  for (size_t kk = blockIdx.x * (size_t)blockDim.x + threadIdx.x; kk < n; kk += (size_t)gridDim.x * blockDim.x) {
+  const size_t stride = (size_t)gridDim.x * kRateWarps;
+  for (size_t kk = (size_t)blockIdx.x * kRateWarps + wib; kk < n; kk += stride) {
     const int c = (int)(kk % ncell), j = (int)(kk / ncell);
     if (W.cactive && !W.cactive[j]) continue;
     const int li = W.ci[j], lj = W.cj[j], fs = W.cblue[j], fe = W.cred[j], off = W.coff[j];
     if ((W.ev[lj] - W.ev[li]) * e_kT[c] > W.cut_x) continue;
-    float sum_abs = 0, sum_ems = 0, sum_pre = 0;
-    for (int f = fs; f <= fe; f++) {
-      const size_t k = (size_t)f + nf * c;
-      const int o = off + f - fs;
-      const float wmunu = (float)(0.5 * W.cwnu[o]);
-      const float vij = twohnu3_c2[f] * W.alpha[o] * wmunu;
-      const float vji = vij * beta[k];
-      const float phi = PsiJ[k] * W.alpha[o];
-      sum_abs = sum_abs + vij * Jnu[k];
-      sum_ems = sum_ems + vji * (Jnu[k] + 1.0f);
-      sum_pre = sum_pre + vji * phi;
+    // lanes 0, 1, 2 accumulate sum_abs, sum_ems, sum_pre
+    float acc = 0.0f;
+    for (int f0 = fs; f0 <= fe; f0 += 32) {
+      const int f = f0 + lane;
+      float t0 = 0.0f, t1 = 0.0f, t2 = 0.0f;
+      if (f <= fe) {
+        const size_t k = (size_t)f + nf * c;
+        const int o = off + f - fs;
+        const float wmunu = (float)(0.5 * W.cwnu[o]);
+        const float vij = twohnu3_c2[f] * W.alpha[o] * wmunu;
+        const float vji = vij * beta[k];
+        const float phi = PsiJ[k] * W.alpha[o];
+        t0 = vij * Jnu[k];
+        t1 = vji * (Jnu[k] + 1.0f);
+        t2 = vji * phi;
+      }
+      T[0][lane] = t0;
+      T[1][lane] = t1;
+      T[2][lane] = t2;
+      T[3][lane] = 0.0f;
+      rate_chunk_sum(T, lane, min(32, fe - f0 + 1), acc);
     }
-    float g_ij = sum_abs, g_ji = sum_ems;
-    if (precond) {
-      const double nsi = nstar[(size_t)c + (size_t)ncell * li];
-      g_ij = (float)((double)g_ij - (double)sum_pre * nsi * b[(size_t)c + (size_t)ncell * lj]);
-      g_ji = (float)((double)g_ji - (double)sum_pre * nsi * b[(size_t)c + (size_t)ncell * li]);
+    const float sum_abs = __shfl_sync(0xffffffffu, acc, 0), sum_ems = __shfl_sync(0xffffffffu, acc, 1);
+    const float sum_pre = __shfl_sync(0xffffffffu, acc, 2);
+    if (lane == 0) {
+      float g_ij = sum_abs, g_ji = sum_ems;
+      if (precond) {
+        const double nsi = nstar[(size_t)c + (size_t)ncell * li];
+        g_ij = (float)((double)g_ij - (double)sum_pre * nsi * b[(size_t)c + (size_t)ncell * lj]);
+        g_ji = (float)((double)g_ji - (double)sum_pre * nsi * b[(size_t)c + (size_t)ncell * li]);
+      }
+      const size_t kg = (size_t)c + (size_t)ncell * (W.nline + j);
+      gamma_ij[kg] = gamma_ij[kg] + g_ij;
+      gamma_ji[kg] = gamma_ji[kg] + g_ji;
     }
-    const size_t kg = (size_t)c + (size_t)ncell * (W.nline + j);
-    gamma_ij[kg] = gamma_ij[kg] + g_ij;
-    gamma_ji[kg] = gamma_ji[kg] + g_ji;
   }
 }
 

@@ -132,7 +132,16 @@ def line_opacity(ll: dict, llam, chi, eta, cont, logref, cells: dict, dep_mem=No
 
 
 def lte_background(nu, temp):
+    """beta, Bnu (ncell, nf); device tensors in, device tensors out (nu float64)."""
     init()
+    if _is_dev(temp):
+        import torch
+        nu = torch.as_tensor(nu, dtype=torch.float64, device=temp.device).contiguous()
+        beta = torch.empty((temp.numel(), nu.numel()), dtype=torch.float32, device=temp.device)
+        Bnu = torch.empty_like(beta)
+        check(lib().m3d_lte_background(C.c_int(nu.numel()), C.c_int(temp.numel()), ptr(nu), ptr(temp), ptr(beta),
+                                       ptr(Bnu), C.c_uint(DEVICE_PTRS)), "m3d_lte_background")
+        return beta, Bnu
     nu = np.ascontiguousarray(nu, np.float64)
     temp = np.ascontiguousarray(temp, _F32)
     beta = np.empty((temp.size, nu.size), _F32)

@@ -139,9 +139,9 @@ def gaussian_field(rng, shape, ell, sigma):
     return f * (sigma / f.std())
 
 
-def cube_atmosphere(seed, nx, ny, nz, sigma_t=300.0, ell=8.0, sigma_vz_kms=2.0, log_tau=(-6.0, 2.0)):
+def cube_atmosphere(seed, nx, ny, nz, sigma_t=300.0, ell=8.0, sigma_vz_kms=2.0, log_tau=(-6.0, 2.0), aspect=2.0):
     """3D cube, z index 0 = bottom (deepest).  Returns dict of (nz, ny, nx) arrays
-    plus the cell size [cm]."""
+    plus the cell size [cm]; the horizontal cell size is aspect times the vertical."""
     rng = np.random.default_rng(seed)
     # mean model on a fine tau grid -> geometric depth
     lt = np.linspace(log_tau[1], log_tau[0], 4001)
@@ -167,7 +167,7 @@ def cube_atmosphere(seed, nx, ny, nz, sigma_t=300.0, ell=8.0, sigma_vz_kms=2.0, 
         P[k] = P[k + 1] * np.exp(g * MU_MOL * MH / (BK * Tm) * ds_z)
     rho = P * MU_MOL * MH / (BK * temp)
     nH = rho / (1.4 * MH)
-    ds_xy = ds_z * 2.0
+    ds_xy = ds_z * aspect
     return {"temp": temp.astype(np.float32), "rho": rho, "nH": nH, "ne": 1e-4 * nH,
             "chi_c": (KAPPA500 * rho).astype(np.float32), "vz": (vz / CC).astype(np.float32),
             "ds_cm": (ds_xy, ds_xy, ds_z)}
@@ -183,43 +183,89 @@ def column_1d(ndep=80, log_tau=(-6.0, 2.0)):
             "chi_c": (KAPPA500 * rho).astype(np.float32), "dz": dz}
 
 
-def lobatto_rays(ntheta=4, nphi=4):
-    """Output rays of set_lobatto_quadratures + nphi_copies with flux weights
-    (SRC/ray_mod.f90:224-262, 392-490): mu = 1 once, every other mu with nphi
-    azimuths; weights wmu/nphi times mu."""
+def lobatto_rays(ntheta=4, nphi=4, jnu_weights=False):
+    """set_lobatto_quadratures + nphi_copies (SRC/ray_mod.f90:224-262, 392-490):
+    mu = 1 once, every other mu with nphi azimuths.  The table is the reference's
+    default-real literals, so mu and the weights are float32 values.  Flux
+    weights wmu/nphi times mu; with jnu_weights the set mirrored to the
+    downward hemisphere (vec -> -vec) and the weights halved."""
     tab = {4: ([1.0, 0.87174015, 0.59170018, 0.20929922], [0.03571428, 0.21070422, 0.34112270, 0.41245880]),
            3: ([1.0, 0.76505532, 0.28523152], [0.06666667, 0.37847496, 0.55485838]),
-           2: ([1.0, 0.44721360], [0.16666667, 0.83333333])}
+           2: ([1.0, 0.44721360], [0.16666667, 0.83333333]),
+           1: ([1.0], [1.0])}
     mu, wmu = tab[ntheta]
-    return _nphi_copies(nphi, np.array(mu), np.array(wmu))
+    return _nphi_copies(nphi, _f32(mu), _f32(wmu), jnu_weights=jnu_weights)
 
 
-def gauss_rays(ntheta=5):
-    """Gauss-Legendre mu on (0, 1), plane parallel (one azimuth), flux weights."""
+def gauss_rays(ntheta=5, nphi=1, jnu_weights=False):
+    """set_gauss_quadratures: Gauss-Legendre mu on (0, 1), descending, rounded to
+    float32 as the reference's default-real table is; then nphi_copies."""
     x, w = np.polynomial.legendre.leggauss(ntheta)
     mu = 0.5 * (x + 1.0)
     wmu = 0.5 * w
     order = np.argsort(-mu)
-    return _nphi_copies(1, mu[order], wmu[order])
+    return _nphi_copies(nphi, _f32(mu[order]), _f32(wmu[order]), jnu_weights=jnu_weights)
 
 
-def _nphi_copies(nphi, mu, wmu):
+def radau_nodes(k: int):
+    """radau%init (solvers/rt/radau_mod.f90): the k-point Gauss-Radau rule on
+    [-1, 1] with the fixed node -1, mapped to mu = 1 - (x + 1)/2 on [0, 1] with
+    weights w/2, in real(4) as the reference stores them; ascending in mu.  The
+    free nodes are the roots of (P_{k-1} + P_k)/(1 + x) and their weights
+    (1 - x)/(k P_{k-1}(x))^2 (the rule the reference tabulates for k <= 10)."""
+    if not 1 <= k <= 10:
+        raise ValueError("Radau quadrature: 1 <= ntheta <= 10")
+    if k == 1:
+        x, w = np.array([-1.0]), np.array([2.0])
+    else:
+        c = np.zeros(k + 1)
+        c[k - 1] = c[k] = 1.0
+        x = np.sort(np.real(np.polynomial.legendre.legroots(c)))
+        x[0] = -1.0
+        pk1 = np.polynomial.legendre.legval(x, np.eye(k)[k - 1])
+        w = (1.0 - x) / (k * k * pk1 * pk1)
+        w[0] = 2.0 / (k * k)
+    # xi(i) = 1 - (c + d xn(k0(k+1)-i)): the table's nodes from the last down
+    mu = (1.0 - (0.5 + 0.5 * x[::-1])).astype(np.float32)
+    wmu = (0.5 * w[::-1]).astype(np.float32)
+    return mu, wmu
+
+
+def radau_rays(ntheta=2, nphi=1, jnu_weights=False):
+    """set_radau_quadratures (SRC/ray_mod.f90:365-384): Radau mu including 1,
+    descending, azimuths rotated by zrot = pi/4, then nphi_copies."""
+    mu2, wmu2 = radau_nodes(ntheta)
+    mu = mu2[::-1].astype(np.float64)
+    wmu = wmu2[::-1].astype(np.float64)
+    return _nphi_copies(nphi, mu, wmu, zrot=np.full(ntheta, PI / 4.0), jnu_weights=jnu_weights)
+
+
+def _f32(v):
+    return np.asarray(np.asarray(v, np.float32), np.float64)
+
+
+def _nphi_copies(nphi, mu, wmu, zrot=None, jnu_weights=False, one_dimensional=False):
+    """nphi_copies (SRC/ray_mod.f90:392-465)."""
+    nphi = 1 if one_dimensional else nphi
     vec, wts = [], []
-    for m, w in zip(mu, wmu):
+    for k, (m, w) in enumerate(zip(mu, wmu)):
         if m == 1.0:
             vec.append([0.0, 0.0, 1.0])
             wts.append(w)
             continue
         th = math.acos(m)
+        xoff = 0.0 if zrot is None else float(zrot[k])
         for p in range(nphi):
-            ph = 2.0 * math.pi / nphi * p
+            ph = 2.0 * PI / nphi * p + xoff
             v = [math.sin(th) * math.cos(ph), math.sin(th) * math.sin(ph), m]
             v = [0.0 if abs(c) < 1e-3 else c for c in v]
             vec.append(v)
             wts.append(w / nphi)
     vec = np.array(vec, np.float64)
-    wts = np.array(wts, np.float64) * vec[:, 2]
-    return vec, wts
+    wts = np.array(wts, np.float64)
+    if jnu_weights:
+        return np.concatenate([vec, -vec]), np.concatenate([wts, wts]) / 2.0
+    return vec, wts * vec[:, 2]
 
 
 def lte_config(kind: str, seed: int | None = None, nf: int | None = None, window: int = 0,
@@ -431,7 +477,7 @@ def _set_weights(x):
 
 
 def atom_window(atom: dict, nper: int = 25, seed: int = 2, qmax_doppler: float = 5.0, idf_ref: float = 1.8e5,
-                adamp=(1e-3, 1e-1), sums=None) -> dict:
+                adamp=(1e-3, 1e-1), sums=None, transitions=None) -> dict:
     """The atom's transitions on one frequency window holding every transition:
     nper points per line on q = 1 - lam/lam0 in +-qmax_doppler/idf_ref, nper
     points per continuum from 0.3 of its edge wavelength to the edge, merged
@@ -442,7 +488,10 @@ def atom_window(atom: dict, nper: int = 25, seed: int = 2, qmax_doppler: float =
     coefficients of init_einstein_coefficients (bbtrans_mod.f90:55-67) from the
     atom's f values, damping a log-uniform in adamp (grad = a/idf_ref), no van der
     Waals or Stark terms; continua: Kramers-shaped alpha0 (lam/lam_edge)^3.
-    sums: per line sums_over_windows (default none)."""
+    sums: per line sums_over_windows (default none).  transitions: the atom's
+    transition indices the window holds (default all), the reference's split of
+    the spectrum into frequency windows; a transition keeps its damping in every
+    window."""
     rng = np.random.default_rng(seed + 5000)
     nline = atom["nline"]
     ti, tj, ev, g = atom["ti"], atom["tj"], atom["ev"], atom["g"]
@@ -450,29 +499,30 @@ def atom_window(atom: dict, nper: int = 25, seed: int = 2, qmax_doppler: float =
     lam_pts = []
     q0 = np.linspace(-qmax_doppler / idf_ref, qmax_doppler / idf_ref, nper)
     lam0 = np.array([HH * CC / ((ev[tj[k]] - ev[ti[k]]) * EE) * 1e8 for k in range(nrad)])
+    ks = list(range(nrad)) if transitions is None else sorted(int(k) for k in transitions)
     for k in range(nrad):
         if k < nline:
             lam_pts.append(lam0[k] * (1.0 - q0))
         else:
             lam_pts.append(np.geomspace(0.3 * lam0[k], lam0[k] * (1.0 - 1e-7), nper))
-    grid = np.unique(np.concatenate(lam_pts))
+    grid = np.unique(np.concatenate([lam_pts[k] for k in ks]))
     nu = HZ_TO_AA / grid
     nf = grid.size
     li, lj, lb, lr, lo, q, wnu, wq = [], [], [], [], [], [], [], []
     ci, cj, cb, cr, co, alpha, cwnu = [], [], [], [], [], [], []
     off_l = off_c = 0
     f_osc = atom.get("line_f", np.full(nline, 0.1))
-    Aij = np.empty(nline)
-    Bij = np.empty(nline)
-    for k in range(nrad):
+    Aij, Bij, lk = [], [], []
+    for k in ks:
         lo_lam, hi_lam = lam_pts[k].min(), lam_pts[k].max()
         blue = int(np.searchsorted(grid, lo_lam, "left"))
         red = int(np.searchsorted(grid, hi_lam, "right")) - 1
         sl = slice(blue, red + 1)
         if k < nline:
             nu0 = CC / (lam0[k] * 1e-8)
-            Aij[k] = F_CONV * f_osc[k] * nu0**2
-            Bij[k] = C2_2H / nu0**3 * (Aij[k] * H_4PI)
+            Aij.append(F_CONV * f_osc[k] * nu0**2)
+            Bij.append(C2_2H / nu0**3 * (Aij[-1] * H_4PI))
+            lk.append(k)
             qq = (1.0 - grid[sl] / lam0[k]).astype(np.float32)
             li.append(ti[k]); lj.append(tj[k]); lb.append(blue); lr.append(red); lo.append(off_l)
             q.append(qq)
@@ -487,16 +537,21 @@ def atom_window(atom: dict, nper: int = 25, seed: int = 2, qmax_doppler: float =
             off_c += red - blue + 1
     a = 10.0 ** rng.uniform(math.log10(adamp[0]), math.log10(adamp[1]), nline)
     sums = np.zeros(nline, np.uint8) if sums is None else np.asarray(sums, np.uint8)
+    lk = np.asarray(lk, np.int64)
+    nl = lk.size
+    ck = [k for k in ks if k >= nline]
     i32 = lambda v: np.asarray(v, np.int32)
-    return {"nf": nf, "lam": grid, "nu": nu, "nline": nline, "ncont": nrad - nline, "nlevel": atom["nlevel"],
-            "line_i": i32(li), "line_j": i32(lj), "line_ntrans": i32(np.arange(nline)),
-            "line_index": i32(np.arange(nline) + 1), "line_blue": i32(lb), "line_red": i32(lr), "line_off": i32(lo),
-            "q": np.concatenate(q).astype(np.float32), "wnu": np.concatenate(wnu), "wq": np.concatenate(wq),
-            "Bij": Bij, "Aij": Aij, "lower_ev": np.asarray(ev[ti[:nline]], np.float64),
-            "line_active": None, "sums_over_windows": sums,
-            "grad": a / idf_ref, "gw1": np.zeros(nline), "gw2": np.zeros(nline), "gstk": np.zeros(nline),
-            "unsold": np.zeros(nline, np.uint8),
-            "cont_i": i32(ci), "cont_j": i32(cj), "cont_ntrans": i32(np.arange(nline, nrad)),
+    cat = lambda v, dt: np.concatenate(v).astype(dt) if v else np.zeros(0, dt)
+    return {"nf": nf, "lam": grid, "nu": nu, "nline": nl, "ncont": len(ck), "nlevel": atom["nlevel"],
+            "line_i": i32(li), "line_j": i32(lj), "line_ntrans": i32(lk),
+            "line_index": i32(lk + 1), "line_blue": i32(lb), "line_red": i32(lr), "line_off": i32(lo),
+            "q": cat(q, np.float32), "wnu": cat(wnu, np.float64), "wq": cat(wq, np.float64),
+            "Bij": np.asarray(Bij, np.float64), "Aij": np.asarray(Aij, np.float64),
+            "lower_ev": np.asarray(ev[ti[lk]], np.float64),
+            "line_active": None, "sums_over_windows": sums[lk],
+            "grad": a[lk] / idf_ref, "gw1": np.zeros(nl), "gw2": np.zeros(nl), "gstk": np.zeros(nl),
+            "unsold": np.zeros(nl, np.uint8),
+            "cont_i": i32(ci), "cont_j": i32(cj), "cont_ntrans": i32(ck),
             "cont_blue": i32(cb), "cont_red": i32(cr), "cont_off": i32(co),
             "alpha": np.concatenate(alpha).astype(np.float32) if alpha else np.zeros(0, np.float32),
             "cwnu": np.concatenate(cwnu) if cwnu else np.zeros(0),

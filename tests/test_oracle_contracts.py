@@ -221,4 +221,5 @@ def test_quadrature_weights():
     assert w.sum() == pytest.approx(0.5, abs=0.01)     # flux weights integrate mu over mu in [0,1]
     vec, w = synth.gauss_rays(5)
     assert vec.shape == (5, 3)
-    assert w.sum() == pytest.approx(0.5, abs=1e-12)
+    # mu and the weights are default-real (float32) values in the reference's table
+    assert w.sum() == pytest.approx(0.5, abs=1e-7)
