@@ -42,6 +42,7 @@ def _args():
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-fp64", action="store_true")
+    p.add_argument("--no-ali", action="store_true", help="skip the NLTE ALI window measurement")
     p.add_argument("--cube", type=int, default=240, help="cube edge (240 = the configuration; smaller for profiling)")
     return p.parse_args()
 
@@ -218,6 +219,48 @@ def run_reference(a):
     print(json.dumps(line), flush=True)
 
 
+def _nlte_ali(steps=2):
+    """The ALI window of the 3D NLTE configuration, measured beside the headline: the
+    120^3 cube, the 20-level atom, a frequency window holding 10 of its 80 transitions
+    (every eighth: 8 lines and 2 continua, 250 frequencies), both hemispheres of the
+    Lobatto 4x4 directions (26).  A sweep is one ALI iteration's formal solutions with
+    the opacities, J, PsiJ and rate integrals of every direction; the update is the
+    FP64 statistical equilibrium of all 1.728 M cells (fused collision rates, the Ng
+    gate).  Device-resident inputs; CUDA events on torch's stream."""
+    from dispatch_b200 import ali
+    cube, atom, win, vec, wts = ali.cube_problem("c2", transitions=list(range(0, 80, 8)))
+    A = ali.AliWindow(cube, atom, win, vec, wts)
+    A.sweep()
+    A.iter = 1
+    A.update()
+    cur = torch.cuda.current_stream()
+    sw, up, n0 = [], [], m.launch_count()
+    for _ in range(steps):
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        torch.cuda.synchronize()
+        e0.record(cur)
+        A.sweep()
+        e1.record(cur)
+        A.iter += 1
+        rec = A.update()
+        e2.record(cur)
+        torch.cuda.synchronize()
+        sw.append(e0.elapsed_time(e1))
+        up.append(e1.elapsed_time(e2))
+    pts = A.points()
+    sweep_ms = float(np.median(sw))
+    out = {"workload": "c2 3D NLTE ALI window: 120^3 cube, 20-level atom, 10 of 80 transitions (8 lines, "
+                       "2 continua; 250 frequencies), 26 directions (Lobatto 4x4, both hemispheres), "
+                       "short_char with split rates ('largest'), lineq_no_pivot",
+           "unit": UNIT, "value": pts / (sweep_ms / 1e3) / 1e9, "sweep_ms": sweep_ms,
+           "update_ms": float(np.median(up)), "cells_per_s_update": A.ncell / (float(np.median(up)) / 1e3),
+           "ray_pt_nu_per_sweep": pts, "gpu_launches_per_iteration": (m.launch_count() - n0) // steps,
+           "maxerr_last": rec["maxerr"], "data": "synthetic (seeded grey cube, seeded model atom)"}
+    del A
+    torch.cuda.empty_cache()
+    return out
+
+
 def run_b200(a):
     import torch
     import torch.distributed as dist
@@ -345,6 +388,10 @@ def run_b200(a):
                 "solve_fp32_over_fp64": sv64_ms / sv_ms if sv_ms else None,
                 "path": "same kernels in FP64 for units, rotation and solver, one launch per ray and slab"}
 
+    nlte = None
+    if rank == 0 and not a.no_ali:
+        nlte = _nlte_ali()
+
     cpu = None
     if rank == 0 and not a.no_cpu_baseline:
         nu, llam = _window(llam_all, nu_all, nf, wins[a.warmup])
@@ -358,7 +405,7 @@ def run_b200(a):
             "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic (seeded grey cube, random line list)", "config": _workload(nf, a.cube),
             "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline, "cpu_baseline": cpu,
-            "clocks": clocks, "stages": stages, "fp64_plain": fp64}
+            "clocks": clocks, "stages": stages, "fp64_plain": fp64, "nlte_ali": nlte}
     print(json.dumps(line), flush=True)
 
 

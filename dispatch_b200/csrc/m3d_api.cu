@@ -759,8 +759,16 @@ int solve_impl(int solver, const m3d_slab_t *s, unsigned flags, T *work, T *psi,
       const int zs = a.dir > 0 ? 1 : a.nz;
       if (solver == M3D_SOLVER_SHORT_LINEAR) {
         const T dsup05 = (T)(0.5f * (float)dsup);
+        const size_t smem = sizeof(T) * 3 * (SC_TX + 3) * (SC_TY + 3) * SC_TF;
+        static bool attr_set[2] = {false, false};
+        if (!attr_set[sizeof(T) == 8]) {
+          CUDA_TRY(cudaFuncSetAttribute(k_short_char_tile<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+          attr_set[sizeof(T) == 8] = true;
+        }
+        const int tgrid = ((a.nx + SC_TX - 1) / SC_TX) * ((a.ny + SC_TY - 1) / SC_TY) * ((a.nf + SC_TF - 1) / SC_TF);
         for (int i = 0, z = zs; i < a.nz; i++, z += a.dir)
-          LAUNCH_S(M3D_STAGE_SOLVE, k_short_char_plane<T>, grid, block, 0, a, z, work, psi, irem, esc, xt, yt, kx, ky, dsup05);
+          LAUNCH_S(M3D_STAGE_SOLVE, k_short_char_tile<T>, tgrid, 256, smem, a, z, work, psi, irem, esc, xt, yt, kx, ky,
+                   dsup05);
       } else {
         if (!chi500 || !chi500_up || !g500) return fail(M3D_EINVAL, "linear2 needs chi500, chi500_up and g500");
         const float hx = 2.0f * kx.w + (-kx.x + kx.z), hy = 2.0f * ky.w + (-ky.x + ky.z);

@@ -650,59 +650,100 @@ __global__ void k_upstream_boundary(int nf, int nx, int ny, int nz, int dir, T *
   }
 }
 
-// short_char / short_char2 on plane z: each thread forms the row sums of its
-// four upwind rows itself, in the reference's order (row pass, then column)
+
+// short_char (rt_solvers_mod.f90:19-189) on one plane z: the 4x4 cubic upwind
+// interpolation of chi, S and I (the row pass, then the column pass), clamped
+// below by the inner 2x2 minimum; dt = dsup/2 (chi_up + chi) capped at
+// -maser_dtau_max; the linear step, I clamped to +-maser_Inu_max; Psi/chi, and Irem
+// and the escape factor for split rates.  Tiled: a block takes SC_TX x SC_TY
+// columns of SC_TF frequencies and stages the upstream (SC_TX+3) x (SC_TY+3)
+// patch of chi, S and I in shared memory once (every upstream value feeds up to
+// 16 stencils).  The upwind
+// tables are xt[4x+ii] = (xt[0] + x + ii) mod nx, so a tile's stencils cover
+// consecutive upstream columns starting at xt[4 x0].
+constexpr int SC_TX = 8, SC_TY = 8, SC_TF = 32;
+
 template <typename T>
-__global__ void k_short_char_plane(SlabArgs s, int z, T *work, T *psi, T *irem, T *esc, const int *xt, const int *yt,
-                                   float4 kx, float4 ky, T dsup05) {
-  const size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(256) k_short_char_tile(SlabArgs s, int z, T *work, T *psi, T *irem, T *esc,
+                                                         const int *xt, const int *yt, float4 kx, float4 ky,
+                                                         T dsup05) {
+  extern __shared__ __align__(16) unsigned char sc_smem[];
+  T *up = (T *)sc_smem;  // [3][SC_TY+3][SC_TX+3][SC_TF]
+  constexpr int PX = SC_TX + 3, PY = SC_TY + 3;
+  __shared__ int sxu[PX], syu[PY];
   const int nf = s.nf, nx = s.nx, ny = s.ny, nz = s.nz, dir = s.dir;
-  if (g >= (size_t)nf * nx * ny) return;
-  const int f = (int)(g % nf), x = (int)((g / nf) % nx), y = (int)(g / ((size_t)nf * nx));
+  const int ntx = (nx + SC_TX - 1) / SC_TX, nty = (ny + SC_TY - 1) / SC_TY;
+  const int bt = blockIdx.x;
+  const int tx = bt % ntx, ty = (bt / ntx) % nty, fc = bt / (ntx * nty);
+  const int x0 = tx * SC_TX, y0 = ty * SC_TY, f0 = fc * SC_TF;
   const int zup = z - dir;
+  if (threadIdx.x < PX) sxu[threadIdx.x] = (xt[4 * x0] + threadIdx.x) % nx;
+  else if (threadIdx.x < PX + PY) syu[threadIdx.x - PX] = (yt[4 * y0] + threadIdx.x - PX) % ny;
+  __syncthreads();
+  // one warp per upstream row of SC_TF frequencies (coalesced)
+  {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const bool fin = f0 + lane < nf && lane < SC_TF;
+    const size_t plane = (size_t)nf * nx * ny, slot = plane * (nz + 2);
+    for (int row = wid; row < 3 * PY * PX; row += nw) {
+      const int xi = row % PX, yj = (row / PX) % PY, i = row / (PX * PY);
+      const size_t base = slot * i + plane * zup + (size_t)nf * (sxu[xi] + (size_t)nx * syu[yj]) + f0;
+      if (fin) up[row * SC_TF + lane] = work[base + lane];
+    }
+  }
+  __syncthreads();
   const T dtmax = -(T)s.maser_dtau_max, Imax = (T)s.maser_Inu_max;
   const T k_x[4] = {(T)kx.x, (T)kx.y, (T)kx.z, (T)kx.w};
   const T k_y[4] = {(T)ky.x, (T)ky.y, (T)ky.z, (T)ky.w};
-  T up[3], mn[3];
-  for (int i = 0; i < 3; i++) {
-    T r = 0;
-    for (int jj = 0; jj < 4; jj++) {
-      const int yu = yt[4 * y + jj];
-      T rr = 0;
-      for (int ii = 0; ii < 4; ii++) rr = fma_t(k_x[ii], work[iw(f, xt[4 * x + ii], yu, zup, i, nf, nx, ny, nz)], rr);
-      r = fma_t(k_y[jj], rr, r);
-    }
-    T m = (T)FLT_MAX;
-    if (sizeof(T) == 8) m = (T)DBL_MAX;
-    for (int jj = 1; jj <= 2; jj++)
-      for (int ii = 1; ii <= 2; ii++) m = tmin(m, work[iw(f, xt[4 * x + ii], yt[4 * y + jj], zup, i, nf, nx, ny, nz)]);
-    up[i] = r;
-    mn[i] = m;
-  }
-  const T xxup = tmax(up[0], mn[0]), ssup = tmax(up[1], mn[1]), Inuup = tmax(up[2], mn[2]);
-  const size_t o = iw(f, x, y, z, 0, nf, nx, ny, nz);
   const size_t k1 = (size_t)nf * nx * ny * (nz + 2);
-  const T xx = work[o], ss = work[o + k1];
-  T dt = dsup05 * (xxup + xx);
-  dt = tmax(dt, dtmax);
-  T E, W, Psi, Esc;
-  linear_weights(dt, E, W, Psi, Esc);
-  T Inu = fma_t(Psi, ss, fma_t(W, ssup, Inuup * E));
-  const size_t p = ip(f, x, y, z, nf, nx, ny);
-  if (s.split_rates) {
-    const bool off = dt <= 0 || xx <= 0 || tabs(Inu) > Imax;
-    const T Irem = fma_t(W, ssup, Inuup * E);
-    Inu = tmax(-Imax, tmin(Imax, Inu));
-    Psi = off ? (T)0 : Psi;
-    irem[p] = off ? Inu : Irem;
-    esc[p] = off ? (T)1 : Esc;
-  } else {
-    Inu = tmax(-Imax, tmin(Imax, Inu));
+  for (int pnt = threadIdx.x; pnt < SC_TX * SC_TY * SC_TF; pnt += blockDim.x) {
+    const int f = pnt % SC_TF, xl = (pnt / SC_TF) % SC_TX, yl = pnt / (SC_TF * SC_TX);
+    const int x = x0 + xl, y = y0 + yl;
+    if (x >= nx || y >= ny || f0 + f >= nf) continue;
+    T upv[3], mn[3];
+    for (int i = 0; i < 3; i++) {
+      const T *u = up + (size_t)i * PY * PX * SC_TF;
+      T r = 0;
+      for (int jj = 0; jj < 4; jj++) {
+        const T *row = u + ((size_t)(yl + jj) * PX + xl) * SC_TF + f;
+        T rr = 0;
+        for (int ii = 0; ii < 4; ii++) rr = fma_t(k_x[ii], row[ii * SC_TF], rr);
+        r = fma_t(k_y[jj], rr, r);
+      }
+      T m = (T)FLT_MAX;
+      if (sizeof(T) == 8) m = (T)DBL_MAX;
+      for (int jj = 1; jj <= 2; jj++)
+        for (int ii = 1; ii <= 2; ii++) m = tmin(m, u[((size_t)(yl + jj) * PX + xl + ii) * SC_TF + f]);
+      upv[i] = r;
+      mn[i] = m;
+    }
+    const T xxup = tmax(upv[0], mn[0]), ssup = tmax(upv[1], mn[1]), Inuup = tmax(upv[2], mn[2]);
+    const size_t o = iw(f0 + f, x, y, z, 0, nf, nx, ny, nz);
+    const T xx = work[o], ss = work[o + k1];
+    T dt = dsup05 * (xxup + xx);
+    dt = tmax(dt, dtmax);
+    T E, W, Psi, Esc;
+    linear_weights(dt, E, W, Psi, Esc);
+    T Inu = fma_t(Psi, ss, fma_t(W, ssup, Inuup * E));
+    const size_t p = ip(f0 + f, x, y, z, nf, nx, ny);
+    if (s.split_rates) {
+      const bool off = dt <= 0 || xx <= 0 || tabs(Inu) > Imax;
+      const T Irem = fma_t(W, ssup, Inuup * E);
+      Inu = tmax(-Imax, tmin(Imax, Inu));
+      Psi = off ? (T)0 : Psi;
+      irem[p] = off ? Inu : Irem;
+      esc[p] = off ? (T)1 : Esc;
+    } else {
+      Inu = tmax(-Imax, tmin(Imax, Inu));
+    }
+    work[o + 2 * k1] = Inu;
+    if (s.get_psi) psi[p] = (dt > 0 && xx > 0) ? Psi / xx : (T)0;
   }
-  work[o + 2 * k1] = Inu;
-  if (s.get_psi) psi[p] = (dt > 0 && xx > 0) ? Psi / xx : (T)0;
 }
 
+// short_char2 (rt_solvers_mod.f90:224-507) on plane z: each thread forms the row
+// sums of its four upwind rows itself, in the reference's order (row pass, then
+// column pass)
 template <typename T>
 __global__ void k_short_char2_plane(SlabArgs s, int z, T *work, T *psi, T *irem, T *esc, const int *xt, const int *yt,
                                     float4 kx, float4 ky, float hx, float hy, const float *chi500,

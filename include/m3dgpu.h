@@ -157,7 +157,9 @@ int m3d_work_to_transfer_units(int nf, int ncell, float *w1, float *w2, const fl
  * applies rotate_array to work(:,:,:,1:nz,1:2), which then holds the sheared
  * chi and Snu as in the reference; rot_ds_code, rot_bot2pivot, rot_offset are
  * rotate_array's cell size [code units], pivot height above the slab bottom and
- * ray_offset [cells]. */
+ * ray_offset [cells].  The short-characteristics solvers need the upwind point
+ * within one cell horizontally, |vec[0]/vec[2]| ds[2] <= ds[0] and the same in y
+ * (set_stencil, ray_mod.f90:493-512); other directions return M3D_EINVAL. */
 int m3d_formal_solve(int solver, const m3d_slab_t *slab, void *work, void *psi, void *irem,
                      void *escape, const float *chi500, const float *chi500_up, const float *g500,
                      const int *eta_row, const unsigned char *eta_mask, const double *rot_ds_code,
