@@ -23,7 +23,7 @@ __all__ = ["M3DError", "lib", "Slab", "LineList", "Species", "Atmos", "init", "L
            "DEVICE_PTRS", "FP64", "GET_PSI", "SPLIT_RATES", "LINE_DIAG", "ROTATE"]
 
 # include/m3dgpu.h
-DEVICE_PTRS, FP64, GET_PSI, SPLIT_RATES, LINE_DIAG, ROTATE = 0x1, 0x2, 0x4, 0x8, 0x10, 0x20
+DEVICE_PTRS, FP64, GET_PSI, SPLIT_RATES, LINE_DIAG, ROTATE, AUTOTUNE = 0x1, 0x2, 0x4, 0x8, 0x10, 0x20, 0x40
 LINEAR, LINEAR2, QUADRATIC, SHORT_LINEAR, SHORT_LINEAR2 = range(5)
 BND_MEM, BND_ZERO, BND_PCHIP, BND_LTE = range(4)
 
@@ -36,7 +36,8 @@ EXPORTS = ("m3d_init", "m3d_free", "m3d_last_error", "m3d_version", "m3d_set_str
            "m3d_stateq_update", "m3d_ng_accumulate", "m3d_ng_extrapolate", "m3d_bb_damping", "m3d_bf_opacity",
            "m3d_bb_opacity", "m3d_work_to_transfer_units_split", "m3d_bb_rates", "m3d_bf_rates",
            "m3d_integrate_rates", "m3d_normalize_profiles", "m3d_combine_twins", "m3d_update_eta_mask",
-           "m3d_lte_populations", "m3d_particle_fields", "m3d_lte_emission")
+           "m3d_lte_populations", "m3d_particle_fields", "m3d_lte_emission", "m3d_col_plan_create",
+           "m3d_col_plan_sweep", "m3d_col_plan_fields", "m3d_col_plan_destroy")
 
 
 class M3DError(RuntimeError):

@@ -23,11 +23,13 @@ z = 0 the bottom plane; per-level (nlevel, ncell).
 """
 from __future__ import annotations
 
+import ctypes as C
 from dataclasses import dataclass, field
 
 import numpy as np
 
-from . import (BND_PCHIP, BND_ZERO, SHORT_LINEAR, M3DError, init, make_slab, nlte, rt, stateq, synth)
+from . import (AUTOTUNE, BND_PCHIP, BND_ZERO, SHORT_LINEAR, M3DError, check, init, lib, make_slab, nlte,
+               order_after_torch, ptr, rt, stateq, synth)
 
 
 @dataclass
@@ -52,7 +54,106 @@ class AliParams:
     ng: stateq.NgParams = field(default_factory=stateq.NgParams)
 
 
-class AliWindow:
+class _AtomIteration:
+    """The model atom's state on the cells of a sweep, and the update between sweeps
+    (nlte_patch_t%execute: normalize_profiles, update_populations, the convergence
+    bookkeeping and ng_acceleration)."""
+
+    def _init_atom(self, atom: dict, wins: list, temp, ne, nH, abundance, awgt: float, vmic_kms: float, dev):
+        import torch
+
+        f32 = lambda a: torch.as_tensor(np.ascontiguousarray(a, np.float32), device=dev)
+        f64 = lambda a: torch.as_tensor(np.ascontiguousarray(a, np.float64), device=dev)
+        temp = np.ascontiguousarray(temp, np.float32).ravel()
+        ne = np.asarray(ne, np.float64).ravel()
+        nH = np.asarray(nH, np.float64).ravel()
+        nc = temp.size
+        self.atom = atom
+        self.ncell = nc
+        totn0 = 10.0 ** (np.asarray(abundance, np.float64) - 12.0) * nH
+        nstar, totn = synth.lte_populations(atom, temp, ne, totn0)
+        self.temp32 = temp
+        self.temp, self.ne = f64(temp), f64(ne)
+        self.e_kT = f64(synth.EE / synth.BK / temp.astype(np.float64))
+        self.nstar, self.totn = f64(nstar), f64(totn)
+        self.pop_ratio = torch.ones(nc, dtype=torch.float64, device=dev)
+        idf = synth.inverse_doppler_factor(temp, awgt, vmic_kms).astype(np.float32)
+        self.idf_host = idf
+        self.inv_df = f32(idf)
+        vbar2 = synth.compute_vbar2(temp, awgt).astype(np.float32)
+        ne32, nh32 = ne.astype(np.float32), nH.astype(np.float32)
+        stark = (ne32 * temp ** np.float32(1.0 / 6.0)).astype(np.float32)
+        uns = (vbar2.astype(np.float64) ** 0.3 * nH).astype(np.float32)
+        self.adamps = [f32(nlte.bb_damping(w, ne32, nh32, vbar2, stark, uns, idf)) for w in wins]
+        nl = self.nlevel = int(atom["nlevel"])
+        self.nrad = len(atom["ti"])
+        self.b = torch.ones((nl, nc), dtype=torch.float64, device=dev)
+        self.oldb = torch.zeros((3, nl, nc), dtype=torch.float64, device=dev)
+        self.gamma_ij = torch.zeros((self.nrad, nc), dtype=torch.float32, device=dev)
+        self.gamma_ji = torch.zeros_like(self.gamma_ij)
+        sums = np.zeros(int(atom["nline"]), np.uint8)
+        for w in wins:
+            sums[np.asarray(w["line_ntrans"], np.int64)] = np.asarray(w["sums_over_windows"], np.uint8)
+        self.has_wphi = sums
+        # profile integrals of the lines whose windows are summed (rows of the others stay 0)
+        self.wphi = torch.zeros((max(int(atom["nline"]), 1), nc), dtype=torch.float32, device=dev)
+        self.ng = stateq.NgState(params=self.p.ng)
+        self.iter = 0
+        self.history: list[dict] = []
+        self._sweep_maxerr = 0.0
+        self._last_maxerr = 0.0
+        self._global = 0.0
+        self.converged = False
+
+    def sweep(self) -> None:
+        raise NotImplementedError
+
+    # ---- nlte_patch_t%execute ----------------------------------------------------------
+    def update(self) -> dict:
+        """The atom update of iteration self.iter (>= 1): returns its record."""
+        p, it = self.p, self.iter
+        nlte.normalize_profiles(self.atom, self.nstar, self.wphi, self.gamma_ij, self.gamma_ji, self.has_wphi,
+                                first_iter=it == 1)
+        stateq.shift_oldb(self.oldb, self.b)
+        res, _ = stateq.stateq_update(self.atom, self.b, self.nstar, self.totn, self.e_kT, self.gamma_ij,
+                                      self.gamma_ji, temp=self.temp, ne=self.ne, solver=p.se_solver,
+                                      max_update=p.max_update, sor_w=p.sor_w, min_pop_frac=p.min_pop_frac)
+        maxerr = float(res["maxerr"])
+        self.ng.count_clamped(res["nclamp"], res["ntot"])
+        rec = {"iter": it, "maxerr": maxerr, "epos_cell": int(res["epos_cell"]), "epos_level": int(res["epos_level"]),
+               "ng": None}
+        convmax = 0.1 * max(p.convlim, 0.0)
+        atom_converged = abs(maxerr) < convmax
+        if p.ng_step >= 0 and not atom_converged:
+            ng = stateq.ng_acceleration(self.ng, it, self._global, p.convlim, self.b, self.oldb, self.nstar,
+                                        self.totn, extrapolate=abs(maxerr) >= p.convlim, ng_step=p.ng_step,
+                                        ng_start=p.ng_start)
+            rec["ng"] = ng
+        # the sweep bookkeeping of one patch: the Ng gate reads the change of the
+        # iteration before the last (self%global = last_maxerr)
+        self._last_maxerr = self._sweep_maxerr
+        self._sweep_maxerr = maxerr
+        self._global = self._last_maxerr
+        applied = bool(rec["ng"] and rec["ng"].get("applied"))
+        self.converged = atom_converged or (0.0 < abs(maxerr) < p.convlim and not applied)
+        self.gamma_ij.zero_()
+        self.gamma_ji.zero_()
+        self.history.append(rec)
+        return rec
+
+    def run(self, maxiter: int) -> list[dict]:
+        """Iteration 0 (LTE start, b = 1) and up to maxiter updates, each followed by
+        the next iteration's formal solutions unless it converged."""
+        if self.iter == 0:
+            self.sweep()
+        while self.iter < maxiter and not self.converged:
+            self.iter += 1
+            self.update()
+            if not self.converged and self.iter < maxiter:
+                self.sweep()
+        return self.history
+
+class AliWindow(_AtomIteration):
     """One frequency window of a model atom on a periodic cube, device resident.
 
     cube: temp, ne, nH (ncell,), chi_c (ncell,) grey continuum [1/cm], vz (ncell,)
@@ -91,41 +192,18 @@ class AliWindow:
         f32 = lambda a: torch.as_tensor(np.ascontiguousarray(a, np.float32), device=dev)
         f64 = lambda a: torch.as_tensor(np.ascontiguousarray(a, np.float64), device=dev)
 
-        temp = np.ascontiguousarray(cube["temp"], np.float32).ravel()
-        ne = np.asarray(cube["ne"], np.float64).ravel()
-        nH = np.asarray(cube["nH"], np.float64).ravel()
-        totn0 = 10.0 ** (abundance - 12.0) * nH
-        nstar, totn = synth.lte_populations(atom, temp, ne, totn0)
-        self.temp, self.ne = f64(temp), f64(ne)
-        self.e_kT = f64(synth.EE / synth.BK / temp.astype(np.float64))
-        self.nstar, self.totn = f64(nstar), f64(totn)
-        self.pop_ratio = torch.ones(nc, dtype=torch.float64, device=dev)
-        idf = synth.inverse_doppler_factor(temp, awgt, vmic_kms).astype(np.float32)
-        self.inv_df = f32(idf)
-        vbar2 = synth.compute_vbar2(temp, awgt).astype(np.float32)
-        ne32, nh32 = ne.astype(np.float32), nH.astype(np.float32)
-        stark = (ne32 * temp ** np.float32(1.0 / 6.0)).astype(np.float32)
-        uns = (vbar2.astype(np.float64) ** 0.3 * nH).astype(np.float32)
-        self.adamp = f32(nlte.bb_damping(win, ne32, nh32, vbar2, stark, uns, idf))
+        self._init_atom(atom, [win], cube["temp"], cube["ne"], cube["nH"], abundance, awgt, vmic_kms, dev)
+        self.adamp = self.adamps[0]
+        nc = self.ncell
+        temp = self.temp32
         vz = np.ascontiguousarray(cube["vz"], np.float32).ravel()
         self.vproj = [f32(vz * np.float32(v[2])) for v in vec]
         self.beta, self.Bnu = rt.lte_background(f64(win["nu"]), f32(temp))
         self.chi_c = f32(np.asarray(cube["chi_c"], np.float32).ravel())[:, None].expand(nc, self.nf).contiguous()
 
-        nl = self.nlevel = int(atom["nlevel"])
-        self.nrad = len(atom["ti"])
-        self.b = torch.ones((nl, nc), dtype=torch.float64, device=dev)
-        self.oldb = torch.zeros((3, nl, nc), dtype=torch.float64, device=dev)
-        self.gamma_ij = torch.zeros((self.nrad, nc), dtype=torch.float32, device=dev)
-        self.gamma_ji = torch.zeros_like(self.gamma_ij)
         nw = int(win["nline"]) + int(win["ncont"])
         self.gw_ij = torch.zeros((max(nw, 1), nc), dtype=torch.float32, device=dev)
         self.gw_ji = torch.zeros_like(self.gw_ij)
-        sums = np.zeros(int(atom["nline"]), np.uint8)
-        sums[np.asarray(win["line_ntrans"], np.int64)] = np.asarray(win["sums_over_windows"], np.uint8)
-        self.has_wphi = sums
-        # profile integrals of the lines whose windows are summed (rows of the others stay 0)
-        self.wphi = torch.zeros((max(int(atom["nline"]), 1), nc), dtype=torch.float32, device=dev)
 
         shp = (nc, self.nf)
         self.work = torch.zeros((3, self.nz + 2, self.ny, self.nx, self.nf), dtype=torch.float32, device=dev)
@@ -142,13 +220,6 @@ class AliWindow:
         self.slabs = [make_slab(self.nf, self.nx, self.ny, self.nz, 1 if v[2] > 0 else -1, self.ds, v, get_psi=True,
                                 split_rates=self.p.split_rates, maser_dtau_max=self.p.maser_dtau_max,
                                 maser_Inu_max=self.p.maser_Inu_max) for v in vec]
-        self.ng = stateq.NgState(params=self.p.ng)
-        self.iter = 0
-        self.history: list[dict] = []
-        self._sweep_maxerr = 0.0
-        self._last_maxerr = 0.0
-        self._global = 0.0
-        self.converged = False
 
     # ---- rt_patch_t%execute, ALI branch -------------------------------------------------
     def sweep(self) -> None:
@@ -198,54 +269,139 @@ class AliWindow:
         nlte.combine_twins(self.J[0], self.J[1])
         nlte.combine_twins(self.PsiJ[0], self.PsiJ[1])
 
-    # ---- nlte_patch_t%execute ----------------------------------------------------------
-    def update(self) -> dict:
-        """The atom update of iteration self.iter (>= 1): returns its record."""
-        p, it = self.p, self.iter
-        nlte.normalize_profiles(self.atom, self.nstar, self.wphi, self.gamma_ij, self.gamma_ji, self.has_wphi,
-                                first_iter=it == 1)
-        stateq.shift_oldb(self.oldb, self.b)
-        res, _ = stateq.stateq_update(self.atom, self.b, self.nstar, self.totn, self.e_kT, self.gamma_ij,
-                                      self.gamma_ji, temp=self.temp, ne=self.ne, solver=p.se_solver,
-                                      max_update=p.max_update, sor_w=p.sor_w, min_pop_frac=p.min_pop_frac)
-        maxerr = float(res["maxerr"])
-        self.ng.count_clamped(res["nclamp"], res["ntot"])
-        rec = {"iter": it, "maxerr": maxerr, "epos_cell": int(res["epos_cell"]), "epos_level": int(res["epos_level"]),
-               "ng": None}
-        convmax = 0.1 * max(p.convlim, 0.0)
-        atom_converged = abs(maxerr) < convmax
-        if p.ng_step >= 0 and not atom_converged:
-            ng = stateq.ng_acceleration(self.ng, it, self._global, p.convlim, self.b, self.oldb, self.nstar,
-                                        self.totn, extrapolate=abs(maxerr) >= p.convlim, ng_step=p.ng_step,
-                                        ng_start=p.ng_start)
-            rec["ng"] = ng
-        # the sweep bookkeeping of one patch: the Ng gate reads the change of the
-        # iteration before the last (self%global = last_maxerr)
-        self._last_maxerr = self._sweep_maxerr
-        self._sweep_maxerr = maxerr
-        self._global = self._last_maxerr
-        applied = bool(rec["ng"] and rec["ng"].get("applied"))
-        self.converged = atom_converged or (0.0 < abs(maxerr) < p.convlim and not applied)
-        self.gamma_ij.zero_()
-        self.gamma_ji.zero_()
-        self.history.append(rec)
-        return rec
-
-    def run(self, maxiter: int) -> list[dict]:
-        """Iteration 0 (LTE start, b = 1) and up to maxiter updates, each followed by
-        the next iteration's formal solutions unless it converged."""
-        if self.iter == 0:
-            self.sweep()
-        while self.iter < maxiter and not self.converged:
-            self.iter += 1
-            self.update()
-            if not self.converged and self.iter < maxiter:
-                self.sweep()
-        return self.history
-
     def points(self) -> int:
         """Ray-point-frequency visits of one sweep (both twins)."""
         return len(self.slabs) * self.ncell * self.nf
+
+
+class _ColProblem(C.Structure):
+    """m3d_col_problem_t."""
+
+    _fields_ = [("ncol", C.c_int), ("ncell", C.c_int), ("col_off", C.c_void_p), ("dz", C.c_void_p),
+                ("nray", C.c_int), ("mu", C.c_void_p), ("wmu", C.c_void_p), ("b", C.c_void_p),
+                ("nstar", C.c_void_p), ("pop_ratio", C.c_void_p), ("e_kT", C.c_void_p), ("inv_df", C.c_void_p),
+                ("vz", C.c_void_p), ("chi_c", C.c_void_p), ("temp", C.c_void_p), ("maser_dtau_max", C.c_double),
+                ("maser_Inu_max", C.c_double), ("maser_chi_floor", C.c_double), ("preconditioning", C.c_int),
+                ("bottom", C.c_int), ("nline_atom", C.c_int), ("nrad_atom", C.c_int)]
+
+
+class AliColumns(_AtomIteration):
+    """The batched 1.5D ALI: columns of uneven depth for one model atom over its
+    frequency windows, through the library's column plan (m3d_col_plan_*).
+
+    cols: synth.column_set (cells of every column back to back, abundance variants
+    packed as further columns); wins: the atom's frequency windows
+    (synth.atom_window with transition subsets); mu, wmu: the directions with
+    mean-intensity weights, the upward half first (synth.radau_rays(2,
+    jnu_weights=True)[...,2] in 1D).  Each sweep is the plan's fixed launch
+    sequence, replayed from a CUDA graph when use_graph; the update between sweeps
+    is the base class's.  With autotune the plan times the column solver's launch
+    shapes once.
+    """
+
+    def __init__(self, cols: dict, atom: dict, wins: list, mu, wmu, params: AliParams | None = None,
+                 abundance: float = 7.5, awgt: float = 56.0, vmic_kms: float = 1.0, use_graph: bool = True,
+                 autotune: bool = True, device: str = "cuda"):
+        import torch
+
+        init()
+        self.p = params or AliParams()
+        dev = torch.device(device)
+        self.dev = dev
+        self.wins = list(wins)
+        self.use_graph = bool(use_graph)
+        abund = abundance + np.asarray(cols.get("abund_dex", 0.0), np.float64)
+        self._init_atom(atom, self.wins, cols["temp"], cols["ne"], cols["nH"], abund, awgt, vmic_kms, dev)
+        nc = self.ncell
+        f32 = lambda a: torch.as_tensor(np.ascontiguousarray(a, np.float32), device=dev)
+        self.col_off = torch.as_tensor(np.asarray(cols["col_off"], np.int32), device=dev)
+        self.dz = torch.as_tensor(np.asarray(cols["dz"], np.float64), device=dev)
+        self.ncol = int(self.col_off.numel()) - 1
+        self.vz, self.chi_c, self.tempd = f32(cols["vz"]), f32(cols["chi_c"]), f32(cols["temp"])
+        self.mu = np.ascontiguousarray(mu, np.float64)
+        self.wmu = np.ascontiguousarray(wmu, np.float32)
+        self.nf = [int(w["nf"]) for w in self.wins]
+        prob = _ColProblem(self.ncol, nc, self.col_off.data_ptr(), self.dz.data_ptr(), len(self.mu),
+                           self.mu.ctypes.data, self.wmu.ctypes.data, self.b.data_ptr(), self.nstar.data_ptr(),
+                           self.pop_ratio.data_ptr(), self.e_kT.data_ptr(), self.inv_df.data_ptr(),
+                           self.vz.data_ptr(), self.chi_c.data_ptr(), self.tempd.data_ptr(), self.p.maser_dtau_max,
+                           self.p.maser_Inu_max, self.p.maser_chi_floor, int(self.p.preconditioning),
+                           int(self.p.bottom), int(atom["nline"]), self.nrad)
+        nw = len(self.wins)
+        ws = (nlte.AtomWindow * nw)()
+        self._keep = []
+        nus, twos = [], []
+        for i, w in enumerate(self.wins):
+            st, keep = nlte.make_window(w)
+            ws[i] = st
+            self._keep.append(keep)
+            nus.append(np.ascontiguousarray(w["nu"], np.float64))
+            twos.append(np.ascontiguousarray(w["twohnu3_c2"], np.float32))
+        self._keep += [nus, twos]
+        pv = lambda arrs: (C.c_void_p * nw)(*[a.ctypes.data for a in arrs])
+        ad = (C.c_void_p * nw)(*[a.data_ptr() if a.numel() else None for a in self.adamps])
+        order_after_torch(self.b)
+        self._plan = C.c_void_p()
+        check(lib().m3d_col_plan_create(C.byref(prob), C.c_int(nw), ws, pv(nus), pv(twos), ad,
+                                        C.c_uint(AUTOTUNE if autotune else 0), C.byref(self._plan)),
+              "m3d_col_plan_create")
+        nfo, blk = C.c_int(), C.c_int()
+        check(lib().m3d_col_plan_fields(self._plan, None, None, C.byref(nfo), C.byref(blk)), "m3d_col_plan_fields")
+        self.solver_block = blk.value
+
+    def sweep(self) -> None:
+        """The formal solutions and rate sums of every window and direction."""
+        order_after_torch(self.b)
+        check(lib().m3d_col_plan_sweep(self._plan, C.c_int(int(self.iter == 0)), ptr(self.gamma_ij),
+                                       ptr(self.gamma_ji), ptr(self.wphi), C.c_int(int(self.use_graph))),
+              "m3d_col_plan_sweep")
+
+    def fields(self):
+        """(J, PsiJ) of the last window, 2 x (ncell, nf) torch tensors (the twins combined)."""
+        import torch
+
+        n = (2, self.ncell, self.nf[-1])
+        J = torch.empty(n, dtype=torch.float32, device=self.dev)
+        P = torch.empty_like(J)
+        order_after_torch(J)
+        check(lib().m3d_col_plan_fields(self._plan, ptr(J), ptr(P), None, None), "m3d_col_plan_fields")
+        return J, P
+
+    def points(self) -> int:
+        """Ray-point-frequency visits of one sweep over every window."""
+        return len(self.mu) * self.ncell * sum(self.nf)
+
+    def close(self) -> None:
+        if getattr(self, "_plan", None) is not None and self._plan.value:
+            lib().m3d_col_plan_destroy(self._plan)
+            self._plan = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def column_problem(kind: str = "small", seed: int = 3, ncol: int = 6, depth=(8, 16), nz: int = 16, nxy: int = 4,
+                   nbound: int = 5, nline: int = 6, nper: int = 25, nwin: int = 2, variants=(0.0,),
+                   ntheta: int = 2):
+    """(cols, atom, wins, mu, wmu) of the batched 1.5D configuration: columns of
+    uneven depth from a seeded cube, a model atom split into nwin frequency windows
+    (its transitions dealt round-robin), and Radau directions with mean-intensity
+    weights.  kind 'c3': 4096 columns of 60-256 cells from a 64 x 64 x 256 cube,
+    the 20-level atom (nline 60) in windows of about 10 transitions, abundance
+    variants 0 and +-0.2 dex."""
+    if kind == "c3":
+        ncol, depth, nz, nxy = 4096, (60, 256), 256, 64
+        variants = (0.0, 0.2, -0.2)
+    cols = synth.column_set(seed, ncol=ncol, depth=depth, nz=nz, nxy=nxy, variants=variants)
+    atom = synth.model_atom(seed, nbound=nbound, nline=nline)
+    nrad = len(atom["ti"])
+    wins = [synth.atom_window(atom, nper=nper, seed=seed, transitions=list(range(k, nrad, nwin)))
+            for k in range(nwin)]
+    vec, wts = synth.radau_rays(ntheta, 1, jnu_weights=True)
+    return cols, atom, wins, vec[:, 2].copy(), wts
 
 
 def cube_problem(kind: str = "small", seed: int = 2, nx: int = 8, ny: int = 8, nz: int = 12, nbound: int = 6,
@@ -273,4 +429,4 @@ def cube_problem(kind: str = "small", seed: int = 2, nx: int = 8, ny: int = 8, n
     return cube, atom, win, vec, wts
 
 
-__all__ = ["AliParams", "AliWindow", "cube_problem"]
+__all__ = ["AliParams", "AliWindow", "AliColumns", "cube_problem", "column_problem"]

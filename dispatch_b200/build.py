@@ -19,7 +19,7 @@ LIB = os.path.join(HERE, "libm3dgpu.so")
 SOURCES = ["m3d_api.cu"]
 HEADERS = ["m3d_math.cuh", "m3d_qlg.cuh", "m3d_kernels.cuh", "m3d_pipeline.cuh", "m3d_stateq.cuh",
            "m3d_stateq_api.inc", "m3d_nlte.cuh", "m3d_nlte_api.inc",
-           "m3d_aux.cuh", "m3d_aux_api.inc"]
+           "m3d_aux.cuh", "m3d_aux_api.inc", "m3d_columns.cuh", "m3d_columns_api.inc"]
 
 
 def nvcc() -> str:

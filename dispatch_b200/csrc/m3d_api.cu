@@ -10,6 +10,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -19,6 +20,7 @@
 #include "m3d_stateq.cuh"
 #include "m3d_nlte.cuh"
 #include "m3d_aux.cuh"
+#include "m3d_columns.cuh"
 
 using namespace m3d;
 
@@ -1149,6 +1151,7 @@ int m3d_lte_synthesis(const m3d_atmos_t *atm, int nf, const double *nu, const do
 #include "m3d_stateq_api.inc"
 #include "m3d_nlte_api.inc"
 #include "m3d_aux_api.inc"
+#include "m3d_columns_api.inc"
 
 // ===========================================================================
 // rotate_array without any allocation.

@@ -173,6 +173,41 @@ def cube_atmosphere(seed, nx, ny, nz, sigma_t=300.0, ell=8.0, sigma_vz_kms=2.0, 
             "ds_cm": (ds_xy, ds_xy, ds_z)}
 
 
+def column_set(seed=3, ncol=4096, depth=(60, 256), nz=256, nxy=64, variants=(0.0,), sigma_t=300.0):
+    """Columns of uneven depth drawn from a seeded cube (the batched 1.5D
+    configuration): the cube_atmosphere of nxy^2 columns and nz planes, ncol of its
+    columns, each cut to its top d cells with d uniform in depth (inclusive).  The
+    columns are packed back to back, bottom to top, once per abundance variant
+    (a dex offset each).  Returns the per-cell fields (temp, ne, nH, chi_c, vz,
+    abund_dex), col_off (ncol*len(variants)+1), dz per column [cm] and the column
+    of the cube each packed column came from."""
+    c = cube_atmosphere(seed, nxy, nxy, nz, sigma_t=sigma_t)
+    rng = np.random.default_rng(seed + 6000)
+    pick = rng.choice(nxy * nxy, size=ncol, replace=ncol > nxy * nxy)
+    d = rng.integers(depth[0], depth[1] + 1, size=ncol)
+    d = np.minimum(d, nz)
+    fields = {k: [] for k in ("temp", "ne", "nH", "chi_c", "vz", "abund_dex")}
+    off = [0]
+    src = []
+    for v in variants:
+        for j, (col, dj) in enumerate(zip(pick, d)):
+            y, x = divmod(int(col), nxy)
+            zs = slice(nz - int(dj), nz)
+            for k in ("temp", "ne", "nH", "chi_c", "vz"):
+                fields[k].append(np.asarray(c[k])[zs, y, x])
+            fields["abund_dex"].append(np.full(int(dj), float(v)))
+            off.append(off[-1] + int(dj))
+            src.append(int(col))
+    out = {k: np.concatenate(v) for k, v in fields.items()}
+    out["temp"] = out["temp"].astype(np.float32)
+    out["chi_c"] = out["chi_c"].astype(np.float32)
+    out["vz"] = out["vz"].astype(np.float32)
+    out["col_off"] = np.asarray(off, np.int32)
+    out["dz"] = np.full(len(src), float(c["ds_cm"][2]))
+    out["source_column"] = np.asarray(src, np.int64)
+    return out
+
+
 def column_1d(ndep=80, log_tau=(-6.0, 2.0)):
     """The 1D grey model on log tau uniform, z index 0 = bottom."""
     lt = np.linspace(log_tau[1], log_tau[0], ndep)

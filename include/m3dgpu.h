@@ -42,6 +42,7 @@ extern "C" {
 #define M3D_SPLIT_RATES 0x8u  /* rate_formulation='largest': also Irem and escape */
 #define M3D_LINE_DIAG 0x10u   /* accumulate the line diagnostics used/strength/reach */
 #define M3D_ROTATE 0x20u      /* quadratic solver: apply rotate_array first (3D output pass) */
+#define M3D_AUTOTUNE 0x40u    /* m3d_col_plan_create: time the launch shapes and keep the fastest */
 
 /* ---- formal solvers (rt_patch_mod.f90:1649-1721, rt_params_mod.f90 solver names) ---- */
 #define M3D_SOLVER_LINEAR 0        /* long_char_linear, rt_solvers_mod.f90:666 ('linear', 1D) */
@@ -474,6 +475,54 @@ int m3d_lte_emission(int nf, int ncell, const float *chi_cont, const float *sigm
 int m3d_particle_fields(int ncell, double awgt, float vmic, double iso_frac, double population_scale,
                         const float *temp, const double *n, const double *part, float *inv_df, float *vbar2,
                         float *lnbase, unsigned flags);
+
+/* ---- batched 1.5D ALI: columns of uneven depth -------------------------------------
+ * The cells of all columns lie back to back: column c owns cells col_off[c] ..
+ * col_off[c+1]-1, bottom to top, each with its own cell height dz[c] [cm].  The
+ * per-cell inputs are device pointers the caller keeps alive for the plan's life
+ * (b and nstar (nlevel, ncell) float64; pop_ratio and e_kT (ncell) float64; inv_df,
+ * vz [c], chi_c (the grey continuum [1/cm]) and temp (ncell) float32).  mu/wmu are
+ * the directions (host): the upward half, then the same mirrored, mean-intensity
+ * weights (nphi_copies with Jnu_weights).  bottom: M3D_BND_PCHIP or M3D_BND_ZERO for
+ * the ghost of upward rays; downward rays enter through a zero top. */
+typedef struct {
+  int ncol, ncell;
+  const int *col_off;    /* ncol+1 (device) */
+  const double *dz;      /* ncol (device) */
+  int nray;
+  const double *mu;      /* nray (host) */
+  const float *wmu;      /* nray (host) */
+  const double *b, *nstar, *pop_ratio, *e_kT;
+  const float *inv_df, *vz, *chi_c, *temp;
+  double maser_dtau_max, maser_Inu_max, maser_chi_floor;
+  int preconditioning, bottom;
+  int nline_atom, nrad_atom;  /* the atom's lines and transitions (rows of wphi and gamma) */
+} m3d_col_problem_t;
+
+typedef struct m3d_col_plan m3d_col_plan_t;
+
+/* A plan for one model atom over its frequency windows: the windows' tables are
+ * staged once (win_nu float64, win_twohnu3_c2 float32 per window, host or device;
+ * win_adamp the window lines' damping (nline, ncell), device), and the plan owns
+ * work arrays sized for the widest window.  With M3D_AUTOTUNE the column solver's
+ * block size is chosen by timing. */
+int m3d_col_plan_create(const m3d_col_problem_t *p, int nwin, const m3d_atom_window_t *wins,
+                        const double *const *win_nu, const float *const *win_twohnu3_c2,
+                        const float *const *win_adamp, unsigned flags, m3d_col_plan_t **plan);
+/* One ALI sweep over every window and direction (rt_patch_t%execute's ALI branch
+ * for both hemisphere twins, the long characteristics along each column): the
+ * rates accumulate into gamma_ij/gamma_ji (nrad_atom, ncell, device) and, with
+ * first_iter, the profile integrals into wphi (nline_atom, ncell, device; may be
+ * NULL).  The sweep is a fixed sequence of launches on the library stream; with
+ * use_graph it is captured once per (first_iter, gamma, wphi) into a CUDA graph and
+ * replayed. */
+int m3d_col_plan_sweep(m3d_col_plan_t *plan, int first_iter, float *gamma_ij, float *gamma_ji, float *wphi,
+                       int use_graph);
+/* Copies the combined J and PsiJ of the last window (2 x (ncell, nf): both twins
+ * hold the average) into J, PsiJ (host or device, may be NULL) and returns that
+ * window's nf and the column solver's block size; synchronises. */
+int m3d_col_plan_fields(m3d_col_plan_t *plan, float *J, float *PsiJ, int *nf, int *solver_block);
+int m3d_col_plan_destroy(m3d_col_plan_t *plan);
 
 #ifdef __cplusplus
 }

@@ -200,3 +200,137 @@ def run(cube: dict, atom: dict, win: dict, vec, wts, maxiter: int, convlim: floa
         if not S["converged"] and S["iter"] < maxiter:
             _sweep_twins(S)
     return hist, S
+
+
+# ---- the batched 1.5D iteration: columns of uneven depth ---------------------------------
+def _solve_columns(S: dict, Wd: dict, mu: float) -> None:
+    """long_char_linear along every column with its upstream ghost (set_upstream_boundary:
+    PCHIP at the bottom for upward rays, zero at the top), one 1-column slab each."""
+    nf = Wd["nf"]
+    off, dz = S["col_off"], S["dz"]
+    d = 1 if mu > 0 else -1
+    for c in range(len(off) - 1):
+        k0, k1 = int(off[c]), int(off[c + 1])
+        nz = k1 - k0
+        work = np.zeros((3, nz + 2, 1, 1, nf), np.float32)
+        work[0, 1:nz + 1, 0, 0] = Wd["w1"][k0:k1]
+        work[1, 1:nz + 1, 0, 0] = Wd["w2"][k0:k1]
+        slab = orc.make_slab(nf, 1, 1, nz, d, [dz[c]] * 3, [0.0, 0.0, mu], get_psi=True, split_rates=True)
+        mode = S["bottom"] if d > 0 else orc.BND_ZERO
+        orc.upstream_boundary(slab, work, mode, ds3_code=1.0)
+        psi = np.zeros((nz, 1, 1, nf), np.float32)
+        irem, esc = np.zeros_like(psi), np.zeros_like(psi)
+        orc.formal_solve(orc.LINEAR, slab, work, psi=psi, irem=irem, escape=esc)
+        Wd["inu"][k0:k1] = work[2, 1:nz + 1, 0, 0]
+        Wd["psi"][k0:k1] = psi[:, 0, 0]
+        Wd["irem"][k0:k1] = irem[:, 0, 0]
+        Wd["escape"][k0:k1] = esc[:, 0, 0]
+
+
+def _sweep_columns(S: dict) -> None:
+    first = S["iter"] == 0
+    nd = len(S["mu"])
+    for Wd in S["wins"]:
+        win = Wd["win"]
+        nc, nf = S["ncell"], Wd["nf"]
+        beta, Bnu = orc.lte_background(win["nu"], S["temp32"])
+        chi = np.ascontiguousarray(np.broadcast_to(S["chi_c"][:, None], (nc, nf)))
+        z = lambda dt=np.float32: np.zeros((nc, nf), dt)
+        split = {"opac_L": z(), "opac_R": z(), "id": z(np.int32), "chi_L": z(), "chi_R": z(), "chi_id": z(np.int32)}
+        Wd.update({"w1": z(), "w2": z(), "inu": z(), "psi": z(), "irem": z(), "escape": z()})
+        J = np.zeros((2, nc, nf), np.float32)
+        PsiJ = np.zeros((2, nc, nf), np.float32)
+        ntr = max(int(win["nline"]) + int(win["ncont"]), 1)
+        for h in range(2):
+            xhat, ehat, _, _ = onlte.lte_emission(chi, np.zeros_like(Bnu), Bnu, beta, jmode=1)
+            onlte.bf_opacity(win, S["b"], S["nstar"], S["pop_ratio"], S["e_kT"], xhat, ehat)
+            gw_ij = np.zeros((ntr, nc), np.float32)
+            gw_ji = np.zeros((ntr, nc), np.float32)
+            for d in range(h * nd // 2, (h + 1) * nd // 2):
+                mu, wmu = float(S["mu"][d]), float(S["wmu"][d])
+                vp = (S["vz"] * np.float32(mu)).astype(np.float32)
+                Wd["w1"][:] = xhat
+                Wd["w2"][:] = ehat
+                onlte.bb_opacity(win, S["b"], S["nstar"], S["pop_ratio"], S["e_kT"], S["inv_df"], vp, Wd["adamp"],
+                                 Wd["w1"], Wd["w2"], lte=False, wmu=wmu, split=split,
+                                 wphi=S["wphi"] if first else None)
+                onlte.transfer_units_split(Wd["w1"], Wd["w2"], beta, split, maser_chi_floor=1e-4)
+                _solve_columns(S, Wd, mu)
+                orc.integrate_intensity(wmu, Wd["inu"], Wd["psi"], J[h], PsiJ[h])
+                onlte.bb_rates(win, S["b"], S["nstar"], S["pop_ratio"], S["e_kT"], S["inv_df"], vp, Wd["adamp"],
+                               Wd["inu"], beta, Bnu, gw_ij, gw_ji, work1=Wd["w1"], psi=Wd["psi"],
+                               irem=Wd["irem"], escape=Wd["escape"], split=split, split_rates=True,
+                               preconditioning=True, per_direction=True, wmu=wmu, wtot=S["wtot"])
+            if int(win["ncont"]) > 0:
+                onlte.bf_rates(win, S["b"], S["nstar"], S["e_kT"], J[h], PsiJ[h], beta, gw_ij, gw_ji,
+                               preconditioning=True)
+            nl = int(win["nline"])
+            for i, k in enumerate(np.asarray(win["line_ntrans"], np.int64)):
+                S["gamma_ij"][k] = S["gamma_ij"][k] + gw_ij[i]
+                S["gamma_ji"][k] = S["gamma_ji"][k] + gw_ji[i]
+            for i, k in enumerate(np.asarray(win["cont_ntrans"], np.int64)):
+                S["gamma_ij"][k] = S["gamma_ij"][k] + gw_ij[nl + i]
+                S["gamma_ji"][k] = S["gamma_ji"][k] + gw_ji[nl + i]
+        m = ((J[0] + J[1]) * np.float32(0.5)).astype(np.float32)
+        mp = ((PsiJ[0] + PsiJ[1]) * np.float32(0.5)).astype(np.float32)
+        S["J"] = np.stack([m, m])
+        S["PsiJ"] = np.stack([mp, mp])
+
+
+def setup_columns(cols: dict, atom: dict, wins: list, mu, wmu, abundance: float = 7.5, awgt: float = 56.0,
+                  vmic_kms: float = 1.0, bottom: int = orc.BND_PCHIP) -> dict:
+    """The state of iteration 0 of the batched 1.5D problem (dispatch_b200.ali.AliColumns)."""
+    from dispatch_b200 import synth
+
+    temp = np.ascontiguousarray(cols["temp"], np.float32)
+    ne = np.asarray(cols["ne"], np.float64)
+    nH = np.asarray(cols["nH"], np.float64)
+    nc = temp.size
+    abund = abundance + np.asarray(cols.get("abund_dex", 0.0), np.float64)
+    nstar, totn = synth.lte_populations(atom, temp, ne, 10.0 ** (abund - 12.0) * nH)
+    e_kT = synth.EE / synth.BK / temp.astype(np.float64)
+    idf = synth.inverse_doppler_factor(temp, awgt, vmic_kms).astype(np.float32)
+    vbar2 = synth.compute_vbar2(temp, awgt).astype(np.float32)
+    ne32, nh32 = ne.astype(np.float32), nH.astype(np.float32)
+    stark = (ne32 * temp ** np.float32(1.0 / 6.0)).astype(np.float32)
+    uns = (vbar2.astype(np.float64) ** 0.3 * nH).astype(np.float32)
+    wmu32 = np.asarray(wmu, np.float32)
+    wt = np.float32(0.0)
+    for w in wmu32:
+        wt = np.float32(wt + w)
+    sums = np.zeros(int(atom["nline"]), np.uint8)
+    for w in wins:
+        sums[np.asarray(w["line_ntrans"], np.int64)] = np.asarray(w["sums_over_windows"], np.uint8)
+    return {"atom": atom, "ncell": nc, "iter": 0, "temp32": temp, "temp": temp.astype(np.float64),
+            "e_kT": e_kT, "nstar": nstar, "totn": totn, "pop_ratio": np.ones(nc), "inv_df": idf,
+            "cup": ostq.collision_rates(atom, temp.astype(np.float64), ne, e_kT),
+            "vz": np.ascontiguousarray(cols["vz"], np.float32), "chi_c": np.ascontiguousarray(cols["chi_c"], np.float32),
+            "col_off": np.asarray(cols["col_off"]), "dz": np.asarray(cols["dz"], np.float64),
+            "mu": np.asarray(mu, np.float64), "wmu": wmu32, "wtot": float(wt), "bottom": bottom,
+            "wins": [{"win": w, "nf": int(w["nf"]),
+                      "adamp": onlte.bb_damping(w, ne32, nh32, vbar2, stark, uns, idf)} for w in wins],
+            "b": np.ones((int(atom["nlevel"]), nc)), "oldb": np.zeros((3, int(atom["nlevel"]), nc)),
+            "gamma_ij": np.zeros((len(atom["ti"]), nc), np.float32),
+            "gamma_ji": np.zeros((len(atom["ti"]), nc), np.float32),
+            "has_wphi": sums, "wphi": np.zeros((max(int(atom["nline"]), 1), nc), np.float32),
+            "sweep": 0.0, "last": 0.0, "global": 0.0, "converged": False}
+
+
+def sweep_columns(S: dict) -> None:
+    _sweep_columns(S)
+
+
+def run_columns(cols, atom, wins, mu, wmu, maxiter: int, convlim: float = 1e-3, ng_step: int = 0, **kw):
+    """Iteration 0 and up to maxiter updates of the batched 1.5D problem."""
+    from dispatch_b200.stateq import NgState
+
+    S = setup_columns(cols, atom, wins, mu, wmu, **kw)
+    ng_state = NgState()
+    hist = []
+    _sweep_columns(S)
+    while S["iter"] < maxiter and not S["converged"]:
+        S["iter"] += 1
+        hist.append(_update(S, ng_state, convlim, ng_step))
+        if not S["converged"] and S["iter"] < maxiter:
+            _sweep_columns(S)
+    return hist, S

@@ -92,3 +92,31 @@ def test_oracle_ali_conserves_and_contracts(oracle_run):
     assert np.all(np.isfinite(S["J"])) and np.all(S["J"] >= 0)
     # the twins are combined: both hemispheres hold the mean intensity
     np.testing.assert_array_equal(S["J"][0], S["J"][1])
+
+
+def test_column_set_layout():
+    from dispatch_b200 import synth
+    c = synth.column_set(3, ncol=5, depth=(6, 9), nz=12, nxy=3, variants=(0.0, 0.2))
+    off = c["col_off"]
+    assert off[0] == 0 and off[-1] == c["temp"].size and len(off) == 11
+    d = np.diff(off)
+    assert d.min() >= 6 and d.max() <= 9
+    # the second variant repeats the columns with the abundance offset
+    np.testing.assert_array_equal(d[:5], d[5:])
+    np.testing.assert_array_equal(c["temp"][:off[5]], c["temp"][off[5]:])
+    assert np.all(c["abund_dex"][off[5]:] == 0.2) and np.all(c["abund_dex"][:off[5]] == 0.0)
+    # each column runs bottom to top: the temperature falls upwards on average
+    assert np.mean([c["temp"][off[k]] > c["temp"][off[k + 1] - 1] for k in range(10)]) > 0.5
+
+
+def test_oracle_columns_conserve_and_contract():
+    from dispatch_b200 import ali
+    from oracle import ali as oali
+    from oracle import oracle as O
+    O.build()
+    cols, atom, wins, mu, wmu = ali.column_problem(ncol=4, depth=(6, 10), nz=12, nxy=3, nbound=4, nline=4)
+    hist, S = oali.run_columns(cols, atom, wins, mu, wmu, maxiter=5, convlim=1e-6)
+    np.testing.assert_allclose((S["b"] * S["nstar"]).sum(axis=0), S["totn"], rtol=1e-12)
+    err = [abs(h["maxerr"]) for h in hist]
+    assert err[-1] < err[0]
+    np.testing.assert_array_equal(S["J"][0], S["J"][1])
