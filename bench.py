@@ -42,7 +42,7 @@ def _args():
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-fp64", action="store_true")
-    p.add_argument("--no-ali", action="store_true", help="skip the NLTE ALI window measurement")
+    p.add_argument("--no-ali", action="store_true", help="skip the NLTE measurements (3D window, batched columns)")
     p.add_argument("--cube", type=int, default=240, help="cube edge (240 = the configuration; smaller for profiling)")
     return p.parse_args()
 
@@ -227,6 +227,9 @@ def _nlte_ali(steps=2):
     the opacities, J, PsiJ and rate integrals of every direction; the update is the
     FP64 statistical equilibrium of all 1.728 M cells (fused collision rates, the Ng
     gate).  Device-resident inputs; CUDA events on torch's stream."""
+    import torch
+
+    import dispatch_b200 as m
     from dispatch_b200 import ali
     cube, atom, win, vec, wts = ali.cube_problem("c2", transitions=list(range(0, 80, 8)))
     A = ali.AliWindow(cube, atom, win, vec, wts)
@@ -257,6 +260,63 @@ def _nlte_ali(steps=2):
            "ray_pt_nu_per_sweep": pts, "gpu_launches_per_iteration": (m.launch_count() - n0) // steps,
            "maxerr_last": rec["maxerr"], "data": "synthetic (seeded grey cube, seeded model atom)"}
     del A
+    torch.cuda.empty_cache()
+    return out
+
+
+def _nlte_batched(steps=2):
+    """The batched 1.5D NLTE configuration, measured beside the headline: 4096 columns
+    of 60-256 cells from a seeded 64 x 64 x 256 cube, three abundance variants
+    (0, +-0.2 dex) packed as further columns (1.94 M cells), the 21-level atom (80
+    transitions, 8 windows, 2000 frequencies) and the 61-level atom (240 transitions,
+    24 windows, 6000 frequencies), Radau 2 directions and their mirror (4).  Each
+    atom's sweep is one CUDA-graph replay of its column plan; an ALI iteration is
+    both sweeps and both atoms' statistical-equilibrium updates."""
+    import torch
+
+    import dispatch_b200 as m
+    from dispatch_b200 import ali, synth
+    cols = synth.column_set(3, ncol=4096, depth=(60, 256), nz=256, nxy=64, variants=(0.0, 0.2, -0.2))
+    vec, wts = synth.radau_rays(2, 1, jnu_weights=True)
+    plans = []
+    for nb, nl in ((20, 60), (60, 180)):
+        atom = synth.model_atom(3, nbound=nb, nline=nl)
+        nrad = len(atom["ti"])
+        nwin = max(1, nrad // 10)
+        wins = [synth.atom_window(atom, seed=3, transitions=list(range(k, nrad, nwin))) for k in range(nwin)]
+        plans.append(ali.AliColumns(cols, atom, wins, vec[:, 2].copy(), wts, params=ali.AliParams(convlim=1e-9)))
+    for A in plans:
+        A.sweep()
+    cur = torch.cuda.current_stream()
+    sw, up, n0 = [], [], m.launch_count()
+    for _ in range(steps):
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        torch.cuda.synchronize()
+        e0.record(cur)
+        for A in plans:
+            A.iter += 1
+            A.update()
+        e1.record(cur)
+        for A in plans:
+            A.sweep()
+        e2.record(cur)
+        torch.cuda.synchronize()
+        up.append(e0.elapsed_time(e1))
+        sw.append(e1.elapsed_time(e2))
+    pts = sum(A.points() for A in plans)
+    sweep_ms, update_ms = float(np.median(sw)), float(np.median(up))
+    out = {"workload": "batched 1.5D NLTE: 4096 columns of 60-256 cells (seeded 64x64x256 cube), 3 abundance "
+                       "variants (1.94 M cells), 21-level atom (2000 frequencies, 8 windows) and 61-level atom "
+                       "(6000 frequencies, 24 windows), Radau 2 + mirror (4 directions), long_char_linear along "
+                       "each column with split rates; each atom's sweep one CUDA graph replay",
+           "unit": UNIT, "value": pts / (sweep_ms / 1e3) / 1e9, "sweep_ms": sweep_ms, "update_ms": update_ms,
+           "iteration_ms": sweep_ms + update_ms, "ray_pt_nu_per_iteration": pts,
+           "graph_launches_per_iteration": (m.launch_count() - n0) // steps,
+           "solver_block_autotuned": [A.solver_block for A in plans], "cells": plans[0].ncell,
+           "data": "synthetic (seeded grey cube, seeded model atoms)"}
+    for A in plans:
+        A.close()
+    del plans
     torch.cuda.empty_cache()
     return out
 
@@ -368,7 +428,7 @@ def run_b200(a):
     fp64 = None
     if not a.no_fp64:
         nu_d, llam_d = dwin[a.warmup]
-        _, f32, _ = m.lte_synthesis(datm, nu_d, llam_d, vec, wmu, device=True)
+        _, f32, it32 = m.lte_synthesis(datm, nu_d, llam_d, vec, wmu, device=True, return_itop=True)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
@@ -377,6 +437,13 @@ def run_b200(a):
         torch.cuda.synchronize()
         t64 = e0.elapsed_time(e1)
         err = float(torch.max(torch.abs(f32 - f64) / torch.abs(f64)).item())
+        # the emergent intensity of every column and ray: the flux averages the columns'
+        # independent FP32 roundings away, a single column keeps them
+        _, _, it64 = m.lte_synthesis(datm, nu_d, llam_d, vec, wmu, device=True, fp64=True, return_itop=True)
+        rel = torch.abs(it32.double() - it64) / torch.clamp(torch.abs(it64), min=1e-300)
+        err_col = float(rel.max().item())
+        err_col_med = float(rel.flatten()[:: max(1, rel.numel() // 1000000)].median().item())
+        del it32, it64, rel
         m.profile_enable(True)
         m.lte_synthesis(datm, nu_d, llam_d, vec, wmu, device=True, fp64=True)
         sv64_ms, sv64_n = m.profile_read(m.STAGE_SOLVE)
@@ -384,13 +451,16 @@ def run_b200(a):
         fp64 = {"value": work_per_step / (t64 / 1e3) / 1e9, "unit": UNIT, "ms_per_step": t64,
                 "fp32_over_fp64": value / ws / (work_per_step / (t64 / 1e3) / 1e9),
                 "max_rel_flux_err_fp32_vs_fp64": err,
+                "max_rel_column_intensity_err_fp32_vs_fp64": err_col,
+                "median_rel_column_intensity_err_fp32_vs_fp64": err_col_med,
                 "solve_ms_per_step": sv64_ms, "solve_launches": sv64_n,
                 "solve_fp32_over_fp64": sv64_ms / sv_ms if sv_ms else None,
                 "path": "same kernels in FP64 for units, rotation and solver, one launch per ray and slab"}
 
-    nlte = None
+    nlte = batched = None
     if rank == 0 and not a.no_ali:
         nlte = _nlte_ali()
+        batched = _nlte_batched()
 
     cpu = None
     if rank == 0 and not a.no_cpu_baseline:
@@ -405,7 +475,8 @@ def run_b200(a):
             "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic (seeded grey cube, random line list)", "config": _workload(nf, a.cube),
             "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline, "cpu_baseline": cpu,
-            "clocks": clocks, "stages": stages, "fp64_plain": fp64, "nlte_ali": nlte}
+            "clocks": clocks, "stages": stages, "fp64_plain": fp64, "nlte_ali": nlte,
+            "nlte_batched": batched}
     print(json.dumps(line), flush=True)
 
 
