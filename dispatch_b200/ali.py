@@ -395,6 +395,7 @@ def column_problem(kind: str = "small", seed: int = 3, ncol: int = 6, depth=(8, 
     if kind == "c3":
         ncol, depth, nz, nxy = 4096, (60, 256), 256, 64
         variants = (0.0, 0.2, -0.2)
+        nbound, nline, nwin = 20, 60, 8
     cols = synth.column_set(seed, ncol=ncol, depth=depth, nz=nz, nxy=nxy, variants=variants)
     atom = synth.model_atom(seed, nbound=nbound, nline=nline)
     nrad = len(atom["ti"])

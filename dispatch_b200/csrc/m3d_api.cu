@@ -556,7 +556,20 @@ int m3d_line_opacity(const m3d_linelist_t *ll, int nf, const double *llam, int n
                      const float *tothi, const float *stark_pe, const float *dep_mem, int nlevel, int do_nlte,
                      float tol, float line_reject_frac, unsigned char *used, float *strength, float *reach,
                      unsigned flags) {
+  return m3d_line_opacity_scat(ll, nf, llam, ncell, chi, eta, cont, logref, vproj, inv_df, vbar2, e_kT, lnbase, ne,
+                               tothi, stark_pe, dep_mem, nlevel, do_nlte, tol, line_reject_frac, used, strength,
+                               reach, nullptr, nullptr, flags);
+}
+
+int m3d_line_opacity_scat(const m3d_linelist_t *ll, int nf, const double *llam, int ncell, float *chi, float *eta,
+                          const float *cont, const float *logref, const float *vproj, const float *inv_df,
+                          const float *vbar2, const float *e_kT, const float *lnbase, const float *ne,
+                          const float *tothi, const float *stark_pe, const float *dep_mem, int nlevel, int do_nlte,
+                          float tol, float line_reject_frac, unsigned char *used, float *strength, float *reach,
+                          const float *one_m_eps, float *chi_scat, unsigned flags) {
   TRY(need_init());
+  if ((one_m_eps == nullptr) != (chi_scat == nullptr))
+    return fail(M3D_EINVAL, "m3d_line_opacity_scat: give both one_m_eps and chi_scat, or neither");
   if (!ll || !llam) return fail(M3D_EINVAL, "m3d_line_opacity: NULL line list or grid");
   if (ll->nline == 0 || nf < 2 || ncell == 0) return M3D_OK;
   if (ncell < 0 || ll->nline < 0) return fail(M3D_EINVAL, "m3d_line_opacity: negative size");
@@ -578,6 +591,12 @@ int m3d_line_opacity(const m3d_linelist_t *ll, int nf, const double *llam, int n
   TRY(st.in(e_kT, ncell, &dek)); TRY(st.in(lnbase, ncell, &dlb)); TRY(st.in(ne, ncell, &dne));
   TRY(st.in(tothi, ncell, &dth)); TRY(st.in(stark_pe, ncell, &dsp));
   if (do_nlte) TRY(st.in(dep_mem, (size_t)ncell * nlevel, &ddep));
+  const float *dome = nullptr;
+  float *dcs = nullptr;
+  if (chi_scat) {
+    TRY(st.in(one_m_eps, nfc, &dome));
+    TRY(st.map(chi_scat, nfc, true, true, &dcs));
+  }
   unsigned char *dused = nullptr;
   float *dstr = nullptr, *dreach = nullptr;
   if (diag) {
@@ -609,7 +628,7 @@ int m3d_line_opacity(const m3d_linelist_t *ll, int nf, const double *llam, int n
   int grid = (ncell + warps - 1) / warps;
   if (grid > 148 * 8) grid = 148 * 8;
   LAUNCH_S(M3D_STAGE_OPACITY, k_line_opacity, grid, block, smem, L, G, ncell, dchi, deta, dcont, dlr, dvp, didf, dvb, dek, dlb, dne, dth,
-         dsp, ddep, do_nlte, diag ? 1 : 0, dused, dstr, dreach, g_ctx.d_tab);
+         dsp, ddep, do_nlte, diag ? 1 : 0, dused, dstr, dreach, g_ctx.d_tab, dome, dcs);
   return st.finish();
 }
 

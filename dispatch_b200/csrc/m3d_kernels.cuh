@@ -124,7 +124,8 @@ __device__ __forceinline__ float line_damping_a(const LineArgs &L, int l, float 
 template <class DepFn>
 __device__ void warp_cell_lines(const LineArgs &L, const GridArgs &G, const CellArgs &c, float *chi, float *eta,
                                 const float *cont, const float *logref, DepFn dep, bool do_nlte, bool diag,
-                                uint8_t *used, float *strength, float *reach, const float2 *tab, int lane) {
+                                uint8_t *used, float *strength, float *reach, const float2 *tab, int lane,
+                                const float *one_m_eps = nullptr, float *chi_scat = nullptr) {
   const float ex_cutoff = -85.0f, voigt_peak = 0.5641895835f, sqrt_pi = 1.7724538509f;
   const int nf = G.nf;
   const QlgCell qw = qlg_cell(G.sdl / c.idf);
@@ -193,7 +194,8 @@ __device__ void warp_cell_lines(const LineArgs &L, const GridArgs &G, const Cell
       const float Rij = exp4(arg);
       if (!outside && voigt_peak * Rij <= refl) continue;
       float bi = 1.0f, bj = 1.0f;
-      if (do_nlte && L.lev_i && L.lev_j && L.lev_i[ln] > 0 && L.lev_j[ln] > 0) {
+      const bool nlte_line = do_nlte && L.lev_i && L.lev_j && L.lev_i[ln] > 0 && L.lev_j[ln] > 0;
+      if (nlte_line) {
         bi = dep(L.lev_i[ln]);
         bj = dep(L.lev_j[ln]);
       }
@@ -219,10 +221,14 @@ __device__ void warp_cell_lines(const LineArgs &L, const GridArgs &G, const Cell
       if (fa > fb) continue;
       if (diag && lane == 0) used[ln] = 1;
       const float x0 = x1 - (float)(i1 - fa);
+      // line_scattering: an LTE line also gives (1-eps) of its profile to chi_scat
+      // (bi = bj = 1 there, so chi and eta gain the profile itself)
+      const bool scat = chi_scat && !nlte_line;
       for (int f = fa + lane; f <= fb; f += 32) {
         const float K = qlg_eval(tab, cf, x0 + (float)(f - fa));
         chi[f - 1] = fmaf(K, bi, chi[f - 1]);
         eta[f - 1] = fmaf(K, bj, eta[f - 1]);
+        if (scat) chi_scat[f - 1] = fmaf(one_m_eps[f - 1], K, chi_scat[f - 1]);
       }
       __syncwarp();
     }
@@ -298,7 +304,7 @@ __global__ void __launch_bounds__(256) k_line_opacity(LineArgs L, GridArgs G, in
                                                       const float *lnbase, const float *ne, const float *tothi,
                                                       const float *stark_pe, const float *dep_mem, int do_nlte,
                                                       int diag, uint8_t *used, float *strength, float *reach,
-                                                      const float2 *tab) {
+                                                      const float2 *tab, const float *one_m_eps, float *chi_scat) {
   extern __shared__ float smem[];
   float2 *s_tab = reinterpret_cast<float2 *>(smem);
   stage_tables(s_tab, tab);
@@ -311,7 +317,7 @@ __global__ void __launch_bounds__(256) k_line_opacity(LineArgs L, GridArgs G, in
     const size_t o = (size_t)G.nf * cell;
     auto dep = [&](int lev) { return dep_mem[(size_t)cell + (size_t)ncell * (size_t)(lev - 1)]; };
     warp_cell_lines(L, G, c, chi + o, eta + o, cont + o, logref + o, dep, do_nlte != 0, diag != 0, used, strength,
-                    reach, s_tab, lane);
+                    reach, s_tab, lane, one_m_eps ? one_m_eps + o : nullptr, chi_scat ? chi_scat + o : nullptr);
   }
 }
 

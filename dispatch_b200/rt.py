@@ -95,8 +95,9 @@ def make_linelist(ll: dict, keep: list) -> LineList:
 
 
 def line_opacity(ll: dict, llam, chi, eta, cont, logref, cells: dict, dep_mem=None, nlevel=0, do_nlte=False,
-                 tol=1e-4, line_reject_frac=0.0, diag=False):
+                 tol=1e-4, line_reject_frac=0.0, diag=False, one_m_eps=None, chi_scat=None):
     """add_opacity_equi over ncell cells, in place on chi/eta ((ncell, nf) in C order).
+    one_m_eps, chi_scat: the line_scattering split (chi_scat accumulated in place).
     Returns (used, strength, reach) with diag, else None."""
     init()
     keep = []
@@ -123,10 +124,15 @@ def line_opacity(ll: dict, llam, chi, eta, cont, logref, cells: dict, dep_mem=No
         logref = np.ascontiguousarray(logref, _F32)
         if dep_mem is not None:
             dep_mem = np.ascontiguousarray(dep_mem, _F32)
-    check(lib().m3d_line_opacity(C.byref(s), C.c_int(nf), ptr(llam), C.c_int(ncell), ptr(chi), ptr(eta), ptr(cont),
-                                 ptr(logref), *[ptr(c) for c in cf], ptr(dep_mem), C.c_int(nlevel),
-                                 C.c_int(int(do_nlte)), C.c_float(tol), C.c_float(line_reject_frac), ptr(used),
-                                 ptr(strength), ptr(reach), C.c_uint(flags)), "m3d_line_opacity")
+        if one_m_eps is not None:
+            one_m_eps = np.ascontiguousarray(one_m_eps, _F32)
+        if chi_scat is not None and (chi_scat.dtype != _F32 or not chi_scat.flags.c_contiguous):
+            raise ValueError("chi_scat must be a C-contiguous float32 array (accumulated in place)")
+    check(lib().m3d_line_opacity_scat(C.byref(s), C.c_int(nf), ptr(llam), C.c_int(ncell), ptr(chi), ptr(eta),
+                                      ptr(cont), ptr(logref), *[ptr(c) for c in cf], ptr(dep_mem), C.c_int(nlevel),
+                                      C.c_int(int(do_nlte)), C.c_float(tol), C.c_float(line_reject_frac), ptr(used),
+                                      ptr(strength), ptr(reach), ptr(one_m_eps), ptr(chi_scat), C.c_uint(flags)),
+          "m3d_line_opacity_scat")
     del keep
     return (used, strength, reach) if diag else None
 

@@ -129,14 +129,26 @@ int m3d_qlg_bot_profile(int n, const float *a, const float *q, const float *vpr,
  * With reach_in the lines are those select_lines keeps (linelist_mod.f90:1110-1142:
  * centres within the chunk widened by half a grid step, max |vproj| and each line's
  * reach), and lines centred beyond the chunk take the unfloored reference at the
- * nearer end and a window capped by their reach (:844-854, 914-921).  No LTE
- * scattering split. */
+ * nearer end and a window capped by their reach (:844-854, 914-921).  The LTE
+ * scattering split is m3d_line_opacity_scat. */
 int m3d_line_opacity(const m3d_linelist_t *ll, int nf, const double *llam, int ncell,
                      float *chi, float *eta, const float *cont, const float *logref,
                      const float *vproj, const float *inv_df, const float *vbar2, const float *e_kT,
                      const float *lnbase, const float *ne, const float *tothi, const float *stark_pe,
                      const float *dep_mem, int nlevel, int do_nlte, float tol, float line_reject_frac,
                      unsigned char *used, float *strength, float *reach, unsigned flags);
+/* add_opacity_equi with line_scattering (do_scat, linelist_mod.f90:933-939): every
+ * LTE line (not a departure-carrying one) also adds one_m_eps times its profile to
+ * chi_scat, both (nf, ncell) like chi, chi_scat accumulated in place, in line order.
+ * The caller forms one_m_eps per stage (compute_epsilon_stage) and folds chi_scat
+ * into the source (work_to_transfer_units' chi_scat*dJnu, m3d_lte_emission's dJnu). */
+int m3d_line_opacity_scat(const m3d_linelist_t *ll, int nf, const double *llam, int ncell,
+                          float *chi, float *eta, const float *cont, const float *logref,
+                          const float *vproj, const float *inv_df, const float *vbar2, const float *e_kT,
+                          const float *lnbase, const float *ne, const float *tothi, const float *stark_pe,
+                          const float *dep_mem, int nlevel, int do_nlte, float tol, float line_reject_frac,
+                          unsigned char *used, float *strength, float *reach, const float *one_m_eps,
+                          float *chi_scat, unsigned flags);
 
 /* ---- background and work units ---- */
 /* beta = max(exp(-h nu/kT), tiny), Bnu = beta/(1-beta): (nf, ncell)

@@ -481,6 +481,23 @@ int or_add_opacity_equi(const float *tgx, const float *th2x, const or_linelist_t
                         const float *dep_mem, int nlevel, int do_nlte, float tol, float line_reject_frac,
                         uint8_t *used, float *strength, float *reach)
 {
+  return or_add_opacity_equi_scat(tgx, th2x, ll, nf, llam, ncell, chi, eta, cont, logref, vproj, inv_df, vbar2,
+                                  e_kT, lnbase, ne, tothi, stark_pe, dep_mem, nlevel, do_nlte, tol,
+                                  line_reject_frac, used, strength, reach, NULL, NULL);
+}
+
+/* add_opacity_equi with line_scattering (do_scat, linelist_mod.f90:933-939): an LTE
+ * line adds its profile to chi and eta and (1-eps) of it to chi_scat, in line order;
+ * one_m_eps and chi_scat are (nf, ncell) like chi, NULL without do_scat. */
+int or_add_opacity_equi_scat(const float *tgx, const float *th2x, const or_linelist_t *ll,
+                             int nf, const double *llam, int ncell,
+                             float *chi, float *eta, const float *cont, const float *logref,
+                             const float *vproj, const float *inv_df, const float *vbar2, const float *e_kT,
+                             const float *lnbase, const float *ne, const float *tothi, const float *stark_pe,
+                             const float *dep_mem, int nlevel, int do_nlte, float tol, float line_reject_frac,
+                             uint8_t *used, float *strength, float *reach, const float *one_m_eps,
+                             float *chi_scat)
+{
   const float ex_cutoff = -85.0f, voigt_peak = 0.5641895835f, sqrt_pi = 1.7724538509f;
   if (ll->nline == 0 || nf < 2) return 0;
   if (llam[nf - 1] < llam[0]) return 1;
@@ -576,10 +593,21 @@ int or_add_opacity_equi(const float *tgx, const float *th2x, const or_linelist_t
       }
       if (nk == 0) continue;
       if (used) used[l] = 1;
-      for (int f = fa; f <= fb; f++) {
-        float lte = Kbuf[f - fa];
-        ch[f - 1] = fmaf(lte, bi, ch[f - 1]);
-        et[f - 1] = fmaf(lte, bj, et[f - 1]);
+      if (chi_scat && !nlte) {
+        float *cs = chi_scat + (size_t)nf * i;
+        const float *om = one_m_eps + (size_t)nf * i;
+        for (int f = fa; f <= fb; f++) {
+          float lte = Kbuf[f - fa];
+          ch[f - 1] = ch[f - 1] + lte;
+          et[f - 1] = et[f - 1] + lte;
+          cs[f - 1] = fmaf(om[f - 1], lte, cs[f - 1]);
+        }
+      } else {
+        for (int f = fa; f <= fb; f++) {
+          float lte = Kbuf[f - fa];
+          ch[f - 1] = fmaf(lte, bi, ch[f - 1]);
+          et[f - 1] = fmaf(lte, bj, et[f - 1]);
+        }
       }
       f0_prev = -1;
     }

@@ -92,6 +92,14 @@ int or_add_opacity_equi(const float *tgx, const float *th2x, const or_linelist_t
                         const float *lnbase, const float *ne, const float *tothi, const float *stark_pe,
                         const float *dep_mem, int nlevel, int do_nlte, float tol, float line_reject_frac,
                         uint8_t *used, float *strength, float *reach);
+int or_add_opacity_equi_scat(const float *tgx, const float *th2x, const or_linelist_t *ll,
+                             int nf, const double *llam, int ncell,
+                             float *chi, float *eta, const float *cont, const float *logref,
+                             const float *vproj, const float *inv_df, const float *vbar2, const float *e_kT,
+                             const float *lnbase, const float *ne, const float *tothi, const float *stark_pe,
+                             const float *dep_mem, int nlevel, int do_nlte, float tol, float line_reject_frac,
+                             uint8_t *used, float *strength, float *reach, const float *one_m_eps,
+                             float *chi_scat);
 
 /* ---- background and work units (rt_patch_mod.f90:1983-2023, 3518-3651) ---- */
 void or_lte_background(int nf, int ncell, const double *nu, const float *temp, float *beta, float *Bnu);

@@ -204,9 +204,10 @@ def select_lines(ll: dict, llam, vmax: float):
 
 
 def add_opacity_equi(ll: dict, llam, chi, eta, cont, logref, cells: dict, dep_mem=None,
-                     nlevel=0, do_nlte=False, tol=1e-4, line_reject_frac=0.0):
+                     nlevel=0, do_nlte=False, tol=1e-4, line_reject_frac=0.0, one_m_eps=None, chi_scat=None):
     """In place on chi/eta (nf, ncell) f32.  cells: vproj, inv_df, vbar2, e_kT, lnbase,
-    ne, tothi, stark_pe (ncell,) f32.  Returns (used, strength, reach)."""
+    ne, tothi, stark_pe (ncell,) f32.  one_m_eps, chi_scat: the line_scattering split
+    (chi_scat accumulated in place).  Returns (used, strength, reach)."""
     tgx, th2x = qlg_tables()
     s, keep = make_linelist(ll)
     nl = s.nline
@@ -220,13 +221,16 @@ def add_opacity_equi(ll: dict, llam, chi, eta, cont, logref, cells: dict, dep_me
     dm = None if dep_mem is None else np.ascontiguousarray(dep_mem, np.float32)
     for a in (chi, eta):
         assert a.dtype == np.float32 and a.flags.c_contiguous
-    rc = lib().or_add_opacity_equi(
+    om = None if one_m_eps is None else np.ascontiguousarray(one_m_eps, np.float32)
+    if chi_scat is not None:
+        assert chi_scat.dtype == np.float32 and chi_scat.flags.c_contiguous and om is not None
+    rc = lib().or_add_opacity_equi_scat(
         _p(tgx), _p(th2x), C.byref(s), C.c_int(llam.size), _p(llam), C.c_int(ncell),
         _p(chi), _p(eta), _p(np.ascontiguousarray(cont, np.float32)),
         _p(np.ascontiguousarray(logref, np.float32)),
         *[_p(cf[k]) for k in ("vproj", "inv_df", "vbar2", "e_kT", "lnbase", "ne", "tothi", "stark_pe")],
         _p(dm), C.c_int(nlevel), C.c_int(int(do_nlte)), C.c_float(tol), C.c_float(line_reject_frac),
-        _p(used), _p(strength), _p(reach))
+        _p(used), _p(strength), _p(reach), _p(om), _p(chi_scat))
     assert rc == 0
     del keep
     return used, strength, reach

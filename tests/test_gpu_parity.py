@@ -328,3 +328,27 @@ def test_full_size_window_properties(m3d):
     _, fc, _ = m3d.lte_synthesis(cont, nu, llam, vec, wmu)
     assert np.all(flux <= fc * (1 + 1e-6))
     assert np.min(flux / fc) < 0.9
+
+
+@pytest.mark.parametrize("nlte", [False, True])
+def test_line_opacity_scattering_split_bit_exact(m3d, oracle, nlte):
+    """line_scattering (linelist_mod.f90:933-939): an LTE line adds (1-eps) of its
+    profile to chi_scat; a departure-carrying line adds none."""
+    sp, llam, xhat, cells, dep = _line_case(21 + nlte)
+    lr = oracle.logref(xhat)
+    rng = np.random.default_rng(4)
+    ome = rng.uniform(0.0, 1.0, xhat.shape).astype(np.float32)
+    chi0 = (xhat * rng.uniform(0, 2, xhat.shape)).astype(np.float32)
+    out = {}
+    for name, mod in (("o", oracle), ("g", m3d)):
+        c, e, cs = chi0.copy(), (chi0 * 0.5).astype(np.float32), np.zeros_like(chi0)
+        if name == "o":
+            oracle.add_opacity_equi(sp, llam, c, e, xhat, lr, cells, dep_mem=dep, nlevel=dep.shape[0], do_nlte=nlte,
+                                    one_m_eps=ome, chi_scat=cs)
+        else:
+            m3d.line_opacity(sp, llam, c, e, xhat, lr, cells, dep_mem=dep, nlevel=dep.shape[0], do_nlte=nlte,
+                             one_m_eps=ome, chi_scat=cs)
+        out[name] = (c, e, cs)
+    for a, b in zip(out["g"], out["o"]):
+        np.testing.assert_array_equal(a, b)
+    assert out["o"][2].max() > 0

@@ -223,3 +223,40 @@ def test_quadrature_weights():
     assert vec.shape == (5, 3)
     # mu and the weights are default-real (float32) values in the reference's table
     assert w.sum() == pytest.approx(0.5, abs=1e-7)
+
+
+def test_scattering_split_identities(oracle):
+    """With eps = 0 every LTE line scatters wholly: from zero opacity, chi_scat takes the
+    same additions in the same order as chi and equals it bit for bit; with eps = 1 it
+    stays zero; departure-carrying lines never scatter."""
+    from dispatch_b200 import synth
+    rng = np.random.default_rng(7)
+    raw = synth.random_linelist(rng, 60, 5000.0, 5003.0)
+    ncell = 12
+    temp = rng.uniform(4000, 8000, ncell).astype(np.float32)
+    lt = rng.uniform(-4, 0, ncell)
+    _, _, _, nH, ne = synth.grey_model(lt)
+    sp = synth.species_arrays(raw, temp, 10 ** -4.5 * nH)
+    cf = synth.cell_fields(temp, nH, ne)
+    llam, nu = synth.frequency_grid(5000.2, 5002.8, 120)
+    beta = np.exp(-6.626176e-27 * nu[None, :] / (1.380662e-16 * temp[:, None])).astype(np.float32)
+    xhat = (2e-8 * (1 + beta / (1 - beta))).astype(np.float32)
+    cells = {"vproj": np.zeros(ncell, np.float32), "inv_df": sp["inv_df"], "vbar2": sp["vbar2"],
+             "lnbase": sp["lnbase"], **cf}
+    lr = oracle.logref(xhat)
+    for ome_val in (1.0, 0.0):
+        chi, eta, cs = (np.zeros_like(xhat) for _ in range(3))
+        ome = np.full_like(xhat, ome_val)
+        oracle.add_opacity_equi(sp, llam, chi, eta, xhat, lr, cells, one_m_eps=ome, chi_scat=cs)
+        assert chi.max() > 0
+        if ome_val == 1.0:
+            np.testing.assert_array_equal(cs, chi)
+        else:
+            assert not cs.any()
+    # every line carries departures: nothing scatters
+    sp2 = dict(sp, lev_i=np.ones(60, np.int32), lev_j=np.full(60, 2, np.int32))
+    chi, eta, cs = (np.zeros_like(xhat) for _ in range(3))
+    dep = np.ones((2, ncell), np.float32)
+    oracle.add_opacity_equi(sp2, llam, chi, eta, xhat, lr, cells, dep_mem=dep, nlevel=2, do_nlte=True,
+                            one_m_eps=np.ones_like(xhat), chi_scat=cs)
+    assert chi.max() > 0 and not cs.any()
