@@ -178,4 +178,11 @@ __global__ void k_lte_emission(size_t n, EmissionArgs E, const float *__restrict
   if (nneg && neg) atomicAdd(nneg, neg);
 }
 
+// add_linelist_opacities' last step for line scattering (composition_mod.f90:1864-1874):
+// chi_scat in working units to physical extinction, chi_scat *= 1 - beta
+__global__ void k_chi_scat_units(size_t n, float *__restrict__ cs, const float *__restrict__ beta) {
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
+    cs[k] = cs[k] * (1.0f - beta[k]);
+}
+
 }  // namespace m3d

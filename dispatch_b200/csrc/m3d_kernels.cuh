@@ -669,6 +669,15 @@ __global__ void k_upstream_boundary(int nf, int nx, int ny, int nz, int dir, T *
 // consecutive upstream columns starting at xt[4 x0].
 constexpr int SC_TX = 8, SC_TY = 8, SC_TF = 32;
 
+// one element global -> shared without a register round trip (cp.async, sm_80+);
+// all of a block's copies are in flight together and complete at cp_async_wait_all
+template <typename T>
+__device__ __forceinline__ void cp_async_elem(T *dst, const T *src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(d), "l"(src), "n"(sizeof(T)));
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 template <typename T>
 __global__ void __launch_bounds__(256) k_short_char_tile(SlabArgs s, int z, T *work, T *psi, T *irem, T *esc,
                                                          const int *xt, const int *yt, float4 kx, float4 ky,
@@ -694,44 +703,79 @@ __global__ void __launch_bounds__(256) k_short_char_tile(SlabArgs s, int z, T *w
     for (int row = wid; row < 3 * PY * PX; row += nw) {
       const int xi = row % PX, yj = (row / PX) % PY, i = row / (PX * PY);
       const size_t base = slot * i + plane * zup + (size_t)nf * (sxu[xi] + (size_t)nx * syu[yj]) + f0;
-      if (fin) up[row * SC_TF + lane] = work[base + lane];
+      if (fin) cp_async_elem(&up[row * SC_TF + lane], &work[base + lane]);
     }
+    cp_async_wait_all();
   }
   __syncthreads();
   const T dtmax = -(T)s.maser_dtau_max, Imax = (T)s.maser_Inu_max;
   const T k_x[4] = {(T)kx.x, (T)kx.y, (T)kx.z, (T)kx.w};
   const T k_y[4] = {(T)ky.x, (T)ky.y, (T)ky.z, (T)ky.w};
-  const size_t k1 = (size_t)nf * nx * ny * (nz + 2);
-  for (int pnt = threadIdx.x; pnt < SC_TX * SC_TY * SC_TF; pnt += blockDim.x) {
-    const int f = pnt % SC_TF, xl = (pnt / SC_TF) % SC_TX, yl = pnt / (SC_TF * SC_TX);
-    const int x = x0 + xl, y = y0 + yl;
-    if (x >= nx || y >= ny || f0 + f >= nf) continue;
-    T upv[3], mn[3];
+  // one warp per column x of the tile, lanes along f, sliding down y: the row sums
+  // of an upstream row serve the four targets whose stencils hold it
+  const int lane = threadIdx.x & 31, xl = threadIdx.x >> 5;
+  const int x = x0 + xl, f = lane;
+  if (x >= nx || f0 + f >= nf || xl >= SC_TX) return;
+  const size_t plane = (size_t)nf * nx * ny, k1 = plane * (nz + 2);
+  const size_t pz = plane * (size_t)z, pp = plane * (size_t)(z - 1);
+  constexpr int RS = PX * SC_TF;   // one upstream row in shared memory
+  constexpr int FS = PY * RS;      // one field
+  const T *u0 = up + (size_t)xl * SC_TF + f;
+  // window of the four upstream rows yl..yl+3: row sums, and the two inner values
+  T rr[3][4], v1[3][4], v2[3][4];
+  auto load_row = [&](int r, int slot) {
+#pragma unroll
     for (int i = 0; i < 3; i++) {
-      const T *u = up + (size_t)i * PY * PX * SC_TF;
+      const T *row = u0 + (size_t)i * FS + (size_t)r * RS;
+      T a = 0;
+#pragma unroll
+      for (int ii = 0; ii < 4; ii++) a = fma_t(k_x[ii], row[ii * SC_TF], a);
+      rr[i][slot] = a;
+      v1[i][slot] = row[1 * SC_TF];
+      v2[i][slot] = row[2 * SC_TF];
+    }
+  };
+  // this column's chi and S on plane z for all the tile's rows, loaded up front
+  T xxv[SC_TY], ssv[SC_TY];
+#pragma unroll
+  for (int yl = 0; yl < SC_TY; yl++) {
+    const int y = y0 + yl < ny ? y0 + yl : ny - 1;
+    const size_t o = pz + (size_t)nf * ((size_t)x + (size_t)nx * (size_t)y) + (size_t)(f0 + f);
+    xxv[yl] = work[o];
+    ssv[yl] = work[o + k1];
+  }
+#pragma unroll
+  for (int jj = 0; jj < 3; jj++) load_row(jj, jj);
+#pragma unroll
+  for (int yl = 0; yl < SC_TY; yl++) {
+    const int y = y0 + yl;
+    if (y >= ny) break;
+    load_row(yl + 3, 3);
+    T upv[3], mn[3];
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
       T r = 0;
-      for (int jj = 0; jj < 4; jj++) {
-        const T *row = u + ((size_t)(yl + jj) * PX + xl) * SC_TF + f;
-        T rr = 0;
-        for (int ii = 0; ii < 4; ii++) rr = fma_t(k_x[ii], row[ii * SC_TF], rr);
-        r = fma_t(k_y[jj], rr, r);
-      }
+#pragma unroll
+      for (int jj = 0; jj < 4; jj++) r = fma_t(k_y[jj], rr[i][jj], r);
       T m = (T)FLT_MAX;
       if (sizeof(T) == 8) m = (T)DBL_MAX;
-      for (int jj = 1; jj <= 2; jj++)
-        for (int ii = 1; ii <= 2; ii++) m = tmin(m, u[((size_t)(yl + jj) * PX + xl + ii) * SC_TF + f]);
+      m = tmin(m, v1[i][1]);
+      m = tmin(m, v2[i][1]);
+      m = tmin(m, v1[i][2]);
+      m = tmin(m, v2[i][2]);
       upv[i] = r;
       mn[i] = m;
     }
     const T xxup = tmax(upv[0], mn[0]), ssup = tmax(upv[1], mn[1]), Inuup = tmax(upv[2], mn[2]);
-    const size_t o = iw(f0 + f, x, y, z, 0, nf, nx, ny, nz);
-    const T xx = work[o], ss = work[o + k1];
+    const size_t col = (size_t)nf * ((size_t)x + (size_t)nx * (size_t)y) + (size_t)(f0 + f);
+    const size_t o = pz + col;
+    const T xx = xxv[yl], ss = ssv[yl];
     T dt = dsup05 * (xxup + xx);
     dt = tmax(dt, dtmax);
     T E, W, Psi, Esc;
     linear_weights(dt, E, W, Psi, Esc);
     T Inu = fma_t(Psi, ss, fma_t(W, ssup, Inuup * E));
-    const size_t p = ip(f0 + f, x, y, z, nf, nx, ny);
+    const size_t p = pp + col;
     if (s.split_rates) {
       const bool off = dt <= 0 || xx <= 0 || tabs(Inu) > Imax;
       const T Irem = fma_t(W, ssup, Inuup * E);
@@ -744,6 +788,15 @@ __global__ void __launch_bounds__(256) k_short_char_tile(SlabArgs s, int z, T *w
     }
     work[o + 2 * k1] = Inu;
     if (s.get_psi) psi[p] = (dt > 0 && xx > 0) ? Psi / xx : (T)0;
+    // slide the window down one row
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+      for (int jj = 0; jj < 3; jj++) {
+        rr[i][jj] = rr[i][jj + 1];
+        v1[i][jj] = v1[i][jj + 1];
+        v2[i][jj] = v2[i][jj + 1];
+      }
   }
 }
 

@@ -230,7 +230,14 @@ __device__ __forceinline__ void rate_chunk_sum(float (*T)[33], int lane, int cnt
   __syncwarp();
 }
 
-__global__ void __launch_bounds__(kRateWarps * 32)
+// bound_bound_rates: one warp per (line, 32 consecutive cells).  Each lane forms
+// its cell's per-line constants; the terms of every (cell, f) are then evaluated
+// with the lanes along f (a half-warp per cell, 16 frequencies at a time, loads
+// coalesced), written to shared memory, and each lane adds its own cell's terms in
+// ascending f -- the reference's order -- so no lane idles in either phase.
+constexpr int kBbWarps = 4, kBbF = 16;
+
+__global__ void __launch_bounds__(kBbWarps * 32)
 k_bb_rates(NlWinDev W, NlRateOpts O, int ncell, const double *__restrict__ b,
            const double *__restrict__ nstar, const double *__restrict__ pop_ratio,
            const double *__restrict__ e_kT, const float *__restrict__ inv_df,
@@ -238,99 +245,133 @@ k_bb_rates(NlWinDev W, NlRateOpts O, int ncell, const double *__restrict__ b,
            const float2 *__restrict__ tab, NlRadField R, const unsigned *__restrict__ flags_in,
            unsigned *__restrict__ flags_raise, float *__restrict__ gamma_ij,
            float *__restrict__ gamma_ji) {
-  __shared__ float sh[kRateWarps][4][33];
+  __shared__ float sh[kBbWarps][4][32][kBbF + 1];
+  __shared__ int shr[kBbWarps][32];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  float (*T)[33] = sh[wib];
-  const size_t nf = (size_t)W.nf, n = (size_t)ncell * W.nline;
-  const size_t stride = (size_t)gridDim.x * kRateWarps;
-  for (size_t kk = (size_t)blockIdx.x * kRateWarps + wib; kk < n; kk += stride) {
-    const int c = (int)(kk % ncell), i = (int)(kk / ncell);
+  float (*T)[32][kBbF + 1] = sh[wib];
+  const size_t nf = (size_t)W.nf;
+  const int ctiles = (ncell + 31) / 32;
+  const size_t ntile = (size_t)ctiles * W.nline;
+  const size_t stride = (size_t)gridDim.x * kBbWarps;
+  for (size_t tt = (size_t)blockIdx.x * kBbWarps + wib; tt < ntile; tt += stride) {
+    const int i = (int)(tt / ctiles), c0 = (int)(tt % ctiles) * 32;
     if (W.lactive && !W.lactive[i]) continue;
     const int li = W.li[i], lj = W.lj[i], fs = W.lblue[i], fe = W.lred[i], off = W.loff[i];
     const bool own_norm = O.per_direction && !W.lsums[i];
     const int index = W.lindex[i];
     const double Aij = W.Aij[i];
-    const double nsi = nstar[(size_t)c + (size_t)ncell * li], nsj = nstar[(size_t)c + (size_t)ncell * lj];
-    const double bbi = b[(size_t)c + (size_t)ncell * li], bbj = b[(size_t)c + (size_t)ncell * lj];
-    float ni = (float)(bbi * nsi), nj = (float)(bbj * nsj);
-    const float idf = inv_df[c], vpr = vproj[c], a = adamp[kk], ekt = (float)e_kT[c];
     const float lower_off = (float)(W.lower_ev[i] - W.ev[li]);
-    float inv_nref = 0.0f;
-    if (nsi > 0 && nsj > 0) {
-      const double beta_ref = nsj * W.g[li] / (nsi * W.g[lj]);
-      inv_nref = (float)fmin((1.0 - beta_ref) / beta_ref, 1e35);
-    }
-    if (lower_off != 0.0f) {
-      ni = ni * expf(-lower_off * ekt);
-      nj = nj * expf(-lower_off * ekt);
-    }
-    float eta_coef = 0.0f, abs_coef = 0.0f, g_ratio = 0.0f;
-    if (O.precond) {
-      float split_bj = (float)bbj;
-      if (lower_off != 0.0f) split_bj = split_bj * expf(-lower_off * ekt);
-      float split_Rij = (float)(nsi * pop_ratio[c]);
-      split_Rij = (float)((double)split_Rij * W.Bij[i]);
-      eta_coef = split_Rij * split_bj;
-      float split_bi = (float)bbi;
-      if (lower_off != 0.0f) split_bi = split_bi * expf(-lower_off * ekt);
-      abs_coef = split_Rij * split_bi;
-      if (nj > 0.0f) g_ratio = (float)((double)(ni / nj) * (W.g[lj] / W.g[li]));
-    }
-    // lane j < 4 accumulates sum j: (A, I, P, w) without the split, (T, U, -, w) with it
-    float acc = 0.0f;
-    int in_force = 0, raise = 0;
     const int t = W.lntrans[i], pw = t >> 5, pb = t & 31;
-    if (O.split && O.precond && O.use_flags) in_force = (flags_in[(size_t)c + (size_t)ncell * pw] >> pb) & 1u;
-    for (int f0 = fs; f0 <= fe; f0 += 32) {
-      const int f = f0 + lane;
-      float t0 = 0.0f, t1 = 0.0f, t2 = 0.0f, t3 = 0.0f;
-      if (f <= fe) {
-        const size_t k = (size_t)f + nf * c;
-        const int o = off + f - fs;
-        const float phi = nl_profile(tab, a, W.q[o], vpr, idf);
-        const float wmunu = (float)((double)O.wmu * W.wnu[o] * Aij);
-        const float wqf = (float)W.wq[o];
-        t3 = phi * wqf;
-        if (!O.split) {
-          const float vvv = phi * wmunu;
-          t0 = vvv * (R.Bnu[k] * inv_nref);
-          t1 = vvv * R.inu[k];
-          t2 = vvv * phi * R.psi[k] * R.beta[k];
-        } else {
-          const float nb = R.Bnu[k];
-          const float vvv = phi * wmunu;
-          if (O.precond) {
-            const float be = R.beta[k];
-            float psi = R.psi[k];
-            const float eta_u = phi * eta_coef;
-            const float eta_t = eta_u * be;
-            const float chi_t = phi * abs_coef - eta_t;
-            const float eta_other = be * other_contribution(eta_u, index, R.sopL[k], R.sopR[k], R.sid[k]);
-            const float chi_other = other_contribution(phi * abs_coef, index, R.schL[k], R.schR[k], R.schid[k]) - eta_other;
-            float other = eta_other;
-            if (O.do_scat) other = other + R.scat[k];
-            if (chi_t < 0.0f || in_force) psi = 0.0f;
-            raise = raise || psi == 0.0f;
-            const float up = psi == 0.0f ? R.inu[k] : R.irem[k] + psi * other;
-            const float spont = psi == 0.0f ? 1.0f : (chi_other + R.escape[k] * chi_t) / R.work1[k];
-            t0 = vvv * spont * (nb * inv_nref);
-            t1 = vvv * (up - nb * spont);
+    const int ncl = min(32, ncell - c0);
+    // this lane's cell: the constants of the line
+    const int c = c0 + lane;
+    const bool mine = lane < ncl;
+    float ni = 0.0f, nj = 0.0f, inv_nref = 0.0f, eta_coef = 0.0f, abs_coef = 0.0f, g_ratio = 0.0f;
+    float idf = 0.0f, vpr = 0.0f, a = 0.0f;
+    int in_force = 0;
+    if (mine) {
+      const double nsi = nstar[(size_t)c + (size_t)ncell * li], nsj = nstar[(size_t)c + (size_t)ncell * lj];
+      const double bbi = b[(size_t)c + (size_t)ncell * li], bbj = b[(size_t)c + (size_t)ncell * lj];
+      ni = (float)(bbi * nsi);
+      nj = (float)(bbj * nsj);
+      idf = inv_df[c];
+      vpr = vproj[c];
+      a = adamp[(size_t)c + (size_t)ncell * i];
+      const float ekt = (float)e_kT[c];
+      if (nsi > 0 && nsj > 0) {
+        const double beta_ref = nsj * W.g[li] / (nsi * W.g[lj]);
+        inv_nref = (float)fmin((1.0 - beta_ref) / beta_ref, 1e35);
+      }
+      if (lower_off != 0.0f) {
+        ni = ni * expf(-lower_off * ekt);
+        nj = nj * expf(-lower_off * ekt);
+      }
+      if (O.precond) {
+        float split_bj = (float)bbj;
+        if (lower_off != 0.0f) split_bj = split_bj * expf(-lower_off * ekt);
+        float split_Rij = (float)(nsi * pop_ratio[c]);
+        split_Rij = (float)((double)split_Rij * W.Bij[i]);
+        eta_coef = split_Rij * split_bj;
+        float split_bi = (float)bbi;
+        if (lower_off != 0.0f) split_bi = split_bi * expf(-lower_off * ekt);
+        abs_coef = split_Rij * split_bi;
+        if (nj > 0.0f) g_ratio = (float)((double)(ni / nj) * (W.g[lj] / W.g[li]));
+      }
+      if (O.split && O.precond && O.use_flags) in_force = (flags_in[(size_t)c + (size_t)ncell * pw] >> pb) & 1u;
+    }
+    shr[wib][lane] = 0;
+    __syncwarp();
+    // lane k accumulates sums (A, I, P, w) without the split, (T, U, -, w) with it, of cell c0 + k
+    float s0 = 0.0f, s1 = 0.0f, s2 = 0.0f, s3 = 0.0f;
+    const int half = lane >> 4, hl = lane & 15;
+    for (int f0 = fs; f0 <= fe; f0 += kBbF) {
+      const int f = f0 + hl;
+      const int o = off + f - fs;
+      float phi_q = 0.0f, wmunu = 0.0f, wqf = 0.0f, qf = 0.0f;
+      const bool fin = f <= fe;
+      if (fin) {
+        qf = W.q[o];
+        wmunu = (float)((double)O.wmu * W.wnu[o] * Aij);
+        wqf = (float)W.wq[o];
+      }
+      for (int cc = 0; cc < 32; cc += 2) {
+        const int ci = cc + half;
+        const float c_idf = __shfl_sync(0xffffffffu, idf, ci), c_vpr = __shfl_sync(0xffffffffu, vpr, ci);
+        const float c_a = __shfl_sync(0xffffffffu, a, ci), c_inr = __shfl_sync(0xffffffffu, inv_nref, ci);
+        const float c_eta = __shfl_sync(0xffffffffu, eta_coef, ci), c_abs = __shfl_sync(0xffffffffu, abs_coef, ci);
+        const int c_if = __shfl_sync(0xffffffffu, in_force, ci);
+        float t0 = 0.0f, t1 = 0.0f, t2 = 0.0f, t3 = 0.0f;
+        if (fin && ci < ncl) {
+          const size_t k = (size_t)f + nf * (size_t)(c0 + ci);
+          const float phi = nl_profile(tab, c_a, qf, c_vpr, c_idf);
+          t3 = phi * wqf;
+          if (!O.split) {
+            const float vvv = phi * wmunu;
+            t0 = vvv * (R.Bnu[k] * c_inr);
+            t1 = vvv * R.inu[k];
+            t2 = vvv * phi * R.psi[k] * R.beta[k];
           } else {
-            t0 = vvv * (nb * inv_nref);
-            t1 = vvv * (R.inu[k] - nb);
+            const float nb = R.Bnu[k];
+            const float vvv = phi * wmunu;
+            if (O.precond) {
+              const float be = R.beta[k];
+              float psi = R.psi[k];
+              const float eta_u = phi * c_eta;
+              const float eta_t = eta_u * be;
+              const float chi_t = phi * c_abs - eta_t;
+              const float eta_other = be * other_contribution(eta_u, index, R.sopL[k], R.sopR[k], R.sid[k]);
+              const float chi_other = other_contribution(phi * c_abs, index, R.schL[k], R.schR[k], R.schid[k]) - eta_other;
+              float other = eta_other;
+              if (O.do_scat) other = other + R.scat[k];
+              if (chi_t < 0.0f || c_if) psi = 0.0f;
+              if (psi == 0.0f) shr[wib][ci] = 1;
+              const float up = psi == 0.0f ? R.inu[k] : R.irem[k] + psi * other;
+              const float spont = psi == 0.0f ? 1.0f : (chi_other + R.escape[k] * chi_t) / R.work1[k];
+              t0 = vvv * spont * (nb * c_inr);
+              t1 = vvv * (up - nb * spont);
+            } else {
+              t0 = vvv * (nb * c_inr);
+              t1 = vvv * (R.inu[k] - nb);
+            }
           }
         }
+        T[0][ci][hl] = t0;
+        T[1][ci][hl] = t1;
+        T[2][ci][hl] = t2;
+        T[3][ci][hl] = t3;
       }
-      T[0][lane] = t0;
-      T[1][lane] = t1;
-      T[2][lane] = t2;
-      T[3][lane] = t3;
-      rate_chunk_sum(T, lane, min(32, fe - f0 + 1), acc);
+      __syncwarp();
+      const int cnt = min(kBbF, fe - f0 + 1);
+      for (int j = 0; j < cnt; j++) {
+        s0 = s0 + T[0][lane][j];
+        s1 = s1 + T[1][lane][j];
+        s2 = s2 + T[2][lane][j];
+        s3 = s3 + T[3][lane][j];
+      }
+      __syncwarp();
     }
-    raise = __any_sync(0xffffffffu, raise);
-    const float s0 = __shfl_sync(0xffffffffu, acc, 0), s1 = __shfl_sync(0xffffffffu, acc, 1);
-    const float s2 = __shfl_sync(0xffffffffu, acc, 2), sum_w = __shfl_sync(0xffffffffu, acc, 3);
-    if (lane == 0) {
+    if (mine) {
+      const int raise = shr[wib][lane];
       if (O.split && O.precond && O.use_flags && raise && !in_force)
         atomicOr(&flags_raise[(size_t)c + (size_t)ncell * pw], 1u << pb);
       float g_th = s0, g_dev = s1;
@@ -341,13 +382,15 @@ k_bb_rates(NlWinDev W, NlRateOpts O, int ncell, const double *__restrict__ b,
         }
         if (inv_nref > 0.0f) g_dev = g_dev - g_th / inv_nref;
       }
-      if (own_norm && sum_w > 0.0f) {
-        g_th = g_th / (sum_w * O.wtot);
-        g_dev = g_dev / (sum_w * O.wtot);
+      if (own_norm && s3 > 0.0f) {
+        g_th = g_th / (s3 * O.wtot);
+        g_dev = g_dev / (s3 * O.wtot);
       }
+      const size_t kk = (size_t)c + (size_t)ncell * i;
       gamma_ij[kk] = gamma_ij[kk] + g_th;
       gamma_ji[kk] = gamma_ji[kk] + g_dev;
     }
+    __syncwarp();
   }
 }
 

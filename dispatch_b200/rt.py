@@ -137,6 +137,19 @@ def line_opacity(ll: dict, llam, chi, eta, cont, logref, cells: dict, dep_mem=No
     return (used, strength, reach) if diag else None
 
 
+def chi_scat_units(chi_scat, beta):
+    """chi_scat *= 1 - beta in place (add_linelist_opacities, composition_mod.f90:1864-1874)."""
+    init()
+    dev = _is_dev(chi_scat)
+    if not dev:
+        if chi_scat.dtype != _F32 or not chi_scat.flags.c_contiguous:
+            raise ValueError("chi_scat must be a C-contiguous float32 array (updated in place)")
+        beta = np.ascontiguousarray(beta, _F32)
+    n = int(np.prod(chi_scat.shape))
+    check(lib().m3d_chi_scat_units(C.c_longlong(n), ptr(chi_scat), ptr(beta), C.c_uint(DEVICE_PTRS if dev else 0)),
+          "m3d_chi_scat_units")
+
+
 def lte_background(nu, temp):
     """beta, Bnu (ncell, nf); device tensors in, device tensors out (nu float64)."""
     init()

@@ -150,6 +150,10 @@ int m3d_line_opacity_scat(const m3d_linelist_t *ll, int nf, const double *llam, 
                           unsigned char *used, float *strength, float *reach, const float *one_m_eps,
                           float *chi_scat, unsigned flags);
 
+/* add_linelist_opacities' last step with line scattering (composition_mod.f90:1864-1874):
+ * chi_scat *= 1 - beta over n points, after every species has been added. */
+int m3d_chi_scat_units(long long n, float *chi_scat, const float *beta, unsigned flags);
+
 /* ---- background and work units ---- */
 /* beta = max(exp(-h nu/kT), tiny), Bnu = beta/(1-beta): (nf, ncell)
  * (lte_background_opacities, rt_patch_mod.f90:2004-2023) */

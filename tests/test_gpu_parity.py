@@ -352,3 +352,14 @@ def test_line_opacity_scattering_split_bit_exact(m3d, oracle, nlte):
     for a, b in zip(out["g"], out["o"]):
         np.testing.assert_array_equal(a, b)
     assert out["o"][2].max() > 0
+
+
+def test_chi_scat_units(m3d):
+    """chi_scat * (1 - beta) in real(4), as add_linelist_opacities converts it."""
+    rng = np.random.default_rng(8)
+    cs = rng.uniform(0, 1e-6, (50, 37)).astype(np.float32)
+    beta = rng.uniform(0, 1, cs.shape).astype(np.float32)
+    exp = (cs * (np.float32(1.0) - beta)).astype(np.float32)
+    got = cs.copy()
+    m3d.rt.chi_scat_units(got, beta)
+    np.testing.assert_array_equal(got, exp)
