@@ -230,12 +230,12 @@ __device__ __forceinline__ void rate_chunk_sum(float (*T)[33], int lane, int cnt
   __syncwarp();
 }
 
-// bound_bound_rates: one warp per (line, 32 consecutive cells).  Each lane forms
-// its cell's per-line constants; the terms of every (cell, f) are then evaluated
-// with the lanes along f (a half-warp per cell, 16 frequencies at a time, loads
-// coalesced), written to shared memory, and each lane adds its own cell's terms in
-// ascending f -- the reference's order -- so no lane idles in either phase.
-constexpr int kBbWarps = 4, kBbF = 16;
+// bound_bound_rates: one warp per (line, 16 consecutive cells).  Lanes 0..15 form
+// their cell's per-line constants; the terms of every (cell, f) are then evaluated
+// a cell at a time with all 32 lanes along f (one 128-byte load per array), written
+// to shared memory, and lane k adds cell k's terms in ascending f -- the
+// reference's order.  A line window of up to 32 points takes a single chunk.
+constexpr int kBbWarps = 4, kBbCells = 16;
 
 __global__ void __launch_bounds__(kBbWarps * 32)
 k_bb_rates(NlWinDev W, NlRateOpts O, int ncell, const double *__restrict__ b,
@@ -245,16 +245,16 @@ k_bb_rates(NlWinDev W, NlRateOpts O, int ncell, const double *__restrict__ b,
            const float2 *__restrict__ tab, NlRadField R, const unsigned *__restrict__ flags_in,
            unsigned *__restrict__ flags_raise, float *__restrict__ gamma_ij,
            float *__restrict__ gamma_ji) {
-  __shared__ float sh[kBbWarps][4][32][kBbF + 1];
-  __shared__ int shr[kBbWarps][32];
+  __shared__ float sh[kBbWarps][4][kBbCells][33];
+  __shared__ int shr[kBbWarps][kBbCells];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  float (*T)[32][kBbF + 1] = sh[wib];
+  float (*T)[kBbCells][33] = sh[wib];
   const size_t nf = (size_t)W.nf;
-  const int ctiles = (ncell + 31) / 32;
+  const int ctiles = (ncell + kBbCells - 1) / kBbCells;
   const size_t ntile = (size_t)ctiles * W.nline;
   const size_t stride = (size_t)gridDim.x * kBbWarps;
   for (size_t tt = (size_t)blockIdx.x * kBbWarps + wib; tt < ntile; tt += stride) {
-    const int i = (int)(tt / ctiles), c0 = (int)(tt % ctiles) * 32;
+    const int i = (int)(tt / ctiles), c0 = (int)(tt % ctiles) * kBbCells;
     if (W.lactive && !W.lactive[i]) continue;
     const int li = W.li[i], lj = W.lj[i], fs = W.lblue[i], fe = W.lred[i], off = W.loff[i];
     const bool own_norm = O.per_direction && !W.lsums[i];
@@ -262,8 +262,8 @@ k_bb_rates(NlWinDev W, NlRateOpts O, int ncell, const double *__restrict__ b,
     const double Aij = W.Aij[i];
     const float lower_off = (float)(W.lower_ev[i] - W.ev[li]);
     const int t = W.lntrans[i], pw = t >> 5, pb = t & 31;
-    const int ncl = min(32, ncell - c0);
-    // this lane's cell: the constants of the line
+    const int ncl = min(kBbCells, ncell - c0);
+    // lane k < ncl: the constants of cell c0 + k for this line
     const int c = c0 + lane;
     const bool mine = lane < ncl;
     float ni = 0.0f, nj = 0.0f, inv_nref = 0.0f, eta_coef = 0.0f, abs_coef = 0.0f, g_ratio = 0.0f;
@@ -299,29 +299,27 @@ k_bb_rates(NlWinDev W, NlRateOpts O, int ncell, const double *__restrict__ b,
       }
       if (O.split && O.precond && O.use_flags) in_force = (flags_in[(size_t)c + (size_t)ncell * pw] >> pb) & 1u;
     }
-    shr[wib][lane] = 0;
+    if (lane < kBbCells) shr[wib][lane] = 0;
     __syncwarp();
-    // lane k accumulates sums (A, I, P, w) without the split, (T, U, -, w) with it, of cell c0 + k
+    // lane k < 16 accumulates sums (A, I, P, w) without the split, (T, U, -, w) with it, of cell c0 + k
     float s0 = 0.0f, s1 = 0.0f, s2 = 0.0f, s3 = 0.0f;
-    const int half = lane >> 4, hl = lane & 15;
-    for (int f0 = fs; f0 <= fe; f0 += kBbF) {
-      const int f = f0 + hl;
+    for (int f0 = fs; f0 <= fe; f0 += 32) {
+      const int f = f0 + lane;
       const int o = off + f - fs;
-      float phi_q = 0.0f, wmunu = 0.0f, wqf = 0.0f, qf = 0.0f;
       const bool fin = f <= fe;
+      float wmunu = 0.0f, wqf = 0.0f, qf = 0.0f;
       if (fin) {
         qf = W.q[o];
         wmunu = (float)((double)O.wmu * W.wnu[o] * Aij);
         wqf = (float)W.wq[o];
       }
-      for (int cc = 0; cc < 32; cc += 2) {
-        const int ci = cc + half;
+      for (int ci = 0; ci < ncl; ci++) {
         const float c_idf = __shfl_sync(0xffffffffu, idf, ci), c_vpr = __shfl_sync(0xffffffffu, vpr, ci);
         const float c_a = __shfl_sync(0xffffffffu, a, ci), c_inr = __shfl_sync(0xffffffffu, inv_nref, ci);
         const float c_eta = __shfl_sync(0xffffffffu, eta_coef, ci), c_abs = __shfl_sync(0xffffffffu, abs_coef, ci);
         const int c_if = __shfl_sync(0xffffffffu, in_force, ci);
         float t0 = 0.0f, t1 = 0.0f, t2 = 0.0f, t3 = 0.0f;
-        if (fin && ci < ncl) {
+        if (fin) {
           const size_t k = (size_t)f + nf * (size_t)(c0 + ci);
           const float phi = nl_profile(tab, c_a, qf, c_vpr, c_idf);
           t3 = phi * wqf;
@@ -355,18 +353,20 @@ k_bb_rates(NlWinDev W, NlRateOpts O, int ncell, const double *__restrict__ b,
             }
           }
         }
-        T[0][ci][hl] = t0;
-        T[1][ci][hl] = t1;
-        T[2][ci][hl] = t2;
-        T[3][ci][hl] = t3;
+        T[0][ci][lane] = t0;
+        T[1][ci][lane] = t1;
+        T[2][ci][lane] = t2;
+        T[3][ci][lane] = t3;
       }
       __syncwarp();
-      const int cnt = min(kBbF, fe - f0 + 1);
-      for (int j = 0; j < cnt; j++) {
-        s0 = s0 + T[0][lane][j];
-        s1 = s1 + T[1][lane][j];
-        s2 = s2 + T[2][lane][j];
-        s3 = s3 + T[3][lane][j];
+      if (mine) {
+        const int cnt = min(32, fe - f0 + 1);
+        for (int j = 0; j < cnt; j++) {
+          s0 = s0 + T[0][lane][j];
+          s1 = s1 + T[1][lane][j];
+          s2 = s2 + T[2][lane][j];
+          s3 = s3 + T[3][lane][j];
+        }
       }
       __syncwarp();
     }
