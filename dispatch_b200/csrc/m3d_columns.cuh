@@ -22,7 +22,10 @@ struct ColArgs {
 // chi, S are the transfer units; inu, psi, irem, esc receive the solution.
 __global__ void k_long_char_columns(ColArgs A, PchipConst pc, const float *__restrict__ chi,
                                     const float *__restrict__ S, float *__restrict__ inu, float *__restrict__ psi,
-                                    float *__restrict__ irem, float *__restrict__ esc) {
+                                    float *__restrict__ irem, float *__restrict__ esc, float *__restrict__ Jnu,
+                                    float *__restrict__ PsiJ, float wmu) {
+  // with Jnu, the epilogue of integrate_intensity (rt_patch_mod.f90:3399-3431) too
+  const float w2 = 2.0f * wmu;
   const size_t nf = (size_t)A.nf;
   const size_t n = nf * A.ncol;
   for (size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x; g < n; g += (size_t)gridDim.x * blockDim.x) {
@@ -65,7 +68,12 @@ __global__ void k_long_char_columns(ColArgs A, PchipConst pc, const float *__res
       irem[o] = off ? Inu : Irem;
       esc[o] = off ? 1.0f : Esc;
       inu[o] = Inu;
-      psi[o] = (dt > 0 && xx > 0) ? Psi / xx : 0.0f;
+      const float ps = (dt > 0 && xx > 0) ? Psi / xx : 0.0f;
+      psi[o] = ps;
+      if (Jnu) {
+        Jnu[o] = fmaf(w2, Inu, Jnu[o]);
+        PsiJ[o] = fmaf(w2, ps, PsiJ[o]);
+      }
       xxup = xx;
       ssup = ss;
       Inuup = Inu;

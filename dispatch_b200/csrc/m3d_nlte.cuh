@@ -111,6 +111,22 @@ __device__ __forceinline__ float other_contribution(float value, int index, floa
   return index == largest_index ? rest : largest + (rest - value);
 }
 
+// work_to_transfer_units of one point with split rates: (xhat, L, R) -> (chi, S)
+__device__ __forceinline__ bool units_split_point(float xhat, float be, float sL, float sR, float sc, bool has_scat,
+                                                  float fl, int suppress, float &chi_out, float &S_out) {
+  const float eta_rest = be * sR;
+  float eta = be * sL + eta_rest;
+  float chi = xhat - eta;
+  if (has_scat) eta = be * sL + (eta_rest + sc);
+  const float floor_ = fmaxf(fl * fabsf(xhat), FLT_MIN);
+  bool floored = false;
+  if (suppress) chi = fmaxf(chi, floor_);
+  else if (fabsf(chi) < floor_) { chi = copysignf(floor_, chi); floored = true; }
+  chi_out = chi;
+  S_out = eta / chi;
+  return floored;
+}
+
 struct NlSplit {
   float *sopL, *sopR, *schL, *schR;
   int *sid, *schid;
@@ -120,7 +136,8 @@ __global__ void k_bb_opacity(NlWinDev W, int ncell, const double *__restrict__ b
                              const double *__restrict__ pop_ratio, const double *__restrict__ e_kT,
                              const float *__restrict__ inv_df, const float *__restrict__ vproj,
                              const float *__restrict__ adamp, const float2 *__restrict__ tab, int lte,
-                             float *__restrict__ xhat, float *__restrict__ ehat, NlSplit S) {
+                             float *__restrict__ xhat, float *__restrict__ ehat, NlSplit S,
+                             const float *__restrict__ units_beta = nullptr, float units_floor = 0.0f) {
   const size_t nf = (size_t)W.nf, n = nf * ncell;
   for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
     const int f = (int)(k % nf), c = (int)(k / nf);
@@ -154,8 +171,18 @@ __global__ void k_bb_opacity(NlWinDev W, int ncell, const double *__restrict__ b
           add_largest(phi * chi_fac, W.lindex[i], cL, cR, cid);
         }
       }
-      xhat[k] = xh;
-      ehat[k] = eh;
+      if (!units_beta) {
+        xhat[k] = xh;
+        ehat[k] = eh;
+      }
+    }
+    // fused work_to_transfer_units (split form, no scattering term, masers floored):
+    // every point leaves as chi and S
+    if (units_beta) {
+      float chi, Sv;
+      units_split_point(xh, units_beta[k], oL, oR, 0.0f, false, units_floor, 0, chi, Sv);
+      xhat[k] = chi;
+      ehat[k] = Sv;
     }
     if (S.sopL) {
       S.sopL[k] = oL;
@@ -194,17 +221,11 @@ __global__ void k_transfer_units_split(size_t n, float *__restrict__ w1, float *
                                        int suppress, int *n_floored) {
   int cnt = 0;
   for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
-    const float be = beta[k];
-    const float eta_rest = be * sopR[k];
-    float eta = be * sopL[k] + eta_rest;
-    const float xhat = w1[k];
-    float chi = xhat - eta;
-    if (scat) eta = be * sopL[k] + (eta_rest + scat[k]);
-    const float floor_ = fmaxf(fl * fabsf(xhat), FLT_MIN);
-    if (suppress) chi = fmaxf(chi, floor_);
-    else if (fabsf(chi) < floor_) { chi = copysignf(floor_, chi); cnt++; }
+    float chi, S;
+    cnt += units_split_point(w1[k], beta[k], sopL[k], sopR[k], scat ? scat[k] : 0.0f, scat != nullptr, fl,
+                             suppress, chi, S);
     w1[k] = chi;
-    w2[k] = eta / chi;
+    w2[k] = S;
   }
   if (n_floored && cnt) atomicAdd(n_floored, cnt);
 }
