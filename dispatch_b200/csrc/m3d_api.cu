@@ -501,11 +501,11 @@ int m3d_profile_read(int stage, double *ms, long long *launches) {
 
 int m3d_weights(int which, int n, const void *t, void *o1, void *o2, void *o3, void *o4, unsigned flags) {
   TRY(need_init());
-  if (n < 0 || which < 0 || which > 4) return fail(M3D_EINVAL, "m3d_weights: bad which/n");
+  if (n < 0 || which < 0 || which > 5) return fail(M3D_EINVAL, "m3d_weights: bad which/n");
   if (n == 0) return M3D_OK;
   const bool f64 = flags & M3D_FP64;
   if (f64 && which != 1 && which != 2) return fail(M3D_EUNSUPPORTED, "m3d_weights: FP64 has which = 1, 2 only");
-  const int nout = which == 0 ? 2 : (which >= 3 ? 1 : 4);
+  const int nout = which == 0 ? 2 : ((which == 3 || which == 4) ? 1 : 4);
   Staging st(flags);
   if (f64) {
     const double *dt; double *d[4] = {nullptr, nullptr, nullptr, nullptr};

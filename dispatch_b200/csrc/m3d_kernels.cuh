@@ -49,6 +49,7 @@ __global__ void k_weights_f32(int which, int n, const float *t, float *o1, float
       case 1: { float E, W, P, S; linear_weights(x, E, W, P, S); o1[i] = E; o2[i] = W; o3[i] = P; o4[i] = S; } break;
       case 2: { float E, U0, U1, q; parab_moments(x, E, U0, U1, q); o1[i] = E; o2[i] = U0; o3[i] = U1; o4[i] = q; } break;
       case 3: o1[i] = exp4(x); break;
+      case 5: { float E; bezier3_weights(x, E, o1[i], o2[i], o3[i], o4[i]); } break;
       default: o1[i] = logf_m3d(x); break;
     }
   }

@@ -90,6 +90,56 @@ __device__ __forceinline__ void linear_weights(float t, float &E, float &W, floa
   W = thin ? u0 - ps : ut - E;
 }
 
+// bezier3_weights (rt_solvers_mod.f90:1280-1304): the cubic-Bezier weights over
+// optical depth t, w_k = t int_0^1 b_k(u) exp(-t u) du, b = u^3, 3u^2(1-u),
+// 3u(1-u)^2, (1-u)^3.  For t <= 3 the series t E P3(-t), t E P2(-t), t P2(t),
+// t P3(t), P2 and P3 the reference's minimax fits (b3_p2, b3_p3, :1305-1331);
+// above, the moments M_n = n M_(n-1) - t^n E from M0 = 1 - E at max(t, 3).
+__device__ __forceinline__ float b3_p2(float t) {
+  float p = fmaf(t, +7.658396139e-10f, -1.100420821e-08f);
+  p = fmaf(t, p, +1.137804801e-07f);
+  p = fmaf(t, p, -1.190877015e-06f);
+  p = fmaf(t, p, +1.156294547e-05f);
+  p = fmaf(t, p, -9.924791084e-05f);
+  p = fmaf(t, p, +7.440865738e-04f);
+  p = fmaf(t, p, -4.761847202e-03f);
+  p = fmaf(t, p, +2.499995567e-02f);
+  p = fmaf(t, p, -1.000000238e-01f);
+  return fmaf(t, p, +2.500000000e-01f);
+}
+__device__ __forceinline__ float b3_p3(float t) {
+  float p = fmaf(t, -1.025371787e-09f, +1.414234507e-08f);
+  p = fmaf(t, p, -1.503805294e-07f);
+  p = fmaf(t, p, +1.640762775e-06f);
+  p = fmaf(t, p, -1.653099389e-05f);
+  p = fmaf(t, p, +1.488493726e-04f);
+  p = fmaf(t, p, -1.190488110e-03f);
+  p = fmaf(t, p, +8.333289996e-03f);
+  p = fmaf(t, p, -4.999998957e-02f);
+  return fmaf(t, p, +2.500000000e-01f);
+}
+__device__ __forceinline__ void bezier3_weights(float t, float &E, float &w0, float &w1, float &w2, float &w3) {
+  const float tser = 3.0f;
+  float M0;
+  exp_neg(t, E, M0);
+  const float tb = fmaxf(t, tser);
+  const float tb2 = tb * tb;
+  const float tb3 = tb2 * tb;
+  const float r3 = 1.0f / tb3;
+  const float M1 = fmaf(-tb, E, M0);
+  const float M2 = fmaf(-tb2, E, 2.0f * M1);
+  const float M3 = fmaf(-tb3, E, 3.0f * M2);
+  const float b0 = M3 * r3;
+  const float b1 = (3.0f * fmaf(M2, tb, -M3)) * r3;
+  const float b2 = (3.0f * (fmaf(M1, tb2, -((2.0f * M2) * tb)) + M3)) * r3;
+  const bool ser = t <= tser;
+  const float tE = t * E;
+  w0 = ser ? tE * b3_p3(-t) : b0;
+  w1 = ser ? tE * b3_p2(-t) : b1;
+  w2 = ser ? t * b3_p2(t) : b2;
+  w3 = ser ? t * b3_p3(t) : ((M0 - b0) - b1) - b2;
+}
+
 // Taylor sums of the FP64 forms below |t| = 0.1 where the closed forms cancel:
 // sum_{k=k0}^{k0+11} scale (-1)^k t^(k-shift)/k!  (Psi: k0=2, shift=1; U1: k0=2,
 // shift=0; q: k0=3, shift=1, scale=-2), truncation below 1e-17 relative.

@@ -40,11 +40,12 @@ def _flags(arrays, extra=0) -> int:
 
 def weights(which: int, t, fp64: bool = False):
     """K0 elementwise: 0 exp_neg (E, u0), 1 linear_weights (E, W, Psi, Esc),
-    2 parab_moments (E, U0, U1, q), 3 exp4, 4 the library's fp32 log."""
+    2 parab_moments (E, U0, U1, q), 3 exp4, 4 the library's fp32 log,
+    5 bezier3_weights (w0, w1, w2, w3)."""
     init()
     dt = np.float64 if fp64 else np.float32
     t = np.ascontiguousarray(t, dt)
-    nout = 2 if which == 0 else (1 if which >= 3 else 4)
+    nout = 2 if which == 0 else (1 if which in (3, 4) else 4)
     outs = [np.empty_like(t) for _ in range(nout)] + [None] * (4 - nout)
     check(lib().m3d_weights(C.c_int(which), C.c_int(t.size), ptr(t), *[ptr(o) for o in outs],
                             C.c_uint(FP64 if fp64 else 0)), "m3d_weights")

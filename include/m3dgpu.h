@@ -109,7 +109,8 @@ int m3d_profile_read(int stage, double *ms, long long *launches);
 
 /* ---- K0: the transfer weights, elementwise over n points (diagnostics) ----
  * which: 0 exp_neg (E, u0), 1 linear_weights (E, W, Psi, Esc), 2 parab_moments
- * (E, U0, U1, q), 3 exp4 (y), 4 the library's fp32 log (y).
+ * (E, U0, U1, q), 3 exp4 (y), 4 the library's fp32 log (y), 5 bezier3_weights
+ * (w0, w1, w2, w3; rt_solvers_mod.f90:1280-1331).
  * Replaces exp_neg.inc:20-74 and rt_solvers_mod.f90:785-877. */
 int m3d_weights(int which, int n, const void *t, void *o1, void *o2, void *o3, void *o4, unsigned flags);
 

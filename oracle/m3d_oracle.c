@@ -202,6 +202,64 @@ static inline void pm64(double t, double *E, double *U0, double *U1, double *q)
   }
 }
 
+/* bezier3_weights (rt_solvers_mod.f90:1280-1304): the cubic-Bezier weights over
+ * an interval of optical depth t, w_k = t int_0^1 b_k(u) exp(-t u) du with
+ * b = u^3, 3u^2(1-u), 3u(1-u)^2, (1-u)^3.  For t <= 3 the series t E P3(-t),
+ * t E P2(-t), t P2(t), t P3(t) with P2 = w2/t, P3 = w3/t the reference's own
+ * relative-error minimax fits of degree 10 and 9 (b3_p2, b3_p3, :1305-1331);
+ * above, the moments M_n = n M_(n-1) - t^n E from M0 = 1 - E, formed at
+ * max(t, 3).  The a*b - c forms are fused. */
+static const float B3_P2[11] = {+2.500000000e-01f, -1.000000238e-01f, +2.499995567e-02f, -4.761847202e-03f,
+                                +7.440865738e-04f, -9.924791084e-05f, +1.156294547e-05f, -1.190877015e-06f,
+                                +1.137804801e-07f, -1.100420821e-08f, +7.658396139e-10f};
+static const float B3_P3[10] = {+2.500000000e-01f, -4.999998957e-02f, +8.333289996e-03f, -1.190488110e-03f,
+                                +1.488493726e-04f, -1.653099389e-05f, +1.640762775e-06f, -1.503805294e-07f,
+                                +1.414234507e-08f, -1.025371787e-09f};
+
+static inline float or_b3_p2(float t)
+{
+  float p = fmaf(t, B3_P2[10], B3_P2[9]);
+  for (int k = 8; k >= 0; k--) p = fmaf(t, p, B3_P2[k]);
+  return p;
+}
+static inline float or_b3_p3(float t)
+{
+  float p = fmaf(t, B3_P3[9], B3_P3[8]);
+  for (int k = 7; k >= 0; k--) p = fmaf(t, p, B3_P3[k]);
+  return p;
+}
+
+static inline void bz32(float t, float *E, float *w0, float *w1, float *w2, float *w3)
+{
+  const float tser = 3.0f;
+  float M0;
+  or_exp_neg1(t, E, &M0);
+  const float tb = fmaxf(t, tser);
+  const float tb2 = tb * tb;
+  const float tb3 = tb2 * tb;
+  const float r3 = 1.0f / tb3;
+  const float M1 = fmaf(-tb, *E, M0);
+  const float M2 = fmaf(-tb2, *E, 2.0f * M1);
+  const float M3 = fmaf(-tb3, *E, 3.0f * M2);
+  const float b0 = M3 * r3;
+  const float b1 = (3.0f * fmaf(M2, tb, -M3)) * r3;
+  const float b2 = (3.0f * (fmaf(M1, tb2, -((2.0f * M2) * tb)) + M3)) * r3;
+  const int ser = t <= tser;
+  const float tE = t * *E;
+  *w0 = ser ? tE * or_b3_p3(-t) : b0;
+  *w1 = ser ? tE * or_b3_p2(-t) : b1;
+  *w2 = ser ? t * or_b3_p2(t) : b2;
+  *w3 = ser ? t * or_b3_p3(t) : ((M0 - b0) - b1) - b2;
+}
+
+void or_bezier3_weights_f32(int n, const float *t, float *w0, float *w1, float *w2, float *w3)
+{
+  for (int i = 0; i < n; i++) {
+    float E;
+    bz32(t[i], &E, &w0[i], &w1[i], &w2[i], &w3[i]);
+  }
+}
+
 void or_linear_weights_f32(int n, const float *t, float *E, float *W, float *Psi, float *Esc)
 {
   for (int i = 0; i < n; i++) lw32(t[i], &E[i], &W[i], &Psi[i], &Esc[i]);

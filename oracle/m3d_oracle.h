@@ -50,6 +50,7 @@ void or_exp_neg_f32(int n, const float *t, float *E, float *u0);
 void or_exp4_f32(int n, const float *x, float *y);
 void or_log_f32(int n, const float *x, float *y);
 void or_linear_weights_f32(int n, const float *t, float *E, float *W, float *Psi, float *Esc);
+void or_bezier3_weights_f32(int n, const float *t, float *w0, float *w1, float *w2, float *w3);
 void or_linear_weights_f64(int n, const double *t, double *E, double *W, double *Psi, double *Esc);
 void or_parab_moments_f32(int n, const float *t, float *E, float *U0, float *U1, float *q);
 void or_parab_moments_f64(int n, const double *t, double *E, double *U0, double *U1, double *q);

@@ -101,6 +101,11 @@ def parab_moments(t, fp64=False):
                  np.float64 if fp64 else np.float32, 4)
 
 
+def bezier3_weights(t):
+    """(w0, w1, w2, w3) of bezier3_weights (rt_solvers_mod.f90:1280-1331), fp32."""
+    return _vec1("or_bezier3_weights_f32", t, np.float32, 4)
+
+
 def set_stencil(ds, vec):
     ds = (C.c_double * 3)(*ds)
     vec = (C.c_double * 3)(*vec)

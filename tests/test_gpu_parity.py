@@ -31,6 +31,8 @@ def test_k0_bit_exact(m3d, oracle):
     eE, eu0 = oracle.exp_neg(t)
     np.testing.assert_array_equal(E, eE)
     np.testing.assert_array_equal(u0, eu0)
+    for g, e in zip(m3d.weights(5, t), oracle.bezier3_weights(t)):
+        np.testing.assert_array_equal(g, e)
     x = np.linspace(-90, 90, 5001).astype(np.float32)
     np.testing.assert_array_equal(m3d.weights(3, x), oracle.exp4(x))
     x = np.float32(np.logspace(-40, 38, 5001))

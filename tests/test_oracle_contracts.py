@@ -5,6 +5,8 @@ Pins (the reference's own stated guarantees, cited):
   * linear_weights: every output within 4 fp32 ulp of exact over -2 <= t <= 90
     (SRC/rt_solvers_mod.f90:772-775); E is clamped at t = 87 by design (:774-775).
   * parab_moments: within 4 ulp over -2 <= t <= 87 (SRC/rt_solvers_mod.f90:858-860).
+  * bezier3_weights: every weight within 8 ulp over -3 <= t <= 87
+    (SRC/rt_solvers_mod.f90:1275-1276).
   * QLG-bot fit: 5.6923e-3 max relative error against qlg_ref_f64
     (HOP/qlg_mod.f90:218-221); the tabulated fp32 form adds the nearest-node error.
   * The window extent never ends inside the true tolerance crossing
@@ -260,3 +262,33 @@ def test_scattering_split_identities(oracle):
     oracle.add_opacity_equi(sp2, llam, chi, eta, xhat, lr, cells, dep_mem=dep, nlevel=2, do_nlte=True,
                             one_m_eps=np.ones_like(xhat), chi_scat=cs)
     assert chi.max() > 0 and not cs.any()
+
+
+def test_bezier3_weights_within_8_ulp(oracle):
+    """bezier3_weights (SRC/rt_solvers_mod.f90:1280-1304): every weight within 8 fp32
+    ulp of the exact Bernstein integrals over -3 <= t <= 87, the reference's stated
+    bound.  Exact values from the moments M_n = n! (1 - e^-t sum_k<=n t^k/k!)."""
+    rng = np.random.default_rng(3)
+    t = np.concatenate([rng.uniform(-3.0, 87.0, 400), np.logspace(-6, 0.4, 60), -np.logspace(-6, 0.47, 60),
+                        [3.0, np.nextafter(np.float32(3.0), np.float32(4.0)), -3.0, 87.0]]).astype(np.float32)
+    t = t[t != 0]
+    got = oracle.bezier3_weights(t)
+    exact = [[], [], [], []]
+    with mpmath.workdps(80):
+        for tt in t.astype(np.float64):
+            x = mpmath.mpf(float(tt))
+            e = mpmath.exp(-x)
+            M = [mpmath.factorial(n) * (1 - e * sum(x ** k / mpmath.factorial(k) for k in range(n + 1)))
+                 for n in range(4)]
+            w0 = M[3] / x ** 3
+            w1 = 3 * (M[2] / x ** 2 - M[3] / x ** 3)
+            w2 = 3 * (M[1] / x - 2 * M[2] / x ** 2 + M[3] / x ** 3)
+            w3 = M[0] - w0 - w1 - w2
+            for k, w in enumerate((w0, w1, w2, w3)):
+                exact[k].append(float(w))
+    for k in range(4):
+        assert _ulp_err(got[k], exact[k]).max() <= 8, k
+    # the weights sum to 1 - e^-t, the integral of the basis against exp(-tau)
+    E, u0 = oracle.exp_neg(t)
+    s = got[0].astype(np.float64) + got[1] + got[2] + got[3]
+    np.testing.assert_allclose(s, u0, rtol=3e-6, atol=1e-12)
