@@ -892,6 +892,54 @@ int m3d_formal_solve(int solver, const m3d_slab_t *slab, void *work, void *psi, 
                                rot_ds_code, rot_bot2pivot, rot_offset, flags);
 }
 
+int m3d_long_char_hermite(const m3d_slab_t *slab, float *work, float *psi, const m3d_hermite_t *h,
+                          unsigned flags) {
+  TRY(need_init());
+  TRY(check_slab(slab));
+  if (!work || !h || !h->beta || !h->pe || !h->dpe_dz || !h->dlnt_dz || !h->temp || !h->hknu)
+    return fail(M3D_EINVAL, "m3d_long_char_hermite: NULL argument");
+  if (slab->nz < 3) return fail(M3D_EINVAL, "m3d_long_char_hermite: needs nz >= 3 (got %d)", slab->nz);
+  if (flags & M3D_FP64) return fail(M3D_EUNSUPPORTED, "m3d_long_char_hermite: FP32 only");
+  const bool gt = h->ghost_pe != nullptr;
+  if (gt && (!h->ghost_dpe_dz || !h->ghost_dlnt_dz || !h->ghost_temp))
+    return fail(M3D_EINVAL, "m3d_long_char_hermite: give all four ghost fields or none");
+  if (!(h->code_length > 0)) return fail(M3D_EINVAL, "m3d_long_char_hermite: code_length must be > 0");
+  const SlabArgs a = slab_args(slab, flags);
+  if (a.get_psi && !psi) return fail(M3D_EINVAL, "m3d_long_char_hermite: get_psi without psi");
+  const int nf = a.nf, nx = a.nx, ny = a.ny, nz = a.nz;
+  const size_t plane = (size_t)nf * nx * ny, cells = (size_t)nx * ny * nz;
+  Staging st(flags);
+  float *dw, *dp = nullptr;
+  TRY(st.map(work, plane * (nz + 2) * 3, true, true, &dw));
+  if (a.get_psi) TRY(st.map(psi, plane * nz, true, true, &dp));
+  HermArgs K{};
+  TRY(st.in(h->beta, plane * nz, &K.beta));
+  TRY(st.in(h->pe, cells, &K.pe));
+  TRY(st.in(h->dpe_dz, cells, &K.dpe_dz));
+  TRY(st.in(h->dlnt_dz, cells, &K.dlnt_dz));
+  TRY(st.in(h->temp, cells, &K.temp));
+  TRY(st.in(h->hknu, nf, &K.hknu));
+  if (gt) {
+    TRY(st.in(h->ghost_pe, (size_t)nx * ny, &K.g_pe));
+    TRY(st.in(h->ghost_dpe_dz, (size_t)nx * ny, &K.g_dpe_dz));
+    TRY(st.in(h->ghost_dlnt_dz, (size_t)nx * ny, &K.g_dlnt_dz));
+    TRY(st.in(h->ghost_temp, (size_t)nx * ny, &K.g_temp));
+  }
+  // the step constants of long_char_hermite's set-up (rt_solvers_mod.f90:1075-1081)
+  const float ds = (float)slab->ds[2];
+  const float dsup = (float)((double)ds / fabs(slab->vec[2]));
+  K.rdsup = 1.0f / dsup;
+  K.dsup1 = 0.5f * dsup;
+  K.dsup2 = (0.0833333358f * dsup) * dsup;
+  K.dtmax = -(float)slab->maser_dtau_max;
+  K.Imax = (float)slab->maser_Inu_max;
+  K.gfac = (float)((double)a.dir * fabs(slab->vec[2]) / h->code_length);
+  K.get_rates = a.get_psi;
+  K.ghost_thermo = gt ? 1 : 0;
+  LAUNCH_S(M3D_STAGE_SOLVE, k_long_char_hermite, grid_for(plane), 256, 0, K, nf, nx, ny, nz, a.dir, dw, dp);
+  return st.finish();
+}
+
 int m3d_rotate_array(const m3d_slab_t *slab, void *work, const double *ds_code, double bot2pivot,
                      const double *ray_offset, unsigned flags) {
   TRY(need_init());

@@ -413,6 +413,165 @@ __global__ void k_long_char_linear(SlabArgs s, T *work, T *psi, T *irem, T *esc,
   }
 }
 
+// long_char_hermite (rt_solvers_mod.f90:1052-1504): the chain-rule cubic-Hermite
+// long characteristics, one thread per (f, x, y), z sequential.  herm_dtau: dchi/ds
+// at both ends by chi = (chi/Pe) Pe from a parabola through three samples,
+// MC-clamped, then the Euler-Maclaurin trapezoid.  herm_source: dS/dtau by
+// S = rho Bnu, the cubic-Bezier control points clamped to [min, max] of the end
+// values, bezier3_weights.  herm_first: the zeroed top ghost's secant step.
+// Slabs of at least 3 planes.
+struct HermArgs {
+  float rdsup, dsup1, dsup2, dtmax, Imax, gfac;
+  int get_rates, ghost_thermo;
+  const float *beta, *pe, *dpe_dz, *dlnt_dz, *temp, *hknu;
+  const float *g_pe, *g_dpe_dz, *g_dlnt_dz, *g_temp;
+};
+
+__device__ __forceinline__ float herm_dtau(const HermArgs &K, float xxup, float xxc, float xx3, float peu, float rpeu,
+                                           float gpu, float pec, float rpec, float gpc, float rpe3, bool center) {
+  const float dtmin = 1e-20f;
+  const float hh = 0.5f * K.rdsup;
+  const float t1 = (xxc - xxup) * K.rdsup;
+  const float sgn = copysignf(1.0f, t1);
+  const float rxpu = xxup * rpeu, rxpc = xxc * rpec, rxp3 = xx3 * rpe3;
+  float drxpu, drxpc;
+  if (center) {
+    drxpc = (rxp3 - rxpu) * hh;
+    drxpu = (fmaf(-3.0f, rxpu, 4.0f * rxpc) - rxp3) * hh;
+  } else {
+    drxpu = (rxpc - rxp3) * hh;
+    drxpc = fmaf(3.0f, rxpc, fmaf(-4.0f, rxpu, rxp3)) * hh;
+  }
+  float mup = fmaf(rxpu, gpu, peu * drxpu);
+  float mc = fmaf(rxpc, gpc, pec * drxpc);
+  mup = sgn * fmaxf(0.0f, fminf(sgn * mup, 2.0f * fabsf(t1)));
+  mc = sgn * fmaxf(0.0f, fminf(sgn * mc, 2.0f * fabsf(t1)));
+  float dt = fmaf(K.dsup1, xxup + xxc, K.dsup2 * (mup - mc));
+  return fmaxf(copysignf(fmaxf(fabsf(dt), dtmin), dt), K.dtmax);
+}
+
+__device__ __forceinline__ void herm_source(const HermArgs &K, float xxup, float xxc, float ssup, float ssc, float ss3,
+                                            float betau, float betac, float beta3, float hk, float Inuup, float aTu,
+                                            float aTc, bool center, float dt, float ex, float w0, float w1, float w2,
+                                            float w3, float &Inu, float &plam) {
+  const float third = 0.333333343f;
+  const float hh = 0.5f * K.rdsup;
+  const float r1mbu = 1.0f / (1.0f - betau), r1mbc = 1.0f / (1.0f - betac), r1mb3 = 1.0f / (1.0f - beta3);
+  const float Bu = betau * r1mbu, Bc = betac * r1mbc, B3 = beta3 * r1mb3;
+  const float rhou = ssup / Bu, rhoc = ssc / Bc, rho3 = ss3 / B3;
+  float drhu, drhc;
+  if (center) {
+    drhc = (rho3 - rhou) * hh;
+    drhu = (fmaf(-3.0f, rhou, 4.0f * rhoc) - rho3) * hh;
+  } else {
+    drhu = (rhoc - rho3) * hh;
+    drhc = fmaf(3.0f, rhoc, fmaf(-4.0f, rhou, rho3)) * hh;
+  }
+  const float rxxu = 1.0f / xxup, rxxc = 1.0f / xxc;
+  const float gu = ((hk * r1mbu) * aTu) * rxxu;
+  const float gc = ((hk * r1mbc) * aTc) * rxxc;
+  const float dt3 = dt * third;
+  float P1 = fmaf(dt3, fmaf(ssup, gu, (Bu * drhu) * rxxu), ssup);
+  float P2 = fmaf(-dt3, fmaf(ssc, gc, (Bc * drhc) * rxxc), ssc);
+  const float smin = fminf(ssup, ssc), smax = fmaxf(ssup, ssc);
+  P1 = fminf(fmaxf(P1, smin), smax);
+  P2 = fminf(fmaxf(P2, smin), smax);
+  const float I = fmaf(w3, ssc, fmaf(w2, P2, fmaf(w1, P1, fmaf(w0, ssup, Inuup * ex))));
+  Inu = fmaxf(-K.Imax, fminf(K.Imax, I));
+  const float d1 = fminf(fmaxf((Bu * third) / Bc, 0.0f), 1.0f);
+  const float d2 = fminf(fmaxf(fmaf(-dt3, gc, 0.666666687f), 0.0f), 1.0f);
+  plam = (K.get_rates && dt > 0 && xxc > 0) ? (fmaf(w1, d1, w2 * d2) + w3) * rxxc : 0.0f;
+}
+
+__device__ __forceinline__ void herm_first(const HermArgs &K, float xxup, float xxc, float xxdn, float ssup, float ssc,
+                                           float ssdn, float betac, float betadn, float hk, float Inuup, float pec,
+                                           float rpec, float rpedn, float gpc, float aTc, float &Inu, float &plam) {
+  const float dtmin = 1e-20f, third = 0.333333343f;
+  const float t1 = (xxc - xxup) * K.rdsup;
+  const float sgn = copysignf(1.0f, t1);
+  const float rxpc = xxc * rpec;
+  float mc = fmaf(rxpc, gpc, (pec * fmaf(xxdn, rpedn, -rxpc)) * K.rdsup);
+  mc = sgn * fmaxf(0.0f, fminf(sgn * mc, 2.0f * fabsf(t1)));
+  float dt = fmaf(K.dsup1, xxup + xxc, K.dsup2 * (t1 - mc));
+  dt = fmaxf(copysignf(fmaxf(fabsf(dt), dtmin), dt), K.dtmax);
+  float ex, w0, w1, w2, w3;
+  bezier3_weights(dt, ex, w0, w1, w2, w3);
+  const float r1mbc = 1.0f / (1.0f - betac), r1mbdn = 1.0f / (1.0f - betadn);
+  const float Bc = betac * r1mbc, Bdn = betadn * r1mbdn;
+  const float Gc = ((hk * r1mbc) * aTc) / xxc;
+  const float rhoc = ssc / Bc, rhodn = ssdn / Bdn;
+  float taudn = K.dsup1 * (xxc + xxdn);
+  taudn = copysignf(fmaxf(fabsf(taudn), dtmin), taudn);
+  const float dSc = fmaf(ssc, Gc, (Bc * (rhodn - rhoc)) / taudn);
+  const float dSu = (ssc - ssup) / dt;
+  const float dt3 = dt * third;
+  float P1 = fmaf(dt3, dSu, ssup);
+  float P2 = fmaf(-dt3, dSc, ssc);
+  const float smin = fminf(ssup, ssc), smax = fmaxf(ssup, ssc);
+  P1 = fminf(fmaxf(P1, smin), smax);
+  P2 = fminf(fmaxf(P2, smin), smax);
+  const float I = fmaf(w3, ssc, fmaf(w2, P2, fmaf(w1, P1, fmaf(w0, ssup, Inuup * ex))));
+  Inu = fmaxf(-K.Imax, fminf(K.Imax, I));
+  plam = (K.get_rates && dt > 0 && xxc > 0) ? (fmaf(w1, third, w2) + w3) / xxc : 0.0f;
+}
+
+__global__ void k_long_char_hermite(HermArgs K, int nf, int nx, int ny, int nz, int dir, float *work, float *psi) {
+  const size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (g >= (size_t)nf * nx * ny) return;
+  const int f = (int)(g % nf), x = (int)((g / nf) % nx), y = (int)(g / ((size_t)nf * nx));
+  const size_t plane = (size_t)nf * nx * ny, k1 = plane * (nz + 2);
+  const size_t cplane = (size_t)nx * ny, cxy = (size_t)x + (size_t)nx * y;
+  const int zs = dir > 0 ? 1 : nz, ze = dir > 0 ? nz : 1;
+  const float hk = K.hknu[f];
+  for (int i = 0, z = zs; i < nz; i++, z += dir) {
+    const int zup = z - dir;
+    const bool first = z == zs, last = z == ze;
+    const int zt = last ? ze - 2 * dir : z + dir;
+    const size_t cz = cxy + cplane * (size_t)(z - 1);
+    const float pec = K.pe[cz], rpec = 1.0f / pec;
+    const float gpc = K.gfac * K.dpe_dz[cz];
+    const float aTc = (K.gfac * K.dlnt_dz[cz]) / K.temp[cz];
+    const size_t wz = g + plane * (size_t)z, wu = g + plane * (size_t)zup;
+    const size_t pz = g + plane * (size_t)(z - 1);
+    float I, pl;
+    if (first && !K.ghost_thermo) {
+      const int zdn = z + dir;
+      const size_t wd = g + plane * (size_t)zdn;
+      const float rpedn = 1.0f / K.pe[cxy + cplane * (size_t)(zdn - 1)];
+      herm_first(K, work[wu], work[wz], work[wd], work[wu + k1], work[wz + k1], work[wd + k1], K.beta[pz],
+                 K.beta[g + plane * (size_t)(zdn - 1)], hk, work[wu + 2 * k1], pec, rpec, rpedn, gpc, aTc, I, pl);
+    } else {
+      float peu, rpeu, gpu, aTu, bu;
+      if (first) {
+        peu = K.g_pe[cxy];
+        rpeu = 1.0f / peu;
+        gpu = K.gfac * K.g_dpe_dz[cxy];
+        const float rTup = 1.0f / K.g_temp[cxy];
+        aTu = (K.gfac * K.g_dlnt_dz[cxy]) * rTup;
+        bu = fmaxf(exp4(-(hk * rTup)), FLT_MIN);
+      } else {
+        const size_t cu = cxy + cplane * (size_t)(zup - 1);
+        peu = K.pe[cu];
+        rpeu = 1.0f / peu;
+        gpu = K.gfac * K.dpe_dz[cu];
+        aTu = (K.gfac * K.dlnt_dz[cu]) / K.temp[cu];
+        bu = K.beta[g + plane * (size_t)(zup - 1)];
+      }
+      const float rpet = 1.0f / K.pe[cxy + cplane * (size_t)(zt - 1)];
+      const size_t wt = g + plane * (size_t)zt;
+      const float xxup = work[wu], xxc = work[wz];
+      const float dt = herm_dtau(K, xxup, xxc, work[wt], peu, rpeu, gpu, pec, rpec, gpc, rpet, !last);
+      float ex, w0, w1, w2, w3;
+      bezier3_weights(dt, ex, w0, w1, w2, w3);
+      herm_source(K, xxup, xxc, work[wu + k1], work[wz + k1], work[wt + k1], bu, K.beta[pz],
+                  K.beta[g + plane * (size_t)(zt - 1)], hk, work[wu + 2 * k1], aTu, aTc, !last, dt, ex, w0, w1, w2,
+                  w3, I, pl);
+    }
+    work[wz + 2 * k1] = I;
+    if (psi && K.get_rates) psi[pz] = pl;
+  }
+}
+
 template <typename T>
 __device__ __forceinline__ T dt500_of(double dsup, double c, double cu) {
   const double r = cu / c;

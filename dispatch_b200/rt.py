@@ -207,6 +207,30 @@ def formal_solve(solver, slab, work, psi=None, irem=None, escape=None, chi500=No
                                  C.c_double(b2p), off, C.c_uint(flags)), "m3d_formal_solve")
 
 
+class Hermite(C.Structure):
+    """m3d_hermite_t."""
+
+    _fields_ = [(k, C.c_void_p) for k in ("beta", "pe", "dpe_dz", "dlnt_dz", "temp", "hknu", "ghost_pe",
+                                           "ghost_dpe_dz", "ghost_dlnt_dz", "ghost_temp")] + [("code_length",
+                                                                                               C.c_double)]
+
+
+def long_char_hermite(slab, work, psi, beta, pe, dpe_dz, dlnt_dz, temp, hknu, ghost=None, code_length=1.0):
+    """long_char_hermite (rt_solvers_mod.f90:1052-1504) of one slab, in place on work
+    (float32).  ghost: dict pe, dpe_dz, dlnt_dz, temp (ny, nx) of the upstream
+    ghost's state, or None for the zeroed top ghost."""
+    init()
+    dev = _is_dev(work)
+    conv = (lambda a: a) if dev else (lambda a: np.ascontiguousarray(a, _F32))
+    keep = [conv(a) for a in (beta, pe, dpe_dz, dlnt_dz, temp, hknu)]
+    g = [None] * 4 if not ghost else [conv(ghost[k]) for k in ("pe", "dpe_dz", "dlnt_dz", "temp")]
+    keep += g
+    h = Hermite(*[ptr(a) for a in keep[:6]], *[ptr(a) for a in g], float(code_length))
+    check(lib().m3d_long_char_hermite(C.byref(slab), ptr(work), ptr(psi), C.byref(h),
+                                      C.c_uint(DEVICE_PTRS if dev else 0)), "m3d_long_char_hermite")
+    del keep
+
+
 def rotate_array(slab, work, ds_code, bot2pivot, ray_offset=(0.0, 0.0)):
     init()
     check(lib().m3d_rotate_array(C.byref(slab), ptr(work), (C.c_double * 3)(*ds_code), C.c_double(bot2pivot),

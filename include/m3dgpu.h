@@ -183,6 +183,24 @@ int m3d_formal_solve(int solver, const m3d_slab_t *slab, void *work, void *psi, 
                      const int *eta_row, const unsigned char *eta_mask, const double *rot_ds_code,
                      double rot_bot2pivot, const double *rot_offset, unsigned flags);
 
+/* ---- long_char_hermite (rt_solvers_mod.f90:1052-1504), the optional 'hermite'
+ * solver: chain-rule cubic-Hermite long characteristics along z for one slab of
+ * at least 3 planes, FP32.  work (nf, nx, ny, 0:nz+1, 3) holds chi, Snu and the
+ * upstream ghost plane (m3d_upstream_boundary); Inu is written to slot 3 and, with
+ * slab->get_psi, the Lambda diagonal per chi to psi (nf, nx, ny, nz).  The ghost's
+ * thermodynamic state (the model below the bottom, or an upstream neighbour's
+ * exit plane) takes the full step; without it (all ghost_* NULL) the first plane
+ * takes herm_first's secant step from the zeroed top ghost. */
+typedef struct {
+  const float *beta;                                   /* (nf, nx, ny, nz): exp(-h nu/kT) */
+  const float *pe, *dpe_dz, *dlnt_dz, *temp;           /* (nx, ny, nz): Pe, dPe/dz, dlnT/dz, T */
+  const float *hknu;                                   /* (nf): h nu / k */
+  const float *ghost_pe, *ghost_dpe_dz, *ghost_dlnt_dz, *ghost_temp; /* (nx, ny), or NULL */
+  double code_length;                                  /* cm per length unit of the d/dz (scaling%l) */
+} m3d_hermite_t;
+int m3d_long_char_hermite(const m3d_slab_t *slab, float *work, float *psi, const m3d_hermite_t *h,
+                          unsigned flags);
+
 /* rotate_array (rt_patch_mod.f90:3809-3866) on work(:,:,:,1:nz,1:2), in place. */
 int m3d_rotate_array(const m3d_slab_t *slab, void *work, const double *ds_code, double bot2pivot,
                      const double *ray_offset, unsigned flags);

@@ -810,3 +810,196 @@ static inline double huge_f64(void) { return DBL_MAX; }
 #define LW lw64
 #define PM pm64
 #include "or_solvers.inc"
+
+/* =========================================================================
+ * long_char_hermite (rt_solvers_mod.f90:1052-1504), fp32: the chain-rule
+ * cubic-Hermite long characteristics.  dchi/ds by chi = (chi/Pe) Pe and dS/dtau
+ * by S = rho Bnu from parabolas through three samples (herm_dtau, herm_source),
+ * cubic-Bezier weights (bezier3_weights), the monotone clamp of the control
+ * points.  The first plane starts from the upstream ghost: with its
+ * thermodynamic state given (the bottom's ghost model or an upstream
+ * neighbour) the full step, else the zeroed top ghost's secant step
+ * (herm_first).  Slabs of at least 3 planes (the third parabola sample is then
+ * always a plane of the slab).  The a*b + c forms are fused as listed.
+ * ========================================================================= */
+typedef struct {
+  float rdsup, dsup1, dsup2, dtmax, Imax;
+  int get_rates;
+} or_herm_c;
+
+static float herm_dtau(const or_herm_c *K, float xxup, float xxc, float xx3, float peu, float rpeu, float gpu,
+                       float pec, float rpec, float gpc, float rpe3, int center)
+{
+  const float dtmin = 1e-20f;
+  const float hh = 0.5f * K->rdsup;
+  const float t1 = (xxc - xxup) * K->rdsup;
+  const float sgn = copysignf(1.0f, t1);
+  const float rxpu = xxup * rpeu, rxpc = xxc * rpec, rxp3 = xx3 * rpe3;
+  float drxpu, drxpc;
+  if (center) {
+    drxpc = (rxp3 - rxpu) * hh;
+    drxpu = (fmaf(-3.0f, rxpu, 4.0f * rxpc) - rxp3) * hh;
+  } else {
+    drxpu = (rxpc - rxp3) * hh;
+    drxpc = fmaf(3.0f, rxpc, fmaf(-4.0f, rxpu, rxp3)) * hh;
+  }
+  float mup = fmaf(rxpu, gpu, peu * drxpu);
+  float mc = fmaf(rxpc, gpc, pec * drxpc);
+  mup = sgn * fmaxf(0.0f, fminf(sgn * mup, 2.0f * fabsf(t1)));
+  mc = sgn * fmaxf(0.0f, fminf(sgn * mc, 2.0f * fabsf(t1)));
+  float dt = fmaf(K->dsup1, xxup + xxc, K->dsup2 * (mup - mc));
+  dt = fmaxf(copysignf(fmaxf(fabsf(dt), dtmin), dt), K->dtmax);
+  return dt;
+}
+
+static void herm_source(const or_herm_c *K, float xxup, float xxc, float ssup, float ssc, float ss3, float betau,
+                        float betac, float beta3, float hk, float Inuup, float aTu, float aTc, int center, float dt,
+                        float ex, float w0, float w1, float w2, float w3, float *Inu, float *plam)
+{
+  const float third = 0.333333343f;
+  const float hh = 0.5f * K->rdsup;
+  const float r1mbu = 1.0f / (1.0f - betau), r1mbc = 1.0f / (1.0f - betac), r1mb3 = 1.0f / (1.0f - beta3);
+  const float Bu = betau * r1mbu, Bc = betac * r1mbc, B3 = beta3 * r1mb3;
+  const float rhou = ssup / Bu, rhoc = ssc / Bc, rho3 = ss3 / B3;
+  float drhu, drhc;
+  if (center) {
+    drhc = (rho3 - rhou) * hh;
+    drhu = (fmaf(-3.0f, rhou, 4.0f * rhoc) - rho3) * hh;
+  } else {
+    drhu = (rhoc - rho3) * hh;
+    drhc = fmaf(3.0f, rhoc, fmaf(-4.0f, rhou, rho3)) * hh;
+  }
+  const float rxxu = 1.0f / xxup, rxxc = 1.0f / xxc;
+  const float gu = ((hk * r1mbu) * aTu) * rxxu;
+  const float gc = ((hk * r1mbc) * aTc) * rxxc;
+  const float dt3 = dt * third;
+  float P1 = fmaf(dt3, fmaf(ssup, gu, (Bu * drhu) * rxxu), ssup);
+  float P2 = fmaf(-dt3, fmaf(ssc, gc, (Bc * drhc) * rxxc), ssc);
+  const float smin = fminf(ssup, ssc), smax = fmaxf(ssup, ssc);
+  P1 = fminf(fmaxf(P1, smin), smax);
+  P2 = fminf(fmaxf(P2, smin), smax);
+  float I = fmaf(w3, ssc, fmaf(w2, P2, fmaf(w1, P1, fmaf(w0, ssup, Inuup * ex))));
+  *Inu = fmaxf(-K->Imax, fminf(K->Imax, I));
+  const float d1 = fminf(fmaxf((Bu * third) / Bc, 0.0f), 1.0f);
+  const float d2 = fminf(fmaxf(fmaf(-dt3, gc, 0.666666687f), 0.0f), 1.0f);
+  *plam = (K->get_rates && dt > 0 && xxc > 0) ? (fmaf(w1, d1, w2 * d2) + w3) * rxxc : 0.0f;
+}
+
+static void herm_first(const or_herm_c *K, float xxup, float xxc, float xxdn, float ssup, float ssc, float ssdn,
+                       float betac, float betadn, float hk, float Inuup, float pec, float rpec, float rpedn,
+                       float gpc, float aTc, float *Inu, float *plam)
+{
+  const float dtmin = 1e-20f, third = 0.333333343f;
+  const float t1 = (xxc - xxup) * K->rdsup;
+  const float sgn = copysignf(1.0f, t1);
+  const float rxpc = xxc * rpec;
+  float mc = fmaf(rxpc, gpc, (pec * fmaf(xxdn, rpedn, -rxpc)) * K->rdsup);
+  mc = sgn * fmaxf(0.0f, fminf(sgn * mc, 2.0f * fabsf(t1)));
+  float dt = fmaf(K->dsup1, xxup + xxc, K->dsup2 * (t1 - mc));
+  dt = fmaxf(copysignf(fmaxf(fabsf(dt), dtmin), dt), K->dtmax);
+  float ex, w0, w1, w2, w3;
+  bz32(dt, &ex, &w0, &w1, &w2, &w3);
+  const float r1mbc = 1.0f / (1.0f - betac), r1mbdn = 1.0f / (1.0f - betadn);
+  const float Bc = betac * r1mbc, Bdn = betadn * r1mbdn;
+  const float Gc = ((hk * r1mbc) * aTc) / xxc;
+  const float rhoc = ssc / Bc, rhodn = ssdn / Bdn;
+  float taudn = K->dsup1 * (xxc + xxdn);
+  taudn = copysignf(fmaxf(fabsf(taudn), dtmin), taudn);
+  const float dSc = fmaf(ssc, Gc, (Bc * (rhodn - rhoc)) / taudn);
+  const float dSu = (ssc - ssup) / dt;
+  const float dt3 = dt * third;
+  float P1 = fmaf(dt3, dSu, ssup);
+  float P2 = fmaf(-dt3, dSc, ssc);
+  const float smin = fminf(ssup, ssc), smax = fmaxf(ssup, ssc);
+  P1 = fminf(fmaxf(P1, smin), smax);
+  P2 = fminf(fmaxf(P2, smin), smax);
+  float I = fmaf(w3, ssc, fmaf(w2, P2, fmaf(w1, P1, fmaf(w0, ssup, Inuup * ex))));
+  *Inu = fmaxf(-K->Imax, fminf(K->Imax, I));
+  *plam = (K->get_rates && dt > 0 && xxc > 0) ? (fmaf(w1, third, w2) + w3) / xxc : 0.0f;
+}
+
+/* work (nf, nx, ny, 0:nz+1, 3) with the upstream ghost plane already set; beta
+ * (nf, nx, ny, nz); pe, dpe_dz, dlnt_dz, temp (nx, ny, nz); hknu (nf) = h/k nu;
+ * g_* (nx, ny) the ghost's thermodynamics, all NULL for the zeroed top ghost;
+ * gfac = dir |mu| / (code length) converts the d/dz to d/ds along the ray. */
+int or_long_char_hermite(const or_slab_t *s, float *work, float *psi, const float *beta, const float *pe,
+                         const float *dpe_dz, const float *dlnt_dz, const float *temp, const float *hknu,
+                         const float *g_pe, const float *g_dpe_dz, const float *g_dlnt_dz, const float *g_temp,
+                         double code_length)
+{
+  const int nf = s->nf, nx = s->nx, ny = s->ny, nz = s->nz, dir = s->dir;
+  if (nz < 3) return 1;
+  const float ds = (float)(s->ds[2]);
+  const float dsup = (float)((double)ds / fabs(s->vec[2]));
+  or_herm_c K;
+  K.rdsup = 1.0f / dsup;
+  K.dsup1 = 0.5f * dsup;
+  K.dsup2 = (0.0833333358f * dsup) * dsup;
+  K.dtmax = -(float)s->maser_dtau_max;
+  K.Imax = (float)s->maser_Inu_max;
+  K.get_rates = s->get_psi;
+  const float gfac = (float)((double)dir * fabs(s->vec[2]) / code_length);
+  const int ghost_thermo = g_pe != NULL;
+  const int zs = dir > 0 ? 1 : nz, ze = dir > 0 ? nz : 1;
+#define HW(f, x, y, z, k) ((size_t)(f) + (size_t)nf * ((size_t)(x) + (size_t)nx * ((size_t)(y) + (size_t)ny * ((size_t)(z) + (size_t)(nz + 2) * (size_t)(k)))))
+#define HP(f, x, y, z) ((size_t)(f) + (size_t)nf * ((size_t)(x) + (size_t)nx * ((size_t)(y) + (size_t)ny * (size_t)((z) - 1))))
+#define HC(x, y, z) ((size_t)(x) + (size_t)nx * ((size_t)(y) + (size_t)ny * (size_t)((z) - 1)))
+  for (int z = zs; dir > 0 ? z <= ze : z >= ze; z += dir) {
+    const int zup = z - dir;
+    const int first = z == zs, last = z == ze;
+    const int center = !last;
+    const int zt = last ? ze - 2 * dir : z + dir;
+    for (int y = 0; y < ny; y++)
+      for (int x = 0; x < nx; x++) {
+        const float pec = pe[HC(x, y, z)], rpec = 1.0f / pec;
+        const float gpc = gfac * dpe_dz[HC(x, y, z)];
+        const float aTc = (gfac * dlnt_dz[HC(x, y, z)]) / temp[HC(x, y, z)];
+        if (first && !ghost_thermo) {
+          const int zdn = z + dir;
+          const float rpedn = 1.0f / pe[HC(x, y, zdn)];
+          for (int f = 0; f < nf; f++) {
+            float I, pl;
+            herm_first(&K, work[HW(f, x, y, zup, 0)], work[HW(f, x, y, z, 0)], work[HW(f, x, y, zdn, 0)],
+                       work[HW(f, x, y, zup, 1)], work[HW(f, x, y, z, 1)], work[HW(f, x, y, zdn, 1)],
+                       beta[HP(f, x, y, z)], beta[HP(f, x, y, zdn)], hknu[f], work[HW(f, x, y, zup, 2)], pec, rpec,
+                       rpedn, gpc, aTc, &I, &pl);
+            work[HW(f, x, y, z, 2)] = I;
+            if (psi && K.get_rates) psi[HP(f, x, y, z)] = pl;
+          }
+          continue;
+        }
+        float peu, rpeu, gpu, aTu, rTup = 0.0f;
+        if (first) {
+          peu = g_pe[x + (size_t)nx * y];
+          rpeu = 1.0f / peu;
+          gpu = gfac * g_dpe_dz[x + (size_t)nx * y];
+          rTup = 1.0f / g_temp[x + (size_t)nx * y];
+          aTu = (gfac * g_dlnt_dz[x + (size_t)nx * y]) * rTup;
+        } else {
+          peu = pe[HC(x, y, zup)];
+          rpeu = 1.0f / peu;
+          gpu = gfac * dpe_dz[HC(x, y, zup)];
+          aTu = (gfac * dlnt_dz[HC(x, y, zup)]) / temp[HC(x, y, zup)];
+        }
+        const float rpet = 1.0f / pe[HC(x, y, zt)];
+        for (int f = 0; f < nf; f++) {
+          const float bu = first ? fmaxf(or_exp4(-(hknu[f] * rTup)), FLT_MIN) : beta[HP(f, x, y, zup)];
+          const float xxup = work[HW(f, x, y, zup, 0)], xxc = work[HW(f, x, y, z, 0)];
+          const float dt = herm_dtau(&K, xxup, xxc, work[HW(f, x, y, zt, 0)], peu, rpeu, gpu, pec, rpec, gpc, rpet,
+                                     center);
+          float ex, w0, w1, w2, w3;
+          bz32(dt, &ex, &w0, &w1, &w2, &w3);
+          float I, pl;
+          herm_source(&K, xxup, xxc, work[HW(f, x, y, zup, 1)], work[HW(f, x, y, z, 1)], work[HW(f, x, y, zt, 1)], bu,
+                      beta[HP(f, x, y, z)], beta[HP(f, x, y, zt)], hknu[f], work[HW(f, x, y, zup, 2)], aTu, aTc,
+                      center, dt, ex, w0, w1, w2, w3, &I, &pl);
+          work[HW(f, x, y, z, 2)] = I;
+          if (psi && K.get_rates) psi[HP(f, x, y, z)] = pl;
+        }
+      }
+  }
+#undef HW
+#undef HP
+#undef HC
+  return 0;
+}

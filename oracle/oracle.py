@@ -287,6 +287,22 @@ def formal_solve(solver, slab: Slab, work, psi=None, irem=None, escape=None, chi
         raise RuntimeError(f"oracle formal_solve rc={rc}")
 
 
+def long_char_hermite(slab: Slab, work, psi, beta, pe, dpe_dz, dlnt_dz, temp, hknu, ghost=None,
+                      code_length=1.0):
+    """long_char_hermite (rt_solvers_mod.f90:1052-1504) in place on work (fp32).
+    ghost: dict pe, dpe_dz, dlnt_dz, temp (ny, nx) of the upstream ghost, or None
+    for the zeroed top ghost."""
+    f32 = lambda a: np.ascontiguousarray(a, np.float32)
+    g = ghost or {}
+    args = [f32(x) for x in (beta, pe, dpe_dz, dlnt_dz, temp, hknu)]
+    gargs = [None if not g else f32(g[k]) for k in ("pe", "dpe_dz", "dlnt_dz", "temp")]
+    assert work.dtype == np.float32 and work.flags.c_contiguous
+    rc = lib().or_long_char_hermite(C.byref(slab), _p(work), _p(psi), *[_p(a) for a in args],
+                                    *[_p(a) for a in gargs], C.c_double(code_length))
+    if rc:
+        raise RuntimeError(f"oracle long_char_hermite rc={rc}")
+
+
 def rotate_array(slab: Slab, work, ds_code, bot2pivot, ray_offset=(0.0, 0.0)):
     fp64 = work.dtype == np.float64
     fn = lib().or_rotate_array_f64 if fp64 else lib().or_rotate_array_f32

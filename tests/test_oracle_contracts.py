@@ -292,3 +292,55 @@ def test_bezier3_weights_within_8_ulp(oracle):
     E, u0 = oracle.exp_neg(t)
     s = got[0].astype(np.float64) + got[1] + got[2] + got[3]
     np.testing.assert_allclose(s, u0, rtol=3e-6, atol=1e-12)
+
+
+def test_hermite_isothermal_exact(oracle):
+    """long_char_hermite in an isothermal slab of constant chi with Snu = Bnu: the
+    control points sit on the flat source and the Bezier weights sum to 1 - e^-dtau,
+    so every plane holds I = S (1 - e^-dtau) + I_up e^-dtau to fp32 rounding, through
+    the full step from the ghost's state (upward) and through herm_first's secant
+    step without it (downward), a flat ghost plane of incoming I = 1 in both."""
+    nf, nx, ny, nz = 4, 2, 2, 8
+    for d in (1, -1):
+        s = oracle.make_slab(nf, nx, ny, nz, d, [1e6] * 3, [0.0, 0.0, float(d)], get_psi=True)
+        work = np.zeros((3, nz + 2, ny, nx, nf), np.float32)
+        work[0] = 2e-7
+        work[1] = 3.0
+        zg = 0 if d > 0 else nz + 1
+        work[2, zg] = 1.0
+        beta = np.full((nz, ny, nx, nf), 0.75, np.float32)          # Bnu = beta/(1-beta) = 3
+        pe = np.full((nz, ny, nx), 10.0, np.float32)
+        zero = np.zeros_like(pe)
+        T = np.full_like(pe, 6000.0)
+        hk = np.full(nf, 1e-4, np.float32)
+        ghost = {k: v[0] for k, v in (("pe", pe), ("dpe_dz", zero), ("dlnt_dz", zero), ("temp", T))} if d > 0 else None
+        psi = np.zeros((nz, ny, nx, nf), np.float32)
+        oracle.long_char_hermite(s, work, psi, beta, pe, zero, zero, T, hk, ghost=ghost)
+        E = math.exp(-2e-7 * 1e6)
+        I = 1.0
+        for k in range(nz):
+            I = I * E + 3.0 * (1 - E)
+            z = 1 + k if d > 0 else nz - k
+            np.testing.assert_allclose(work[2, z], I, rtol=3e-6)
+        assert psi.min() > 0
+
+
+def test_hermite_agrees_with_linear_solver_on_smooth_slab(oracle):
+    """On a smooth stratified LTE slab the cubic-Hermite and the linear long
+    characteristics agree to the linear solver's truncation error."""
+    import sys
+    import os
+    sys.path.insert(0, os.path.dirname(__file__))
+    from hermite_cases import slab_case
+    work, fld, ghosts, ds = slab_case(seed=9, nz=40, ds=5e5)
+    nz, ny, nx, nf = work.shape[1] - 2, work.shape[2], work.shape[3], work.shape[4]
+    w_h = work.copy()
+    w_h[2, 0] = w_h[1, 0]
+    w_l = w_h.copy()
+    s = oracle.make_slab(nf, nx, ny, nz, 1, [ds] * 3, [0.0, 0.0, 1.0])
+    oracle.long_char_hermite(s, w_h, None, *[fld[k] for k in ("beta", "pe", "dpe_dz", "dlnt_dz", "temp", "hknu")],
+                             ghost=ghosts["bottom"])
+    oracle.formal_solve(oracle.LINEAR, s, w_l)
+    rel = np.abs(w_h[2, 1:-1] - w_l[2, 1:-1]) / w_l[2, 1:-1]
+    assert np.isfinite(w_h).all()
+    assert rel.max() < 1e-2
