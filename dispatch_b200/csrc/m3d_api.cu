@@ -940,6 +940,48 @@ int m3d_long_char_hermite(const m3d_slab_t *slab, float *work, float *psi, const
   return st.finish();
 }
 
+int m3d_long_char_hermite2(const m3d_slab_t *slab, float *work, float *psi, const float *pe, const float *dpe_dz,
+                           const float *ghost_pe, const float *ghost_dpe_dz, int ghost, double code_length,
+                           unsigned flags) {
+  TRY(need_init());
+  TRY(check_slab(slab));
+  if (!work || !pe || !dpe_dz) return fail(M3D_EINVAL, "m3d_long_char_hermite2: NULL argument");
+  if (slab->nz < 2) return fail(M3D_EINVAL, "m3d_long_char_hermite2: needs nz >= 2 (got %d)", slab->nz);
+  if (flags & M3D_FP64) return fail(M3D_EUNSUPPORTED, "m3d_long_char_hermite2: FP32 only");
+  if (ghost < 0 || ghost > 2) return fail(M3D_EINVAL, "m3d_long_char_hermite2: ghost must be 0, 1 or 2 (got %d)", ghost);
+  if (ghost && (!ghost_pe || !ghost_dpe_dz))
+    return fail(M3D_EINVAL, "m3d_long_char_hermite2: ghost %d needs ghost_pe and ghost_dpe_dz", ghost);
+  if (!(code_length > 0)) return fail(M3D_EINVAL, "m3d_long_char_hermite2: code_length must be > 0");
+  const SlabArgs a = slab_args(slab, flags);
+  if (a.get_psi && !psi) return fail(M3D_EINVAL, "m3d_long_char_hermite2: get_psi without psi");
+  const int nf = a.nf, nx = a.nx, ny = a.ny, nz = a.nz;
+  const size_t plane = (size_t)nf * nx * ny, cells = (size_t)nx * ny * nz;
+  Staging st(flags);
+  float *dw, *dp = nullptr;
+  TRY(st.map(work, plane * (nz + 2) * 3, true, true, &dw));
+  if (a.get_psi) TRY(st.map(psi, plane * nz, true, true, &dp));
+  Herm2Args K{};
+  TRY(st.in(pe, cells, &K.pe));
+  TRY(st.in(dpe_dz, cells, &K.dpe_dz));
+  if (ghost) {
+    TRY(st.in(ghost_pe, (size_t)nx * ny, &K.g_pe));
+    TRY(st.in(ghost_dpe_dz, (size_t)nx * ny, &K.g_dpe_dz));
+  }
+  // the step constants of long_char_hermite2's set-up (rt_solvers_mod.f90:1560-1566)
+  const float ds = (float)slab->ds[2];
+  const float dsup = (float)((double)ds / fabs(slab->vec[2]));
+  K.rdsup = 1.0f / dsup;
+  K.dsup1 = 0.5f * dsup;
+  K.dsup2 = (0.0833333358f * dsup) * dsup;
+  K.dtmax = -slab->maser_dtau_max;
+  K.Imax = (float)slab->maser_Inu_max;
+  K.gfac = (float)((double)a.dir * fabs(slab->vec[2]) / code_length);
+  K.get_rates = a.get_psi;
+  K.ghost = ghost;
+  LAUNCH_S(M3D_STAGE_SOLVE, k_long_char_hermite2, grid_for(plane), 256, 0, K, nf, nx, ny, nz, a.dir, dw, dp);
+  return st.finish();
+}
+
 int m3d_rotate_array(const m3d_slab_t *slab, void *work, const double *ds_code, double bot2pivot,
                      const double *ray_offset, unsigned flags) {
   TRY(need_init());

@@ -572,6 +572,144 @@ __global__ void k_long_char_hermite(HermArgs K, int nf, int nx, int ny, int nz, 
   }
 }
 
+// long_char_hermite2 (rt_solvers_mod.f90:1536-1895): the hybrid solver, one thread
+// per (f, x, y), z sequential.  dtau by herm_dtau's chain rule with the control-point
+// bound 3 |secant|; dtau, 1/dtau and the parabola's weights in FP64 as the reference
+// declares them; the source is long_char_quadratic's parabola with dS/dtau at the
+// target MC-limited from the two adjacent secants (herm2_step), on the last plane a
+// one-sided difference when the third sample is a plane of the slab, and the zeroed
+// top ghost's secant step (herm2_first).  ghost: 0 zeroed top, 1 neighbour, 2 bottom.
+struct Herm2Args {
+  float rdsup, dsup1, dsup2, Imax, gfac;
+  double dtmax;
+  int get_rates, ghost;
+  const float *pe, *dpe_dz, *g_pe, *g_dpe_dz;
+};
+
+__device__ __forceinline__ double herm2_clamp(double dt, double dtmax) {
+  return fmax(copysign(fmax(fabs(dt), (double)1e-20f), dt), dtmax);
+}
+
+__device__ __forceinline__ void herm2_weights(const Herm2Args &K, double dt, double rdt, float ex, float U0, float U1,
+                                              float q, float xxc, float ssup, float ssc, float dsdtau, float Inuup,
+                                              float &Inu, float &plam) {
+  const double B = __dmul_rn(__dsub_rn(2.0 * (double)U1, (double)q), rdt);
+  const double A = __dsub_rn((double)U0, B);
+  const float C = q - U1;
+  const float I = fmaf(C, dsdtau, fmaf((float)B, ssc, fmaf((float)A, ssup, Inuup * ex)));
+  Inu = fmaxf(-K.Imax, fminf(K.Imax, I));
+  plam = (K.get_rates && dt > 0 && xxc > 0) ? (float)B / xxc : 0.0f;
+}
+
+__device__ __forceinline__ void herm2_step(const Herm2Args &K, float xxup, float xxc, float xx3, float ssup,
+                                           float ssc, float ss3, float Inuup, float peu, float rpeu, float gpu,
+                                           float pec, float rpec, float gpc, float pe3, float rpe3, float gp3,
+                                           bool center, bool onesided, float &Inu, float &plam) {
+  const float hh = 0.5f * K.rdsup;
+  const float t1 = (xxc - xxup) * K.rdsup;
+  const float sgn = copysignf(1.0f, t1);
+  const float rxpu = xxup * rpeu, rxpc = xxc * rpec, rxp3 = xx3 * rpe3;
+  float drxpu, drxpc;
+  if (center) {
+    drxpc = (rxp3 - rxpu) * hh;
+    drxpu = (fmaf(-3.0f, rxpu, 4.0f * rxpc) - rxp3) * hh;
+  } else {
+    drxpu = (rxpc - rxp3) * hh;
+    drxpc = fmaf(3.0f, rxpc, fmaf(-4.0f, rxpu, rxp3)) * hh;
+  }
+  float mup = fmaf(rxpu, gpu, peu * drxpu);
+  float mc = fmaf(rxpc, gpc, pec * drxpc);
+  mup = sgn * fmaxf(0.0f, fminf(sgn * mup, 3.0f * fabsf(t1)));
+  mc = sgn * fmaxf(0.0f, fminf(sgn * mc, 3.0f * fabsf(t1)));
+  const double dt = herm2_clamp((double)fmaf(K.dsup1, xxup + xxc, K.dsup2 * (mup - mc)), K.dtmax);
+  const double rdt = __drcp_rn(dt);
+  float ex, U0, U1, q;
+  parab_moments((float)dt, ex, U0, U1, q);
+  const float s1 = (ssc - ssup) * (float)rdt;
+  float dsdtau = s1;
+  if (center) {
+    const float t3 = (xx3 - xxc) * K.rdsup;
+    const float sgn3 = copysignf(1.0f, t3);
+    const float drxp3 = fmaf(3.0f, rxp3, fmaf(-4.0f, rxpc, rxpu)) * hh;
+    float m3 = fmaf(rxp3, gp3, pe3 * drxp3);
+    m3 = sgn3 * fmaxf(0.0f, fminf(sgn3 * m3, 3.0f * fabsf(t3)));
+    const double dt3 = herm2_clamp((double)fmaf(K.dsup1, xxc + xx3, K.dsup2 * (mc - m3)), K.dtmax);
+    const float s3 = (ss3 - ssc) / (float)dt3;
+    const float avg = 0.5f * (s1 + s3);
+    dsdtau = (copysignf(1.0f, s1) + copysignf(1.0f, s3)) * fminf(fminf(fabsf(s1), fabsf(s3)), fabsf(0.5f * avg));
+  } else if (onesided && xxc > 0.0f) {
+    const float d = (fmaf(3.0f, ssc, fmaf(-4.0f, ssup, ss3)) * hh) / xxc;
+    const float sg = copysignf(1.0f, s1);
+    dsdtau = sg * fmaxf(0.0f, fminf(sg * d, 2.0f * fabsf(s1)));
+  }
+  herm2_weights(K, dt, rdt, ex, U0, U1, q, xxc, ssup, ssc, dsdtau, Inuup, Inu, plam);
+}
+
+__device__ __forceinline__ void herm2_first(const Herm2Args &K, float xxup, float xxc, float xxdn, float ssup,
+                                            float ssc, float Inuup, float pec, float rpec, float rpedn, float gpc,
+                                            float &Inu, float &plam) {
+  const float t1 = (xxc - xxup) * K.rdsup;
+  const float sgn = copysignf(1.0f, t1);
+  const float rxpc = xxc * rpec;
+  float mc = fmaf(rxpc, gpc, (pec * fmaf(xxdn, rpedn, -rxpc)) * K.rdsup);
+  mc = sgn * fmaxf(0.0f, fminf(sgn * mc, 3.0f * fabsf(t1)));
+  const double dt = herm2_clamp((double)fmaf(K.dsup1, xxup + xxc, K.dsup2 * (t1 - mc)), K.dtmax);
+  const double rdt = __drcp_rn(dt);
+  float ex, U0, U1, q;
+  parab_moments((float)dt, ex, U0, U1, q);
+  const float dsdtau = (ssc - ssup) * (float)rdt;
+  herm2_weights(K, dt, rdt, ex, U0, U1, q, xxc, ssup, ssc, dsdtau, Inuup, Inu, plam);
+}
+
+__global__ void k_long_char_hermite2(Herm2Args K, int nf, int nx, int ny, int nz, int dir, float *work, float *psi) {
+  const size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (g >= (size_t)nf * nx * ny) return;
+  const int x = (int)((g / nf) % nx), y = (int)(g / ((size_t)nf * nx));
+  const size_t plane = (size_t)nf * nx * ny, k1 = plane * (nz + 2);
+  const size_t cplane = (size_t)nx * ny, cxy = (size_t)x + (size_t)nx * y;
+  const int zs = dir > 0 ? 1 : nz, ze = dir > 0 ? nz : 1;
+  for (int i = 0, z = zs; i < nz; i++, z += dir) {
+    const int zup = z - dir;
+    const bool first = z == zs, last = z == ze;
+    const size_t cz = cxy + cplane * (size_t)(z - 1);
+    const float pec = K.pe[cz], rpec = 1.0f / pec;
+    const float gpc = K.gfac * K.dpe_dz[cz];
+    float peu = 0.0f, rpeu = 0.0f, gpu = 0.0f;
+    if (first && K.ghost) {
+      peu = K.g_pe[cxy];
+      rpeu = 1.0f / peu;
+      gpu = K.gfac * K.g_dpe_dz[cxy];
+    } else if (!first) {
+      const size_t cu = cxy + cplane * (size_t)(zup - 1);
+      peu = K.pe[cu];
+      rpeu = 1.0f / peu;
+      gpu = K.gfac * K.dpe_dz[cu];
+    }
+    const int z3 = last ? z - 2 * dir : z + dir;
+    float pe3 = 0.0f, rpe3, gp3 = 0.0f;
+    if (!last) {
+      const size_t c3 = cxy + cplane * (size_t)(z3 - 1);
+      pe3 = K.pe[c3];
+      rpe3 = 1.0f / pe3;
+      gp3 = K.gfac * K.dpe_dz[c3];
+    } else if (nz >= 3) {
+      rpe3 = 1.0f / K.pe[cxy + cplane * (size_t)(z3 - 1)];
+    } else {
+      rpe3 = K.ghost == 1 ? 1.0f / K.g_pe[cxy] : rpec;
+    }
+    const size_t wz = g + plane * (size_t)z, wu = g + plane * (size_t)zup, w3 = g + plane * (size_t)z3;
+    float I, pl;
+    if (first && !K.ghost)
+      herm2_first(K, work[wu], work[wz], work[w3], work[wu + k1], work[wz + k1], work[wu + 2 * k1], pec, rpec, rpe3,
+                  gpc, I, pl);
+    else
+      herm2_step(K, work[wu], work[wz], work[w3], work[wu + k1], work[wz + k1], work[w3 + k1], work[wu + 2 * k1], peu,
+                 rpeu, gpu, pec, rpec, gpc, pe3, rpe3, gp3, !last, last && nz >= 3, I, pl);
+    work[wz + 2 * k1] = I;
+    if (psi && K.get_rates) psi[g + plane * (size_t)(z - 1)] = pl;
+  }
+}
+
 template <typename T>
 __device__ __forceinline__ T dt500_of(double dsup, double c, double cu) {
   const double r = cu / c;

@@ -231,6 +231,23 @@ def long_char_hermite(slab, work, psi, beta, pe, dpe_dz, dlnt_dz, temp, hknu, gh
     del keep
 
 
+def long_char_hermite2(slab, work, psi, pe, dpe_dz, ghost=None, ghost_kind=0, code_length=1.0):
+    """long_char_hermite2 (rt_solvers_mod.f90:1536-1895) of one slab, in place on work
+    (float32).  ghost: dict pe, dpe_dz (ny, nx) of the upstream ghost, or None for
+    the zeroed top ghost; ghost_kind 1 = an upstream neighbour's exit plane,
+    2 = the model below the bottom (the default when a ghost is given)."""
+    init()
+    dev = _is_dev(work)
+    conv = (lambda a: a) if dev else (lambda a: np.ascontiguousarray(a, _F32))
+    keep = [conv(pe), conv(dpe_dz)]
+    g = [None, None] if not ghost else [conv(ghost["pe"]), conv(ghost["dpe_dz"])]
+    kind = 0 if not ghost else (ghost_kind or 2)
+    check(lib().m3d_long_char_hermite2(C.byref(slab), ptr(work), ptr(psi), ptr(keep[0]), ptr(keep[1]), ptr(g[0]),
+                                       ptr(g[1]), C.c_int(kind), C.c_double(code_length),
+                                       C.c_uint(DEVICE_PTRS if dev else 0)), "m3d_long_char_hermite2")
+    del keep, g
+
+
 def rotate_array(slab, work, ds_code, bot2pivot, ray_offset=(0.0, 0.0)):
     init()
     check(lib().m3d_rotate_array(C.byref(slab), ptr(work), (C.c_double * 3)(*ds_code), C.c_double(bot2pivot),

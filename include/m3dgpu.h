@@ -201,6 +201,20 @@ typedef struct {
 int m3d_long_char_hermite(const m3d_slab_t *slab, float *work, float *psi, const m3d_hermite_t *h,
                           unsigned flags);
 
+/* ---- long_char_hermite2 (rt_solvers_mod.f90:1536-1895), the optional 'hermite2'
+ * solver: dtau by long_char_hermite's chain rule (control points bounded by
+ * 3 |secant|), the source by long_char_quadratic's parabola with dS/dtau at the
+ * target MC-limited from the two adjacent intervals; dtau, 1/dtau and the weights
+ * in FP64 as the reference declares them.  One slab of at least 2 planes, FP32;
+ * work and psi as m3d_long_char_hermite.  pe, dpe_dz (nx, ny, nz); ghost selects
+ * the upstream ghost's Pe: 0 the zeroed top ghost (ghost_* NULL; herm2_first's
+ * secant step), 1 an upstream neighbour's exit plane, 2 the model below the bottom
+ * (ghost_pe, ghost_dpe_dz (nx, ny)); 1 and 2 differ only for nz == 2, where the
+ * last plane's third sample is the ghost and only a neighbour supplies its Pe. */
+int m3d_long_char_hermite2(const m3d_slab_t *slab, float *work, float *psi, const float *pe, const float *dpe_dz,
+                           const float *ghost_pe, const float *ghost_dpe_dz, int ghost, double code_length,
+                           unsigned flags);
+
 /* rotate_array (rt_patch_mod.f90:3809-3866) on work(:,:,:,1:nz,1:2), in place. */
 int m3d_rotate_array(const m3d_slab_t *slab, void *work, const double *ds_code, double bot2pivot,
                      const double *ray_offset, unsigned flags);

@@ -1003,3 +1003,171 @@ int or_long_char_hermite(const or_slab_t *s, float *work, float *psi, const floa
 #undef HC
   return 0;
 }
+
+/* =========================================================================
+ * long_char_hermite2 (rt_solvers_mod.f90:1536-1895), fp32 with the reference's
+ * real(8) dtau, 1/dtau and weights: the hybrid solver.  dtau as herm_dtau with
+ * the control-point bound |dchi/ds| <= 3 |secant| (herm2_step :1758-1862);
+ * the source is long_char_quadratic's parabola, dS/dtau at the target MC-limited
+ * from the secants of the two intervals beside it (the second interval's dtau by
+ * the same chain rule), on the last plane the backward one-sided difference over
+ * (two-up, up, target) clamped to 2 |secant| when that sample is a plane of the
+ * slab, else the interval secant.  herm2_first (:1869-1894) is the zeroed top
+ * ghost's step.  Slabs of at least 2 planes.  ghost: 0 the zeroed top ghost,
+ * 1 an upstream neighbour's exit plane, 2 the bottom's ghost model; 1 and 2
+ * differ only for nz == 2 (the last plane's third-sample Pe, :1704-1709).
+ * ========================================================================= */
+typedef struct {
+  float rdsup, dsup1, dsup2, Imax;
+  double dtmax;
+  int get_rates;
+} or_herm2_c;
+
+static double herm2_clamp(double dt, double dtmax)
+{
+  return fmax(copysign(fmax(fabs(dt), (double)1e-20f), dt), dtmax);
+}
+
+static void herm2_weights(const or_herm2_c *K, double dt, double rdt, float ex, float U0, float U1, float q,
+                          float xxc, float ssup, float ssc, float dsdtau, float Inuup, float *Inu, float *plam)
+{
+  const double B = (2.0 * (double)U1 - (double)q) * rdt;
+  const double A = (double)U0 - B;
+  const float C = q - U1;
+  const float I = fmaf(C, dsdtau, fmaf((float)B, ssc, fmaf((float)A, ssup, Inuup * ex)));
+  *Inu = fmaxf(-K->Imax, fminf(K->Imax, I));
+  *plam = (K->get_rates && dt > 0 && xxc > 0) ? (float)B / xxc : 0.0f;
+}
+
+static void herm2_step(const or_herm2_c *K, float xxup, float xxc, float xx3, float ssup, float ssc, float ss3,
+                       float Inuup, float peu, float rpeu, float gpu, float pec, float rpec, float gpc, float pe3,
+                       float rpe3, float gp3, int center, int onesided, float *Inu, float *plam)
+{
+  const float hh = 0.5f * K->rdsup;
+  const float t1 = (xxc - xxup) * K->rdsup;
+  const float sgn = copysignf(1.0f, t1);
+  const float rxpu = xxup * rpeu, rxpc = xxc * rpec, rxp3 = xx3 * rpe3;
+  float drxpu, drxpc;
+  if (center) {
+    drxpc = (rxp3 - rxpu) * hh;
+    drxpu = (fmaf(-3.0f, rxpu, 4.0f * rxpc) - rxp3) * hh;
+  } else {
+    drxpu = (rxpc - rxp3) * hh;
+    drxpc = fmaf(3.0f, rxpc, fmaf(-4.0f, rxpu, rxp3)) * hh;
+  }
+  float mup = fmaf(rxpu, gpu, peu * drxpu);
+  float mc = fmaf(rxpc, gpc, pec * drxpc);
+  mup = sgn * fmaxf(0.0f, fminf(sgn * mup, 3.0f * fabsf(t1)));
+  mc = sgn * fmaxf(0.0f, fminf(sgn * mc, 3.0f * fabsf(t1)));
+  const double dt = herm2_clamp((double)fmaf(K->dsup1, xxup + xxc, K->dsup2 * (mup - mc)), K->dtmax);
+  const double rdt = 1.0 / dt;
+  float ex, U0, U1, q;
+  pm32((float)dt, &ex, &U0, &U1, &q);
+  const float s1 = (ssc - ssup) * (float)rdt;
+  float dsdtau = s1;
+  if (center) {
+    const float t3 = (xx3 - xxc) * K->rdsup;
+    const float sgn3 = copysignf(1.0f, t3);
+    const float drxp3 = fmaf(3.0f, rxp3, fmaf(-4.0f, rxpc, rxpu)) * hh;
+    float m3 = fmaf(rxp3, gp3, pe3 * drxp3);
+    m3 = sgn3 * fmaxf(0.0f, fminf(sgn3 * m3, 3.0f * fabsf(t3)));
+    const double dt3 = herm2_clamp((double)fmaf(K->dsup1, xxc + xx3, K->dsup2 * (mc - m3)), K->dtmax);
+    const float s3 = (ss3 - ssc) / (float)dt3;
+    const float avg = 0.5f * (s1 + s3);
+    dsdtau = (copysignf(1.0f, s1) + copysignf(1.0f, s3)) * fminf(fminf(fabsf(s1), fabsf(s3)), fabsf(0.5f * avg));
+  } else if (onesided && xxc > 0.0f) {
+    const float d = (fmaf(3.0f, ssc, fmaf(-4.0f, ssup, ss3)) * hh) / xxc;
+    const float sg = copysignf(1.0f, s1);
+    dsdtau = sg * fmaxf(0.0f, fminf(sg * d, 2.0f * fabsf(s1)));
+  }
+  herm2_weights(K, dt, rdt, ex, U0, U1, q, xxc, ssup, ssc, dsdtau, Inuup, Inu, plam);
+}
+
+static void herm2_first(const or_herm2_c *K, float xxup, float xxc, float xxdn, float ssup, float ssc, float Inuup,
+                        float pec, float rpec, float rpedn, float gpc, float *Inu, float *plam)
+{
+  const float t1 = (xxc - xxup) * K->rdsup;
+  const float sgn = copysignf(1.0f, t1);
+  const float rxpc = xxc * rpec;
+  float mc = fmaf(rxpc, gpc, (pec * fmaf(xxdn, rpedn, -rxpc)) * K->rdsup);
+  mc = sgn * fmaxf(0.0f, fminf(sgn * mc, 3.0f * fabsf(t1)));
+  const double dt = herm2_clamp((double)fmaf(K->dsup1, xxup + xxc, K->dsup2 * (t1 - mc)), K->dtmax);
+  const double rdt = 1.0 / dt;
+  float ex, U0, U1, q;
+  pm32((float)dt, &ex, &U0, &U1, &q);
+  const float dsdtau = (ssc - ssup) * (float)rdt;
+  herm2_weights(K, dt, rdt, ex, U0, U1, q, xxc, ssup, ssc, dsdtau, Inuup, Inu, plam);
+}
+
+/* work (nf, nx, ny, 0:nz+1, 3) with the upstream ghost plane set; pe, dpe_dz
+ * (nx, ny, nz); g_pe, g_dpe_dz (nx, ny) the ghost's Pe (ghost 1 or 2) or NULL. */
+int or_long_char_hermite2(const or_slab_t *s, float *work, float *psi, const float *pe, const float *dpe_dz,
+                          const float *g_pe, const float *g_dpe_dz, int ghost, double code_length)
+{
+  const int nf = s->nf, nx = s->nx, ny = s->ny, nz = s->nz, dir = s->dir;
+  if (nz < 2 || ghost < 0 || ghost > 2 || (ghost && (!g_pe || !g_dpe_dz))) return 1;
+  const float ds = (float)(s->ds[2]);
+  const float dsup = (float)((double)ds / fabs(s->vec[2]));
+  or_herm2_c K;
+  K.rdsup = 1.0f / dsup;
+  K.dsup1 = 0.5f * dsup;
+  K.dsup2 = (0.0833333358f * dsup) * dsup;
+  K.dtmax = -s->maser_dtau_max;
+  K.Imax = (float)s->maser_Inu_max;
+  K.get_rates = s->get_psi;
+  const float gfac = (float)((double)dir * fabs(s->vec[2]) / code_length);
+  const int zs = dir > 0 ? 1 : nz, ze = dir > 0 ? nz : 1;
+#define HW(f, x, y, z, k) ((size_t)(f) + (size_t)nf * ((size_t)(x) + (size_t)nx * ((size_t)(y) + (size_t)ny * ((size_t)(z) + (size_t)(nz + 2) * (size_t)(k)))))
+#define HP(f, x, y, z) ((size_t)(f) + (size_t)nf * ((size_t)(x) + (size_t)nx * ((size_t)(y) + (size_t)ny * (size_t)((z) - 1))))
+#define HC(x, y, z) ((size_t)(x) + (size_t)nx * ((size_t)(y) + (size_t)ny * (size_t)((z) - 1)))
+  for (int z = zs; dir > 0 ? z <= ze : z >= ze; z += dir) {
+    const int zup = z - dir;
+    const int first = z == zs, last = z == ze;
+    for (int y = 0; y < ny; y++)
+      for (int x = 0; x < nx; x++) {
+        const size_t cxy = x + (size_t)nx * y;
+        const float pec = pe[HC(x, y, z)], rpec = 1.0f / pec;
+        const float gpc = gfac * dpe_dz[HC(x, y, z)];
+        float peu = 0.0f, rpeu = 0.0f, gpu = 0.0f;
+        if (first && ghost) {
+          peu = g_pe[cxy];
+          rpeu = 1.0f / peu;
+          gpu = gfac * g_dpe_dz[cxy];
+        } else if (!first) {
+          peu = pe[HC(x, y, zup)];
+          rpeu = 1.0f / peu;
+          gpu = gfac * dpe_dz[HC(x, y, zup)];
+        }
+        /* the third parabola sample: downwind, or on the last plane two planes up */
+        const int z3 = last ? z - 2 * dir : z + dir;
+        float pe3 = 0.0f, rpe3, gp3 = 0.0f;
+        if (!last) {
+          pe3 = pe[HC(x, y, z3)];
+          rpe3 = 1.0f / pe3;
+          gp3 = gfac * dpe_dz[HC(x, y, z3)];
+        } else if (nz >= 3) {
+          rpe3 = 1.0f / pe[HC(x, y, z3)];
+        } else {
+          rpe3 = ghost == 1 ? 1.0f / g_pe[cxy] : rpec;
+        }
+        for (int f = 0; f < nf; f++) {
+          float I, pl;
+          if (first && !ghost)
+            herm2_first(&K, work[HW(f, x, y, zup, 0)], work[HW(f, x, y, z, 0)], work[HW(f, x, y, z3, 0)],
+                        work[HW(f, x, y, zup, 1)], work[HW(f, x, y, z, 1)], work[HW(f, x, y, zup, 2)], pec, rpec,
+                        rpe3, gpc, &I, &pl);
+          else
+            herm2_step(&K, work[HW(f, x, y, zup, 0)], work[HW(f, x, y, z, 0)], work[HW(f, x, y, z3, 0)],
+                       work[HW(f, x, y, zup, 1)], work[HW(f, x, y, z, 1)], work[HW(f, x, y, z3, 1)],
+                       work[HW(f, x, y, zup, 2)], peu, rpeu, gpu, pec, rpec, gpc, pe3, rpe3, gp3, !last,
+                       last && nz >= 3, &I, &pl);
+          work[HW(f, x, y, z, 2)] = I;
+          if (psi && K.get_rates) psi[HP(f, x, y, z)] = pl;
+        }
+      }
+  }
+#undef HW
+#undef HP
+#undef HC
+  return 0;
+}

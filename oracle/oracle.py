@@ -303,6 +303,22 @@ def long_char_hermite(slab: Slab, work, psi, beta, pe, dpe_dz, dlnt_dz, temp, hk
         raise RuntimeError(f"oracle long_char_hermite rc={rc}")
 
 
+def long_char_hermite2(slab: Slab, work, psi, pe, dpe_dz, ghost=None, ghost_kind=0, code_length=1.0):
+    """long_char_hermite2 (rt_solvers_mod.f90:1536-1895) in place on work (fp32).
+    ghost: dict pe, dpe_dz (ny, nx) of the upstream ghost, or None for the zeroed
+    top ghost; ghost_kind 1 = an upstream neighbour's exit plane, 2 = the bottom's
+    ghost model (they differ only for nz == 2)."""
+    f32 = lambda a: np.ascontiguousarray(a, np.float32)
+    g = [None, None] if not ghost else [f32(ghost["pe"]), f32(ghost["dpe_dz"])]
+    kind = 0 if not ghost else (ghost_kind or 2)
+    pe, dpe_dz = f32(pe), f32(dpe_dz)
+    assert work.dtype == np.float32 and work.flags.c_contiguous
+    rc = lib().or_long_char_hermite2(C.byref(slab), _p(work), _p(psi), _p(pe), _p(dpe_dz), _p(g[0]), _p(g[1]),
+                                     C.c_int(kind), C.c_double(code_length))
+    if rc:
+        raise RuntimeError(f"oracle long_char_hermite2 rc={rc}")
+
+
 def rotate_array(slab: Slab, work, ds_code, bot2pivot, ray_offset=(0.0, 0.0)):
     fp64 = work.dtype == np.float64
     fn = lib().or_rotate_array_f64 if fp64 else lib().or_rotate_array_f32

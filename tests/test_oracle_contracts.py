@@ -344,3 +344,87 @@ def test_hermite_agrees_with_linear_solver_on_smooth_slab(oracle):
     rel = np.abs(w_h[2, 1:-1] - w_l[2, 1:-1]) / w_l[2, 1:-1]
     assert np.isfinite(w_h).all()
     assert rel.max() < 1e-2
+
+
+def _hermite2_linear_source_case(oracle, d, nz, ghost_kind, chi_slope=0.0, ghost_pe=10.0):
+    """Chi = chi0 (1 + chi_slope z), constant Pe, Snu linear in z, incoming I = 1."""
+    nf, nx, ny = 3, 2, 2
+    chi, ds = 3e-7, 1e6
+    s = oracle.make_slab(nf, nx, ny, nz, d, [ds] * 3, [0.0, 0.0, float(d)], get_psi=True)
+    work = np.zeros((3, nz + 2, ny, nx, nf), np.float32)
+    zz = np.arange(nz + 2, dtype=np.float64)
+    work[0] = (chi * (1.0 + chi_slope * zz))[:, None, None, None]
+    work[1] = (2.0 + 0.25 * zz)[:, None, None, None]
+    zg = 0 if d > 0 else nz + 1
+    pe = np.full((nz, ny, nx), 10.0, np.float32)
+    zero = np.zeros_like(pe)
+    ghost = {"pe": np.full_like(pe[0], ghost_pe), "dpe_dz": zero[0]} if ghost_kind else None
+    if not ghost_kind:
+        work[:2, zg] = 0.0                        # the zeroed top ghost
+    work[2, zg] = 1.0
+    psi = np.zeros((nz, ny, nx, nf), np.float32)
+    oracle.long_char_hermite2(s, work, psi, pe, zero, ghost=ghost, ghost_kind=ghost_kind)
+    return work, psi, chi * ds
+
+
+def test_hermite2_linear_source_exact(oracle):
+    """long_char_hermite2 with constant chi and Pe and a source linear in tau: the
+    chain-rule dtau is chi ds, the MC-limited dS/dtau of two equal secants and the
+    last plane's one-sided difference are both the exact slope, and the parabolic
+    weights integrate a linear source exactly, so every plane holds
+    I = I_up e^-D + S_c (1 - e^-D) - s (1 - e^-D (1 + D)) to fp32 rounding, for
+    slabs of 2 and 9 planes in both directions."""
+    for d in (1, -1):
+        for nz in (2, 9):
+            work, psi, D = _hermite2_linear_source_case(oracle, d, nz, 2)
+            E = math.exp(-D)
+            I = 1.0
+            sl = 0.25 * d / D                     # dS/dtau along the ray
+            for k in range(nz):
+                z = 1 + k if d > 0 else nz - k
+                Sc = 2.0 + 0.25 * z
+                I = I * E + Sc * (1 - E) - sl * (1 - E * (1 + D))
+                np.testing.assert_allclose(work[2, z], I, rtol=2e-6)
+            assert psi.min() > 0
+
+
+def test_hermite2_zeroed_ghost_and_neighbour_kinds(oracle):
+    """The zeroed top ghost's first step (herm2_first) stays finite and positive.
+    A neighbour's exit plane and the bottom's ghost model give the same slab of 9
+    planes; in a slab of 2 the last plane's third sample is the ghost, whose Pe
+    only the neighbour supplies, and the two differ there alone."""
+    work, psi, _ = _hermite2_linear_source_case(oracle, -1, 9, 0, chi_slope=0.1)
+    assert np.isfinite(work).all() and work[2, 1:-1].min() > 0 and psi.min() > 0
+    a = _hermite2_linear_source_case(oracle, 1, 9, 1, chi_slope=0.1, ghost_pe=20.0)[0]
+    b = _hermite2_linear_source_case(oracle, 1, 9, 2, chi_slope=0.1, ghost_pe=20.0)[0]
+    np.testing.assert_array_equal(a, b)
+    a = _hermite2_linear_source_case(oracle, 1, 2, 1, chi_slope=0.1, ghost_pe=20.0)[0]
+    b = _hermite2_linear_source_case(oracle, 1, 2, 2, chi_slope=0.1, ghost_pe=20.0)[0]
+    np.testing.assert_array_equal(a[2, 1], b[2, 1])
+    assert not np.array_equal(a[2, 2], b[2, 2])
+
+
+def test_hermite2_agrees_with_hermite_on_smooth_slab(oracle):
+    """On a smooth stratified LTE slab the hybrid solver agrees with the linear
+    long characteristics and with the full cubic-Hermite solver to the linear
+    solver's truncation error."""
+    import sys
+    import os
+    sys.path.insert(0, os.path.dirname(__file__))
+    from hermite_cases import slab_case
+    work, fld, ghosts, ds = slab_case(seed=9, nz=40, ds=5e5)
+    nz, ny, nx, nf = work.shape[1] - 2, work.shape[2], work.shape[3], work.shape[4]
+    w_h = work.copy()
+    w_h[2, 0] = w_h[1, 0]
+    w_l, w_2 = w_h.copy(), w_h.copy()
+    s = oracle.make_slab(nf, nx, ny, nz, 1, [ds] * 3, [0.0, 0.0, 1.0])
+    oracle.long_char_hermite(s, w_h, None, *[fld[k] for k in ("beta", "pe", "dpe_dz", "dlnt_dz", "temp", "hknu")],
+                             ghost=ghosts["bottom"])
+    oracle.long_char_hermite2(s, w_2, None, fld["pe"], fld["dpe_dz"], ghost=ghosts["bottom"], ghost_kind=2)
+    oracle.formal_solve(oracle.LINEAR, s, w_l)
+    inner = slice(1, nz + 1)
+    rel_l = np.abs(w_2[2, inner] - w_l[2, inner]) / w_l[2, inner]
+    rel_h = np.abs(w_2[2, inner] - w_h[2, inner]) / w_h[2, inner]
+    assert np.isfinite(w_2).all()
+    assert rel_l.max() < 1e-2
+    assert rel_h.max() < 1e-2
