@@ -187,6 +187,7 @@ class Staging {
     if (rc_ != M3D_OK) return rc_; \
   } while (0)
 
+int wrap_host(int v, int n) { v %= n; return v < 0 ? v + n : v; }
 int grid_for(size_t n, int block = 256) {
   size_t g = (n + block - 1) / block;
   const size_t cap = (size_t)148 * 32;
@@ -979,6 +980,80 @@ int m3d_long_char_hermite2(const m3d_slab_t *slab, float *work, float *psi, cons
   K.get_rates = a.get_psi;
   K.ghost = ghost;
   LAUNCH_S(M3D_STAGE_SOLVE, k_long_char_hermite2, grid_for(plane), 256, 0, K, nf, nx, ny, nz, a.dir, dw, dp);
+  return st.finish();
+}
+
+int m3d_short_char_hermite(const m3d_slab_t *slab, float *work, float *psi, float *irem, float *escape,
+                           const m3d_hermite3d_t *h, unsigned flags) {
+  TRY(need_init());
+  TRY(check_slab(slab));
+  if (!work || !h || !h->beta || !h->pe || !h->dpe_dx || !h->dpe_dy || !h->dpe_dz || !h->dlnt_dx || !h->dlnt_dy ||
+      !h->dlnt_dz || !h->temp || !h->hknu)
+    return fail(M3D_EINVAL, "m3d_short_char_hermite: NULL argument");
+  if (flags & M3D_FP64) return fail(M3D_EUNSUPPORTED, "m3d_short_char_hermite: FP32 only");
+  if (!(h->code_length > 0)) return fail(M3D_EINVAL, "m3d_short_char_hermite: code_length must be > 0");
+  const SlabArgs a = slab_args(slab, flags);
+  if (a.get_psi && !psi) return fail(M3D_EINVAL, "m3d_short_char_hermite: get_psi without psi");
+  if (a.split_rates && (!irem || !escape)) return fail(M3D_EINVAL, "m3d_short_char_hermite: split_rates without irem/escape");
+  double xk[4], yk[4], dsup;
+  int upo1, upo2;
+  set_stencil(slab->ds, slab->vec, xk, yk, &upo1, &upo2, &dsup);
+  {
+    const double wt1 = -slab->vec[0] / slab->ds[0] * dsup, wt2 = -slab->vec[1] / slab->ds[1] * dsup;
+    if (fabs(wt1) > 1.0 || fabs(wt2) > 1.0)
+      return fail(M3D_EINVAL,
+                  "short characteristics: the upwind point of direction (%g, %g, %g) lies (%g, %g) cells away; "
+                  "the stencil reaches one cell (ds_x >= |v_x/v_z| ds_z)",
+                  slab->vec[0], slab->vec[1], slab->vec[2], wt1, wt2);
+  }
+  const int nf = a.nf, nx = a.nx, ny = a.ny, nz = a.nz;
+  const size_t plane = (size_t)nf * nx * ny, cells = (size_t)nx * ny * nz;
+  Staging st(flags);
+  float *dw, *dp = nullptr, *dr = nullptr, *de = nullptr;
+  TRY(st.map(work, plane * (nz + 2) * 3, true, true, &dw));
+  if (a.get_psi) TRY(st.map(psi, plane * nz, true, true, &dp));
+  if (a.split_rates) {
+    TRY(st.map(irem, plane * nz, true, true, &dr));
+    TRY(st.map(escape, plane * nz, true, true, &de));
+  }
+  SCHermArgs K{};
+  TRY(st.in(h->beta, plane * nz, &K.beta));
+  TRY(st.in(h->pe, cells, &K.pe));
+  TRY(st.in(h->dpe_dx, cells, &K.dpe_dx));
+  TRY(st.in(h->dpe_dy, cells, &K.dpe_dy));
+  TRY(st.in(h->dpe_dz, cells, &K.dpe_dz));
+  TRY(st.in(h->dlnt_dx, cells, &K.dlnt_dx));
+  TRY(st.in(h->dlnt_dy, cells, &K.dlnt_dy));
+  TRY(st.in(h->dlnt_dz, cells, &K.dlnt_dz));
+  TRY(st.in(h->temp, cells, &K.temp));
+  TRY(st.in(h->hknu, nf, &K.hknu));
+  std::vector<int> tab(4 * (nx + ny));
+  for (int x = 0; x < nx; x++)
+    for (int ii = 0; ii < 4; ii++) tab[4 * x + ii] = wrap_host((ii + 1) + (x + 1) + (upo1 - 2), nx);
+  for (int y = 0; y < ny; y++)
+    for (int jj = 0; jj < 4; jj++) tab[4 * nx + 4 * y + jj] = wrap_host((jj + 1) + (y + 1) + (upo2 - 2), ny);
+  void *dtab;
+  TRY(scratch(3, sizeof(int) * tab.size(), &dtab));
+  CUDA_TRY(cudaMemcpyAsync(dtab, tab.data(), sizeof(int) * tab.size(), cudaMemcpyHostToDevice, g_ctx.stream));
+  K.xt = (const int *)dtab;
+  K.yt = K.xt + 4 * nx;
+  K.kx = make_float4((float)xk[0], (float)xk[1], (float)xk[2], (float)xk[3]);
+  K.ky = make_float4((float)yk[0], (float)yk[1], (float)yk[2], (float)yk[3]);
+  // the set-up of short_char_hermite (rt_solvers_mod.f90:1961-1999)
+  const double sg = copysign(1.0, slab->vec[2]) * (double)a.dir;
+  K.v1 = (float)(slab->vec[0] * sg / h->code_length);
+  K.v2 = (float)(slab->vec[1] * sg / h->code_length);
+  K.v3 = (float)(slab->vec[2] * sg / h->code_length);
+  K.dsup05 = 0.5f * (float)dsup;
+  K.rpath = 0.5f / K.dsup05;
+  K.dsc2 = (K.dsup05 * K.dsup05) / 3.0f;
+  K.dtmaxf = -(float)slab->maser_dtau_max;
+  K.dtmax = -slab->maser_dtau_max;
+  K.Imax = (float)slab->maser_Inu_max;
+  const int zs = a.dir > 0 ? 1 : nz;
+  for (int i = 0, z = zs; i < nz; i++, z += a.dir)
+    LAUNCH_S(M3D_STAGE_SOLVE, k_short_char_hermite_plane, grid_for(plane), 256, 0, a, K, z, dw, dp, dr, de);
+  CUDA_TRY(cudaStreamSynchronize(g_ctx.stream));
   return st.finish();
 }
 

@@ -1166,4 +1166,143 @@ __global__ void k_short_char2_plane(SlabArgs s, int z, T *work, T *psi, T *irem,
   if (s.get_psi) psi[p] = ps;
 }
 
+// short_char_hermite (rt_solvers_mod.f90:1917-2248) for plane z: one thread per
+// (f, x, y).  short_char's 4x4 kernel sums and 2x2 minimum, past the first plane
+// also over the ratios chi/Pe and Snu/Bnu formed at the upwind nodes, in the same
+// order as the row pass and the column pass (a fused multiply-add per tap from
+// zero); then the quadratic weights with the product-rule slopes at the target,
+// dtau and the weights in FP64 as declared there, the positivity clamp of dS/dtau
+// resolved by branch so the Lambda diagonal B + C kf follows it.  The first plane
+// takes short_char's linear step.
+struct SCHermArgs {
+  float4 kx, ky;
+  float v1, v2, v3, dsup05, rpath, dsc2, dtmaxf, Imax;
+  double dtmax;
+  const int *xt, *yt;
+  const float *beta, *pe, *dpe_dx, *dpe_dy, *dpe_dz, *dlnt_dx, *dlnt_dy, *dlnt_dz, *temp, *hknu;
+};
+
+__global__ void __launch_bounds__(256) k_short_char_hermite_plane(SlabArgs s, SCHermArgs K, int z, float *work,
+                                                                  float *psi, float *irem, float *esc) {
+  const size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  const int nf = s.nf, nx = s.nx, ny = s.ny, nz = s.nz, dir = s.dir;
+  if (g >= (size_t)nf * nx * ny) return;
+  const int f = (int)(g % nf), x = (int)((g / nf) % nx), y = (int)(g / ((size_t)nf * nx));
+  const int zup = z - dir;
+  const bool chain = z != (dir > 0 ? 1 : nz);
+  const float kx[4] = {K.kx.x, K.kx.y, K.kx.z, K.kx.w}, ky[4] = {K.ky.x, K.ky.y, K.ky.z, K.ky.w};
+  const size_t k1 = (size_t)nf * nx * ny * (nz + 2);
+  float up[5] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+  float mn[5] = {FLT_MAX, FLT_MAX, FLT_MAX, FLT_MAX, FLT_MAX};
+  const int nfld = chain ? 5 : 3;
+  for (int jj = 0; jj < 4; jj++) {
+    const int yu = K.yt[4 * y + jj];
+    float row[5] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+    for (int ii = 0; ii < 4; ii++) {
+      const int xu = K.xt[4 * x + ii];
+      const size_t o = iw(f, xu, yu, zup, 0, nf, nx, ny, nz);
+      float v[5];
+      v[0] = work[o];
+      v[1] = work[o + k1];
+      v[2] = work[o + 2 * k1];
+      v[3] = v[4] = 0.0f;
+      if (chain) {
+        const float rpe = 1.0f / K.pe[ic3(xu, yu, zup, nx, ny)];
+        const float bet = K.beta[ip(f, xu, yu, zup, nf, nx, ny)];
+        v[3] = v[0] * rpe;
+        v[4] = (v[1] * (1.0f - bet)) / bet;
+      }
+      const bool inner = jj >= 1 && jj <= 2 && ii >= 1 && ii <= 2;
+#pragma unroll
+      for (int i = 0; i < 5; i++) {
+        if (i >= nfld) break;
+        row[i] = fmaf(kx[ii], v[i], row[i]);
+        if (inner) mn[i] = fminf(mn[i], v[i]);
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < 5; i++)
+      if (i < nfld) up[i] = fmaf(ky[jj], row[i], up[i]);
+  }
+#pragma unroll
+  for (int i = 0; i < 5; i++)
+    if (i < nfld) up[i] = fmaxf(up[i], mn[i]);
+  const float xxup = up[0], ssup = up[1], Inuup = up[2];
+  const size_t o = iw(f, x, y, z, 0, nf, nx, ny, nz);
+  const float xx = work[o], ss = work[o + k1];
+  const size_t p = ip(f, x, y, z, nf, nx, ny);
+  const float Imax = K.Imax;
+  if (!chain) {
+    const float dt = fmaxf(K.dsup05 * (xxup + xx), K.dtmaxf);
+    float E, W, Psi, Esc;
+    linear_weights(dt, E, W, Psi, Esc);
+    float Inu = fmaf(Psi, ss, fmaf(W, ssup, Inuup * E));
+    if (s.split_rates) {
+      const bool off = dt <= 0 || xx <= 0 || fabsf(Inu) > Imax;
+      const float Irem = fmaf(W, ssup, Inuup * E);
+      Inu = fmaxf(-Imax, fminf(Imax, Inu));
+      Psi = off ? 0.0f : Psi;
+      irem[p] = off ? Inu : Irem;
+      esc[p] = off ? 1.0f : Esc;
+    } else {
+      Inu = fmaxf(-Imax, fminf(Imax, Inu));
+    }
+    work[o + 2 * k1] = Inu;
+    if (s.get_psi) psi[p] = (dt > 0 && xx > 0) ? Psi / xx : 0.0f;
+    return;
+  }
+  const size_t c = ic3(x, y, z, nx, ny);
+  const float gpe = fmaf(K.v3, K.dpe_dz[c], fmaf(K.v2, K.dpe_dy[c], K.v1 * K.dpe_dx[c]));
+  const float aT = fmaf(K.v3, K.dlnt_dz[c], fmaf(K.v2, K.dlnt_dy[c], K.v1 * K.dlnt_dx[c])) / K.temp[c];
+  const float pec = K.pe[c], rpec = 1.0f / pec;
+  const float rxpup = up[3], rhou = up[4];
+  const float betc = K.beta[p];
+  const float t1 = (xx - xxup) * K.rpath;
+  const float sgn = copysignf(1.0f, t1);
+  const float rxpc = xx * rpec;
+  float mc = fmaf(rxpc, gpe, (pec * (rxpc - rxpup)) * K.rpath);
+  mc = sgn * fmaxf(0.0f, fminf(sgn * mc, 2.0f * fabsf(t1)));
+  const double dt = herm2_clamp((double)fmaf(K.dsup05, xxup + xx, K.dsc2 * (t1 - mc)), K.dtmax);
+  const double rdt = __drcp_rn(dt);
+  const float rdt4 = (float)rdt;
+  float ex, U0, U1, q;
+  parab_moments((float)dt, ex, U0, U1, q);
+  const float r1mbc = 1.0f / (1.0f - betc);
+  const float Bc = betc * r1mbc;
+  const float gc = ((K.hknu[f] * r1mbc) * aT) / xx;
+  const float rhoc = ss / Bc;
+  const float t1s = (ss - ssup) * rdt4;
+  const float sgns = copysignf(1.0f, t1s);
+  float dsdtau = fmaf(ss, gc, (Bc * (rhoc - rhou)) * rdt4);
+  float kf, srem;
+  if (sgns * dsdtau <= 0.0f) {
+    dsdtau = 0.0f;
+    kf = 0.0f;
+    srem = 0.0f;
+  } else if (sgns * dsdtau >= 2.0f * fabsf(t1s)) {
+    dsdtau = 2.0f * t1s;
+    kf = 2.0f * rdt4;
+    srem = -((2.0f * rdt4) * ssup);
+  } else {
+    kf = gc + rdt4;
+    srem = -((Bc * rhou) * rdt4);
+  }
+  const double B = __dmul_rn(__dsub_rn(2.0 * (double)U1, (double)q), rdt);
+  const double A = __dsub_rn((double)U0, B);
+  const float C = q - U1;
+  float Inu = fmaf(C, dsdtau, fmaf((float)B, ss, fmaf((float)A, ssup, Inuup * ex)));
+  Inu = fmaxf(-Imax, fminf(Imax, Inu));
+  work[o + 2 * k1] = Inu;
+  if (s.get_psi) {
+    const double pl = __dadd_rn(B, __dmul_rn((double)C, (double)kf));
+    const float Psi_loc = (float)pl;
+    const bool on = dt > 0 && xx > 0 && Psi_loc >= 0.0f && Psi_loc <= 1.0f && fabsf(Inu) < Imax;
+    psi[p] = on ? Psi_loc / xx : 0.0f;
+    if (s.split_rates) {
+      irem[p] = on ? fmaf(C, srem, fmaf((float)A, ssup, Inuup * ex)) : Inu;
+      esc[p] = on ? (float)__dsub_rn(1.0, pl) : 1.0f;
+    }
+  }
+}
+
 }  // namespace m3d

@@ -248,6 +248,28 @@ def long_char_hermite2(slab, work, psi, pe, dpe_dz, ghost=None, ghost_kind=0, co
     del keep, g
 
 
+class Hermite3D(C.Structure):
+    """m3d_hermite3d_t."""
+
+    _fields_ = [(n, C.c_void_p) for n in ("beta", "pe", "dpe_dx", "dpe_dy", "dpe_dz", "dlnt_dx", "dlnt_dy",
+                                          "dlnt_dz", "temp", "hknu")] + [("code_length", C.c_double)]
+
+
+def short_char_hermite(slab, work, psi, irem, esc, beta, pe, dpe_dx, dpe_dy, dpe_dz, dlnt_dx, dlnt_dy, dlnt_dz,
+                       temp, hknu, code_length=1.0):
+    """short_char_hermite (rt_solvers_mod.f90:1917-2248) of one slab, in place on
+    work (float32); psi, irem, esc (nz, ny, nx, nf) or None as the slab's get_psi
+    and split_rates ask."""
+    init()
+    dev = _is_dev(work)
+    conv = (lambda a: a) if dev else (lambda a: np.ascontiguousarray(a, _F32))
+    keep = [conv(a) for a in (beta, pe, dpe_dx, dpe_dy, dpe_dz, dlnt_dx, dlnt_dy, dlnt_dz, temp, hknu)]
+    h = Hermite3D(*[ptr(a) for a in keep], float(code_length))
+    check(lib().m3d_short_char_hermite(C.byref(slab), ptr(work), ptr(psi), ptr(irem), ptr(esc), C.byref(h),
+                                       C.c_uint(DEVICE_PTRS if dev else 0)), "m3d_short_char_hermite")
+    del keep
+
+
 def rotate_array(slab, work, ds_code, bot2pivot, ray_offset=(0.0, 0.0)):
     init()
     check(lib().m3d_rotate_array(C.byref(slab), ptr(work), (C.c_double * 3)(*ds_code), C.c_double(bot2pivot),

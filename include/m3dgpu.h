@@ -215,6 +215,24 @@ int m3d_long_char_hermite2(const m3d_slab_t *slab, float *work, float *psi, cons
                            const float *ghost_pe, const float *ghost_dpe_dz, int ghost, double code_length,
                            unsigned flags);
 
+/* ---- short_char_hermite (rt_solvers_mod.f90:1917-2248), the chain-rule Hermite
+ * short characteristics ('hermite' on the 3D iteration path), FP32: short_char's
+ * 4x4 upwind kernels and 2x2 minimum, also over chi/Pe and Snu/Bnu formed at the
+ * upwind nodes, and the quadratic weights with product-rule slopes along the ray
+ * (directional derivatives from the x/y/z partials); dtau and the weights in FP64
+ * as the reference declares them.  The first plane takes short_char's linear
+ * step.  work, psi, irem, escape as m3d_formal_solve's short characteristics
+ * (periodic x/y, the same stencil precondition); irem/escape with split_rates. */
+typedef struct {
+  const float *beta;                                   /* (nf, nx, ny, nz): exp(-h nu/kT) */
+  const float *pe, *dpe_dx, *dpe_dy, *dpe_dz;          /* (nx, ny, nz): Pe and its partials */
+  const float *dlnt_dx, *dlnt_dy, *dlnt_dz, *temp;     /* (nx, ny, nz): ln T partials, T */
+  const float *hknu;                                   /* (nf): h nu / k */
+  double code_length;                                  /* cm per length unit of the partials */
+} m3d_hermite3d_t;
+int m3d_short_char_hermite(const m3d_slab_t *slab, float *work, float *psi, float *irem, float *escape,
+                           const m3d_hermite3d_t *h, unsigned flags);
+
 /* rotate_array (rt_patch_mod.f90:3809-3866) on work(:,:,:,1:nz,1:2), in place. */
 int m3d_rotate_array(const m3d_slab_t *slab, void *work, const double *ds_code, double bot2pivot,
                      const double *ray_offset, unsigned flags);

@@ -1171,3 +1171,173 @@ int or_long_char_hermite2(const or_slab_t *s, float *work, float *psi, const flo
 #undef HC
   return 0;
 }
+
+/* =========================================================================
+ * short_char_hermite (rt_solvers_mod.f90:1917-2248), fp32 with the reference's
+ * real(8) dtau, 1/dtau and weights: short_char's 4x4 upwind interpolation and
+ * 2x2 minimum limiter, applied also to the ratios chi/Pe and Snu/Bnu formed at
+ * the upwind grid points (:2014-2026), and the quadratic weights with the
+ * product-rule slopes at the target: dchi/ds = (chi/Pe) dPe/ds + Pe d(chi/Pe)/ds
+ * with the directional derivative v.grad, clamped to 2 |secant|; dS/dtau =
+ * S (dBnu/dtau)/Bnu + Bnu d(S/Bnu)/dtau with the positivity clamp resolved by
+ * branch (:2125-2139) so the Lambda diagonal B + C kf (:2155) follows the branch.
+ * The first plane takes short_char's linear step.  Periodic x/y; the AMR
+ * boundary stencil is not supported.
+ * ========================================================================= */
+int or_short_char_hermite(const or_slab_t *s, float *work, float *psi, float *irem, float *esc,
+                          const float *beta, const float *pe, const float *dpe_dx, const float *dpe_dy,
+                          const float *dpe_dz, const float *dlnt_dx, const float *dlnt_dy, const float *dlnt_dz,
+                          const float *temp, const float *hknu, double code_length)
+{
+  const int nf = s->nf, nx = s->nx, ny = s->ny, nz = s->nz, dir = s->dir;
+  double xk[4], yk[4], dsup;
+  int upo1, upo2;
+  or_set_stencil(s->ds, s->vec, xk, yk, &upo1, &upo2, &dsup);
+  float kx[4], ky[4];
+  for (int i = 0; i < 4; i++) { kx[i] = (float)xk[i]; ky[i] = (float)yk[i]; }
+  const double sg = copysign(1.0, s->vec[2]) * (double)dir;
+  const float v1 = (float)(s->vec[0] * sg / code_length);
+  const float v2 = (float)(s->vec[1] * sg / code_length);
+  const float v3 = (float)(s->vec[2] * sg / code_length);
+  const float dsup05 = 0.5f * (float)dsup;
+  const float rpath = 0.5f / dsup05, dsc2 = (dsup05 * dsup05) / 3.0f;
+  const float dtmaxf = -(float)s->maser_dtau_max, Imax = (float)s->maser_Inu_max;
+  const double dtmax = -s->maser_dtau_max;
+  int *xt = (int *)malloc(sizeof(int) * 4 * nx), *yt = (int *)malloc(sizeof(int) * 4 * ny);
+  up_tables_f32(nx, upo1, xt);
+  up_tables_f32(ny, upo2, yt);
+#define HW(f, x, y, z, k) ((size_t)(f) + (size_t)nf * ((size_t)(x) + (size_t)nx * ((size_t)(y) + (size_t)ny * ((size_t)(z) + (size_t)(nz + 2) * (size_t)(k)))))
+#define HP(f, x, y, z) ((size_t)(f) + (size_t)nf * ((size_t)(x) + (size_t)nx * ((size_t)(y) + (size_t)ny * (size_t)((z) - 1))))
+#define HC(x, y, z) ((size_t)(x) + (size_t)nx * ((size_t)(y) + (size_t)ny * (size_t)((z) - 1)))
+  const int zs = dir > 0 ? 1 : nz, ze = dir > 0 ? nz : 1;
+  for (int z = zs; dir > 0 ? z <= ze : z >= ze; z += dir) {
+    const int zup = z - dir;
+    const int chain = z != zs;
+    for (int y = 0; y < ny; y++)
+      for (int x = 0; x < nx; x++) {
+        float gpe = 0.0f, aT = 0.0f, pec = 0.0f, rpec = 0.0f;
+        if (chain) {
+          const size_t c = HC(x, y, z);
+          gpe = fmaf(v3, dpe_dz[c], fmaf(v2, dpe_dy[c], v1 * dpe_dx[c]));
+          aT = fmaf(v3, dlnt_dz[c], fmaf(v2, dlnt_dy[c], v1 * dlnt_dx[c])) / temp[c];
+          pec = pe[c];
+          rpec = 1.0f / pec;
+        }
+        for (int f = 0; f < nf; f++) {
+          /* the upwind values: fields chi, Snu, Inu and, past the first plane, the ratios */
+          const int nfld = chain ? 5 : 3;
+          float up[5], mn[5];
+          for (int i = 0; i < 5; i++) { up[i] = 0.0f; mn[i] = FLT_MAX; }
+          for (int jj = 0; jj < 4; jj++) {
+            const int yu = yt[4 * y + jj];
+            float row[5] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+            for (int ii = 0; ii < 4; ii++) {
+              const int xu = xt[4 * x + ii];
+              float v[5];
+              v[0] = work[HW(f, xu, yu, zup, 0)];
+              v[1] = work[HW(f, xu, yu, zup, 1)];
+              v[2] = work[HW(f, xu, yu, zup, 2)];
+              if (chain) {
+                const float rpe = 1.0f / pe[HC(xu, yu, zup)];
+                const float bet = beta[HP(f, xu, yu, zup)];
+                v[3] = v[0] * rpe;
+                v[4] = (v[1] * (1.0f - bet)) / bet;
+              }
+              for (int i = 0; i < nfld; i++) {
+                row[i] = fmaf(kx[ii], v[i], row[i]);
+                if (jj >= 1 && jj <= 2 && ii >= 1 && ii <= 2) mn[i] = fminf(mn[i], v[i]);
+              }
+            }
+            for (int i = 0; i < nfld; i++) up[i] = fmaf(ky[jj], row[i], up[i]);
+          }
+          for (int i = 0; i < nfld; i++) up[i] = fmaxf(up[i], mn[i]);
+          const float xxup = up[0], ssup = up[1], Inuup = up[2];
+          const float xx = work[HW(f, x, y, z, 0)], ss = work[HW(f, x, y, z, 1)];
+          const size_t p = HP(f, x, y, z);
+          if (!chain) {
+            float dt = fmaxf(dsup05 * (xxup + xx), dtmaxf);
+            float E, W, Psi, Esc;
+            lw32(dt, &E, &W, &Psi, &Esc);
+            float Inu = fmaf(Psi, ss, fmaf(W, ssup, Inuup * E));
+            if (s->split_rates) {
+              const int off = dt <= 0 || xx <= 0 || fabsf(Inu) > Imax;
+              const float Irem = fmaf(W, ssup, Inuup * E);
+              Inu = fmaxf(-Imax, fminf(Imax, Inu));
+              Psi = off ? 0.0f : Psi;
+              irem[p] = off ? Inu : Irem;
+              esc[p] = off ? 1.0f : Esc;
+            } else {
+              Inu = fmaxf(-Imax, fminf(Imax, Inu));
+            }
+            work[HW(f, x, y, z, 2)] = Inu;
+            if (s->get_psi) psi[p] = (dt > 0 && xx > 0) ? Psi / xx : 0.0f;
+            continue;
+          }
+          const float rxpup = up[3], rhou = up[4];
+          const float betc = beta[p];
+          const float t1 = (xx - xxup) * rpath;
+          const float sgn = copysignf(1.0f, t1);
+          const float rxpc = xx * rpec;
+          float mc = fmaf(rxpc, gpe, (pec * (rxpc - rxpup)) * rpath);
+          mc = sgn * fmaxf(0.0f, fminf(sgn * mc, 2.0f * fabsf(t1)));
+          double dt = (double)fmaf(dsup05, xxup + xx, dsc2 * (t1 - mc));
+          dt = fmax(copysign(fmax(fabs(dt), (double)1e-20f), dt), dtmax);
+          const double rdt = 1.0 / dt;
+          const float rdt4 = (float)rdt;
+          float ex, U0, U1, q;
+          pm32((float)dt, &ex, &U0, &U1, &q);
+          const float r1mbc = 1.0f / (1.0f - betc);
+          const float Bc = betc * r1mbc;
+          const float gc = ((hknu[f] * r1mbc) * aT) / xx;
+          const float rhoc = ss / Bc;
+          const float t1s = (ss - ssup) * rdt4;
+          const float sgns = copysignf(1.0f, t1s);
+          float dsdtau = fmaf(ss, gc, (Bc * (rhoc - rhou)) * rdt4);
+          float kf, srem;
+          if (sgns * dsdtau <= 0.0f) {
+            dsdtau = 0.0f;
+            kf = 0.0f;
+            srem = 0.0f;
+          } else if (sgns * dsdtau >= 2.0f * fabsf(t1s)) {
+            dsdtau = 2.0f * t1s;
+            kf = 2.0f * rdt4;
+            srem = -((2.0f * rdt4) * ssup);
+          } else {
+            kf = gc + rdt4;
+            srem = -((Bc * rhou) * rdt4);
+          }
+          const double B = (2.0 * (double)U1 - (double)q) * rdt;
+          const double A = (double)U0 - B;
+          const float C = q - U1;
+          float Inu = fmaf(C, dsdtau, fmaf((float)B, ss, fmaf((float)A, ssup, Inuup * ex)));
+          Inu = fmaxf(-Imax, fminf(Imax, Inu));
+          work[HW(f, x, y, z, 2)] = Inu;
+          if (s->get_psi) {
+            const double pl = B + (double)C * (double)kf;
+            const float Psi_loc = (float)pl;
+            float ps, rm, es;
+            if (dt > 0 && xx > 0 && Psi_loc >= 0.0f && Psi_loc <= 1.0f && fabsf(Inu) < Imax) {
+              ps = Psi_loc / xx;
+              rm = fmaf(C, srem, fmaf((float)A, ssup, Inuup * ex));
+              es = (float)(1.0 - pl);
+            } else {
+              ps = 0.0f;
+              rm = Inu;
+              es = 1.0f;
+            }
+            psi[p] = ps;
+            if (s->split_rates) {
+              irem[p] = rm;
+              esc[p] = es;
+            }
+          }
+        }
+      }
+  }
+#undef HW
+#undef HP
+#undef HC
+  free(xt);
+  free(yt);
+  return 0;
+}

@@ -57,6 +57,10 @@ int or_long_char_hermite(const or_slab_t *s, float *work, float *psi, const floa
                          double code_length);
 int or_long_char_hermite2(const or_slab_t *s, float *work, float *psi, const float *pe, const float *dpe_dz,
                           const float *g_pe, const float *g_dpe_dz, int ghost, double code_length);
+int or_short_char_hermite(const or_slab_t *s, float *work, float *psi, float *irem, float *esc,
+                          const float *beta, const float *pe, const float *dpe_dx, const float *dpe_dy,
+                          const float *dpe_dz, const float *dlnt_dx, const float *dlnt_dy, const float *dlnt_dz,
+                          const float *temp, const float *hknu, double code_length);
 void or_linear_weights_f64(int n, const double *t, double *E, double *W, double *Psi, double *Esc);
 void or_parab_moments_f32(int n, const float *t, float *E, float *U0, float *U1, float *q);
 void or_parab_moments_f64(int n, const double *t, double *E, double *U0, double *U1, double *q);

@@ -319,6 +319,19 @@ def long_char_hermite2(slab: Slab, work, psi, pe, dpe_dz, ghost=None, ghost_kind
         raise RuntimeError(f"oracle long_char_hermite2 rc={rc}")
 
 
+def short_char_hermite(slab: Slab, work, psi, irem, esc, beta, pe, dpe_dx, dpe_dy, dpe_dz, dlnt_dx, dlnt_dy,
+                       dlnt_dz, temp, hknu, code_length=1.0):
+    """short_char_hermite (rt_solvers_mod.f90:1917-2248) in place on work (fp32);
+    psi, irem, esc (nz, ny, nx, nf) or None as get_psi / split_rates ask."""
+    f32 = lambda a: np.ascontiguousarray(a, np.float32)
+    args = [f32(a) for a in (beta, pe, dpe_dx, dpe_dy, dpe_dz, dlnt_dx, dlnt_dy, dlnt_dz, temp, hknu)]
+    assert work.dtype == np.float32 and work.flags.c_contiguous
+    rc = lib().or_short_char_hermite(C.byref(slab), _p(work), _p(psi), _p(irem), _p(esc), *[_p(a) for a in args],
+                                     C.c_double(code_length))
+    if rc:
+        raise RuntimeError(f"oracle short_char_hermite rc={rc}")
+
+
 def rotate_array(slab: Slab, work, ds_code, bot2pivot, ray_offset=(0.0, 0.0)):
     fp64 = work.dtype == np.float64
     fn = lib().or_rotate_array_f64 if fp64 else lib().or_rotate_array_f32

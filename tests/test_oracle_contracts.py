@@ -428,3 +428,61 @@ def test_hermite2_agrees_with_hermite_on_smooth_slab(oracle):
     assert np.isfinite(w_2).all()
     assert rel_l.max() < 1e-2
     assert rel_h.max() < 1e-2
+
+
+def test_short_char_hermite_uniform_medium(oracle):
+    """short_char_hermite in a uniform medium (constant chi, Pe, T, Snu = Bnu) along
+    an oblique ray: the kernels reproduce the constants, the product-rule slopes
+    vanish, and every plane holds I = S + (I_up - S) e^-dtau with
+    dtau = chi ds/|mu_z|, through the first plane's linear step and the chain-rule
+    steps after it, in both directions, with and without the split rates."""
+    nf, nx, ny, nz = 3, 5, 4, 6
+    ds = 1e6
+    for d in (1, -1):
+        for split in (False, True):
+            vec = np.array([0.25, -0.15, 0.0])
+            vec[2] = d * np.sqrt(1 - vec[0] ** 2 - vec[1] ** 2)
+            s = oracle.make_slab(nf, nx, ny, nz, d, [ds] * 3, vec, get_psi=True, split_rates=split)
+            work = np.zeros((3, nz + 2, ny, nx, nf), np.float32)
+            work[0] = 2e-7
+            work[1] = 3.0
+            work[2, 0 if d > 0 else nz + 1] = 1.0
+            beta = np.full((nz, ny, nx, nf), 0.75, np.float32)
+            pe = np.full((nz, ny, nx), 10.0, np.float32)
+            z0 = np.zeros_like(pe)
+            T = np.full_like(pe, 6000.0)
+            hk = np.full(nf, 1e-4, np.float32)
+            psi, irem, esc = (np.zeros((nz, ny, nx, nf), np.float32) for _ in range(3))
+            oracle.short_char_hermite(s, work, psi, irem, esc, beta, pe, z0, z0, z0, z0, z0, z0, T, hk)
+            E = math.exp(-2e-7 * ds / abs(vec[2]))
+            I = 1.0
+            for k in range(nz):
+                I = 3.0 + (I - 3.0) * E
+                z = 1 + k if d > 0 else nz - k
+                np.testing.assert_allclose(work[2, z], I, rtol=3e-6)
+            assert psi.min() > 0
+            if split:
+                np.testing.assert_allclose(esc, 1 - psi * 2e-7, rtol=1e-5)
+
+
+def test_short_char_hermite_agrees_with_linear_short_char(oracle):
+    """On a smooth stratified slab with horizontal waves the chain-rule Hermite
+    short characteristics agree with the linear ones to the linear solver's
+    truncation error along an oblique ray."""
+    import sys
+    import os
+    sys.path.insert(0, os.path.dirname(__file__))
+    from hermite_cases import slab_case3d, HERM3D_KEYS
+    work, fld, ds = slab_case3d(seed=2, nz=24, ds=5e5)
+    nz, ny, nx, nf = work.shape[1] - 2, work.shape[2], work.shape[3], work.shape[4]
+    vec = np.array([0.2, 0.1, 0.0])
+    vec[2] = np.sqrt(1 - 0.05)
+    w_h = work.copy()
+    w_h[2, 0] = w_h[1, 0]
+    w_l = w_h.copy()
+    s = oracle.make_slab(nf, nx, ny, nz, 1, [ds] * 3, vec)
+    oracle.short_char_hermite(s, w_h, None, None, None, *[fld[k] for k in HERM3D_KEYS])
+    oracle.formal_solve(oracle.SHORT_LINEAR, s, w_l)
+    rel = np.abs(w_h[2, 1:-1] - w_l[2, 1:-1]) / w_l[2, 1:-1]
+    assert np.isfinite(w_h).all()
+    assert rel.max() < 1e-2
