@@ -592,3 +592,86 @@ def atom_window(atom: dict, nper: int = 25, seed: int = 2, qmax_doppler: float =
             "cwnu": np.concatenate(cwnu) if cwnu else np.zeros(0),
             "cont_active": None, "g": np.asarray(g, np.float64), "ev": np.asarray(ev, np.float64), "cut_x": 70.0,
             "twohnu3_c2": (2.0 * HH * nu**3 / CC**2).astype(np.float32)}
+
+
+def pca_grid(temp, ne, ldtemp=0.05, ldne=0.25, npad=2):
+    """An orthogonal PC basis of (ln T, ln ne) over the given cells and a regular
+    node grid along its axes (the pca_transform_type of optab_mod.f90:26-31):
+    mu the mean, rot the unit eigenvectors as columns (largest variance first,
+    first component of each made positive), c0 the first node and dc the spacing
+    (the requested ln T / ln ne steps projected onto each axis), npad nodes past
+    the data at either end.  Returns (pca dict, n1, n2)."""
+    x = np.stack([np.log(np.asarray(temp, np.float64).ravel()), np.log(np.asarray(ne, np.float64).ravel())])
+    mu = x.mean(axis=1)
+    w, v = np.linalg.eigh(np.cov(x))
+    rot = v[:, ::-1].copy()
+    rot *= np.sign(rot[0])[None, :]
+    p = rot.T @ (x - mu[:, None])
+    step = np.array([ldtemp, ldne])
+    dc = np.array([1.0 / np.sqrt(np.sum((rot[:, k] / step) ** 2)) for k in range(2)])
+    c0 = p.min(axis=1) - npad * dc
+    n = np.floor((p.max(axis=1) - c0) / dc).astype(int) + 1 + npad
+    return {"mu": mu, "rot": rot, "c0": c0, "dc": dc}, int(n[0]), int(n[1])
+
+
+def table_nodes(pca, n1, n2):
+    """(T, ne) at the PC grid nodes, (n2, n1) each (pca_opac_grid, optab_mod.f90:515-523)."""
+    i = np.arange(n1)[None, :]
+    j = np.arange(n2)[:, None]
+    p1 = pca["c0"][0] + i * pca["dc"][0]
+    p2 = pca["c0"][1] + j * pca["dc"][1]
+    r = np.asarray(pca["rot"])
+    lnT = pca["mu"][0] + r[0, 0] * p1 + r[0, 1] * p2
+    lnN = pca["mu"][1] + r[1, 0] * p1 + r[1, 1] * p2
+    return np.exp(lnT), np.exp(lnN)
+
+
+def sample_table(seed, temp, ne, nnu=800, lam=(4000.0, 9000.0), kind="background", scat=True, ldtemp=0.05,
+                 ldne=0.25, npad=2, nline=40):
+    """A synthetic sampled opacity table over the (T, ne) of the given cells: an
+    irregular ascending wavelength grid, the PC node grid of pca_grid, and a
+    positive opacity per unit chi500 on it.  kind "background": a smooth H- like
+    continuum with edges plus, as the scattering component, a Rayleigh-like
+    lambda^-4 term; kind "linelist": nline Lorentzian lines whose strengths follow
+    Boltzmann factors of the node temperatures, with (1-eps) = 0.3 of each as the
+    scattering component.  Returns a dict: lam (nnu,), val and scat (nne, ntemp,
+    nnu) or scat None, pca."""
+    rng = np.random.default_rng(seed)
+    pca, n1, n2 = pca_grid(temp, ne, ldtemp, ldne, npad)
+    u = np.sort(rng.random(nnu - 2))
+    lam_n = np.concatenate([[lam[0]], lam[0] * (lam[1] / lam[0]) ** u, [lam[1]]])
+    lam_n = np.unique(lam_n)
+    while lam_n.size < nnu:
+        lam_n = np.unique(np.concatenate([lam_n, [lam_n[0] + (lam_n[1] - lam_n[0]) * 0.5]]))
+    Tn, Nn = table_nodes(pca, n1, n2)
+    th = 5040.0 / Tn[:, :, None]
+    L = lam_n[None, None, :] / 5000.0
+    if kind == "background":
+        cont = (Nn[:, :, None] / 1e14) ** 0.8 * np.exp(-0.75 * th) * L ** 1.5
+        edges = sum(a * (L > e) * L ** 3 for a, e in ((0.6, 0.82), (0.3, 1.3), (0.2, 1.65)))
+        val = cont * (1.0 + edges) * (1.0 + 0.05 * np.sin(7.0 * L))
+        sc = 0.02 * L ** -4 * (1.0 + 0.5 * th) * np.ones_like(val)
+    else:
+        val = np.zeros((n2, n1, lam_n.size))
+        l0 = rng.uniform(lam[0], lam[1], nline)
+        w = rng.uniform(0.05, 0.3, nline)
+        chi_ex = rng.uniform(0.0, 4.0, nline)
+        s0 = 10.0 ** rng.uniform(-1.0, 2.0, nline)
+        for k in range(nline):
+            prof = w[k] ** 2 / ((lam_n - l0[k]) ** 2 + w[k] ** 2)
+            val += s0[k] * 10.0 ** (-chi_ex[k] * th) * prof[None, None, :]
+        sc = 0.3 * val
+    out = {"lam": lam_n, "val": val.astype(np.float32), "pca": pca}
+    out["scat"] = sc.astype(np.float32) if scat else None
+    return out
+
+
+def optab_cells(seed, nx, ny, nz):
+    """Cell temperatures, electron densities, chi500 and projected velocities
+    (v/c) of a seeded cube, flat (nz*ny*nx,), with ne tied to T as well as to the
+    density so that (ln T, ln ne) spread about their principal axis."""
+    atm = cube_atmosphere(seed, nx, ny, nz)
+    T = atm["temp"].astype(np.float64)
+    ne = atm["ne"] * np.exp((T - 6000.0) / 1500.0)
+    return {"temp": T.ravel(), "ne": ne.ravel(), "chi500": atm["chi_c"].ravel().astype(np.float32),
+            "vproj": atm["vz"].ravel().astype(np.float32)}

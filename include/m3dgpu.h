@@ -233,6 +233,40 @@ typedef struct {
 int m3d_short_char_hermite(const m3d_slab_t *slab, float *work, float *psi, float *irem, float *escape,
                            const m3d_hermite3d_t *h, unsigned flags);
 
+/* ---- sampled opacity tables (HOP/optab_mod.f90:37-166, :181-409): an opacity
+ * per unit chi500 on (wavelength, PC axis 1, PC axis 2) of (ln T, ln ne), held
+ * resident on the device with its monotone node slopes and sampled per
+ * (frequency, cell) by a separable cubic Hermite.  rot is pca_transform_type's
+ * rot(2,2) in Fortran order: rot(1,1), rot(2,1), rot(1,2), rot(2,2). */
+typedef struct {
+  double mu[2];     /* mean of (ln T, ln ne) */
+  double rot[4];    /* PC directions, columns */
+  double c0[2];     /* first node coordinate along each PC axis */
+  double dc[2];     /* node spacing along each PC axis */
+} m3d_pca_t;
+typedef struct m3d_optab m3d_optab_t;
+/* sample_optab_type with sample_build_derivatives: val, scat (nnu, ntemp, nne),
+ * wavelength fastest, over the ascending nodes lam (nnu) [A]; scat may be NULL
+ * (a line-list table without line scattering).  Needs nnu, ntemp, nne >= 2. */
+int m3d_optab_create(int nnu, int ntemp, int nne, const double *lam, const float *val, const float *scat,
+                     const m3d_pca_t *pca, unsigned flags, m3d_optab_t **out);
+/* the node slopes along wavelength, PC axis 1 and PC axis 2 (dl, dt, de; or sl,
+ * st, se for component 1), (nnu, ntemp, nne) each */
+int m3d_optab_slopes(const m3d_optab_t *t, int component, float *dl, float *dt, float *de, unsigned flags);
+/* sample_interpolate: per cell temp, ne (fp64) and chi500; the frequencies' vacuum
+ * wavelengths lam_q (nf); back = total extinction, scat = its scattering part,
+ * (nf, ncell) frequency fastest, set.  The table needs its scattering component. */
+int m3d_optab_sample(const m3d_optab_t *t, long long ncell, const double *temp, const double *ne, const float *chi500,
+                     int nf, const double *lam_q, float *back, float *scat, unsigned flags);
+/* sample_interpolate_ll: the query wavelength of a cell is lam_q (1 + vproj);
+ * xhat and ehat (nf, ncell) += kappa chi500 (pass the two work slots); chi_scat
+ * (nf, ncell) += the scattering component's kappa chi500 when it and the table's
+ * scattering component are both given. */
+int m3d_optab_sample_ll(const m3d_optab_t *t, long long ncell, const double *temp, const double *ne,
+                        const float *chi500, const float *vproj, int nf, const double *lam_q, float *xhat,
+                        float *ehat, float *chi_scat, unsigned flags);
+int m3d_optab_destroy(m3d_optab_t *t);
+
 /* rotate_array (rt_patch_mod.f90:3809-3866) on work(:,:,:,1:nz,1:2), in place. */
 int m3d_rotate_array(const m3d_slab_t *slab, void *work, const double *ds_code, double bot2pivot,
                      const double *ray_offset, unsigned flags);
