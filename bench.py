@@ -43,6 +43,7 @@ def _args():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-fp64", action="store_true")
     p.add_argument("--no-ali", action="store_true", help="skip the NLTE measurements (3D window, batched columns)")
+    p.add_argument("--no-optab", action="store_true", help="skip the sampled opacity table measurement")
     p.add_argument("--cube", type=int, default=240, help="cube edge (240 = the configuration; smaller for profiling)")
     return p.parse_args()
 
@@ -321,6 +322,78 @@ def _nlte_batched(steps=2):
     return out
 
 
+def _optab(steps=5, warmup=3):
+    """The sampled opacity tables (HOP/optab_mod.f90), measured beside the headline:
+    2.1 M cells of a seeded 128^3 cube and one window of 256 frequencies at R = 1e5,
+    the tables built as the reference builds them for a window: the background
+    table on the window's own wavelengths (every query on a node), the line-list
+    table on them padded for the largest Doppler shift.  sample_interpolate sets
+    back and scat; sample_interpolate_ll with the cube's projected velocities adds
+    into xhat, ehat and chi_scat.  Device-resident inputs, outputs larger than L2;
+    CUDA events on torch's stream.  Algorithmic bytes per (frequency, cell): 8
+    written by sample_interpolate, 24 read and written by sample_interpolate_ll;
+    per cell 20 and 24 read.  The tables (a few tens of MB) stay in L2."""
+    import torch
+
+    import dispatch_b200 as m
+    from dispatch_b200 import synth
+    from dispatch_b200.optab import SampleOptab
+    c = synth.optab_cells(7, 128, 128, 128)
+    ncell, nf = c["temp"].size, 256
+    lam_q, bg, ll = synth.window_tables(8, c["temp"], c["ne"], c["vproj"], nf=nf)
+    dev = lambda x: torch.from_numpy(np.ascontiguousarray(x)).cuda()
+    T, N, X, V = dev(c["temp"]), dev(c["ne"]), dev(c["chi500"]), dev(c["vproj"])
+    q = dev(lam_q)
+    tb, tl = SampleOptab.from_dict(bg), SampleOptab.from_dict(ll)
+    back = torch.empty((ncell, nf), dtype=torch.float32, device="cuda")
+    scat = torch.empty_like(back)
+    xh, eh, cs = torch.zeros_like(back), torch.zeros_like(back), torch.zeros_like(back)
+    cur = torch.cuda.current_stream()
+
+    def timed(fn):
+        for _ in range(warmup):
+            fn()
+        ts = []
+        for _ in range(steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(cur)
+            fn()
+            e1.record(cur)
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return float(np.median(ts))
+
+    n0 = m.launch_count()
+    t_s = timed(lambda: tb.interpolate(T, N, X, q, back, scat))
+    t_l = timed(lambda: tl.interpolate_ll(T, N, X, xh, eh, q, V, cs))
+    launches = (m.launch_count() - n0) // (2 * (steps + warmup))
+    peaks = _peaks() or {}
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    pts = ncell * nf
+    out = {"workload": "sampled opacity tables: 2.1 M cells (seeded 128^3 cube), one window of 256 frequencies at "
+                       "R = 1e5; background table %d x %d x %d nodes on the window's wavelengths (value + "
+                       "scattering), line-list table %d x %d x %d padded for the Doppler shifts"
+                       % (tb.nnu, tb.ntemp, tb.nne, tl.nnu, tl.ntemp, tl.nne),
+           "unit": "Gpt*nu/s", "launches_per_call": launches, "data": "synthetic (seeded cube, seeded tables)"}
+    for name, t, per_pt, per_cell in (("sample_interpolate", t_s, 8, 20), ("sample_interpolate_ll", t_l, 24, 24)):
+        gbs = (per_pt * pts + per_cell * ncell) / (t / 1e3) / 1e9
+        out[name] = {"ms": t, "value": pts / (t / 1e3) / 1e9, "achieved_gbs": gbs, "peak_gbs": hbm,
+                     "frac": gbs / hbm, "peak_kind": "measured" if peaks else "fallback"}
+    # the oracle on a bounded sample of the same cells, one host thread
+    from oracle import optab as oopt
+    k = 4096
+    t0 = time.perf_counter()
+    oopt.sample(bg, c["temp"][:k], c["ne"][:k], c["chi500"][:k], lam_q)
+    out["cpu_baseline"] = {"value": k * nf / (time.perf_counter() - t0) / 1e9, "unit": "Gpt*nu/s", "cores": 1,
+                           "kind": "port", "sample": f"{k} cells x {nf} frequencies, including the node slopes"}
+    tb.close()
+    tl.close()
+    del back, scat, xh, eh, cs
+    torch.cuda.empty_cache()
+    return out
+
+
 def run_b200(a):
     import torch
     import torch.distributed as dist
@@ -457,10 +530,12 @@ def run_b200(a):
                 "solve_fp32_over_fp64": sv64_ms / sv_ms if sv_ms else None,
                 "path": "same kernels in FP64 for units, rotation and solver, one launch per ray and slab"}
 
-    nlte = batched = None
+    nlte = batched = optab = None
     if rank == 0 and not a.no_ali:
         nlte = _nlte_ali()
         batched = _nlte_batched()
+    if rank == 0 and not a.no_optab:
+        optab = _optab()
 
     cpu = None
     if rank == 0 and not a.no_cpu_baseline:
@@ -476,7 +551,7 @@ def run_b200(a):
             "dtype": "f32", "data": "synthetic (seeded grey cube, random line list)", "config": _workload(nf, a.cube),
             "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline, "cpu_baseline": cpu,
             "clocks": clocks, "stages": stages, "fp64_plain": fp64, "nlte_ali": nlte,
-            "nlte_batched": batched}
+            "nlte_batched": batched, "optab": optab}
     print(json.dumps(line), flush=True)
 
 

@@ -22,11 +22,25 @@ struct OptabDev {
 };
 
 // per-frequency bracket on the wavelength nodes: cnt = number of nodes below the
-// query, k the 0-based interval, and hermite_coefs of the position in it
+// query, k the 0-based interval, and hermite_coefs of the position in it; node is
+// the wavelength node the query sits on (the interval's end with weights 0 and 1
+// and vanishing slope weights) or -1
 struct OptabFreq {
   int k, cnt;
-  float pl, wc0, wc1, wcm0, wcm1, pad;
+  float pl, wc0, wc1, wcm0, wcm1;
+  int node;
 };
+
+// A query on a node: the weights are (c0, c1) = (1, 0) or (0, 1) and cm0 = cm1 = 0,
+// so each term the collapse forms from the other node is a product with an exact
+// zero and it returns the node's own value and PC slopes.  The node's float4 alone
+// then gives the same result for finite tables (a -0 can come out as +0).
+__device__ __forceinline__ int optab_on_node(const float c[5], int k) {
+  if (c[3] != 0.0f || c[4] != 0.0f) return -1;
+  if (c[1] == 1.0f && c[2] == 0.0f) return k;
+  if (c[1] == 0.0f && c[2] == 1.0f) return k + 1;
+  return -1;
+}
 
 // hermite_coefs (interpol_mod.f90:171-188): p, c0, c1, cm0, cm1
 __host__ __device__ __forceinline__ void optab_hcoefs(float t, float h, float c[5]) {
@@ -68,7 +82,7 @@ __global__ void k_optab_freq(int nf, const double *lam_q, int nnu, const double 
   o.wc1 = c[2];
   o.wcm0 = c[3];
   o.wcm1 = c[4];
-  o.pad = 0.0f;
+  o.node = optab_on_node(c, o.k);
   fc[f] = o;
 }
 
@@ -111,7 +125,28 @@ __device__ __forceinline__ float optab_collapse(const float4 *t, size_t base, si
   return fmaf(nc[4], ge1, fmaf(nc[3], ge0, fmaf(nc[2], f1, nc[1] * f0)));
 }
 
+// the collapse of a query on node n: the node's value and PC slopes at the four
+// (temp, ne) corners, then temp, then ne, as optab_collapse forms them
+__device__ __forceinline__ float optab_collapse_node(const float4 *t, size_t base, size_t sit, size_t sje,
+                                                     const float tc[5], const float nc[5]) {
+  float v[4], gt[4], ge[4];
+#pragma unroll
+  for (int c = 0; c < 4; c++) {
+    const float4 A = __ldg(t + base + (c & 1) * sit + (c >> 1) * sje);
+    v[c] = A.x;
+    gt[c] = A.z;
+    ge[c] = A.w;
+  }
+  const float pt = tc[0], opt = 1.0f - pt;
+  const float f0 = fmaf(tc[4], gt[1], fmaf(tc[3], gt[0], fmaf(tc[2], v[1], tc[1] * v[0])));
+  const float f1 = fmaf(tc[4], gt[3], fmaf(tc[3], gt[2], fmaf(tc[2], v[3], tc[1] * v[2])));
+  const float ge0 = fmaf(pt, ge[1], opt * ge[0]);
+  const float ge1 = fmaf(pt, ge[3], opt * ge[2]);
+  return fmaf(nc[4], ge1, fmaf(nc[3], ge0, fmaf(nc[2], f1, nc[1] * f0)));
+}
+
 constexpr int kOptabWarps = 8;
+constexpr int kOptabUnroll = 2;   // frequencies per lane per pass of sample_interpolate_ll
 
 // sample_interpolate (optab_mod.f90:181-287): one warp per cell, lanes over the
 // frequencies; back = (kappa + kappa_scat) chi500, scat = kappa_scat chi500
@@ -131,9 +166,15 @@ __global__ void __launch_bounds__(32 * kOptabWarps) k_optab_sample(OptabDev T, i
     const size_t cb = (size_t)it * sit + (size_t)je * sje;
     for (int f = lane; f < nf; f += 32) {
       const OptabFreq q = fc[f];
-      const float w[5] = {q.pl, q.wc0, q.wc1, q.wcm0, q.wcm1};
-      const float kap = optab_collapse(T.tv, cb + q.k, sit, sje, w, tc, nc);
-      const float kas = optab_collapse(T.ts, cb + q.k, sit, sje, w, tc, nc);
+      float kap, kas;
+      if (q.node >= 0) {
+        kap = optab_collapse_node(T.tv, cb + q.node, sit, sje, tc, nc);
+        kas = optab_collapse_node(T.ts, cb + q.node, sit, sje, tc, nc);
+      } else {
+        const float w[5] = {q.pl, q.wc0, q.wc1, q.wcm0, q.wcm1};
+        kap = optab_collapse(T.tv, cb + q.k, sit, sje, w, tc, nc);
+        kas = optab_collapse(T.ts, cb + q.k, sit, sje, w, tc, nc);
+      }
       const size_t o = (size_t)c * nf + f;
       back[o] = (kap + kas) * ch;
       scat[o] = kas * ch;
@@ -143,7 +184,10 @@ __global__ void __launch_bounds__(32 * kOptabWarps) k_optab_sample(OptabDev T, i
 
 // sample_interpolate_ll (optab_mod.f90:300-409): the query wavelength of each
 // cell is lam_q (1 + vproj), bracketed by walking from the unshifted count;
-// xhat, ehat += kappa chi500, and chi_scat += kappa_scat chi500 when given
+// xhat, ehat += kappa chi500, and chi_scat += kappa_scat chi500 when given.
+// A lane takes kOptabUnroll frequencies per pass: their work slots are read and
+// their brackets found before the table lookups, so the slow reads of the slots
+// and of the wavelength nodes are in flight together.
 __global__ void __launch_bounds__(32 * kOptabWarps) k_optab_sample_ll(OptabDev T, int nf, long long ncell,
                                                                       const double *temp, const double *ne,
                                                                       const float *chi500, const float *vproj,
@@ -162,18 +206,49 @@ __global__ void __launch_bounds__(32 * kOptabWarps) k_optab_sample_ll(OptabDev T
     const float ch = chi500[c];
     const double vf = 1.0 + (double)vproj[c];
     const size_t cb = (size_t)it * sit + (size_t)je * sje;
-    for (int f = lane; f < nf; f += 32) {
-      const double x = __dmul_rn(lam_q[f], vf);
-      int cnt = fc[f].cnt;
-      while (cnt < nnu && lam[cnt] < x) cnt++;
-      while (cnt > 0 && lam[cnt - 1] >= x) cnt--;
-      float w[5];
-      const int k = optab_interval(nnu, lam, cnt, x, w);
-      const size_t o = (size_t)c * nf + f;
-      const float add = optab_collapse(T.tv, cb + k, sit, sje, w, tc, nc) * ch;
-      xhat[o] = xhat[o] + add;
-      ehat[o] = ehat[o] + add;
-      if (chi_scat) chi_scat[o] = chi_scat[o] + optab_collapse(T.ts, cb + k, sit, sje, w, tc, nc) * ch;
+    for (int f0 = lane; f0 < nf; f0 += 32 * kOptabUnroll) {
+      float xv[kOptabUnroll], ev[kOptabUnroll], sv[kOptabUnroll];
+      int k[kOptabUnroll], nd[kOptabUnroll];
+      float w[kOptabUnroll][5];
+#pragma unroll
+      for (int u = 0; u < kOptabUnroll; u++) {
+        const int f = f0 + 32 * u;
+        if (f >= nf) break;
+        const size_t o = (size_t)c * nf + f;
+        xv[u] = xhat[o];
+        ev[u] = ehat[o];
+        if (chi_scat) sv[u] = chi_scat[o];
+        const double x = __dmul_rn(lam_q[f], vf);
+        int cnt = fc[f].cnt;
+        while (cnt < nnu && lam[cnt] < x) cnt++;
+        while (cnt > 0 && lam[cnt - 1] >= x) cnt--;
+        k[u] = optab_interval(nnu, lam, cnt, x, w[u]);
+        nd[u] = optab_on_node(w[u], k[u]);
+      }
+#pragma unroll
+      for (int u = 0; u < kOptabUnroll; u++) {
+        const int f = f0 + 32 * u;
+        if (f >= nf) break;
+        const float kap = nd[u] >= 0 ? optab_collapse_node(T.tv, cb + nd[u], sit, sje, tc, nc)
+                                     : optab_collapse(T.tv, cb + k[u], sit, sje, w[u], tc, nc);
+        const float add = kap * ch;
+        xv[u] = xv[u] + add;
+        ev[u] = ev[u] + add;
+        if (chi_scat) {
+          const float kas = nd[u] >= 0 ? optab_collapse_node(T.ts, cb + nd[u], sit, sje, tc, nc)
+                                       : optab_collapse(T.ts, cb + k[u], sit, sje, w[u], tc, nc);
+          sv[u] = sv[u] + kas * ch;
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < kOptabUnroll; u++) {
+        const int f = f0 + 32 * u;
+        if (f >= nf) break;
+        const size_t o = (size_t)c * nf + f;
+        xhat[o] = xv[u];
+        ehat[o] = ev[u];
+        if (chi_scat) chi_scat[o] = sv[u];
+      }
     }
   }
 }

@@ -627,22 +627,28 @@ def table_nodes(pca, n1, n2):
 
 
 def sample_table(seed, temp, ne, nnu=800, lam=(4000.0, 9000.0), kind="background", scat=True, ldtemp=0.05,
-                 ldne=0.25, npad=2, nline=40):
+                 ldne=0.25, npad=2, nline=40, lam_nodes=None):
     """A synthetic sampled opacity table over the (T, ne) of the given cells: an
     irregular ascending wavelength grid, the PC node grid of pca_grid, and a
     positive opacity per unit chi500 on it.  kind "background": a smooth H- like
     continuum with edges plus, as the scattering component, a Rayleigh-like
     lambda^-4 term; kind "linelist": nline Lorentzian lines whose strengths follow
     Boltzmann factors of the node temperatures, with (1-eps) = 0.3 of each as the
-    scattering component.  Returns a dict: lam (nnu,), val and scat (nne, ntemp,
-    nnu) or scat None, pca."""
+    scattering component.  lam_nodes, when given, are the wavelength nodes (the
+    reference tabulates on the window's own frequencies, rt_patch_mod.f90:2359,
+    padded for Doppler shifts on the line-list path, :2440-2466).  Returns a
+    dict: lam (nnu,), val and scat (nne, ntemp, nnu) or scat None, pca."""
     rng = np.random.default_rng(seed)
     pca, n1, n2 = pca_grid(temp, ne, ldtemp, ldne, npad)
-    u = np.sort(rng.random(nnu - 2))
-    lam_n = np.concatenate([[lam[0]], lam[0] * (lam[1] / lam[0]) ** u, [lam[1]]])
-    lam_n = np.unique(lam_n)
-    while lam_n.size < nnu:
-        lam_n = np.unique(np.concatenate([lam_n, [lam_n[0] + (lam_n[1] - lam_n[0]) * 0.5]]))
+    if lam_nodes is not None:
+        lam_n = np.asarray(lam_nodes, np.float64)
+        lam = (float(lam_n[0]), float(lam_n[-1]))
+    else:
+        u = np.sort(rng.random(nnu - 2))
+        lam_n = np.concatenate([[lam[0]], lam[0] * (lam[1] / lam[0]) ** u, [lam[1]]])
+        lam_n = np.unique(lam_n)
+        while lam_n.size < nnu:
+            lam_n = np.unique(np.concatenate([lam_n, [lam_n[0] + (lam_n[1] - lam_n[0]) * 0.5]]))
     Tn, Nn = table_nodes(pca, n1, n2)
     th = 5040.0 / Tn[:, :, None]
     L = lam_n[None, None, :] / 5000.0
@@ -675,3 +681,20 @@ def optab_cells(seed, nx, ny, nz):
     ne = atm["ne"] * np.exp((T - 6000.0) / 1500.0)
     return {"temp": T.ravel(), "ne": ne.ravel(), "chi500": atm["chi_c"].ravel().astype(np.float32),
             "vproj": atm["vz"].ravel().astype(np.float32)}
+
+
+def window_tables(seed, temp, ne, vproj, nf=256, lam0=5040.0, R=1e5, pad_guard=2, nline=30):
+    """The two tables of one frequency window as the reference builds them: the
+    window's nf wavelengths uniform in ln lambda at resolution R (lam_q); the
+    background table on exactly those nodes (rt_patch_mod.f90:2359); the line-list
+    table on them extended by ceil(vmax / dlnlam) + pad_guard nodes at either end
+    (:2440-2466), vmax the largest |vproj|.  Returns (lam_q, background, linelist)."""
+    dl = 1.0 / R
+    lam_q = lam0 * np.exp(dl * np.arange(nf))
+    vmax = float(np.max(np.abs(vproj))) if np.size(vproj) else 0.0
+    npad = int(np.ceil(vmax / dl)) + pad_guard
+    plam = lam0 * np.exp(dl * np.arange(-npad, nf + npad))
+    plam[npad:npad + nf] = lam_q
+    bg = sample_table(seed, temp, ne, kind="background", lam_nodes=lam_q)
+    ll = sample_table(seed + 1, temp, ne, kind="linelist", lam_nodes=plam, nline=nline)
+    return lam_q, bg, ll

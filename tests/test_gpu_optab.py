@@ -104,3 +104,35 @@ def test_device_tensors_and_checks(m3d, oracle):
     with pytest.raises(m3d.M3DError, match="scattering component"):
         T2.interpolate(c["temp"], c["ne"], c["chi500"], q)
     T2.close()
+
+
+def test_window_tables_bit_exact(m3d, oracle):
+    """The tables as the reference builds them for a window: every background
+    query on a node (the device's one-node collapse against the oracle's full
+    one), the line-list queries shifted between the padded nodes."""
+    from dispatch_b200 import synth
+    from dispatch_b200.optab import SampleOptab
+    from oracle import optab
+    c = oc.cells(seed=5)
+    q, bg, ll = synth.window_tables(3, c["temp"], c["ne"], c["vproj"], nf=96)
+    T = SampleOptab.from_dict(bg)
+    b_g, s_g = T.interpolate(c["temp"], c["ne"], c["chi500"], q)
+    b_o, s_o = optab.sample(bg, c["temp"], c["ne"], c["chi500"], q)
+    np.testing.assert_array_equal(b_g, b_o)
+    np.testing.assert_array_equal(s_g, s_o)
+    T.close()
+    T = SampleOptab.from_dict(ll)
+    n = c["temp"].size
+    vp = c["vproj"].copy()
+    vp[::7] = 0.0                                     # cells at rest query the nodes themselves
+    out = {}
+    for name in ("g", "o"):
+        x, e, s = (np.zeros((n, q.size), np.float32) for _ in range(3))
+        if name == "g":
+            T.interpolate_ll(c["temp"], c["ne"], c["chi500"], x, e, q, vp, s)
+        else:
+            optab.sample_ll(ll, c["temp"], c["ne"], c["chi500"], vp, q, x, e, s)
+        out[name] = (x, e, s)
+    for a, b in zip(out["g"], out["o"]):
+        np.testing.assert_array_equal(a, b)
+    T.close()
