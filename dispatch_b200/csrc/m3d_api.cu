@@ -22,6 +22,7 @@
 #include "m3d_aux.cuh"
 #include "m3d_columns.cuh"
 #include "m3d_optab.cuh"
+#include "m3d_hprof.cuh"
 
 using namespace m3d;
 
@@ -1338,6 +1339,7 @@ int m3d_lte_synthesis(const m3d_atmos_t *atm, int nf, const double *nu, const do
 #include "m3d_aux_api.inc"
 #include "m3d_columns_api.inc"
 #include "m3d_optab_api.inc"
+#include "m3d_hprof_api.inc"
 
 // ===========================================================================
 // rotate_array without any allocation.

@@ -267,6 +267,39 @@ int m3d_optab_sample_ll(const m3d_optab_t *t, long long ncell, const double *tem
                         float *ehat, float *chi_scat, unsigned flags);
 int m3d_optab_destroy(m3d_optab_t *t);
 
+/* ---- hydrogen line profiles (HOP/hprofl_mod.f90, after HLINOP), the analytic path:
+ * Griem's Stark profile with the VCS-approximating corrections and the Holtsmark
+ * ion field, QLG-bot Voigt profiles over the fine-structure components, Lyman
+ * alpha's quasi-molecular satellite wings.  hline_t (hprofl_mod.f90:156-165): */
+typedef struct {
+  int n, m, bpo, io;                  /* lower and upper level, BPO self-broadening, components */
+  double nu0, grad, gstk, gw1, gw2, gw3;
+  double dq[14], wt[14];              /* fine-structure offsets [nu/nu0] and weights */
+  double dqbar, dqmax, qray;
+} m3d_hline_t;
+/* the per-cell inputs of add_h_opacities (float, ncell each): projected velocity
+ * [v/c], inverse Doppler width c/v_th, T, lower-level density, ne, neutral H,
+ * mean relative speed squared with H, Holtsmark normal field, (T/1e4)^0.3 n(He) */
+typedef struct {
+  const float *vproj, *inv_df, *temp, *ni, *ne, *tothi, *vbar2h, *fo, *t3nhe;
+} m3d_hcells_t;
+#define M3D_H_NO_RAD 1u    /* disable_rad */
+#define M3D_H_NO_STARK 2u  /* disable_stk */
+#define M3D_H_NO_VDW 4u    /* disable_vdw */
+#define M3D_H_NO_BPO 8u    /* hydrogen_BPO = .false. */
+/* hydrogen_line (hprofl_mod.f90:703-810): the line's widths and fine structure, on the host */
+int m3d_hydrogen_line(int n, int m, double nu0, unsigned opts, m3d_hline_t *h);
+/* hcell_prepare + hprofile per cell at nq detunings q = (nu - nu0)/nu0: phi (ncell, nq), q fastest */
+int m3d_h_profile(const m3d_hline_t *h, long long ncell, const m3d_hcells_t *cells, int nq, const double *q,
+                  float *phi, unsigned flags);
+/* add_h_opacities (hprofl_mod.f90:208-385): from the line-centre index f0 (0-based)
+ * outwards in both directions until the line opacity falls below 1e-7 of cont at f0
+ * in each cell, chi += phi R bi, eta += phi R bj with R = ni Bij (bi = bj = NULL in
+ * LTE); chi, eta, cont (nf, ncell).  line_used and line_strength are raised. */
+int m3d_h_opacity(const m3d_hline_t *h, double Bij, int f0, int nf, const double *nu, long long ncell,
+                  const m3d_hcells_t *cells, const float *bi, const float *bj, float *chi, float *eta,
+                  const float *cont, int *line_used, float *line_strength, unsigned flags);
+
 /* rotate_array (rt_patch_mod.f90:3809-3866) on work(:,:,:,1:nz,1:2), in place. */
 int m3d_rotate_array(const m3d_slab_t *slab, void *work, const double *ds_code, double bot2pivot,
                      const double *ray_offset, unsigned flags);

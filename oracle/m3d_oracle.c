@@ -407,6 +407,24 @@ static inline float bot_eval(const float *tgx, const float *th2x, const qlg_coef
   return fmaf(L, p, G * c->gG);
 }
 
+/* qlg_bot_coef / qlg_bot_eval (qlg_mod.f90:515-528): the split one-point form the
+ * hydrogen profiles use, c[5] = (ih, bL, gG, cZH, cL2) */
+void or_qlg_coef(float a, float c[5])
+{
+  qlg_coef_t k = bot_setup(a, 1.0f, QLG_SQL2, QLG_RPI);
+  c[0] = k.ih;
+  c[1] = k.bL;
+  c[2] = k.gG;
+  c[3] = k.cZH;
+  c[4] = k.cL2;
+}
+
+float or_qlg_eval(const float *tgx, const float *th2x, const float c[5], float v)
+{
+  qlg_coef_t k = {c[0], c[1], c[2], c[3], c[4]};
+  return bot_eval(tgx, th2x, &k, v) * QLG_ISQPI;
+}
+
 /* qlg_bot_sweep (qlg_mod.f90:222-257) = bot_setup(a, 1, SQL2, RPI) + eval */
 void or_qlg_bot_sweep(const float *tgx, const float *th2x, float a, float v0, float dv, int n, float *K)
 {

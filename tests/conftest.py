@@ -20,6 +20,14 @@ def oracle():
 
 
 @pytest.fixture(scope="session")
+def m3d_lib():
+    """The package with its library loaded but no device initialised (host-side entries)."""
+    import dispatch_b200 as m
+    m.lib()
+    return m
+
+
+@pytest.fixture(scope="session")
 def m3d():
     import dispatch_b200 as m
     m.init(0)
