@@ -22,7 +22,8 @@ NO_RAD, NO_STARK, NO_VDW, NO_BPO = 1, 2, 4, 8
 class HLine(C.Structure):
     """m3d_hline_t."""
 
-    _fields_ = [("n", C.c_int), ("m", C.c_int), ("bpo", C.c_int), ("io", C.c_int), ("nu0", C.c_double),
+    _fields_ = [("n", C.c_int), ("m", C.c_int), ("bpo", C.c_int), ("io", C.c_int), ("opts", C.c_int),
+                ("pad", C.c_int), ("nu0", C.c_double),
                 ("grad", C.c_double), ("gstk", C.c_double), ("gw1", C.c_double), ("gw2", C.c_double),
                 ("gw3", C.c_double), ("dq", C.c_double * 14), ("wt", C.c_double * 14), ("dqbar", C.c_double),
                 ("dqmax", C.c_double), ("qray", C.c_double)]
@@ -83,3 +84,18 @@ def add_h_opacities(h: HLine, Bij: float, f0: int, nu, cells: dict, chi, eta, co
                               C.byref(strength), C.c_uint(DEVICE_PTRS if dev else 0)), "m3d_h_opacity")
     del keep
     return bool(used.value), float(strength.value)
+
+
+def vcs_load(series: int, path: str, radiative: bool) -> None:
+    """read_vcs_grid of one series (1 Balmer, 2 Paschen, 3 Brackett)."""
+    init()
+    check(lib().m3d_vcs_load(C.c_int(series), str(path).encode(), C.c_int(int(radiative))), "m3d_vcs_load")
+
+
+def vcs_clear() -> None:
+    init()
+    lib().m3d_vcs_clear()
+
+
+def vcs_supported(n: int, m: int) -> bool:
+    return bool(lib().m3d_vcs_supported(C.c_int(n), C.c_int(m)))

@@ -273,6 +273,7 @@ int m3d_optab_destroy(m3d_optab_t *t);
  * alpha's quasi-molecular satellite wings.  hline_t (hprofl_mod.f90:156-165): */
 typedef struct {
   int n, m, bpo, io;                  /* lower and upper level, BPO self-broadening, components */
+  int opts, pad;                      /* the M3D_H_* switches it was built with */
   double nu0, grad, gstk, gw1, gw2, gw3;
   double dq[14], wt[14];              /* fine-structure offsets [nu/nu0] and weights */
   double dqbar, dqmax, qray;
@@ -287,6 +288,14 @@ typedef struct {
 #define M3D_H_NO_STARK 2u  /* disable_stk */
 #define M3D_H_NO_VDW 4u    /* disable_vdw */
 #define M3D_H_NO_BPO 8u    /* hydrogen_BPO = .false. */
+/* The tabulated profiles of HOP/hvcs_mod.f90 (read_vcs_grid): load one series'
+ * table file (1 Balmer, 2 Paschen, 3 Brackett; radiative = the table includes
+ * radiative damping), as hydrogen_profiles = 'stehle' or 'lemke' selects them.
+ * While a line's series holds its (n, m), its profile is the table's, with the
+ * missing broadening added as a Lorentzian; otherwise the analytic one. */
+int m3d_vcs_load(int series, const char *path, int radiative);
+int m3d_vcs_clear(void);
+int m3d_vcs_supported(int n, int m);   /* 1 when the loaded tables hold the line */
 /* hydrogen_line (hprofl_mod.f90:703-810): the line's widths and fine structure, on the host */
 int m3d_hydrogen_line(int n, int m, double nu0, unsigned opts, m3d_hline_t *h);
 /* hcell_prepare + hprofile per cell at nq detunings q = (nu - nu0)/nu0: phi (ncell, nq), q fastest */

@@ -15,7 +15,8 @@ CELL_FIELDS = ("vproj", "inv_df", "temp", "ni", "ne", "tothi", "vbar2h", "fo", "
 
 
 class HLine(C.Structure):
-    _fields_ = [("n", C.c_int), ("m", C.c_int), ("bpo", C.c_int), ("io", C.c_int), ("nu0", C.c_double),
+    _fields_ = [("n", C.c_int), ("m", C.c_int), ("bpo", C.c_int), ("io", C.c_int), ("opts", C.c_int),
+                ("pad", C.c_int), ("nu0", C.c_double),
                 ("grad", C.c_double), ("gstk", C.c_double), ("gw1", C.c_double), ("gw2", C.c_double),
                 ("gw3", C.c_double), ("dq", C.c_double * 14), ("wt", C.c_double * 14), ("dqbar", C.c_double),
                 ("dqmax", C.c_double), ("qray", C.c_double)]
@@ -65,3 +66,14 @@ def add_h_opacities(h: HLine, Bij, f0, nu, cells: dict, chi, eta, cont, bi=None,
     f(C.byref(h), _p(tgx), _p(th2x), float(Bij), int(f0), nu.size, _p(nu), keep["temp"].size, C.byref(hc),
       _p(bi), _p(bj), _p(chi), _p(eta), _p(cont), C.byref(used), C.byref(strength))
     return bool(used.value), float(strength.value)
+
+
+def vcs_load(series: int, path: str, radiative: bool) -> None:
+    """read_vcs_grid of one series (1 Balmer, 2 Paschen, 3 Brackett)."""
+    rc = lib().or_vcs_load(C.c_int(series), str(path).encode(), C.c_int(int(radiative)))
+    if rc:
+        raise RuntimeError(f"oracle vcs_load({series}, {path}) rc={rc}")
+
+
+def vcs_clear() -> None:
+    lib().or_vcs_clear()

@@ -13,10 +13,12 @@
  */
 #include "or_hprof.h"
 
+#include <float.h>
 #include <math.h>
 #include <stddef.h>
 
 #include "or_htables.inc"
+#include "or_vcs.h"
 
 void or_qlg_coef(float a, float c[5]);
 float or_qlg_eval(const float *tgx, const float *th2x, const float c[5], float v);
@@ -59,6 +61,8 @@ void or_hydrogen_line(int n, int m, double nu0, unsigned opts, or_hline_t *h)
   h->m = m;
   h->nu0 = nu0;
   h->bpo = 0;
+  h->opts = (int)opts;
+  h->pad = 0;
   h->qray = -HUGE_VAL;
   float xknm;
   if (mmn <= 3 && n <= 4) xknm = H_XKNM[(mmn - 1) * 4 + (n - 1)];
@@ -264,6 +268,9 @@ static double lyman_interp(const float *tab, int n, float dx, float x0, double n
 
 typedef struct {
   float idf, ne, tothi, resont, vdw, hwstk, hwlor, hfwid;
+  float hwadd;
+  int use_vcs;
+  or_vcs_cell_t vcs;
   int lymanalf;
   stark_t st;
   float vcore[5], vwing[5], vwing_ray[5];
@@ -283,6 +290,21 @@ static void hcell_prepare(const or_hline_t *h, float temp, float ne, float fo, f
   c->vdw = (float)(h->gw3 * (double)t3nhe);
   c->hwlor = (float)(h->grad + (double)c->resont + (double)c->vdw);
   c->hfwid = fmaxf(fmaxf(1.0f / idf, c->hwlor), c->hwstk);
+  c->hwadd = 0.0f;
+  c->use_vcs = or_vcs_supported(h->n, h->m);
+  if (c->use_vcs) {
+    /* the tabulated profile, with the broadening the table lacks added as one
+     * Lorentzian (hprofl_mod.f90:412-426) */
+    c->hwadd = c->vdw;
+    if (!or_vcs_radiative(h->n)) c->hwadd = c->hwadd + (float)h->grad;
+    if (h->bpo || !or_vcs_resonance(h->n, h->m)) c->hwadd = c->hwadd + c->resont;
+    float nh_table = tothi;
+    if (h->bpo || (h->opts & 4)) nh_table = 0.0f;
+    c->hfwid = fmaxf(1.0f / idf, c->hwadd);
+    or_vcs_prepare(h->n, h->m, h->nu0, temp, ne, nh_table, &c->vcs);
+    c->lymanalf = 0;
+    return;
+  }
   c->lymanalf = h->n == 1 && h->m == 2;
   stark_prepare(h->n, h->m, h->nu0, temp, ne, c->hwstk, &c->st);
   or_qlg_coef((c->hwlor + c->hwstk) * idf, c->vcore);
@@ -359,9 +381,51 @@ static float lyman_voigt(const float *tgx, const float *th2x, const or_hline_t *
   return phi;
 }
 
+/* added_wing (hprofl_mod.f90:560-574) */
+static float added_wing(const hcell_t *c, double d)
+{
+  if (fabs(d) > (double)c->hfwid)
+    return (float)((double)c->hwadd / (H_PI * (d * d + (double)c->hwadd * (double)c->hwadd))) * classical_wing(d);
+  return 0.0f;
+}
+
+/* vcs_fine (hprofl_mod.f90:514-536) */
+static float vcs_fine(const or_hline_t *h, const hcell_t *c, double q)
+{
+  float phi;
+  if (fabs(q) - h->dqmax > c->vcs.q_tail) {
+    phi = (float)or_vcs_tail(&c->vcs, log(fabs(q - h->dqbar)));
+    if (c->hwadd > 0.0f) phi = phi + added_wing(c, q - h->dqbar);
+    return phi;
+  }
+  phi = 0.0f;
+  for (int i = 0; i < h->io; i++) phi = (float)((double)phi + h->wt[i] * (double)(float)or_vcs_eval(&c->vcs, q - h->dq[i]));
+  if (c->hwadd > 0.0f)
+    for (int i = 0; i < h->io; i++) phi = (float)((double)phi + h->wt[i] * (double)added_wing(c, q - h->dq[i]));
+  return phi;
+}
+
 static float hprofile(const float *tgx, const float *th2x, const or_hline_t *h, const hcell_t *c, double q)
 {
+  if (c->use_vcs) return vcs_fine(h, c, q);
   return c->lymanalf ? lyman_voigt(tgx, th2x, h, c, q) : hvoigt(tgx, th2x, h, c, q);
+}
+
+/* profile_at (hprofl_mod.f90:336-350): past qt every component is on the table's
+ * power-law tail, evaluated from ln|d| of the rest-frame detuning and the shift */
+static float profile_at(const float *tgx, const float *th2x, const or_hline_t *h, const hcell_t *c, double qt,
+                        double vp, double nu_f, double q)
+{
+  if (fabs(q) > qt) {
+    double d = (nu_f - h->nu0) / h->nu0 - h->dqbar;
+    d = copysign(fmax(fabs(d), DBL_MIN), d);
+    const double lnd = log(fabs(d)), invd = 1.0 / d;
+    const double r = vp * invd;
+    float phi = (float)or_vcs_tail(&c->vcs, lnd - r * (1.0 + 0.5 * r));
+    if (c->hwadd > 0.0f) phi = phi + added_wing(c, q - h->dqbar);
+    return phi;
+  }
+  return hprofile(tgx, th2x, h, c, q);
 }
 
 void or_hprofile(const or_hline_t *h, const float *tgx, const float *th2x, float temp, float ne, float fo,
@@ -389,11 +453,13 @@ void or_add_h_opacities(const or_hline_t *h, const float *tgx, const float *th2x
     hcell_t c;
     hcell_prepare(h, cl->temp[i], cl->ne[i], cl->fo[i], cl->vbar2h[i], cl->tothi[i], cl->t3nhe[i], idf, &c);
     const size_t base = (size_t)nf * (size_t)i;
+    const double qt = c.use_vcs ? c.vcs.q_tail + h->dqmax : HUGE_VAL;
+    const double vp = (double)cl->vproj[i];
     const float ref = tol * cont[base + f0];
     float lchi = ref;
     for (int f = f0; lchi >= ref && f < nf; f++) {
       const double q = (nu[f] - (double)v) * (double)inv_nu0;
-      const float phi = hprofile(tgx, th2x, h, &c, q);
+      const float phi = profile_at(tgx, th2x, h, &c, qt, vp, nu[f], q);
       lchi = phi * cchi;
       const float leta = phi * ceta;
       chi[base + f] = chi[base + f] + lchi;
@@ -406,7 +472,7 @@ void or_add_h_opacities(const or_hline_t *h, const float *tgx, const float *th2x
     lchi = ref;
     for (int f = f0 - 1; lchi >= ref && f >= 0; f--) {
       const double q = (nu[f] - (double)v) * (double)inv_nu0;
-      const float phi = hprofile(tgx, th2x, h, &c, q);
+      const float phi = profile_at(tgx, th2x, h, &c, qt, vp, nu[f], q);
       lchi = phi * cchi;
       const float leta = phi * ceta;
       chi[base + f] = chi[base + f] + lchi;

@@ -16,6 +16,7 @@ extern "C" {
 /* hline_t (hprofl_mod.f90:156-165) */
 typedef struct or_hline {
   int n, m, bpo, io;
+  int opts, pad;             /* the switches it was built with (disable_vdw reaches hcell_prepare) */
   double nu0, grad, gstk, gw1, gw2, gw3;
   double dq[14], wt[14];
   double dqbar, dqmax, qray;

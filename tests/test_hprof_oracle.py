@@ -77,3 +77,59 @@ def test_walk_adds_the_profile_until_below_tolerance(oracle):
             assert want[nz[-1]] < ref or nz[-1] == 800
             assert want[nz[0]] < ref or nz[0] == 0
             assert (want[nz[0] + 1:f0] >= ref).all() and (want[f0:nz[-1]] >= ref).all()
+
+
+def _load_synthetic(tmp_path, oh):
+    import vcs_cases
+    paths = vcs_cases.write_all(str(tmp_path))
+    for s, p in paths.items():
+        oh.vcs_load(s, p, s == 3)
+    return paths
+
+
+def test_vcs_profile_is_normalised_and_continues_into_its_tail(oracle, tmp_path):
+    """The prepared table profile has unit area under the trapezium rule
+    vcs_cell_profile normalises with, and the power-law tail meets vcs_eval at the
+    table's outer edge (tail_coef extrapolates qpol's log-log line there)."""
+    from oracle import hprof as oh
+    _load_synthetic(tmp_path, oh)
+    try:
+        for n, m, lam in [(2, 3, 6564.61), (2, 12, 3751.2), (3, 4, 18756.1), (4, 7, 21661.2)]:
+            h = oh.hydrogen_line(n, m, hc.nu0(lam))
+            for T, ne, nH in [(4500.0, 3e11, 1e15), (9000.0, 5e14, 1e13), (20000.0, 1e17, 1e17)]:
+                cell = {"temp": T, "ne": ne, "tothi": nH, "fo": 1.25e-9 * ne ** (2 / 3), "vbar2h": 1e11,
+                        "t3nhe": 1e10, "inv_df": 2.99792458e10 / 1.1e6}
+                lam0 = lam
+                q_edge = 10 ** (-2.0 + 4.3) / lam0
+                q = np.array([q_edge * (1 - 1e-7), q_edge * (1 + 1e-7), -q_edge * (1 - 1e-7)])
+                # the tail's own branch starts past q_edge + dqmax; close to it both sides agree
+                phi = oh.hprofile(h, cell, q)
+                assert phi[0] == pytest.approx(phi[1], rel=2e-3)
+                # unit area in q over the table (trapezium over a fine grid, both wings)
+                qq = np.concatenate([-np.logspace(np.log10(q_edge), -9, 6000), np.logspace(-9, np.log10(q_edge), 6000)])
+                area = np.trapezoid(oh.hprofile(h, cell, qq).astype(np.float64), qq)
+                assert 0.9 < area < 1.05
+    finally:
+        oh.vcs_clear()
+
+
+def test_vcs_reads_the_reference_tables_when_present(oracle):
+    """With the reference's own table files at hand (not on every machine), every
+    series loads and every tabulated Balmer line gives a finite, positive profile."""
+    import os
+    from oracle import hprof as oh
+    d = "/root/reference/experiments/OpenMULTI3D/HOP/hopacity/data/vcs"
+    if not os.path.isdir(d):
+        pytest.skip("the reference's VCS tables are not present")
+    try:
+        oh.vcs_load(1, os.path.join(d, "stehle_balmer.txt"), False)
+        oh.vcs_load(2, os.path.join(d, "stehle_paschen.txt"), False)
+        oh.vcs_load(3, os.path.join(d, "vcs_bracket.txt"), True)
+        q = np.linspace(-1e-3, 1e-3, 101)
+        for m in range(3, 12):
+            h = oh.hydrogen_line(2, m, 2.99792458e18 / (911.5 / (0.25 - 1.0 / m ** 2) / 4))
+            phi = oh.hprofile(h, {"temp": 6000.0, "ne": 1e14, "tothi": 1e16, "fo": 1.25e-9 * 1e14 ** (2 / 3),
+                                  "vbar2h": 1e11, "t3nhe": 1e14, "inv_df": 2.99792458e10 / 1.1e6}, q)
+            assert np.isfinite(phi).all() and phi.min() > 0
+    finally:
+        oh.vcs_clear()
