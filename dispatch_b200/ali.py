@@ -59,7 +59,8 @@ class _AtomIteration:
     (nlte_patch_t%execute: normalize_profiles, update_populations, the convergence
     bookkeeping and ng_acceleration)."""
 
-    def _init_atom(self, atom: dict, wins: list, temp, ne, nH, abundance, awgt: float, vmic_kms: float, dev):
+    def _init_atom(self, atom: dict, wins: list, temp, ne, nH, abundance, awgt: float, vmic_kms: float, dev,
+                   all_wins: list | None = None):
         import torch
 
         f32 = lambda a: torch.as_tensor(np.ascontiguousarray(a, np.float32), device=dev)
@@ -92,7 +93,7 @@ class _AtomIteration:
         self.gamma_ij = torch.zeros((self.nrad, nc), dtype=torch.float32, device=dev)
         self.gamma_ji = torch.zeros_like(self.gamma_ij)
         sums = np.zeros(int(atom["nline"]), np.uint8)
-        for w in wins:
+        for w in (all_wins if all_wins is not None else wins):
             sums[np.asarray(w["line_ntrans"], np.int64)] = np.asarray(w["sums_over_windows"], np.uint8)
         self.has_wphi = sums
         # profile integrals of the lines whose windows are summed (rows of the others stay 0)
@@ -104,9 +105,18 @@ class _AtomIteration:
         self._last_maxerr = 0.0
         self._global = 0.0
         self.converged = False
+        self.group = None
 
     def sweep(self) -> None:
         raise NotImplementedError
+
+    def _exchange(self) -> None:
+        """With a process group, the rates of every rank's windows summed on all ranks
+        (and the first sweep's profile integrals), before the update."""
+        if self.group is None:
+            return
+        from . import shard
+        shard.allreduce_rates(self.gamma_ij, self.gamma_ji, self.wphi if self.iter == 0 else None, self.group)
 
     # ---- nlte_patch_t%execute ----------------------------------------------------------
     def update(self) -> dict:
@@ -146,11 +156,13 @@ class _AtomIteration:
         the next iteration's formal solutions unless it converged."""
         if self.iter == 0:
             self.sweep()
+            self._exchange()
         while self.iter < maxiter and not self.converged:
             self.iter += 1
             self.update()
             if not self.converged and self.iter < maxiter:
                 self.sweep()
+                self._exchange()
         return self.history
 
 class AliWindow(_AtomIteration):
@@ -296,22 +308,39 @@ class AliColumns(_AtomIteration):
     jnu_weights=True)[...,2] in 1D).  Each sweep is the plan's fixed launch
     sequence, replayed from a CUDA graph when use_graph; the update between sweeps
     is the base class's.  With autotune the plan times the column solver's launch
-    shapes once.
+    shapes once.  With a process group the windows are shared out over its ranks
+    (every world-th one, or the indices given as windows) and run() sums the rates
+    over the ranks before each update (shard.allreduce_rates).
     """
 
     def __init__(self, cols: dict, atom: dict, wins: list, mu, wmu, params: AliParams | None = None,
                  abundance: float = 7.5, awgt: float = 56.0, vmic_kms: float = 1.0, use_graph: bool = True,
-                 autotune: bool = True, device: str = "cuda"):
+                 autotune: bool = True, device: str = "cuda", group=None, windows=None):
         import torch
 
         init()
         self.p = params or AliParams()
         dev = torch.device(device)
         self.dev = dev
-        self.wins = list(wins)
+        all_wins = list(wins)
+        if group is not None and windows is None:
+            # frequency windows across the ranks of group: this rank's plan holds every
+            # world-th window, and run() sums the rates over the ranks (shard.py)
+            import torch.distributed as dist
+
+            from . import shard
+            windows = shard.windows_for_rank(dist.get_rank(group), dist.get_world_size(group), len(all_wins))
+        if windows is not None:
+            if not len(windows):
+                raise M3DError(f"AliColumns: no window of {len(all_wins)} for this plan")
+            self.wins = [all_wins[w] for w in windows]
+        else:
+            self.wins = all_wins
         self.use_graph = bool(use_graph)
         abund = abundance + np.asarray(cols.get("abund_dex", 0.0), np.float64)
-        self._init_atom(atom, self.wins, cols["temp"], cols["ne"], cols["nH"], abund, awgt, vmic_kms, dev)
+        self._init_atom(atom, self.wins, cols["temp"], cols["ne"], cols["nH"], abund, awgt, vmic_kms, dev,
+                        all_wins=all_wins)
+        self.group = group
         nc = self.ncell
         f32 = lambda a: torch.as_tensor(np.ascontiguousarray(a, np.float32), device=dev)
         self.col_off = torch.as_tensor(np.asarray(cols["col_off"], np.int32), device=dev)

@@ -2,9 +2,12 @@
 
 The reference splits the spectrum into n_windows frequency windows whose
 opacities and sweeps are independent for all rays (E/SRC/ray_patch_mod.f90:97-127).
-A rank takes every world-th window; the spectra of the windows a rank computed
-are gathered to every rank only for output, and the step time reported is the
-maximum over ranks.  Nothing on the data path is exchanged.
+A rank takes every world-th window.  In LTE the spectra of the windows a rank
+computed are gathered to every rank only for output, and the step time reported
+is the maximum over ranks.  In an NLTE iteration the radiative rates are sums over
+all windows: each rank sums its own windows' rates, one all-reduce (sum) per
+iteration forms the totals on every rank (and once the profile integrals of the
+first sweep), and every rank then takes the same statistical-equilibrium update.
 """
 from __future__ import annotations
 
@@ -50,3 +53,16 @@ def max_over_ranks(ms: float) -> float:
     t = torch.tensor([ms], dtype=torch.float64)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def allreduce_rates(gamma_ij, gamma_ji, wphi=None, group=None) -> None:
+    """The NLTE exchange of one ALI iteration: gamma_ij and gamma_ji (nrad, ncell),
+    and the profile integrals wphi of the first sweep when given, summed over the
+    ranks in place (torch.distributed; NCCL on the GPUs, gloo on CPU).  The sum
+    groups the windows by rank, so against one rank summing every window in order
+    the rates differ by float32 reassociation only."""
+    import torch.distributed as dist
+
+    for t in (gamma_ij, gamma_ji, wphi):
+        if t is not None:
+            dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)

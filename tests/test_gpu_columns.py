@@ -93,3 +93,57 @@ def test_column_plan_rejects_bad_input(m3d):
         ali.AliColumns(cols, atom, wins, mu[::-1].copy(), wmu)
     torch.cuda.synchronize()
     assert m3d.lib().m3d_col_plan_destroy(C.c_void_p()) == 0
+
+
+def test_windows_shared_over_ranks_equal_one_plan(m3d):
+    """The frequency-sharded iteration on one GPU: two plans each holding every
+    other window (what two ranks hold), their rates summed as the exchange sums
+    them, equal the plan of all windows bit for bit (every transition sits in one
+    window), and so does the update that follows."""
+    from dispatch_b200 import ali
+    cols, atom, wins, mu, wmu = _problem(sums=True)
+    wins = wins + [w for w in _problem()[2]]      # four windows
+    full = ali.AliColumns(cols, atom, wins, mu, wmu, use_graph=False)
+    part = [ali.AliColumns(cols, atom, wins, mu, wmu, use_graph=False, windows=list(range(r, len(wins), 2)))
+            for r in range(2)]
+    for A in [full] + part:
+        A.sweep()
+    for name in ("gamma_ij", "gamma_ji", "wphi"):
+        s = getattr(part[0], name) + getattr(part[1], name)
+        np.testing.assert_array_equal(s.cpu().numpy(), getattr(full, name).cpu().numpy())
+        getattr(part[0], name).copy_(s)
+    for A in (full, part[0]):
+        A.iter = 1
+        A.update()
+    np.testing.assert_array_equal(part[0].b.cpu().numpy(), full.b.cpu().numpy())
+    for A in [full] + part:
+        A.close()
+
+
+def test_process_group_of_one_runs_the_exchange(m3d):
+    """A one-rank NCCL group: the windows all stay on the rank and run() calls the
+    exchange each iteration; the iterations equal those without a group."""
+    import socket
+
+    import torch
+    import torch.distributed as dist
+    from dispatch_b200 import ali
+    cols, atom, wins, mu, wmu = _problem()
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    from datetime import timedelta
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
+                            timeout=timedelta(seconds=60), device_id=torch.device("cuda", 0))
+    try:
+        A = ali.AliColumns(cols, atom, wins, mu, wmu, params=ali.AliParams(convlim=1e-9), group=dist.group.WORLD,
+                           use_graph=False)
+        A.run(3)
+        B = ali.AliColumns(cols, atom, wins, mu, wmu, params=ali.AliParams(convlim=1e-9), use_graph=False)
+        B.run(3)
+        np.testing.assert_array_equal(A.b.cpu().numpy(), B.b.cpu().numpy())
+        A.close()
+        B.close()
+    finally:
+        dist.destroy_process_group()

@@ -49,3 +49,56 @@ def test_gather_and_max_over_two_gloo_ranks():
     for rank, full, t in res:
         np.testing.assert_array_equal(full, exp)
         assert t == 11.0
+
+
+def _rates_worker(rank, world, port, q):
+    import torch
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        from dispatch_b200 import ali
+        from dispatch_b200.shard import allreduce_rates, windows_for_rank
+        from oracle import ali as oali
+        cols, atom, wins, mu, wmu = ali.column_problem(variants=(0.0,))
+        mine = [wins[w] for w in windows_for_rank(rank, world, len(wins))]
+        S = oali.setup_columns(cols, atom, mine, mu, wmu)
+        oali.sweep_columns(S)
+        gij, gji = torch.from_numpy(S["gamma_ij"].copy()), torch.from_numpy(S["gamma_ji"].copy())
+        wphi = torch.from_numpy(S["wphi"].copy())
+        allreduce_rates(gij, gji, wphi)
+        q.put((rank, gij.numpy(), gji.numpy(), wphi.numpy()))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_rates_summed_over_two_gloo_ranks_equal_one_rank():
+    """Two ranks each sweep half of the atom's windows (the oracle's composition
+    stands in for the device sweep on CPU) and sum their rates with the NLTE
+    exchange: every transition sits in one window, so the sums equal the single
+    sweep over all windows bit for bit."""
+    import multiprocessing as mp
+    import socket
+    from dispatch_b200 import ali
+    from oracle import ali as oali
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_rates_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=300) for _ in procs]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    cols, atom, wins, mu, wmu = ali.column_problem(variants=(0.0,))
+    S = oali.setup_columns(cols, atom, wins, mu, wmu)
+    oali.sweep_columns(S)
+    for rank, gij, gji, wphi in res:
+        np.testing.assert_array_equal(gij, S["gamma_ij"])
+        np.testing.assert_array_equal(gji, S["gamma_ji"])
+        np.testing.assert_array_equal(wphi, S["wphi"])
+    assert np.abs(S["gamma_ij"]).max() > 0
