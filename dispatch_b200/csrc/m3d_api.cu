@@ -13,6 +13,8 @@
 #include <type_traits>
 #include <vector>
 
+#include <sys/stat.h>
+
 #include <cuda_runtime.h>
 
 #include "../../include/m3dgpu.h"
@@ -1340,6 +1342,7 @@ int m3d_lte_synthesis(const m3d_atmos_t *atm, int nf, const double *nu, const do
 #include "m3d_columns_api.inc"
 #include "m3d_optab_api.inc"
 #include "m3d_hprof_api.inc"
+#include "m3d_io_api.inc"
 
 // ===========================================================================
 // rotate_array without any allocation.

@@ -309,6 +309,16 @@ int m3d_h_opacity(const m3d_hline_t *h, double Bij, int f0, int nf, const double
                   const m3d_hcells_t *cells, const float *bi, const float *bj, float *chi, float *eta,
                   const float *cont, int *line_used, float *line_strength, unsigned flags);
 
+/* ---- output files: patch_t%save5 (tasks/patch_mod.f90:4248-4346) from the library's
+ * buffers.  Writes <run_dir>/save/<label>_<key>.bin, the float32 array of shape dims
+ * (5, Fortran order, first fastest) raw, and with add2meta appends its line to
+ * <label>_meta.txt (header on creation).  key: 1 to 3 integers (abs, 3 digits each),
+ * as patch_t%key(1:3) or (1:2).  mem is a host pointer, or a device pointer with
+ * M3D_DEVICE_PTRS.  save_intensity's 'ie' (nf,1,1,nmu,nset) and 'flux' (nf,1,1,1,nset),
+ * and the J/PsiJ/Jali of rt_to_file, are such arrays. */
+int m3d_save5(const char *run_dir, const char *label, const int *key, int nkey, const float *mem, const int *dims,
+              int add2meta, unsigned flags);
+
 /* rotate_array (rt_patch_mod.f90:3809-3866) on work(:,:,:,1:nz,1:2), in place. */
 int m3d_rotate_array(const m3d_slab_t *slab, void *work, const double *ds_code, double bot2pivot,
                      const double *ray_offset, unsigned flags);

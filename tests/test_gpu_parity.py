@@ -365,3 +365,17 @@ def test_chi_scat_units(m3d):
     got = cs.copy()
     m3d.rt.chi_scat_units(got, beta)
     np.testing.assert_array_equal(got, exp)
+
+
+def test_save5_from_device_buffers(m3d, tmp_path):
+    """The output files written straight from device tensors equal those from host buffers."""
+    import os
+
+    import torch
+    from dispatch_b200 import output
+    a = np.random.default_rng(2).random((2, 1, 1, 3, 40)).astype(np.float32)
+    output.save5(str(tmp_path / "h"), "J", (3, 1, 7), a)
+    output.save5(str(tmp_path / "d"), "J", (3, 1, 7), torch.from_numpy(a).cuda())
+    for f in ("J_003001007.bin", "J_meta.txt"):
+        assert open(os.path.join(str(tmp_path / "h"), "save", f), "rb").read() == \
+            open(os.path.join(str(tmp_path / "d"), "save", f), "rb").read()
