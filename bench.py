@@ -220,6 +220,19 @@ def run_reference(a):
     print(json.dumps(line), flush=True)
 
 
+def _issue_from_profiles():
+    """The issue-slot utilisation ncu measured for the line-opacity kernel (the
+    fraction of cycles an SM sub-partition issued), from the committed summary."""
+    path = os.path.join(ROOT, "profiles", "k_lte_opacity_units_lane_c1_48.md")
+    try:
+        for line in open(path):
+            if line.startswith("issue_active_fraction:"):
+                return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
 def _nlte_ali(steps=2):
     """The ALI window of the 3D NLTE configuration, measured beside the headline: the
     120^3 cube, the 20-level atom, a frequency window holding 10 of its 80 transitions
@@ -470,6 +483,12 @@ def run_b200(a):
                 "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak if achieved else None,
                 "traffic": traffic, "peak_source": "measured" if peaks else "fallback",
                 "algorithmic_bytes_per_launch": bytes_launch}
+    # the step's dominant kernel is the line opacity, bound by instruction issue
+    # (FP32/ALU, 0.01 % of DRAM peak); its roofline is the issue rate
+    dominant = {"kernel": "k_lte_opacity_units_lane<32> (line opacity + transfer units, every ray)",
+                "share_of_step": op_ms / (op_ms + sv_ms + rd_ms) if op_ms else None, "bound": "issue (fp32 alu)",
+                "issue_active_frac": _issue_from_profiles(),
+                "issue_source": "ncu smsp__issue_active, profiles/k_lte_opacity_units_lane_c1_48.md (48^3 case)"}
     stages = {"opacity_ms_per_step": op_ms, "opacity_launches": op_n, "solve_ms_per_step": sv_ms,
               "solve_launches": sv_n, "reduce_ms_per_step": rd_ms,
               "solve_gpt_per_s": work_per_step / (sv_ms / 1e3) / 1e9 if sv_ms else None}
@@ -549,7 +568,8 @@ def run_b200(a):
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic (seeded grey cube, random line list)", "config": _workload(nf, a.cube),
-            "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline, "cpu_baseline": cpu,
+            "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline, "dominant_kernel": dominant,
+            "cpu_baseline": cpu,
             "clocks": clocks, "stages": stages, "fp64_plain": fp64, "nlte_ali": nlte,
             "nlte_batched": batched, "optab": optab}
     print(json.dumps(line), flush=True)
