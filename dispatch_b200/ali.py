@@ -75,6 +75,7 @@ class _AtomIteration:
         nstar, totn = synth.lte_populations(atom, temp, ne, totn0)
         self.temp32 = temp
         self.temp, self.ne = f64(temp), f64(ne)
+        self.nh1 = f64(synth.hydrogen_ground(nH, ne)) if atom.get("col_hkind") is not None else None
         self.e_kT = f64(synth.EE / synth.BK / temp.astype(np.float64))
         self.nstar, self.totn = f64(nstar), f64(totn)
         self.pop_ratio = torch.ones(nc, dtype=torch.float64, device=dev)
@@ -126,7 +127,7 @@ class _AtomIteration:
                                 first_iter=it == 1)
         stateq.shift_oldb(self.oldb, self.b)
         res, _ = stateq.stateq_update(self.atom, self.b, self.nstar, self.totn, self.e_kT, self.gamma_ij,
-                                      self.gamma_ji, temp=self.temp, ne=self.ne, solver=p.se_solver,
+                                      self.gamma_ji, temp=self.temp, ne=self.ne, nh1=self.nh1, solver=p.se_solver,
                                       max_update=p.max_update, sor_w=p.sor_w, min_pop_frac=p.min_pop_frac)
         maxerr = float(res["maxerr"])
         self.ng.count_clamped(res["nclamp"], res["ntot"])

@@ -1,6 +1,6 @@
 // Statistical equilibrium on the device, FP64: the rate matrix of every cell
 // (setup_transition_matrix, SRC/atom_mod.f90:740-841, with line_rate_coefficients
-// :862-884 and the electron branches of classic_col :1758-1850), its dense solve
+// :862-884 and the electron and hydrogen recipes of classic_col :1758-1880), its dense solve
 // (lineq_no_pivot / lineq, HOP/op_math_mod.f90:263-356, 420-449, or LU with
 // partial pivoting) and the population update (update_populations :439-732);
 // then Ng's accumulation and extrapolation in ln b (SRC/ng_mod.f90:241-390).
@@ -21,6 +21,7 @@ namespace m3d {
 
 constexpr int SE_NMAX = 64;
 constexpr int SE_COL_REGEMORTER = 1, SE_COL_SEATON = 2;
+constexpr int SE_COLH_DRAWIN = 1, SE_COLH_TAKEDA = 2;
 
 // Atom tables in device memory.  Transitions are listed by round: the
 // transitions of one round touch pairwise different matrix elements, and a
@@ -36,7 +37,9 @@ struct SeAtomDev {
   const int *ion;        // [n]
   const int *ci, *cj, *ckind;  // [ncol]
   const float *cfac;           // [ncol]
+  const int *chkind;           // [ncol] hydrogen recipes, or null: none
   double fmin, cbbesc, cbfesc, colscale, upsilon_floor, cut_x, bf_cut_rate;
+  double drawin, cbbhsc, cbfhsc;
 };
 
 struct SeParams {
@@ -47,7 +50,7 @@ struct SeParams {
 struct SeCells {
   int ncell;
   double *b;
-  const double *nstar, *totn, *temp, *ne, *e_kT, *dxi;
+  const double *nstar, *totn, *temp, *ne, *e_kT, *dxi, *nh1;
   const float *gij, *gji;
   const double *cup;  // precomputed collision rates, or null to form them here
 };
@@ -119,9 +122,9 @@ __device__ __forceinline__ double se_kramer(double lam, double dev) {
   return 0.0;
 }
 
-struct SeColCell { double allen, regemorter, seaton, ekt, dxi; };
+struct SeColCell { double allen, regemorter, seaton, ekt, dxi, sqt, ne, nh1; };
 
-__device__ __forceinline__ SeColCell se_col_cell(double temp, double ne, double ekt, double dxi) {
+__device__ __forceinline__ SeColCell se_col_cell(double temp, double ne, double ekt, double dxi, double nh1) {
   const double PI = 3.14159265359, BK = 1.380662e-16, EM = 9.109534e-28, RB = 5.29177349e-9;
   const double E_K = 1.602189e-12 / BK, RYDK = 13.605 * E_K;
   const double sq8bmp = sqrt(8 * BK / EM / PI);
@@ -133,11 +136,17 @@ __device__ __forceinline__ SeColCell se_col_cell(double temp, double ne, double 
   w.seaton = (double)1.55e13f * ne / sqt;
   w.ekt = ekt;
   w.dxi = dxi;
+  w.sqt = sqt;
+  w.ne = ne;
+  w.nh1 = nh1;
   return w;
 }
 
-// upward electron-collision rate of pair p [1/s], colscale applied
-__device__ __forceinline__ double se_col_rate(const SeAtomDev &A, const SeColCell &w, int p) {
+// upward collision rates of pair p [1/s], colscale applied: ue by the pair's
+// electron recipe, uh by its hydrogen recipe (0 without one).  The electron mass
+// ame of the hydrogen recipes is a default-real literal (atom_mod.f90:220-222).
+__device__ __forceinline__ void se_col_rates(const SeAtomDev &A, const SeColCell &w, int p, double &ue,
+                                             double &uh) {
   const double sqr3_2pi = (sqrt(3.0) / 2.0) / 3.14159265359;
   const int i = A.ci[p], j = A.cj[p], kind = A.ckind[p];
   const int ioni = A.ion[i], ionj = A.ion[j];
@@ -169,16 +178,48 @@ __device__ __forceinline__ double se_col_rate(const SeAtomDev &A, const SeColCel
     v = v * A.cbbesc;
   }
   if (v != 0) v = v * A.colscale;
-  return v;
+  ue = v;
+  // hydrogen (atom_mod.f90:1854-1876): Takeda for a line without an f value,
+  // else Drawin
+  const int hkind = A.chkind ? A.chkind[p] : 0;
+  double h = 0;
+  const double ame = (double)5.485799e-4f, amh = 1.0;
+  if (!cont && (double)A.cfac[p] == 0 && hkind == SE_COLH_TAKEDA) {
+    h = w.nh1 * (w.allen / w.ne) * (double)ioni / A.g[i] * ex * sqrt(ame / amh);
+    h = h * A.cbbhsc;
+  } else if (hkind == SE_COLH_DRAWIN) {
+    const double mu_e = ame / (ame + amh);
+    const double q = 13.605 / dev;
+    const double divu = q * q;
+    double tmp = 2.0 / u0;
+    const double mt = mu_e * tmp;
+    tmp = (1.0 + tmp) / (1.0 + mt * mt);
+    h = w.nh1 * A.drawin * divu * tmp * ex * w.sqt;
+    if (cont) {
+      h = h * A.cbfhsc;
+    } else {
+      h = h * f;
+      h = h * A.cbbhsc;
+    }
+  }
+  if (h != 0) h = h * A.colscale;
+  uh = h;
 }
 
-// cup[cell + ncell*p], one thread per cell
+// cup[cell + ncell*p] the electron rates; with hydrogen recipes
+// cup[cell + ncell*(ncol + p)] the hydrogen ones.  One thread per cell.
 __global__ void k_collision_rates(SeAtomDev A, int ncell, const double *__restrict__ temp,
                                   const double *__restrict__ ne, const double *__restrict__ ekt,
-                                  const double *__restrict__ dxi, double *__restrict__ cup) {
+                                  const double *__restrict__ dxi, const double *__restrict__ nh1,
+                                  double *__restrict__ cup) {
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += gridDim.x * blockDim.x) {
-    const SeColCell w = se_col_cell(temp[c], ne[c], ekt[c], dxi ? dxi[c] : 0.0);
-    for (int p = 0; p < A.ncol; p++) cup[(size_t)c + (size_t)ncell * p] = se_col_rate(A, w, p);
+    const SeColCell w = se_col_cell(temp[c], ne[c], ekt[c], dxi ? dxi[c] : 0.0, nh1 ? nh1[c] : 0.0);
+    for (int p = 0; p < A.ncol; p++) {
+      double ue, uh;
+      se_col_rates(A, w, p, ue, uh);
+      cup[(size_t)c + (size_t)ncell * p] = ue;
+      if (A.chkind) cup[(size_t)c + (size_t)ncell * (A.ncol + p)] = uh;
+    }
   }
 }
 
@@ -426,17 +467,33 @@ __global__ void k_stateq_update(SeAtomDev A, SeParams P, SeCells C, SeWarpBest *
       }
       __syncwarp();
     }
-    // collisions times cswitch; the pairs are distinct
+    // collisions times cswitch; the pairs are distinct.  c starts at zero and
+    // takes each nonzero rate, the electron one first (classic_col :1846-1876).
     if (P.cswitch > 0 && A.ncol > 0) {
-      SeColCell cw{0, 0, 0, 0, 0};
-      if (!C.cup) cw = se_col_cell(C.temp[c], C.ne[c], ekt, C.dxi ? C.dxi[c] : 0.0);
+      SeColCell cw{0, 0, 0, 0, 0, 0, 0, 0};
+      if (!C.cup) cw = se_col_cell(C.temp[c], C.ne[c], ekt, C.dxi ? C.dxi[c] : 0.0, C.nh1 ? C.nh1[c] : 0.0);
       for (int p = lane; p < A.ncol; p += 32) {
-        const double u = C.cup ? C.cup[(size_t)c + (size_t)ncell * p] : se_col_rate(A, cw, p);
-        if (u == 0) continue;
+        double ue, uh = 0;
+        if (C.cup) {
+          ue = C.cup[(size_t)c + (size_t)ncell * p];
+          if (A.chkind) uh = C.cup[(size_t)c + (size_t)ncell * (A.ncol + p)];
+        } else {
+          se_col_rates(A, cw, p, ue, uh);
+        }
+        if (ue == 0 && uh == 0) continue;
         const int i = A.ci[p], j = A.cj[p];
         const double nij = ns[i] / ns[j];
-        W[j + n * i] = W[j + n * i] + u * P.cswitch;
-        W[i + n * j] = W[i + n * j] + (u * nij) * P.cswitch;
+        double cu = 0, cd = 0;
+        if (ue != 0) {
+          cu = cu + ue;
+          cd = cd + ue * nij;
+        }
+        if (uh != 0) {
+          cu = cu + uh;
+          cd = cd + uh * nij;
+        }
+        W[j + n * i] = W[j + n * i] + cu * P.cswitch;
+        W[i + n * j] = W[i + n * j] + cd * P.cswitch;
       }
       __syncwarp();
     }

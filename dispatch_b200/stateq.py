@@ -10,8 +10,9 @@ extrapolation itself run on the device.
 
 Atoms are dicts of numpy arrays (dispatch_b200.synth.model_atom builds them):
 nlevel, g, ev, ion, ti, tj, nline, Aji, active (or None), col_i, col_j,
-col_kind, col_fac and the scalar factors fmin, cbbesc, cbfesc, colscale,
-upsilon_floor, cut_x, bf_cut_rate.  Level and transition indices are 0-based.
+col_kind, col_fac, optionally col_hkind with awgt (hydrogen recipes), and the
+scalar factors fmin, cbbesc, cbfesc, colscale, upsilon_floor, cut_x,
+bf_cut_rate, cbbhsc, cbfhsc.  Level and transition indices are 0-based.
 Per-cell arrays are numpy (C order (level, cell), i.e. the reference's
 (cell, level) with the cell fastest) or torch CUDA tensors.
 """
@@ -27,6 +28,7 @@ from . import DEVICE_PTRS, M3DError, check, init, lib, order_after_torch, ptr
 
 LINEQ_NO_PIVOT, LINEQ, LU_PARTIAL = 0, 1, 2
 COL_REGEMORTER, COL_SEATON = 1, 2
+COLH_DRAWIN, COLH_TAKEDA = 1, 2
 ENONFINITE = 5
 
 
@@ -38,7 +40,8 @@ class Atom(C.Structure):
                 ("g", C.c_void_p), ("ev", C.c_void_p), ("ion", C.c_void_p),
                 ("col_i", C.c_void_p), ("col_j", C.c_void_p), ("col_kind", C.c_void_p), ("col_fac", C.c_void_p),
                 ("fmin", C.c_double), ("cbbesc", C.c_double), ("cbfesc", C.c_double), ("colscale", C.c_double),
-                ("upsilon_floor", C.c_double), ("cut_x", C.c_double), ("bf_cut_rate", C.c_double)]
+                ("upsilon_floor", C.c_double), ("cut_x", C.c_double), ("bf_cut_rate", C.c_double),
+                ("col_hkind", C.c_void_p), ("drawin", C.c_double), ("cbbhsc", C.c_double), ("cbfhsc", C.c_double)]
 
 
 class SeParams(C.Structure):
@@ -95,7 +98,82 @@ def make_atom(atom: dict) -> tuple[Atom, list]:
     for k, d in (("fmin", float(np.float32(1e-6))), ("cbbesc", 1.0), ("cbfesc", 1.0), ("colscale", 1.0),
                  ("upsilon_floor", 0.0), ("cut_x", 70.0), ("bf_cut_rate", 1.0)):
         setattr(s, k, float(atom.get(k, d)))
+    s.col_hkind = arr("col_hkind", np.int32)
+    s.drawin = prepare_drawin(float(atom["awgt"])) if s.col_hkind is not None else 0.0
+    s.cbbhsc, s.cbfhsc = float(atom.get("cbbhsc", 1.0)), float(atom.get("cbfhsc", 1.0))
     return s, keep
+
+
+# constants of prepare_Drawin (HOP/const_mod.f90:14-47, atom_mod.f90:220-222); ame is
+# a default-real literal there, so its single-precision value enters the double
+# arithmetic
+_PI, _BK, _MH, _RBOHR = 3.14159265359, 1.380662e-16, 1.6726e-24, 5.29177349e-9
+_AME = float(np.float32(5.485799e-4))
+_AMH = 1.0
+_MU_E = _AME / (_AME + _AMH)
+
+
+def prepare_drawin(awgt: float) -> float:
+    """prepare_Drawin (atom_mod.f90:1741-1750): the prefactor of Drawin's hydrogen
+    rate, 16 pi a0^2 sqrt(2k / (pi m_H A mu_H)) mu_e / mu_H with mu_H = 1 / (A + 1),
+    for an atom of weight awgt [amu]."""
+    c = (16 * _PI) * (_RBOHR * _RBOHR)
+    mu_h = _AMH / (awgt + _AMH)
+    drmu = _PI * _MH * awgt * mu_h
+    return c * math.sqrt(2.0 * _BK / drmu) * _MU_E / mu_h
+
+
+def classic_pairs(ion, cont_up, cdata, ecol=None, hcol=None, e_excitation: str = "regemorter",
+                  e_ionisation: str = "seaton", h_excitation: str = "", h_ionisation: str = "",
+                  h_forbidden: str = "") -> dict:
+    """The level pairs classic_col fills and the recipe of each (atom_mod.f90:1790-1876).
+
+    ion (nlevel): ion stage of each level; cont_up (nlevel): the upper level of
+    each level's continuum (-1 without one); cdata (nlevel, nlevel): the pair's
+    f value (line) or alpha0 (continuum), 0 for none, read at [i, j]; ecol /
+    hcol (nlevel, nlevel) bool or None: the pair has electron / hydrogen data in
+    the atom file.  A pair i < j enters when ion(j) >= ion(i), a continuum only
+    towards cont_up(i), and one of its recipes is unset by the file.  Returns
+    col_i, col_j, col_kind, col_hkind (None when no hydrogen recipe is
+    selected) and col_fac.
+    """
+    ion = np.asarray(ion)
+    n = ion.size
+    cdata = np.asarray(cdata, np.float32)
+    ci, cj, ck, chk, cf = [], [], [], [], []
+    for i in range(n):
+        for j in range(i + 1, n):
+            if ion[j] < ion[i]:
+                continue
+            cont = bool(ion[j] > ion[i])
+            if cont and j != cont_up[i]:
+                continue
+            has_e = bool(ecol[i, j]) if ecol is not None else False
+            has_h = bool(hcol[i, j]) if hcol is not None else False
+            if has_e and has_h:
+                continue
+            fac = float(cdata[i, j])
+            kind = 0
+            if not has_e:
+                if cont and e_ionisation == "seaton":
+                    kind = COL_SEATON
+                elif not cont and e_excitation == "regemorter":
+                    kind = COL_REGEMORTER
+            hkind = 0
+            if not has_h:
+                if not cont and fac == 0 and h_forbidden == "takeda":
+                    hkind = COLH_TAKEDA
+                elif (h_ionisation if cont else h_excitation) == "drawin":
+                    hkind = COLH_DRAWIN
+            if kind == 0 and hkind == 0:
+                continue
+            ci.append(i)
+            cj.append(j)
+            ck.append(kind)
+            chk.append(hkind)
+            cf.append(fac)
+    return {"col_i": np.array(ci, np.int32), "col_j": np.array(cj, np.int32), "col_kind": np.array(ck, np.int32),
+            "col_hkind": np.array(chk, np.int32) if any(chk) else None, "col_fac": np.array(cf, np.float32)}
 
 
 def _flags(*arrays) -> int:
@@ -118,21 +196,24 @@ def _f32(a):
     return np.ascontiguousarray(a, np.float32)
 
 
-def collision_rates(atom: dict, temp, ne, e_kT, dxi=None, out=None):
-    """classic_col's upward electron rates (ncol, ncell) [1/s], colscale applied."""
+def collision_rates(atom: dict, temp, ne, e_kT, dxi=None, nh1=None, out=None):
+    """classic_col's upward rates [1/s], colscale applied: (ncol, ncell) of the
+    electron recipes, then, when the atom has col_hkind, ncol more rows of the
+    hydrogen recipes, which read nh1 (the neutral hydrogen ground-level density)."""
     init()
     st, keep = make_atom(atom)
-    temp, ne, e_kT, dxi = _f64(temp), _f64(ne), _f64(e_kT), _f64(dxi)
+    temp, ne, e_kT, dxi, nh1 = _f64(temp), _f64(ne), _f64(e_kT), _f64(dxi), _f64(nh1)
     ncell = int(temp.shape[-1])
+    rows = 2 * st.ncol if st.col_hkind is not None else st.ncol
     if out is None:
-        out = np.zeros((st.ncol, ncell), np.float64)
+        out = np.zeros((rows, ncell), np.float64)
     check(lib().m3d_collision_rates(C.byref(st), C.c_int(ncell), ptr(temp), ptr(ne), ptr(e_kT), ptr(dxi),
-                                    ptr(out), C.c_uint(_flags(temp, out))), "m3d_collision_rates")
+                                    ptr(nh1), ptr(out), C.c_uint(_flags(temp, out))), "m3d_collision_rates")
     return out
 
 
 def stateq_update(atom: dict, b, nstar, totn, e_kT, gamma_ij, gamma_ji, temp=None, ne=None, dxi=None, cup=None,
-                  solver: int = LINEQ_NO_PIVOT, max_update: float = 1e2, sor_w: float = 1.0,
+                  nh1=None, solver: int = LINEQ_NO_PIVOT, max_update: float = 1e2, sor_w: float = 1.0,
                   min_pop_frac: float = 1e-30, conv_pop_floor: float = 0.0, tmax_update: float = 1e7,
                   cswitch: float = 1.0) -> tuple[dict, np.ndarray]:
     """update_populations over all cells; b (nlevel, ncell) float64 is updated in place.
@@ -146,14 +227,15 @@ def stateq_update(atom: dict, b, nstar, totn, e_kT, gamma_ij, gamma_ji, temp=Non
     if isinstance(b, np.ndarray) and (b.dtype != np.float64 or not b.flags.c_contiguous):
         raise M3DError("b must be a C-contiguous float64 array (it is updated in place)")
     nstar, totn, e_kT = _f64(nstar), _f64(totn), _f64(e_kT)
-    temp, ne, dxi, cup = _f64(temp), _f64(ne), _f64(dxi), _f64(cup)
+    temp, ne, dxi, cup, nh1 = _f64(temp), _f64(ne), _f64(dxi), _f64(cup), _f64(nh1)
     gamma_ij, gamma_ji = _f32(gamma_ij), _f32(gamma_ji)
     ncell = int(totn.shape[-1])
     par = SeParams(max_update, sor_w, min_pop_frac, conv_pop_floor, tmax_update, cswitch, int(solver), 0)
     res = SeResult()
     lvlerr = np.zeros(st.nlevel, np.float64)
     rc = lib().m3d_stateq_update(C.byref(st), C.byref(par), C.c_int(ncell), ptr(b), ptr(nstar), ptr(totn),
-                                 ptr(temp), ptr(ne), ptr(e_kT), ptr(dxi), ptr(gamma_ij), ptr(gamma_ji), ptr(cup),
+                                 ptr(temp), ptr(ne), ptr(e_kT), ptr(dxi), ptr(nh1), ptr(gamma_ij), ptr(gamma_ji),
+                                 ptr(cup),
                                  C.c_void_p(lvlerr.ctypes.data), C.byref(res),
                                  C.c_uint(_flags(b, nstar, totn, e_kT)))
     out = res.as_dict()

@@ -368,7 +368,7 @@ RYDV = 13.605
 
 
 def model_atom(seed: int = 2, nbound: int = 20, nline: int = 60, e_max: float = 7.0, e_ion: float = 7.9,
-               logf=(-4.0, 0.0)) -> dict:
+               logf=(-4.0, 0.0), h_recipes=None, awgt: float = 40.08) -> dict:
     """A seeded model atom: nbound levels of the neutral (ground at 0 eV, the rest
     uniform in [0, e_max]) plus the ground level of the ion at e_ion; nline lines
     between distinct random bound pairs with log f uniform in logf; one continuum
@@ -376,7 +376,10 @@ def model_atom(seed: int = 2, nbound: int = 20, nline: int = 60, e_max: float = 
     them for an atom without collision data: van Regemorter for every bound pair
     (f of the pair's line, or 0) and Seaton for every continuum, whose alpha0 is
     the hydrogenic 7.91e-18 n_eff cm^2 for even levels and 0 (Kramers inside
-    the collision recipe) for odd ones.  Indices are 0-based."""
+    the collision recipe) for odd ones.  h_recipes = (h_excitation, h_ionisation,
+    h_forbidden), e.g. ('drawin', 'drawin', 'takeda'), adds the hydrogen recipes
+    of every pair (col_hkind): Takeda for a bound pair without a line, else
+    Drawin.  awgt: the atom's weight [amu].  Indices are 0-based."""
     rng = np.random.default_rng(seed + 2000)
     ev = np.concatenate([[0.0], np.sort(rng.uniform(0.0, e_max, nbound - 1)), [e_ion]])
     g = np.concatenate([rng.choice([1.0, 3.0, 5.0, 7.0, 9.0], nbound), [1.0]])
@@ -412,7 +415,32 @@ def model_atom(seed: int = 2, nbound: int = 20, nline: int = 60, e_max: float = 
             "col_i": np.array(col_i, np.int32), "col_j": np.array(col_j, np.int32),
             "col_kind": np.array(col_kind, np.int32), "col_fac": np.array(col_fac, np.float32),
             "fmin": float(np.float32(1e-6)), "cbbesc": 1.0, "cbfesc": 1.0, "colscale": 1.0,
-            "upsilon_floor": 0.0, "cut_x": 70.0, "bf_cut_rate": 1.0}
+            "upsilon_floor": 0.0, "cut_x": 70.0, "bf_cut_rate": 1.0, "awgt": float(awgt),
+            "col_hkind": _hydrogen_kinds(ion, col_i, col_j, col_fac, h_recipes)}
+
+
+def _hydrogen_kinds(ion, col_i, col_j, col_fac, h_recipes):
+    if not h_recipes:
+        return None
+    h_exc, h_ion, h_forb = h_recipes
+    out = []
+    for i, j, fac in zip(col_i, col_j, np.asarray(col_fac, np.float32)):
+        cont = ion[j] > ion[i]
+        if not cont and fac == 0 and h_forb == "takeda":
+            out.append(2)
+        elif (h_ion if cont else h_exc) == "drawin":
+            out.append(1)
+        else:
+            out.append(0)
+    return np.array(out, np.int32)
+
+
+def hydrogen_ground(nH, ne):
+    """A synthetic neutral hydrogen ground-level density: nH less the protons that
+    charge neutrality with hydrogen as the only electron donor allows, at least 1%
+    of nH."""
+    nH = np.asarray(nH, np.float64)
+    return nH * np.clip(1.0 - np.asarray(ne, np.float64) / nH, 0.01, 1.0)
 
 
 def lte_populations(atom: dict, temp, ne, totn, dxi=None):
@@ -469,16 +497,18 @@ def se_inputs(atom: dict, temp, ne, nH, seed: int = 2, dilution=None, perturb: f
             gji[kr] = 1e3 * nstar[i] / nstar[j]
     b = np.exp(perturb * rng.standard_normal((atom["nlevel"], ncell))) if perturb > 0 else np.ones((atom["nlevel"], ncell))
     return {"temp": temp, "ne": ne, "e_kT": e_kT, "nstar": np.ascontiguousarray(nstar),
-            "totn": np.ascontiguousarray(totn), "b": np.ascontiguousarray(b), "gamma_ij": gij, "gamma_ji": gji}
+            "totn": np.ascontiguousarray(totn), "b": np.ascontiguousarray(b), "gamma_ij": gij, "gamma_ji": gji,
+            "nh1": hydrogen_ground(nH, ne)}
 
 
 def se_config(kind: str = "small", seed: int | None = None, ncell: int | None = None, lte: bool = False,
-              nbound: int = 20, nline: int = 60) -> tuple:
+              nbound: int = 20, nline: int = 60, h_recipes=None) -> tuple:
     """(atom, inputs) of an SE case.  'c2': the 120^3 cube of seed 2 and the
     20-level atom (a radiation field diluted upwards, W = exp(-3 z/nz));
     'small': ncell cells (default 2048) drawn from a 16^3 cube with W uniform
     in [0.05, 1]; lte: W = 1.  nbound/nline: the atom's bound levels and lines
-    (60/180 for the larger atom of the batched configuration)."""
+    (60/180 for the larger atom of the batched configuration); h_recipes: the
+    hydrogen collision recipes of model_atom."""
     if kind == "c2":
         seed = 2 if seed is None else seed
         cube = cube_atmosphere(seed, 120, 120, 120)
@@ -490,7 +520,7 @@ def se_config(kind: str = "small", seed: int | None = None, ncell: int | None = 
         W = np.random.default_rng(seed + 4000).uniform(0.05, 1.0, 16**3)
     else:
         raise ValueError(kind)
-    atom = model_atom(seed, nbound=nbound, nline=nline)
+    atom = model_atom(seed, nbound=nbound, nline=nline, h_recipes=h_recipes)
     temp, ne, nH = cube["temp"].ravel(), cube["ne"].ravel(), cube["nH"].ravel()
     W = np.asarray(W).ravel()
     if ncell is not None:

@@ -406,10 +406,15 @@ int m3d_lte_synthesis(const m3d_atmos_t *atm, int nf, const double *nu, const do
 #define M3D_SE_LU_PARTIAL 2     /* LU with partial (row) pivoting */
 #define M3D_COL_REGEMORTER 1    /* e_excitation='regemorter' (atom_mod.f90:1825-1832) */
 #define M3D_COL_SEATON 2        /* e_ionisation='seaton' (atom_mod.f90:1814-1822) */
+#define M3D_COLH_DRAWIN 1       /* h_excitation / h_ionisation='drawin' (atom_mod.f90:1861-1871) */
+#define M3D_COLH_TAKEDA 2       /* h_forbidden='takeda', a pair without a line (atom_mod.f90:1856-1860) */
 
 /* The model atom (atom_type, atom_mod.f90:120-160).  Transitions 0..nline-1 are the
  * lines, nline..nrad-1 the continua.  Collision pairs are the (i < j) pairs that
- * classic_col fills with an electron recipe, each pair at most once. */
+ * classic_col fills with a recipe, each pair at most once: col_kind its electron
+ * recipe (0 none), col_hkind its hydrogen one (NULL or 0 none).  With hydrogen
+ * recipes the per-cell neutral hydrogen ground-level density nh1 is needed and a
+ * precomputed cup holds 2 ncol rows: the electron rates, then the hydrogen ones. */
 typedef struct m3d_atom {
   int nlevel;                  /* 1..64 */
   int nrad, nline;             /* transitions, of which lines */
@@ -424,6 +429,9 @@ typedef struct m3d_atom {
   double fmin;                    /* atom_params fmin, (double)1e-6f */
   double cbbesc, cbfesc, colscale, upsilon_floor; /* 1, 1, 1, 0 */
   double cut_x, bf_cut_rate;      /* radiative cut, 70 and 1 [1/s] (atom_mod.f90:256-257) */
+  const int *col_hkind;           /* (ncol) M3D_COLH_*, or NULL for electron recipes only */
+  double drawin;                  /* prepare_Drawin's prefactor for the atom's weight (atom_mod.f90:1741-1750) */
+  double cbbhsc, cbfhsc;          /* factors on the bound-bound and bound-free hydrogen rates, 1 and 1 */
 } m3d_atom_t;
 
 typedef struct m3d_se_params {
@@ -449,7 +457,7 @@ typedef struct m3d_se_result {
 /* classic_col's electron rates (atom_mod.f90:1758-1850): cup (ncell, ncol) [1/s],
  * upward, colscale applied; the downward rate is cup * n*_i/n*_j.  dxi may be NULL (0). */
 int m3d_collision_rates(const m3d_atom_t *atom, int ncell, const double *temp, const double *ne,
-                        const double *e_kT, const double *dxi, double *cup, unsigned flags);
+                        const double *e_kT, const double *dxi, const double *nh1, double *cup, unsigned flags);
 
 /* update_populations (atom_mod.f90:439-732) with setup_transition_matrix (:740-841):
  * for every cell with totn > 0 (and temp < tmax_update when temp is given) the rate
@@ -463,7 +471,7 @@ int m3d_collision_rates(const m3d_atom_t *atom, int ncell, const double *temp, c
  * M3D_ENONFINITE with res->nonfinite_cell set (the reference stops the run there). */
 int m3d_stateq_update(const m3d_atom_t *atom, const m3d_se_params_t *par, int ncell, double *b,
                       const double *nstar, const double *totn, const double *temp, const double *ne,
-                      const double *e_kT, const double *dxi, const float *gamma_ij,
+                      const double *e_kT, const double *dxi, const double *nh1, const float *gamma_ij,
                       const float *gamma_ji, const double *cup, double *lvlerr,
                       m3d_se_result_t *res, unsigned flags);
 

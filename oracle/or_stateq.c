@@ -42,6 +42,11 @@
 /* kramer_const = 64 PI^4 EC^10 EM / (3 sqrt(3) CC HH^6) (atom_mod.f90:2414) as the
  * compiler folds it: every power and product rounded to double once */
 #define SQ_KRAMER_CONST 0x1.c6dc1aa1038f0p+97
+#define SQ_MH 1.6726e-24
+/* ame is a default-real literal in the reference (atom_mod.f90:220-222) */
+#define SQ_AME ((double)5.485799e-4f)
+#define SQ_AMH 1.0
+#define SQ_MU_E (SQ_AME / (SQ_AME + SQ_AMH))
 
 /* expin: E1(x) by rational approximations, 0 for x <= 0 (atom_mod.f90:2362-2397) */
 double sq_expin(double x)
@@ -102,21 +107,35 @@ double sq_kramer(double lam, double dev)
   return 0.0;
 }
 
-/* classic_col, electron branches: cup(cell, pair) [1/s] upward, colscale applied
- * (atom_mod.f90:1776-1836); the downward rate is cup * n*_i/n*_j */
+/* prepare_Drawin (atom_mod.f90:1741-1750): 16 pi a0^2 sqrt(2k / (pi m_H A mu_H)) mu_e / mu_H
+ * with mu_H = 1 / (A + 1); const is folded at compile time in the reference, each
+ * operation rounded to double */
+double sq_prepare_drawin(double awgt)
+{
+  const double c = (16 * SQ_PI) * (SQ_RBOHR * SQ_RBOHR);
+  const double mu_h = SQ_AMH / (awgt + SQ_AMH);
+  const double drmu = SQ_PI * SQ_MH * awgt * mu_h;
+  return c * sqrt(2.0 * SQ_BK / drmu) * SQ_MU_E / mu_h;
+}
+
+/* classic_col (atom_mod.f90:1758-1880): cup(cell, pair) [1/s] upward, colscale
+ * applied, the electron recipe's rate in rows 0..ncol-1 and, with chkind, the
+ * hydrogen recipe's in rows ncol..2ncol-1; the downward rate of each is
+ * cup * n*_i/n*_j */
 void or_collisions(const sq_atom_t *at, int ncell, const double *temp, const double *ne, const double *e_kT,
-                   const double *dxi, double *cup)
+                   const double *dxi, const double *nh1, double *cup)
 {
   const double sq32 = sqrt(3.0) / 2.0;
   const double sqr3_2pi = sq32 / SQ_PI;
   const double sq8bmp = sqrt(8 * SQ_BK / SQ_EM / SQ_PI);
   const double c0 = SQ_PI * (SQ_RBOHR * SQ_RBOHR) * sq8bmp;
+  const int ncol = at->ncol;
   for (int c = 0; c < ncell; c++) {
     const double sqt = sqrt(temp[c]);
     const double allen = c0 * SQ_RYDK * ne[c] / sqt;
     const double regemorter = 14.5 * allen * SQ_RYDK / SQ_E_K;
     const double seaton = (double)1.55e13f * ne[c] / sqt;
-    for (int p = 0; p < at->ncol; p++) {
+    for (int p = 0; p < ncol; p++) {
       const int i = at->ci[p], j = at->cj[p];
       const int cont = at->ion[j] > at->ion[i];
       double fac = at->cfac[p], f = 0;
@@ -147,6 +166,28 @@ void or_collisions(const sq_atom_t *at, int ncell, const double *temp, const dou
       }
       if (v != 0) v = v * at->colscale;
       cup[(size_t)c + (size_t)ncell * p] = v;
+      if (!at->chkind) continue;
+      /* hydrogen (:1854-1876); Takeda only for a line without an f value */
+      double h = 0;
+      if (!cont && at->cfac[p] == 0 && at->chkind[p] == SQ_COLH_TAKEDA) {
+        h = nh1[c] * (allen / ne[c]) * at->ion[i] / at->g[i] * ex * sqrt(SQ_AME / SQ_AMH);
+        h = h * at->cbbhsc;
+      } else if (at->chkind[p] == SQ_COLH_DRAWIN) {
+        const double q = SQ_RYDV / dev;
+        const double divu = q * q;
+        double tmp = 2.0 / u0;
+        const double mt = SQ_MU_E * tmp;
+        tmp = (1.0 + tmp) / (1.0 + mt * mt);
+        h = nh1[c] * at->drawin * divu * tmp * ex * sqt;
+        if (cont) {
+          h = h * at->cbfhsc;
+        } else {
+          h = h * f;
+          h = h * at->cbbhsc;
+        }
+      }
+      if (h != 0) h = h * at->colscale;
+      cup[(size_t)c + (size_t)ncell * (ncol + p)] = h;
     }
   }
 }
@@ -270,7 +311,8 @@ void sq_lu_partial(double *a, double *b, int n)
 /* setup_transition_matrix of one cell (atom_mod.f90:740-841) with
  * line_rate_coefficients (:862-884).  bl, ns: b and n* of the cell; gij, gji:
  * the cell's gamma_ij / gamma_ji per transition; cupc: the cell's upward
- * collision rate per pair (unused when cswitch == 0).  Returns W in w
+ * collision rate per pair, electrons then (with chkind) hydrogen, as
+ * or_collisions lays them out (unused when cswitch == 0).  Returns W in w
  * (column-major) and the right-hand side in e. */
 void or_rate_matrix(const sq_atom_t *at, const sq_params_t *pr, const double *bl, const double *ns, double totn,
                     double ekt, const float *gij, const float *gji, const double *cupc, double *w, double *e)
@@ -308,15 +350,25 @@ void or_rate_matrix(const sq_atom_t *at, const sq_params_t *pr, const double *bl
     W(i, j) = W(i, j) + r_down;
   }
   if (pr->cswitch > 0) {
-    /* c(j,i) = cup and c(i,j) = cup * n*_i/n*_j (classic_col :1834-1836), then
+    /* c starts at zero; each nonzero rate adds c(j,i) += cup and c(i,j) += cup *
+     * n*_i/n*_j, electrons first, then hydrogen (classic_col :1846-1876); then
      * w += c * cswitch over the whole matrix (:806-811) */
     for (int p = 0; p < at->ncol; p++) {
-      const double u = cupc[p];
-      if (u == 0) continue;
+      const double ue = cupc[p], uh = at->chkind ? cupc[at->ncol + p] : 0.0;
+      if (ue == 0 && uh == 0) continue;
       const int i = at->ci[p], j = at->cj[p];
       const double nij = ns[i] / ns[j];
-      W(j, i) = W(j, i) + u * pr->cswitch;
-      W(i, j) = W(i, j) + (u * nij) * pr->cswitch;
+      double cu = 0, cd = 0;
+      if (ue != 0) {
+        cu = cu + ue;
+        cd = cd + ue * nij;
+      }
+      if (uh != 0) {
+        cu = cu + uh;
+        cd = cd + uh * nij;
+      }
+      W(j, i) = W(j, i) + cu * pr->cswitch;
+      W(i, j) = W(i, j) + cd * pr->cswitch;
     }
   }
   for (int i = 0; i < n; i++) {
@@ -347,7 +399,8 @@ int or_stateq_update(const sq_atom_t *at, const sq_params_t *pr, int ncell, doub
 {
   const int n = at->nlevel, nrad = at->nrad;
   double *w = (double *)malloc(sizeof(double) * n * n);
-  double *cupc = (double *)malloc(sizeof(double) * (at->ncol > 0 ? at->ncol : 1));
+  const int ncup = at->chkind ? 2 * at->ncol : at->ncol;
+  double *cupc = (double *)malloc(sizeof(double) * (ncup > 0 ? ncup : 1));
   float *gij = (float *)malloc(sizeof(float) * (nrad > 0 ? nrad : 1));
   float *gji = (float *)malloc(sizeof(float) * (nrad > 0 ? nrad : 1));
   double e[64], bl[64], ns[64], bold[64];
@@ -371,7 +424,7 @@ int or_stateq_update(const sq_atom_t *at, const sq_params_t *pr, int ncell, doub
       gji[kr] = gamma_ji[(size_t)c + (size_t)ncell * kr];
     }
     if (pr->cswitch > 0)
-      for (int p = 0; p < at->ncol; p++) cupc[p] = cup[(size_t)c + (size_t)ncell * p];
+      for (int p = 0; p < ncup; p++) cupc[p] = cup[(size_t)c + (size_t)ncell * p];
     or_rate_matrix(at, pr, bl, ns, totn[c], e_kT[c], gij, gji, cupc, w, e);
     if (pr->solver == 0) sq_lineq_no_pivot(w, e, n);
     else if (pr->solver == 1) sq_lineq(w, e, n);

@@ -15,12 +15,14 @@
 extern "C" {
 #endif
 
-/* collision pair kinds of classic_col (atom_mod.f90:1758-1850) */
+/* collision pair kinds of classic_col (atom_mod.f90:1758-1880): electron recipes in
+ * ckind, hydrogen recipes in chkind */
 enum { SQ_COL_REGEMORTER = 1, SQ_COL_SEATON = 2 };
+enum { SQ_COLH_DRAWIN = 1, SQ_COLH_TAKEDA = 2 };
 
 typedef struct sq_atom {
   int nlevel, nrad, nline;     /* transitions 0..nline-1 are lines, nline..nrad-1 continua */
-  int ncol;                    /* electron-collision pairs */
+  int ncol;                    /* collision pairs */
   const int *ti, *tj;          /* [nrad] lower / upper level */
   const unsigned char *active; /* [nrad] or NULL (all active) */
   const double *Aji;           /* [nrad] line Einstein A [1/s] (continua unused) */
@@ -30,6 +32,9 @@ typedef struct sq_atom {
   const float *cfac;           /* [ncol] cdata of the pair (real(4)): f of a line, alpha0 of a continuum, 0 = none */
   double fmin, cbbesc, cbfesc, colscale, upsilon_floor; /* classic_col factors */
   double cut_x, bf_cut_rate;   /* radiative cut (atom_mod.f90:256-257) */
+  const int *chkind;           /* [ncol] SQ_COLH_* or NULL: no hydrogen recipes */
+  double drawin;               /* sq_prepare_drawin(awgt) */
+  double cbbhsc, cbfhsc;       /* factors on the hydrogen rates */
 } sq_atom_t;
 
 typedef struct sq_params {
@@ -51,8 +56,14 @@ double sq_expin(double x);
 double sq_gaunt(double lam, int n);
 double sq_kramer(double lam, double dev);
 
+/* prepare_Drawin's prefactor for an atom of weight awgt [amu] (atom_mod.f90:1741-1750) */
+double sq_prepare_drawin(double awgt);
+
+/* cup (ncell, ncol) of the electron rates, then with chkind (ncell, ncol) more of
+ * the hydrogen rates; nh1 (ncell) the hydrogen ground-level density, read only
+ * with chkind */
 void or_collisions(const sq_atom_t *at, int ncell, const double *temp, const double *ne, const double *e_kT,
-                   const double *dxi, double *cup);
+                   const double *dxi, const double *nh1, double *cup);
 
 void sq_lineq_no_pivot(double *a, double *b, int n);
 void sq_lineq(double *a, double *b, int n);

@@ -19,7 +19,8 @@ class SqAtom(C.Structure):
                 ("g", C.c_void_p), ("ev", C.c_void_p), ("ion", C.c_void_p),
                 ("ci", C.c_void_p), ("cj", C.c_void_p), ("ckind", C.c_void_p), ("cfac", C.c_void_p),
                 ("fmin", C.c_double), ("cbbesc", C.c_double), ("cbfesc", C.c_double), ("colscale", C.c_double),
-                ("upsilon_floor", C.c_double), ("cut_x", C.c_double), ("bf_cut_rate", C.c_double)]
+                ("upsilon_floor", C.c_double), ("cut_x", C.c_double), ("bf_cut_rate", C.c_double),
+                ("chkind", C.c_void_p), ("drawin", C.c_double), ("cbbhsc", C.c_double), ("cbfhsc", C.c_double)]
 
 
 class SqParams(C.Structure):
@@ -58,7 +59,17 @@ def make_atom(atom: dict):
     for k, d in (("fmin", float(np.float32(1e-6))), ("cbbesc", 1.0), ("cbfesc", 1.0), ("colscale", 1.0),
                  ("upsilon_floor", 0.0), ("cut_x", 70.0), ("bf_cut_rate", 1.0)):
         setattr(s, k, float(atom.get(k, d)))
+    s.chkind = arr("col_hkind", np.int32)
+    s.drawin = prepare_drawin(float(atom["awgt"])) if s.chkind is not None else 0.0
+    s.cbbhsc, s.cbfhsc = float(atom.get("cbbhsc", 1.0)), float(atom.get("cbfhsc", 1.0))
     return s, keep
+
+
+def prepare_drawin(awgt: float) -> float:
+    """prepare_Drawin (atom_mod.f90:1741-1750) for an atom of weight awgt [amu]."""
+    f = lib().sq_prepare_drawin
+    f.restype = C.c_double
+    return f(C.c_double(awgt))
 
 
 def _f64(a):
@@ -77,11 +88,17 @@ def kramer(lam, dev):
     return f(C.c_double(lam), C.c_double(dev))
 
 
-def collision_rates(atom: dict, temp, ne, e_kT, dxi=None):
+def collision_rates(atom: dict, temp, ne, e_kT, dxi=None, nh1=None):
+    """classic_col's upward rates (ncol, ncell): electrons, then with col_hkind
+    (2 ncol rows) hydrogen, whose recipes read nh1."""
     st, keep = make_atom(atom)
-    temp, ne, e_kT, dxi = _f64(temp), _f64(ne), _f64(e_kT), _f64(dxi)
-    cup = np.zeros((st.ncol, temp.size), np.float64)
-    lib().or_collisions(C.byref(st), C.c_int(temp.size), _vp(temp), _vp(ne), _vp(e_kT), _vp(dxi), _vp(cup))
+    temp, ne, e_kT, dxi, nh1 = _f64(temp), _f64(ne), _f64(e_kT), _f64(dxi), _f64(nh1)
+    rows = 2 * st.ncol if st.chkind is not None else st.ncol
+    if st.chkind is not None and nh1 is None:
+        raise ValueError("hydrogen collision recipes need nh1")
+    cup = np.zeros((rows, temp.size), np.float64)
+    lib().or_collisions(C.byref(st), C.c_int(temp.size), _vp(temp), _vp(ne), _vp(e_kT), _vp(dxi), _vp(nh1),
+                        _vp(cup))
     return cup
 
 
@@ -105,7 +122,7 @@ def rate_matrix(atom: dict, inputs: dict, cell: int, cup=None, cswitch: float = 
     ns = np.ascontiguousarray(inputs["nstar"][:, cell], np.float64)
     gij = np.ascontiguousarray(inputs["gamma_ij"][:, cell], np.float32)
     gji = np.ascontiguousarray(inputs["gamma_ji"][:, cell], np.float32)
-    cupc = np.ascontiguousarray(cup[:, cell], np.float64) if cup is not None else np.zeros(max(st.ncol, 1))
+    cupc = np.ascontiguousarray(cup[:, cell], np.float64) if cup is not None else np.zeros(max(2 * st.ncol, 1))
     w = np.zeros(n * n, np.float64)
     e = np.zeros(n, np.float64)
     lib().or_rate_matrix(C.byref(st), C.byref(par), _vp(bl), _vp(ns), C.c_double(float(inputs["totn"][cell])),

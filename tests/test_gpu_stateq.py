@@ -106,6 +106,63 @@ def test_update_fused_collisions(sq, se):
     assert rg["maxerr"] == pytest.approx(ro["maxerr"], rel=1e-10)
 
 
+H_RECIPES = ("drawin", "drawin", "takeda")
+
+
+def test_collision_rates_hydrogen(sq, se):
+    """Drawin and Takeda (atom_mod.f90:1854-1876) beside the electron recipes."""
+    atom, inp = synth.se_config("small", ncell=1024, h_recipes=H_RECIPES)
+    ncol = len(atom["col_i"])
+    dxi = np.full_like(inp["temp"], 0.05)
+    ref = sq.collision_rates(atom, inp["temp"], inp["ne"], inp["e_kT"], dxi, nh1=inp["nh1"])
+    got = se.collision_rates(atom, inp["temp"], inp["ne"], inp["e_kT"], dxi, nh1=inp["nh1"])
+    assert got.shape == ref.shape == (2 * ncol, 1024)
+    assert np.count_nonzero(got[ncol:]) > 0.9 * ncol * 1024
+    np.testing.assert_allclose(got, ref, rtol=1e-12, atol=0)   # device exp
+
+
+@pytest.mark.parametrize("solver", [0, 1, 2])
+def test_update_bitexact_hydrogen(sq, se, solver):
+    atom, inp = synth.se_config("small", ncell=1500, h_recipes=H_RECIPES)
+    cup = sq.collision_rates(atom, inp["temp"], inp["ne"], inp["e_kT"], nh1=inp["nh1"])
+    bo, ro, lo, rc = _oracle_update(sq, atom, inp, cup, solver=solver)
+    assert rc == 0
+    bg, rg, lg = _gpu_update(se, atom, inp, cup=cup, solver=solver)
+    assert np.array_equal(bg, bo) and rg == ro and np.array_equal(lg, lo)
+    # the hydrogen rates move the solution
+    b0, _, _, _ = _oracle_update(sq, dict(atom, col_hkind=None), inp, cup[:len(atom["col_i"])], solver=solver)
+    assert not np.array_equal(b0, bo)
+
+
+def test_update_fused_hydrogen(sq, se):
+    atom, inp = synth.se_config("small", ncell=2048, h_recipes=H_RECIPES)
+    cup = sq.collision_rates(atom, inp["temp"], inp["ne"], inp["e_kT"], nh1=inp["nh1"])
+    bo, ro, lo, rc = _oracle_update(sq, atom, inp, cup)
+    bg, rg, lg = _gpu_update(se, atom, inp, cup=None, nh1=inp["nh1"])
+    np.testing.assert_allclose(bg, bo, rtol=1e-10, atol=0)   # device exp, amplified by the solve
+    assert rg["epos_cell"] == ro["epos_cell"] and rg["epos_level"] == ro["epos_level"]
+
+
+def test_hydrogen_recipe_checks(se):
+    from dispatch_b200 import M3DError
+    atom, inp = synth.se_config("small", ncell=64, h_recipes=H_RECIPES)
+    args = (inp["temp"], inp["ne"], inp["e_kT"])
+    with pytest.raises(M3DError, match="nh1"):
+        se.collision_rates(atom, *args)
+    hk = atom["col_hkind"].copy()
+    bad = dict(atom, col_hkind=np.where(atom["col_fac"] != 0, 2, hk).astype(np.int32))
+    with pytest.raises(M3DError, match="Takeda"):
+        se.collision_rates(bad, *args, nh1=inp["nh1"])
+    hk[0] = 7
+    with pytest.raises(M3DError, match="hydrogen kind"):
+        se.collision_rates(dict(atom, col_hkind=hk), *args, nh1=inp["nh1"])
+    b = inp["b"].copy()
+    with pytest.raises(M3DError, match="nh1"):
+        se.stateq_update(atom, b, inp["nstar"], inp["totn"], inp["e_kT"], inp["gamma_ij"], inp["gamma_ji"],
+                         temp=inp["temp"], ne=inp["ne"])
+    assert np.array_equal(b, inp["b"])
+
+
 def test_update_limiter_sor_floor(sq, se):
     atom, inp = synth.se_config("small", ncell=1024)
     inp = dict(inp)
