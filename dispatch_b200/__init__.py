@@ -32,7 +32,8 @@ EXPORTS = ("m3d_init", "m3d_free", "m3d_last_error", "m3d_version", "m3d_set_str
            "m3d_launch_count", "m3d_weights", "m3d_qlg_init", "m3d_qlg_tables", "m3d_qlg_bot_profile",
            "m3d_line_opacity", "m3d_lte_background", "m3d_work_to_transfer_units", "m3d_formal_solve",
            "m3d_rotate_array", "m3d_upstream_boundary", "m3d_integrate_intensity", "m3d_lte_synthesis",
-           "m3d_profile_enable", "m3d_profile_read", "m3d_rotate_array_noalloc", "m3d_collision_rates",
+           "m3d_profile_enable", "m3d_profile_read", "m3d_rotate_array_noalloc", "m3d_collision_nrows",
+           "m3d_collision_rates",
            "m3d_stateq_update", "m3d_ng_accumulate", "m3d_ng_extrapolate", "m3d_bb_damping", "m3d_bf_opacity",
            "m3d_bb_opacity", "m3d_work_to_transfer_units_split", "m3d_bb_rates", "m3d_bf_rates",
            "m3d_integrate_rates", "m3d_normalize_profiles", "m3d_combine_twins", "m3d_update_eta_mask",

@@ -40,6 +40,15 @@ struct SeAtomDev {
   const int *chkind;           // [ncol] hydrogen recipes, or null: none
   double fmin, cbbesc, cbfesc, colscale, upsilon_floor, cut_x, bf_cut_rate;
   double drawin, cbbhsc, cbfhsc;
+  // gencol's records (atom_mod.f90:2223-2360) and, with records, the matrix
+  // elements that collisions reach: element e is W[el_w[e]], its contributions
+  // el_src[el_off[e] .. el_off[e+1]) in the order the reference adds them, each
+  // (index << 2 | type), type 0/1 a classic pair's upward/downward rate, 2/3 a
+  // record's upward/downward rate
+  int ngrec, ntemp, ch0_hmip, nel;
+  const double *gt, *glnc, *gdc;  // [ntemp], [ngrec * ntemp] x 2
+  const int *gll, *gul, *gkind, *gcoll;
+  const int *el_w, *el_off, *el_src;
 };
 
 struct SeParams {
@@ -50,7 +59,7 @@ struct SeParams {
 struct SeCells {
   int ncell;
   double *b;
-  const double *nstar, *totn, *temp, *ne, *e_kT, *dxi, *nh1;
+  const double *nstar, *totn, *temp, *ne, *e_kT, *dxi, *nh1, *lsaha, *coll;
   const float *gij, *gji;
   const double *cup;  // precomputed collision rates, or null to form them here
 };
@@ -145,6 +154,7 @@ __device__ __forceinline__ SeColCell se_col_cell(double temp, double ne, double 
 // upward collision rates of pair p [1/s], colscale applied: ue by the pair's
 // electron recipe, uh by its hydrogen recipe (0 without one).  The electron mass
 // ame of the hydrogen recipes is a default-real literal (atom_mod.f90:220-222).
+template <bool HYD>
 __device__ __forceinline__ void se_col_rates(const SeAtomDev &A, const SeColCell &w, int p, double &ue,
                                              double &uh) {
   const double sqr3_2pi = (sqrt(3.0) / 2.0) / 3.14159265359;
@@ -179,6 +189,8 @@ __device__ __forceinline__ void se_col_rates(const SeAtomDev &A, const SeColCell
   }
   if (v != 0) v = v * A.colscale;
   ue = v;
+  uh = 0;
+  if (!HYD) return;
   // hydrogen (atom_mod.f90:1854-1876): Takeda for a line without an f value,
   // else Drawin
   const int hkind = A.chkind ? A.chkind[p] : 0;
@@ -206,19 +218,123 @@ __device__ __forceinline__ void se_col_rates(const SeAtomDev &A, const SeColCell
   uh = h;
 }
 
+// ---- gencol (atom_mod.f90:2223-2360) -------------------------------------------
+// hermite_interpolation_single (interpol_mod.f90:558-578): the end values outside
+// the nodes, else BinarySearch8's bracket (op_math_mod.f90:179-199), x[i] < xx <=
+// x[i+1], and hermite_value8 (interpol_mod.f90:149-162)
+__device__ __forceinline__ double se_hermite8(const double *x, const double *y, const double *m, int n,
+                                              double xx) {
+  if (xx <= x[0]) return y[0];
+  if (xx >= x[n - 1]) return y[n - 1];
+  int l = 0, r = n - 1;
+  while (r - l > 1) {
+    const int mid = l + (r - l) / 2;
+    if (x[mid] >= xx) r = mid;
+    else l = mid;
+  }
+  const double h = x[l + 1] - x[l];
+  const double t = (xx - x[l]) / h;
+  const double t2 = t * t, t3 = t2 * t;
+  const double p = 3.0 * t2 - 2.0 * t3;
+  return (1.0 - p) * y[l] + p * y[l + 1] + h * ((t3 - 2.0 * t2 + t) * m[l] + (t3 - t2) * m[l + 1]);
+}
+
+// record r's upward and downward rates [1/s], colscale applied; nll, nul the
+// cell's n* of the record's levels, ncoll its collider's density (UP/DN)
+__device__ __forceinline__ void se_gencol_rates(const SeAtomDev &A, int r, double temp, double ne, double dxi,
+                                                double nh1, double lsaha, double ncoll, double ekt, double nll,
+                                                double nul, double &up, double &dn) {
+  const double PI = 3.14159265359, BK = 1.380662e-16, EM = 9.109534e-28, RB = 5.29177349e-9;
+  const double ERYD = 13.605 * 1.602189e-12;
+  const double c0 = ((ERYD / sqrt(EM)) * PI * (RB * RB)) * sqrt(8.0 / (PI * BK));
+  const int ll = A.gll[r], ul = A.gul[r], kind = A.gkind[r];
+  double dev = A.ev[ul] - A.ev[ll];
+  if (A.ion[ul] > A.ion[ll]) {
+    const int ii = A.ion[ll] * (A.ion[ll] - 1), jj = A.ion[ul] * (A.ion[ul] - 1);
+    dev = dev - dxi * 0.5 * (double)(jj - ii);
+  }
+  double nji;
+  if (nll > 0) {
+    nji = nul / nll;
+  } else {
+    const double tns = -(dev * ekt) + (double)(A.ion[ul] - A.ion[ll]) * lsaha;
+    nji = A.g[ul] / A.g[ll] * exp(tns);
+  }
+  const double stg = sqrt(temp);
+  const size_t o = (size_t)r * A.ntemp;
+  const double ct = exp(se_hermite8(A.gt, A.glnc + o, A.gdc + o, A.ntemp, temp));
+  double u = 0, d = 0;
+  switch (kind) {
+    case 1:  // OHM
+      d = c0 / A.g[ul] * ct * ne / stg;
+      u = d * nji;
+      break;
+    case 2:  // CE
+      d = A.g[ll] / A.g[ul] * ct * ne * stg;
+      d = d * A.cbbesc;
+      u = d * nji;
+      break;
+    case 3:  // CH
+      d = ct * nh1;
+      d = d * A.cbbhsc;
+      u = d * nji;
+      break;
+    case 4:  // CHI
+      u = ct * nh1;
+      u = u * A.cbfhsc;
+      d = u / nji;
+      break;
+    case 5:  // CI
+      u = ct * ne * stg * exp(-(A.ev[ul] - A.ev[ll]) * ekt);
+      u = u * A.cbfesc;
+      d = u / nji;
+      break;
+    case 6:  // CH0; 0.754 is a default-real literal
+      u = ct * nh1;
+      if (A.ch0_hmip) u = u * exp(-(double)0.754f * ekt);
+      u = u * A.cbfhsc;
+      d = u / nji;
+      break;
+    case 7:  // UP
+      u = ct * ncoll;
+      d = u / nji;
+      break;
+    case 8:  // DN
+      d = ct * ncoll;
+      u = d * nji;
+      break;
+    default:
+      break;
+  }
+  up = u * A.colscale;
+  dn = d * A.colscale;
+}
+
 // cup[cell + ncell*p] the electron rates; with hydrogen recipes
 // cup[cell + ncell*(ncol + p)] the hydrogen ones.  One thread per cell.
-__global__ void k_collision_rates(SeAtomDev A, int ncell, const double *__restrict__ temp,
-                                  const double *__restrict__ ne, const double *__restrict__ ekt,
-                                  const double *__restrict__ dxi, const double *__restrict__ nh1,
-                                  double *__restrict__ cup) {
+// cup[cell + ncell*(r0 + r)] and cup[cell + ncell*(r0 + ngrec + r)] record r's
+// upward and downward rates, r0 = ncol (x2 with hydrogen recipes).
+__global__ void k_collision_rates(SeAtomDev A, SeCells C, double *__restrict__ cup) {
+  const int ncell = C.ncell;
+  const int r0 = A.chkind ? 2 * A.ncol : A.ncol;
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += gridDim.x * blockDim.x) {
-    const SeColCell w = se_col_cell(temp[c], ne[c], ekt[c], dxi ? dxi[c] : 0.0, nh1 ? nh1[c] : 0.0);
+    const double dxi = C.dxi ? C.dxi[c] : 0.0, nh1 = C.nh1 ? C.nh1[c] : 0.0;
+    const SeColCell w = se_col_cell(C.temp[c], C.ne[c], C.e_kT[c], dxi, nh1);
     for (int p = 0; p < A.ncol; p++) {
       double ue, uh;
-      se_col_rates(A, w, p, ue, uh);
+      se_col_rates<true>(A, w, p, ue, uh);
       cup[(size_t)c + (size_t)ncell * p] = ue;
       if (A.chkind) cup[(size_t)c + (size_t)ncell * (A.ncol + p)] = uh;
+    }
+    for (int r = 0; r < A.ngrec; r++) {
+      const int k = A.gcoll ? A.gcoll[r] : -1;
+      const double nc = k >= 0 ? C.coll[(size_t)c + (size_t)ncell * k] : 0.0;
+      double up, dn;
+      se_gencol_rates(A, r, C.temp[c], C.ne[c], dxi, nh1, C.lsaha ? C.lsaha[c] : 0.0, nc, C.e_kT[c],
+                      C.nstar[(size_t)c + (size_t)ncell * A.gll[r]], C.nstar[(size_t)c + (size_t)ncell * A.gul[r]],
+                      up, dn);
+      cup[(size_t)c + (size_t)ncell * (r0 + r)] = up;
+      cup[(size_t)c + (size_t)ncell * (r0 + A.ngrec + r)] = dn;
     }
   }
 }
@@ -399,6 +515,10 @@ __device__ __forceinline__ void se_solve_partial(double *W, double *e, int n, in
 __host__ __device__ inline size_t se_warp_doubles(int n) { return (size_t)n * n + 4 * (size_t)n + (size_t)(n + 1) / 2; }
 
 // update_populations over all cells: warps stride over the cells in ascending order
+// CM 0: collision rates read from C.cup (or none); 1: formed here, electron
+// recipes only; 2: formed here, any recipes and records.  The host picks the
+// least general form, which keeps the common ones' register use down.
+template <int CM>
 __global__ void k_stateq_update(SeAtomDev A, SeParams P, SeCells C, SeWarpBest *__restrict__ wbest,
                                 double *__restrict__ lvl_val, long long *__restrict__ lvl_cell,
                                 unsigned long long *__restrict__ counts, long long *__restrict__ nonfinite) {
@@ -467,33 +587,79 @@ __global__ void k_stateq_update(SeAtomDev A, SeParams P, SeCells C, SeWarpBest *
       }
       __syncwarp();
     }
-    // collisions times cswitch; the pairs are distinct.  c starts at zero and
-    // takes each nonzero rate, the electron one first (classic_col :1846-1876).
-    if (P.cswitch > 0 && A.ncol > 0) {
+    // collisions times cswitch (:806-811).  c starts at zero and takes each
+    // nonzero classic rate, the electron one first (classic_col :1846-1876), then
+    // every record's rates in order (gencol :2350-2351).  Without records the
+    // pairs are distinct and each lane takes whole pairs; with records each lane
+    // sums whole matrix elements.
+    if (P.cswitch > 0 && (A.ncol > 0 || A.nel > 0)) {
       SeColCell cw{0, 0, 0, 0, 0, 0, 0, 0};
-      if (!C.cup) cw = se_col_cell(C.temp[c], C.ne[c], ekt, C.dxi ? C.dxi[c] : 0.0, C.nh1 ? C.nh1[c] : 0.0);
-      for (int p = lane; p < A.ncol; p += 32) {
-        double ue, uh = 0;
-        if (C.cup) {
+      double temp = 0, lsaha = 0;
+      if (CM != 0) {
+        temp = C.temp[c];
+        cw = se_col_cell(temp, C.ne[c], ekt, C.dxi ? C.dxi[c] : 0.0, C.nh1 ? C.nh1[c] : 0.0);
+        if (CM == 2) lsaha = C.lsaha ? C.lsaha[c] : 0.0;
+      }
+      auto pair_rates = [&](int p, double &ue, double &uh) {
+        if (CM == 0) {
           ue = C.cup[(size_t)c + (size_t)ncell * p];
-          if (A.chkind) uh = C.cup[(size_t)c + (size_t)ncell * (A.ncol + p)];
+          uh = A.chkind ? C.cup[(size_t)c + (size_t)ncell * (A.ncol + p)] : 0.0;
         } else {
-          se_col_rates(A, cw, p, ue, uh);
+          se_col_rates<CM == 2>(A, cw, p, ue, uh);
         }
-        if (ue == 0 && uh == 0) continue;
-        const int i = A.ci[p], j = A.cj[p];
-        const double nij = ns[i] / ns[j];
-        double cu = 0, cd = 0;
-        if (ue != 0) {
-          cu = cu + ue;
-          cd = cd + ue * nij;
+      };
+      if (CM != 1 && A.nel > 0) {
+        const int r0 = A.chkind ? 2 * A.ncol : A.ncol;
+        for (int e = lane; e < A.nel; e += 32) {
+          double cv = 0;
+          for (int k = A.el_off[e]; k < A.el_off[e + 1]; k++) {
+            const int code = A.el_src[k], idx = code >> 2, type = code & 3;
+            if (type < 2) {
+              double ue, uh;
+              pair_rates(idx, ue, uh);
+              if (type == 0) {
+                if (ue != 0) cv = cv + ue;
+                if (uh != 0) cv = cv + uh;
+              } else {
+                const double nij = ns[A.ci[idx]] / ns[A.cj[idx]];
+                if (ue != 0) cv = cv + ue * nij;
+                if (uh != 0) cv = cv + uh * nij;
+              }
+            } else {
+              double up, dn;
+              if (CM == 0) {
+                up = C.cup[(size_t)c + (size_t)ncell * (r0 + idx)];
+                dn = C.cup[(size_t)c + (size_t)ncell * (r0 + A.ngrec + idx)];
+              } else {
+                const int kc = A.gcoll ? A.gcoll[idx] : -1;
+                const double nc = kc >= 0 ? C.coll[(size_t)c + (size_t)ncell * kc] : 0.0;
+                se_gencol_rates(A, idx, temp, cw.ne, cw.dxi, cw.nh1, lsaha, nc, ekt, ns[A.gll[idx]],
+                                ns[A.gul[idx]], up, dn);
+              }
+              cv = cv + (type == 2 ? up : dn);
+            }
+          }
+          W[A.el_w[e]] = W[A.el_w[e]] + cv * P.cswitch;
         }
-        if (uh != 0) {
-          cu = cu + uh;
-          cd = cd + uh * nij;
+      } else {
+        for (int p = lane; p < A.ncol; p += 32) {
+          double ue, uh;
+          pair_rates(p, ue, uh);
+          if (ue == 0 && uh == 0) continue;
+          const int i = A.ci[p], j = A.cj[p];
+          const double nij = ns[i] / ns[j];
+          double cu = 0, cd = 0;
+          if (ue != 0) {
+            cu = cu + ue;
+            cd = cd + ue * nij;
+          }
+          if (uh != 0) {
+            cu = cu + uh;
+            cd = cd + uh * nij;
+          }
+          W[j + n * i] = W[j + n * i] + cu * P.cswitch;
+          W[i + n * j] = W[i + n * j] + cd * P.cswitch;
         }
-        W[j + n * i] = W[j + n * i] + cu * P.cswitch;
-        W[i + n * j] = W[i + n * j] + cd * P.cswitch;
       }
       __syncwarp();
     }

@@ -29,6 +29,8 @@ from . import DEVICE_PTRS, M3DError, check, init, lib, order_after_torch, ptr
 LINEQ_NO_PIVOT, LINEQ, LU_PARTIAL = 0, 1, 2
 COL_REGEMORTER, COL_SEATON = 1, 2
 COLH_DRAWIN, COLH_TAKEDA = 1, 2
+# gencol's record kinds (atom_mod.f90:2288-2344), by the atom file's keys
+GENCOL_KINDS = {"OHM": 1, "OHMEGA": 1, "CE": 2, "CH": 3, "CHI": 4, "CI": 5, "CH0": 6, "UP": 7, "DN": 8}
 ENONFINITE = 5
 
 
@@ -41,7 +43,23 @@ class Atom(C.Structure):
                 ("col_i", C.c_void_p), ("col_j", C.c_void_p), ("col_kind", C.c_void_p), ("col_fac", C.c_void_p),
                 ("fmin", C.c_double), ("cbbesc", C.c_double), ("cbfesc", C.c_double), ("colscale", C.c_double),
                 ("upsilon_floor", C.c_double), ("cut_x", C.c_double), ("bf_cut_rate", C.c_double),
-                ("col_hkind", C.c_void_p), ("drawin", C.c_double), ("cbbhsc", C.c_double), ("cbfhsc", C.c_double)]
+                ("col_hkind", C.c_void_p), ("drawin", C.c_double), ("cbbhsc", C.c_double), ("cbfhsc", C.c_double),
+                ("gencol", C.c_void_p)]
+
+
+class Gencol(C.Structure):
+    """m3d_gencol_t."""
+
+    _fields_ = [("nrec", C.c_int), ("ntemp", C.c_int), ("tgrid", C.c_void_p), ("lnc", C.c_void_p),
+                ("dlnc", C.c_void_p), ("ll", C.c_void_p), ("ul", C.c_void_p), ("kind", C.c_void_p),
+                ("collider", C.c_void_p), ("ch0_hmip", C.c_int), ("pad", C.c_int)]
+
+
+class ColCells(C.Structure):
+    """m3d_col_cells_t."""
+
+    _fields_ = [("temp", C.c_void_p), ("ne", C.c_void_p), ("dxi", C.c_void_p), ("nh1", C.c_void_p),
+                ("lsaha", C.c_void_p), ("colliders", C.c_void_p), ("ncollider", C.c_int), ("pad", C.c_int)]
 
 
 class SeParams(C.Structure):
@@ -75,13 +93,15 @@ def make_atom(atom: dict) -> tuple[Atom, list]:
     """The m3d_atom_t of an atom dict, and the arrays it points into."""
     keep = []
 
-    def arr(key, dtype):
-        v = atom.get(key)
+    def arr_of(v, dtype):
         if v is None:
             return None
         a = np.ascontiguousarray(v, dtype)
         keep.append(a)
         return C.c_void_p(a.ctypes.data)
+
+    def arr(key, dtype):
+        return arr_of(atom.get(key), dtype)
 
     s = Atom()
     s.nlevel = int(atom["nlevel"])
@@ -101,6 +121,20 @@ def make_atom(atom: dict) -> tuple[Atom, list]:
     s.col_hkind = arr("col_hkind", np.int32)
     s.drawin = prepare_drawin(float(atom["awgt"])) if s.col_hkind is not None else 0.0
     s.cbbhsc, s.cbfhsc = float(atom.get("cbbhsc", 1.0)), float(atom.get("cbfhsc", 1.0))
+    gc = atom.get("gencol")
+    if gc is not None and len(gc["ll"]) > 0:
+        g = Gencol()
+        lnc = np.ascontiguousarray(gc["lnc"], np.float64)
+        keep.append(lnc)
+        g.nrec, g.ntemp = lnc.shape
+        g.lnc = C.c_void_p(lnc.ctypes.data)
+        g.tgrid = arr_of(gc["tgrid"], np.float64)
+        g.dlnc = arr_of(gc.get("dlnc"), np.float64)
+        g.ll, g.ul, g.kind = arr_of(gc["ll"], np.int32), arr_of(gc["ul"], np.int32), arr_of(gc["kind"], np.int32)
+        g.collider = arr_of(gc.get("collider"), np.int32)
+        g.ch0_hmip = int(bool(gc.get("ch0_hmip", False)))
+        keep.append(g)
+        s.gencol = C.c_void_p(C.addressof(g))
     return s, keep
 
 
@@ -196,25 +230,45 @@ def _f32(a):
     return np.ascontiguousarray(a, np.float32)
 
 
-def collision_rates(atom: dict, temp, ne, e_kT, dxi=None, nh1=None, out=None):
-    """classic_col's upward rates [1/s], colscale applied: (ncol, ncell) of the
-    electron recipes, then, when the atom has col_hkind, ncol more rows of the
-    hydrogen recipes, which read nh1 (the neutral hydrogen ground-level density)."""
+def _cells(temp, ne, dxi, nh1, lsaha, colliders):
+    """The m3d_col_cells_t of the per-cell collision inputs, and the arrays it points into."""
+    temp, ne, dxi, nh1, lsaha, colliders = (_f64(a) for a in (temp, ne, dxi, nh1, lsaha, colliders))
+    c = ColCells()
+    c.temp, c.ne, c.dxi, c.nh1, c.lsaha, c.colliders = (ptr(a) for a in (temp, ne, dxi, nh1, lsaha, colliders))
+    c.ncollider = int(colliders.shape[0]) if colliders is not None else 0
+    return c, [temp, ne, dxi, nh1, lsaha, colliders]
+
+
+def collision_nrows(atom: dict) -> int:
+    """Rows of a cup buffer: ncol, ncol more with col_hkind, 2 nrec with gencol records."""
+    ncol = len(atom["col_i"]) if atom.get("col_i") is not None else 0
+    gc = atom.get("gencol")
+    return ncol * (2 if atom.get("col_hkind") is not None else 1) + (2 * len(gc["ll"]) if gc is not None else 0)
+
+
+def collision_rates(atom: dict, temp, ne, e_kT, dxi=None, nh1=None, nstar=None, lsaha=None, colliders=None,
+                    out=None):
+    """collision_rates' rates [1/s], colscale applied, (collision_nrows, ncell):
+    classic_col's upward electron rates, with col_hkind its hydrogen ones (which
+    read nh1, the neutral hydrogen ground-level density), then with gencol
+    records their upward and downward rates (which read nstar (nlevel, ncell),
+    lsaha and, for UP/DN records, colliders (ncollider, ncell))."""
     init()
     st, keep = make_atom(atom)
-    temp, ne, e_kT, dxi, nh1 = _f64(temp), _f64(ne), _f64(e_kT), _f64(dxi), _f64(nh1)
-    ncell = int(temp.shape[-1])
-    rows = 2 * st.ncol if st.col_hkind is not None else st.ncol
+    cells, keep2 = _cells(temp, ne, dxi, nh1, lsaha, colliders)
+    e_kT, nstar = _f64(e_kT), _f64(nstar)
+    ncell = int(keep2[0].shape[-1])
     if out is None:
-        out = np.zeros((rows, ncell), np.float64)
-    check(lib().m3d_collision_rates(C.byref(st), C.c_int(ncell), ptr(temp), ptr(ne), ptr(e_kT), ptr(dxi),
-                                    ptr(nh1), ptr(out), C.c_uint(_flags(temp, out))), "m3d_collision_rates")
+        out = np.zeros((collision_nrows(atom), ncell), np.float64)
+    rc = lib().m3d_collision_rates(C.byref(st), C.c_int(ncell), ptr(e_kT), ptr(nstar), C.byref(cells), ptr(out),
+                                   C.c_uint(_flags(keep2[0], out)))
+    check(rc, "m3d_collision_rates")
     return out
 
 
 def stateq_update(atom: dict, b, nstar, totn, e_kT, gamma_ij, gamma_ji, temp=None, ne=None, dxi=None, cup=None,
-                  nh1=None, solver: int = LINEQ_NO_PIVOT, max_update: float = 1e2, sor_w: float = 1.0,
-                  min_pop_frac: float = 1e-30, conv_pop_floor: float = 0.0, tmax_update: float = 1e7,
+                  nh1=None, lsaha=None, colliders=None, solver: int = LINEQ_NO_PIVOT, max_update: float = 1e2,
+                  sor_w: float = 1.0, min_pop_frac: float = 1e-30, conv_pop_floor: float = 0.0, tmax_update: float = 1e7,
                   cswitch: float = 1.0) -> tuple[dict, np.ndarray]:
     """update_populations over all cells; b (nlevel, ncell) float64 is updated in place.
 
@@ -227,15 +281,15 @@ def stateq_update(atom: dict, b, nstar, totn, e_kT, gamma_ij, gamma_ji, temp=Non
     if isinstance(b, np.ndarray) and (b.dtype != np.float64 or not b.flags.c_contiguous):
         raise M3DError("b must be a C-contiguous float64 array (it is updated in place)")
     nstar, totn, e_kT = _f64(nstar), _f64(totn), _f64(e_kT)
-    temp, ne, dxi, cup, nh1 = _f64(temp), _f64(ne), _f64(dxi), _f64(cup), _f64(nh1)
+    cup = _f64(cup)
+    cells, keep2 = _cells(temp, ne, dxi, nh1, lsaha, colliders)
     gamma_ij, gamma_ji = _f32(gamma_ij), _f32(gamma_ji)
     ncell = int(totn.shape[-1])
     par = SeParams(max_update, sor_w, min_pop_frac, conv_pop_floor, tmax_update, cswitch, int(solver), 0)
     res = SeResult()
     lvlerr = np.zeros(st.nlevel, np.float64)
     rc = lib().m3d_stateq_update(C.byref(st), C.byref(par), C.c_int(ncell), ptr(b), ptr(nstar), ptr(totn),
-                                 ptr(temp), ptr(ne), ptr(e_kT), ptr(dxi), ptr(nh1), ptr(gamma_ij), ptr(gamma_ji),
-                                 ptr(cup),
+                                 ptr(e_kT), C.byref(cells), ptr(gamma_ij), ptr(gamma_ji), ptr(cup),
                                  C.c_void_p(lvlerr.ctypes.data), C.byref(res),
                                  C.c_uint(_flags(b, nstar, totn, e_kT)))
     out = res.as_dict()

@@ -368,7 +368,7 @@ RYDV = 13.605
 
 
 def model_atom(seed: int = 2, nbound: int = 20, nline: int = 60, e_max: float = 7.0, e_ion: float = 7.9,
-               logf=(-4.0, 0.0), h_recipes=None, awgt: float = 40.08) -> dict:
+               logf=(-4.0, 0.0), h_recipes=None, awgt: float = 40.08, gencol: bool = False) -> dict:
     """A seeded model atom: nbound levels of the neutral (ground at 0 eV, the rest
     uniform in [0, e_max]) plus the ground level of the ion at e_ion; nline lines
     between distinct random bound pairs with log f uniform in logf; one continuum
@@ -379,7 +379,9 @@ def model_atom(seed: int = 2, nbound: int = 20, nline: int = 60, e_max: float = 
     the collision recipe) for odd ones.  h_recipes = (h_excitation, h_ionisation,
     h_forbidden), e.g. ('drawin', 'drawin', 'takeda'), adds the hydrogen recipes
     of every pair (col_hkind): Takeda for a bound pair without a line, else
-    Drawin.  awgt: the atom's weight [amu].  Indices are 0-based."""
+    Drawin.  awgt: the atom's weight [amu].  gencol adds tabulated collision
+    records of every kind (model_gencol); classic_col then leaves out the recipes
+    the records' data replaces, as the reference does.  Indices are 0-based."""
     rng = np.random.default_rng(seed + 2000)
     ev = np.concatenate([[0.0], np.sort(rng.uniform(0.0, e_max, nbound - 1)), [e_ion]])
     g = np.concatenate([rng.choice([1.0, 3.0, 5.0, 7.0, 9.0], nbound), [1.0]])
@@ -409,6 +411,18 @@ def model_atom(seed: int = 2, nbound: int = 20, nline: int = 60, e_max: float = 
                 col_j.append(j)
                 col_kind.append(1)
                 col_fac.append(fpair.get((i, j), 0.0))
+    gc, hkind = None, None
+    if gencol:
+        from .stateq import classic_pairs
+        gc, ecol, hcol = model_gencol(n, nbound, seed)
+        cdata = np.zeros((n, n), np.float32)
+        cdata[col_i, col_j] = col_fac
+        cp = classic_pairs(ion, np.where(ion == 1, nbound, -1), cdata, ecol=ecol, hcol=hcol,
+                           **dict(zip(("h_excitation", "h_ionisation", "h_forbidden"), h_recipes or ("", "", ""))))
+        col_i, col_j, col_kind, col_fac = cp["col_i"], cp["col_j"], cp["col_kind"], cp["col_fac"]
+        hkind = cp["col_hkind"]
+    else:
+        hkind = _hydrogen_kinds(ion, col_i, col_j, col_fac, h_recipes)
     return {"nlevel": n, "g": g, "ev": ev, "ion": ion,
             "ti": np.array(ti, np.int32), "tj": np.array(tj, np.int32), "nline": len(lines),
             "Aji": aji, "active": None, "line_f": f,
@@ -416,7 +430,44 @@ def model_atom(seed: int = 2, nbound: int = 20, nline: int = 60, e_max: float = 
             "col_kind": np.array(col_kind, np.int32), "col_fac": np.array(col_fac, np.float32),
             "fmin": float(np.float32(1e-6)), "cbbesc": 1.0, "cbfesc": 1.0, "colscale": 1.0,
             "upsilon_floor": 0.0, "cut_x": 70.0, "bf_cut_rate": 1.0, "awgt": float(awgt),
-            "col_hkind": _hydrogen_kinds(ion, col_i, col_j, col_fac, h_recipes)}
+            "col_hkind": hkind, "gencol": gc}
+
+
+def model_gencol(n: int, nbound: int, seed: int = 2, ntemp: int = 9):
+    """Tabulated collision records for model_atom's levels (n = nbound + 1, the last
+    the ion): every kind of record, two records on one level pair, one with its
+    levels reversed, tables with a flat stretch and a turning point, on ntemp nodes
+    from 2500 to 12000 K.  Returns (gencol dict, ecol, hcol): ecol / hcol mark the
+    pairs whose electron / hydrogen rates the records supply."""
+    rng = np.random.default_rng(seed + 5000)
+    ion_lv = n - 1
+    recs = [("CE", 0, 1), ("CE", 2, 5), ("CE", 3, 4), ("OHM", 4, 9), ("OHM", 8, 3), ("CH", 0, 1), ("CH", 5, 6),
+            ("CI", 0, ion_lv), ("CI", 3, ion_lv), ("CHI", 1, ion_lv), ("CHI", 0, ion_lv), ("CH0", 2, ion_lv),
+            ("UP", 2, 3), ("DN", 10 % nbound, 12 % nbound), ("NONE", 11 % nbound, 13 % nbound), ("CE", 0, 1)]
+    recs = [r for r in recs if r[1] != r[2]]
+    base = {"CE": -23.0, "OHM": -3.0, "CH": -31.0, "CI": -25.0, "CHI": -31.0, "CH0": -27.0, "UP": -29.0,
+            "DN": -29.0, "NONE": -29.0}
+    kinds = {"CE": 2, "OHM": 1, "CH": 3, "CHI": 4, "CI": 5, "CH0": 6, "UP": 7, "DN": 8, "NONE": 0}
+    tgrid = np.geomspace(2500.0, 12000.0, ntemp)
+    x = np.log(tgrid / 5000.0)
+    lnc = np.zeros((len(recs), ntemp))
+    for r, (key, _, _) in enumerate(recs):
+        lnc[r] = base[key] + rng.uniform(0.2, 1.5) * x + 0.1 * np.sin(rng.uniform(1.0, 4.0) * x + rng.uniform(0, 6))
+    lnc[1, 3:5] = lnc[1, 3]                # a flat stretch: zero slopes there
+    lnc[2] = base["CE"] - 0.8 * x**2       # a turning point
+    ecol = np.zeros((n, n), bool)
+    hcol = np.zeros((n, n), bool)
+    for key, l, u in recs:
+        lo, hi = min(l, u), max(l, u)
+        if key in ("CE", "CI", "OHM"):
+            ecol[lo, hi] = True
+        elif key in ("CH", "CHI", "CH0"):
+            hcol[lo, hi] = True
+    gc = {"tgrid": tgrid, "lnc": lnc, "ll": np.array([r[1] for r in recs], np.int32),
+          "ul": np.array([r[2] for r in recs], np.int32), "kind": np.array([kinds[r[0]] for r in recs], np.int32),
+          "collider": np.array([0 if r[0] == "UP" else 1 if r[0] == "DN" else -1 for r in recs], np.int32),
+          "ch0_hmip": True}
+    return gc, ecol, hcol
 
 
 def _hydrogen_kinds(ion, col_i, col_j, col_fac, h_recipes):
@@ -498,17 +549,25 @@ def se_inputs(atom: dict, temp, ne, nH, seed: int = 2, dilution=None, perturb: f
     b = np.exp(perturb * rng.standard_normal((atom["nlevel"], ncell))) if perturb > 0 else np.ones((atom["nlevel"], ncell))
     return {"temp": temp, "ne": ne, "e_kT": e_kT, "nstar": np.ascontiguousarray(nstar),
             "totn": np.ascontiguousarray(totn), "b": np.ascontiguousarray(b), "gamma_ij": gij, "gamma_ji": gji,
-            "nh1": hydrogen_ground(nH, ne)}
+            "nh1": hydrogen_ground(nH, ne), "lsaha": lsaha(temp, ne),
+            "colliders": np.ascontiguousarray(np.stack([0.1 * nH, 1e-3 * nH]))}
+
+
+def lsaha(temp, ne):
+    """comp%lsaha (composition_mod.f90:2423): ln(2 (2 pi m_e k / h^2)^(3/2) T^(3/2) / ne)."""
+    temp = np.asarray(temp, np.float64)
+    op_saha_const = (2 * math.pi * EM * BK / HH**2) ** 1.5
+    return np.log(2 * op_saha_const * temp * np.sqrt(temp)) - np.log(np.asarray(ne, np.float64))
 
 
 def se_config(kind: str = "small", seed: int | None = None, ncell: int | None = None, lte: bool = False,
-              nbound: int = 20, nline: int = 60, h_recipes=None) -> tuple:
+              nbound: int = 20, nline: int = 60, h_recipes=None, gencol: bool = False) -> tuple:
     """(atom, inputs) of an SE case.  'c2': the 120^3 cube of seed 2 and the
     20-level atom (a radiation field diluted upwards, W = exp(-3 z/nz));
     'small': ncell cells (default 2048) drawn from a 16^3 cube with W uniform
     in [0.05, 1]; lte: W = 1.  nbound/nline: the atom's bound levels and lines
     (60/180 for the larger atom of the batched configuration); h_recipes: the
-    hydrogen collision recipes of model_atom."""
+    hydrogen collision recipes of model_atom; gencol: its tabulated records."""
     if kind == "c2":
         seed = 2 if seed is None else seed
         cube = cube_atmosphere(seed, 120, 120, 120)
@@ -520,7 +579,7 @@ def se_config(kind: str = "small", seed: int | None = None, ncell: int | None = 
         W = np.random.default_rng(seed + 4000).uniform(0.05, 1.0, 16**3)
     else:
         raise ValueError(kind)
-    atom = model_atom(seed, nbound=nbound, nline=nline, h_recipes=h_recipes)
+    atom = model_atom(seed, nbound=nbound, nline=nline, h_recipes=h_recipes, gencol=gencol)
     temp, ne, nH = cube["temp"].ravel(), cube["ne"].ravel(), cube["nH"].ravel()
     W = np.asarray(W).ravel()
     if ncell is not None:

@@ -400,7 +400,8 @@ int m3d_lte_synthesis(const m3d_atmos_t *atm, int nf, const double *nu, const do
  * Level and transition indices are 0-based (the reference's minus one).  Per-cell
  * arrays keep the cell index fastest: b(cell, level) at b[cell + ncell*level], as
  * adata%b(x,y,z,level) with cell = x + nx*(y + ny*z).  The atom tables are host
- * memory whatever the flags; M3D_DEVICE_PTRS applies to the per-cell arrays. */
+ * memory whatever the flags; M3D_DEVICE_PTRS applies to the per-cell arrays, those an
+ * m3d_col_cells_t points to included (the struct itself is host memory). */
 #define M3D_SE_LINEQ_NO_PIVOT 0 /* lse_solver='lineq_no_pivot' (default; 'eqsyst' rounds identically) */
 #define M3D_SE_LINEQ 1          /* lse_solver='lineq': full pivoting */
 #define M3D_SE_LU_PARTIAL 2     /* LU with partial (row) pivoting */
@@ -409,16 +410,41 @@ int m3d_lte_synthesis(const m3d_atmos_t *atm, int nf, const double *nu, const do
 #define M3D_COLH_DRAWIN 1       /* h_excitation / h_ionisation='drawin' (atom_mod.f90:1861-1871) */
 #define M3D_COLH_TAKEDA 2       /* h_forbidden='takeda', a pair without a line (atom_mod.f90:1856-1860) */
 
+/* gencol's record kinds (atom_mod.f90:2288-2344) */
+#define M3D_GENCOL_NONE 0       /* a named collider the composition lacks: no rate */
+#define M3D_GENCOL_OHM 1        /* 'OHM', 'OHMEGA': electrons on positive ions, a collision strength */
+#define M3D_GENCOL_CE 2         /* 'CE': electron excitation of neutrals */
+#define M3D_GENCOL_CH 3         /* 'CH': bound-bound with neutral hydrogen, a downward rate */
+#define M3D_GENCOL_CHI 4        /* 'CHI': bound-free with neutral hydrogen, an upward rate */
+#define M3D_GENCOL_CI 5         /* 'CI': electron ionisation */
+#define M3D_GENCOL_CH0 6        /* 'CH0': charge transfer with H-, an upward rate */
+#define M3D_GENCOL_UP 7         /* 'UP' + a collider's name: an upward rate */
+#define M3D_GENCOL_DN 8         /* 'DN' + a collider's name: a downward rate */
+
+/* The tabulated collision records of an atom file (coll_type, atom_mod.f90:180-191,
+ * read at :1412-1530): ln of the rate coefficient at the temperature nodes, which
+ * gencol (:2223-2360) interpolates in T by cubic Hermite.  FOSC records fill col_fac
+ * instead and are not records here. */
+typedef struct m3d_gencol {
+  int nrec, ntemp;             /* records, temperature nodes (>= 2) */
+  const double *tgrid;         /* (ntemp) ascending [K] */
+  const double *lnc;           /* (nrec, ntemp): lnc[rec*ntemp + k], ln of the table values */
+  const double *dlnc;          /* same layout: node slopes, or NULL for hermite_derivative's (pchip_slopes8) */
+  const int *ll, *ul;          /* (nrec) lower and upper level of the record */
+  const int *kind;             /* (nrec) M3D_GENCOL_* */
+  const int *collider;         /* (nrec) row of m3d_col_cells_t.colliders for UP/DN, or NULL */
+  int ch0_hmip, pad;           /* CH0 rates times exp(-0.754 eV / kT) */
+} m3d_gencol_t;
+
 /* The model atom (atom_type, atom_mod.f90:120-160).  Transitions 0..nline-1 are the
  * lines, nline..nrad-1 the continua.  Collision pairs are the (i < j) pairs that
  * classic_col fills with a recipe, each pair at most once: col_kind its electron
- * recipe (0 none), col_hkind its hydrogen one (NULL or 0 none).  With hydrogen
- * recipes the per-cell neutral hydrogen ground-level density nh1 is needed and a
- * precomputed cup holds 2 ncol rows: the electron rates, then the hydrogen ones. */
+ * recipe (0 none), col_hkind its hydrogen one (NULL or 0 none).  gencol adds the
+ * atom file's records after them. */
 typedef struct m3d_atom {
   int nlevel;                  /* 1..64 */
   int nrad, nline;             /* transitions, of which lines */
-  int ncol;                    /* electron-collision pairs */
+  int ncol;                    /* classic_col pairs */
   const int *trans_i, *trans_j;   /* (nrad) lower, upper level */
   const unsigned char *active;    /* (nrad) trans%active, or NULL for all */
   const double *Aji;              /* (nrad) line Einstein A [1/s]; the cut rate of a line */
@@ -432,7 +458,24 @@ typedef struct m3d_atom {
   const int *col_hkind;           /* (ncol) M3D_COLH_*, or NULL for electron recipes only */
   double drawin;                  /* prepare_Drawin's prefactor for the atom's weight (atom_mod.f90:1741-1750) */
   double cbbhsc, cbfhsc;          /* factors on the bound-bound and bound-free hydrogen rates, 1 and 1 */
+  const m3d_gencol_t *gencol;     /* the atom file's collision records, or NULL */
 } m3d_atom_t;
+
+/* The per-cell inputs of the collision rates (collision_rates, atom_mod.f90:918-930),
+ * each (ncell) unless stated.  A pointer the atom's recipes do not read may be NULL. */
+typedef struct m3d_col_cells {
+  const double *temp;          /* [K]; also the tmax_update filter of m3d_stateq_update */
+  const double *ne;            /* electron density */
+  const double *dxi;           /* ionisation-energy lowering [eV], or NULL for 0 */
+  const double *nh1;           /* neutral hydrogen ground level: hydrogen recipes, CH, CHI, CH0 */
+  const double *lsaha;         /* comp%lsaha: gencol's n_ul/n_ll where n*_ll = 0 */
+  const double *colliders;     /* (ncollider, ncell): the colliders of UP/DN records */
+  int ncollider, pad;
+} m3d_col_cells_t;
+
+/* Rows of a cup buffer for the atom: ncol electron rates, ncol hydrogen rates with
+ * col_hkind, then 2 nrec for gencol's records (upward, then downward). */
+int m3d_collision_nrows(const m3d_atom_t *atom);
 
 typedef struct m3d_se_params {
   double max_update;     /* 100 */
@@ -454,26 +497,30 @@ typedef struct m3d_se_result {
   long long nonfinite_cell; /* first cell whose solution was not finite, -1 if none */
 } m3d_se_result_t;
 
-/* classic_col's electron rates (atom_mod.f90:1758-1850): cup (ncell, ncol) [1/s],
- * upward, colscale applied; the downward rate is cup * n*_i/n*_j.  dxi may be NULL (0). */
-int m3d_collision_rates(const m3d_atom_t *atom, int ncell, const double *temp, const double *ne,
-                        const double *e_kT, const double *dxi, const double *nh1, double *cup, unsigned flags);
+/* collision_rates (atom_mod.f90:918-930) of every cell: cup (ncell, m3d_collision_nrows)
+ * [1/s], colscale applied.  Rows 0..ncol-1 the upward electron rates of classic_col
+ * (:1758-1850), then with col_hkind ncol rows of its hydrogen rates (:1854-1876), the
+ * downward rate of each being cup * n*_i/n*_j; then with gencol nrec rows of each
+ * record's upward and nrec of its downward rate (:2223-2360), for which nstar
+ * (ncell, nlevel) is read. */
+int m3d_collision_rates(const m3d_atom_t *atom, int ncell, const double *e_kT, const double *nstar,
+                        const m3d_col_cells_t *cells, double *cup, unsigned flags);
 
 /* update_populations (atom_mod.f90:439-732) with setup_transition_matrix (:740-841):
- * for every cell with totn > 0 (and temp < tmax_update when temp is given) the rate
- * matrix from gamma_ij/gamma_ji (ncell, nrad) float32 -- a line's thermal and
+ * for every cell with totn > 0 (and temp < tmax_update when cells->temp is given) the
+ * rate matrix from gamma_ij/gamma_ji (ncell, nrad) float32 -- a line's thermal and
  * deviation integrals, a continuum's upward and downward rates -- plus
  * collisions x cswitch, the solve, the limiter, e^sor_w, renormalisation to totn and
  * the population floor; b (ncell, nlevel) is updated in place.  Collisions come from
- * cup (ncell, ncol) when given, else from temp, ne, e_kT, dxi as m3d_collision_rates
- * forms them.  lvlerr (nlevel, host) and res (host) receive the convergence record.
+ * cup (as m3d_collision_rates lays it out) when given, else from cells as
+ * m3d_collision_rates forms them.  cells may be NULL without collisions or temp
+ * filter.  lvlerr (nlevel, host) and res (host) receive the convergence record.
  * A cell whose solution is not finite keeps its b, and the call returns
  * M3D_ENONFINITE with res->nonfinite_cell set (the reference stops the run there). */
 int m3d_stateq_update(const m3d_atom_t *atom, const m3d_se_params_t *par, int ncell, double *b,
-                      const double *nstar, const double *totn, const double *temp, const double *ne,
-                      const double *e_kT, const double *dxi, const double *nh1, const float *gamma_ij,
-                      const float *gamma_ji, const double *cup, double *lvlerr,
-                      m3d_se_result_t *res, unsigned flags);
+                      const double *nstar, const double *totn, const double *e_kT,
+                      const m3d_col_cells_t *cells, const float *gamma_ij, const float *gamma_ji,
+                      const double *cup, double *lvlerr, m3d_se_result_t *res, unsigned flags);
 
 /* ng_accumulate (ng_mod.f90:241-287): gram (host, 7) = d01, d02, d11, d12, d21, d22
  * and |d0|^2 over all cells and levels of ln b; oldb is (ncell, nlevel, 3), the

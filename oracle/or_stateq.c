@@ -47,6 +47,7 @@
 #define SQ_AME ((double)5.485799e-4f)
 #define SQ_AMH 1.0
 #define SQ_MU_E (SQ_AME / (SQ_AME + SQ_AMH))
+#define SQ_ERYD (13.605 * SQ_EE)
 
 /* expin: E1(x) by rational approximations, 0 for x <= 0 (atom_mod.f90:2362-2397) */
 double sq_expin(double x)
@@ -118,12 +119,128 @@ double sq_prepare_drawin(double awgt)
   return c * sqrt(2.0 * SQ_BK / drmu) * SQ_MU_E / mu_h;
 }
 
+void sq_hermite_derivative(int n, const double *x, const double *y, double *d)
+{
+#define DX(i) (x[(i) + 1] - x[(i)])
+#define DY(i) (y[(i) + 1] - y[(i)])
+  for (int i = 0; i < n; i++) d[i] = 0.0;
+  if (n == 2) {
+    d[0] = DY(0) / DX(0);
+    d[1] = d[0];
+  }
+  for (int i = 1; i <= n - 2; i++) {
+    if (DY(i - 1) == 0 || DY(i) == 0) continue;
+    const double d1 = DY(i - 1) / DX(i - 1), d2 = DY(i) / DX(i);
+    if (copysign(1.0, d1) == copysign(1.0, d2)) {
+      const double alpha = (1.0 + DX(i - 1) / (DX(i) + DX(i - 1))) / 3.0;
+      d[i] = 1.0 / ((1.0 - alpha) / d1 + alpha / d2);
+    }
+  }
+  d[0] = 2.0 * DY(0) / DX(0) - d[1];
+  d[n - 1] = 2.0 * DY(n - 2) / DX(n - 2) - d[n - 2];
+#undef DX
+#undef DY
+}
+
+/* BinarySearch8 (op_math_mod.f90:179-199), 1-based as there: arr(l) < x <= arr(r) */
+static int sq_bsearch8(const double *arr, int l, int r, double x)
+{
+  if (r - l > 1) {
+    const int mid = l + (r - l) / 2;
+    if (arr[mid - 1] >= x) return sq_bsearch8(arr, l, mid, x);
+    return sq_bsearch8(arr, mid, r, x);
+  }
+  return l;
+}
+
+double sq_hermite_interp(int n, const double *x, const double *y, const double *d, double xx)
+{
+  if (xx <= x[0]) return y[0];
+  if (xx >= x[n - 1]) return y[n - 1];
+  const int i = sq_bsearch8(x, 1, n, xx) - 1;
+  const double dx = x[i + 1] - x[i];
+  /* hermite_value8 (interpol_mod.f90:149-162) */
+  const double t = (xx - x[i]) / dx;
+  const double t2 = t * t, t3 = t2 * t;
+  const double p = 3.0 * t2 - 2.0 * t3;
+  return (1.0 - p) * y[i] + p * y[i + 1] + dx * ((t3 - 2.0 * t2 + t) * d[i] + (t3 - t2) * d[i + 1]);
+}
+
+/* gencol (atom_mod.f90:2223-2360) for one record and cell: upward and downward rate */
+static void sq_gencol_record(const sq_atom_t *at, int r, double temp, double ne, double dxi, double e_kT,
+                             double lsaha, double nh1, double n_collider, double nll, double nul, double *cup,
+                             double *cdn)
+{
+  const double c0 = ((SQ_ERYD / sqrt(SQ_EM)) * SQ_PI * (SQ_RBOHR * SQ_RBOHR)) * sqrt(8.0 / (SQ_PI * SQ_BK));
+  const int ll = at->gll[r], ul = at->gul[r];
+  double u = 0, d = 0, nji;
+  double dev = at->ev[ul] - at->ev[ll];
+  if (at->ion[ul] > at->ion[ll]) {
+    const int ii = at->ion[ll] * (at->ion[ll] - 1), jj = at->ion[ul] * (at->ion[ul] - 1);
+    dev = dev - dxi * 0.5 * (jj - ii);
+  }
+  if (nll > 0) {
+    nji = nul / nll;
+  } else {
+    const double tns = -dev * e_kT + (at->ion[ul] - at->ion[ll]) * lsaha;
+    nji = at->g[ul] / at->g[ll] * exp(tns);
+  }
+  const double stg = sqrt(temp);
+  const size_t o = (size_t)r * at->ntemp;
+  const double ct = exp(sq_hermite_interp(at->ntemp, at->gt, at->glnc + o, at->gdc + o, temp));
+  switch (at->gkind[r]) {
+  case SQ_GC_OHM:
+    d = c0 / at->g[ul] * ct * ne / stg;
+    u = d * nji;
+    break;
+  case SQ_GC_CE:
+    d = at->g[ll] / at->g[ul] * ct * ne * stg;
+    d = d * at->cbbesc;
+    u = d * nji;
+    break;
+  case SQ_GC_CH:
+    d = ct * nh1;
+    d = d * at->cbbhsc;
+    u = d * nji;
+    break;
+  case SQ_GC_CHI:
+    u = ct * nh1;
+    u = u * at->cbfhsc;
+    d = u / nji;
+    break;
+  case SQ_GC_CI:
+    u = ct * ne * stg * exp(-(at->ev[ul] - at->ev[ll]) * e_kT);
+    u = u * at->cbfesc;
+    d = u / nji;
+    break;
+  case SQ_GC_CH0:
+    u = ct * nh1;
+    if (at->ch0_hmip) u = u * exp(-(double)0.754f * e_kT);
+    u = u * at->cbfhsc;
+    d = u / nji;
+    break;
+  case SQ_GC_UP:
+    u = ct * n_collider;
+    d = u / nji;
+    break;
+  case SQ_GC_DN:
+    d = ct * n_collider;
+    u = d * nji;
+    break;
+  default:
+    break;
+  }
+  *cup = u * at->colscale;
+  *cdn = d * at->colscale;
+}
+
 /* classic_col (atom_mod.f90:1758-1880): cup(cell, pair) [1/s] upward, colscale
  * applied, the electron recipe's rate in rows 0..ncol-1 and, with chkind, the
  * hydrogen recipe's in rows ncol..2ncol-1; the downward rate of each is
  * cup * n*_i/n*_j */
 void or_collisions(const sq_atom_t *at, int ncell, const double *temp, const double *ne, const double *e_kT,
-                   const double *dxi, const double *nh1, double *cup)
+                   const double *dxi, const double *nh1, const double *nstar, const double *lsaha,
+                   const double *coll, double *cup)
 {
   const double sq32 = sqrt(3.0) / 2.0;
   const double sqr3_2pi = sq32 / SQ_PI;
@@ -188,6 +305,17 @@ void or_collisions(const sq_atom_t *at, int ncell, const double *temp, const dou
       }
       if (h != 0) h = h * at->colscale;
       cup[(size_t)c + (size_t)ncell * (ncol + p)] = h;
+    }
+    const int r0 = at->chkind ? 2 * ncol : ncol;
+    for (int r = 0; r < at->ngrec; r++) {
+      const int k = at->gcoll ? at->gcoll[r] : -1;
+      double u, d;
+      sq_gencol_record(at, r, temp[c], ne[c], dxi ? dxi[c] : 0.0, e_kT[c], lsaha ? lsaha[c] : 0.0,
+                       nh1 ? nh1[c] : 0.0, k >= 0 ? coll[(size_t)c + (size_t)ncell * k] : 0.0,
+                       nstar[(size_t)c + (size_t)ncell * at->gll[r]], nstar[(size_t)c + (size_t)ncell * at->gul[r]],
+                       &u, &d);
+      cup[(size_t)c + (size_t)ncell * (r0 + r)] = u;
+      cup[(size_t)c + (size_t)ncell * (r0 + at->ngrec + r)] = d;
     }
   }
 }
@@ -350,26 +478,38 @@ void or_rate_matrix(const sq_atom_t *at, const sq_params_t *pr, const double *bl
     W(i, j) = W(i, j) + r_down;
   }
   if (pr->cswitch > 0) {
-    /* c starts at zero; each nonzero rate adds c(j,i) += cup and c(i,j) += cup *
-     * n*_i/n*_j, electrons first, then hydrogen (classic_col :1846-1876); then
-     * w += c * cswitch over the whole matrix (:806-811) */
+    /* collision_rates (:918-930): c = 0; classic_col adds each nonzero rate,
+     * c(j,i) += cup and c(i,j) += cup * n*_i/n*_j, electrons first, then hydrogen
+     * (:1846-1876); gencol adds every record's rates (:2350-2351); then w += c *
+     * cswitch over the whole matrix (:806-811) */
+    double *cm = (double *)calloc((size_t)n * n, sizeof(double));
+#define CM(i, j) cm[(i) + n * (j)]
     for (int p = 0; p < at->ncol; p++) {
-      const double ue = cupc[p], uh = at->chkind ? cupc[at->ncol + p] : 0.0;
-      if (ue == 0 && uh == 0) continue;
       const int i = at->ci[p], j = at->cj[p];
       const double nij = ns[i] / ns[j];
-      double cu = 0, cd = 0;
+      const double ue = cupc[p];
       if (ue != 0) {
-        cu = cu + ue;
-        cd = cd + ue * nij;
+        CM(j, i) = CM(j, i) + ue;
+        CM(i, j) = CM(i, j) + ue * nij;
       }
-      if (uh != 0) {
-        cu = cu + uh;
-        cd = cd + uh * nij;
+      if (at->chkind) {
+        const double uh = cupc[at->ncol + p];
+        if (uh != 0) {
+          CM(j, i) = CM(j, i) + uh;
+          CM(i, j) = CM(i, j) + uh * nij;
+        }
       }
-      W(j, i) = W(j, i) + cu * pr->cswitch;
-      W(i, j) = W(i, j) + cd * pr->cswitch;
     }
+    const int r0 = at->chkind ? 2 * at->ncol : at->ncol;
+    for (int r = 0; r < at->ngrec; r++) {
+      const int ll = at->gll[r], ul = at->gul[r];
+      CM(ul, ll) = CM(ul, ll) + cupc[r0 + r];
+      CM(ll, ul) = CM(ll, ul) + cupc[r0 + at->ngrec + r];
+    }
+    for (int j = 0; j < n; j++)
+      for (int i = 0; i < n; i++) W(i, j) = W(i, j) + CM(i, j) * pr->cswitch;
+#undef CM
+    free(cm);
   }
   for (int i = 0; i < n; i++) {
     double s = 0;
@@ -399,7 +539,7 @@ int or_stateq_update(const sq_atom_t *at, const sq_params_t *pr, int ncell, doub
 {
   const int n = at->nlevel, nrad = at->nrad;
   double *w = (double *)malloc(sizeof(double) * n * n);
-  const int ncup = at->chkind ? 2 * at->ncol : at->ncol;
+  const int ncup = (at->chkind ? 2 * at->ncol : at->ncol) + 2 * at->ngrec;
   double *cupc = (double *)malloc(sizeof(double) * (ncup > 0 ? ncup : 1));
   float *gij = (float *)malloc(sizeof(float) * (nrad > 0 ? nrad : 1));
   float *gji = (float *)malloc(sizeof(float) * (nrad > 0 ? nrad : 1));

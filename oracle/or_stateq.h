@@ -19,6 +19,8 @@ extern "C" {
  * ckind, hydrogen recipes in chkind */
 enum { SQ_COL_REGEMORTER = 1, SQ_COL_SEATON = 2 };
 enum { SQ_COLH_DRAWIN = 1, SQ_COLH_TAKEDA = 2 };
+/* gencol's record kinds (atom_mod.f90:2288-2344) */
+enum { SQ_GC_NONE = 0, SQ_GC_OHM, SQ_GC_CE, SQ_GC_CH, SQ_GC_CHI, SQ_GC_CI, SQ_GC_CH0, SQ_GC_UP, SQ_GC_DN };
 
 typedef struct sq_atom {
   int nlevel, nrad, nline;     /* transitions 0..nline-1 are lines, nline..nrad-1 continua */
@@ -35,6 +37,11 @@ typedef struct sq_atom {
   const int *chkind;           /* [ncol] SQ_COLH_* or NULL: no hydrogen recipes */
   double drawin;               /* sq_prepare_drawin(awgt) */
   double cbbhsc, cbfhsc;       /* factors on the hydrogen rates */
+  /* gencol's records (atom_mod.f90:2223-2360): ln of the rate coefficient on tgrid
+   * and its node slopes, both (ngrec, ntemp) with the temperature fastest */
+  int ngrec, ntemp, ch0_hmip, pad;
+  const double *gt, *glnc, *gdc;
+  const int *gll, *gul, *gkind, *gcoll; /* gcoll: collider row of UP/DN records, or NULL */
 } sq_atom_t;
 
 typedef struct sq_params {
@@ -59,11 +66,19 @@ double sq_kramer(double lam, double dev);
 /* prepare_Drawin's prefactor for an atom of weight awgt [amu] (atom_mod.f90:1741-1750) */
 double sq_prepare_drawin(double awgt);
 
-/* cup (ncell, ncol) of the electron rates, then with chkind (ncell, ncol) more of
- * the hydrogen rates; nh1 (ncell) the hydrogen ground-level density, read only
- * with chkind */
+/* hermite_derivative (interpol_mod.f90:544-553): pchip_slopes8 over a whole line */
+void sq_hermite_derivative(int n, const double *x, const double *y, double *d);
+/* hermite_interpolation_single (interpol_mod.f90:558-578) */
+double sq_hermite_interp(int n, const double *x, const double *y, const double *d, double xx);
+
+/* cup (ncell, rows) of collision_rates (atom_mod.f90:918-930): ncol rows of the
+ * electron rates, with chkind ncol more of the hydrogen rates, then with records
+ * ngrec rows of their upward and ngrec of their downward rates.  nh1 (ncell) the
+ * hydrogen ground-level density, nstar (ncell, nlevel), lsaha (ncell) and coll
+ * (ncollider, ncell) are read where the recipes and records need them. */
 void or_collisions(const sq_atom_t *at, int ncell, const double *temp, const double *ne, const double *e_kT,
-                   const double *dxi, const double *nh1, double *cup);
+                   const double *dxi, const double *nh1, const double *nstar, const double *lsaha,
+                   const double *coll, double *cup);
 
 void sq_lineq_no_pivot(double *a, double *b, int n);
 void sq_lineq(double *a, double *b, int n);

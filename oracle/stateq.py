@@ -20,7 +20,10 @@ class SqAtom(C.Structure):
                 ("ci", C.c_void_p), ("cj", C.c_void_p), ("ckind", C.c_void_p), ("cfac", C.c_void_p),
                 ("fmin", C.c_double), ("cbbesc", C.c_double), ("cbfesc", C.c_double), ("colscale", C.c_double),
                 ("upsilon_floor", C.c_double), ("cut_x", C.c_double), ("bf_cut_rate", C.c_double),
-                ("chkind", C.c_void_p), ("drawin", C.c_double), ("cbbhsc", C.c_double), ("cbfhsc", C.c_double)]
+                ("chkind", C.c_void_p), ("drawin", C.c_double), ("cbbhsc", C.c_double), ("cbfhsc", C.c_double),
+                ("ngrec", C.c_int), ("ntemp", C.c_int), ("ch0_hmip", C.c_int), ("pad", C.c_int),
+                ("gt", C.c_void_p), ("glnc", C.c_void_p), ("gdc", C.c_void_p),
+                ("gll", C.c_void_p), ("gul", C.c_void_p), ("gkind", C.c_void_p), ("gcoll", C.c_void_p)]
 
 
 class SqParams(C.Structure):
@@ -62,7 +65,47 @@ def make_atom(atom: dict):
     s.chkind = arr("col_hkind", np.int32)
     s.drawin = prepare_drawin(float(atom["awgt"])) if s.chkind is not None else 0.0
     s.cbbhsc, s.cbfhsc = float(atom.get("cbbhsc", 1.0)), float(atom.get("cbfhsc", 1.0))
+    gc = atom.get("gencol")
+    if gc is not None and len(gc["ll"]) > 0:
+        lnc = np.ascontiguousarray(gc["lnc"], np.float64)
+        s.ngrec, s.ntemp = lnc.shape
+        s.ch0_hmip = int(bool(gc.get("ch0_hmip", False)))
+        tg = np.ascontiguousarray(gc["tgrid"], np.float64)
+        dl = gc.get("dlnc")
+        dl = hermite_derivative(tg, lnc) if dl is None else np.ascontiguousarray(dl, np.float64)
+        keep.extend([lnc, tg, dl])
+        s.gt, s.glnc, s.gdc = _vp(tg), _vp(lnc), _vp(dl)
+        src = {"gll": gc["ll"], "gul": gc["ul"], "gkind": gc["kind"], "gcoll": gc.get("collider")}
+        for k, v in src.items():
+            if v is not None:
+                a = np.ascontiguousarray(v, np.int32)
+                keep.append(a)
+                setattr(s, k, _vp(a))
     return s, keep
+
+
+def hermite_derivative(tgrid, lnc):
+    """hermite_derivative (pchip_slopes8) of every row of lnc (nrec, ntemp)."""
+    tg = np.ascontiguousarray(tgrid, np.float64)
+    lnc = np.ascontiguousarray(lnc, np.float64)
+    out = np.zeros_like(lnc)
+    for r in range(lnc.shape[0]):
+        lib().sq_hermite_derivative(C.c_int(tg.size), _vp(tg), C.c_void_p(lnc[r].ctypes.data),
+                                    C.c_void_p(out[r].ctypes.data))
+    return out
+
+
+def hermite_interp(x, y, d, xx):
+    f = lib().sq_hermite_interp
+    f.restype = C.c_double
+    x, y, d = (np.ascontiguousarray(v, np.float64) for v in (x, y, d))
+    return f(C.c_int(x.size), _vp(x), _vp(y), _vp(d), C.c_double(xx))
+
+
+def collision_rows(atom: dict) -> int:
+    ncol = len(atom["col_i"]) if atom.get("col_i") is not None else 0
+    gc = atom.get("gencol")
+    return ncol * (2 if atom.get("col_hkind") is not None else 1) + (2 * len(gc["ll"]) if gc is not None else 0)
 
 
 def prepare_drawin(awgt: float) -> float:
@@ -88,17 +131,21 @@ def kramer(lam, dev):
     return f(C.c_double(lam), C.c_double(dev))
 
 
-def collision_rates(atom: dict, temp, ne, e_kT, dxi=None, nh1=None):
-    """classic_col's upward rates (ncol, ncell): electrons, then with col_hkind
-    (2 ncol rows) hydrogen, whose recipes read nh1."""
+def collision_rates(atom: dict, temp, ne, e_kT, dxi=None, nh1=None, nstar=None, lsaha=None, colliders=None):
+    """collision_rates' rows (collision_rows(atom), ncell): classic_col's upward
+    electron rates, with col_hkind its hydrogen ones (reading nh1), then with
+    gencol records their upward and downward rates (reading nstar, lsaha and,
+    for UP/DN records, colliders (ncollider, ncell))."""
     st, keep = make_atom(atom)
     temp, ne, e_kT, dxi, nh1 = _f64(temp), _f64(ne), _f64(e_kT), _f64(dxi), _f64(nh1)
-    rows = 2 * st.ncol if st.chkind is not None else st.ncol
+    nstar, lsaha, colliders = _f64(nstar), _f64(lsaha), _f64(colliders)
     if st.chkind is not None and nh1 is None:
         raise ValueError("hydrogen collision recipes need nh1")
-    cup = np.zeros((rows, temp.size), np.float64)
+    if st.ngrec > 0 and (nstar is None or lsaha is None):
+        raise ValueError("gencol records need nstar and lsaha")
+    cup = np.zeros((collision_rows(atom), temp.size), np.float64)
     lib().or_collisions(C.byref(st), C.c_int(temp.size), _vp(temp), _vp(ne), _vp(e_kT), _vp(dxi), _vp(nh1),
-                        _vp(cup))
+                        _vp(nstar), _vp(lsaha), _vp(colliders), _vp(cup))
     return cup
 
 
@@ -122,7 +169,8 @@ def rate_matrix(atom: dict, inputs: dict, cell: int, cup=None, cswitch: float = 
     ns = np.ascontiguousarray(inputs["nstar"][:, cell], np.float64)
     gij = np.ascontiguousarray(inputs["gamma_ij"][:, cell], np.float32)
     gji = np.ascontiguousarray(inputs["gamma_ji"][:, cell], np.float32)
-    cupc = np.ascontiguousarray(cup[:, cell], np.float64) if cup is not None else np.zeros(max(2 * st.ncol, 1))
+    cupc = (np.ascontiguousarray(cup[:, cell], np.float64) if cup is not None
+            else np.zeros(max(collision_rows(atom), 1)))
     w = np.zeros(n * n, np.float64)
     e = np.zeros(n, np.float64)
     lib().or_rate_matrix(C.byref(st), C.byref(par), _vp(bl), _vp(ns), C.c_double(float(inputs["totn"][cell])),
@@ -139,7 +187,7 @@ def stateq_update(atom: dict, b, nstar, totn, e_kT, gamma_ij, gamma_ji, temp=Non
     nstar, totn, e_kT, temp, cup = _f64(nstar), _f64(totn), _f64(e_kT), _f64(temp), _f64(cup)
     gamma_ij = np.ascontiguousarray(gamma_ij, np.float32)
     gamma_ji = np.ascontiguousarray(gamma_ji, np.float32)
-    if cswitch > 0 and st.ncol > 0 and cup is None:
+    if cswitch > 0 and (st.ncol > 0 or st.ngrec > 0) and cup is None:
         raise ValueError("the oracle takes the collision rates precomputed (collision_rates)")
     par = SqParams(max_update, sor_w, min_pop_frac, conv_pop_floor, tmax_update, cswitch, int(solver), 0)
     res = SqResult()
