@@ -342,20 +342,59 @@ __global__ void k_collision_rates(SeAtomDev A, SeCells C, double *__restrict__ c
 // ---- the per-warp dense solvers ------------------------------------------------
 // a(i,j) = W[i + n*j]; e is the right-hand side, the solution on return.
 
-// lineq_no_pivot (op_math_mod.f90:420-449)
+// a(i,j) - l a(k,j) of one element, skipped where a(k,j) = 0 as the reference skips it
+__device__ __forceinline__ double se_elim(double aij, double l, double akj) {
+  return akj != 0 ? aij - l * akj : aij;
+}
+
+// lineq_no_pivot (op_math_mod.f90:420-449).  In step k a lane owns the rows
+// k+1+lane (and k+33+lane while more than 32 rows remain); when fewer rows than
+// lanes remain, the lanes split the columns into G groups.  The multiplier
+// l(i) = a(i,k)/a(k,k) stays in a register, and four columns' loads precede their
+// stores, so the FP64 chains of a lane overlap.  Every element still takes its one
+// update per step, a(i,j) - l(i) a(k,j), so the roundings are the sequential loop's.
 __device__ __forceinline__ void se_solve_no_pivot(double *W, double *e, int n, int lane) {
   for (int k = 0; k < n - 1; k++) {
-    const double pk = W[k + n * k];
-    for (int i = k + 1 + lane; i < n; i += 32) W[i + n * k] = W[i + n * k] / pk;
-    __syncwarp();
     const int m = n - k - 1;
-    int ii = lane % m, jj = lane / m;
-    for (int idx = lane; idx < m * m; idx += 32) {
-      const int i = k + 1 + ii, j = k + 1 + jj;
-      const double akj = W[k + n * j];
-      if (akj != 0) W[i + n * j] = W[i + n * j] - W[i + n * k] * akj;
-      ii += 32;
-      while (ii >= m) { ii -= m; jj++; }
+    const double pk = W[k + n * k];
+    const int G = m >= 32 ? 1 : 32 / m;
+    const int g = m >= 32 ? 0 : lane / m;
+    const bool act = g < G;
+    const int i0 = k + 1 + (m >= 32 ? lane : lane % m), i1 = i0 + 32;
+    const bool two = m > 32 && i1 < n;
+    double l0 = 0, l1 = 0;
+    if (act) {
+      l0 = W[i0 + n * k] / pk;
+      if (two) l1 = W[i1 + n * k] / pk;
+    }
+    __syncwarp();  // every group has read a(i,k) before group 0 overwrites it with l(i)
+    if (act) {
+      if (g == 0) {
+        W[i0 + n * k] = l0;
+        if (two) W[i1 + n * k] = l1;
+      }
+      int j = k + 1 + g;
+      for (; j + 3 * G < n; j += 4 * G) {
+        const int c0 = n * j, c1 = c0 + n * G, c2 = c1 + n * G, c3 = c2 + n * G;
+        const double a0 = W[k + c0], a1 = W[k + c1], a2 = W[k + c2], a3 = W[k + c3];
+        const double x0 = W[i0 + c0], x1 = W[i0 + c1], x2 = W[i0 + c2], x3 = W[i0 + c3];
+        if (two) {
+          const double y0 = W[i1 + c0], y1 = W[i1 + c1], y2 = W[i1 + c2], y3 = W[i1 + c3];
+          W[i1 + c0] = se_elim(y0, l1, a0);
+          W[i1 + c1] = se_elim(y1, l1, a1);
+          W[i1 + c2] = se_elim(y2, l1, a2);
+          W[i1 + c3] = se_elim(y3, l1, a3);
+        }
+        W[i0 + c0] = se_elim(x0, l0, a0);
+        W[i0 + c1] = se_elim(x1, l0, a1);
+        W[i0 + c2] = se_elim(x2, l0, a2);
+        W[i0 + c3] = se_elim(x3, l0, a3);
+      }
+      for (; j < n; j += G) {
+        const double a = W[k + n * j];
+        if (two) W[i1 + n * j] = se_elim(W[i1 + n * j], l1, a);
+        W[i0 + n * j] = se_elim(W[i0 + n * j], l0, a);
+      }
     }
     __syncwarp();
   }
