@@ -342,62 +342,70 @@ __global__ void k_collision_rates(SeAtomDev A, SeCells C, double *__restrict__ c
 // ---- the per-warp dense solvers ------------------------------------------------
 // a(i,j) = W[i + n*j]; e is the right-hand side, the solution on return.
 
-// a(i,j) - l a(k,j) of one element, skipped where a(k,j) = 0 as the reference skips it
+// a(i,j) - l a(k,j) of one element; SKIP: left alone where a(k,j) = 0, as
+// lineq_no_pivot skips it
+template <bool SKIP>
 __device__ __forceinline__ double se_elim(double aij, double l, double akj) {
-  return akj != 0 ? aij - l * akj : aij;
+  if (SKIP) return akj != 0 ? aij - l * akj : aij;
+  return aij - l * akj;
 }
 
-// lineq_no_pivot (op_math_mod.f90:420-449).  In step k a lane owns the rows
-// k+1+lane (and k+33+lane while more than 32 rows remain); when fewer rows than
-// lanes remain, the lanes split the columns into G groups.  The multiplier
-// l(i) = a(i,k)/a(k,k) stays in a register, and four columns' loads precede their
-// stores, so the FP64 chains of a lane overlap.  Every element still takes its one
-// update per step, a(i,j) - l(i) a(k,j), so the roundings are the sequential loop's.
-__device__ __forceinline__ void se_solve_no_pivot(double *W, double *e, int n, int lane) {
-  for (int k = 0; k < n - 1; k++) {
-    const int m = n - k - 1;
-    const double pk = W[k + n * k];
-    const int G = m >= 32 ? 1 : 32 / m;
-    const int g = m >= 32 ? 0 : lane / m;
-    const bool act = g < G;
-    const int i0 = k + 1 + (m >= 32 ? lane : lane % m), i1 = i0 + 32;
-    const bool two = m > 32 && i1 < n;
-    double l0 = 0, l1 = 0;
-    if (act) {
-      l0 = W[i0 + n * k] / pk;
-      if (two) l1 = W[i1 + n * k] / pk;
-    }
-    __syncwarp();  // every group has read a(i,k) before group 0 overwrites it with l(i)
-    if (act) {
-      if (g == 0) {
-        W[i0 + n * k] = l0;
-        if (two) W[i1 + n * k] = l1;
-      }
-      int j = k + 1 + g;
-      for (; j + 3 * G < n; j += 4 * G) {
-        const int c0 = n * j, c1 = c0 + n * G, c2 = c1 + n * G, c3 = c2 + n * G;
-        const double a0 = W[k + c0], a1 = W[k + c1], a2 = W[k + c2], a3 = W[k + c3];
-        const double x0 = W[i0 + c0], x1 = W[i0 + c1], x2 = W[i0 + c2], x3 = W[i0 + c3];
-        if (two) {
-          const double y0 = W[i1 + c0], y1 = W[i1 + c1], y2 = W[i1 + c2], y3 = W[i1 + c3];
-          W[i1 + c0] = se_elim(y0, l1, a0);
-          W[i1 + c1] = se_elim(y1, l1, a1);
-          W[i1 + c2] = se_elim(y2, l1, a2);
-          W[i1 + c3] = se_elim(y3, l1, a3);
-        }
-        W[i0 + c0] = se_elim(x0, l0, a0);
-        W[i0 + c1] = se_elim(x1, l0, a1);
-        W[i0 + c2] = se_elim(x2, l0, a2);
-        W[i0 + c3] = se_elim(x3, l0, a3);
-      }
-      for (; j < n; j += G) {
-        const double a = W[k + n * j];
-        if (two) W[i1 + n * j] = se_elim(W[i1 + n * j], l1, a);
-        W[i0 + n * j] = se_elim(W[i0 + n * j], l0, a);
-      }
-    }
-    __syncwarp();
+// One elimination step k: the multipliers l(i) = a(i,k)/a(k,k) of the rows below
+// k go to lstore[i] (column k of W itself, or a separate vector), and the trailing
+// block takes a(i,j) - l(i) a(k,j).  A lane owns the rows k+1+lane (and k+33+lane
+// while more than 32 rows remain); when fewer rows than lanes remain, the lanes split
+// the columns into G groups.  l(i) stays in a register and four columns' loads
+// precede their stores, so the FP64 chains of a lane overlap.  Every element takes
+// its one update per step, so the roundings are the sequential loop's.
+template <bool SKIP>
+__device__ __forceinline__ void se_elim_step(double *W, double *lstore, int n, int k, int lane) {
+  const int m = n - k - 1;
+  const double pk = W[k + n * k];
+  const int G = m >= 32 ? 1 : 32 / m;
+  const int g = m >= 32 ? 0 : lane / m;
+  const bool act = g < G;
+  const int i0 = k + 1 + (m >= 32 ? lane : lane % m), i1 = i0 + 32;
+  const bool two = m > 32 && i1 < n;
+  double l0 = 0, l1 = 0;
+  if (act) {
+    l0 = W[i0 + n * k] / pk;
+    if (two) l1 = W[i1 + n * k] / pk;
   }
+  __syncwarp();  // every group has read a(i,k) before group 0 may overwrite it with l(i)
+  if (act) {
+    if (g == 0) {
+      lstore[i0] = l0;
+      if (two) lstore[i1] = l1;
+    }
+    int j = k + 1 + g;
+    for (; j + 3 * G < n; j += 4 * G) {
+      const int c0 = n * j, c1 = c0 + n * G, c2 = c1 + n * G, c3 = c2 + n * G;
+      const double a0 = W[k + c0], a1 = W[k + c1], a2 = W[k + c2], a3 = W[k + c3];
+      const double x0 = W[i0 + c0], x1 = W[i0 + c1], x2 = W[i0 + c2], x3 = W[i0 + c3];
+      if (two) {
+        const double y0 = W[i1 + c0], y1 = W[i1 + c1], y2 = W[i1 + c2], y3 = W[i1 + c3];
+        W[i1 + c0] = se_elim<SKIP>(y0, l1, a0);
+        W[i1 + c1] = se_elim<SKIP>(y1, l1, a1);
+        W[i1 + c2] = se_elim<SKIP>(y2, l1, a2);
+        W[i1 + c3] = se_elim<SKIP>(y3, l1, a3);
+      }
+      W[i0 + c0] = se_elim<SKIP>(x0, l0, a0);
+      W[i0 + c1] = se_elim<SKIP>(x1, l0, a1);
+      W[i0 + c2] = se_elim<SKIP>(x2, l0, a2);
+      W[i0 + c3] = se_elim<SKIP>(x3, l0, a3);
+    }
+    for (; j < n; j += G) {
+      const double a = W[k + n * j];
+      if (two) W[i1 + n * j] = se_elim<SKIP>(W[i1 + n * j], l1, a);
+      W[i0 + n * j] = se_elim<SKIP>(W[i0 + n * j], l0, a);
+    }
+  }
+  __syncwarp();
+}
+
+// lineq_no_pivot (op_math_mod.f90:420-449)
+__device__ __forceinline__ void se_solve_no_pivot(double *W, double *e, int n, int lane) {
+  for (int k = 0; k < n - 1; k++) se_elim_step<true>(W, W + n * k, n, k, lane);
   // forward substitution: per row the terms arrive in ascending j, as in the row loop
   for (int j = 0; j < n - 1; j++) {
     const double ej = e[j];
@@ -464,17 +472,7 @@ __device__ __forceinline__ void se_solve_lineq(double *W, double *e, double *q, 
       icol[jma] = it;
     }
     __syncwarp();
-    const double piv = W[s + n * s];
-    for (int i = s + 1 + lane; i < n; i += 32) q[i] = W[i + n * s] / piv;
-    __syncwarp();
-    const int mm = n - s - 1;
-    int ii = mm > 0 ? lane % mm : 0, jj = mm > 0 ? lane / mm : 0;
-    for (int idx = lane; idx < mm * mm; idx += 32) {
-      const int i = s + 1 + ii, j = s + 1 + jj;
-      W[i + n * j] = W[i + n * j] - q[i] * W[s + n * j];
-      ii += 32;
-      while (ii >= mm) { ii -= mm; jj++; }
-    }
+    se_elim_step<false>(W, q, n, s, lane);
     const double es = e[s];
     for (int i = s + 1 + lane; i < n; i += 32) e[i] = e[i] - q[i] * es;
     __syncwarp();
@@ -523,18 +521,7 @@ __device__ __forceinline__ void se_solve_partial(double *W, double *e, int n, in
       }
     }
     __syncwarp();
-    const double pk = W[k + n * k];
-    for (int i = k + 1 + lane; i < n; i += 32) W[i + n * k] = W[i + n * k] / pk;
-    __syncwarp();
-    const int m = n - k - 1;
-    int ii = lane % m, jj = lane / m;
-    for (int idx = lane; idx < m * m; idx += 32) {
-      const int i = k + 1 + ii, j = k + 1 + jj;
-      W[i + n * j] = W[i + n * j] - W[i + n * k] * W[k + n * j];
-      ii += 32;
-      while (ii >= m) { ii -= m; jj++; }
-    }
-    __syncwarp();
+    se_elim_step<false>(W, W + n * k, n, k, lane);
   }
   for (int j = 0; j < n - 1; j++) {
     const double ej = e[j];
