@@ -240,8 +240,12 @@ __global__ void __launch_bounds__(256, 3) k_lte_opacity_units_lane(AtmosDev A, G
         const float xnear = (x0 > 0.0f) ? x0 : ((xe < 0.0f) ? -xe : 0.0f);
         // A window over the whole frequency range -- most lines -- runs without
         // per-point predicates, and with fa = 1 the offset (float)f + kfa is (float)f.
-        const bool full = fa == 1 && fb == NF;
-        if (fminf((xnear * cf.ih) * 800.0f, 9019.0f) >= 9018.5f) {
+        // The far-wing and whole-window forms are taken only when every converged
+        // lane of the warp qualifies: the general forms give the same values where
+        // the special ones apply, so the warp never runs two forms of one line.
+        const unsigned conv = __activemask();
+        const bool full = __all_sync(conv, fa == 1 && fb == NF);
+        if (__all_sync(conv, fminf((xnear * cf.ih) * 800.0f, 9019.0f) >= 9018.5f)) {
           const float2 gw = s_tab[QLG_NTAB - 1];
           const float p1 = fmaf(cf.cZH, gw.y, cf.cL2);
           const float gg = gw.x * cf.gG;
