@@ -141,6 +141,18 @@ __global__ void __launch_bounds__(256) k_lte_opacity_units(AtmosDev A, GridArgs 
 // the spot otherwise; the accumulated line opacity there is picked out of the
 // register array.  Results are bit-identical to k_lte_opacity_units.
 // ---------------------------------------------------------------------------
+// 1/d correctly rounded for d in [1, 2^126): the approximate reciprocal refined by
+// one Newton step in fused multiply-adds, e = 1 - d r, r + r e (Markstein's method,
+// IBM J. Res. Dev. 34 (1990) 111).  Equal to __frcp_rn on every float of that range
+// (an exhaustive comparison on the B200); outside it the approximation's flush to
+// zero would differ, so callers bound d first.
+__device__ __forceinline__ float rcp_markstein(float d) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(d));
+  const float e = fmaf(-d, r, 1.0f);
+  return fmaf(r, e, r);
+}
+
 template <int NF>
 __device__ __forceinline__ float pick(const float (&a)[NF], int i) {
   float v = a[0];
@@ -249,7 +261,19 @@ __global__ void __launch_bounds__(256, 3) k_lte_opacity_units_lane(AtmosDev A, G
           const float2 gw = s_tab[QLG_NTAB - 1];
           const float p1 = fmaf(cf.cZH, gw.y, cf.cL2);
           const float gg = gw.x * cf.gG;
-          if (full) {
+          // the window's largest |x| ih bounds every point's 1 + xs^2 (rounded
+          // products are monotone): below 2^62 it stays under 2^126, where one
+          // Markstein step gives the correctly rounded reciprocal
+          const float xmax = fmaxf(fabsf(x0), fabsf(x0 + (float)(NF - 1))) * cf.ih;
+          if (full && __all_sync(conv, xmax <= 4611686018427387904.0f)) {
+#pragma unroll
+            for (int f = 0; f < NF; f++) {
+              const float xs = fabsf(x0 + (float)f) * cf.ih;
+              const float L = rcp_markstein(1.0f + xs * xs);
+              const float K = fmaf(L, fmaf(L, p1, cf.bL), gg);
+              chl[f] = fmaf(K, 1.0f, chl[f]);
+            }
+          } else if (full) {
 #pragma unroll
             for (int f = 0; f < NF; f++) {
               const float xs = fabsf(x0 + (float)f) * cf.ih;
