@@ -141,16 +141,53 @@ __global__ void __launch_bounds__(256) k_lte_opacity_units(AtmosDev A, GridArgs 
 // the spot otherwise; the accumulated line opacity there is picked out of the
 // register array.  Results are bit-identical to k_lte_opacity_units.
 // ---------------------------------------------------------------------------
-// 1/d correctly rounded for d in [1, 2^126): the approximate reciprocal refined by
-// one Newton step in fused multiply-adds, e = 1 - d r, r + r e (Markstein's method,
-// IBM J. Res. Dev. 34 (1990) 111).  Equal to __frcp_rn on every float of that range
-// (an exhaustive comparison on the B200); outside it the approximation's flush to
-// zero would differ, so callers bound d first.
-__device__ __forceinline__ float rcp_markstein(float d) {
-  float r;
-  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(d));
-  const float e = fmaf(-d, r, 1.0f);
-  return fmaf(r, e, r);
+// One line's profile over the window into chl.  far: every window point lies
+// beyond the QLG table, where G and W are the last node's at every point and the
+// evaluation is qlg_eval's with them folded in; full: the line covers the whole
+// window, which then runs without per-point predicates (with fa = 1 the offset
+// (float)f + kfa is (float)f).  MK: every point's 1 + xs^2 is below 2^126, so the
+// reciprocal is rcp_markstein's.  All forms give the bits of the general one.
+template <int NF, bool MK>
+__device__ __forceinline__ void deposit_window(float (&chl)[NF], const float2 *s_tab, const QlgCoef &cf, float x0,
+                                               float kfa, int fa, int fb, bool full, bool far) {
+  if (far) {
+    const float2 gw = s_tab[QLG_NTAB - 1];
+    const float p1 = fmaf(cf.cZH, gw.y, cf.cL2);
+    const float gg = gw.x * cf.gG;
+    if (full) {
+#pragma unroll
+      for (int f = 0; f < NF; f++) {
+        const float xs = fabsf(x0 + (float)f) * cf.ih;
+        const float L = qlg_rcp<MK>(1.0f + xs * xs);
+        const float K = fmaf(L, fmaf(L, p1, cf.bL), gg);
+        chl[f] = fmaf(K, 1.0f, chl[f]);
+      }
+    } else {
+#pragma unroll
+      for (int f = 0; f < NF; f++) {
+        if (f + 1 >= fa && f + 1 <= fb) {
+          const float xs = fabsf(x0 + ((float)f + kfa)) * cf.ih;
+          const float L = qlg_rcp<MK>(1.0f + xs * xs);
+          const float K = fmaf(L, fmaf(L, p1, cf.bL), gg);
+          chl[f] = fmaf(K, 1.0f, chl[f]);
+        }
+      }
+    }
+  } else if (full) {
+#pragma unroll
+    for (int f = 0; f < NF; f++) {
+      const float K = qlg_eval<MK>(s_tab, cf, x0 + (float)f);
+      chl[f] = fmaf(K, 1.0f, chl[f]);
+    }
+  } else {
+#pragma unroll
+    for (int f = 0; f < NF; f++) {
+      if (f + 1 >= fa && f + 1 <= fb) {
+        const float K = qlg_eval<MK>(s_tab, cf, x0 + ((float)f + kfa));
+        chl[f] = fmaf(K, 1.0f, chl[f]);
+      }
+    }
+  }
 }
 
 template <int NF>
@@ -257,56 +294,15 @@ __global__ void __launch_bounds__(256, 3) k_lte_opacity_units_lane(AtmosDev A, G
         // the special ones apply, so the warp never runs two forms of one line.
         const unsigned conv = __activemask();
         const bool full = __all_sync(conv, fa == 1 && fb == NF);
-        if (__all_sync(conv, fminf((xnear * cf.ih) * 800.0f, 9019.0f) >= 9018.5f)) {
-          const float2 gw = s_tab[QLG_NTAB - 1];
-          const float p1 = fmaf(cf.cZH, gw.y, cf.cL2);
-          const float gg = gw.x * cf.gG;
-          // the window's largest |x| ih bounds every point's 1 + xs^2 (rounded
-          // products are monotone): below 2^62 it stays under 2^126, where one
-          // Markstein step gives the correctly rounded reciprocal
-          const float xmax = fmaxf(fabsf(x0), fabsf(x0 + (float)(NF - 1))) * cf.ih;
-          if (full && __all_sync(conv, xmax <= 4611686018427387904.0f)) {
-#pragma unroll
-            for (int f = 0; f < NF; f++) {
-              const float xs = fabsf(x0 + (float)f) * cf.ih;
-              const float L = rcp_markstein(1.0f + xs * xs);
-              const float K = fmaf(L, fmaf(L, p1, cf.bL), gg);
-              chl[f] = fmaf(K, 1.0f, chl[f]);
-            }
-          } else if (full) {
-#pragma unroll
-            for (int f = 0; f < NF; f++) {
-              const float xs = fabsf(x0 + (float)f) * cf.ih;
-              const float L = __frcp_rn(1.0f + xs * xs);
-              const float K = fmaf(L, fmaf(L, p1, cf.bL), gg);
-              chl[f] = fmaf(K, 1.0f, chl[f]);
-            }
-          } else {
-#pragma unroll
-            for (int f = 0; f < NF; f++) {
-              if (f + 1 >= fa && f + 1 <= fb) {
-                const float xs = fabsf(x0 + ((float)f + kfa)) * cf.ih;
-                const float L = __frcp_rn(1.0f + xs * xs);
-                const float K = fmaf(L, fmaf(L, p1, cf.bL), gg);
-                chl[f] = fmaf(K, 1.0f, chl[f]);
-              }
-            }
-          }
-        } else if (full) {
-#pragma unroll
-          for (int f = 0; f < NF; f++) {
-            const float K = qlg_eval(s_tab, cf, x0 + (float)f);
-            chl[f] = fmaf(K, 1.0f, chl[f]);
-          }
-        } else {
-#pragma unroll
-          for (int f = 0; f < NF; f++) {
-            if (f + 1 >= fa && f + 1 <= fb) {
-              const float K = qlg_eval(s_tab, cf, x0 + ((float)f + kfa));
-              chl[f] = fmaf(K, 1.0f, chl[f]);
-            }
-          }
-        }
+        const bool far = __all_sync(conv, fminf((xnear * cf.ih) * 800.0f, 9019.0f) >= 9018.5f);
+        // The window's largest |x| ih bounds every point's 1 + xs^2 (rounded products
+        // are monotone): at most 2^62 keeps it under 2^126, where rcp_markstein is
+        // exact.  One vote per line picks the reciprocal for the whole window.
+        const float xmax = fmaxf(fabsf(x0), fabsf(xe)) * cf.ih;
+        if (__all_sync(conv, xmax <= 4611686018427387904.0f))
+          deposit_window<NF, true>(chl, s_tab, cf, x0, kfa, fa, fb, full, far);
+        else
+          deposit_window<NF, false>(chl, s_tab, cf, x0, kfa, fa, fb, full, far);
       }
     }
     // epilogue: transfer units, written as 16-byte stores of this cell's row

@@ -51,10 +51,30 @@ __device__ __forceinline__ QlgCoef qlg_setup(float gL, float D, float SQ, float 
   return c;
 }
 
+// 1/d correctly rounded for d in [1, 2^126): the approximate reciprocal refined by
+// one Newton step in fused multiply-adds, e = 1 - d r, r + r e (Markstein's method,
+// IBM J. Res. Dev. 34 (1990) 111).  Equal to __frcp_rn on every float of that range
+// (an exhaustive comparison on the B200); beyond it the approximation flushes to
+// zero, so callers bound d first.
+__device__ __forceinline__ float rcp_markstein(float d) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(d));
+  const float e = fmaf(-d, r, 1.0f);
+  return fmaf(r, e, r);
+}
+
+// the correctly rounded reciprocal of d >= 1: MK when the caller has bounded d below 2^126
+template <bool MK>
+__device__ __forceinline__ float qlg_rcp(float d) {
+  if (MK) return rcp_markstein(d);
+  return __frcp_rn(d);
+}
+
+template <bool MK = false>
 __device__ __forceinline__ float qlg_eval(const float2 *tab, const QlgCoef &c, float x) {
   const float xs = fabsf(x) * c.ih;
   const float u = xs * xs;
-  const float L = __frcp_rn(1.0f + u);
+  const float L = qlg_rcp<MK>(1.0f + u);
   const float y = fminf(xs * 800.0f, 9019.0f);
   const int ig = y < 0.5f ? 0 : (int)(y + 0.5f);
   const float2 gw = tab[ig];
