@@ -43,7 +43,10 @@ struct NlWinDev {
 __device__ __forceinline__ float nl_profile(const float2 *tab, float a, float q, float vpr, float idf) {
   const float v = fabsf(q - vpr) * idf;
   const QlgCoef c = qlg_setup(a, 1.0f, 0.8325546112f, 1.7724538509f);
-  const float K1 = qlg_eval(tab, c, v);
+  // the reciprocal of 1 + (v ih)^2 by rcp_markstein where the converged lanes all
+  // keep it below 2^126 (v ih <= 2^62), else by __frcp_rn: the same bits either way
+  const bool mk = __all_sync(__activemask(), v * c.ih <= 4611686018427387904.0f);
+  const float K1 = mk ? qlg_eval<true>(tab, c, v) : qlg_eval<false>(tab, c, v);
   return ((K1 * 0.5641895835f) * idf) * (q + 1.0f);
 }
 
