@@ -42,7 +42,7 @@ EXPORTS = ("m3d_init", "m3d_free", "m3d_last_error", "m3d_version", "m3d_set_str
            "m3d_long_char_hermite", "m3d_long_char_hermite2", "m3d_short_char_hermite", "m3d_optab_create", "m3d_optab_slopes", "m3d_optab_sample",
            "m3d_optab_sample_ll", "m3d_optab_destroy", "m3d_hydrogen_line", "m3d_h_profile", "m3d_vcs_load", "m3d_vcs_clear",
            "m3d_vcs_supported",
-           "m3d_h_opacity", "m3d_save5")
+           "m3d_h_opacity", "m3d_save5", "m3d_rcp_check")
 
 
 class M3DError(RuntimeError):

@@ -1448,3 +1448,40 @@ extern "C" int m3d_rotate_array_noalloc(const m3d_slab_t *slab, void *work, cons
   if (flags & M3D_FP64) return rotate_noalloc_t<double>(slab, (double *)work, ds_code, bot2pivot, ray_offset);
   return rotate_noalloc_t<float>(slab, (float *)work, ds_code, bot2pivot, ray_offset);
 }
+
+// ---- self-check of the opacity kernels' reciprocal ------------------------------
+namespace m3d {
+// every float with bit pattern in [lo, hi): rcp_markstein against __frcp_rn
+__global__ void k_rcp_check(unsigned lo, unsigned hi, unsigned long long *count, unsigned *first) {
+  const unsigned long long n = (unsigned long long)hi - lo;
+  for (unsigned long long t = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; t < n;
+       t += (unsigned long long)gridDim.x * blockDim.x) {
+    const unsigned b = lo + (unsigned)t;
+    const float d = __uint_as_float(b);
+    if (__float_as_uint(rcp_markstein(d)) != __float_as_uint(__frcp_rn(d))) {
+      atomicAdd(count, 1ull);
+      atomicMin(first, b);
+    }
+  }
+}
+}  // namespace m3d
+
+extern "C" int m3d_rcp_check(unsigned lo_bits, unsigned hi_bits, unsigned long long *mismatches,
+                             unsigned *first_bits) {
+  using namespace m3d;
+  TRY(need_init());
+  if (!mismatches || !first_bits) return fail(M3D_EINVAL, "m3d_rcp_check: NULL outputs");
+  if (hi_bits < lo_bits) return fail(M3D_EINVAL, "m3d_rcp_check: hi_bits < lo_bits");
+  void *sp = nullptr;
+  TRY(scratch(24, 16, &sp));
+  unsigned long long *dc = (unsigned long long *)sp;
+  unsigned *df = (unsigned *)((char *)sp + 8);
+  const unsigned init_first = 0xffffffffu;
+  CUDA_TRY(cudaMemsetAsync(dc, 0, 8, g_ctx.stream));
+  CUDA_TRY(cudaMemcpyAsync(df, &init_first, 4, cudaMemcpyHostToDevice, g_ctx.stream));
+  LAUNCH(k_rcp_check, sm_count() * 16, 256, 0, lo_bits, hi_bits, dc, df);
+  CUDA_TRY(cudaMemcpyAsync(mismatches, dc, 8, cudaMemcpyDeviceToHost, g_ctx.stream));
+  CUDA_TRY(cudaMemcpyAsync(first_bits, df, 4, cudaMemcpyDeviceToHost, g_ctx.stream));
+  CUDA_TRY(cudaStreamSynchronize(g_ctx.stream));
+  return M3D_OK;
+}

@@ -732,6 +732,14 @@ int m3d_col_plan_sweep(m3d_col_plan_t *plan, int first_iter, float *gamma_ij, fl
 int m3d_col_plan_fields(m3d_col_plan_t *plan, float *J, float *PsiJ, int *nf, int *solver_block);
 int m3d_col_plan_destroy(m3d_col_plan_t *plan);
 
+/* Self-check with no counterpart in the reference.  The opacity kernels form 1/(1+u)
+ * by one Markstein step from the approximate reciprocal wherever the window bounds
+ * 1+u below 2^126, and rely on it being bit-identical to the correctly rounded
+ * reciprocal there.  This compares the two on every float whose bit pattern lies in
+ * [lo_bits, hi_bits) on the current device: mismatches and the first mismatching
+ * pattern (0xffffffff if none) come back on the host. */
+int m3d_rcp_check(unsigned lo_bits, unsigned hi_bits, unsigned long long *mismatches, unsigned *first_bits);
+
 #ifdef __cplusplus
 }
 #endif
