@@ -45,6 +45,19 @@ def _args():
     p.add_argument("--no-ali", action="store_true", help="skip the NLTE measurements (3D window, batched columns)")
     p.add_argument("--no-optab", action="store_true", help="skip the sampled opacity table measurement")
     p.add_argument("--cube", type=int, default=240, help="cube edge (240 = the configuration; smaller for profiling)")
+    # single cases for timing and profiling one kernel family (no JSON line)
+    p.add_argument("--case", default="c1", choices=["c1", "ali-window", "ali-columns", "optab"],
+                   help="c1: the headline (default); the others run one seeded NLTE or table case and print "
+                        "per-iteration times")
+    p.add_argument("--n", type=int, default=64, help="ali-window / optab: cube edge")
+    p.add_argument("--ncol", type=int, default=1024, help="ali-columns: columns")
+    p.add_argument("--nbound", type=int, default=20, help="ali-*: bound levels of the model atom")
+    p.add_argument("--nline", type=int, default=60, help="ali-*: bound-bound transitions of the model atom")
+    p.add_argument("--every", type=int, default=8, help="ali-window: the window holds every k-th transition")
+    p.add_argument("--nwin", type=int, default=8, help="ali-columns: frequency windows")
+    p.add_argument("--iters", type=int, default=2, help="ali-* / optab: iterations")
+    p.add_argument("--no-graph", action="store_true", help="ali-columns: direct launches instead of the graph")
+    p.add_argument("--only", choices=["sample", "ll"], default=None, help="optab: one sampler")
     return p.parse_args()
 
 
@@ -575,9 +588,88 @@ def run_b200(a):
     print(json.dumps(line), flush=True)
 
 
+def run_case_ali(a):
+    """ALI iterations of a seeded problem, one line per iteration (the sweep and
+    update times from CUDA events on torch's stream)."""
+    import torch
+
+    import dispatch_b200 as m
+    from dispatch_b200 import ali
+    m.init(0)
+    t0 = time.time()
+    if a.case == "ali-window":
+        nrad = a.nline + a.nbound
+        cube, atom, win, vec, wts = ali.cube_problem("small", nx=a.n, ny=a.n, nz=a.n, nbound=a.nbound,
+                                                     nline=a.nline, ntheta=4, nphi=4,
+                                                     transitions=list(range(0, nrad, a.every)))
+        A = ali.AliWindow(cube, atom, win, vec, wts, params=ali.AliParams(convlim=1e-9))
+    else:
+        cols, atom, wins, mu, wmu = ali.column_problem(ncol=a.ncol, depth=(60, 256), nz=256, nxy=64,
+                                                       nbound=a.nbound, nline=a.nline, nwin=a.nwin)
+        A = ali.AliColumns(cols, atom, wins, mu, wmu, params=ali.AliParams(convlim=1e-9), use_graph=not a.no_graph)
+    torch.cuda.synchronize()
+    print(f"setup {time.time() - t0:.1f} s, {A.ncell} cells, {A.points():.3e} ray-point-frequencies per sweep",
+          flush=True)
+    cur = torch.cuda.current_stream()
+    A.sweep()
+    for _ in range(a.iters):
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        e[0].record(cur)
+        A.iter += 1
+        rec = A.update()
+        e[1].record(cur)
+        A.sweep()
+        e[2].record(cur)
+        torch.cuda.synchronize()
+        sw = e[1].elapsed_time(e[2])
+        print(f"iter {A.iter}: update {e[0].elapsed_time(e[1]):.1f} ms, sweep {sw:.1f} ms "
+              f"({A.points() / sw / 1e6:.2f} Gpt/s), maxerr {rec['maxerr']:.3e}", flush=True)
+
+
+def run_case_optab(a):
+    """The two table samplers on a seeded n^3 cube, one window of --nf frequencies
+    at R = 1e5: best of --iters, CUDA events on torch's stream."""
+    import torch
+
+    import dispatch_b200 as m
+    from dispatch_b200 import synth
+    from dispatch_b200.optab import SampleOptab
+    m.init(0)
+    c = synth.optab_cells(7, a.n, a.n, a.n)
+    ncell = c["temp"].size
+    dev = lambda x: torch.from_numpy(np.ascontiguousarray(x)).cuda()
+    T, N, X, V = dev(c["temp"]), dev(c["ne"]), dev(c["chi500"]), dev(c["vproj"])
+    back = torch.empty((ncell, a.nf), dtype=torch.float32, device="cuda")
+    scat, xh, eh, cs = (torch.zeros_like(back) for _ in range(4))
+    lam_q, bg, ll = synth.window_tables(8, c["temp"], c["ne"], c["vproj"], nf=a.nf)
+    q = dev(lam_q)
+    for name, tab in (("sample", bg), ("ll", ll)):
+        if a.only and a.only != name:
+            continue
+        t = SampleOptab.from_dict(tab)
+        ts = []
+        for _ in range(a.iters):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            if name == "sample":
+                t.interpolate(T, N, X, q, back, scat)
+            else:
+                t.interpolate_ll(T, N, X, xh, eh, q, V, cs)
+            e1.record()
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        print(f"{name}: {ncell} cells x {a.nf} frequencies, table {t.nnu} x {t.ntemp} x {t.nne}: "
+              f"{min(ts):.3f} ms, {ncell * a.nf / min(ts) / 1e6:.2f} Gpt*nu/s", flush=True)
+        t.close()
+
+
 def main():
     a = _args()
-    if a.impl == "reference":
+    if a.case in ("ali-window", "ali-columns"):
+        run_case_ali(a)
+    elif a.case == "optab":
+        run_case_optab(a)
+    elif a.impl == "reference":
         run_reference(a)
     else:
         run_b200(a)

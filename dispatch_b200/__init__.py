@@ -13,6 +13,7 @@ from __future__ import annotations
 
 import ctypes as C
 import os
+import threading
 
 import numpy as np
 
@@ -29,7 +30,7 @@ BND_MEM, BND_ZERO, BND_PCHIP, BND_LTE = range(4)
 
 # every symbol include/m3dgpu.h declares
 EXPORTS = ("m3d_init", "m3d_free", "m3d_last_error", "m3d_version", "m3d_set_stream", "m3d_synchronize",
-           "m3d_launch_count", "m3d_weights", "m3d_qlg_init", "m3d_qlg_tables", "m3d_qlg_bot_profile",
+           "m3d_launch_count", "m3d_alloc_stats", "m3d_weights", "m3d_qlg_init", "m3d_qlg_tables", "m3d_qlg_bot_profile",
            "m3d_line_opacity", "m3d_lte_background", "m3d_work_to_transfer_units", "m3d_formal_solve",
            "m3d_rotate_array", "m3d_upstream_boundary", "m3d_integrate_intensity", "m3d_lte_synthesis",
            "m3d_profile_enable", "m3d_profile_read", "m3d_rotate_array_noalloc", "m3d_collision_nrows",
@@ -111,14 +112,23 @@ def check(rc: int, what: str = "") -> None:
         raise M3DError(f"{what}: status {rc}: {last_error()}")
 
 
-_initialised = False
+# The library keeps one context per host thread (stream, scratch, error string):
+# every Python thread that calls it initialises its own.
+_tls = threading.local()
 
 
 def init(device: int = 0) -> None:
-    global _initialised
-    if not _initialised:
+    if not getattr(_tls, "initialised", False):
         check(lib().m3d_init(C.c_int(device), C.c_uint(0)), "m3d_init")
-        _initialised = True
+        _tls.initialised = True
+        _tls.stream = 0
+
+
+def free() -> None:
+    """Release the calling thread's context (m3d_free)."""
+    check(lib().m3d_free(), "m3d_free")
+    _tls.initialised = False
+    _tls.stream = 0
 
 
 def launch_count() -> int:
@@ -142,14 +152,10 @@ def synchronize() -> None:
     check(lib().m3d_synchronize(), "m3d_synchronize")
 
 
-_lib_stream = 0
-
-
 def set_stream(stream_ptr: int | None) -> None:
-    """Order the library's work on this CUDA stream (None: its own stream)."""
-    global _lib_stream
+    """Order the calling thread's library work on this CUDA stream (None: its own stream)."""
     check(lib().m3d_set_stream(C.c_void_p(stream_ptr or 0)), "m3d_set_stream")
-    _lib_stream = stream_ptr or 0
+    _tls.stream = stream_ptr or 0
 
 
 def order_after_torch(*arrays) -> None:
@@ -163,7 +169,7 @@ def order_after_torch(*arrays) -> None:
             # torch's default stream is the legacy one (handle 0), which the
             # library names by cudaStreamLegacy (0x1); 0 would select its own
             cur = cur if cur != 0 else 1
-            if cur != _lib_stream:
+            if cur != getattr(_tls, "stream", 0):
                 set_stream(cur)
             return
 

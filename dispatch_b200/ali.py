@@ -461,55 +461,3 @@ def cube_problem(kind: str = "small", seed: int = 2, nx: int = 8, ny: int = 8, n
 
 
 __all__ = ["AliParams", "AliWindow", "AliColumns", "cube_problem", "column_problem"]
-
-
-def _main(argv=None) -> None:
-    """python -m dispatch_b200.ali: run ALI iterations of a seeded problem and print
-    one line per iteration (the sweep and update times from CUDA events)."""
-    import argparse
-    import time
-
-    import torch
-
-    ap = argparse.ArgumentParser(description=_main.__doc__)
-    ap.add_argument("--problem", choices=["window", "columns"], default="window")
-    ap.add_argument("--n", type=int, default=64, help="cube edge (window)")
-    ap.add_argument("--ncol", type=int, default=1024, help="columns (columns)")
-    ap.add_argument("--nbound", type=int, default=20)
-    ap.add_argument("--nline", type=int, default=60)
-    ap.add_argument("--every", type=int, default=8, help="the window holds every k-th transition (window)")
-    ap.add_argument("--nwin", type=int, default=8, help="frequency windows (columns)")
-    ap.add_argument("--iters", type=int, default=2)
-    ap.add_argument("--no-graph", action="store_true")
-    a = ap.parse_args(argv)
-    t0 = time.time()
-    if a.problem == "window":
-        nrad = a.nline + a.nbound
-        cube, atom, win, vec, wts = cube_problem("small", nx=a.n, ny=a.n, nz=a.n, nbound=a.nbound, nline=a.nline,
-                                                 ntheta=4, nphi=4, transitions=list(range(0, nrad, a.every)))
-        A = AliWindow(cube, atom, win, vec, wts, params=AliParams(convlim=1e-9))
-    else:
-        cols, atom, wins, mu, wmu = column_problem(ncol=a.ncol, depth=(60, 256), nz=256, nxy=64, nbound=a.nbound,
-                                                   nline=a.nline, nwin=a.nwin)
-        A = AliColumns(cols, atom, wins, mu, wmu, params=AliParams(convlim=1e-9), use_graph=not a.no_graph)
-    torch.cuda.synchronize()
-    print(f"setup {time.time() - t0:.1f} s, {A.ncell} cells, {A.points():.3e} ray-point-frequencies per sweep",
-          flush=True)
-    cur = torch.cuda.current_stream()
-    A.sweep()
-    for _ in range(a.iters):
-        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
-        e[0].record(cur)
-        A.iter += 1
-        rec = A.update()
-        e[1].record(cur)
-        A.sweep()
-        e[2].record(cur)
-        torch.cuda.synchronize()
-        sw = e[1].elapsed_time(e[2])
-        print(f"iter {A.iter}: update {e[0].elapsed_time(e[1]):.1f} ms, sweep {sw:.1f} ms "
-              f"({A.points() / sw / 1e6:.2f} Gpt/s), maxerr {rec['maxerr']:.3e}", flush=True)
-
-
-if __name__ == "__main__":
-    _main()

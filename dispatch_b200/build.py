@@ -7,6 +7,7 @@ QLG tables and the rotation/stencil coefficients are formed on the host).
 """
 from __future__ import annotations
 
+import glob
 import os
 import shutil
 import subprocess
@@ -17,9 +18,12 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libm3dgpu.so")
 SOURCES = ["m3d_api.cu"]
-HEADERS = ["m3d_math.cuh", "m3d_qlg.cuh", "m3d_kernels.cuh", "m3d_pipeline.cuh", "m3d_stateq.cuh",
-           "m3d_stateq_api.inc", "m3d_nlte.cuh", "m3d_nlte_api.inc",
-           "m3d_aux.cuh", "m3d_aux_api.inc", "m3d_columns.cuh", "m3d_columns_api.inc"]
+
+
+def _deps() -> list[str]:
+    """Every file the library is built from: all of csrc/ and the public header."""
+    files = [f for f in glob.glob(os.path.join(CSRC, "*")) if os.path.isfile(f)]
+    return sorted(files) + [os.path.join(ROOT, "include", "m3dgpu.h")]
 
 
 def nvcc() -> str:
@@ -33,8 +37,7 @@ def _stale() -> bool:
     if not os.path.exists(LIB):
         return True
     t = os.path.getmtime(LIB)
-    deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS] + [os.path.join(ROOT, "include", "m3dgpu.h")]
-    return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
+    return any(os.path.getmtime(d) > t for d in _deps())
 
 
 def build(force: bool = False, verbose: bool = False) -> str:

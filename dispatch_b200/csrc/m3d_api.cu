@@ -9,6 +9,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <type_traits>
 #include <vector>
@@ -52,9 +53,21 @@ struct Ctx {
   std::vector<Rec> recs;
   double stage_ms[4] = {0, 0, 0, 0};
   long long stage_n[4] = {0, 0, 0, 0};
+  // device allocations this context has made (m3d_alloc_stats)
+  long long mallocs = 0;
 };
 
-Ctx g_ctx;
+// One context per host thread: a thread that calls m3d_init gets its own stream,
+// scratch and staging buffers, QLG tables, error string and counters, so slabs
+// handled by different host threads run concurrently on their own streams.
+thread_local Ctx g_ctx;
+
+// every device allocation of the library goes through here and is counted
+template <typename T>
+cudaError_t dev_malloc(T **p, size_t bytes) {
+  g_ctx.mallocs++;
+  return cudaMalloc(reinterpret_cast<void **>(p), bytes);
+}
 
 int fail(int code, const char *fmt, ...) {
   char buf[512];
@@ -120,7 +133,7 @@ int scratch(int slot, size_t bytes, void **out) {
       g_ctx.scratch[slot] = nullptr;
       g_ctx.scratch_bytes[slot] = 0;
     }
-    CUDA_TRY(cudaMalloc(&g_ctx.scratch[slot], bytes));
+    CUDA_TRY(dev_malloc(&g_ctx.scratch[slot], bytes));
     g_ctx.scratch_bytes[slot] = bytes;
   }
   *out = g_ctx.scratch[slot];
@@ -153,7 +166,7 @@ class Staging {
       }
       g_ctx.stage_buf[slot] = nullptr;
       g_ctx.stage_bytes[slot] = 0;
-      CUDA_TRY(cudaMalloc(&g_ctx.stage_buf[slot], b.bytes));
+      CUDA_TRY(dev_malloc(&g_ctx.stage_buf[slot], b.bytes));
       g_ctx.stage_bytes[slot] = b.bytes;
     }
     b.dptr = g_ctx.stage_buf[slot];
@@ -251,13 +264,13 @@ int ensure_tables() {
     g_ctx.h_tgx[i] = (float)pow(2.0, -x * x);
     g_ctx.h_th2x[i] = (float)z02_over_l2(x * x);
   }
-  CUDA_TRY(cudaMalloc(&g_ctx.d_tgx, 2 * QLG_NTAB * sizeof(float)));
+  CUDA_TRY(dev_malloc(&g_ctx.d_tgx, 2 * QLG_NTAB * sizeof(float)));
   g_ctx.d_th2x = g_ctx.d_tgx + QLG_NTAB;
   CUDA_TRY(cudaMemcpy(g_ctx.d_tgx, g_ctx.h_tgx.data(), QLG_NTAB * sizeof(float), cudaMemcpyHostToDevice));
   CUDA_TRY(cudaMemcpy(g_ctx.d_th2x, g_ctx.h_th2x.data(), QLG_NTAB * sizeof(float), cudaMemcpyHostToDevice));
   std::vector<float2> tab(QLG_NTAB);
   for (int i = 0; i < QLG_NTAB; i++) tab[i] = make_float2(g_ctx.h_tgx[i], g_ctx.h_th2x[i]);
-  CUDA_TRY(cudaMalloc(&g_ctx.d_tab, QLG_NTAB * sizeof(float2)));
+  CUDA_TRY(dev_malloc(&g_ctx.d_tab, QLG_NTAB * sizeof(float2)));
   CUDA_TRY(cudaMemcpy(g_ctx.d_tab, tab.data(), QLG_NTAB * sizeof(float2), cudaMemcpyHostToDevice));
   return M3D_OK;
 }
@@ -326,27 +339,32 @@ PchipConst pchip_const(float ds3_code) {
   return c;
 }
 
-// rotate_array coefficients of local planes 1..nz of a slab (rt_patch_mod.f90:3821-3841)
-void rot_planes(const double vec[3], const double ds_code[3], double bot2pivot, const double ray_offset[2], int nz,
-                RotPlane *out) {
+// rotate_array coefficients of local plane z of a slab (rt_patch_mod.f90:3821-3841).
+// rot_planes and the no-allocation rotation both take their weights from here.
+RotPlane rot_plane_at(const double vec[3], const double ds_code[3], double bot2pivot, const double ray_offset[2],
+                      int z) {
   const float delta0 = (float)(vec[0] / (vec[2] * ds_code[0]));
   const float delta1 = (float)(vec[1] / (vec[2] * ds_code[1]));
   const float b2p = (float)bot2pivot;
-  for (int z = 1; z <= nz; z++) {
-    const float height = (float)((double)z * ds_code[2]);
-    const float dk0 = (float)((double)((b2p - height) * delta0) + ray_offset[0]);
-    const float dk1 = (float)((double)((b2p - height) * delta1) + ray_offset[1]);
-    const int up1 = (int)floorf(dk0), up2 = (int)floorf(dk1);
-    const float f1 = dk0 - (float)up1, f2 = dk1 - (float)up2;
-    RotPlane r;
-    r.up1 = up1;
-    r.up2 = up2;
-    r.a = (1.0f - f1) * (1.0f - f2);
-    r.b = f1 * (1.0f - f2);
-    r.c = (1.0f - f1) * f2;
-    r.d = f1 * f2;
-    out[z - 1] = r;
-  }
+  const float height = (float)((double)z * ds_code[2]);
+  const float dk0 = (float)((double)((b2p - height) * delta0) + ray_offset[0]);
+  const float dk1 = (float)((double)((b2p - height) * delta1) + ray_offset[1]);
+  const int up1 = (int)floorf(dk0), up2 = (int)floorf(dk1);
+  const float f1 = dk0 - (float)up1, f2 = dk1 - (float)up2;
+  RotPlane r;
+  r.up1 = up1;
+  r.up2 = up2;
+  r.a = (1.0f - f1) * (1.0f - f2);
+  r.b = f1 * (1.0f - f2);
+  r.c = (1.0f - f1) * f2;
+  r.d = f1 * f2;
+  return r;
+}
+
+// the weights of local planes 1..nz
+void rot_planes(const double vec[3], const double ds_code[3], double bot2pivot, const double ray_offset[2], int nz,
+                RotPlane *out) {
+  for (int z = 1; z <= nz; z++) out[z - 1] = rot_plane_at(vec, ds_code, bot2pivot, ray_offset, z);
 }
 
 LineArgs line_args(const m3d_linelist_t *ll) {
@@ -449,6 +467,7 @@ int m3d_free(void) {
   if (g_ctx.own) cudaStreamDestroy(g_ctx.own);
   g_ctx.own = g_ctx.stream = nullptr;
   g_ctx.init = false;
+  g_ctx.mallocs = 0;
   return M3D_OK;
 }
 
@@ -478,6 +497,16 @@ int m3d_synchronize(void) {
 }
 
 long long m3d_launch_count(void) { return g_ctx.launches; }
+
+int m3d_alloc_stats(long long *mallocs, unsigned long long *scratch_bytes, unsigned long long *staging_bytes) {
+  unsigned long long sb = 0, tb = 0;
+  for (size_t b : g_ctx.scratch_bytes) sb += b;
+  for (size_t b : g_ctx.stage_bytes) tb += b;
+  if (mallocs) *mallocs = g_ctx.mallocs;
+  if (scratch_bytes) *scratch_bytes = sb;
+  if (staging_bytes) *staging_bytes = tb;
+  return M3D_OK;
+}
 
 int m3d_profile_enable(int on) {
   TRY(need_init());
@@ -613,7 +642,7 @@ int m3d_line_opacity_scat(const m3d_linelist_t *ll, int nf, const double *llam, 
   if (!(G.dllam > 0)) return fail(M3D_EINVAL, "m3d_line_opacity: log(lambda) grid must be ascending");
   const int block = 256, warps = block / 32;
   const size_t smem = 2 * QLG_NTAB * sizeof(float);
-  static bool attr = false;
+  thread_local bool attr = false;
   if (!attr) {
     CUDA_TRY(cudaFuncSetAttribute(k_line_opacity, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     attr = true;
@@ -786,7 +815,7 @@ int solve_impl(int solver, const m3d_slab_t *s, unsigned flags, T *work, T *psi,
       if (solver == M3D_SOLVER_SHORT_LINEAR) {
         const T dsup05 = (T)(0.5f * (float)dsup);
         const size_t smem = sizeof(T) * 3 * (SC_TX + 3) * (SC_TY + 3) * SC_TF;
-        static bool attr_set[2] = {false, false};
+        thread_local bool attr_set[2] = {false, false};
         if (!attr_set[sizeof(T) == 8]) {
           CUDA_TRY(cudaFuncSetAttribute(k_short_char_tile<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
           attr_set[sizeof(T) == 8] = true;
@@ -1214,7 +1243,7 @@ int m3d_lte_synthesis(const m3d_atmos_t *atm, int nf, const double *nu, const do
   const size_t smem_op = lane32 ? 2 * QLG_NTAB * sizeof(float)
                                 : (2 * QLG_NTAB + (size_t)warps * 4 * nf) * sizeof(float);
   {
-    static size_t attr[4] = {0, 0, 0, 0};
+    thread_local size_t attr[4] = {0, 0, 0, 0};
     const int which = (lane32 ? 2 : 0) + (fp64 ? 1 : 0);
     if (attr[which] < smem_op) {
       const void *fn = lane32 ? (fp64 ? (const void *)k_lte_opacity_units_lane<32, double, false>
@@ -1349,53 +1378,34 @@ int m3d_lte_synthesis(const m3d_atmos_t *atm, int nf, const double *nu, const do
 //
 // Some callers cannot let the library allocate device memory: a host program
 // that hands all device memory to its own pool (PyTorch's caching allocator, a
-// preallocated arena) leaves nothing for cudaMalloc, and a program that drives
-// the device from several host threads at once cannot afford the device-wide
-// synchronisation that cudaMalloc/cudaFree imply.  This entry point therefore
-// takes its scratch from a fixed array in the library's own device image,
-// M3D_NOALLOC_SCRATCH_BYTES (8 MiB) large, which every GPU that loads the
-// library holds until the process exits.  It rotates one plane at a time
-// through that array, so the limit is one plane, nf*nx*ny values.
+// preallocated arena) leaves nothing for cudaMalloc, and a program whose other
+// streams must not stall cannot afford the device-wide synchronisation that
+// cudaMalloc/cudaFree imply.  This entry point therefore takes its scratch from a
+// fixed array in the library's own device image, M3D_NOALLOC_SCRATCH_BYTES
+// (8 MiB) large, which every GPU that loads the library holds until the process
+// exits.  It rotates one plane at a time through that array, so the limit is one
+// plane, nf*nx*ny values.  The array is one per device, shared by every call and
+// every host thread's context: calls that overlap on the GPU race on it, so the
+// caller serialises them (one stream, or events between streams).
 // ===========================================================================
 namespace {
 
 constexpr size_t M3D_NOALLOC_SCRATCH_BYTES = (size_t)8 << 20;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[M3D_NOALLOC_SCRATCH_BYTES];
-// device address of g_noalloc_scratch, looked up once per device
-void *g_noalloc_addr[64] = {};
-
+// The device address of g_noalloc_scratch on the context's device.  The lookup
+// allocates nothing and is repeated on every call, so no address outlives a
+// device reset; the context's device is made current for it (and the caller's
+// current device restored), since the launches go to that device's stream.
 int noalloc_scratch(void **out) {
-  int dev = 0;
-  CUDA_TRY(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= 64) return fail(M3D_EUNSUPPORTED, "device %d: no-alloc scratch supports devices 0..63", dev);
-  if (!g_noalloc_addr[dev]) {
-    void *p = nullptr;
-    CUDA_TRY(cudaGetSymbolAddress(&p, g_noalloc_scratch));
-    g_noalloc_addr[dev] = p;
-  }
-  *out = g_noalloc_addr[dev];
+  int cur = 0;
+  CUDA_TRY(cudaGetDevice(&cur));
+  if (cur != g_ctx.device) CUDA_TRY(cudaSetDevice(g_ctx.device));
+  void *p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (cur != g_ctx.device) CUDA_TRY(cudaSetDevice(cur));
+  if (e != cudaSuccess) return fail(M3D_ECUDA, "cudaGetSymbolAddress(g_noalloc_scratch): %s", cudaGetErrorString(e));
+  *out = p;
   return M3D_OK;
-}
-
-// the rotate_array weights of local plane z, formed as rot_planes forms them
-RotPlane rot_plane_at(const double vec[3], const double ds_code[3], double bot2pivot, const double ray_offset[2],
-                      int z) {
-  const float delta0 = (float)(vec[0] / (vec[2] * ds_code[0]));
-  const float delta1 = (float)(vec[1] / (vec[2] * ds_code[1]));
-  const float b2p = (float)bot2pivot;
-  const float height = (float)((double)z * ds_code[2]);
-  const float dk0 = (float)((double)((b2p - height) * delta0) + ray_offset[0]);
-  const float dk1 = (float)((double)((b2p - height) * delta1) + ray_offset[1]);
-  const int up1 = (int)floorf(dk0), up2 = (int)floorf(dk1);
-  const float f1 = dk0 - (float)up1, f2 = dk1 - (float)up2;
-  RotPlane r;
-  r.up1 = up1;
-  r.up2 = up2;
-  r.a = (1.0f - f1) * (1.0f - f2);
-  r.b = f1 * (1.0f - f2);
-  r.c = (1.0f - f1) * f2;
-  r.d = f1 * f2;
-  return r;
 }
 
 // one plane of rotate_array into dst, the weights passed by value

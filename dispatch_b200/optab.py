@@ -105,49 +105,3 @@ class SampleOptab:
             import torch
             return torch.empty((ncell, nf), dtype=torch.float32, device="cuda")
         return np.empty((ncell, nf), np.float32)
-
-
-def _main():
-    """Command-line runner of the two samplers on a seeded cube, for timing and
-    profiling: python -m dispatch_b200.optab [--n 64] [--nf 256] [--iters 3]."""
-    import argparse
-
-    import torch
-
-    from . import synth
-    p = argparse.ArgumentParser()
-    p.add_argument("--n", type=int, default=64, help="cube edge")
-    p.add_argument("--nf", type=int, default=256, help="frequencies in the window (R = 1e5)")
-    p.add_argument("--iters", type=int, default=3)
-    p.add_argument("--only", choices=["sample", "ll"], default=None)
-    a = p.parse_args()
-    c = synth.optab_cells(7, a.n, a.n, a.n)
-    ncell = c["temp"].size
-    dev = lambda x: torch.from_numpy(np.ascontiguousarray(x)).cuda()
-    T, N, X, V = dev(c["temp"]), dev(c["ne"]), dev(c["chi500"]), dev(c["vproj"])
-    back = torch.empty((ncell, a.nf), dtype=torch.float32, device="cuda")
-    scat, xh, eh, cs = (torch.zeros_like(back) for _ in range(4))
-    lam_q, bg, ll = synth.window_tables(8, c["temp"], c["ne"], c["vproj"], nf=a.nf)
-    q = dev(lam_q)
-    for name, tab in (("sample", bg), ("ll", ll)):
-        if a.only and a.only != name:
-            continue
-        t = SampleOptab.from_dict(tab)
-        ts = []
-        for _ in range(a.iters):
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record()
-            if name == "sample":
-                t.interpolate(T, N, X, q, back, scat)
-            else:
-                t.interpolate_ll(T, N, X, xh, eh, q, V, cs)
-            e1.record()
-            torch.cuda.synchronize()
-            ts.append(e0.elapsed_time(e1))
-        print(f"{name}: {ncell} cells x {a.nf} frequencies, table {t.nnu} x {t.ntemp} x {t.nne}: "
-              f"{min(ts):.3f} ms, {ncell * a.nf / min(ts) / 1e6:.2f} Gpt*nu/s", flush=True)
-        t.close()
-
-
-if __name__ == "__main__":
-    _main()

@@ -18,7 +18,13 @@
  * array is a device pointer on the current device and the call is ordered on the
  * library stream (m3d_set_stream) and returns without synchronising.
  *
- * Thread safety: one process-wide context, not re-entrant, as libhop.
+ * Thread safety: one context per host thread.  Each thread that calls the library
+ * calls m3d_init first (and m3d_free before it exits); its context holds its own
+ * stream, scratch and staging buffers, QLG tables, error string and counters, so
+ * slabs handed to different host threads (the reference's OpenMP threads, one slab
+ * each) run concurrently on their own streams.  libhop itself is one process-wide
+ * instance; this library relaxes that.  Process-wide state: the loaded VCS tables
+ * (m3d_vcs_load, guarded by a lock) and the no-allocation scratch array below.
  */
 #ifndef M3DGPU_H
 #define M3DGPU_H
@@ -96,6 +102,13 @@ int m3d_set_stream(void *cuda_stream);        /* NULL: the library's own (non-bl
 int m3d_synchronize(void);
 /* Number of kernel launches the library has issued since m3d_init. */
 long long m3d_launch_count(void);
+
+/* Device allocations and cached bytes of the calling thread's context: the number
+ * of cudaMalloc calls the library has made for it, and the bytes its scratch and
+ * host-staging caches hold.  No counterpart in the reference (a test hook that shows
+ * which entry points allocate). */
+int m3d_alloc_stats(long long *mallocs, unsigned long long *scratch_bytes, unsigned long long *staging_bytes);
+
 /* Stage timing with CUDA events on the library stream (off by default).
  * Stages: 0 line opacity + transfer units, 1 formal solution (sweep), 2 intensity
  * reduction, 3 everything else.  m3d_profile_read synchronises and returns the
@@ -323,19 +336,21 @@ int m3d_save5(const char *run_dir, const char *label, const int *key, int nkey, 
 int m3d_rotate_array(const m3d_slab_t *slab, void *work, const double *ds_code, double bot2pivot,
                      const double *ray_offset, unsigned flags);
 
-/* m3d_rotate_array for callers that cannot let the library allocate device memory
- * (programs whose own pool holds all device memory, or that drive the device from
- * several host threads where cudaMalloc/cudaFree would stall the other streams).
+/* m3d_rotate_array for callers that cannot let the library allocate device memory:
+ * programs whose own pool holds all device memory, or whose other streams must not
+ * stall on the device-wide synchronisation of cudaMalloc/cudaFree.
  * It has no counterpart in the reference.  It allocates nothing: its scratch is one
  * fixed 8 MiB array inside the library's device image, held by every GPU that loads
  * the library until the process exits, so one plane (nf*nx*ny values of the chosen
  * precision) may use at most 8 MiB; larger slabs are rejected with M3D_EINVAL.
  * work must be a device pointer (M3D_DEVICE_PTRS is required; M3D_FP64 optional).
- * The first call on a device looks up the array's device address on that device
- * (cudaGetSymbolAddress); make that first call before any stream capture.  All
- * calls share the one array, so calls that overlap on the GPU (on different streams
- * at the same time) race; each call overwrites the scratch before reading it, so
- * nothing in it has to start at zero.  Results are bit-identical to m3d_rotate_array. */
+ * Every call looks up the array's device address on the context's device
+ * (cudaGetSymbolAddress, which allocates nothing); make the first call on a device
+ * before any stream capture.  The array is one per device, shared by all calls and
+ * all host threads' contexts: calls that overlap on the GPU (different streams or
+ * threads at the same time) race, so serialise them.  Each call overwrites the
+ * scratch before reading it, so nothing in it has to start at zero.  Results are
+ * bit-identical to m3d_rotate_array. */
 int m3d_rotate_array_noalloc(const m3d_slab_t *slab, void *work, const double *ds_code, double bot2pivot,
                              const double *ray_offset, unsigned flags);
 

@@ -118,8 +118,9 @@ def test_vcs_reads_the_reference_tables_when_present(oracle):
     series loads and every tabulated Balmer line gives a finite, positive profile."""
     import os
     from oracle import hprof as oh
-    d = "/root/reference/experiments/OpenMULTI3D/HOP/hopacity/data/vcs"
-    if not os.path.isdir(d):
+    ref = os.environ.get("M3D_REFERENCE_ROOT", "")   # the reference's experiments/OpenMULTI3D tree
+    d = os.path.join(ref, "HOP", "hopacity", "data", "vcs")
+    if not ref or not os.path.isdir(d):
         pytest.skip("the reference's VCS tables are not present")
     try:
         oh.vcs_load(1, os.path.join(d, "stehle_balmer.txt"), False)
