@@ -37,6 +37,7 @@ struct Ctx {
   cudaStream_t own = nullptr, stream = nullptr;
   float *d_tgx = nullptr, *d_th2x = nullptr;
   float2 *d_tab = nullptr;  // (TGX(i), TH2X(i)) interleaved, read by the kernels
+  double2 *d_tab64 = nullptr;  // the same two tables in fp64, for the plain FP64 opacity
   std::vector<float> h_tgx, h_th2x;
   long long launches = 0;
   std::string err;
@@ -272,6 +273,13 @@ int ensure_tables() {
   for (int i = 0; i < QLG_NTAB; i++) tab[i] = make_float2(g_ctx.h_tgx[i], g_ctx.h_th2x[i]);
   CUDA_TRY(dev_malloc(&g_ctx.d_tab, QLG_NTAB * sizeof(float2)));
   CUDA_TRY(cudaMemcpy(g_ctx.d_tab, tab.data(), QLG_NTAB * sizeof(float2), cudaMemcpyHostToDevice));
+  std::vector<double2> tab64(QLG_NTAB);
+  for (int i = 0; i < QLG_NTAB; i++) {
+    const double x = (double)i / 800.0;
+    tab64[i] = make_double2(pow(2.0, -x * x), z02_over_l2(x * x));
+  }
+  CUDA_TRY(dev_malloc(&g_ctx.d_tab64, QLG_NTAB * sizeof(double2)));
+  CUDA_TRY(cudaMemcpy(g_ctx.d_tab64, tab64.data(), QLG_NTAB * sizeof(double2), cudaMemcpyHostToDevice));
   return M3D_OK;
 }
 
@@ -464,6 +472,8 @@ int m3d_free(void) {
   g_ctx.d_tgx = g_ctx.d_th2x = nullptr;
   if (g_ctx.d_tab) cudaFree(g_ctx.d_tab);
   g_ctx.d_tab = nullptr;
+  if (g_ctx.d_tab64) cudaFree(g_ctx.d_tab64);
+  g_ctx.d_tab64 = nullptr;
   if (g_ctx.own) cudaStreamDestroy(g_ctx.own);
   g_ctx.own = g_ctx.stream = nullptr;
   g_ctx.init = false;
@@ -1121,14 +1131,189 @@ int m3d_upstream_boundary(const m3d_slab_t *slab, void *work, int mode, const vo
 // ---------------------------------------------------------------------------
 // LTE synthesis output pass of one window
 // ---------------------------------------------------------------------------
+}  // extern "C"
+
+namespace {
+
+// The atmosphere, line lists and window of the LTE pass on the device
+struct SynthIn {
+  AtmosDev A;
+  std::vector<SpeciesDev> sp;
+  bool reach = false;
+  unsigned *d_vmax = nullptr;
+  std::vector<int *> d_sel, d_nsel;
+  GridArgs G;
+  const double *dnu = nullptr, *dllam = nullptr;
+  int nf = 0;
+  size_t ncell = 0;
+};
+
+int stage_synthesis(Staging &st, const m3d_atmos_t *atm, int nf, const double *nu, const double *llam, bool fp64,
+                    const char *who, SynthIn *in) {
+  const int nx = atm->nx, ny = atm->ny, nz = atm->nz;
+  const size_t ncell = (size_t)nx * ny * nz;
+  if (ncell > (size_t)INT_MAX / 2) return fail(M3D_EUNSUPPORTED, "%s: %zu cells", who, ncell);
+  in->nf = nf;
+  in->ncell = ncell;
+  AtmosDev &A = in->A;
+  A.ncell = (int)ncell;
+  TRY(st.in(atm->temp, ncell, &A.temp)); TRY(st.in(atm->chi_c, ncell, &A.chi_c));
+  TRY(st.in(atm->vx, ncell, &A.vx)); TRY(st.in(atm->vy, ncell, &A.vy)); TRY(st.in(atm->vz, ncell, &A.vz));
+  TRY(st.in(atm->e_kT, ncell, &A.e_kT)); TRY(st.in(atm->ne, ncell, &A.ne));
+  TRY(st.in(atm->tothi, ncell, &A.tothi)); TRY(st.in(atm->stark_pe, ncell, &A.stark_pe));
+  if (!A.temp || !A.chi_c || !A.vx || !A.vy || !A.vz || !A.e_kT || !A.ne || !A.tothi || !A.stark_pe)
+    return fail(M3D_EINVAL, "%s: NULL atmosphere field", who);
+  A.maser_chi_floor = (float)atm->maser_chi_floor;
+  A.nspecies = atm->nspecies;
+  in->sp.assign(atm->nspecies > 0 ? atm->nspecies : 1, SpeciesDev{});
+  auto &sp = in->sp;
+  size_t nsel_all = 0;
+  for (int k = 0; k < atm->nspecies; k++) {
+    TRY(stage_linelist(st, &atm->species[k].ll, &sp[k].L));
+    TRY(st.in(atm->species[k].inv_df, ncell, &sp[k].inv_df));
+    TRY(st.in(atm->species[k].vbar2, ncell, &sp[k].vbar2));
+    TRY(st.in(atm->species[k].lnbase, ncell, &sp[k].lnbase));
+    if (sp[k].L.reach_in) in->reach = true;
+    nsel_all += (size_t)sp[k].L.nline + 8;
+  }
+  if (in->reach && fp64) return fail(M3D_EUNSUPPORTED, "%s: reach_in with the FP64 path", who);
+  // select_lines per ray: a vmax word, then per species its count and its list
+  in->d_sel.assign(sp.size(), nullptr);
+  in->d_nsel.assign(sp.size(), nullptr);
+  if (in->reach) {
+    for (int k = 0; k < atm->nspecies; k++)
+      if (!sp[k].L.reach_in) return fail(M3D_EINVAL, "%s: reach_in given for some species only", who);
+    void *sbuf = nullptr;
+    TRY(scratch(21, sizeof(int) * (nsel_all + 8), &sbuf));
+    in->d_vmax = (unsigned *)sbuf;
+    int *p = (int *)sbuf + 8;
+    for (int k = 0; k < atm->nspecies; k++) {
+      in->d_nsel[k] = p;
+      in->d_sel[k] = p + 8;
+      p += sp[k].L.nline + 8;
+      sp[k].L.sel = in->d_sel[k];
+      sp[k].L.nsel = in->d_nsel[k];
+    }
+  }
+  void *dsp;
+  TRY(scratch(4, sizeof(SpeciesDev) * sp.size(), &dsp));
+  CUDA_TRY(cudaMemcpyAsync(dsp, sp.data(), sizeof(SpeciesDev) * sp.size(), cudaMemcpyHostToDevice, g_ctx.stream));
+  A.species = (const SpeciesDev *)dsp;
+  TRY(st.in(nu, nf, &in->dnu));
+  TRY(st.in(llam, nf, &in->dllam));
+  in->G = grid_args(nf, llam, in->dllam, st.device(), (float)atm->tol, 0.0f);
+  if (!(in->G.dllam > 0)) return fail(M3D_EINVAL, "%s: log(lambda) grid must be ascending", who);
+  return M3D_OK;
+}
+
+// Line opacity + transfer units of every cell for direction v: (chi, S) of the
+// window, frequency fastest per cell.  FP32: the lane-per-cell kernel for windows of
+// 32 frequencies, the warp-per-cell kernel otherwise; FP64: the plain FP64 kernel.
+int launch_opacity(SynthIn &in, const double *v, bool fp64, void *dchi, void *dS) {
+  const int nf = in.nf;
+  const size_t ncell = in.ncell;
+  const int block = 256, warps = block / 32;
+  if (fp64) {
+    int grid = (int)((ncell + block - 1) / block);
+    if (grid > 148 * 8) grid = 148 * 8;
+    if (nf == 32)
+      LAUNCH_S(M3D_STAGE_OPACITY, k_lte_opacity_units_f64<32>, grid, block, 0, in.A, in.G, in.dnu, v[0], v[1], v[2],
+               (double *)dchi, (double *)dS, (const double2 *)g_ctx.d_tab64);
+    else
+      LAUNCH_S(M3D_STAGE_OPACITY, k_lte_opacity_units_f64<0>, grid, block, 0, in.A, in.G, in.dnu, v[0], v[1], v[2],
+               (double *)dchi, (double *)dS, (const double2 *)g_ctx.d_tab64);
+    return M3D_OK;
+  }
+  const bool lane32 = nf == 32;
+  const size_t smem_op = lane32 ? 2 * QLG_NTAB * sizeof(float)
+                                : (2 * QLG_NTAB + (size_t)warps * 4 * nf) * sizeof(float);
+  {
+    thread_local size_t attr[2] = {0, 0};
+    const int which = lane32 ? 1 : 0;
+    if (attr[which] < smem_op) {
+      if (lane32) {
+        CUDA_TRY(cudaFuncSetAttribute((const void *)k_lte_opacity_units_lane<32, float, false>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_op));
+        CUDA_TRY(cudaFuncSetAttribute((const void *)k_lte_opacity_units_lane<32, float, true>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_op));
+      } else {
+        CUDA_TRY(cudaFuncSetAttribute((const void *)k_lte_opacity_units<float>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_op));
+      }
+      attr[which] = smem_op;
+    }
+  }
+  if (in.reach) {
+    CUDA_TRY(cudaMemsetAsync(in.d_vmax, 0, sizeof(unsigned), g_ctx.stream));
+    LAUNCH(k_vproj_absmax, grid_for(ncell), 256, 0, in.A, v[0], v[1], v[2], in.d_vmax);
+    for (int k = 0; k < in.A.nspecies; k++)
+      LAUNCH(k_select_lines, 1, 32, 0, in.sp[k].L, in.dllam, nf, (const unsigned *)in.d_vmax, in.d_sel[k],
+             in.d_nsel[k]);
+  }
+  if (lane32) {
+    // lane kernel: one warp per 32 cells, grid-stride over warps
+    int lgrid = (int)((ncell + block - 1) / block);
+    if (lgrid > 148 * 3 * 8) lgrid = 148 * 3 * 8;
+    if (in.reach)
+      LAUNCH_S(M3D_STAGE_OPACITY, (k_lte_opacity_units_lane<32, float, true>), lgrid, block, smem_op, in.A, in.G,
+               in.dnu, v[0], v[1], v[2], (float *)dchi, (float *)dS, g_ctx.d_tab);
+    else
+      LAUNCH_S(M3D_STAGE_OPACITY, (k_lte_opacity_units_lane<32, float, false>), lgrid, block, smem_op, in.A, in.G,
+               in.dnu, v[0], v[1], v[2], (float *)dchi, (float *)dS, g_ctx.d_tab);
+  } else {
+    int ogrid = (int)((ncell + warps - 1) / warps);
+    if (ogrid > 148 * 16) ogrid = 148 * 16;
+    LAUNCH_S(M3D_STAGE_OPACITY, k_lte_opacity_units<float>, ogrid, block, smem_op, in.A, in.G, in.dnu, v[0], v[1],
+             v[2], (float *)dchi, (float *)dS, g_ctx.d_tab);
+  }
+  return M3D_OK;
+}
+
+int check_synthesis_args(const m3d_atmos_t *atm, int nf, const char *who) {
+  if (nf < 2) return fail(M3D_EINVAL, "%s: need nf >= 2", who);
+  if (nf > 1024) return fail(M3D_EUNSUPPORTED, "%s: nf = %d > 1024 per window", who, nf);
+  if (atm->nx < 1 || atm->ny < 1 || atm->nz < 1) return fail(M3D_EINVAL, "%s: bad atmosphere shape", who);
+  return M3D_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int m3d_lte_transfer_units(const m3d_atmos_t *atm, int nf, const double *nu, const double *llam, const double *vec,
+                           void *chi, void *S, unsigned flags) {
+  TRY(need_init());
+  if (!atm || !nu || !llam || !vec || !chi || !S) return fail(M3D_EINVAL, "m3d_lte_transfer_units: NULL argument");
+  TRY(check_synthesis_args(atm, nf, "m3d_lte_transfer_units"));
+  const bool fp64 = flags & M3D_FP64;
+  Staging st(flags);
+  SynthIn in;
+  TRY(stage_synthesis(st, atm, nf, nu, llam, fp64, "m3d_lte_transfer_units", &in));
+  const size_t n = (size_t)nf * in.ncell;
+  void *dchi, *dS;
+  if (fp64) {
+    double *a, *b;
+    TRY(st.map((double *)chi, n, false, true, &a));
+    TRY(st.map((double *)S, n, false, true, &b));
+    dchi = a; dS = b;
+  } else {
+    float *a, *b;
+    TRY(st.map((float *)chi, n, false, true, &a));
+    TRY(st.map((float *)S, n, false, true, &b));
+    dchi = a; dS = b;
+  }
+  TRY(launch_opacity(in, vec, fp64, dchi, dS));
+  return st.finish();
+}
+
 int m3d_lte_synthesis(const m3d_atmos_t *atm, int nf, const double *nu, const double *llam, int nray,
                       const double *vec, const double *wmu, void *i_top, float *ie, float *flux, unsigned flags) {
   TRY(need_init());
   if (!atm || !nu || !llam || !vec || !wmu || !ie || !flux) return fail(M3D_EINVAL, "m3d_lte_synthesis: NULL argument");
-  if (nf < 2 || nray < 1) return fail(M3D_EINVAL, "m3d_lte_synthesis: need nf >= 2 and nray >= 1");
-  if (nf > 1024) return fail(M3D_EUNSUPPORTED, "m3d_lte_synthesis: nf = %d > 1024 per window", nf);
+  if (nray < 1) return fail(M3D_EINVAL, "m3d_lte_synthesis: need nray >= 1");
+  TRY(check_synthesis_args(atm, nf, "m3d_lte_synthesis"));
   const int nx = atm->nx, ny = atm->ny, nz = atm->nz;
-  if (nx < 1 || ny < 1 || nz < 2 || atm->nslab < 1 || !atm->slab_nz) return fail(M3D_EINVAL, "m3d_lte_synthesis: bad atmosphere shape");
+  if (nz < 2 || atm->nslab < 1 || !atm->slab_nz) return fail(M3D_EINVAL, "m3d_lte_synthesis: bad atmosphere shape");
   std::vector<int> z0(atm->nslab + 1, 0);
   for (int s = 0; s < atm->nslab; s++) {
     if (atm->slab_nz[s] < 2) return fail(M3D_EINVAL, "slab %d has %d < 2 planes", s, atm->slab_nz[s]);
@@ -1138,60 +1323,13 @@ int m3d_lte_synthesis(const m3d_atmos_t *atm, int nf, const double *nu, const do
   for (int r = 0; r < nray; r++)
     if (!(vec[3 * r + 2] > 0)) return fail(M3D_EINVAL, "ray %d is not upward (vec(3) <= 0)", r);
   const bool fp64 = flags & M3D_FP64;
-  const size_t ncell = (size_t)nx * ny * nz;
   const size_t ncol = (size_t)nx * ny;
   const size_t plane = (size_t)nf * ncol;
 
   Staging st(flags);
-  AtmosDev A;
-  A.ncell = (int)ncell;
-  TRY(st.in(atm->temp, ncell, &A.temp)); TRY(st.in(atm->chi_c, ncell, &A.chi_c));
-  TRY(st.in(atm->vx, ncell, &A.vx)); TRY(st.in(atm->vy, ncell, &A.vy)); TRY(st.in(atm->vz, ncell, &A.vz));
-  TRY(st.in(atm->e_kT, ncell, &A.e_kT)); TRY(st.in(atm->ne, ncell, &A.ne));
-  TRY(st.in(atm->tothi, ncell, &A.tothi)); TRY(st.in(atm->stark_pe, ncell, &A.stark_pe));
-  if (!A.temp || !A.chi_c || !A.vx || !A.vy || !A.vz || !A.e_kT || !A.ne || !A.tothi || !A.stark_pe)
-    return fail(M3D_EINVAL, "m3d_lte_synthesis: NULL atmosphere field");
-  A.maser_chi_floor = (float)atm->maser_chi_floor;
-  A.nspecies = atm->nspecies;
-  std::vector<SpeciesDev> sp(atm->nspecies > 0 ? atm->nspecies : 1);
-  bool reach = false;
-  size_t nsel_all = 0;
-  for (int k = 0; k < atm->nspecies; k++) {
-    TRY(stage_linelist(st, &atm->species[k].ll, &sp[k].L));
-    TRY(st.in(atm->species[k].inv_df, ncell, &sp[k].inv_df));
-    TRY(st.in(atm->species[k].vbar2, ncell, &sp[k].vbar2));
-    TRY(st.in(atm->species[k].lnbase, ncell, &sp[k].lnbase));
-    if (sp[k].L.reach_in) reach = true;
-    nsel_all += (size_t)sp[k].L.nline + 8;
-  }
-  if (reach && fp64) return fail(M3D_EUNSUPPORTED, "m3d_lte_synthesis: reach_in with the FP64 path");
-  // select_lines per ray: a vmax word, then per species its count and its list
-  unsigned *d_vmax = nullptr;
-  std::vector<int *> d_sel(sp.size(), nullptr), d_nsel(sp.size(), nullptr);
-  if (reach) {
-    for (int k = 0; k < atm->nspecies; k++)
-      if (!sp[k].L.reach_in) return fail(M3D_EINVAL, "m3d_lte_synthesis: reach_in given for some species only");
-    void *sbuf = nullptr;
-    TRY(scratch(21, sizeof(int) * (nsel_all + 8), &sbuf));
-    d_vmax = (unsigned *)sbuf;
-    int *p = (int *)sbuf + 8;
-    for (int k = 0; k < atm->nspecies; k++) {
-      d_nsel[k] = p;
-      d_sel[k] = p + 8;
-      p += sp[k].L.nline + 8;
-      sp[k].L.sel = d_sel[k];
-      sp[k].L.nsel = d_nsel[k];
-    }
-  }
-  void *dsp;
-  TRY(scratch(4, sizeof(SpeciesDev) * sp.size(), &dsp));
-  CUDA_TRY(cudaMemcpyAsync(dsp, sp.data(), sizeof(SpeciesDev) * sp.size(), cudaMemcpyHostToDevice, g_ctx.stream));
-  A.species = (const SpeciesDev *)dsp;
-  const double *dnu, *dllam;
-  TRY(st.in(nu, nf, &dnu));
-  TRY(st.in(llam, nf, &dllam));
-  GridArgs G = grid_args(nf, llam, dllam, st.device(), (float)atm->tol, 0.0f);
-  if (!(G.dllam > 0)) return fail(M3D_EINVAL, "m3d_lte_synthesis: log(lambda) grid must be ascending");
+  SynthIn in;
+  TRY(stage_synthesis(st, atm, nf, nu, llam, fp64, "m3d_lte_synthesis", &in));
+  const double *dnu = in.dnu;
 
   // rotation table of every global plane, per ray; slab starts
   // A single column is a plane-parallel atmosphere: radiative_transfer applies no
@@ -1237,30 +1375,6 @@ int m3d_lte_synthesis(const m3d_atmos_t *atm, int nf, const double *nu, const do
   float *die;
   TRY(st.map(ie, (size_t)nf * nray, false, true, &die));
 
-  const int block = 256, warps = block / 32;
-  // windows of 32 frequencies take the lane-per-cell kernel, others the warp-per-cell one
-  const bool lane32 = nf == 32;
-  const size_t smem_op = lane32 ? 2 * QLG_NTAB * sizeof(float)
-                                : (2 * QLG_NTAB + (size_t)warps * 4 * nf) * sizeof(float);
-  {
-    thread_local size_t attr[4] = {0, 0, 0, 0};
-    const int which = (lane32 ? 2 : 0) + (fp64 ? 1 : 0);
-    if (attr[which] < smem_op) {
-      const void *fn = lane32 ? (fp64 ? (const void *)k_lte_opacity_units_lane<32, double, false>
-                                      : (const void *)k_lte_opacity_units_lane<32, float, false>)
-                              : (fp64 ? (const void *)k_lte_opacity_units<double> : (const void *)k_lte_opacity_units<float>);
-      CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_op));
-      if (lane32 && !fp64)
-        CUDA_TRY(cudaFuncSetAttribute((const void *)k_lte_opacity_units_lane<32, float, true>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_op));
-      attr[which] = smem_op;
-    }
-  }
-  int ogrid = (int)((ncell + warps - 1) / warps);
-  if (ogrid > 148 * 16) ogrid = 148 * 16;
-  // lane kernel: one warp per 32 cells, grid-stride over warps
-  int lgrid = (int)((ncell + block - 1) / block);
-  if (lgrid > 148 * 3 * 8) lgrid = 148 * 3 * 8;
   const float dtmax = -(float)atm->maser_dtau_max, Imax = (float)atm->maser_Inu_max;
   const PchipConst pc = pchip_const((float)atm->ds_code[2]);
 
@@ -1280,22 +1394,8 @@ int m3d_lte_synthesis(const m3d_atmos_t *atm, int nf, const double *nu, const do
 
   for (int r = 0; r < nray; r++) {
     const double *v = vec + 3 * r;
+    TRY(launch_opacity(in, v, fp64, dchi, dS));
     if (!fp64) {
-      if (reach) {
-        CUDA_TRY(cudaMemsetAsync(d_vmax, 0, sizeof(unsigned), g_ctx.stream));
-        LAUNCH(k_vproj_absmax, grid_for(ncell), 256, 0, A, v[0], v[1], v[2], d_vmax);
-        for (int k = 0; k < atm->nspecies; k++)
-          LAUNCH(k_select_lines, 1, 32, 0, sp[k].L, dllam, nf, (const unsigned *)d_vmax, d_sel[k], d_nsel[k]);
-      }
-      if (reach && lane32)
-        LAUNCH_S(M3D_STAGE_OPACITY, (k_lte_opacity_units_lane<32, float, true>), lgrid, block, smem_op, A, G, dnu, v[0],
-                 v[1], v[2], (float *)dchi, (float *)dS, g_ctx.d_tab);
-      else if (lane32)
-        LAUNCH_S(M3D_STAGE_OPACITY, (k_lte_opacity_units_lane<32, float, false>), lgrid, block, smem_op, A, G, dnu, v[0],
-                 v[1], v[2], (float *)dchi, (float *)dS, g_ctx.d_tab);
-      else
-        LAUNCH_S(M3D_STAGE_OPACITY, k_lte_opacity_units<float>, ogrid, block, smem_op, A, G, dnu, v[0], v[1], v[2],
-                 (float *)dchi, (float *)dS, g_ctx.d_tab);
       const QuadConst qc = quad_const(atm->ds_cm[2], v[2]);
       LAUNCH_S(M3D_STAGE_SOLVE, k_quad_rot_column, (int)((plane + 255) / 256), 256, 0, nf, nx, ny, nz, (const float *)dchi, (const float *)dS, (const RotCol *)drot + (size_t)r * nz,
              (const int *)dz0, atm->nslab, qc, pc, dtmax, Imax, (float *)dtop + plane * r);
@@ -1304,12 +1404,6 @@ int m3d_lte_synthesis(const m3d_atmos_t *atm, int nf, const double *nu, const do
       LAUNCH_S(M3D_STAGE_REDUCE, k_save_final, (nf + 127) / 128, 128, 0, nf, (int)ncol, kParts, (const double *)dpart,
                die + (size_t)nf * r);
     } else {
-      if (lane32)
-        LAUNCH_S(M3D_STAGE_OPACITY, (k_lte_opacity_units_lane<32, double, false>), lgrid, block, smem_op, A, G, dnu,
-                 v[0], v[1], v[2], (double *)dchi, (double *)dS, g_ctx.d_tab);
-      else
-        LAUNCH_S(M3D_STAGE_OPACITY, k_lte_opacity_units<double>, ogrid, block, smem_op, A, G, dnu, v[0], v[1], v[2],
-                 (double *)dchi, (double *)dS, g_ctx.d_tab);
       for (int s = 0; s < atm->nslab; s++) {
         const int n = atm->slab_nz[s];
         m3d_slab_t sl;

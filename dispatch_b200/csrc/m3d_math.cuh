@@ -202,6 +202,48 @@ __device__ __forceinline__ void parab_moments(double t, double &E, double &U0, d
   }
 }
 
+// ---- packed FP32 pairs (sm_100's f32x2 add/mul/fma) ------------------------
+// Each half is rounded exactly as the scalar instruction rounds it (IEEE, round to
+// nearest even unless the name says otherwise), so a pair evaluation is bit-identical
+// to two scalar ones; it takes one issue slot instead of two.
+typedef unsigned long long f32x2;
+
+__device__ __forceinline__ f32x2 pk2(float lo, float hi) {
+  f32x2 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ void up2(f32x2 v, float &lo, float &hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ f32x2 add2(f32x2 a, f32x2 b) {
+  f32x2 r;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+// a + b rounded toward zero
+__device__ __forceinline__ f32x2 add2_rz(f32x2 a, f32x2 b) {
+  f32x2 r;
+  asm("add.rz.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ f32x2 sub2(f32x2 a, f32x2 b) {
+  f32x2 r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ f32x2 mul2(f32x2 a, f32x2 b) {
+  f32x2 r;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ f32x2 fma2(f32x2 a, f32x2 b, f32x2 c) {
+  f32x2 r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+  return r;
+}
+__device__ __forceinline__ f32x2 splat2(float v) { return pk2(v, v); }
+
 template <typename T> __device__ __forceinline__ T tiny_of();
 template <> __device__ __forceinline__ float tiny_of<float>() { return FLT_MIN; }
 template <> __device__ __forceinline__ double tiny_of<double>() { return DBL_MIN; }

@@ -190,6 +190,118 @@ __device__ __forceinline__ void deposit_window(float (&chl)[NF], const float2 *s
   }
 }
 
+// The same deposit, two window points per instruction (packed f32x2 arithmetic,
+// each half rounded as the scalar form rounds it), for windows whose every 1 + xs^2
+// is below 2^126 (the Markstein reciprocal).  Three exact rewrites beside the packing:
+//  * xs is formed with its sign, x ih; only xs^2 and |xs| are used, and the rounded
+//    product is symmetric in the sign;
+//  * -(1 + u) is formed as -1 - u (the rounding is symmetric), which is the -d of
+//    the Newton step, and the approximate reciprocal is taken of its negation;
+//  * the snapped node nint(min(|xs| 800, 9019)) is floor(RZ(y + 0.5)): rounding
+//    toward zero never carries a positive sum past the integer below it, so this is
+//    round-half-up of y >= 0, i.e. nint, with no special case below y = 0.5.  Adding
+//    2^23 toward zero then leaves that integer in the low mantissa bits, so the
+//    node's shared-memory address is one shift-add from the sum's bits.
+// Points outside a partial window add +0; the running sum is never -0 (it starts at
+// +0, and in round-to-nearest a sum is -0 only when both terms are), so adding +0
+// leaves it unchanged, exactly as skipping the point does.
+__device__ __forceinline__ float rcp_approx(float d) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(d));
+  return r;
+}
+
+__device__ __forceinline__ float2 lds_node(unsigned addr) {
+  float2 v;
+  asm volatile("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(addr));
+  return v;
+}
+
+template <int NF, bool FULL, bool FAR>
+__device__ __forceinline__ void deposit_window_x2(float (&chl)[NF], const float2 *s_tab, const QlgCoef &cf,
+                                                  float x0, float kfa, int fa, int fb) {
+  static_assert(NF % 2 == 0, "pairs of window points");
+  const f32x2 X0 = splat2(x0), IH = splat2(cf.ih), M1 = splat2(-1.0f), ONE = splat2(1.0f), BL = splat2(cf.bL);
+  const f32x2 KF = splat2(kfa);
+  f32x2 P1 = 0, GG = 0, CZH = 0, CL2 = 0, GGc = 0;
+  unsigned base = 0;
+  if (FAR) {
+    const float2 gw = s_tab[QLG_NTAB - 1];
+    P1 = splat2(fmaf(cf.cZH, gw.y, cf.cL2));
+    GG = splat2(gw.x * cf.gG);
+  } else {
+    CZH = splat2(cf.cZH);
+    CL2 = splat2(cf.cL2);
+    GGc = splat2(cf.gG);
+    // node i sits at byte 8 i; the sum's bits are 0x4B000000 + i
+    base = (unsigned)__cvta_generic_to_shared(s_tab) - (0x4B000000u << 3);
+  }
+#pragma unroll
+  for (int k = 0; k < NF / 2; k++) {
+    f32x2 F = pk2((float)(2 * k), (float)(2 * k + 1));
+    if (!FULL) F = add2(F, KF);  // (float)f + kfa, exact
+    const f32x2 x = add2(X0, F);
+    const f32x2 xs = mul2(x, IH);
+    const f32x2 u = mul2(xs, xs);
+    const f32x2 nd = sub2(M1, u);
+    float nda, ndb;
+    up2(nd, nda, ndb);
+    const f32x2 r = pk2(rcp_approx(-nda), rcp_approx(-ndb));
+    const f32x2 e = fma2(nd, r, ONE);
+    const f32x2 L = fma2(r, e, r);
+    f32x2 K;
+    if (FAR) {
+      K = fma2(L, fma2(L, P1, BL), GG);
+    } else {
+      float xa, xb;
+      up2(xs, xa, xb);
+      const f32x2 y = pk2(fminf(fabsf(xa) * 800.0f, 9019.0f), fminf(fabsf(xb) * 800.0f, 9019.0f));
+      const f32x2 v = add2_rz(add2_rz(y, splat2(0.5f)), splat2(8388608.0f));
+      float va, vb;
+      up2(v, va, vb);
+      const float2 ga = lds_node(base + (__float_as_uint(va) << 3));
+      const float2 gb = lds_node(base + (__float_as_uint(vb) << 3));
+      f32x2 p = fma2(CZH, pk2(ga.y, gb.y), CL2);
+      p = fma2(L, p, BL);
+      K = fma2(L, p, mul2(pk2(ga.x, gb.x), GGc));
+    }
+    if (!FULL) {
+      float ka, kb;
+      up2(K, ka, kb);
+      ka = (2 * k + 1 >= fa && 2 * k + 1 <= fb) ? ka : 0.0f;
+      kb = (2 * k + 2 >= fa && 2 * k + 2 <= fb) ? kb : 0.0f;
+      K = pk2(ka, kb);
+    }
+    float lo, hi;
+    up2(add2(K, pk2(chl[2 * k], chl[2 * k + 1])), lo, hi);
+    chl[2 * k] = lo;
+    chl[2 * k + 1] = hi;
+  }
+}
+
+template <int NF>
+__device__ __forceinline__ void deposit_window_mk(float (&chl)[NF], const float2 *s_tab, const QlgCoef &cf, float x0,
+                                                  float kfa, int fa, int fb, bool full, bool far) {
+  if (far) {
+    if (full) deposit_window_x2<NF, true, true>(chl, s_tab, cf, x0, kfa, fa, fb);
+    else deposit_window_x2<NF, false, true>(chl, s_tab, cf, x0, kfa, fa, fb);
+  } else {
+    if (full) deposit_window_x2<NF, true, false>(chl, s_tab, cf, x0, kfa, fa, fb);
+    else deposit_window_x2<NF, false, false>(chl, s_tab, cf, x0, kfa, fa, fb);
+  }
+}
+
+// lround of a double (half away from zero) for |x| < 2^31: floor(|x| + 0.5) with the
+// sum rounded toward zero, which never reaches the next integer below the exact sum
+// (an integer below 2^53 is representable), so it is exact; the conversion truncates.
+__device__ __forceinline__ int lround_d(double x) {
+  const int m = __double2int_rz(__dadd_rz(fabs(x), 0.5));
+  return x < 0.0 ? -m : m;
+}
+
+// lroundf of v >= 0, the same way in float (above 2^23 v is an integer and stays)
+__device__ __forceinline__ int lround_pos(float v) { return __float2int_rz(__fadd_rz(v, 0.5f)); }
+
 template <int NF>
 __device__ __forceinline__ float pick(const float (&a)[NF], int i) {
   float v = a[0];
@@ -227,6 +339,7 @@ __global__ void __launch_bounds__(256, 3) k_lte_opacity_units_lane(AtmosDev A, G
     const float x_lo = point_xhat(chi_c, h_kT, nu[0]), x_hi = point_xhat(chi_c, h_kT, nu[NF - 1]);
     const float lr_lo = x_lo > 0.0f ? lt + logf_m3d(x_lo) : -FLT_MAX;
     const float lr_hi = x_hi > 0.0f ? lt + logf_m3d(x_hi) : -FLT_MAX;
+    const double llam_hi = G.llam[NF - 1];
     for (int sp = 0; sp < A.nspecies; sp++) {
       const SpeciesDev &Sd = A.species[sp];
       const LineArgs &L = Sd.L;
@@ -238,31 +351,32 @@ __global__ void __launch_bounds__(256, 3) k_lte_opacity_units_lane(AtmosDev A, G
       for (int s = 0; s < nline; s++) {
         const int l = REACH ? L.sel[s] : s;
         if (L.active && !L.active[l]) continue;
-        const double llc = L.llam0[l] - (double)vproj;
-        const double pos = (llc - G.llam1) * G.inv_dllam;
-        const int ic = (int)lround(pos) + 1;
-        const int f0 = ic < 1 ? 1 : (ic > NF ? NF : ic);
         const float ex = L.lower_ev[l] * ekt;
         const float arg = (base + L.gpref[l]) - ex;
         if (arg < ex_cutoff) continue;
-        float cont0, lr0;
-        if (f0 == 1) { cont0 = x_lo; lr0 = lr_lo; }
-        else if (f0 == NF) { cont0 = x_hi; lr0 = lr_hi; }
+        const double llc = L.llam0[l] - (double)vproj;
+        const double pos = (llc - G.llam1) * G.inv_dllam;
+        const int ic = lround_d(pos) + 1;
+        const int f0 = ic < 1 ? 1 : (ic > NF ? NF : ic);
+        // the nearest node's xhat, its log and the line opacity there: a line centred
+        // outside the window -- nearly all of them -- lands on an edge, whose values
+        // are at hand; an interior node forms them (one branch, taken rarely)
+        float cont0, lr0, chl0;
+        if (f0 == 1) { cont0 = x_lo; lr0 = lr_lo; chl0 = chl[0]; }
+        else if (f0 == NF) { cont0 = x_hi; lr0 = lr_hi; chl0 = chl[NF - 1]; }
         else {
           cont0 = point_xhat(chi_c, h_kT, nu[f0 - 1]);
           lr0 = cont0 > 0.0f ? lt + logf_m3d(cont0) : -FLT_MAX;
+          chl0 = pick<NF>(chl, f0 - 1);
         }
         float refl = G.tol * cont0;
         float lref, cap = FLT_MAX;
-        const bool outside = REACH && (llc < G.llam[0] || llc > G.llam[NF - 1]);
+        const bool outside = REACH && (llc < G.llam[0] || llc > llam_hi);
         if (outside) {
           lref = lr0;
           if (arg <= lref) continue;
           cap = (float)((double)L.reach_in[l] * G.inv_dllam);
         } else {
-          // chi_l at f0: a line centred outside the window -- nearly all of them --
-          // lands on an edge, read directly instead of through the select chain
-          const float chl0 = f0 == 1 ? chl[0] : (f0 == NF ? chl[NF - 1] : pick<NF>(chl, f0 - 1));
           const float flo = G.flo_scale * chl0;
           if (flo > refl) { refl = flo; lref = logf_m3d(flo * sqrt_pi); }
           else lref = lr0;
@@ -272,10 +386,13 @@ __global__ void __launch_bounds__(256, 3) k_lte_opacity_units_lane(AtmosDev A, G
         if (!outside && voigt_peak * Rij <= refl) continue;
         const float a = line_damping_a(L, l, unsold_c, lvb2, tothi, ne, starkpe) * G.sdl;
         const float S = Rij * qw.D;
-        const float x1 = (float)((G.llam[f0 - 1] - llc) * G.inv_dllam);
+        // (llam(f0) - llc)/dllam; at f0 = 1 it is -pos exactly (the rounded difference
+        // and product are odd in their sign)
+        const float x1 = f0 == 1 ? (float)(-pos)
+                                 : (float)(((f0 == NF ? llam_hi : G.llam[f0 - 1]) - llc) * G.inv_dllam);
         const QlgCoef cf = qlg_setup(a, qw.D, qw.SQ, S);
         const float hw = qlg_halfwidth(qw, a, S, refl, arg - lref);
-        const int noff = (int)lroundf(fminf(fminf(hw, cap), (float)(NF + abs(ic))));
+        const int noff = lround_pos(fminf(fminf(hw, cap), (float)(NF + abs(ic))));
         const int fa = ic - noff > 1 ? ic - noff : 1;
         const int fb = ic + noff < NF ? ic + noff : NF;
         if (fa > fb) continue;
@@ -330,6 +447,170 @@ __global__ void __launch_bounds__(256, 3) k_lte_opacity_units_lane(AtmosDev A, G
           reinterpret_cast<double2 *>(so + f)[1] = make_double2(s4[2], s4[3]);
         }
       }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// The plain FP64 path of the same pass: the line opacity, the QLG-bot profile and
+// the transfer units all in double.  One lane per cell, chi_l of the window in
+// double registers, the general window form (per-point predicates) for every line.
+// The algorithm is the FP32 pass's step for step; what changes is the arithmetic:
+//  * the tables TGX = 2^-u and TH2X = Z_0.2(u)(1+u)^2 are the fp64 values of
+//    qlg_init's formulas (not rounded to float), read from global memory;
+//  * the QLG-bot constants are the exact values the fitted float parameters stand
+//    for (1/pi, sqrt(ln2/pi), sqrt(ln2), 1/sqrt(pi)); the fit's own coefficients are
+//    the published digits;
+//  * exp and log are the device's double exp/log (Rij, the damping power, logref);
+//  * vproj, the tolerance references and xhat are formed in double.
+// It is the accuracy reference the FP32 pass is measured against.
+// ---------------------------------------------------------------------------
+struct QlgCoef64 { double ih, bL, gG, cZH, cL2; };
+
+__device__ __forceinline__ QlgCoef64 qlg_setup64(double gL, double D, double SQ, double S) {
+  QlgCoef64 c;
+  const double e = fma(gL, 0.60602209212341318, D);
+  c.ih = e / fma(gL, e, SQ);
+  const double r = gL * c.ih;
+  const double q = r * (1.0 - r);
+  const double sc = S * c.ih;
+  const double qs = q * sc;
+  const double x = 2.0 * r - 1.0;
+  c.bL = (0.31830988618379067 * r) * sc;
+  c.gG = fma(qs, fma(x, -0.11019326278794868, -0.064924393191013452), (0.46971863934982566 * (1.0 - r)) * sc);
+  c.cZH = qs * fma(x, -0.10567135279610407, 0.38494195930078284);
+  c.cL2 = qs * fma(x, 0.16241029253712097, 0.04054415746208978);
+  return c;
+}
+
+__device__ __forceinline__ double qlg_eval64(const double2 *tab, const QlgCoef64 &c, double x) {
+  const double xs = fabs(x) * c.ih;
+  const double u = xs * xs;
+  const double L = 1.0 / (1.0 + u);
+  const int ig = (int)lround(fmin(xs * 800.0, 9019.0));
+  const double2 gw = __ldg(tab + ig);
+  double p = fma(c.cZH, gw.y, c.cL2);
+  p = fma(L, p, c.bL);
+  return fma(L, p, gw.x * c.gG);
+}
+
+__device__ __forceinline__ double qlg_halfwidth64(double D2, double gL, double S, double ref, double lnq) {
+  const double AL = ((0.31830988618379067 * gL) * S) / ref;
+  const double h1 = fma(D2, lnq, fmin(AL, 1.5 * D2));
+  const double h2 = (AL - fmax(fma(gL, gL, -0.5 * D2), 0.0)) + fmin(AL, 5.0 * D2);
+  return sqrt(fmax(fmax(h1, h2), 0.0));
+}
+
+__device__ __forceinline__ double point_xhat64(double chi_c, double T, double nu) {
+  const double hv = nu * (M3D_H_K / T);
+  const double beta = fmax(exp(-hv), DBL_MIN);
+  const double Bnu = beta / (-expm1(-hv));
+  return chi_c + chi_c * Bnu;
+}
+
+// chi_l of a window: NF > 0 in registers; NF = 0 (any window size) in the cell's
+// row of chi_out, which the epilogue then overwrites with the transfer units
+template <int NF>
+struct ChlF64 {
+  double v[NF];
+  __device__ __forceinline__ ChlF64(double *) {}
+  __device__ __forceinline__ double &operator[](int i) { return v[i]; }
+};
+template <>
+struct ChlF64<0> {
+  double *p;
+  __device__ __forceinline__ ChlF64(double *row) : p(row) {}
+  __device__ __forceinline__ double &operator[](int i) { return p[i]; }
+};
+
+template <int NF>
+__global__ void __launch_bounds__(256) k_lte_opacity_units_f64(AtmosDev A, GridArgs G, const double *nu, double v0,
+                                                               double v1, double v2, double *chi_out, double *S_out,
+                                                               const double2 *tab) {
+  const double ex_cutoff = -85.0, voigt_peak = 0.56418958354775628, sqrt_pi = 1.7724538509055160;
+  const double tol = (double)G.tol, sdl = G.inv_dllam, flo_scale = (double)G.flo_scale;
+  const double lt = log(tol / voigt_peak);
+  const int ncell = A.ncell;
+  const int nf = NF > 0 ? NF : G.nf;
+  for (int cell = blockIdx.x * blockDim.x + threadIdx.x; cell < ncell; cell += gridDim.x * blockDim.x) {
+    const double T = A.temp[cell], chi_c = A.chi_c[cell];
+    double *co = chi_out + (size_t)nf * cell, *so = S_out + (size_t)nf * cell;
+    ChlF64<NF> chl(co);
+#pragma unroll
+    for (int f = 0; f < nf; f++) chl[f] = 0.0;
+    const double vproj = (v0 * (double)A.vx[cell] + v1 * (double)A.vy[cell]) + v2 * (double)A.vz[cell];
+    const double ekt = A.e_kT[cell], ne = A.ne[cell], tothi = A.tothi[cell], starkpe = A.stark_pe[cell];
+    // xhat and logref at the window edges, where every line centred outside lands
+    const double x_lo = point_xhat64(chi_c, T, nu[0]), x_hi = point_xhat64(chi_c, T, nu[nf - 1]);
+    const double lr_lo = x_lo > 0.0 ? lt + log(x_lo) : -DBL_MAX, lr_hi = x_hi > 0.0 ? lt + log(x_hi) : -DBL_MAX;
+    for (int sp = 0; sp < A.nspecies; sp++) {
+      const SpeciesDev &Sd = A.species[sp];
+      const LineArgs &L = Sd.L;
+      const double idf = Sd.inv_df[cell], base = Sd.lnbase[cell];
+      const double D = sdl / idf, D2 = D * D, SQ = 0.83255461115769776 * D2;
+      const double lvb2 = log((double)Sd.vbar2[cell]);
+      const double unsold_c = exp(0.3 * lvb2) * tothi;
+      for (int l = 0; l < L.nline; l++) {
+        if (L.active && !L.active[l]) continue;
+        const double llc = L.llam0[l] - vproj;
+        const double pos = (llc - G.llam1) * G.inv_dllam;
+        const int ic = (int)lround(pos) + 1;
+        const int f0 = ic < 1 ? 1 : (ic > nf ? nf : ic);
+        const double arg = (base + (double)L.gpref[l]) - (double)L.lower_ev[l] * ekt;
+        if (arg < ex_cutoff) continue;
+        double cont0, lr0, chl0;
+        if (f0 == 1) { cont0 = x_lo; lr0 = lr_lo; chl0 = chl[0]; }
+        else if (f0 == nf) { cont0 = x_hi; lr0 = lr_hi; chl0 = chl[nf - 1]; }
+        else {
+          cont0 = point_xhat64(chi_c, T, nu[f0 - 1]);
+          lr0 = cont0 > 0.0 ? lt + log(cont0) : -DBL_MAX;
+          if constexpr (NF > 0) {
+            chl0 = chl[0];
+#pragma unroll
+            for (int k = 1; k < NF; k++) chl0 = (k == f0 - 1) ? chl[k] : chl0;
+          } else {
+            chl0 = chl[f0 - 1];
+          }
+        }
+        double refl = tol * cont0, lref;
+        const double flo = flo_scale * chl0;
+        if (flo > refl) { refl = flo; lref = log(flo * sqrt_pi); }
+        else lref = lr0;
+        if (arg <= lref) continue;
+        const double Rij = exp(arg);
+        if (voigt_peak * Rij <= refl) continue;
+        double a = (double)L.grad[l];
+        const double gw1 = L.gw1[l];
+        if (L.unsold[l]) a = fma(gw1, unsold_c, a);
+        else if (gw1 != 0.0) a = fma(gw1 * exp((double)L.gw2[l] * lvb2), tothi, a);
+        const double gs = L.gstk[l];
+        a = gs >= 0.0 ? fma(gs, ne, a) : fma(-gs, starkpe, a);
+        a *= sdl;
+        const double S = Rij * D;
+        const double x1 = (G.llam[f0 - 1] - llc) * G.inv_dllam;
+        const QlgCoef64 cf = qlg_setup64(a, D, SQ, S);
+        const double hw = qlg_halfwidth64(D2, a, S, refl, arg - lref);
+        const int noff = (int)lround(fmin(hw, (double)(nf + abs(ic))));
+        const int fa = ic - noff > 1 ? ic - noff : 1;
+        const int fb = ic + noff < nf ? ic + noff : nf;
+        if (fa > fb) continue;
+        const double x0 = x1 - (double)(f0 - fa);
+        if constexpr (NF > 0) {
+#pragma unroll
+          for (int f = 0; f < NF; f++)
+            if (f + 1 >= fa && f + 1 <= fb) chl[f] += qlg_eval64(tab, cf, x0 + (double)(f + 1 - fa));
+        } else {
+          for (int f = fa - 1; f < fb; f++) chl[f] += qlg_eval64(tab, cf, x0 + (double)(f + 1 - fa));
+        }
+      }
+    }
+    // epilogue: transfer units (in place over the accumulator row when NF = 0)
+#pragma unroll
+    for (int f = 0; f < nf; f++) {
+      double c, sv;
+      point_units(chi_c, T, nu[f], chl[f], chl[f], (double)A.maser_chi_floor, c, sv);
+      co[f] = c;
+      so[f] = sv;
     }
   }
 }

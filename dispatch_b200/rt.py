@@ -289,24 +289,17 @@ def integrate_intensity(wmu, inu, psi, Jnu, PsiJ):
                                         ptr(Jnu), ptr(PsiJ), C.c_uint(_flags([inu]))), "m3d_integrate_intensity")
 
 
-def lte_synthesis(atm: dict, nu, llam, vec, wmu, fp64=False, return_itop=False, device=False):
-    """The LTE output pass of one frequency window for every ray (m3d_lte_synthesis).
-
-    atm: dict with nx, ny, nz, slab_nz, ds_cm, ds_code, pivot_z, ray_offset and the
-    per-cell fields (numpy for host buffers, torch CUDA tensors with device=True),
-    species: list of dicts (linelist arrays + inv_df, vbar2, lnbase).
-    Returns (ie (nray, nf), flux (nf,), i_top or None)."""
-    init()
-    keep = []
+def _atmos(atm: dict, keep: list) -> Atmos:
+    """m3d_atmos_t of an atmosphere dict (numpy host arrays or torch CUDA tensors)."""
     a = Atmos()
     a.nx, a.ny, a.nz = atm["nx"], atm["ny"], atm["nz"]
-    slab_nz = np.ascontiguousarray(atm["slab_nz"], np.int32)
+    slab_nz = np.ascontiguousarray(atm.get("slab_nz", [atm["nz"]]), np.int32)
     keep.append(slab_nz)
     a.nslab = slab_nz.size
     a.slab_nz = ptr(slab_nz)
-    a.ds_cm[:] = list(atm["ds_cm"])
-    a.ds_code[:] = list(atm["ds_code"])
-    a.pivot_z = float(atm["pivot_z"])
+    a.ds_cm[:] = list(atm.get("ds_cm", (1.0, 1.0, 1.0)))
+    a.ds_code[:] = list(atm.get("ds_code", (1.0, 1.0, 1.0)))
+    a.pivot_z = float(atm.get("pivot_z", 0.0))
     a.ray_offset[:] = list(atm.get("ray_offset", (0.0, 0.0)))
 
     def fld(x):
@@ -331,6 +324,19 @@ def lte_synthesis(atm: dict, nu, llam, vec, wmu, fp64=False, return_itop=False, 
     a.maser_chi_floor = atm.get("maser_chi_floor", 1e-4)
     a.maser_dtau_max = atm.get("maser_dtau_max", 2.0)
     a.maser_Inu_max = atm.get("maser_Inu_max", 1e30)
+    return a
+
+
+def lte_synthesis(atm: dict, nu, llam, vec, wmu, fp64=False, return_itop=False, device=False):
+    """The LTE output pass of one frequency window for every ray (m3d_lte_synthesis).
+
+    atm: dict with nx, ny, nz, slab_nz, ds_cm, ds_code, pivot_z, ray_offset and the
+    per-cell fields (numpy for host buffers, torch CUDA tensors with device=True),
+    species: list of dicts (linelist arrays + inv_df, vbar2, lnbase).
+    Returns (ie (nray, nf), flux (nf,), i_top or None)."""
+    init()
+    keep = []
+    a = _atmos(atm, keep)
     vec = np.ascontiguousarray(vec, np.float64)
     wmu = np.ascontiguousarray(wmu, np.float64)
     nray = wmu.size
@@ -353,6 +359,37 @@ def lte_synthesis(atm: dict, nu, llam, vec, wmu, fp64=False, return_itop=False, 
                                   ptr(itop), ptr(ie), ptr(flux), C.c_uint(flags)), "m3d_lte_synthesis")
     del keep
     return ie, flux, itop
+
+
+def lte_transfer_units(atm: dict, nu, llam, vec, fp64=False, device=False, out=None):
+    """The opacity stage of the LTE pass for one direction (m3d_lte_transfer_units):
+    (chi, S), each (ncell, nf), float32 (float64 with fp64).  out: preallocated
+    (chi, S) to write into."""
+    init()
+    keep = []
+    a = _atmos(atm, keep)
+    vec = np.ascontiguousarray(vec, np.float64).reshape(3)
+    nf = int(nu.shape[0])
+    ncell = a.nx * a.ny * a.nz
+    flags = (FP64 if fp64 else 0) | (DEVICE_PTRS if device else 0)
+    if out is not None:
+        chi, S = out
+    elif device:
+        import torch
+        dt = torch.float64 if fp64 else torch.float32
+        chi = torch.empty((ncell, nf), dtype=dt, device=atm["temp"].device)
+        S = torch.empty_like(chi)
+    else:
+        nu = np.ascontiguousarray(nu, np.float64)
+        llam = np.ascontiguousarray(llam, np.float64)
+        chi = np.empty((ncell, nf), np.float64 if fp64 else _F32)
+        S = np.empty_like(chi)
+    if device:
+        order_after_torch(chi)
+    check(lib().m3d_lte_transfer_units(C.byref(a), C.c_int(nf), ptr(nu), ptr(llam), ptr(vec), ptr(chi), ptr(S),
+                                       C.c_uint(flags)), "m3d_lte_transfer_units")
+    del keep
+    return chi, S
 
 
 def eta_spread(vecs, ds, dz_upstream=None, one_dimensional=False) -> tuple[int, int]:

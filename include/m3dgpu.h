@@ -405,8 +405,19 @@ typedef struct m3d_atmos {
 /* nu (nf) [Hz], llam (nf) = ln(lambda/AA), uniform; vec (3, nray) (host), wmu (nray)
  * flux weights (host).  Outputs: i_top (nf, nx, ny, nray) the emergent intensity in
  * transfer units (may be NULL), ie (nf, nray) and flux (nf) as save_intensity writes
- * them.  With M3D_FP64 the transfer units, rotation and solver run in FP64, one
- * launch per ray and slab (the plain FP64 path); i_top is then float64. */
+ * them.  With M3D_FP64 the whole pass runs in FP64 (the plain FP64 path): the line
+ * opacity and its QLG-bot profile with fp64 tables, exp and log, the transfer units,
+ * and rotate_array + the quadratic solver one launch per ray and slab; i_top is then
+ * float64. */
+/* The opacity stage of m3d_lte_synthesis for one direction vec (3, host): the
+ * background (beta, Bnu), work units, add_opacity_equi of every species in line
+ * order with the Doppler shift v.vec, and work_to_transfer_units (rt_patch_mod.f90:
+ * 2004-2023, 3518-3536, 3571-3651; linelist_mod.f90:729-960).  Outputs chi and S
+ * (nf, ncell), frequency fastest, cell index x fastest then y then z; float64 with
+ * M3D_FP64 (the plain FP64 path). */
+int m3d_lte_transfer_units(const m3d_atmos_t *atm, int nf, const double *nu, const double *llam, const double *vec,
+                           void *chi, void *S, unsigned flags);
+
 int m3d_lte_synthesis(const m3d_atmos_t *atm, int nf, const double *nu, const double *llam,
                       int nray, const double *vec, const double *wmu, void *i_top, float *ie,
                       float *flux, unsigned flags);

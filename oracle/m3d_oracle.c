@@ -694,6 +694,122 @@ int or_add_opacity_equi_scat(const float *tgx, const float *th2x, const or_linel
 }
 
 /* =========================================================================
+ * The plain FP64 path of the LTE pass's line opacity: add_opacity_equi
+ * (HOP/linelist_mod.f90:729-960) and the QLG-bot profile (qlg_mod.f90:538-671)
+ * step for step in double.  The tables are qlg_init's formulas in fp64 (not
+ * rounded to float), the fitted float constants are the exact values they stand
+ * for (1/pi, sqrt(ln2/pi), sqrt(ln2), 1/sqrt(pi)), exp and log are libm's double
+ * functions, and the Doppler shift, the tolerance references and xhat are double.
+ * No line selection by reach, no NLTE departures, no scattering split.
+ * ========================================================================= */
+void or_qlg_tables_f64(double *tgx, double *th2x)
+{
+  for (int i = 0; i <= QLG_NX; i++) {
+    double x = (double)i / 800.0;
+    tgx[i] = pow(2.0, -x * x);
+    th2x[i] = qlg_wr02(x * x);
+  }
+}
+
+typedef struct { double ih, bL, gG, cZH, cL2; } qlg_coef64_t;
+
+static qlg_coef64_t bot_setup64(double gL, double D, double SQ, double S)
+{
+  qlg_coef64_t c;
+  double e = fma(gL, 0.60602209212341318, D);
+  c.ih = e / fma(gL, e, SQ);
+  double r = gL * c.ih;
+  double q = r * (1.0 - r);
+  double sc = S * c.ih;
+  double qs = q * sc;
+  double x = 2.0 * r - 1.0;
+  c.bL = (0.31830988618379067 * r) * sc;
+  c.gG = fma(qs, fma(x, -0.11019326278794868, -0.064924393191013452), (0.46971863934982566 * (1.0 - r)) * sc);
+  c.cZH = qs * fma(x, -0.10567135279610407, 0.38494195930078284);
+  c.cL2 = qs * fma(x, 0.16241029253712097, 0.04054415746208978);
+  return c;
+}
+
+static double bot_eval64(const double *tgx, const double *th2x, const qlg_coef64_t *c, double x)
+{
+  double xs = fabs(x) * c->ih;
+  double u = xs * xs;
+  double L = 1.0 / (1.0 + u);
+  int ig = (int)lround(fmin(xs * 800.0, 9019.0));
+  double p = fma(c->cZH, th2x[ig], c->cL2);
+  p = fma(L, p, c->bL);
+  return fma(L, p, tgx[ig] * c->gG);
+}
+
+/* chl (nf, ncell) accumulated in place for one species; xhat (nf, ncell) in double */
+int or_opacity_f64(const double *tgx, const double *th2x, const or_linelist_t *ll, int nf, const double *llam,
+                   int ncell, double *chl, const double *xhat, const double *vproj, const float *inv_df,
+                   const float *vbar2, const float *e_kT, const float *lnbase, const float *ne, const float *tothi,
+                   const float *stark_pe, double tol)
+{
+  const double ex_cutoff = -85.0, voigt_peak = 0.56418958354775628, sqrt_pi = 1.7724538509055160;
+  if (ll->nline == 0 || nf < 2) return 0;
+  if (llam[nf - 1] < llam[0]) return 1;
+  const double llam1 = llam[0];
+  const double dllam = (llam[nf - 1] - llam[0]) / (double)(nf - 1);
+  const double inv_dllam = 1.0 / dllam;
+  const double sdl = inv_dllam;
+  const float tolf = (float)tol;
+  const double flo_scale = (double)(tolf * tolf);
+  const double lt = log(tol / voigt_peak);
+  for (int i = 0; i < ncell; i++) {
+    double *ch = chl + (size_t)nf * i;
+    const double *xh = xhat + (size_t)nf * i;
+    const double D = sdl / (double)inv_df[i], D2 = D * D, SQ = 0.83255461115769776 * D2;
+    const double lvb2 = log((double)vbar2[i]);
+    const double unsold_c = exp(0.3 * lvb2) * (double)tothi[i];
+    const double ekt = e_kT[i], ne_c = ne[i], tothi_c = tothi[i], starkpe = stark_pe[i], base = lnbase[i];
+    for (int l = 0; l < ll->nline; l++) {
+      if (ll->active && !ll->active[l]) continue;
+      const double llc = ll->llam0[l] - vproj[i];
+      const double pos = (llc - llam1) * inv_dllam;
+      const int ic = (int)lround(pos) + 1;
+      const int f0 = ic < 1 ? 1 : (ic > nf ? nf : ic);
+      const double arg = (base + (double)ll->gpref[l]) - (double)ll->lower_ev[l] * ekt;
+      if (arg < ex_cutoff) continue;
+      const double cont0 = xh[f0 - 1];
+      double refl = tol * cont0, lref;
+      const double flo = flo_scale * ch[f0 - 1];
+      if (flo > refl) {
+        refl = flo;
+        lref = log(flo * sqrt_pi);
+      } else {
+        lref = cont0 > 0.0 ? lt + log(cont0) : -DBL_MAX;
+      }
+      if (arg <= lref) continue;
+      const double Rij = exp(arg);
+      if (voigt_peak * Rij <= refl) continue;
+      double a = ll->grad[l];
+      const double gw1 = ll->gw1[l];
+      if (ll->unsold[l]) a = fma(gw1, unsold_c, a);
+      else if (gw1 != 0.0) a = fma(gw1 * exp((double)ll->gw2[l] * lvb2), tothi_c, a);
+      const double gs = ll->gstk[l];
+      a = gs >= 0.0 ? fma(gs, ne_c, a) : fma(-gs, starkpe, a);
+      a *= sdl;
+      const double S = Rij * D;
+      const double x1 = (llam[f0 - 1] - llc) * inv_dllam;
+      const qlg_coef64_t c = bot_setup64(a, D, SQ, S);
+      const double AL = ((0.31830988618379067 * a) * S) / refl;
+      const double h1 = fma(D2, arg - lref, fmin(AL, 1.5 * D2));
+      const double h2 = (AL - fmax(fma(a, a, -0.5 * D2), 0.0)) + fmin(AL, 5.0 * D2);
+      const double hw = sqrt(fmax(fmax(h1, h2), 0.0));
+      const int noff = (int)lround(fmin(hw, (double)(nf + abs(ic))));
+      const int fa = ic - noff > 1 ? ic - noff : 1;
+      const int fb = ic + noff < nf ? ic + noff : nf;
+      if (fa > fb) continue;
+      const double x0 = x1 - (double)(f0 - fa);
+      for (int f = fa; f <= fb; f++) ch[f - 1] += bot_eval64(tgx, th2x, &c, x0 + (double)(f - fa));
+    }
+  }
+  return 0;
+}
+
+/* =========================================================================
  * Background and work units
  * ========================================================================= */
 /* lte_background_opacities (rt_patch_mod.f90:2004-2023): beta, Bnu */

@@ -112,6 +112,14 @@ int or_add_opacity_equi_scat(const float *tgx, const float *th2x, const or_linel
                              uint8_t *used, float *strength, float *reach, const float *one_m_eps,
                              float *chi_scat);
 
+/* The plain FP64 line opacity (add_opacity_equi and QLG-bot in double, fp64 tables):
+ * chl (nf, ncell) accumulated for one species, xhat (nf, ncell) and vproj in double */
+void or_qlg_tables_f64(double *tgx, double *th2x);
+int or_opacity_f64(const double *tgx, const double *th2x, const or_linelist_t *ll, int nf, const double *llam,
+                   int ncell, double *chl, const double *xhat, const double *vproj, const float *inv_df,
+                   const float *vbar2, const float *e_kT, const float *lnbase, const float *ne, const float *tothi,
+                   const float *stark_pe, double tol);
+
 /* ---- background and work units (rt_patch_mod.f90:1983-2023, 3518-3651) ---- */
 void or_lte_background(int nf, int ncell, const double *nu, const float *temp, float *beta, float *Bnu);
 void or_lte_work(int nf, int ncell, const float *chi_c, const float *beta, const float *Bnu,

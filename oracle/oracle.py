@@ -129,6 +129,42 @@ def qlg_tables():
     return _tables
 
 
+_tables64 = None
+
+
+def qlg_tables_f64():
+    """qlg_init's two tables in fp64 (the plain FP64 path's tables)."""
+    global _tables64
+    if _tables64 is None:
+        tgx = np.empty(9020, np.float64)
+        th2x = np.empty(9020, np.float64)
+        lib().or_qlg_tables_f64(_p(tgx), _p(th2x))
+        _tables64 = (tgx, th2x)
+    return _tables64
+
+
+def opacity_f64(ll: dict, llam, chl, xhat, vproj, cells: dict, tol=1e-4):
+    """The plain FP64 line opacity of one species, accumulated in place on chl
+    (ncell, nf) f64.  xhat (ncell, nf) and vproj (ncell,) f64; cells: inv_df, vbar2,
+    e_kT, lnbase, ne, tothi, stark_pe (ncell,) f32.  tol is the float tolerance."""
+    tgx, th2x = qlg_tables_f64()
+    s, keep = make_linelist(ll)
+    llam = np.ascontiguousarray(llam, np.float64)
+    assert chl.dtype == np.float64 and chl.flags.c_contiguous
+    xh = np.ascontiguousarray(xhat, np.float64)
+    vp = np.ascontiguousarray(vproj, np.float64)
+    cf = {k: np.ascontiguousarray(cells[k], np.float32) for k in
+          ("inv_df", "vbar2", "e_kT", "lnbase", "ne", "tothi", "stark_pe")}
+    f = lib().or_opacity_f64
+    f.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
+                  C.c_void_p] + [C.c_void_p] * 7 + [C.c_double]
+    rc = f(_p(tgx), _p(th2x), C.byref(s), llam.size, _p(llam), vp.size, _p(chl), _p(xh), _p(vp),
+           *[_p(cf[k]) for k in ("inv_df", "vbar2", "e_kT", "lnbase", "ne", "tothi", "stark_pe")],
+           float(np.float32(tol)))
+    assert rc == 0
+    del keep
+
+
 def qlg_ref_f64(a, v):
     v = np.ascontiguousarray(v, np.float64)
     out = np.empty_like(v)

@@ -14,7 +14,10 @@ H_K = 6.626176e-27 / 1.380662e-16
 
 
 def transfer_units(atm, nu, llam, vec, tol=1e-4, fp64=False):
-    """(chi, S) of every cell for direction vec: (ncell, nf), f32 or f64."""
+    """(chi, S) of every cell for direction vec: (ncell, nf), f32 or f64.  fp64: the
+    plain FP64 path, line opacity and profile included (oracle.opacity_f64)."""
+    if fp64:
+        return _transfer_units_f64(atm, nu, llam, vec, tol)
     vx = atm["vx"].astype(np.float64)
     vy = atm["vy"].astype(np.float64)
     vz = atm["vz"].astype(np.float64)
@@ -29,19 +32,29 @@ def transfer_units(atm, nu, llam, vec, tol=1e-4, fp64=False):
         cells = {"vproj": vproj, "inv_df": sp["inv_df"], "vbar2": sp["vbar2"], "lnbase": sp["lnbase"],
                  "e_kT": atm["e_kT"], "ne": atm["ne"], "tothi": atm["tothi"], "stark_pe": atm["stark_pe"]}
         O.add_opacity_equi(sp, llam, chil, etal, xhat, lr, cells, tol=tol)
-    if not fp64:
-        w1 = (xhat + chil).astype(np.float32)
-        w2 = (ehat + etal).astype(np.float32)
-        O.work_to_transfer_units(w1, w2, beta, atm.get("maser_chi_floor", 1e-4))
-        return w1, w2
+    w1 = (xhat + chil).astype(np.float32)
+    w2 = (ehat + etal).astype(np.float32)
+    O.work_to_transfer_units(w1, w2, beta, atm.get("maser_chi_floor", 1e-4))
+    return w1, w2
+
+
+def _transfer_units_f64(atm, nu, llam, vec, tol):
+    vproj = (vec[0] * atm["vx"].astype(np.float64) + vec[1] * atm["vy"].astype(np.float64)) \
+        + vec[2] * atm["vz"].astype(np.float64)
     T = atm["temp"].astype(np.float64)[:, None]
     hv = nu[None, :] * (H_K / T)
     b = np.maximum(np.exp(-hv), np.finfo(np.float64).tiny)
     Bn = b / (-np.expm1(-hv))
     cc = atm["chi_c"].astype(np.float64)[:, None]
     eta_c = cc * Bn
-    w1 = (cc + eta_c) + chil.astype(np.float64)
-    w2 = eta_c / b + etal.astype(np.float64)
+    xhat = cc + eta_c
+    chil = np.zeros((atm["temp"].size, nu.size), np.float64)
+    for sp in atm["species"]:
+        cells = {"inv_df": sp["inv_df"], "vbar2": sp["vbar2"], "lnbase": sp["lnbase"], "e_kT": atm["e_kT"],
+                 "ne": atm["ne"], "tothi": atm["tothi"], "stark_pe": atm["stark_pe"]}
+        O.opacity_f64(sp, llam, chil, xhat, vproj, cells, tol=tol)
+    w1 = xhat + chil
+    w2 = eta_c / b + chil
     etav = w2 * b
     chi = w1 - etav
     fl = np.maximum(np.float64(np.float32(atm.get("maser_chi_floor", 1e-4))) * np.abs(w1), np.finfo(np.float64).tiny)
