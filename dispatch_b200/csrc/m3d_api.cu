@@ -1397,8 +1397,17 @@ int m3d_lte_synthesis(const m3d_atmos_t *atm, int nf, const double *nu, const do
     TRY(launch_opacity(in, v, fp64, dchi, dS));
     if (!fp64) {
       const QuadConst qc = quad_const(atm->ds_cm[2], v[2]);
-      LAUNCH_S(M3D_STAGE_SOLVE, k_quad_rot_column, (int)((plane + 255) / 256), 256, 0, nf, nx, ny, nz, (const float *)dchi, (const float *)dS, (const RotCol *)drot + (size_t)r * nz,
-             (const int *)dz0, atm->nslab, qc, pc, dtmax, Imax, (float *)dtop + plane * r);
+      if (nf % 2 == 0) {
+        // frequency pairs: 8-byte taps, the ray's rotation weights in shared memory
+        const size_t pairs = plane / 2;
+        LAUNCH_S(M3D_STAGE_SOLVE, k_quad_rot_column2, (int)((pairs + 255) / 256), 256, sizeof(RotCol) * nz, nf, nx, ny,
+                 nz, (const float *)dchi, (const float *)dS, (const RotCol *)drot + (size_t)r * nz, (const int *)dz0,
+                 atm->nslab, qc, pc, dtmax, Imax, (float *)dtop + plane * r);
+      } else {
+        LAUNCH_S(M3D_STAGE_SOLVE, k_quad_rot_column, (int)((plane + 255) / 256), 256, 0, nf, nx, ny, nz,
+                 (const float *)dchi, (const float *)dS, (const RotCol *)drot + (size_t)r * nz, (const int *)dz0,
+                 atm->nslab, qc, pc, dtmax, Imax, (float *)dtop + plane * r);
+      }
       LAUNCH_S(M3D_STAGE_REDUCE, k_save_partial<float>, dim3((nf + 31) / 32, kParts), dim3(32, 8), 0, nf, (int)ncol,
                dnu, (const float *)dtop + plane * r, (double *)dpart);
       LAUNCH_S(M3D_STAGE_REDUCE, k_save_final, (nf + 127) / 128, 128, 0, nf, (int)ncol, kParts, (const double *)dpart,

@@ -803,13 +803,13 @@ __global__ void k_long_char2(SlabArgs s, T *work, T *psi, T *irem, T *esc, const
 }
 
 // quad_step of long_char_quadratic (rt_solvers_mod.f90:966-1019)
+// the step from the two slopes of the extinction on, t1 = (xxc - xxup) rdsup and
+// t3 = (xxdn - xxc) rdsup (a sweep carries t3 into the next step's t1: same operands)
 template <typename T>
-__device__ __forceinline__ void quad_step(T xxup, T xxc, T xxdn, T ssup, T ssc, T ssdn, T Inuup, bool at_target,
-                                          T rdsup, T dsup1, T dsup2, T dtmax, T Imax, bool get_psi, T &Inu_out,
-                                          T &plam_out) {
+__device__ __forceinline__ void quad_step_t13(T t1, T t3, T xxup, T xxc, T xxdn, T ssup, T ssc, T ssdn, T Inuup,
+                                              bool at_target, T dsup1, T dsup2, T dtmax, T Imax, bool get_psi,
+                                              T &Inu_out, T &plam_out) {
   const T dtmin = (T)1e-20f;
-  T t1 = (xxc - xxup) * rdsup;
-  T t3 = (xxdn - xxc) * rdsup;
   T t2 = (T)0.5 * (t1 + t3);
   t2 = (tcopysign((T)1, t1) + tcopysign((T)1, t3)) * tmin(tmin(tabs(t1), tabs(t3)), tabs((T)0.5 * t2));
   T dtup = fma_t(dsup2, t1 - t2, dsup1 * (xxup + xxc));
@@ -845,6 +845,16 @@ __device__ __forceinline__ void quad_step(T xxup, T xxc, T xxdn, T ssup, T ssc, 
   }
   Inu_out = tmax(-Imax, tmin(Imax, Inu));
   plam_out = plam;
+}
+
+template <typename T>
+__device__ __forceinline__ void quad_step(T xxup, T xxc, T xxdn, T ssup, T ssc, T ssdn, T Inuup, bool at_target,
+                                          T rdsup, T dsup1, T dsup2, T dtmax, T Imax, bool get_psi, T &Inu_out,
+                                          T &plam_out) {
+  const T t1 = (xxc - xxup) * rdsup;
+  const T t3 = (xxdn - xxc) * rdsup;
+  quad_step_t13<T>(t1, t3, xxup, xxc, xxdn, ssup, ssc, ssdn, Inuup, at_target, dsup1, dsup2, dtmax, Imax, get_psi,
+                   Inu_out, plam_out);
 }
 
 struct QuadConst { float rdsup, dsup1, dsup2; };

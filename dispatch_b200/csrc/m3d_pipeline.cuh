@@ -717,6 +717,128 @@ __global__ void __launch_bounds__(256) k_quad_rot_column(int nf, int nx, int ny,
   I_top[g] = gI;
 }
 
+// The same sweep with two neighbouring frequencies per thread (nf even): every tap
+// is one 8-byte load of a frequency pair, so the sheared plane's index arithmetic
+// and the loads serve two points; the rotation weights of the ray's planes sit in
+// shared memory; the taps are loaded two planes ahead of their use; and the
+// extinction slope t3 of a step is carried into the next step's t1 (same operands,
+// same rounding).  Bit-identical to k_quad_rot_column.
+struct Taps2 { float2 c11, c21, c12, c22, s11, s21, s12, s22; };
+
+__device__ __forceinline__ Taps2 load_taps2(const float2 *chi, const float2 *S, size_t plane_off, const RotCol &r,
+                                            int f2, int x, int y, int nf2, int nx, int ny) {
+  int x1 = x + r.ux;
+  x1 = x1 >= nx ? x1 - nx : x1;
+  const int x2 = x1 + 1 == nx ? 0 : x1 + 1;
+  int y1 = y + r.uy;
+  y1 = y1 >= ny ? y1 - ny : y1;
+  const int y2 = y1 + 1 == ny ? 0 : y1 + 1;
+  const unsigned rx1 = (unsigned)nf2 * x1, rx2 = (unsigned)nf2 * x2;
+  const unsigned ry1 = (unsigned)nf2 * nx * y1, ry2 = (unsigned)nf2 * nx * y2;
+  const float2 *pc = chi + plane_off + f2, *ps = S + plane_off + f2;
+  Taps2 t;
+  t.c11 = __ldg(pc + rx1 + ry1); t.c21 = __ldg(pc + rx2 + ry1);
+  t.c12 = __ldg(pc + rx1 + ry2); t.c22 = __ldg(pc + rx2 + ry2);
+  t.s11 = __ldg(ps + rx1 + ry1); t.s21 = __ldg(ps + rx2 + ry1);
+  t.s12 = __ldg(ps + rx1 + ry2); t.s22 = __ldg(ps + rx2 + ry2);
+  return t;
+}
+
+__device__ __forceinline__ float bilin(const RotCol &r, float p11, float p21, float p12, float p22) {
+  float v = r.a * p11;
+  v = fmaf(r.b, p21, v);
+  v = fmaf(r.c, p12, v);
+  return fmaf(r.d, p22, v);
+}
+
+__device__ __forceinline__ void combine2(const Taps2 &t, const RotCol &r, float2 &xv, float2 &sv) {
+  xv.x = bilin(r, t.c11.x, t.c21.x, t.c12.x, t.c22.x);
+  xv.y = bilin(r, t.c11.y, t.c21.y, t.c12.y, t.c22.y);
+  sv.x = bilin(r, t.s11.x, t.s21.x, t.s12.x, t.s22.x);
+  sv.y = bilin(r, t.s11.y, t.s21.y, t.s12.y, t.s22.y);
+}
+
+__device__ __forceinline__ float pchip_ghost(float y1, float y2, const PchipConst &pc) {
+  const float dydx1 = (2.0f * (y2 - y1)) / pc.dx1 - 0.0f;
+  return fmaxf((pc.c0 * y1 + pc.p * y2) + pc.dx1 * (pc.cm0 * dydx1 + pc.cm1 * 0.0f), 0.0f);
+}
+
+// shared memory: the ray's RotCol of every global plane (nz entries).  Three blocks
+// per SM (79 registers, no spills) measured 11 % faster than the unbounded 97.
+__global__ void __launch_bounds__(256, 3) k_quad_rot_column2(int nf, int nx, int ny, int nz, const float *chi,
+                                                          const float *S, const RotCol *rot, const int *slab_z0,
+                                                          int nslab, QuadConst qc, PchipConst pc, float dtmax,
+                                                          float Imax, float *I_top) {
+  extern __shared__ RotCol s_rot[];
+  for (int i = threadIdx.x; i < nz; i += blockDim.x) s_rot[i] = rot[i];
+  __syncthreads();
+  const int nf2 = nf >> 1;
+  const size_t plane = (size_t)nf2 * nx * ny;  // in frequency pairs
+  const size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (g >= plane) return;
+  const int f2 = (int)(g % nf2), x = (int)((g / nf2) % nx), y = (int)(g / ((size_t)nf2 * nx));
+  const float2 *chi2 = reinterpret_cast<const float2 *>(chi), *S2 = reinterpret_cast<const float2 *>(S);
+  const float rdsup = qc.rdsup, dsup1 = qc.dsup1, dsup2 = qc.dsup2;
+  // PCHIP ghost below the bottom slab from its unrotated planes 1 and 2
+  float2 gx, gs, gI;
+  {
+    const float2 c1 = chi2[g], c2 = chi2[g + plane], s1 = S2[g], s2 = S2[g + plane];
+    gx = make_float2(pchip_ghost(c1.x, c2.x, pc), pchip_ghost(c1.y, c2.y, pc));
+    gs = make_float2(pchip_ghost(s1.x, s2.x, pc), pchip_ghost(s1.y, s2.y, pc));
+    gI = gs;
+  }
+  for (int s = 0; s < nslab; s++) {
+    const int z0 = slab_z0[s], n = slab_z0[s + 1] - z0;
+    float2 xu = gx, su = gs, Iu = gI, xc, sc, xd, sd;
+    {
+      const RotCol r0 = s_rot[z0], r1 = s_rot[z0 + 1];
+      const Taps2 t0 = load_taps2(chi2, S2, plane * z0, r0, f2, x, y, nf2, nx, ny);
+      const Taps2 t1 = load_taps2(chi2, S2, plane * (z0 + 1), r1, f2, x, y, nf2, nx, ny);
+      combine2(t0, r0, xc, sc);
+      combine2(t1, r1, xd, sd);
+    }
+    Taps2 tn;
+    RotCol rn;
+    if (n > 2) {
+      rn = s_rot[z0 + 2];
+      tn = load_taps2(chi2, S2, plane * (z0 + 2), rn, f2, x, y, nf2, nx, ny);
+    }
+    float2 t1 = make_float2((xc.x - xu.x) * rdsup, (xc.y - xu.y) * rdsup);
+    for (int zl = 1; zl < n; zl++) {
+      // the plane two ahead, loaded while this step computes
+      Taps2 tnn;
+      RotCol rnn;
+      if (zl + 2 < n) {
+        rnn = s_rot[z0 + zl + 2];
+        tnn = load_taps2(chi2, S2, plane * (z0 + zl + 2), rnn, f2, x, y, nf2, nx, ny);
+      }
+      const float2 t3 = make_float2((xd.x - xc.x) * rdsup, (xd.y - xc.y) * rdsup);
+      float2 In;
+      float pl;
+      quad_step_t13<float>(t1.x, t3.x, xu.x, xc.x, xd.x, su.x, sc.x, sd.x, Iu.x, true, dsup1, dsup2, dtmax, Imax,
+                           false, In.x, pl);
+      quad_step_t13<float>(t1.y, t3.y, xu.y, xc.y, xd.y, su.y, sc.y, sd.y, Iu.y, true, dsup1, dsup2, dtmax, Imax,
+                           false, In.y, pl);
+      Iu = In;
+      if (zl + 1 < n) {
+        t1 = t3;
+        xu = xc; su = sc; xc = xd; sc = sd;
+        combine2(tn, rn, xd, sd);
+        tn = tnn;
+        rn = rnn;
+      }
+    }
+    float2 In;
+    float pl;
+    quad_step<float>(xu.x, xc.x, xd.x, su.x, sc.x, sd.x, Iu.x, false, rdsup, dsup1, dsup2, dtmax, Imax, false, In.x,
+                     pl);
+    quad_step<float>(xu.y, xc.y, xd.y, su.y, sc.y, sd.y, Iu.y, false, rdsup, dsup1, dsup2, dtmax, Imax, false, In.y,
+                     pl);
+    gx = xd; gs = sd; gI = In;
+  }
+  reinterpret_cast<float2 *>(I_top)[g] = gI;
+}
+
 // save_intensity (rt_patch_mod.f90:4151-4208): ie(f) = <2h nu^5/(c^3 AA) I>_xy, in
 // two deterministic stages: blocks (32 frequencies x 8 rows) sum a fixed stride of
 // columns into partials, then one thread per frequency adds the partials in order.
