@@ -31,6 +31,7 @@ sys.path.insert(0, ROOT)
 METRIC = "formal-solve Gpt*nu*ray/s on 1 B200, FP32 vs FP64 path at <=1e-4 flux error"
 UNIT = "Gpt*nu*ray/s"
 NFREQ_TOTAL = 4000
+REF_NCOLS = 8          # the CPU sample: 8 x 8 columns of the cube, full depth
 
 
 def _args():
@@ -44,6 +45,7 @@ def _args():
     p.add_argument("--no-fp64", action="store_true")
     p.add_argument("--no-ali", action="store_true", help="skip the NLTE measurements (3D window, batched columns)")
     p.add_argument("--no-optab", action="store_true", help="skip the sampled opacity table measurement")
+    p.add_argument("--no-c0", action="store_true", help="skip the 1D LTE synthesis measurement")
     p.add_argument("--cube", type=int, default=240, help="cube edge (240 = the configuration; smaller for profiling)")
     # single cases for timing and profiling one kernel family (no JSON line)
     p.add_argument("--case", default="c1", choices=["c1", "ali-window", "ali-columns", "optab"],
@@ -77,7 +79,7 @@ def _make_inputs(nf, n=240):
 
 
 def _window(llam_all, nu_all, nf, w):
-    nwin = NFREQ_TOTAL // nf
+    nwin = nu_all.size // nf
     w = w % nwin
     sl = slice(w * nf, (w + 1) * nf)
     return np.ascontiguousarray(nu_all[sl]), np.ascontiguousarray(llam_all[sl])
@@ -151,31 +153,18 @@ def _peaks():
         return None
 
 
-def _traffic_from_profiles(ncell, nf):
-    """dram bytes per k_quad_rot_column launch: the committed ncu figure per cell and
-    frequency (a small case of the same kernel) times this launch's cells and frequencies."""
-    path = os.path.join(ROOT, "profiles", "k_quad_rot_column_c1_48.md")
-    try:
-        for line in open(path):
-            if line.startswith("dram_bytes_per_cell_frequency:"):
-                return float(line.split(":")[1]) * ncell * nf
-    except OSError:
-        pass
-    return None
-
-
-def _cpu_baseline(atm, nu, llam, vec, wmu, ncols=2):
-    """The oracle (single thread) on a bounded sample: an ncols x ncols column block
-    of the cube, full depth and all slabs, this window, all rays."""
-    from oracle import pipeline as P
-    sub = _subcube(atm, ncols)
-    t0 = time.perf_counter()
-    P.lte_synthesis(sub, nu, llam, vec, wmu)
-    dt = time.perf_counter() - t0
-    work = wmu.size * sub["nx"] * sub["ny"] * sub["nz"] * nu.size
-    return {"value": work / dt / 1e9, "unit": UNIT, "cores": 1, "kind": "port",
-            "sample": f"{ncols}x{ncols} columns x 240 planes (10 slabs) x {nu.size} frequencies x {wmu.size} rays "
-                      f"of the same cube and window, C restatement of the reference, {dt:.1f} s"}
+# Figures of one ncu capture of the 48^3 case of the same configuration (one launch of
+# each kernel; the command is in the summaries under profiles/).
+#  k_quad_rot_column2: DRAM bytes per cell and frequency of a launch (28,360,192 B read
+#    for 110,592 cells x 32 frequencies), against 8 B algorithmic (chi and Snu once).
+#  k_lte_opacity_units_lane<32>: warp instructions per (cell, line) of a launch
+#    (850,505,012 for 110,592 cells x 500 lines), which scales a full launch's count by
+#    its cells and lines; DRAM bytes per cell: 49.9 B read (measured) plus the chi and
+#    Snu it writes, 8 B per frequency (the small case's 28 MB of output stayed in L2,
+#    a full launch's 3.5 GB cannot).
+NCU_SWEEP_DRAM_BYTES_PER_CELL_FREQ = 8.013
+NCU_OPACITY_WARP_INST_PER_CELL_LINE = 850505012 / (110592 * 500)
+NCU_OPACITY_DRAM_READ_BYTES_PER_CELL = 5518080 / 110592
 
 
 def _subcube(atm, n):
@@ -193,57 +182,98 @@ def _subcube(atm, n):
     return sub
 
 
-def _ref_task(args):
-    sub, nu, llam, vec, wmu = args
+def _cells(atm, lo, hi):
+    """The cells lo:hi of an atmosphere as a row of independent cells (the opacity
+    stage is per cell)."""
+    sub = {"nx": hi - lo, "ny": 1, "nz": 1, "slab_nz": [1]}
+    for k in ("temp", "chi_c", "vx", "vy", "vz", "e_kT", "ne", "tothi", "stark_pe"):
+        sub[k] = np.ascontiguousarray(atm[k][lo:hi])
+    sub["species"] = [{k: (np.ascontiguousarray(v[lo:hi]) if k in ("inv_df", "vbar2", "lnbase") else v)
+                       for k, v in sp.items()} for sp in atm["species"]]
+    return sub
+
+
+def _ref_units(args):
+    sub, nu, llam, v = args
     from oracle import pipeline as P
-    return P.lte_synthesis(sub, nu, llam, vec, wmu)[1]
+    return P.transfer_units(sub, nu, llam, v)
+
+
+def _ref_sweep(args):
+    sub, chi, S, v = args
+    from oracle import pipeline as P
+    return P.column_sweep(sub, chi, S, v)
+
+
+class CpuReference:
+    """The oracle (the C restatement of the reference, built -O3 -march=x86-64-v3 as
+    the reference's release build) on every host core: the opacity stage split over
+    (ray, chunk of cells), then the column sweep of every ray, over an ncols x ncols
+    block of columns of the cube (full depth, all slabs), one window, all rays."""
+
+    def __init__(self, atm, vec, wmu, ncols):
+        import multiprocessing as mp
+        self.sub = _subcube(atm, ncols)
+        self.vec, self.wmu, self.ncols = vec, wmu, ncols
+        self.cores = os.cpu_count() or 1
+        ncell = self.sub["nx"] * self.sub["ny"] * self.sub["nz"]
+        nchunk = max(1, self.cores)
+        edges = np.linspace(0, ncell, nchunk + 1).astype(int)
+        self.chunks = [(int(a), int(b)) for a, b in zip(edges[:-1], edges[1:]) if b > a]
+        self.parts = [_cells(self.sub, a, b) for a, b in self.chunks]
+        self.pool = mp.get_context("spawn").Pool(self.cores)
+        self.work = vec.shape[0] * ncell
+
+    def step(self, nu, llam):
+        from oracle import oracle as O
+        nray = self.vec.shape[0]
+        tasks = [(part, nu, llam, self.vec[r]) for r in range(nray) for part in self.parts]
+        res = self.pool.map(_ref_units, tasks, chunksize=1)
+        k, sweeps = 0, []
+        for r in range(nray):
+            chi = np.concatenate([res[k + i][0] for i in range(len(self.parts))])
+            S = np.concatenate([res[k + i][1] for i in range(len(self.parts))])
+            k += len(self.parts)
+            sweeps.append((self.sub, chi, S, self.vec[r]))
+        tops = self.pool.map(_ref_sweep, sweeps, chunksize=1)
+        return O.save_intensity(nu, np.stack(tops).astype(np.float32), self.wmu)[1]
+
+    def close(self):
+        self.pool.close()
+        self.pool.join()
+
+    def describe(self, nf, seconds):
+        return (f"{self.ncols}x{self.ncols} columns x {self.sub['nz']} planes ({len(self.sub['slab_nz'])} slabs) x "
+                f"{nf} frequencies x {self.vec.shape[0]} rays of the same cube and windows; opacity over "
+                f"(ray, {len(self.parts)} cell chunks), sweep per ray, {self.cores} processes; "
+                f"C restatement of the reference (-O3 -march=x86-64-v3), {seconds:.1f} s")
 
 
 def run_reference(a):
-    """The reference arm: the CPU restatement on all host cores, bounded sample per step."""
+    """The reference arm: the CPU restatement on all host cores, the same windows as
+    the device arm times, a bounded block of columns per step."""
     ws, rank, _ = _dist()
     if rank != 0:
         return
-    import multiprocessing as mp
     atm, llam_all, nu_all, vec, wmu = _make_inputs(a.nf)
-    nu, llam = _window(llam_all, nu_all, a.nf, NFREQ_TOTAL // a.nf // 2)
-    cores = os.cpu_count() or 1
-    ncols = 4
-    sub = _subcube(atm, ncols)
-    tasks = [(sub, nu, llam, vec[r:r + 1], wmu[r:r + 1]) for r in range(wmu.size)]
-    ctx = mp.get_context("spawn")
-    with ctx.Pool(min(cores, len(tasks))) as pool:
-        for _ in range(a.warmup):
-            pool.map(_ref_task, tasks[:1])
-        t0 = time.perf_counter()
-        for _ in range(a.steps):
-            pool.map(_ref_task, tasks)
-        dt = (time.perf_counter() - t0) / a.steps
-    work = wmu.size * ncols * ncols * atm["nz"] * a.nf
-    value = work / dt / 1e9
-    sample = (f"{ncols}x{ncols} columns x 240 planes x {a.nf} frequencies x {wmu.size} rays per step, "
-              f"rays spread over {min(cores, len(tasks))} processes")
-    cfg = _workload(a.nf)
-    cfg["sample"] = sample
+    steps_total = a.warmup + a.steps
+    wins = [i % (NFREQ_TOTAL // a.nf) for i in range(steps_total)]
+    ref = CpuReference(atm, vec, wmu, ncols=REF_NCOLS)
+    for i in range(a.warmup):
+        ref.step(*_window(llam_all, nu_all, a.nf, wins[i]))
+    t0 = time.perf_counter()
+    for i in range(a.warmup, steps_total):
+        ref.step(*_window(llam_all, nu_all, a.nf, wins[i]))
+    dt = (time.perf_counter() - t0) / a.steps
+    ref.close()
+    value = ref.work * a.nf / dt / 1e9
+    sample = ref.describe(a.nf, dt * a.steps)
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": cfg,
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": _workload(a.nf),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": ref.cores, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
-
-
-def _issue_from_profiles():
-    """The issue-slot utilisation ncu measured for the line-opacity kernel (the
-    fraction of cycles an SM sub-partition issued), from the committed summary."""
-    path = os.path.join(ROOT, "profiles", "k_lte_opacity_units_lane_c1_48.md")
-    try:
-        for line in open(path):
-            if line.startswith("issue_active_fraction:"):
-                return float(line.split(":")[1])
-    except OSError:
-        pass
-    return None
 
 
 def _nlte_ali(steps=2):
@@ -420,6 +450,62 @@ def _optab(steps=5, warmup=3):
     return out
 
 
+def _c0(m, a):
+    """The 1D plane-parallel LTE synthesis configuration, measured beside the headline:
+    80 depths, 2000 lines in 5000-5100 A, all 20000 frequencies in 625 windows of 32,
+    5 Gauss-Legendre rays, long_char_quadratic, FP32 and the plain FP64 path; the CPU
+    restatement on a bounded sample of the windows.  Host-side window loop over the
+    device-resident column."""
+    import torch
+    from dispatch_b200 import synth
+    atm, _, _, vec, wmu = synth.lte_config("c0", nf=32, window=0)
+    llam_all, nu_all = synth.frequency_grid(5000.0, 5100.0, 20000)
+    nwin = 20000 // 32
+    dev = lambda x: torch.from_numpy(np.ascontiguousarray(x)).cuda()
+    datm = {k: (dev(v) if isinstance(v, np.ndarray) else v) for k, v in atm.items()}
+    datm["species"] = [{k: dev(v) for k, v in sp.items()} for sp in atm["species"]]
+    wins = [tuple(dev(x) for x in _window(llam_all, nu_all, 32, w)) for w in range(nwin)]
+    cur = torch.cuda.current_stream()
+    out = {"workload": "c0 1D LTE synthesis: 80 depths, 2000 lines 5000-5100 A, 20000 frequencies (625 windows "
+                       "of 32), 5 Gauss rays, long_char_quadratic", "unit": UNIT,
+           "ray_pt_nu": 5 * 80 * 20000, "data": "synthetic (grey column, random line list)"}
+    flux = {}
+    for fp64 in (False, True):
+        for nu_d, llam_d in wins[:3]:
+            m.lte_synthesis(datm, nu_d, llam_d, vec, wmu, device=True, fp64=fp64)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(cur)
+        fl = [m.lte_synthesis(datm, nu_d, llam_d, vec, wmu, device=True, fp64=fp64)[1] for nu_d, llam_d in wins]
+        e1.record(cur)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        flux[fp64] = torch.cat(fl).double()
+        out["fp64" if fp64 else "fp32"] = {"ms": ms, "value": out["ray_pt_nu"] / (ms / 1e3) / 1e9}
+    out["fp32_over_fp64"] = out["fp32"]["value"] / out["fp64"]["value"]
+    out["max_rel_flux_err_fp32_vs_fp64"] = float((torch.abs(flux[False] - flux[True]) / flux[True]).max().item())
+    # the CPU restatement: every 25th window, one process per window over all cores
+    import multiprocessing as mp
+    sample = list(range(0, nwin, 25))
+    tasks = [(atm, *_window(llam_all, nu_all, 32, w), vec, wmu) for w in sample]
+    cores = min(os.cpu_count() or 1, len(tasks))
+    with mp.get_context("spawn").Pool(cores) as pool:
+        pool.map(_c0_task, tasks[:cores])
+        t0 = time.perf_counter()
+        pool.map(_c0_task, tasks, chunksize=1)
+        dt = time.perf_counter() - t0
+    out["cpu_baseline"] = {"value": 5 * 80 * 32 * len(sample) / dt / 1e9, "unit": UNIT, "cores": cores,
+                           "kind": "port", "sample": f"{len(sample)} of the 625 windows (every 25th), one process "
+                                                     f"per window, C restatement (-O3 -march=x86-64-v3), {dt:.1f} s"}
+    return out
+
+
+def _c0_task(args):
+    atm, nu, llam, vec, wmu = args
+    from oracle import pipeline as P
+    return P.lte_synthesis(atm, nu, llam, vec, wmu)[1]
+
+
 def run_b200(a):
     import torch
     import torch.distributed as dist
@@ -489,19 +575,35 @@ def run_b200(a):
     m.profile_enable(False)
     peaks = _peaks()
     peak = peaks["hbm_gbs"] if peaks else 6650.0
-    bytes_launch = 8.0 * ncell * nf                          # chi and Snu read once per ray point frequency
+    peak_kind = "measured" if peaks else "fallback"
+    # the step's dominant kernel, the line opacity, is bound by instruction issue (its
+    # DRAM traffic is a few bytes per cell): its roofline is the issue rate of the SMs,
+    # 148 SMs x 4 schedulers x one warp instruction per cycle at the SM clock sampled
+    # during the timed region; its instructions per launch are the ncu count of the
+    # small case per (cell, line), times this launch's cells and lines
+    nline = sum(len(sp["llam0"]) for sp in atm["species"])
+    sm_hz = (clocks.get("sm_mhz") or 1965.0) * 1e6
+    issue_peak = 148 * 4 * sm_hz / 1e9
+    op_launch_s = op_ms / op_n / 1e3 if op_n else None
+    inst = (NCU_OPACITY_WARP_INST_PER_CELL_LINE * ncell * nline) if NCU_OPACITY_WARP_INST_PER_CELL_LINE else None
+    op_achieved = inst / op_launch_s / 1e9 if (inst and op_launch_s) else None
+    roofline = {"kernel": "k_lte_opacity_units_lane<32> (line opacity + transfer units, one ray)", "bound": "issue",
+                "achieved": op_achieved, "peak": issue_peak, "unit": "G warp-instructions/s",
+                "frac": op_achieved / issue_peak if op_achieved else None,
+                "traffic": (NCU_OPACITY_DRAM_READ_BYTES_PER_CELL + 8.0 * nf) * ncell,
+                "warp_instructions_per_launch": inst, "share_of_step": op_ms / (op_ms + sv_ms + rd_ms) if op_ms else None,
+                "peak_source": "148 SMs x 4 issue slots x sampled SM clock",
+                "hbm_view": {"algorithmic_bytes_per_launch": (8.0 * nf + 52.0) * ncell,
+                             "achieved_gbs": (8.0 * nf + 52.0) * ncell / op_launch_s / 1e9 if op_launch_s else None,
+                             "peak_gbs": peak, "peak_source": peak_kind}}
+    # the formal-solver sweep: HBM roofline, chi and Snu read once per ray point frequency
+    bytes_launch = 8.0 * ncell * nf
     achieved = bytes_launch / (sv_ms / sv_n / 1e3) / 1e9 if sv_n else None
-    traffic = _traffic_from_profiles(ncell, nf)
-    roofline = {"kernel": "k_quad_rot_column (rotate_array + long_char_quadratic, all slabs)", "bound": "hbm",
-                "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak if achieved else None,
-                "traffic": traffic, "peak_source": "measured" if peaks else "fallback",
-                "algorithmic_bytes_per_launch": bytes_launch}
-    # the step's dominant kernel is the line opacity, bound by instruction issue
-    # (FP32/ALU, 0.01 % of DRAM peak); its roofline is the issue rate
-    dominant = {"kernel": "k_lte_opacity_units_lane<32> (line opacity + transfer units, every ray)",
-                "share_of_step": op_ms / (op_ms + sv_ms + rd_ms) if op_ms else None, "bound": "issue (fp32 alu)",
-                "issue_active_frac": _issue_from_profiles(),
-                "issue_source": "ncu smsp__issue_active, profiles/k_lte_opacity_units_lane_c1_48.md (48^3 case)"}
+    roofline_sweep = {"kernel": "k_quad_rot_column2 (rotate_array + long_char_quadratic, all slabs, one ray)",
+                      "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                      "frac": achieved / peak if achieved else None,
+                      "traffic": NCU_SWEEP_DRAM_BYTES_PER_CELL_FREQ * ncell * nf, "peak_source": peak_kind,
+                      "algorithmic_bytes_per_launch": bytes_launch}
     stages = {"opacity_ms_per_step": op_ms, "opacity_launches": op_n, "solve_ms_per_step": sv_ms,
               "solve_launches": sv_n, "reduce_ms_per_step": rd_ms,
               "solve_gpt_per_s": work_per_step / (sv_ms / 1e3) / 1e9 if sv_ms else None}
@@ -529,38 +631,51 @@ def run_b200(a):
     e2e = {"value": ws * work_per_step / e2e_s / 1e9, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
            "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_s * 1e3}
 
-    # the plain FP64 path on the same window, and the FP32 flux error against it
+    # the plain FP64 path on the same window (FP64 end to end: line opacity, QLG-bot,
+    # transfer units, rotate_array and the quadratic solver), and the FP32 error
+    # against it for each output
     fp64 = None
     if not a.no_fp64:
         nu_d, llam_d = dwin[a.warmup]
-        _, f32, it32 = m.lte_synthesis(datm, nu_d, llam_d, vec, wmu, device=True, return_itop=True)
+        ie32, f32, it32 = m.lte_synthesis(datm, nu_d, llam_d, vec, wmu, device=True, return_itop=True)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        _, f64, _ = m.lte_synthesis(datm, nu_d, llam_d, vec, wmu, device=True, fp64=True)
+        ie64, f64, it64 = m.lte_synthesis(datm, nu_d, llam_d, vec, wmu, device=True, fp64=True, return_itop=True)
         e1.record(stream)
         torch.cuda.synchronize()
         t64 = e0.elapsed_time(e1)
-        err = float(torch.max(torch.abs(f32 - f64) / torch.abs(f64)).item())
-        # the emergent intensity of every column and ray: the flux averages the columns'
-        # independent FP32 roundings away, a single column keeps them
-        _, _, it64 = m.lte_synthesis(datm, nu_d, llam_d, vec, wmu, device=True, fp64=True, return_itop=True)
-        rel = torch.abs(it32.double() - it64) / torch.clamp(torch.abs(it64), min=1e-300)
-        err_col = float(rel.max().item())
-        err_col_med = float(rel.flatten()[:: max(1, rel.numel() // 1000000)].median().item())
-        del it32, it64, rel
+
+        def rel(x, y):
+            r = (torch.abs(x.double() - y.double()) / torch.clamp(torch.abs(y.double()), min=1e-300)).flatten()
+            med = float(r[:: max(1, r.numel() // 1000000)].median().item())
+            return {"max": float(r.max().item()), "median": med}
+
+        errors = {"flux": rel(f32, f64), "ie": rel(ie32, ie64), "I_top": rel(it32, it64)}
+        del it32, it64
+        c32, s32 = m.lte_transfer_units(datm, nu_d, llam_d, vec[6], device=True)
+        c64, s64 = m.lte_transfer_units(datm, nu_d, llam_d, vec[6], device=True, fp64=True)
+        torch.cuda.synchronize()
+        errors["chi"] = rel(c32, c64)
+        errors["S"] = rel(s32, s64)
+        del c32, s32, c64, s64
+        torch.cuda.empty_cache()
         m.profile_enable(True)
         m.lte_synthesis(datm, nu_d, llam_d, vec, wmu, device=True, fp64=True)
+        op64_ms, _ = m.profile_read(m.STAGE_OPACITY)
         sv64_ms, sv64_n = m.profile_read(m.STAGE_SOLVE)
         m.profile_enable(False)
         fp64 = {"value": work_per_step / (t64 / 1e3) / 1e9, "unit": UNIT, "ms_per_step": t64,
                 "fp32_over_fp64": value / ws / (work_per_step / (t64 / 1e3) / 1e9),
-                "max_rel_flux_err_fp32_vs_fp64": err,
-                "max_rel_column_intensity_err_fp32_vs_fp64": err_col,
-                "median_rel_column_intensity_err_fp32_vs_fp64": err_col_med,
-                "solve_ms_per_step": sv64_ms, "solve_launches": sv64_n,
+                "fp32_error_vs_fp64": errors,
+                "error_note": "relative; chi and S of ray 7 (mu 0.45), I_top every column and ray, ie and flux of "
+                              "the window; single points of chi/S/I_top can differ by a QLG table node (FP32 and "
+                              "FP64 snap a point to neighbouring nodes)",
+                "opacity_ms_per_step": op64_ms, "solve_ms_per_step": sv64_ms, "solve_launches": sv64_n,
+                "opacity_fp32_over_fp64": op64_ms / op_ms if op_ms else None,
                 "solve_fp32_over_fp64": sv64_ms / sv_ms if sv_ms else None,
-                "path": "same kernels in FP64 for units, rotation and solver, one launch per ray and slab"}
+                "path": "FP64 end to end: line opacity and QLG-bot (fp64 tables, exp, log), transfer units, "
+                        "rotate_array and long_char_quadratic, one launch per ray and slab"}
 
     nlte = batched = optab = None
     if rank == 0 and not a.no_ali:
@@ -569,10 +684,22 @@ def run_b200(a):
     if rank == 0 and not a.no_optab:
         optab = _optab()
 
+    c0 = None
+    if rank == 0 and not a.no_c0:
+        c0 = _c0(m, a)
+
     cpu = None
     if rank == 0 and not a.no_cpu_baseline:
+        # the same block sampler as the reference arm, the first timed window
+        ref = CpuReference(atm, vec, wmu, ncols=REF_NCOLS)
         nu, llam = _window(llam_all, nu_all, nf, wins[a.warmup])
-        cpu = _cpu_baseline(atm, nu, llam, vec, wmu)
+        ref.step(nu, llam)
+        t0 = time.perf_counter()
+        ref.step(nu, llam)
+        dt = time.perf_counter() - t0
+        ref.close()
+        cpu = {"value": ref.work * nf / dt / 1e9, "unit": UNIT, "cores": ref.cores, "kind": "port",
+               "sample": ref.describe(nf, dt)}
 
     if ws > 1:
         dist.destroy_process_group()
@@ -581,10 +708,9 @@ def run_b200(a):
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic (seeded grey cube, random line list)", "config": _workload(nf, a.cube),
-            "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline, "dominant_kernel": dominant,
-            "cpu_baseline": cpu,
-            "clocks": clocks, "stages": stages, "fp64_plain": fp64, "nlte_ali": nlte,
-            "nlte_batched": batched, "optab": optab}
+            "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline, "roofline_sweep": roofline_sweep,
+            "cpu_baseline": cpu, "clocks": clocks, "stages": stages, "fp64_plain": fp64, "c0_1d": c0,
+            "nlte_ali": nlte, "nlte_batched": batched, "optab": optab}
     print(json.dumps(line), flush=True)
 
 

@@ -399,8 +399,12 @@ static inline float bot_eval(const float *tgx, const float *th2x, const qlg_coef
   float xs = fabsf(x) * c->ih;
   float u = xs * xs;
   float L = 1.0f / (1.0f + u);
-  int ig = (int)lroundf(fminf(xs * QLG_XSCL, QLG_RNX));
-  if (ig < 0) ig = 0;
+  /* nint(y) for y = min(xs*800, 9019) >= 0: y + 0.5f is exact or rounds to an
+   * integer no larger than floor(y + 0.5) on [0.5, 9019], and every y below 0.5
+   * (including the float just below, whose sum rounds up to 1) snaps to node 0;
+   * written without lroundf so the point loop vectorises */
+  const float y = fminf(xs * QLG_XSCL, QLG_RNX);
+  const int ig = y < 0.5f ? 0 : (int)(y + 0.5f);
   float G = tgx[ig], W = th2x[ig];
   float p = fmaf(c->cZH, W, c->cL2);
   p = fmaf(L, p, c->bL);
@@ -480,7 +484,32 @@ static int line_sweep(const float *tgx, const float *th2x, const qlg_cell_t *w, 
   *fb = ic + noff < nf ? ic + noff : nf;
   if (*fa > *fb) return 0;
   float x0 = x1 - (float)(i1 - *fa);
-  for (int f = 0; f <= *fb - *fa; f++) K[f] = bot_eval(tgx, th2x, &c, x0 + (float)f);
+  /* The last node's TGX is subnormal, and most window points of most lines snap to
+   * it; its product with gG is the same for every such point, so it is formed once
+   * per line (the same rounding), which keeps subnormal arithmetic -- microcoded
+   * and a hundred times slower on x86 -- out of the point loop. */
+  const float g_end = tgx[QLG_NX] * c.gG;
+  /* That product is itself often a nonzero subnormal.  The last step at such points,
+   * fma(L, p, g), is then taken on operands scaled by 2^64: exact scalings, so the
+   * rounded result is the same whenever it is normal (else the direct form). */
+  const int g_sub = g_end != 0.0f && fabsf(g_end) < FLT_MIN;
+  const float g_big = g_end * 18446744073709551616.0f;      /* 2^64, exact */
+  for (int f = 0; f <= *fb - *fa; f++) {
+    const float x = x0 + (float)f;
+    const float xs = fabsf(x) * c.ih;
+    const float u = xs * xs;
+    const float L = 1.0f / (1.0f + u);
+    const float y = fminf(xs * QLG_XSCL, QLG_RNX);
+    const int ig = y < 0.5f ? 0 : (int)(y + 0.5f);
+    float p = fmaf(c.cZH, th2x[ig], c.cL2);
+    p = fmaf(L, p, c.bL);
+    if (ig == QLG_NX && g_sub) {
+      const float k = fmaf(L, p * 18446744073709551616.0f, g_big) * 5.42101086242752217e-20f;  /* 2^-64 */
+      K[f] = fabsf(k) >= FLT_MIN ? k : fmaf(L, p, g_end);
+    } else {
+      K[f] = fmaf(L, p, ig == QLG_NX ? g_end : tgx[ig] * c.gG);
+    }
+  }
   return *fb - *fa + 1;
 }
 
