@@ -46,6 +46,7 @@ def _args():
     p.add_argument("--no-ali", action="store_true", help="skip the NLTE measurements (3D window, batched columns)")
     p.add_argument("--no-optab", action="store_true", help="skip the sampled opacity table measurement")
     p.add_argument("--no-c0", action="store_true", help="skip the 1D LTE synthesis measurement")
+    p.add_argument("--no-c4", action="store_true", help="skip the differentiable (adjoint) measurement")
     p.add_argument("--cube", type=int, default=240, help="cube edge (240 = the configuration; smaller for profiling)")
     # single cases for timing and profiling one kernel family (no JSON line)
     p.add_argument("--case", default="c1", choices=["c1", "ali-window", "ali-columns", "optab"],
@@ -450,6 +451,67 @@ def _optab(steps=5, warmup=3):
     return out
 
 
+def _c4(m, nwin=2):
+    """The differentiable 3D LTE configuration, measured beside the headline: the
+    96x96x128 seeded cube (8 slabs of 16 planes), ten species of 100 lines in
+    6000-6050 A, windows of 32 of the 8000 frequencies, 13 rays.  Per window: the FP32
+    forward pass (m3d_lte_synthesis), its adjoint (m3d_lte_synthesis_adjoint: the
+    gradients with respect to temperature, e_kT, the Doppler factors, lnbase and every
+    line's gpref), and the plain FP64 forward.  Device-resident inputs; CUDA events on
+    torch's stream."""
+    import torch
+    from dispatch_b200 import synth
+    atm, _, _, vec, wmu, raw = synth.lte_config_c4()
+    dev = lambda x: torch.from_numpy(np.ascontiguousarray(x)).cuda()
+    datm = {k: (dev(v) if isinstance(v, np.ndarray) else v) for k, v in atm.items()}
+    datm["species"] = [{k: dev(v) for k, v in sp.items()} for sp in atm["species"]]
+    ncell = atm["nx"] * atm["ny"] * atm["nz"]
+    nline = sum(len(sp["llam0"]) for sp in atm["species"])
+    wins = [nwin_i * 97 % 250 for nwin_i in range(1, nwin + 1)]
+    cur = torch.cuda.current_stream()
+    rng = np.random.default_rng(5)
+    g_flux = dev(rng.uniform(0.5, 1.5, 32).astype(np.float32))
+    grads = {"temp": torch.zeros(ncell, device="cuda"), "chi_c": torch.zeros(ncell, device="cuda"),
+             "e_kT": torch.zeros(ncell, device="cuda"), "inv_df": torch.zeros((10, ncell), device="cuda"),
+             "lnbase": torch.zeros((10, ncell), device="cuda"), "gpref": torch.zeros(nline, device="cuda")}
+    m.set_stream(cur.cuda_stream or 1)
+
+    def timed(fn):
+        fn(wins[0])
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(cur)
+        for w in wins:
+            fn(w)
+        e1.record(cur)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / len(wins)
+
+    def win(w):
+        return tuple(dev(x) for x in _window(raw["llam_all"], raw["nu_all"], 32, w))
+
+    dw = {w: win(w) for w in wins}
+    fwd = timed(lambda w: m.lte_synthesis(datm, dw[w][0], dw[w][1], vec, wmu, device=True))
+    bwd = timed(lambda w: m.lte_synthesis_adjoint(datm, dw[w][0], dw[w][1], vec, wmu, g_flux, device=True,
+                                                 grads=grads))
+    f64 = timed(lambda w: m.lte_synthesis(datm, dw[w][0], dw[w][1], vec, wmu, device=True, fp64=True))
+    work = vec.shape[0] * ncell * 32
+    out = {"workload": "c4 differentiable 3D LTE: 96x96x128 cube in 8 slabs, 10 species x 100 lines 6000-6050 A, "
+                       "windows of 32 of 8000 frequencies, 13 rays; forward, adjoint (d/dT, e_kT, Doppler "
+                       "factors, lnbase, every line's gpref) and the plain FP64 forward per window",
+           "unit": UNIT, "windows_timed": wins, "ray_pt_nu_per_window": work,
+           "forward_fp32": {"ms": fwd, "value": work / (fwd / 1e3) / 1e9},
+           "adjoint_fp32": {"ms": bwd, "value": work / (bwd / 1e3) / 1e9},
+           "forward_plus_adjoint_fp32": {"ms": fwd + bwd, "value": work / ((fwd + bwd) / 1e3) / 1e9},
+           "forward_fp64_plain": {"ms": f64, "value": work / (f64 / 1e3) / 1e9},
+           "fp32_forward_plus_adjoint_over_fp64_forward": f64 / (fwd + bwd),
+           "gradients_finite": bool(all(torch.isfinite(v).all() for v in grads.values())),
+           "data": "synthetic (seeded cube, ten-species random line list)"}
+    del datm, grads
+    torch.cuda.empty_cache()
+    return out
+
+
 def _c0(m, a):
     """The 1D plane-parallel LTE synthesis configuration, measured beside the headline:
     80 depths, 2000 lines in 5000-5100 A, all 20000 frequencies in 625 windows of 32,
@@ -684,9 +746,12 @@ def run_b200(a):
     if rank == 0 and not a.no_optab:
         optab = _optab()
 
-    c0 = None
+    c0 = c4 = None
     if rank == 0 and not a.no_c0:
         c0 = _c0(m, a)
+    if rank == 0 and not a.no_c4:
+        c4 = _c4(m)
+        m.set_stream(stream.cuda_stream or 1)
 
     cpu = None
     if rank == 0 and not a.no_cpu_baseline:
@@ -709,7 +774,7 @@ def run_b200(a):
             "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic (seeded grey cube, random line list)", "config": _workload(nf, a.cube),
             "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline, "roofline_sweep": roofline_sweep,
-            "cpu_baseline": cpu, "clocks": clocks, "stages": stages, "fp64_plain": fp64, "c0_1d": c0,
+            "cpu_baseline": cpu, "clocks": clocks, "stages": stages, "fp64_plain": fp64, "c0_1d": c0, "c4_adjoint": c4,
             "nlte_ali": nlte, "nlte_batched": batched, "optab": optab}
     print(json.dumps(line), flush=True)
 

@@ -26,6 +26,7 @@
 #include "m3d_columns.cuh"
 #include "m3d_optab.cuh"
 #include "m3d_hprof.cuh"
+#include "m3d_adjoint.cuh"
 
 using namespace m3d;
 
@@ -38,6 +39,7 @@ struct Ctx {
   float *d_tgx = nullptr, *d_th2x = nullptr;
   float2 *d_tab = nullptr;  // (TGX(i), TH2X(i)) interleaved, read by the kernels
   double2 *d_tab64 = nullptr;  // the same two tables in fp64, for the plain FP64 opacity
+  float *d_dW = nullptr;       // W'(u) of the TH2X table, for the adjoint (built on first use)
   std::vector<float> h_tgx, h_th2x;
   long long launches = 0;
   std::string err;
@@ -474,6 +476,8 @@ int m3d_free(void) {
   g_ctx.d_tab = nullptr;
   if (g_ctx.d_tab64) cudaFree(g_ctx.d_tab64);
   g_ctx.d_tab64 = nullptr;
+  if (g_ctx.d_dW) cudaFree(g_ctx.d_dW);
+  g_ctx.d_dW = nullptr;
   if (g_ctx.own) cudaStreamDestroy(g_ctx.own);
   g_ctx.own = g_ctx.stream = nullptr;
   g_ctx.init = false;
@@ -1475,6 +1479,7 @@ int m3d_lte_synthesis(const m3d_atmos_t *atm, int nf, const double *nu, const do
 #include "m3d_optab_api.inc"
 #include "m3d_hprof_api.inc"
 #include "m3d_io_api.inc"
+#include "m3d_adjoint_api.inc"
 
 // ===========================================================================
 // rotate_array without any allocation.

@@ -313,7 +313,9 @@ __device__ __forceinline__ float pick(const float (&a)[NF], int i) {
 // REACH: the line list carries reach_in (has_reach): the lines select_lines kept,
 // and lines centred beyond the window take the unfloored reference at the nearer
 // end, no peak test and a window capped by their reach (linelist_mod.f90:844-854, 914-921)
-template <int NF, typename TO, bool REACH>
+// CHIL: write the line opacity chi_l of the window itself to chi_out (S_out unused):
+// the input of the adjoint's transfer units
+template <int NF, typename TO, bool REACH, bool CHIL = false>
 __global__ void __launch_bounds__(256, 3) k_lte_opacity_units_lane(AtmosDev A, GridArgs G, const double *nu, double v0,
                                                                    double v1, double v2, TO *chi_out, TO *S_out,
                                                                    const float2 *tab) {
@@ -421,6 +423,15 @@ __global__ void __launch_bounds__(256, 3) k_lte_opacity_units_lane(AtmosDev A, G
         else
           deposit_window<NF, false>(chl, s_tab, cf, x0, kfa, fa, fb, full, far);
       }
+    }
+    if (CHIL) {
+      if (live) {
+        float *co = reinterpret_cast<float *>(chi_out) + (size_t)NF * cell;
+#pragma unroll
+        for (int f = 0; f < NF; f += 4)
+          *reinterpret_cast<float4 *>(co + f) = make_float4(chl[f], chl[f + 1], chl[f + 2], chl[f + 3]);
+      }
+      continue;
     }
     // epilogue: transfer units, written as 16-byte stores of this cell's row
     if (live) {

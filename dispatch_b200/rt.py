@@ -392,6 +392,51 @@ def lte_transfer_units(atm: dict, nu, llam, vec, fp64=False, device=False, out=N
     return chi, S
 
 
+class LteGrad(C.Structure):
+    """m3d_lte_grad_t."""
+
+    _fields_ = [(k, C.c_void_p) for k in ("temp", "chi_c", "e_kT", "inv_df", "lnbase", "gpref")]
+
+
+def lte_synthesis_adjoint(atm: dict, nu, llam, vec, wmu, g_flux, device=False, grads=None):
+    """The reverse mode of lte_synthesis for one window of 32 frequencies
+    (m3d_lte_synthesis_adjoint): given g_flux = dL/dflux (nf,), returns the dict of
+    dL/d(input): temp, chi_c, e_kT (ncell,), inv_df, lnbase (nspecies, ncell), gpref
+    (all lines, species in order).  grads: arrays to accumulate into (else zeros)."""
+    init()
+    keep = []
+    a = _atmos(atm, keep)
+    vec = np.ascontiguousarray(vec, np.float64)
+    wmu = np.ascontiguousarray(wmu, np.float64)
+    nray = wmu.size
+    nf = int(nu.shape[0])
+    ncell = a.nx * a.ny * a.nz
+    nsp = len(atm["species"])
+    nline = sum(len(sp["llam0"]) for sp in atm["species"])
+    if grads is None:
+        if device:
+            import torch
+            dev = atm["temp"].device
+            z = lambda *shape: torch.zeros(shape, dtype=torch.float32, device=dev)
+        else:
+            z = lambda *shape: np.zeros(shape, _F32)
+        grads = {"temp": z(ncell), "chi_c": z(ncell), "e_kT": z(ncell), "inv_df": z(max(nsp, 1), ncell),
+                 "lnbase": z(max(nsp, 1), ncell), "gpref": z(max(nline, 1))}
+    if not device:
+        nu = np.ascontiguousarray(nu, np.float64)
+        llam = np.ascontiguousarray(llam, np.float64)
+        g_flux = np.ascontiguousarray(g_flux, _F32)
+    else:
+        order_after_torch(grads["temp"])
+    g = LteGrad(*[ptr(grads[k]) for k in ("temp", "chi_c", "e_kT", "inv_df", "lnbase", "gpref")])
+    flags = DEVICE_PTRS if device else 0
+    check(lib().m3d_lte_synthesis_adjoint(C.byref(a), C.c_int(nf), ptr(nu), ptr(llam), C.c_int(nray), ptr(vec),
+                                          ptr(wmu), ptr(g_flux), C.byref(g), C.c_uint(flags)),
+          "m3d_lte_synthesis_adjoint")
+    del keep
+    return grads
+
+
 def eta_spread(vecs, ds, dz_upstream=None, one_dimensional=False) -> tuple[int, int]:
     """eta_rx, eta_ry of update_eta_mask (rt_patch_mod.f90:3683-3700): the horizontal
     reach of an upwind point over the slab's directions, plus the cell beyond it."""

@@ -363,6 +363,56 @@ def lte_config(kind: str, seed: int | None = None, nf: int | None = None, window
     return atm, np.ascontiguousarray(nu_all[sl]), np.ascontiguousarray(llam_all[sl]), vec, wmu
 
 
+# ---- the differentiable configuration: ten species ------------------------------------
+# (element, atomic mass [u], abundance log eps with log eps(H) = 12): a fixed table of
+# ten metals at roughly solar abundances, the species of the synthetic line list
+C4_SPECIES = (("Fe", 55.845, 7.50), ("Ti", 47.867, 4.95), ("Cr", 51.996, 5.64), ("Ni", 58.693, 6.22),
+              ("Ca", 40.078, 6.34), ("Mg", 24.305, 7.60), ("Si", 28.086, 7.51), ("Na", 22.990, 6.24),
+              ("Mn", 54.938, 5.43), ("Co", 58.933, 4.99))
+
+
+def lte_config_c4(seed: int = 4, size=None, nf: int = 32, window: int = 0, nline_per_species: int = 100,
+                  nfree: int = 8000, lam=(6000.0, 6050.0), cube=None):
+    """One window of the differentiable 3D LTE configuration: a 96x96x128 seeded cube
+    (cube_atmosphere, 8 slabs of 16 planes), 100 lines per species of the ten in
+    C4_SPECIES, uniform in 6000-6050 A, 8000 frequencies uniform in ln(lambda), 13
+    Lobatto rays.  size = (nx, ny, nz) for a smaller cube.  Returns (atm, nu, llam,
+    vec, wmu, raw): raw holds what a differentiable caller re-forms the per-cell fields
+    from -- temp, nH, the species' masses, abundances and raw line parameters."""
+    nx, ny, nz = (96, 96, 128) if size is None else size
+    rng = np.random.default_rng(seed + 1000)
+    if cube is None:
+        cube = cube_atmosphere(seed, nx, ny, nz)
+    temp, nH, ne, chi_c, vz = (cube[k] for k in ("temp", "nH", "ne", "chi_c", "vz"))
+    species, raws = [], []
+    for name, awgt, abund in C4_SPECIES:
+        raw = random_linelist(rng, nline_per_species, *lam)
+        n_x = 10.0 ** (abund - 12.0) * nH
+        sp = species_arrays(raw, temp, n_x, awgt=awgt)
+        species.append({k: (np.ascontiguousarray(v).ravel() if k in ("inv_df", "vbar2", "lnbase") else v)
+                        for k, v in sp.items()})
+        raws.append(raw)
+    llam_all, nu_all = frequency_grid(lam[0], lam[1], nfree)
+    sl = slice(window * nf, (window + 1) * nf)
+    ds_cm = cube["ds_cm"]
+    ds_code = tuple(d / 1e8 for d in ds_cm)
+    nslab = max(1, nz // 16)
+    slab_nz = [nz // nslab] * nslab
+    slab_nz[-1] += nz - sum(slab_nz)
+    atm = {"nx": nx, "ny": ny, "nz": nz, "slab_nz": slab_nz, "ds_cm": ds_cm, "ds_code": ds_code,
+           "pivot_z": nz * ds_code[2], "ray_offset": (0.0, 0.0),
+           "temp": np.ascontiguousarray(temp, np.float32).ravel(),
+           "chi_c": np.ascontiguousarray(chi_c, np.float32).ravel(),
+           "vx": np.zeros(temp.size, np.float32), "vy": np.zeros(temp.size, np.float32),
+           "vz": np.ascontiguousarray(vz, np.float32).ravel(), "species": species}
+    atm.update({k: np.ascontiguousarray(v, np.float32).ravel() for k, v in cell_fields(temp, nH, ne).items()})
+    vec, wmu = lobatto_rays(4, 4)
+    raw = {"temp": np.asarray(temp, np.float64).ravel(), "nH": np.asarray(nH, np.float64).ravel(),
+           "awgt": [c[1] for c in C4_SPECIES], "abund": np.array([c[2] for c in C4_SPECIES]), "lines": raws,
+           "llam_all": llam_all, "nu_all": nu_all}
+    return atm, np.ascontiguousarray(nu_all[sl]), np.ascontiguousarray(llam_all[sl]), vec, wmu, raw
+
+
 # ---- NLTE: a seeded model atom and the per-cell inputs of its SE update ---------------
 RYDV = 13.605
 

@@ -422,6 +422,34 @@ int m3d_lte_synthesis(const m3d_atmos_t *atm, int nf, const double *nu, const do
                       int nray, const double *vec, const double *wmu, void *i_top, float *ie,
                       float *flux, unsigned flags);
 
+/* Gradients of the LTE pass, accumulated (+=) by m3d_lte_synthesis_adjoint.  Cell
+ * arrays (ncell, x fastest); per-species arrays species-major; gpref the species'
+ * line lists one after the other.  Pointers follow M3D_DEVICE_PTRS. */
+typedef struct m3d_lte_grad {
+  float *temp;    /* (ncell) dL/dtemp through the LTE background (beta, Bnu) only */
+  float *chi_c;   /* (ncell) dL/dchi_c */
+  float *e_kT;    /* (ncell) dL/de_kT (the Boltzmann factors of every species) */
+  float *inv_df;  /* (nspecies, ncell) dL/dinv_df (the Doppler width in the profile and in S) */
+  float *lnbase;  /* (nspecies, ncell) dL/dlnbase */
+  float *gpref;   /* (sum of nline) dL/dgpref: gpref = log gf ln 10 + const, so this is dL/dlog gf / ln 10 */
+} m3d_lte_grad_t;
+
+/* The reverse mode of m3d_lte_synthesis for one window of 32 frequencies and every
+ * ray: given g_flux = dL/dflux (nf), adds dL/d(input) into grad.  No counterpart in
+ * the reference (its abundance fits take finite differences of whole syntheses,
+ * tumult/abundance.py).  Stage by stage, backwards: save_intensity; the fused
+ * rotate_array + long_char_quadratic sweep reversed per column from intensities
+ * checkpointed at the slab faces; the transpose of rotate_array; the transfer units;
+ * add_opacity_equi's line loop replayed with the forward's decisions.  Window
+ * limits, tolerance tests, limiter branches and clamps are held as the forward takes
+ * them.  QLG-bot snaps to the nearest table node; its derivative is that of the
+ * continuous member (G(u) = 2^-u, W'(u) from the table's differences).  Damping,
+ * velocities, ne and tothi are held fixed.  Slabs of at most 64 planes, at most 64
+ * slabs, no reach_in; the FP32 pass only. */
+int m3d_lte_synthesis_adjoint(const m3d_atmos_t *atm, int nf, const double *nu, const double *llam, int nray,
+                              const double *vec, const double *wmu, const float *g_flux, const m3d_lte_grad_t *grad,
+                              unsigned flags);
+
 /* ---- statistical equilibrium (FP64) ----
  * Level and transition indices are 0-based (the reference's minus one).  Per-cell
  * arrays keep the cell index fastest: b(cell, level) at b[cell + ncell*level], as
