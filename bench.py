@@ -495,6 +495,10 @@ def _c4(m, nwin=2):
     bwd = timed(lambda w: m.lte_synthesis_adjoint(datm, dw[w][0], dw[w][1], vec, wmu, g_flux, device=True,
                                                  grads=grads))
     f64 = timed(lambda w: m.lte_synthesis(datm, dw[w][0], dw[w][1], vec, wmu, device=True, fp64=True))
+    m.profile_enable(True)
+    m.lte_synthesis_adjoint(datm, dw[wins[0]][0], dw[wins[0]][1], vec, wmu, g_flux, device=True, grads=grads)
+    stages = {"opacity_ms": m.profile_read(m.STAGE_OPACITY)[0], "sweep_ms": m.profile_read(m.STAGE_SOLVE)[0]}
+    m.profile_enable(False)
     work = vec.shape[0] * ncell * 32
     out = {"workload": "c4 differentiable 3D LTE: 96x96x128 cube in 8 slabs, 10 species x 100 lines 6000-6050 A, "
                        "windows of 32 of 8000 frequencies, 13 rays; forward, adjoint (d/dT, e_kT, Doppler "
@@ -505,6 +509,7 @@ def _c4(m, nwin=2):
            "forward_plus_adjoint_fp32": {"ms": fwd + bwd, "value": work / ((fwd + bwd) / 1e3) / 1e9},
            "forward_fp64_plain": {"ms": f64, "value": work / (f64 / 1e3) / 1e9},
            "fp32_forward_plus_adjoint_over_fp64_forward": f64 / (fwd + bwd),
+           "adjoint_stages": stages,
            "gradients_finite": bool(all(torch.isfinite(v).all() for v in grads.values())),
            "data": "synthetic (seeded cube, ten-species random line list)"}
     del datm, grads

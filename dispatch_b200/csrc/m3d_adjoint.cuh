@@ -306,6 +306,19 @@ __global__ void k_unrotate_adj(int nf, int nx, int ny, int nz, const RotCol *rot
   }
 }
 
+// The transfer units of every point from its line opacity chi_l (the opacity
+// kernel's epilogue on its own): chil, chi, S (nf, ncell)
+__global__ void k_units_fwd(int nf, int ncell, const double *nu, const float *temp, const float *chi_c,
+                            float maser_chi_floor, const float *chil, float *chi, float *S) {
+  const size_t n = (size_t)nf * ncell;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const int c = (int)(i / nf), f = (int)(i % nf);
+    const float T = temp[c];
+    const float h_kT = (float)(M3D_H_K / (double)T);
+    point_units(chi_c[c], h_kT, nu[f], chil[i], chil[i], maser_chi_floor, chi[i], S[i]);
+  }
+}
+
 // The adjoint of the transfer units of one point: given dL/dchi, dL/dS and the line
 // opacity chi_l, returns dL/dchi_l and adds the point's dL/dT and dL/dchi_c.
 __device__ __forceinline__ float units_adj(float chi_c, float T, float h_kT, double nu, float chil, float fl, float g_chi,
