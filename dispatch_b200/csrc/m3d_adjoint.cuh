@@ -402,24 +402,83 @@ __device__ __forceinline__ QlgCoefD qlg_setup_dih(float gL, float S, const QlgCo
   return d;
 }
 
-// one profile point: K exactly as qlg_eval forms it, and dK/dih (the continuous
+// one profile point: K exactly as qlg_eval<MK> forms it, and dK/dih (the continuous
 // member: G(u) = 2^-u, W' from the table's differences dW)
+template <bool MK>
 __device__ __forceinline__ float qlg_eval_d(const float2 *tab, const float *dW, const QlgCoef &c, const QlgCoefD &cd,
                                             float x, float &dK_dih) {
   const float xs = fabsf(x) * c.ih;
   const float u = xs * xs;
-  const float L = __frcp_rn(1.0f + u);
+  const float L = qlg_rcp<MK>(1.0f + u);
   const float y = fminf(xs * 800.0f, 9019.0f);
   const int ig = y < 0.5f ? 0 : (int)(y + 0.5f);
   const float2 gw = tab[ig];
   const float G = gw.x, W = gw.y;
   float p = fmaf(c.cZH, W, c.cL2);
+  const float P = p;
   p = fmaf(L, p, c.bL);
   const float K = fmaf(L, p, G * c.gG);
-  const float P = fmaf(c.cZH, W, c.cL2);
-  const float dK_du = -L * L * (2.0f * L * P + c.bL) + L * L * c.cZH * dW[ig] - 0.69314718f * G * c.gG;
-  dK_dih = dK_du * (2.0f * u / c.ih) + L * L * fmaf(W, cd.cZH, cd.cL2) + L * cd.bL + G * cd.gG;
+  const float L2 = L * L;
+  const float dK_du = fmaf(L2, fmaf(c.cZH, dW[ig], -fmaf(2.0f * L, P, c.bL)), -0.69314718f * G * c.gG);
+  dK_dih = fmaf(dK_du, 2.0f * u / c.ih, fmaf(L, fmaf(L, fmaf(W, cd.cZH, cd.cL2), cd.bL), G * cd.gG));
   return K;
+}
+
+// One line's window replayed: chl gets the forward's K bit for bit (the forms the
+// forward chooses by warp vote all give the general form's bits), Gl and Hl the sums
+// of g_chil K and g_chil dK/dih.  FAR: every point beyond the table, whose last node
+// gives G, W and W' at every point, so the per-point work is the forward's far form
+// plus the derivative's few terms.
+template <int NF, bool FULL, bool FAR, bool MK>
+__device__ __forceinline__ void deposit_adj(float (&chl)[NF], const float (&gch)[NF], const float2 *s_tab,
+                                            const float *s_dW, const QlgCoef &cf, const QlgCoefD &cd, float x0,
+                                            float kfa, int fa, int fb, float &Gl, float &Hl) {
+  if (FAR) {
+    const float2 gw = s_tab[QLG_NTAB - 1];
+    const float p1 = fmaf(cf.cZH, gw.y, cf.cL2);
+    const float gg = gw.x * cf.gG;
+    const float ca = cf.cZH * s_dW[QLG_NTAB - 1], cb = -0.69314718f * gg;
+    const float e1 = fmaf(gw.y, cd.cZH, cd.cL2), e3 = gw.x * cd.gG;
+    const float r2ih = 2.0f / cf.ih;
+#pragma unroll
+    for (int f = 0; f < NF; f++) {
+      if (FULL || (f + 1 >= fa && f + 1 <= fb)) {
+        const float xs = fabsf(x0 + (FULL ? (float)f : ((float)f + kfa))) * cf.ih;
+        const float u = xs * xs;
+        const float L = qlg_rcp<MK>(1.0f + u);
+        const float K = fmaf(L, fmaf(L, p1, cf.bL), gg);
+        chl[f] = fmaf(K, 1.0f, chl[f]);
+        const float dK_du = fmaf(L * L, ca - fmaf(2.0f * L, p1, cf.bL), cb);
+        const float dKi = fmaf(dK_du, u * r2ih, fmaf(L, fmaf(L, e1, cd.bL), e3));
+        Gl = fmaf(gch[f], K, Gl);
+        Hl = fmaf(gch[f], dKi, Hl);
+      }
+    }
+  } else {
+#pragma unroll
+    for (int f = 0; f < NF; f++) {
+      if (FULL || (f + 1 >= fa && f + 1 <= fb)) {
+        float dKi;
+        const float K = qlg_eval_d<MK>(s_tab, s_dW, cf, cd, x0 + (FULL ? (float)f : ((float)f + kfa)), dKi);
+        chl[f] = fmaf(K, 1.0f, chl[f]);
+        Gl = fmaf(gch[f], K, Gl);
+        Hl = fmaf(gch[f], dKi, Hl);
+      }
+    }
+  }
+}
+
+template <int NF, bool MK>
+__device__ __forceinline__ void deposit_adj_mk(float (&chl)[NF], const float (&gch)[NF], const float2 *s_tab,
+                                               const float *s_dW, const QlgCoef &cf, const QlgCoefD &cd, float x0,
+                                               float kfa, int fa, int fb, bool full, bool far, float &Gl, float &Hl) {
+  if (far) {
+    if (full) deposit_adj<NF, true, true, MK>(chl, gch, s_tab, s_dW, cf, cd, x0, kfa, fa, fb, Gl, Hl);
+    else deposit_adj<NF, false, true, MK>(chl, gch, s_tab, s_dW, cf, cd, x0, kfa, fa, fb, Gl, Hl);
+  } else {
+    if (full) deposit_adj<NF, true, false, MK>(chl, gch, s_tab, s_dW, cf, cd, x0, kfa, fa, fb, Gl, Hl);
+    else deposit_adj<NF, false, false, MK>(chl, gch, s_tab, s_dW, cf, cd, x0, kfa, fa, fb, Gl, Hl);
+  }
 }
 
 // k_opacity_adj: the line loop of k_lte_opacity_units_lane<32> (no select_lines
@@ -514,16 +573,17 @@ __global__ void __launch_bounds__(256, 2) k_opacity_adj(AtmosDev A, GridArgs G, 
         const float kfa = (float)(1 - fa);
         const QlgCoefD cd = qlg_setup_dih(a, S, cf);
         float Gl = 0.0f, Hl = 0.0f;
-#pragma unroll
-        for (int f = 0; f < NF; f++) {
-          if (f + 1 >= fa && f + 1 <= fb) {
-            float dKi;
-            const float K = qlg_eval_d(s_tab, s_dW, cf, cd, x0 + ((float)f + kfa), dKi);
-            chl[f] = fmaf(K, 1.0f, chl[f]);
-            Gl = fmaf(gch[f], K, Gl);
-            Hl = fmaf(gch[f], dKi, Hl);
-          }
-        }
+        // the forward's window forms, taken by the same warp votes
+        const float xe = x0 + (float)(fb - fa);
+        const float xnear = (x0 > 0.0f) ? x0 : ((xe < 0.0f) ? -xe : 0.0f);
+        const unsigned conv = __activemask();
+        const bool full = __all_sync(conv, fa == 1 && fb == NF);
+        const bool far = __all_sync(conv, fminf((xnear * cf.ih) * 800.0f, 9019.0f) >= 9018.5f);
+        const float xmax = fmaxf(fabsf(x0), fabsf(xe)) * cf.ih;
+        if (__all_sync(conv, xmax <= 4611686018427387904.0f))
+          deposit_adj_mk<NF, true>(chl, gch, s_tab, s_dW, cf, cd, x0, kfa, fa, fb, full, far, Gl, Hl);
+        else
+          deposit_adj_mk<NF, false>(chl, gch, s_tab, s_dW, cf, cd, x0, kfa, fa, fb, full, far, Gl, Hl);
         // K is proportional to S = Rij D: dK/dD = K/D + dK/dih dih/dD
         gB += Gl;
         gE -= L.lower_ev[l] * Gl;

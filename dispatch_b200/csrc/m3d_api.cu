@@ -1480,6 +1480,7 @@ int m3d_lte_synthesis(const m3d_atmos_t *atm, int nf, const double *nu, const do
 #include "m3d_hprof_api.inc"
 #include "m3d_io_api.inc"
 #include "m3d_adjoint_api.inc"
+#include "m3d_hop_api.inc"
 
 // ===========================================================================
 // rotate_array without any allocation.

@@ -437,6 +437,26 @@ def lte_synthesis_adjoint(atm: dict, nu, llam, vec, wmu, g_flux, device=False, g
     return grads
 
 
+def hop_set_state(atm: dict):
+    """m3d_hop_set_state: load a state (host arrays) for hop_opacity."""
+    init()
+    keep = []
+    a = _atmos(atm, keep)
+    check(lib().m3d_hop_set_state(C.byref(a)), "m3d_hop_set_state")
+    del keep
+
+
+def hop_opacity(lam, chi, scat, include_absmet=0, include_llist=1, line_margin=10.0, line_scat=-1):
+    """m3d_hop_opacity with libhop's hop_opacity arguments: adds the loaded state's
+    line list to chi (nlam, n) float32 in place (wavelength fastest per cell)."""
+    init()
+    lam = np.ascontiguousarray(lam, np.float64)
+    assert chi.dtype == np.float32 and chi.flags.c_contiguous and scat.dtype == np.float32
+    check(lib().m3d_hop_opacity(C.c_int(lam.size), ptr(lam), ptr(chi), ptr(scat), C.c_int(include_absmet),
+                                C.c_int(include_llist), C.c_double(line_margin), C.c_int(line_scat)),
+          "m3d_hop_opacity")
+
+
 def eta_spread(vecs, ds, dz_upstream=None, one_dimensional=False) -> tuple[int, int]:
     """eta_rx, eta_ry of update_eta_mask (rt_patch_mod.f90:3683-3700): the horizontal
     reach of an upwind point over the slab's directions, plus the cell beyond it."""

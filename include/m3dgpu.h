@@ -422,6 +422,26 @@ int m3d_lte_synthesis(const m3d_atmos_t *atm, int nf, const double *nu, const do
                       int nray, const double *vec, const double *wmu, void *i_top, float *ie,
                       float *flux, unsigned flags);
 
+/* ---- libhop's opacity call ----
+ * m3d_hop_set_state loads a state for m3d_hop_opacity (host copies; the calling
+ * thread's; velocities, slabs and geometry are ignored): the cells' e_kT, ne, tothi,
+ * stark_pe and every species' line list with its inv_df, vbar2 and lnbase, the
+ * roles hop_load_state and hop_init_linelist play for libhop.
+ * m3d_hop_opacity has hop_opacity's argument list (HOP/standalone/libhop.h:20,
+ * hop_c_api.f90:910-942) with host buffers, so that libhop's hop_opacity can forward
+ * its line-list part unchanged: lam vacuum AA ascending and uniform in ln(lambda)
+ * (constant R); chi (nlam, n) holds the caller's continuum + absmet on entry, which
+ * is the tolerance reference, and gets the line list added as add_linelist_opacities
+ * adds it (composition_mod.f90:1663-1954: a line accumulator from zero, every
+ * species in turn, the lines within line_margin [AA] of the grid); scat is left
+ * alone.  include_absmet must be 0 (the continuum is the caller's), line_scat must be
+ * <= 0 (the scattering split needs HOP's epsilon per stage), include_llist = 0 does
+ * nothing. */
+int m3d_hop_set_state(const m3d_atmos_t *atm);
+int m3d_hop_free_state(void);
+int m3d_hop_opacity(int nlam, const double *lam, float *chi, float *scat, int include_absmet, int include_llist,
+                    double line_margin, int line_scat);
+
 /* Gradients of the LTE pass, accumulated (+=) by m3d_lte_synthesis_adjoint.  Cell
  * arrays (ncell, x fastest); per-species arrays species-major; gpref the species'
  * line lists one after the other.  Pointers follow M3D_DEVICE_PTRS. */
