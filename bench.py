@@ -49,7 +49,7 @@ def _args():
     p.add_argument("--no-c4", action="store_true", help="skip the differentiable (adjoint) measurement")
     p.add_argument("--cube", type=int, default=240, help="cube edge (240 = the configuration; smaller for profiling)")
     # single cases for timing and profiling one kernel family (no JSON line)
-    p.add_argument("--case", default="c1", choices=["c1", "ali-window", "ali-columns", "optab"],
+    p.add_argument("--case", default="c1", choices=["c1", "ali-window", "ali-columns", "optab", "c2"],
                    help="c1: the headline (default); the others run one seeded NLTE or table case and print "
                         "per-iteration times")
     p.add_argument("--n", type=int, default=64, help="ali-window / optab: cube edge")
@@ -784,6 +784,58 @@ def run_b200(a):
     print(json.dumps(line), flush=True)
 
 
+def _c2_full(iters=30):
+    """The 3D NLTE configuration in full: the 120^3 cube, the 20-level atom with its 80
+    transitions in 8 windows of 250 frequencies (2000 in all), 26 directions (Lobatto
+    4x4 and its mirror), short_char with split rates, lineq_no_pivot, Ng on its
+    automatic gate; up to 30 ALI iterations to convlim 1e-3.  Returns the convergence
+    history (maxerr and Ng per iteration) and the sweep and update times (CUDA events
+    on torch's stream)."""
+    import torch
+
+    from dispatch_b200 import ali, synth
+    cube, atom, _, vec, wts = ali.cube_problem("c2")
+    nrad = len(atom["ti"])
+    wins = [synth.atom_window(atom, seed=2, transitions=list(range(k, nrad, 8))) for k in range(8)]
+    A = ali.AliCube(cube, atom, wins, vec, wts, params=ali.AliParams(convlim=1e-3))
+    cur = torch.cuda.current_stream()
+    hist, sw, up = [], [], []
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(cur)
+    A.sweep()
+    e1.record(cur)
+    torch.cuda.synchronize()
+    sw.append(e0.elapsed_time(e1))
+    while A.iter < iters and not A.converged:
+        A.iter += 1
+        e0.record(cur)
+        rec = A.update()
+        e1.record(cur)
+        torch.cuda.synchronize()
+        up.append(e0.elapsed_time(e1))
+        ng = rec.get("ng") or {}
+        hist.append({"iter": rec["iter"], "maxerr": rec["maxerr"], "ng_applied": bool(ng.get("applied", False))})
+        if not A.converged and A.iter < iters:
+            e0.record(cur)
+            A.sweep()
+            e1.record(cur)
+            torch.cuda.synchronize()
+            sw.append(e0.elapsed_time(e1))
+    pts = A.points()
+    out = {"workload": "c2 3D NLTE: 120^3 cube, 20-level atom, 80 transitions in 8 windows (2000 frequencies), "
+                       "26 directions, short_char with split rates, lineq_no_pivot, Ng automatic, convlim 1e-3, "
+                       f"at most {iters} iterations", "unit": UNIT,
+           "iterations": A.iter, "converged": bool(A.converged), "history": hist,
+           "sweep_ms_median": float(np.median(sw)), "update_ms_median": float(np.median(up)) if up else None,
+           "total_s": (sum(sw) + sum(up)) / 1e3, "ray_pt_nu_per_sweep": pts,
+           "value": pts / (float(np.median(sw)) / 1e3) / 1e9,
+           "data": "synthetic (seeded grey cube, seeded model atom)"}
+    del A
+    torch.cuda.empty_cache()
+    return out
+
+
 def run_case_ali(a):
     """ALI iterations of a seeded problem, one line per iteration (the sweep and
     update times from CUDA events on torch's stream)."""
@@ -861,7 +913,11 @@ def run_case_optab(a):
 
 def main():
     a = _args()
-    if a.case in ("ali-window", "ali-columns"):
+    if a.case == "c2":
+        import dispatch_b200 as m
+        m.init(0)
+        print(json.dumps(_c2_full(a.iters if a.iters != 2 else 30)), flush=True)
+    elif a.case in ("ali-window", "ali-columns"):
         run_case_ali(a)
     elif a.case == "optab":
         run_case_optab(a)

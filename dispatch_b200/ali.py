@@ -205,34 +205,66 @@ class AliWindow(_AtomIteration):
         f32 = lambda a: torch.as_tensor(np.ascontiguousarray(a, np.float32), device=dev)
         f64 = lambda a: torch.as_tensor(np.ascontiguousarray(a, np.float64), device=dev)
 
-        self._init_atom(atom, [win], cube["temp"], cube["ne"], cube["nH"], abundance, awgt, vmic_kms, dev)
-        self.adamp = self.adamps[0]
+        wins = self._windows(win)
+        self._init_atom(atom, wins, cube["temp"], cube["ne"], cube["nH"], abundance, awgt, vmic_kms, dev)
         nc = self.ncell
-        temp = self.temp32
         vz = np.ascontiguousarray(cube["vz"], np.float32).ravel()
         self.vproj = [f32(vz * np.float32(v[2])) for v in vec]
-        self.beta, self.Bnu = rt.lte_background(f64(win["nu"]), f32(temp))
-        self.chi_c = f32(np.asarray(cube["chi_c"], np.float32).ravel())[:, None].expand(nc, self.nf).contiguous()
+        self.chi_c1 = f32(np.asarray(cube["chi_c"], np.float32).ravel())
+        # one flat storage per work array, sized for the widest window; each window
+        # takes views of its own shape from the front of them
+        nfmax = max(int(w["nf"]) for w in wins)
+        nwmax = max(max(int(w["nline"]) + int(w["ncont"]), 1) for w in wins)
+        self._pt = nc * nfmax
 
-        nw = int(win["nline"]) + int(win["ncont"])
-        self.gw_ij = torch.zeros((max(nw, 1), nc), dtype=torch.float32, device=dev)
-        self.gw_ji = torch.zeros_like(self.gw_ij)
+        def flat(n, dt=torch.float32):
+            return torch.zeros(n, dtype=dt, device=dev)
 
-        shp = (nc, self.nf)
-        self.work = torch.zeros((3, self.nz + 2, self.ny, self.nx, self.nf), dtype=torch.float32, device=dev)
+        self._st = {k: flat(self._pt) for k in ("psi", "irem", "escape", "xhat", "ehat", "dj", "opac_L", "opac_R",
+                                                 "chi_L", "chi_R", "beta", "Bnu", "chi_c")}
+        self._st.update({k: flat(self._pt, torch.int32) for k in ("id", "chi_id")})
+        self._st["J"], self._st["PsiJ"] = flat(2 * self._pt), flat(2 * self._pt)
+        self._st["work"] = flat(3 * (self.nz + 2) * self.ny * self.nx * nfmax)
+        self._st["gw_ij"], self._st["gw_ji"] = flat(nwmax * nc), flat(nwmax * nc)
+        self._bind(0)
+
+    def _windows(self, win):
+        self.wins = [win]
+        return self.wins
+
+    def _bind(self, k: int) -> None:
+        """The views and tables of window k."""
+        from . import make_slab
+        win = self.wins[k]
+        self.win = win
+        self.adamp = self.adamps[k]
+        nc, nf = self.ncell, int(win["nf"])
+        self.nf = nf
+        shp = (nc, nf)
+        st = self._st
+        v = lambda key: st[key][:nc * nf].view(shp)
+        self.psi, self.irem, self.escape = v("psi"), v("irem"), v("escape")
+        self.xhat, self.ehat, self.dj = v("xhat"), v("ehat"), v("dj")
+        self.split = {"opac_L": v("opac_L"), "opac_R": v("opac_R"), "id": v("id"), "chi_L": v("chi_L"),
+                      "chi_R": v("chi_R"), "chi_id": v("chi_id")}
+        self.J = st["J"][:2 * nc * nf].view((2,) + shp)
+        self.PsiJ = st["PsiJ"][:2 * nc * nf].view((2,) + shp)
+        self.work = st["work"][:3 * (self.nz + 2) * self.ny * self.nx * nf].view(3, self.nz + 2, self.ny, self.nx, nf)
         self.w1 = self.work[0, 1:self.nz + 1].view(shp)
         self.w2 = self.work[1, 1:self.nz + 1].view(shp)
         self.inu = self.work[2, 1:self.nz + 1].view(shp)
-        z = lambda dt=torch.float32: torch.zeros(shp, dtype=dt, device=dev)
-        self.psi, self.irem, self.escape = z(), z(), z()
-        self.xhat, self.ehat, self.dj = z(), z(), z()
-        self.split = {"opac_L": z(), "opac_R": z(), "id": z(torch.int32), "chi_L": z(), "chi_R": z(),
-                      "chi_id": z(torch.int32)}
-        self.J = torch.zeros((2,) + shp, dtype=torch.float32, device=dev)
-        self.PsiJ = torch.zeros_like(self.J)
-        self.slabs = [make_slab(self.nf, self.nx, self.ny, self.nz, 1 if v[2] > 0 else -1, self.ds, v, get_psi=True,
+        nw = max(int(win["nline"]) + int(win["ncont"]), 1)
+        self.gw_ij = st["gw_ij"][:nw * nc].view(nw, nc)
+        self.gw_ji = st["gw_ji"][:nw * nc].view(nw, nc)
+        import torch
+        nu = torch.as_tensor(np.ascontiguousarray(win["nu"], np.float64), device=self.dev)
+        self.beta, self.Bnu = rt.lte_background(nu, torch.as_tensor(self.temp32, device=self.dev),
+                                                out=(v("beta"), v("Bnu")))
+        self.chi_c = v("chi_c")
+        self.chi_c.copy_(self.chi_c1[:, None].expand(shp))
+        self.slabs = [make_slab(nf, self.nx, self.ny, self.nz, 1 if vv[2] > 0 else -1, self.ds, vv, get_psi=True,
                                 split_rates=self.p.split_rates, maser_dtau_max=self.p.maser_dtau_max,
-                                maser_Inu_max=self.p.maser_Inu_max) for v in vec]
+                                maser_Inu_max=self.p.maser_Inu_max) for vv in self.vec]
 
     # ---- rt_patch_t%execute, ALI branch -------------------------------------------------
     def sweep(self) -> None:
@@ -284,7 +316,31 @@ class AliWindow(_AtomIteration):
 
     def points(self) -> int:
         """Ray-point-frequency visits of one sweep (both twins)."""
-        return len(self.slabs) * self.ncell * self.nf
+        return len(self.slabs) * self.ncell * sum(int(w["nf"]) for w in self.wins)
+
+
+class AliCube(AliWindow):
+    """Every frequency window of a model atom on a periodic cube: the reference's
+    n_windows split (ray_patch_mod.f90:97-127), the rates of all windows summed into
+    the atom's gamma_ij/ji before each update, so one sweep is a whole ALI iteration's
+    formal solutions.  The windows share one set of work arrays, sized for the widest
+    (as one rt_patch_t works its windows in turn).  wins: synth.atom_window of each
+    window; the rest as AliWindow."""
+
+    def __init__(self, cube: dict, atom: dict, wins: list, vec, wts, params: AliParams | None = None,
+                 abundance: float = 7.5, awgt: float = 56.0, vmic_kms: float = 1.0, device: str = "cuda"):
+        self._all = list(wins)
+        super().__init__(cube, atom, wins[0], vec, wts, params=params, abundance=abundance, awgt=awgt,
+                         vmic_kms=vmic_kms, device=device)
+
+    def _windows(self, win):
+        self.wins = self._all
+        return self.wins
+
+    def sweep(self) -> None:
+        for k in range(len(self.wins)):
+            self._bind(k)
+            AliWindow.sweep(self)
 
 
 class _ColProblem(C.Structure):
@@ -460,4 +516,4 @@ def cube_problem(kind: str = "small", seed: int = 2, nx: int = 8, ny: int = 8, n
     return cube, atom, win, vec, wts
 
 
-__all__ = ["AliParams", "AliWindow", "AliColumns", "cube_problem", "column_problem"]
+__all__ = ["AliParams", "AliWindow", "AliCube", "AliColumns", "cube_problem", "column_problem"]

@@ -151,14 +151,18 @@ def chi_scat_units(chi_scat, beta):
           "m3d_chi_scat_units")
 
 
-def lte_background(nu, temp):
-    """beta, Bnu (ncell, nf); device tensors in, device tensors out (nu float64)."""
+def lte_background(nu, temp, out=None):
+    """beta, Bnu (ncell, nf); device tensors in, device tensors out (nu float64).
+    out: (beta, Bnu) device tensors to write into."""
     init()
     if _is_dev(temp):
         import torch
         nu = torch.as_tensor(nu, dtype=torch.float64, device=temp.device).contiguous()
-        beta = torch.empty((temp.numel(), nu.numel()), dtype=torch.float32, device=temp.device)
-        Bnu = torch.empty_like(beta)
+        if out is not None:
+            beta, Bnu = out
+        else:
+            beta = torch.empty((temp.numel(), nu.numel()), dtype=torch.float32, device=temp.device)
+            Bnu = torch.empty_like(beta)
         check(lib().m3d_lte_background(C.c_int(nu.numel()), C.c_int(temp.numel()), ptr(nu), ptr(temp), ptr(beta),
                                        ptr(Bnu), C.c_uint(DEVICE_PTRS)), "m3d_lte_background")
         return beta, Bnu

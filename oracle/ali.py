@@ -202,6 +202,48 @@ def run(cube: dict, atom: dict, win: dict, vec, wts, maxiter: int, convlim: floa
     return hist, S
 
 
+# ---- every window of the atom: the n_windows split of one patch -------------------------
+def setup_windows(cube: dict, atom: dict, wins: list, vec, wts, **kw) -> list:
+    """One state per window (ray_patch_mod.f90:97-127), sharing the atom's arrays: the
+    populations, the rates (every window's summed into the same gamma_ij/ji), the
+    profile integrals and the iteration bookkeeping of the first."""
+    Ss = [setup(cube, atom, w, vec, wts, **kw) for w in wins]
+    sums = np.zeros(int(atom["nline"]), np.uint8)
+    for w in wins:
+        sums[np.asarray(w["line_ntrans"], np.int64)] = np.asarray(w["sums_over_windows"], np.uint8)
+    S0 = Ss[0]
+    S0["has_wphi"] = sums
+    for S in Ss[1:]:
+        for k in ("b", "oldb", "gamma_ij", "gamma_ji", "wphi", "has_wphi", "nstar", "totn"):
+            S[k] = S0[k]
+    return Ss
+
+
+def run_windows(cube: dict, atom: dict, wins: list, vec, wts, maxiter: int, convlim: float = 1e-3,
+                ng_step: int = 0, **kw):
+    """Iteration 0 and up to maxiter updates over every window; returns (history, state
+    of the first window, which holds the shared arrays)."""
+    from dispatch_b200.stateq import NgState
+
+    Ss = setup_windows(cube, atom, wins, vec, wts, **kw)
+    S0 = Ss[0]
+    ng_state = NgState()
+    hist = []
+
+    def sweep_all():
+        for S in Ss:
+            S["iter"] = S0["iter"]
+            _sweep_twins(S)
+
+    sweep_all()
+    while S0["iter"] < maxiter and not S0["converged"]:
+        S0["iter"] += 1
+        hist.append(_update(S0, ng_state, convlim, ng_step))
+        if not S0["converged"] and S0["iter"] < maxiter:
+            sweep_all()
+    return hist, S0
+
+
 # ---- the batched 1.5D iteration: columns of uneven depth ---------------------------------
 def _solve_columns(S: dict, Wd: dict, mu: float) -> None:
     """long_char_linear along every column with its upstream ghost (set_upstream_boundary:

@@ -74,3 +74,43 @@ def test_ali_converges_and_conserves(m3d):
     n = (A.b * A.nstar).sum(dim=0)
     np.testing.assert_allclose(n.cpu().numpy(), A.totn.cpu().numpy(), rtol=1e-10)
     assert all(np.isfinite(h["maxerr"]) for h in hist)
+
+
+def test_ali_all_windows_match_oracle(m3d, oracle):
+    """AliCube: every window of the atom (three windows holding every third
+    transition) swept in turn with shared work arrays, the rates of all summed before
+    each update; six iterations against the oracle's composition over the same
+    windows, b within 1e-7."""
+    from dispatch_b200 import ali, synth
+    from oracle import ali as oali
+    cube, atom, _, vec, wts = ali.cube_problem(nx=6, ny=6, nz=10, nbound=5, nline=6, ntheta=2, nphi=4)
+    nrad = len(atom["ti"])
+    wins = [synth.atom_window(atom, seed=2, transitions=list(range(k, nrad, 3))) for k in range(3)]
+    assert len({int(w["nf"]) for w in wins}) > 1          # windows of different widths share the arrays
+    hist_o, S = oali.run_windows(cube, atom, wins, vec, wts, maxiter=6, convlim=1e-6)
+    A = ali.AliCube(cube, atom, wins, vec, wts, params=ali.AliParams(convlim=1e-6))
+    hist_g = A.run(6)
+    assert len(hist_g) == len(hist_o) == 6
+    for g, o in zip(hist_g, hist_o):
+        assert g["maxerr"] == pytest.approx(o["maxerr"], rel=1e-7)
+    np.testing.assert_allclose(A.b.cpu().numpy(), S["b"], rtol=1e-7)
+    assert np.abs(S["b"] - 1.0).max() > 0.05
+    assert A.points() == len(A.slabs) * A.ncell * sum(int(w["nf"]) for w in wins)
+
+
+def test_ali_c2_atom_all_windows(m3d, oracle):
+    """The 3D NLTE configuration's 20-level atom (80 transitions in 8 windows of 250
+    frequencies, 26 directions) on a 6 x 6 x 10 cube: three ALI iterations of every
+    window against the oracle's composition, b within 1e-4 (the configuration's
+    requirement on departure coefficients)."""
+    from dispatch_b200 import ali, synth
+    from oracle import ali as oali
+    cube, atom, _, vec, wts = ali.cube_problem(nx=6, ny=6, nz=10, nbound=20, nline=60, ntheta=4, nphi=4)
+    nrad = len(atom["ti"])
+    wins = [synth.atom_window(atom, seed=2, transitions=list(range(k, nrad, 8))) for k in range(8)]
+    hist_o, S = oali.run_windows(cube, atom, wins, vec, wts, maxiter=3, convlim=1e-3)
+    A = ali.AliCube(cube, atom, wins, vec, wts)
+    hist_g = A.run(3)
+    for g, o in zip(hist_g, hist_o):
+        assert g["maxerr"] == pytest.approx(o["maxerr"], rel=1e-4)
+    np.testing.assert_allclose(A.b.cpu().numpy(), S["b"], rtol=1e-4)
