@@ -807,10 +807,17 @@ def _c2_full(iters=30):
     e1.record(cur)
     torch.cuda.synchronize()
     sw.append(e0.elapsed_time(e1))
+    from dispatch_b200.stateq import NonFiniteSolution
+    failure = None
     while A.iter < iters and not A.converged:
         A.iter += 1
         e0.record(cur)
-        rec = A.update()
+        try:
+            rec = A.update()
+        except NonFiniteSolution as e:
+            # update_populations stops the run here, as the reference's error stop does
+            failure = {"iter": A.iter, "error": str(e).splitlines()[0]}
+            break
         e1.record(cur)
         torch.cuda.synchronize()
         up.append(e0.elapsed_time(e1))
@@ -826,7 +833,7 @@ def _c2_full(iters=30):
     out = {"workload": "c2 3D NLTE: 120^3 cube, 20-level atom, 80 transitions in 8 windows (2000 frequencies), "
                        "26 directions, short_char with split rates, lineq_no_pivot, Ng automatic, convlim 1e-3, "
                        f"at most {iters} iterations", "unit": UNIT,
-           "iterations": A.iter, "converged": bool(A.converged), "history": hist,
+           "iterations": A.iter, "converged": bool(A.converged), "history": hist, "stopped": failure,
            "sweep_ms_median": float(np.median(sw)), "update_ms_median": float(np.median(up)) if up else None,
            "total_s": (sum(sw) + sum(up)) / 1e3, "ray_pt_nu_per_sweep": pts,
            "value": pts / (float(np.median(sw)) / 1e3) / 1e9,

@@ -651,7 +651,7 @@ def _set_weights(x):
 
 
 def atom_window(atom: dict, nper: int = 25, seed: int = 2, qmax_doppler: float = 5.0, idf_ref: float = 1.8e5,
-                adamp=(1e-3, 1e-1), sums=None, transitions=None) -> dict:
+                adamp=(1e-3, 1e-1), sums=None, transitions=None, lam_range=None) -> dict:
     """The atom's transitions on one frequency window holding every transition:
     nper points per line on q = 1 - lam/lam0 in +-qmax_doppler/idf_ref, nper
     points per continuum from 0.3 of its edge wavelength to the edge, merged
@@ -665,7 +665,10 @@ def atom_window(atom: dict, nper: int = 25, seed: int = 2, qmax_doppler: float =
     sums: per line sums_over_windows (default none).  transitions: the atom's
     transition indices the window holds (default all), the reference's split of
     the spectrum into frequency windows; a transition keeps its damping in every
-    window."""
+    window.  lam_range: (lo, hi) [AA], a window by wavelength instead -- the grid's
+    points in [lo, hi), every transition with points there, a transition that
+    straddles the bounds keeping only its part (the reference's contiguous
+    n_windows chunks, where a continuum can span several windows)."""
     rng = np.random.default_rng(seed + 5000)
     nline = atom["nline"]
     ti, tj, ev, g = atom["ti"], atom["tj"], atom["ev"], atom["g"]
@@ -680,6 +683,10 @@ def atom_window(atom: dict, nper: int = 25, seed: int = 2, qmax_doppler: float =
         else:
             lam_pts.append(np.geomspace(0.3 * lam0[k], lam0[k] * (1.0 - 1e-7), nper))
     grid = np.unique(np.concatenate([lam_pts[k] for k in ks]))
+    if lam_range is not None:
+        grid = grid[(grid >= lam_range[0]) & (grid < lam_range[1])]
+        ks = [k for k in ks if np.any((lam_pts[k] >= lam_range[0]) & (lam_pts[k] < lam_range[1]))]
+        lam_pts = [p[(p >= lam_range[0]) & (p < lam_range[1])] for p in lam_pts]
     nu = HZ_TO_AA / grid
     nf = grid.size
     li, lj, lb, lr, lo, q, wnu, wq = [], [], [], [], [], [], [], []
