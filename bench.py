@@ -60,6 +60,8 @@ def _args():
     p.add_argument("--nwin", type=int, default=8, help="ali-columns: frequency windows")
     p.add_argument("--iters", type=int, default=2, help="ali-* / optab: iterations")
     p.add_argument("--no-graph", action="store_true", help="ali-columns: direct launches instead of the graph")
+    p.add_argument("--per-point", action="store_true",
+                   help="ali-columns: the per-point kernels instead of the fused column sweep")
     p.add_argument("--only", choices=["sample", "ll"], default=None, help="optab: one sampler")
     return p.parse_args()
 
@@ -363,17 +365,41 @@ def _nlte_batched(steps=2):
         sw.append(e1.elapsed_time(e2))
     pts = sum(A.points() for A in plans)
     sweep_ms, update_ms = float(np.median(sw)), float(np.median(up))
+    shapes = [A.shape for A in plans]
+    launches = (m.launch_count() - n0) // steps
+    for A in plans:
+        A.close()
+    # the same sweeps by the per-point kernels (opacity, column solver, rate sums as
+    # separate launches through HBM), for comparison: one warm-up and one timed sweep
+    pp = []
+    for nb, nl in ((20, 60), (60, 180)):
+        atom = synth.model_atom(3, nbound=nb, nline=nl)
+        nrad = len(atom["ti"])
+        nwin = max(1, nrad // 10)
+        wins = [synth.atom_window(atom, seed=3, transitions=list(range(k, nrad, nwin))) for k in range(nwin)]
+        A = ali.AliColumns(cols, atom, wins, vec[:, 2].copy(), wts, params=ali.AliParams(convlim=1e-9), fused=False)
+        A.sweep()
+        e0, e1 = (torch.cuda.Event(enable_timing=True) for _ in range(2))
+        torch.cuda.synchronize()
+        e0.record(cur)
+        A.sweep()
+        e1.record(cur)
+        torch.cuda.synchronize()
+        pp.append(e0.elapsed_time(e1))
+        A.close()
+        del A
+        torch.cuda.empty_cache()
     out = {"workload": "batched 1.5D NLTE: 4096 columns of 60-256 cells (seeded 64x64x256 cube), 3 abundance "
                        "variants (1.94 M cells), 21-level atom (2000 frequencies, 8 windows) and 61-level atom "
                        "(6000 frequencies, 24 windows), Radau 2 + mirror (4 directions), long_char_linear along "
                        "each column with split rates; each atom's sweep one CUDA graph replay",
            "unit": UNIT, "value": pts / (sweep_ms / 1e3) / 1e9, "sweep_ms": sweep_ms, "update_ms": update_ms,
            "iteration_ms": sweep_ms + update_ms, "ray_pt_nu_per_iteration": pts,
-           "graph_launches_per_iteration": (m.launch_count() - n0) // steps,
-           "solver_block_autotuned": [A.solver_block for A in plans], "cells": plans[0].ncell,
+           "graph_launches_per_iteration": launches,
+           "plan_shapes_autotuned": shapes, "cells": plans[0].ncell,
+           "per_point_sweep_ms": float(sum(pp)),
+           "per_point_value": pts / (sum(pp) / 1e3) / 1e9,
            "data": "synthetic (seeded grey cube, seeded model atoms)"}
-    for A in plans:
-        A.close()
     del plans
     torch.cuda.empty_cache()
     return out
@@ -861,7 +887,9 @@ def run_case_ali(a):
     else:
         cols, atom, wins, mu, wmu = ali.column_problem(ncol=a.ncol, depth=(60, 256), nz=256, nxy=64,
                                                        nbound=a.nbound, nline=a.nline, nwin=a.nwin)
-        A = ali.AliColumns(cols, atom, wins, mu, wmu, params=ali.AliParams(convlim=1e-9), use_graph=not a.no_graph)
+        A = ali.AliColumns(cols, atom, wins, mu, wmu, params=ali.AliParams(convlim=1e-9), use_graph=not a.no_graph,
+                           fused=not a.per_point)
+        print(f"plan shape {A.shape}", flush=True)
     torch.cuda.synchronize()
     print(f"setup {time.time() - t0:.1f} s, {A.ncell} cells, {A.points():.3e} ray-point-frequencies per sweep",
           flush=True)

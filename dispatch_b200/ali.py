@@ -28,7 +28,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from . import (AUTOTUNE, BND_PCHIP, BND_ZERO, SHORT_LINEAR, M3DError, check, init, lib, make_slab, nlte,
+from . import (AUTOTUNE, BND_PCHIP, BND_ZERO, COL_PERPOINT, SHORT_LINEAR, M3DError, check, init, lib, make_slab, nlte,
                order_after_torch, ptr, rt, stateq, synth)
 
 
@@ -165,6 +165,7 @@ class _AtomIteration:
                 self.sweep()
                 self._exchange()
         return self.history
+
 
 class AliWindow(_AtomIteration):
     """One frequency window of a model atom on a periodic cube, device resident.
@@ -372,7 +373,7 @@ class AliColumns(_AtomIteration):
 
     def __init__(self, cols: dict, atom: dict, wins: list, mu, wmu, params: AliParams | None = None,
                  abundance: float = 7.5, awgt: float = 56.0, vmic_kms: float = 1.0, use_graph: bool = True,
-                 autotune: bool = True, device: str = "cuda", group=None, windows=None):
+                 autotune: bool = True, device: str = "cuda", group=None, windows=None, fused: bool = True):
         import torch
 
         init()
@@ -429,11 +430,17 @@ class AliColumns(_AtomIteration):
         order_after_torch(self.b)
         self._plan = C.c_void_p()
         check(lib().m3d_col_plan_create(C.byref(prob), C.c_int(nw), ws, pv(nus), pv(twos), ad,
-                                        C.c_uint(AUTOTUNE if autotune else 0), C.byref(self._plan)),
+                                        C.c_uint((AUTOTUNE if autotune else 0) | (0 if fused else COL_PERPOINT)),
+                                        C.byref(self._plan)),
               "m3d_col_plan_create")
         nfo, blk = C.c_int(), C.c_int()
         check(lib().m3d_col_plan_fields(self._plan, None, None, C.byref(nfo), C.byref(blk)), "m3d_col_plan_fields")
         self.solver_block = blk.value
+        sh = [C.c_int() for _ in range(4)]
+        check(lib().m3d_col_plan_shape(self._plan, *[C.byref(v) for v in sh]), "m3d_col_plan_shape")
+        # the windows the fused kernel sweeps, its threads per column and cells per
+        # chunk, the per-point column solver's block size
+        self.shape = dict(zip(("fused_windows", "fused_block", "zchunk", "solver_block"), [v.value for v in sh]))
 
     def sweep(self) -> None:
         """The formal solutions and rate sums of every window and direction."""
@@ -491,13 +498,20 @@ def column_problem(kind: str = "small", seed: int = 3, ncol: int = 6, depth=(8, 
     return cols, atom, wins, vec[:, 2].copy(), wts
 
 
+# The 3D NLTE configuration's atom draws its lines between levels at least this far
+# apart [eV]: with the level energies drawn uniformly, pairs a few meV apart give
+# mm-wave lines whose masers drive the iteration to the update limiter.
+C2_MIN_LINE_EV = 0.5
+
+
 def cube_problem(kind: str = "small", seed: int = 2, nx: int = 8, ny: int = 8, nz: int = 12, nbound: int = 6,
                  nline: int = 8, nper: int = 25, transitions=None, ntheta: int = 2, nphi: int = 4,
-                 sums=None) -> tuple[dict, dict, dict, np.ndarray, np.ndarray]:
+                 sums=None, min_line_ev: float | None = None) -> tuple[dict, dict, dict, np.ndarray, np.ndarray]:
     """(cube, atom, win, vec, wts) of a seeded NLTE window: the grey cube with its
     temperature and velocity fields, a model atom with nbound bound levels and
     nline lines, its transitions on one window, and Lobatto directions with
-    mean-intensity weights.  kind 'c2': the 120^3 cube and the 20-level atom.
+    mean-intensity weights.  kind 'c2': the 120^3 cube and the 20-level atom, its
+    lines between levels at least 0.5 eV apart (min_line_ev; default 0 otherwise).
     The horizontal cell size is the vertical one times the largest |tan theta| of
     the directions (rounded up to a half), so that every upwind point of the
     short characteristics lies within one cell (the stencil of set_stencil)."""
@@ -505,13 +519,15 @@ def cube_problem(kind: str = "small", seed: int = 2, nx: int = 8, ny: int = 8, n
         nx = ny = nz = 120
         nbound, nline = 20, 60
         ntheta, nphi = 4, 4
+        if min_line_ev is None:
+            min_line_ev = C2_MIN_LINE_EV
     vec, wts = synth.lobatto_rays(ntheta, nphi, jnu_weights=True)
     tan_max = float(np.max(np.hypot(vec[:, 0], vec[:, 1]) / np.abs(vec[:, 2])))
     aspect = max(2.0, float(np.ceil(2.0 * tan_max * (1.0 + 1e-6)) / 2.0))
     c = synth.cube_atmosphere(seed, nx, ny, nz, aspect=aspect)
     cube = {"temp": c["temp"].ravel(), "ne": c["ne"].ravel(), "nH": c["nH"].ravel(), "chi_c": c["chi_c"].ravel(),
             "vz": c["vz"].ravel(), "shape": (nx, ny, nz), "ds": c["ds_cm"]}
-    atom = synth.model_atom(seed, nbound=nbound, nline=nline)
+    atom = synth.model_atom(seed, nbound=nbound, nline=nline, min_line_ev=min_line_ev or 0.0)
     win = synth.atom_window(atom, nper=nper, seed=seed, transitions=transitions, sums=sums)
     return cube, atom, win, vec, wts
 

@@ -24,6 +24,7 @@
 #include "m3d_nlte.cuh"
 #include "m3d_aux.cuh"
 #include "m3d_columns.cuh"
+#include "m3d_colfused.cuh"
 #include "m3d_optab.cuh"
 #include "m3d_hprof.cuh"
 #include "m3d_adjoint.cuh"

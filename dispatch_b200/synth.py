@@ -418,7 +418,8 @@ RYDV = 13.605
 
 
 def model_atom(seed: int = 2, nbound: int = 20, nline: int = 60, e_max: float = 7.0, e_ion: float = 7.9,
-               logf=(-4.0, 0.0), h_recipes=None, awgt: float = 40.08, gencol: bool = False) -> dict:
+               logf=(-4.0, 0.0), h_recipes=None, awgt: float = 40.08, gencol: bool = False,
+               min_line_ev: float = 0.0) -> dict:
     """A seeded model atom: nbound levels of the neutral (ground at 0 eV, the rest
     uniform in [0, e_max]) plus the ground level of the ion at e_ion; nline lines
     between distinct random bound pairs with log f uniform in logf; one continuum
@@ -431,13 +432,17 @@ def model_atom(seed: int = 2, nbound: int = 20, nline: int = 60, e_max: float = 
     of every pair (col_hkind): Takeda for a bound pair without a line, else
     Drawin.  awgt: the atom's weight [amu].  gencol adds tabulated collision
     records of every kind (model_gencol); classic_col then leaves out the recipes
-    the records' data replaces, as the reference does.  Indices are 0-based."""
+    the records' data replaces, as the reference does.  min_line_ev: lines only
+    between levels at least this far apart (0: any pair; the uniform level draw puts
+    some pairs a few meV apart, whose lines sit in the far infrared and mm, where
+    stimulated emission dominates and small population inversions make masers).
+    Indices are 0-based."""
     rng = np.random.default_rng(seed + 2000)
     ev = np.concatenate([[0.0], np.sort(rng.uniform(0.0, e_max, nbound - 1)), [e_ion]])
     g = np.concatenate([rng.choice([1.0, 3.0, 5.0, 7.0, 9.0], nbound), [1.0]])
     ion = np.concatenate([np.ones(nbound, np.int32), [2]]).astype(np.int32)
     n = nbound + 1
-    pairs = [(i, j) for i in range(nbound) for j in range(i + 1, nbound)]
+    pairs = [(i, j) for i in range(nbound) for j in range(i + 1, nbound) if ev[j] - ev[i] >= min_line_ev]
     pick = np.sort(rng.choice(len(pairs), size=min(nline, len(pairs)), replace=False))
     lines = [pairs[p] for p in pick]
     f = 10.0 ** rng.uniform(*logf, len(lines))
@@ -613,7 +618,8 @@ def lsaha(temp, ne):
 def se_config(kind: str = "small", seed: int | None = None, ncell: int | None = None, lte: bool = False,
               nbound: int = 20, nline: int = 60, h_recipes=None, gencol: bool = False) -> tuple:
     """(atom, inputs) of an SE case.  'c2': the 120^3 cube of seed 2 and the
-    20-level atom (a radiation field diluted upwards, W = exp(-3 z/nz));
+    20-level atom with lines between levels at least 0.5 eV apart (a radiation
+    field diluted upwards, W = exp(-3 z/nz));
     'small': ncell cells (default 2048) drawn from a 16^3 cube with W uniform
     in [0.05, 1]; lte: W = 1.  nbound/nline: the atom's bound levels and lines
     (60/180 for the larger atom of the batched configuration); h_recipes: the
@@ -629,7 +635,8 @@ def se_config(kind: str = "small", seed: int | None = None, ncell: int | None = 
         W = np.random.default_rng(seed + 4000).uniform(0.05, 1.0, 16**3)
     else:
         raise ValueError(kind)
-    atom = model_atom(seed, nbound=nbound, nline=nline, h_recipes=h_recipes, gencol=gencol)
+    atom = model_atom(seed, nbound=nbound, nline=nline, h_recipes=h_recipes, gencol=gencol,
+                      min_line_ev=0.5 if kind == "c2" else 0.0)
     temp, ne, nH = cube["temp"].ravel(), cube["ne"].ravel(), cube["nH"].ravel()
     W = np.asarray(W).ravel()
     if ncell is not None:

@@ -49,6 +49,7 @@ extern "C" {
 #define M3D_LINE_DIAG 0x10u   /* accumulate the line diagnostics used/strength/reach */
 #define M3D_ROTATE 0x20u      /* quadratic solver: apply rotate_array first (3D output pass) */
 #define M3D_AUTOTUNE 0x40u    /* m3d_col_plan_create: time the launch shapes and keep the fastest */
+#define M3D_COL_PERPOINT 0x80u /* m3d_col_plan_create: the per-point kernels instead of the fused column sweep */
 
 /* ---- formal solvers (rt_patch_mod.f90:1649-1721, rt_params_mod.f90 solver names) ---- */
 #define M3D_SOLVER_LINEAR 0        /* long_char_linear, rt_solvers_mod.f90:666 ('linear', 1D) */
@@ -786,8 +787,13 @@ typedef struct m3d_col_plan m3d_col_plan_t;
 /* A plan for one model atom over its frequency windows: the windows' tables are
  * staged once (win_nu float64, win_twohnu3_c2 float32 per window, host or device;
  * win_adamp the window lines' damping (nline, ncell), device), and the plan owns
- * work arrays sized for the widest window.  With M3D_AUTOTUNE the column solver's
- * block size is chosen by timing. */
+ * work arrays sized for the widest window.  A window whose every frequency lies in
+ * at most 4 line windows is swept by one fused kernel per hemisphere (line opacity,
+ * transfer units, the column solve, J/PsiJ and the line rates of a column in one
+ * CTA); the others, and every window with M3D_COL_PERPOINT, by the per-point
+ * kernels.  Both give the same bits.  With M3D_AUTOTUNE the launch shapes (the
+ * fused kernel's threads per column and cells per chunk, the column solver's block
+ * size) are chosen by timing. */
 int m3d_col_plan_create(const m3d_col_problem_t *p, int nwin, const m3d_atom_window_t *wins,
                         const double *const *win_nu, const float *const *win_twohnu3_c2,
                         const float *const *win_adamp, unsigned flags, m3d_col_plan_t **plan);
@@ -802,8 +808,13 @@ int m3d_col_plan_sweep(m3d_col_plan_t *plan, int first_iter, float *gamma_ij, fl
                        int use_graph);
 /* Copies the combined J and PsiJ of the last window (2 x (ncell, nf): both twins
  * hold the average) into J, PsiJ (host or device, may be NULL) and returns that
- * window's nf and the column solver's block size; synchronises. */
+ * window's nf and the block size of the sweep's solver (the fused kernel's when
+ * every window is fused); synchronises. */
 int m3d_col_plan_fields(m3d_col_plan_t *plan, float *J, float *PsiJ, int *nf, int *solver_block);
+/* The plan's launch shapes: how many windows the fused kernel sweeps, its threads
+ * per column and cells per chunk, the per-point column solver's block size (any
+ * pointer may be NULL). */
+int m3d_col_plan_shape(m3d_col_plan_t *plan, int *fused_windows, int *fused_block, int *zchunk, int *solver_block);
 int m3d_col_plan_destroy(m3d_col_plan_t *plan);
 
 /* Self-check with no counterpart in the reference.  The opacity kernels form 1/(1+u)

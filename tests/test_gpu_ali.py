@@ -105,7 +105,8 @@ def test_ali_c2_atom_all_windows(m3d, oracle):
     requirement on departure coefficients)."""
     from dispatch_b200 import ali, synth
     from oracle import ali as oali
-    cube, atom, _, vec, wts = ali.cube_problem(nx=6, ny=6, nz=10, nbound=20, nline=60, ntheta=4, nphi=4)
+    cube, atom, _, vec, wts = ali.cube_problem(nx=6, ny=6, nz=10, nbound=20, nline=60, ntheta=4, nphi=4,
+                                               min_line_ev=ali.C2_MIN_LINE_EV)
     nrad = len(atom["ti"])
     wins = [synth.atom_window(atom, seed=2, transitions=list(range(k, nrad, 8))) for k in range(8)]
     hist_o, S = oali.run_windows(cube, atom, wins, vec, wts, maxiter=3, convlim=1e-3)

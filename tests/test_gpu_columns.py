@@ -26,14 +26,18 @@ def _problem(sums=False, variants=(0.0, 0.2)):
     return cols, atom, wins, mu, wmu
 
 
+@pytest.mark.parametrize("fused", [True, False])
 @pytest.mark.parametrize("sums", [False, True])
-def test_column_sweep_bit_exact(m3d, oracle, sums):
+def test_column_sweep_bit_exact(m3d, oracle, sums, fused):
+    """The fused column sweep (one kernel per window and hemisphere) and the
+    per-point kernels both equal the oracle bit for bit."""
     from dispatch_b200 import ali
     from oracle import ali as oali
     cols, atom, wins, mu, wmu = _problem(sums)
     S = oali.setup_columns(cols, atom, wins, mu, wmu)
     oali.sweep_columns(S)
-    A = ali.AliColumns(cols, atom, wins, mu, wmu, use_graph=False)
+    A = ali.AliColumns(cols, atom, wins, mu, wmu, use_graph=False, fused=fused)
+    assert A.shape["fused_windows"] == (len(wins) if fused else 0)
     A.sweep()
     np.testing.assert_array_equal(A.gamma_ij.cpu().numpy(), S["gamma_ij"])
     np.testing.assert_array_equal(A.gamma_ji.cpu().numpy(), S["gamma_ji"])
@@ -45,6 +49,70 @@ def test_column_sweep_bit_exact(m3d, oracle, sums):
     if sums:
         assert S["wphi"].max() > 0
     A.close()
+
+
+def _overlap_problem():
+    """Columns with an atom whose line windows overlap: one window where up to 3
+    lines share a frequency (fused) and one where up to 9 do (more than the fused
+    kernel keeps in registers: the per-point kernels)."""
+    from dispatch_b200 import ali, synth
+    cols, _, _, mu, wmu = ali.column_problem(variants=(0.0, 0.2))
+    atom = synth.model_atom(3, nbound=8, nline=20)
+    nrad = len(atom["ti"])
+    wins = [synth.atom_window(atom, seed=3, qmax_doppler=5000.0, transitions=list(range(0, nrad, 2))),
+            synth.atom_window(atom, seed=3, qmax_doppler=60000.0, transitions=list(range(1, nrad, 2)))]
+    nper = []
+    for w in wins:
+        c = np.zeros(w["nf"], int)
+        for b, r in zip(w["line_blue"], w["line_red"]):
+            c[b:r + 1] += 1
+        nper.append(int(c.max()))
+    assert 1 < nper[0] <= 4 < nper[1]
+    return cols, atom, wins, mu, wmu
+
+
+def test_column_sweep_overlapping_lines_bit_exact(m3d, oracle):
+    """Several lines on one frequency: the split tracking across lines and the rate
+    rows of each line in the fused kernel, and a window past its limit swept by the
+    per-point kernels within the same plan, all equal to the oracle bit for bit."""
+    from dispatch_b200 import ali
+    from oracle import ali as oali
+    cols, atom, wins, mu, wmu = _overlap_problem()
+    S = oali.setup_columns(cols, atom, wins, mu, wmu)
+    oali.sweep_columns(S)
+    A = ali.AliColumns(cols, atom, wins, mu, wmu, use_graph=False)
+    assert A.shape["fused_windows"] == 1
+    A.sweep()
+    np.testing.assert_array_equal(A.gamma_ij.cpu().numpy(), S["gamma_ij"])
+    np.testing.assert_array_equal(A.gamma_ji.cpu().numpy(), S["gamma_ji"])
+    J, P = A.fields()
+    np.testing.assert_array_equal(J.cpu().numpy(), S["J"])
+    np.testing.assert_array_equal(P.cpu().numpy(), S["PsiJ"])
+    A.close()
+
+
+@pytest.mark.parametrize("precond", [True, False])
+@pytest.mark.parametrize("bottom", ["pchip", "zero"])
+def test_fused_equals_per_point(m3d, precond, bottom):
+    """The fused sweep and the per-point kernels give the same rates and fields bit
+    for bit with and without preconditioning and with either bottom ghost, over
+    two iterations (the update in between) and a third sweep, from the CUDA graph."""
+    from dispatch_b200 import BND_PCHIP, BND_ZERO, ali
+    cols, atom, wins, mu, wmu = _overlap_problem()
+    p = ali.AliParams(preconditioning=precond, bottom=BND_PCHIP if bottom == "pchip" else BND_ZERO, convlim=1e-9)
+    out = []
+    for fused in (True, False):
+        A = ali.AliColumns(cols, atom, wins, mu, wmu, params=p, fused=fused)
+        A.run(2)
+        A.sweep()
+        J, P = A.fields()
+        out.append((A.b.cpu().numpy(), A.gamma_ij.cpu().numpy(), A.gamma_ji.cpu().numpy(), J.cpu().numpy(),
+                    P.cpu().numpy(), [h["maxerr"] for h in A.history]))
+        A.close()
+    for a, b in zip(out[0][:5], out[1][:5]):
+        np.testing.assert_array_equal(a, b)
+    assert out[0][5] == out[1][5]
+    assert np.abs(out[0][1]).max() > 0 and np.abs(out[0][0] - 1.0).max() > 0.01
 
 
 def test_column_graph_replay_equals_launches(m3d):
@@ -76,6 +144,7 @@ def test_column_iterations_match_oracle(m3d, oracle):
     nc1 = int(cols["col_off"][len(cols["col_off"]) // 3])
     assert not np.allclose(S["b"][:, :nc1], S["b"][:, nc1:2 * nc1])
     assert A.solver_block in (64, 128, 256, 512)
+    assert A.shape["fused_windows"] == len(wins) and A.shape["zchunk"] in (4, 8, 16)
     A.close()
 
 
