@@ -49,7 +49,7 @@ def _args():
     p.add_argument("--no-c4", action="store_true", help="skip the differentiable (adjoint) measurement")
     p.add_argument("--cube", type=int, default=240, help="cube edge (240 = the configuration; smaller for profiling)")
     # single cases for timing and profiling one kernel family (no JSON line)
-    p.add_argument("--case", default="c1", choices=["c1", "ali-window", "ali-columns", "optab", "c2"],
+    p.add_argument("--case", default="c1", choices=["c1", "ali-window", "ali-columns", "optab", "c2", "batched"],
                    help="c1: the headline (default); the others run one seeded NLTE or table case and print "
                         "per-iteration times")
     p.add_argument("--n", type=int, default=64, help="ali-window / optab: cube edge")
@@ -952,6 +952,10 @@ def main():
         import dispatch_b200 as m
         m.init(0)
         print(json.dumps(_c2_full(a.iters if a.iters != 2 else 30)), flush=True)
+    elif a.case == "batched":
+        import dispatch_b200 as m
+        m.init(0)
+        print(json.dumps(_nlte_batched()), flush=True)
     elif a.case in ("ali-window", "ali-columns"):
         run_case_ali(a)
     elif a.case == "optab":

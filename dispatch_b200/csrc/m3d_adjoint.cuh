@@ -411,7 +411,7 @@ __device__ __forceinline__ float qlg_eval_d(const float2 *tab, const float *dW, 
   const float u = xs * xs;
   const float L = qlg_rcp<MK>(1.0f + u);
   const float y = fminf(xs * 800.0f, 9019.0f);
-  const int ig = y < 0.5f ? 0 : (int)(y + 0.5f);
+  const int ig = qlg_node(y);
   const float2 gw = tab[ig];
   const float G = gw.x, W = gw.y;
   float p = fmaf(c.cZH, W, c.cL2);

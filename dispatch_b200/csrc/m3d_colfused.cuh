@@ -13,10 +13,12 @@
 //
 // One CTA owns one column; its threads run along frequency and walk the column in
 // chunks of zchunk cells.  Per chunk the CTA stages every (cell, line) constant
-// once (the QLG-bot set-up of the line's damping, Rij b_j, Rij b_i and 1/n_ref);
-// per direction each point's rate terms go to a shared row per cell, and at the
-// chunk's end one thread per (line, cell) adds the line's terms in ascending f --
-// bound_bound_rates' order -- and updates the rates.
+// once (the QLG-bot set-up of the line's damping, Rij b_j, Rij b_i and 1/n_ref).
+// A point's inputs are read once for all the launch's directions, which then run in
+// turn, each with its own upstream state; each direction's rate terms go to its own
+// shared row per cell, and at the chunk's end one thread per (line, cell) adds the
+// line's terms in ascending f -- bound_bound_rates' order -- for each direction in
+// turn and updates the rates.
 #pragma once
 #include "m3d_columns.cuh"
 #include "m3d_nlte.cuh"
@@ -46,8 +48,8 @@ struct ColFusedArgs {
 
 // shared-memory bytes of one CTA
 __host__ __device__ inline size_t col_fused_smem(int nf, int nline, int nslot, int rs, int zchunk, int nd) {
-  const size_t nfl = 3 * (size_t)zchunk * rs + (size_t)zchunk * nline * kColFusedConsts + 2 * (size_t)zchunk +
-                     (2 + (size_t)nd) * nslot + 3 * (size_t)nd * nf;
+  const size_t nfl = 3 * (size_t)nd * zchunk * rs + (size_t)zchunk * nline * kColFusedConsts + 2 * (size_t)zchunk +
+                     (2 + (size_t)nd) * nslot + 3 * (size_t)nd * nf + 3 * (size_t)nd;
   const size_t nint = (size_t)nline * kColFusedLineInts + (nf + 1) + (size_t)nslot;
   return 4 * (nfl + nint);
 }
@@ -125,28 +127,74 @@ __device__ __forceinline__ void colf_opacity(const ColFusedArgs &A, const float 
   units_split_point(xh, be, P.oL, P.oR, 0.0f, false, A.units_floor, 0, P.chi, P.S);
 }
 
+// the upstream ghost of direction d at frequency f: zero, or for upward rays the
+// PCHIP extrapolation from the first two cells' transfer units with I = S
+// (k_long_char_columns); the first chunk holds the first two cells' constants
+__device__ __forceinline__ void colf_ghost(const ColFusedArgs &A, const float *sC, const float *sVz,
+                                           const float *sIdf, const int *sLi, const int *sLx, const float *sq,
+                                           int nl, int f, int p0, int n, int k0, float muf, float &xu, float &su,
+                                           float &iu) {
+  const size_t nfs = (size_t)A.W.nf;
+  ColfPoint P1, P2;
+  const size_t o1 = f + nfs * k0, o2 = f + nfs * (k0 + 1);
+  colf_opacity(A, sC, sLi, sLx, sq, f, p0, n, sVz[0] * muf, sIdf[0], A.xhat[o1], A.ehat[o1], A.beta[o1], P1);
+  colf_opacity(A, sC + (size_t)nl * kColFusedConsts, sLi, sLx, sq, f, p0, n, sVz[1] * muf, sIdf[1], A.xhat[o2],
+               A.ehat[o2], A.beta[o2], P2);
+  const PchipConst pc = A.pc;
+  float gv[2];
+  const float y1s[2] = {P1.chi, P1.S}, y2s[2] = {P2.chi, P2.S};
+#pragma unroll
+  for (int k = 0; k < 2; k++) {
+    const float y1 = y1s[k], y2 = y2s[k];
+    const float dy1 = y2 - y1;
+    const float dydx1 = (2.0f * dy1) / pc.dx1 - 0.0f;
+    const float v = (pc.c0 * y1 + pc.p * y2) + pc.dx1 * (pc.cm0 * dydx1 + pc.cm1 * 0.0f);
+    gv[k] = fmaxf(v, 0.0f);
+  }
+  xu = gv[0];
+  su = gv[1];
+  iu = su;
+}
+
+// a point's inputs, read once per hemisphere (streaming loads: the QLG table keeps L1)
+__device__ __forceinline__ void colf_load(const ColFusedArgs &A, size_t o, float &xh, float &eh, float &be,
+                                          float &nb, float &Jv, float &Pv) {
+  xh = __ldcs(A.xhat + o);
+  eh = __ldcs(A.ehat + o);
+  be = __ldcs(A.beta + o);
+  nb = __ldcs(A.Bnu + o);
+  Jv = A.first ? 0.0f : __ldcs(A.J + o);
+  Pv = A.first ? 0.0f : __ldcs(A.PsiJ + o);
+}
+
+// Every direction of the launch at one point: the point's inputs and J/PsiJ are read
+// once, the directions run in turn (each its own upstream state), J and PsiJ add
+// the directions in order, and each direction's rate terms go to its own rows.
 __global__ void __launch_bounds__(256, 3) k_col_ali_fused(ColFusedArgs A) {
   extern __shared__ float sm[];
   const NlWinDev &W = A.W;
   const int nf = W.nf, nl = W.nline, Z = A.zchunk, RS = A.rs, NS = A.nslot, ND = A.nd;
   const int BS = blockDim.x, tid = threadIdx.x;
-  float *sT0 = sm, *sT1 = sT0 + (size_t)Z * RS, *sT3 = sT1 + (size_t)Z * RS;
-  float *sC = sT3 + (size_t)Z * RS;                      // (Z, nl, 8)
-  float *sVz = sC + (size_t)Z * nl * kColFusedConsts;     // (Z)
-  float *sIdf = sVz + Z;                                  // (Z)
-  float *sq = sIdf + Z;                                   // (NS) q of each line point
-  float *swq = sq + NS;                                   // (NS) profile weights
-  float *swm = swq + NS;                                  // (ND, NS) wmu wnu Aij
-  float *sXu = swm + (size_t)ND * NS;                     // (ND, nf) upstream chi, S, I
+  const size_t ZR = (size_t)Z * RS;
+  float *sT = sm;                                          // (ND, 3, Z, RS) rate terms t0, t1, t3
+  float *sC = sT + (size_t)ND * 3 * ZR;                    // (Z, nl, 8)
+  float *sVz = sC + (size_t)Z * nl * kColFusedConsts;      // (Z)
+  float *sIdf = sVz + Z;                                   // (Z)
+  float *sq = sIdf + Z;                                    // (NS) q of each line point
+  float *swq = sq + NS;                                    // (NS) profile weights
+  float *swm = swq + NS;                                   // (ND, NS) wmu wnu Aij
+  float *sXu = swm + (size_t)ND * NS;                      // (ND, nf) upstream chi, S, I
   float *sSu = sXu + (size_t)ND * nf;
   float *sIu = sSu + (size_t)ND * nf;
-  int *sLi = reinterpret_cast<int *>(sIu + (size_t)ND * nf);  // (nl, 8)
-  int *sLp = sLi + (size_t)kColFusedLineInts * nl;             // (nf + 1) per-frequency line lists
-  int *sLx = sLp + nf + 1;                                     // (NS)
+  float *sDir = sIu + (size_t)ND * nf;                     // (ND, 3): mu, ds/2|mu|, 2 wmu
+  int *sLi = reinterpret_cast<int *>(sDir + 3 * ND);       // (nl, 8)
+  int *sLp = sLi + (size_t)kColFusedLineInts * nl;         // (nf + 1) per-frequency line lists
+  int *sLx = sLp + nf + 1;                                 // (NS)
 
   const int col = blockIdx.x;
   const int k0 = A.col_off[col], k1 = A.col_off[col + 1], nz = k1 - k0;
   const size_t nfs = (size_t)nf;
+  const float ds = (float)A.dz[col];
   for (int i = tid; i < nl; i += BS) {
     const bool act = !W.lactive || W.lactive[i];
     int *Li = sLi + kColFusedLineInts * i;
@@ -167,8 +215,12 @@ __global__ void __launch_bounds__(256, 3) k_col_ali_fused(ColFusedArgs A) {
       for (int d = 0; d < ND; d++) swm[(size_t)d * NS + s] = (float)((double)A.wmu[d] * W.wnu[o] * W.Aij[i]);
     }
   }
+  for (int d = tid; d < ND; d += BS) {
+    sDir[3 * d] = (float)A.mu[d];
+    sDir[3 * d + 1] = (float)((double)(0.5f * ds) / fabs(A.mu[d]));
+    sDir[3 * d + 2] = 2.0f * A.wmu[d];
+  }
   const int dir = A.mu[0] > 0 ? 1 : -1;
-  const float ds = (float)A.dz[col];
   const float dtmax = -A.dtau_max, Imax = A.Inu_max;
 
   for (int i0 = 0; i0 < nz; i0 += Z) {
@@ -186,59 +238,55 @@ __global__ void __launch_bounds__(256, 3) k_col_ali_fused(ColFusedArgs A) {
       sIdf[zz] = A.inv_df[c];
     }
     __syncthreads();
-    for (int d = 0; d < ND; d++) {
-      const double mu = A.mu[d];
-      const float muf = (float)mu, w2 = 2.0f * A.wmu[d];
-      const float dsup05 = (float)((double)(0.5f * ds) / fabs(mu));
-      const float *wm = swm + (size_t)d * NS;
-      float *Xu = sXu + (size_t)d * nf, *Su = sSu + (size_t)d * nf, *Iu = sIu + (size_t)d * nf;
-      const bool init = A.first && d == 0;
-      if (i0 == 0) {
-        // the upstream ghost: zero, or for upward rays the PCHIP extrapolation from
-        // the first two cells' transfer units with I = S (k_long_char_columns)
-        for (int f = tid; f < nf; f += BS) {
+    if (i0 == 0) {
+      for (int f = tid; f < nf; f += BS) {
+        const int p0 = sLp[f], n = sLp[f + 1] - p0;
+        for (int d = 0; d < ND; d++) {
           float xu = 0.0f, su = 0.0f, iu = 0.0f;
-          if (dir > 0 && A.bottom == 2 && nz >= 2) {
-            const int p0 = sLp[f], n = sLp[f + 1] - p0;
-            ColfPoint P1, P2;
-            const size_t o1 = f + nfs * k0, o2 = f + nfs * (k0 + 1);
-            colf_opacity(A, sC, sLi, sLx, sq, f, p0, n, sVz[0] * muf, sIdf[0], A.xhat[o1], A.ehat[o1], A.beta[o1], P1);
-            colf_opacity(A, sC + (size_t)nl * kColFusedConsts, sLi, sLx, sq, f, p0, n, sVz[1] * muf, sIdf[1],
-                         A.xhat[o2], A.ehat[o2], A.beta[o2], P2);
-            const PchipConst pc = A.pc;
-            float gv[2];
-            const float y1s[2] = {P1.chi, P1.S}, y2s[2] = {P2.chi, P2.S};
-#pragma unroll
-            for (int k = 0; k < 2; k++) {
-              const float y1 = y1s[k], y2 = y2s[k];
-              const float dy1 = y2 - y1;
-              const float dydx1 = (2.0f * dy1) / pc.dx1 - 0.0f;
-              const float v = (pc.c0 * y1 + pc.p * y2) + pc.dx1 * (pc.cm0 * dydx1 + pc.cm1 * 0.0f);
-              gv[k] = fmaxf(v, 0.0f);
-            }
-            xu = gv[0];
-            su = gv[1];
-            iu = su;
-          }
-          Xu[f] = xu;
-          Su[f] = su;
-          Iu[f] = iu;
+          if (dir > 0 && A.bottom == 2 && nz >= 2)
+            colf_ghost(A, sC, sVz, sIdf, sLi, sLx, sq, nl, f, p0, n, k0, sDir[3 * d], xu, su, iu);
+          sXu[(size_t)d * nf + f] = xu;
+          sSu[(size_t)d * nf + f] = su;
+          sIu[(size_t)d * nf + f] = iu;
         }
       }
-      for (int zz = 0; zz < zc; zz++) {
+    }
+    // the thread's points of the chunk, cells outer and frequencies inner; the next
+    // point's inputs are loaded (streaming: each is read once per hemisphere) before
+    // the current one is solved
+    int zz = 0, f = tid;
+    bool live = f < nf;
+    float xh = 0.0f, eh = 0.0f, be = 0.0f, nb = 0.0f, Jv = 0.0f, Pv = 0.0f;
+    if (live) {
+      const int c = dir > 0 ? k0 + i0 : k1 - 1 - i0;
+      colf_load(A, f + nfs * c, xh, eh, be, nb, Jv, Pv);
+    }
+    while (live) {
+      int zn = zz, fn = f + BS;
+      if (fn >= nf) {
+        zn = zz + 1;
+        fn = tid;
+      }
+      const bool nlive = zn < zc;
+      float xh2 = 0.0f, eh2 = 0.0f, be2 = 0.0f, nb2 = 0.0f, Jv2 = 0.0f, Pv2 = 0.0f;
+      if (nlive) {
+        const int cn = dir > 0 ? k0 + i0 + zn : k1 - 1 - (i0 + zn);
+        colf_load(A, fn + nfs * cn, xh2, eh2, be2, nb2, Jv2, Pv2);
+      }
+      {
         const int c = dir > 0 ? k0 + i0 + zz : k1 - 1 - (i0 + zz);
-        const float vpr = sVz[zz] * muf, idf = sIdf[zz];
+        const float vz = sVz[zz], idf = sIdf[zz];
         const float *Cz = sC + (size_t)zz * nl * kColFusedConsts;
-        float *T0 = sT0 + (size_t)zz * RS, *T1 = sT1 + (size_t)zz * RS, *T3 = sT3 + (size_t)zz * RS;
-        for (int f = tid; f < nf; f += BS) {
-          const size_t o = f + nfs * c;
-          const float be = A.beta[o], nb = A.Bnu[o];
-          const int p0 = sLp[f], n = sLp[f + 1] - p0;
+        const size_t o = f + nfs * c;
+        const int p0 = sLp[f], n = sLp[f + 1] - p0;
+        for (int d = 0; d < ND; d++) {
+          const float muf = sDir[3 * d], dsup05 = sDir[3 * d + 1], w2 = sDir[3 * d + 2];
           ColfPoint P;
-          colf_opacity(A, Cz, sLi, sLx, sq, f, p0, n, vpr, idf, A.xhat[o], A.ehat[o], be, P);
+          colf_opacity(A, Cz, sLi, sLx, sq, f, p0, n, vz * muf, idf, xh, eh, be, P);
           // long_char_linear's step (k_long_char_columns)
           const float xx = P.chi, ss = P.S;
-          const float xxup = Xu[f], ssup = Su[f], Inuup = Iu[f];
+          const size_t u = (size_t)d * nf + f;
+          const float xxup = sXu[u], ssup = sSu[u], Inuup = sIu[u];
           float dt = dsup05 * (xxup + xx);
           dt = fmaxf(dt, dtmax);
           float E, Wt, Psi, Esc;
@@ -251,12 +299,14 @@ __global__ void __launch_bounds__(256, 3) k_col_ali_fused(ColFusedArgs A) {
           const float irem = off ? Inu : Irem;
           const float esc = off ? 1.0f : Esc;
           const float ps = (dt > 0 && xx > 0) ? Psi / xx : 0.0f;
-          A.J[o] = fmaf(w2, Inu, init ? 0.0f : A.J[o]);
-          A.PsiJ[o] = fmaf(w2, ps, init ? 0.0f : A.PsiJ[o]);
-          Xu[f] = xx;
-          Su[f] = ss;
-          Iu[f] = Inu;
+          Jv = fmaf(w2, Inu, Jv);
+          Pv = fmaf(w2, ps, Pv);
+          sXu[u] = xx;
+          sSu[u] = ss;
+          sIu[u] = Inu;
           // bound_bound_rates' terms of this point (k_bb_rates, split rates)
+          float *T0 = sT + (size_t)d * 3 * ZR + (size_t)zz * RS, *T1 = T0 + ZR, *T3 = T1 + ZR;
+          const float *wm = swm + (size_t)d * NS;
 #pragma unroll
           for (int k = 0; k < kColFusedMaxLines; k++) {
             if (k < n) {
@@ -290,15 +340,31 @@ __global__ void __launch_bounds__(256, 3) k_col_ali_fused(ColFusedArgs A) {
             }
           }
         }
+        __stcs(A.J + o, Jv);
+        __stcs(A.PsiJ + o, Pv);
       }
-      __syncthreads();
-      // each (line, cell): the sums over the line's points in ascending f
-      for (int p = tid; p < nl * zc; p += BS) {
-        const int i = p / zc, zz = p - i * zc;
-        const int *Li = sLi + kColFusedLineInts * i;
-        if (!Li[3]) continue;
-        const float *r0 = sT0 + (size_t)zz * RS + Li[0], *r1 = sT1 + (size_t)zz * RS + Li[0],
-                    *r3 = sT3 + (size_t)zz * RS + Li[0];
+      zz = zn;
+      f = fn;
+      live = nlive;
+      xh = xh2;
+      eh = eh2;
+      be = be2;
+      nb = nb2;
+      Jv = Jv2;
+      Pv = Pv2;
+    }
+    __syncthreads();
+    // each (line, cell): for each direction in turn, the sums over the line's points
+    // in ascending f, then the rates' update (the directions' order of k_bb_rates)
+    for (int p = tid; p < nl * zc; p += BS) {
+      const int i = p / zc, zz = p - i * zc;
+      const int *Li = sLi + kColFusedLineInts * i;
+      if (!Li[3]) continue;
+      const int c = dir > 0 ? k0 + i0 + zz : k1 - 1 - (i0 + zz);
+      const size_t kk = (size_t)c + (size_t)A.ncell * i;
+      float gij = A.gw_ij[kk], gji = A.gw_ji[kk];
+      for (int d = 0; d < ND; d++) {
+        const float *r0 = sT + (size_t)d * 3 * ZR + (size_t)zz * RS + Li[0], *r1 = r0 + ZR, *r3 = r1 + ZR;
         float s0 = 0.0f, s1 = 0.0f, s3 = 0.0f;
         for (int k = 0; k < Li[4]; k++) {
           s0 = s0 + r0[k];
@@ -310,12 +376,11 @@ __global__ void __launch_bounds__(256, 3) k_col_ali_fused(ColFusedArgs A) {
           g_th = g_th / (s3 * A.wtot);
           g_dev = g_dev / (s3 * A.wtot);
         }
-        const int c = dir > 0 ? k0 + i0 + zz : k1 - 1 - (i0 + zz);
-        const size_t kk = (size_t)c + (size_t)A.ncell * i;
-        A.gw_ij[kk] = A.gw_ij[kk] + g_th;
-        A.gw_ji[kk] = A.gw_ji[kk] + g_dev;
+        gij = gij + g_th;
+        gji = gji + g_dev;
       }
-      __syncthreads();
+      A.gw_ij[kk] = gij;
+      A.gw_ji[kk] = gji;
     }
   }
 }

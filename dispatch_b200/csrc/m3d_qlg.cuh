@@ -8,10 +8,8 @@
 // The tables are read interleaved, tab[i] = (TGX(i), TH2X(i)), one 8-byte load per
 // point.  Two exact rewrites keep the point cost down: 1/(1+u) is the correctly
 // rounded reciprocal (__frcp_rn equals the IEEE quotient 1.0f/(1+u)), and the
-// snapped index nint(min(xs*800, 9019)) is formed as (int)(y + 0.5f) for y >= 0.5
-// and 0 below -- for y in [0.5, 9019] the sum y + 0.5f rounds across no integer, so
-// the truncation equals round-half-away-from-zero, and y < 0.5 (including the one
-// float just below 0.5, whose sum rounds up to 1) snaps to node 0.
+// snapped index nint(min(xs*800, 9019)) is floor(y + 0.5), taken from the bits of
+// RZ(RZ(y + 0.5) + 2^23) (qlg_node) without a float-to-int conversion.
 #pragma once
 #include "m3d_math.cuh"
 
@@ -70,14 +68,23 @@ __device__ __forceinline__ float qlg_rcp(float d) {
   return __frcp_rn(d);
 }
 
+// the snapped table node nint(y) of y = min(xs 800, 9019) >= 0 (NaN included: fminf
+// returns 9019): floor(y + 0.5), which is floor(RZ(y + 0.5)) since rounding toward
+// zero never carries a positive sum past the integer below it; adding 2^23 toward
+// zero then leaves that integer in the low mantissa bits.  Two additions and an
+// integer subtraction, no float-to-int conversion; equal to (int)(y + 0.5f) with
+// y < 0.5 sent to node 0 for every y in [0, 9019].
+__device__ __forceinline__ int qlg_node(float y) {
+  return __float_as_int(__fadd_rz(__fadd_rz(y, 0.5f), 8388608.0f)) - 0x4B000000;
+}
+
 template <bool MK = false>
 __device__ __forceinline__ float qlg_eval(const float2 *tab, const QlgCoef &c, float x) {
   const float xs = fabsf(x) * c.ih;
   const float u = xs * xs;
   const float L = qlg_rcp<MK>(1.0f + u);
   const float y = fminf(xs * 800.0f, 9019.0f);
-  const int ig = y < 0.5f ? 0 : (int)(y + 0.5f);
-  const float2 gw = tab[ig];
+  const float2 gw = tab[qlg_node(y)];
   const float G = gw.x, W = gw.y;
   float p = fmaf(c.cZH, W, c.cL2);
   p = fmaf(L, p, c.bL);
