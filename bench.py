@@ -9,8 +9,8 @@ flux.  Metric: Gpt*nu*ray/s = 1e-9 * rays * cells * frequencies / s.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--nf NF] [--impl reference]
 
-Ranks (torchrun) each take their own frequency windows: the windows are
-independent (weak scaling, no data-path collective).  --impl reference times the
+Ranks (torchrun) each take their own frequency windows, spread over the band: the
+windows are independent (weak scaling, no data-path collective).  --impl reference times the
 CPU restatement of the reference on this host's cores on a bounded sample.
 """
 from __future__ import annotations
@@ -252,6 +252,12 @@ class CpuReference:
                 f"C restatement of the reference (-O3 -march=x86-64-v3), {seconds:.1f} s")
 
 
+def _timed_windows(rank: int, steps_total: int, nwin: int) -> list[int]:
+    """The windows a rank's steps take: spread over the band (stride 37, coprime with
+    the 125 windows of 32 frequencies), each rank its own, the same on both arms."""
+    return [((rank * steps_total + i) * 37) % nwin for i in range(steps_total)]
+
+
 def run_reference(a):
     """The reference arm: the CPU restatement on all host cores, the same windows as
     the device arm times, a bounded block of columns per step."""
@@ -260,7 +266,7 @@ def run_reference(a):
         return
     atm, llam_all, nu_all, vec, wmu = _make_inputs(a.nf)
     steps_total = a.warmup + a.steps
-    wins = [i % (NFREQ_TOTAL // a.nf) for i in range(steps_total)]
+    wins = _timed_windows(0, steps_total, NFREQ_TOTAL // a.nf)
     ref = CpuReference(atm, vec, wmu, ncols=REF_NCOLS)
     for i in range(a.warmup):
         ref.step(*_window(llam_all, nu_all, a.nf, wins[i]))
@@ -628,7 +634,7 @@ def run_b200(a):
     datm["species"] = [{k: to_dev(v) for k, v in sp.items()} for sp in atm["species"]]
     nwin = NFREQ_TOTAL // nf
     steps_total = a.warmup + a.steps
-    wins = [(rank * steps_total + i) % nwin for i in range(steps_total)]
+    wins = _timed_windows(rank, steps_total, nwin)
     dwin = [tuple(to_dev(x) for x in _window(llam_all, nu_all, nf, w)) for w in wins]
 
     def step(i):
@@ -803,7 +809,8 @@ def run_b200(a):
         return
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32", "data": "synthetic (seeded grey cube, random line list)", "config": _workload(nf, a.cube),
+            "dtype": "f32", "data": "synthetic (seeded grey cube, random line list)",
+            "config": {**_workload(nf, a.cube), "windows_timed_rank0": wins[a.warmup:]},
             "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline, "roofline_sweep": roofline_sweep,
             "cpu_baseline": cpu, "clocks": clocks, "stages": stages, "fp64_plain": fp64, "c0_1d": c0, "c4_adjoint": c4,
             "nlte_ali": nlte, "nlte_batched": batched, "optab": optab}

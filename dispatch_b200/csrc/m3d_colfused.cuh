@@ -170,7 +170,7 @@ __device__ __forceinline__ void colf_load(const ColFusedArgs &A, size_t o, float
 // Every direction of the launch at one point: the point's inputs and J/PsiJ are read
 // once, the directions run in turn (each its own upstream state), J and PsiJ add
 // the directions in order, and each direction's rate terms go to its own rows.
-__global__ void __launch_bounds__(256, 3) k_col_ali_fused(ColFusedArgs A) {
+__global__ void __launch_bounds__(256, 4) k_col_ali_fused(ColFusedArgs A) {
   extern __shared__ float sm[];
   const NlWinDev &W = A.W;
   const int nf = W.nf, nl = W.nline, Z = A.zchunk, RS = A.rs, NS = A.nslot, ND = A.nd;
