@@ -43,6 +43,7 @@ struct Ctx {
   float *d_dW = nullptr;       // W'(u) of the TH2X table, for the adjoint (built on first use)
   std::vector<float> h_tgx, h_th2x;
   long long launches = 0;
+  int se_team = 0;             // threads per cell of the last m3d_stateq_update
   std::string err;
   // scratch buffers kept between calls, grown on demand
   std::vector<void *> scratch;

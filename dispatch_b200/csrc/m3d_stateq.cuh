@@ -342,6 +342,20 @@ __global__ void k_collision_rates(SeAtomDev A, SeCells C, double *__restrict__ c
 // ---- the per-warp dense solvers ------------------------------------------------
 // a(i,j) = W[i + n*j]; e is the right-hand side, the solution on return.
 
+// A cell's team: TEAM threads share its matrix, one warp (TEAM = 32) or a whole
+// block of 64 or 128 threads, whose barriers are then the block's.
+template <int TEAM>
+__device__ __forceinline__ void team_sync() {
+  if (TEAM == 32) __syncwarp();
+  else __syncthreads();
+}
+
+template <int TEAM>
+__device__ __forceinline__ bool team_all(bool v) {
+  if (TEAM == 32) return __all_sync(0xffffffffu, v);
+  return __syncthreads_and(v) != 0;
+}
+
 // a(i,j) - l a(k,j) of one element; SKIP: left alone where a(k,j) = 0, as
 // lineq_no_pivot skips it
 template <bool SKIP>
@@ -357,21 +371,21 @@ __device__ __forceinline__ double se_elim(double aij, double l, double akj) {
 // the columns into G groups.  l(i) stays in a register and four columns' loads
 // precede their stores, so the FP64 chains of a lane overlap.  Every element takes
 // its one update per step, so the roundings are the sequential loop's.
-template <bool SKIP>
+template <bool SKIP, int TEAM = 32>
 __device__ __forceinline__ void se_elim_step(double *W, double *lstore, int n, int k, int lane) {
   const int m = n - k - 1;
   const double pk = W[k + n * k];
-  const int G = m >= 32 ? 1 : 32 / m;
-  const int g = m >= 32 ? 0 : lane / m;
+  const int G = m >= TEAM ? 1 : TEAM / m;
+  const int g = m >= TEAM ? 0 : lane / m;
   const bool act = g < G;
-  const int i0 = k + 1 + (m >= 32 ? lane : lane % m), i1 = i0 + 32;
-  const bool two = m > 32 && i1 < n;
+  const int i0 = k + 1 + (m >= TEAM ? lane : lane % m), i1 = i0 + TEAM;
+  const bool two = m > TEAM && i1 < n;
   double l0 = 0, l1 = 0;
   if (act) {
     l0 = W[i0 + n * k] / pk;
     if (two) l1 = W[i1 + n * k] / pk;
   }
-  __syncwarp();  // every group has read a(i,k) before group 0 may overwrite it with l(i)
+  team_sync<TEAM>();  // every group has read a(i,k) before group 0 may overwrite it with l(i)
   if (act) {
     if (g == 0) {
       lstore[i0] = l0;
@@ -400,17 +414,18 @@ __device__ __forceinline__ void se_elim_step(double *W, double *lstore, int n, i
       W[i0 + n * j] = se_elim<SKIP>(W[i0 + n * j], l0, a);
     }
   }
-  __syncwarp();
+  team_sync<TEAM>();
 }
 
 // lineq_no_pivot (op_math_mod.f90:420-449)
+template <int TEAM = 32>
 __device__ __forceinline__ void se_solve_no_pivot(double *W, double *e, int n, int lane) {
-  for (int k = 0; k < n - 1; k++) se_elim_step<true>(W, W + n * k, n, k, lane);
+  for (int k = 0; k < n - 1; k++) se_elim_step<true, TEAM>(W, W + n * k, n, k, lane);
   // forward substitution: per row the terms arrive in ascending j, as in the row loop
   for (int j = 0; j < n - 1; j++) {
     const double ej = e[j];
-    for (int i = j + 1 + lane; i < n; i += 32) e[i] = e[i] - W[i + n * j] * ej;
-    __syncwarp();
+    for (int i = j + 1 + lane; i < n; i += TEAM) e[i] = e[i] - W[i + n * j] * ej;
+    team_sync<TEAM>();
   }
   // back substitution: the row loop adds its terms in ascending j, an order no
   // column sweep reproduces, so one lane runs it
@@ -421,7 +436,7 @@ __device__ __forceinline__ void se_solve_no_pivot(double *W, double *e, int n, i
       e[i] = t / W[i + n * i];
     }
   }
-  __syncwarp();
+  team_sync<TEAM>();
 }
 
 // warp arg-max: largest v, ties to the smallest idx; idx < 0 never wins
@@ -432,6 +447,36 @@ __device__ __forceinline__ void warp_argmax(double &v, int &idx) {
     const bool take = oi >= 0 && (idx < 0 || ov > v || (ov == v && oi < idx));
     if (take) { v = ov; idx = oi; }
   }
+}
+
+// the team's arg-max: warp_argmax in each warp, then the warps' winners in warp
+// order with the same rule (largest v, ties to the smallest idx); every thread
+// returns the result
+template <int TEAM>
+__device__ __forceinline__ void team_argmax(double &v, int &idx) {
+  warp_argmax(v, idx);
+  if (TEAM == 32) return;
+  constexpr int NW = TEAM / 32 > 0 ? TEAM / 32 : 1;
+  __shared__ double tv[NW];
+  __shared__ int ti[NW];
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) {
+    tv[threadIdx.x >> 5] = v;
+    ti[threadIdx.x >> 5] = idx;
+  }
+  __syncthreads();
+  double bv = tv[0];
+  int bi = ti[0];
+  for (int w = 1; w < NW; w++) {
+    const double ov = tv[w];
+    const int oi = ti[w];
+    if (oi >= 0 && (bi < 0 || ov > bv || (ov == bv && oi < bi))) {
+      bv = ov;
+      bi = oi;
+    }
+  }
+  v = bv;
+  idx = bi;
 }
 
 // lineq: Gaussian elimination with full pivoting (op_math_mod.f90:263-356)
@@ -544,17 +589,20 @@ __host__ __device__ inline size_t se_warp_doubles(int n) { return (size_t)n * n 
 // CM 0: collision rates read from C.cup (or none); 1: formed here, electron
 // recipes only; 2: formed here, any recipes and records.  The host picks the
 // least general form, which keeps the common ones' register use down.
-template <int CM>
+template <int CM, int TEAM = 32>
 __global__ void k_stateq_update(SeAtomDev A, SeParams P, SeCells C, SeWarpBest *__restrict__ wbest,
                                 double *__restrict__ lvl_val, long long *__restrict__ lvl_cell,
                                 unsigned long long *__restrict__ counts, long long *__restrict__ nonfinite) {
   extern __shared__ double se_smem[];
-  const int n = A.n, lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  // a team of TEAM threads per cell: a warp (several teams per block), or the block
+  const int n = A.n, lane = TEAM == 32 ? (int)(threadIdx.x & 31) : (int)threadIdx.x;
+  const int wib = TEAM == 32 ? (int)(threadIdx.x >> 5) : 0;
   double *W = se_smem + se_warp_doubles(n) * wib;
   double *bl = W + n * n, *ns = bl + n, *e = ns + n, *q = e + n;
   int *icol = (int *)(q + n);
-  const int nwarp = gridDim.x * (blockDim.x >> 5);
-  const int gw = blockIdx.x * (blockDim.x >> 5) + wib;
+  const int tpb = TEAM == 32 ? (int)(blockDim.x >> 5) : 1;  // teams per block
+  const int nwarp = gridDim.x * tpb;
+  const int gw = blockIdx.x * tpb + wib;
   const int ncell = C.ncell;
   const double eup = fmax(P.max_update, 1.0), elo = 1.0 / eup;
 
@@ -573,16 +621,16 @@ __global__ void k_stateq_update(SeAtomDev A, SeParams P, SeCells C, SeWarpBest *
     if (!(totn > 0)) continue;
     if (C.temp && !(C.temp[c] < P.tmax_update)) continue;
     const double ekt = C.e_kT[c];
-    for (int k = lane; k < n; k += 32) {
+    for (int k = lane; k < n; k += TEAM) {
       bl[k] = C.b[(size_t)c + (size_t)ncell * k];
       ns[k] = C.nstar[(size_t)c + (size_t)ncell * k];
       e[k] = 0;
     }
-    for (int idx = lane; idx < n * n; idx += 32) W[idx] = 0;
-    __syncwarp();
+    for (int idx = lane; idx < n * n; idx += TEAM) W[idx] = 0;
+    team_sync<TEAM>();
     // radiative rates, round by round
     for (int r = 0; r < A.nround; r++) {
-      for (int t = A.round_off[r] + lane; t < A.round_off[r + 1]; t += 32) {
+      for (int t = A.round_off[r] + lane; t < A.round_off[r + 1]; t += TEAM) {
         const int kr = A.order[t];
         const int i = A.ti[kr], j = A.tj[kr];
         if ((A.ev[j] - A.ev[i]) * ekt > A.cut_x) {
@@ -611,7 +659,7 @@ __global__ void k_stateq_update(SeAtomDev A, SeParams P, SeCells C, SeWarpBest *
         W[j + n * i] = W[j + n * i] + r_up;
         W[i + n * j] = W[i + n * j] + r_down;
       }
-      __syncwarp();
+      team_sync<TEAM>();
     }
     // collisions times cswitch (:806-811).  c starts at zero and takes each
     // nonzero classic rate, the electron one first (classic_col :1846-1876), then
@@ -636,7 +684,7 @@ __global__ void k_stateq_update(SeAtomDev A, SeParams P, SeCells C, SeWarpBest *
       };
       if (CM != 1 && A.nel > 0) {
         const int r0 = A.chkind ? 2 * A.ncol : A.ncol;
-        for (int e = lane; e < A.nel; e += 32) {
+        for (int e = lane; e < A.nel; e += TEAM) {
           double cv = 0;
           for (int k = A.el_off[e]; k < A.el_off[e + 1]; k++) {
             const int code = A.el_src[k], idx = code >> 2, type = code & 3;
@@ -668,7 +716,7 @@ __global__ void k_stateq_update(SeAtomDev A, SeParams P, SeCells C, SeWarpBest *
           W[A.el_w[e]] = W[A.el_w[e]] + cv * P.cswitch;
         }
       } else {
-        for (int p = lane; p < A.ncol; p += 32) {
+        for (int p = lane; p < A.ncol; p += TEAM) {
           double ue, uh;
           pair_rates(p, ue, uh);
           if (ue == 0 && uh == 0) continue;
@@ -687,10 +735,10 @@ __global__ void k_stateq_update(SeAtomDev A, SeParams P, SeCells C, SeWarpBest *
           W[i + n * j] = W[i + n * j] + cd * P.cswitch;
         }
       }
-      __syncwarp();
+      team_sync<TEAM>();
     }
     // diagonal = -(column sum), each lane one column
-    for (int i = lane; i < n; i += 32) {
+    for (int i = lane; i < n; i += TEAM) {
       double s = 0;
       for (int k = 0; k < n; k++) s = s + W[k + n * i];
       W[i + n * i] = -s;
@@ -704,27 +752,31 @@ __global__ void k_stateq_update(SeAtomDev A, SeParams P, SeCells C, SeWarpBest *
         if (v > bst) { bst = v; pos = k; }
       }
     }
-    __syncwarp();
-    for (int idx = lane; idx < n * n; idx += 32) {
+    team_sync<TEAM>();
+    for (int idx = lane; idx < n * n; idx += TEAM) {
       const int i = idx % n, j = idx / n;
       W[idx] = (i == pos) ? bl[j] * ns[j] : (W[idx] * bl[j]) * ns[j];
     }
     if (lane == 0) e[pos] = totn;
-    __syncwarp();
+    team_sync<TEAM>();
 
-    if (P.solver == 1) se_solve_lineq(W, e, q, icol, n, lane);
-    else if (P.solver == 2) se_solve_partial(W, e, n, lane);
-    else se_solve_no_pivot(W, e, n, lane);
+    if constexpr (TEAM == 32) {
+      if (P.solver == 1) se_solve_lineq(W, e, q, icol, n, lane);
+      else if (P.solver == 2) se_solve_partial(W, e, n, lane);
+      else se_solve_no_pivot(W, e, n, lane);
+    } else {
+      se_solve_no_pivot<TEAM>(W, e, n, lane);  // the host sends only lineq_no_pivot to larger teams
+    }
 
     bool finite = true;
-    for (int k = lane; k < n; k += 32) finite = finite && (fabs(e[k]) <= DBL_MAX);
-    if (!__all_sync(0xffffffffu, finite)) {
+    for (int k = lane; k < n; k += TEAM) finite = finite && (fabs(e[k]) <= DBL_MAX);
+    if (!team_all<TEAM>(finite)) {
       if (lane == 0) atomicMin((unsigned long long *)nonfinite, (unsigned long long)c);
-      __syncwarp();
+      team_sync<TEAM>();
       continue;
     }
     // limiter, under-relaxation, the update
-    for (int k = lane; k < n; k += 32) {
+    for (int k = lane; k < n; k += TEAM) {
       double x = e[k];
       if (x < elo || x > eup) nclamp++;
       ntot++;
@@ -734,13 +786,13 @@ __global__ void k_stateq_update(SeAtomDev A, SeParams P, SeCells C, SeWarpBest *
       q[k] = bl[k];          // bold
       bl[k] = bl[k] * x;
     }
-    __syncwarp();
+    team_sync<TEAM>();
     double sum = 0;
     for (int k = 0; k < n; k++) sum = sum + bl[k] * ns[k];
     const double norm = totn / sum;
     double wv = -1.0;
     int wk = -1;
-    for (int k = lane, slot = 0; k < n; k += 32, slot++) {
+    for (int k = lane, slot = 0; k < n; k += TEAM, slot++) {
       double x = bl[k] * norm;
       if (ns[k] > 0) x = fmax(x, fmin(1.0, P.min_pop_frac * totn / ns[k]));
       const double bold = q[k];
@@ -752,19 +804,19 @@ __global__ void k_stateq_update(SeAtomDev A, SeParams P, SeCells C, SeWarpBest *
       e[k] = ek;
       C.b[(size_t)c + (size_t)ncell * k] = x;
     }
-    warp_argmax(wv, wk);
-    __syncwarp();
+    team_argmax<TEAM>(wv, wk);
+    team_sync<TEAM>();
     if (wk >= 0 && wv > best.maxerr_abs) {
       best.maxerr_abs = wv;
       best.maxerr = copysign(wv, e[wk]);
       best.cell = c;
       best.level = wk;
     }
-    __syncwarp();
+    team_sync<TEAM>();
   }
   // per-warp partials
   if (lane == 0) wbest[gw] = best;
-  for (int k = lane, slot = 0; k < n; k += 32, slot++) {
+  for (int k = lane, slot = 0; k < n; k += TEAM, slot++) {
     lvl_val[(size_t)gw * n + k] = lv[slot];
     lvl_cell[(size_t)gw * n + k] = lc[slot];
   }
@@ -772,7 +824,7 @@ __global__ void k_stateq_update(SeAtomDev A, SeParams P, SeCells C, SeWarpBest *
     nclamp += __shfl_xor_sync(0xffffffffu, nclamp, o);
     ntot += __shfl_xor_sync(0xffffffffu, ntot, o);
   }
-  if (lane == 0 && ntot) {
+  if ((threadIdx.x & 31) == 0 && ntot) {
     atomicAdd(&counts[0], nclamp);
     atomicAdd(&counts[1], ntot);
   }

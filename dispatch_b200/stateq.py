@@ -24,7 +24,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from . import DEVICE_PTRS, M3DError, check, init, lib, order_after_torch, ptr
+from . import DEVICE_PTRS, SE_WARP, M3DError, check, init, lib, order_after_torch, ptr
 
 LINEQ_NO_PIVOT, LINEQ, LU_PARTIAL = 0, 1, 2
 COL_REGEMORTER, COL_SEATON = 1, 2
@@ -269,12 +269,13 @@ def collision_rates(atom: dict, temp, ne, e_kT, dxi=None, nh1=None, nstar=None, 
 def stateq_update(atom: dict, b, nstar, totn, e_kT, gamma_ij, gamma_ji, temp=None, ne=None, dxi=None, cup=None,
                   nh1=None, lsaha=None, colliders=None, solver: int = LINEQ_NO_PIVOT, max_update: float = 1e2,
                   sor_w: float = 1.0, min_pop_frac: float = 1e-30, conv_pop_floor: float = 0.0, tmax_update: float = 1e7,
-                  cswitch: float = 1.0) -> tuple[dict, np.ndarray]:
+                  cswitch: float = 1.0, warp_per_cell: bool = False) -> tuple[dict, np.ndarray]:
     """update_populations over all cells; b (nlevel, ncell) float64 is updated in place.
 
     Returns (result, lvlerr): maxerr, epos_cell, epos_level, nclamp, ntot,
-    nonfinite_cell, and the per-level largest change.  Raises
-    NonFiniteSolution (carrying both) when a cell's solution is not finite.
+    nonfinite_cell, the per-level largest change, and team (threads per cell).
+    Raises NonFiniteSolution (carrying both) when a cell's solution is not finite.
+    warp_per_cell: one warp per cell (M3D_SE_WARP) instead of the library's choice.
     """
     init()
     st, keep = make_atom(atom)
@@ -291,8 +292,9 @@ def stateq_update(atom: dict, b, nstar, totn, e_kT, gamma_ij, gamma_ji, temp=Non
     rc = lib().m3d_stateq_update(C.byref(st), C.byref(par), C.c_int(ncell), ptr(b), ptr(nstar), ptr(totn),
                                  ptr(e_kT), C.byref(cells), ptr(gamma_ij), ptr(gamma_ji), ptr(cup),
                                  C.c_void_p(lvlerr.ctypes.data), C.byref(res),
-                                 C.c_uint(_flags(b, nstar, totn, e_kT)))
+                                 C.c_uint(_flags(b, nstar, totn, e_kT) | (SE_WARP if warp_per_cell else 0)))
     out = res.as_dict()
+    out["team"] = int(lib().m3d_stateq_team())
     if rc == ENONFINITE:
         from . import last_error
         raise NonFiniteSolution(last_error(), out, lvlerr)

@@ -50,6 +50,7 @@ extern "C" {
 #define M3D_ROTATE 0x20u      /* quadratic solver: apply rotate_array first (3D output pass) */
 #define M3D_AUTOTUNE 0x40u    /* m3d_col_plan_create: time the launch shapes and keep the fastest */
 #define M3D_COL_PERPOINT 0x80u /* m3d_col_plan_create: the per-point kernels instead of the fused column sweep */
+#define M3D_SE_WARP 0x100u     /* m3d_stateq_update: one warp per cell whatever the atom's size */
 
 /* ---- formal solvers (rt_patch_mod.f90:1649-1721, rt_params_mod.f90 solver names) ---- */
 #define M3D_SOLVER_LINEAR 0        /* long_char_linear, rt_solvers_mod.f90:666 ('linear', 1D) */
@@ -591,11 +592,19 @@ int m3d_collision_rates(const m3d_atom_t *atom, int ncell, const double *e_kT, c
  * m3d_collision_rates forms them.  cells may be NULL without collisions or temp
  * filter.  lvlerr (nlevel, host) and res (host) receive the convergence record.
  * A cell whose solution is not finite keeps its b, and the call returns
- * M3D_ENONFINITE with res->nonfinite_cell set (the reference stops the run there). */
+ * M3D_ENONFINITE with res->nonfinite_cell set (the reference stops the run there).
+ * Each cell is solved by a team of threads sharing its matrix: one warp, or for
+ * lineq_no_pivot a block of 64 or 128 threads when that keeps more threads resident
+ * (large atoms); every element takes the same operations in the same order either
+ * way.  M3D_SE_WARP keeps one warp per cell. */
 int m3d_stateq_update(const m3d_atom_t *atom, const m3d_se_params_t *par, int ncell, double *b,
                       const double *nstar, const double *totn, const double *e_kT,
                       const m3d_col_cells_t *cells, const float *gamma_ij, const float *gamma_ji,
                       const double *cup, double *lvlerr, m3d_se_result_t *res, unsigned flags);
+
+/* Threads per cell of this thread context's last m3d_stateq_update (32, 64 or 128;
+ * 0 before the first).  Diagnostic. */
+int m3d_stateq_team(void);
 
 /* ng_accumulate (ng_mod.f90:241-287): gram (host, 7) = d01, d02, d11, d12, d21, d22
  * and |d0|^2 over all cells and levels of ln b; oldb is (ncell, nlevel, 3), the

@@ -41,6 +41,7 @@ def _gpu_update(se, atom, inp, cup=None, **kw):
     b = inp["b"].copy()
     res, lvlerr = se.stateq_update(atom, b, inp["nstar"], inp["totn"], inp["e_kT"], inp["gamma_ij"],
                                    inp["gamma_ji"], temp=inp["temp"], ne=inp["ne"], cup=cup, **kw)
+    res.pop("team")
     return b, res, lvlerr
 
 
@@ -68,6 +69,40 @@ def test_update_bitexact(sq, se, solver, nbound, nline):
     assert np.array_equal(bg, bo)
     assert rg == ro
     assert np.array_equal(lg, lo)
+
+
+@pytest.mark.parametrize("nbound,nline", [(20, 60), (60, 180)])
+@pytest.mark.parametrize("form", ["cup", "fused", "hydrogen", "gencol"])
+def test_update_team_equals_warp(se, nbound, nline, form):
+    """A cell solved by a block of 64 or 128 threads (the library's choice for a
+    large atom under lineq_no_pivot) gives the bits of one warp per cell, with the
+    collision rates read, formed from the electron recipes, with the hydrogen
+    recipes, and with tabulated records."""
+    kw = {}
+    if form == "hydrogen":
+        kw["h_recipes"] = H_RECIPES
+    if form == "gencol":
+        kw["gencol"] = True
+    atom, inp = synth.se_config("small", ncell=3000, nbound=nbound, nline=nline, **kw)
+    cup = se.collision_rates(atom, inp["temp"], inp["ne"], inp["e_kT"]) if form == "cup" else None
+    cell_kw = _cell_kw(inp) if form in ("hydrogen", "gencol") else {}
+    out = []
+    for warp in (False, True):
+        b = inp["b"].copy()
+        res, lvlerr = se.stateq_update(atom, b, inp["nstar"], inp["totn"], inp["e_kT"], inp["gamma_ij"],
+                                       inp["gamma_ji"], temp=inp["temp"], ne=inp["ne"], cup=cup,
+                                       warp_per_cell=warp, **cell_kw)
+        out.append((b, res, lvlerr))
+    assert out[1][1]["team"] == 32
+    if nbound == 60:
+        assert out[0][1]["team"] > 32
+    for k in ("team",):
+        out[0][1].pop(k)
+        out[1][1].pop(k)
+    assert np.array_equal(out[0][0], out[1][0])
+    assert out[0][1] == out[1][1]
+    assert np.array_equal(out[0][2], out[1][2])
+    assert out[0][1]["maxerr"] != 0
 
 
 def test_update_rounds_inactive_cut(sq, se):
@@ -272,6 +307,7 @@ def test_update_skips_and_nonfinite(sq, se):
     with pytest.raises(se.NonFiniteSolution) as ei:
         se.stateq_update(atom, b, inp["nstar"], inp["totn"], inp["e_kT"], inp["gamma_ij"], inp["gamma_ji"],
                          temp=inp["temp"], cup=cup)
+    ei.value.result.pop("team")
     assert ei.value.result == ro
     for c in (5, 10, 11, 200):
         assert np.array_equal(b[:, c], inp["b"][:, c])
@@ -285,6 +321,7 @@ def test_update_device_pointers(sq, se):
     d = {k: torch.from_numpy(np.ascontiguousarray(v)).cuda() for k, v in inp.items()}
     rd, ld = se.stateq_update(atom, d["b"], d["nstar"], d["totn"], d["e_kT"], d["gamma_ij"], d["gamma_ji"],
                               temp=d["temp"], ne=d["ne"])
+    rd.pop("team")
     assert np.array_equal(d["b"].cpu().numpy(), bh) and rd == rh and np.array_equal(ld, lh)
 
 
