@@ -161,13 +161,13 @@ def _peaks():
 #  k_quad_rot_column2: DRAM bytes per cell and frequency of a launch (28,360,192 B read
 #    for 110,592 cells x 32 frequencies), against 8 B algorithmic (chi and Snu once).
 #  k_lte_opacity_units_lane<32>: warp instructions per (cell, line) of a launch
-#    (850,505,012 for 110,592 cells x 500 lines), which scales a full launch's count by
+#    (751,598,136 for 110,592 cells x 500 lines), which scales a full launch's count by
 #    its cells and lines; DRAM bytes per cell: 49.9 B read (measured) plus the chi and
 #    Snu it writes, 8 B per frequency (the small case's 28 MB of output stayed in L2,
 #    a full launch's 3.5 GB cannot).
 NCU_SWEEP_DRAM_BYTES_PER_CELL_FREQ = 8.013
-NCU_OPACITY_WARP_INST_PER_CELL_LINE = 850505012 / (110592 * 500)
-NCU_OPACITY_DRAM_READ_BYTES_PER_CELL = 5518080 / 110592
+NCU_OPACITY_WARP_INST_PER_CELL_LINE = 751598136 / (110592 * 500)
+NCU_OPACITY_DRAM_READ_BYTES_PER_CELL = 5516032 / 110592
 
 
 def _subcube(atm, n):

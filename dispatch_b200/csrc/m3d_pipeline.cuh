@@ -192,11 +192,13 @@ __device__ __forceinline__ void deposit_window(float (&chl)[NF], const float2 *s
 
 // The same deposit, two window points per instruction (packed f32x2 arithmetic,
 // each half rounded as the scalar form rounds it), for windows whose every 1 + xs^2
-// is below 2^126 (the Markstein reciprocal).  Three exact rewrites beside the packing:
+// is below 2^126 (the Markstein reciprocal).  Exact rewrites beside the packing:
 //  * xs is formed with its sign, x ih; only xs^2 and |xs| are used, and the rounded
 //    product is symmetric in the sign;
-//  * -(1 + u) is formed as -1 - u (the rounding is symmetric), which is the -d of
-//    the Newton step, and the approximate reciprocal is taken of its negation;
+//  * d = 1 + xs^2 is formed per half in scalar (a packed product feeding a packed
+//    sum was fused into one rounding by the code generator, which left K 1-2 ulp off
+//    at a few points of about one table-form window in 10^4), and -d enters the
+//    Newton step;
 //  * the snapped node nint(min(|xs| 800, 9019)) is floor(RZ(y + 0.5)): rounding
 //    toward zero never carries a positive sum past the integer below it, so this is
 //    round-half-up of y >= 0, i.e. nint, with no special case below y = 0.5.  Adding
@@ -221,7 +223,7 @@ template <int NF, bool FULL, bool FAR>
 __device__ __forceinline__ void deposit_window_x2(float (&chl)[NF], const float2 *s_tab, const QlgCoef &cf,
                                                   float x0, float kfa, int fa, int fb) {
   static_assert(NF % 2 == 0, "pairs of window points");
-  const f32x2 X0 = splat2(x0), IH = splat2(cf.ih), M1 = splat2(-1.0f), ONE = splat2(1.0f), BL = splat2(cf.bL);
+  const f32x2 X0 = splat2(x0), IH = splat2(cf.ih), ONE = splat2(1.0f), BL = splat2(cf.bL);
   const f32x2 KF = splat2(kfa);
   f32x2 P1 = 0, GG = 0, CZH = 0, CL2 = 0, GGc = 0;
   unsigned base = 0;
@@ -242,19 +244,20 @@ __device__ __forceinline__ void deposit_window_x2(float (&chl)[NF], const float2
     if (!FULL) F = add2(F, KF);  // (float)f + kfa, exact
     const f32x2 x = add2(X0, F);
     const f32x2 xs = mul2(x, IH);
-    const f32x2 u = mul2(xs, xs);
-    const f32x2 nd = sub2(M1, u);
-    float nda, ndb;
-    up2(nd, nda, ndb);
-    const f32x2 r = pk2(rcp_approx(-nda), rcp_approx(-ndb));
+    float xa, xb;
+    up2(xs, xa, xb);
+    // 1 + xs^2 in scalar: the code generator fuses a packed product into the packed
+    // sum that consumes it (one rounding where the reference rounds twice), which
+    // the scalar forms under -fmad=false never are
+    const float da = 1.0f + xa * xa, db = 1.0f + xb * xb;
+    const f32x2 nd = pk2(-da, -db);
+    const f32x2 r = pk2(rcp_approx(da), rcp_approx(db));
     const f32x2 e = fma2(nd, r, ONE);
     const f32x2 L = fma2(r, e, r);
     f32x2 K;
     if (FAR) {
       K = fma2(L, fma2(L, P1, BL), GG);
     } else {
-      float xa, xb;
-      up2(xs, xa, xb);
       const f32x2 y = pk2(fminf(fabsf(xa) * 800.0f, 9019.0f), fminf(fabsf(xb) * 800.0f, 9019.0f));
       const f32x2 v = add2_rz(add2_rz(y, splat2(0.5f)), splat2(8388608.0f));
       float va, vb;
@@ -419,7 +422,7 @@ __global__ void __launch_bounds__(256, 3) k_lte_opacity_units_lane(AtmosDev A, G
         // exact.  One vote per line picks the reciprocal for the whole window.
         const float xmax = fmaxf(fabsf(x0), fabsf(xe)) * cf.ih;
         if (__all_sync(conv, xmax <= 4611686018427387904.0f))
-          deposit_window<NF, true>(chl, s_tab, cf, x0, kfa, fa, fb, full, far);
+          deposit_window_mk<NF>(chl, s_tab, cf, x0, kfa, fa, fb, full, far);
         else
           deposit_window<NF, false>(chl, s_tab, cf, x0, kfa, fa, fb, full, far);
       }
