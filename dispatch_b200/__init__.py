@@ -40,7 +40,8 @@ EXPORTS = ("m3d_init", "m3d_free", "m3d_last_error", "m3d_version", "m3d_set_str
            "m3d_stateq_update", "m3d_ng_accumulate", "m3d_ng_extrapolate", "m3d_bb_damping", "m3d_bf_opacity",
            "m3d_bb_opacity", "m3d_work_to_transfer_units_split", "m3d_bb_rates", "m3d_bf_rates",
            "m3d_integrate_rates", "m3d_normalize_profiles", "m3d_combine_twins", "m3d_update_eta_mask",
-           "m3d_lte_populations", "m3d_particle_fields", "m3d_lte_emission", "m3d_col_plan_create", "m3d_col_plan_shape", "m3d_stateq_team",
+           "m3d_lte_populations", "m3d_particle_fields", "m3d_lte_emission", "m3d_col_plan_create",
+           "m3d_col_plan_shape", "m3d_stateq_team", "m3d_continuum_opacities",
            "m3d_col_plan_sweep", "m3d_col_plan_fields", "m3d_col_plan_destroy", "m3d_line_opacity_scat", "m3d_chi_scat_units",
            "m3d_long_char_hermite", "m3d_long_char_hermite2", "m3d_short_char_hermite", "m3d_optab_create", "m3d_optab_slopes", "m3d_optab_sample",
            "m3d_optab_sample_ll", "m3d_optab_destroy", "m3d_hydrogen_line", "m3d_h_profile", "m3d_vcs_load", "m3d_vcs_clear",

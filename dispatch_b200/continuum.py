@@ -1,0 +1,148 @@
+"""The continuum opacity of a frequency window on the device: HOP's
+composition_type%continuum_opacities (HOP/composition_mod.f90:2893-2984) through
+m3d_continuum_opacities.
+
+A component is a dict holding an absdat component's table and flags (bftrans_type,
+HOP/bftrans_mod.f90:19-52) and the number densities its absorption factor reads;
+the cells dict holds the EOS state.  Cell arrays are numpy (host) or CUDA tensors
+(device, then the outputs are CUDA tensors too); tables are numpy.
+
+    xhat, sigma = continuum_opacities(comps, lam, nu, cells)
+
+xhat and sigma are (ncell, nlam): the working-form true absorption and the
+electron + Rayleigh scattering opacity [1/cm].
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import DEVICE_PTRS, M3DError, check, init, lib, order_after_torch, ptr
+
+# absorption_factor's cases (bftrans_mod.f90:500-528), M3D_BF_* of the C header
+HMINUS, NPE, H, H_FF, PAIR, H2PLUS, PEDEP, PEACH, MOLECULAR, REGULAR = range(1, 11)
+
+_FLAGS = ("ilogl", "kvadl", "minex", "maxex", "loglam", "kvadt", "minet", "maxet", "iteta", "lam3", "log_table")
+_CELL = ("n", "n2", "part", "level_n")
+
+
+class BfComp(C.Structure):
+    """m3d_bf_comp_t."""
+
+    _fields_ = ([("kind", C.c_int), ("istim", C.c_int), ("nnu", C.c_int), ("ntt", C.c_int)]
+                + [(k, C.c_int) for k in _FLAGS] + [("k", C.c_int)]
+                + [("lam", C.c_void_p), ("lnlam", C.c_void_p), ("tt", C.c_void_p), ("xkap", C.c_void_p),
+                   ("ldisk", C.c_void_p)]
+                + [(k, C.c_double) for k in ("xkap_scale", "mint", "maxt", "minl", "maxl", "ion_xion", "level_g",
+                                             "level_xion", "awgt")]
+                + [(k, C.c_void_p) for k in _CELL])
+
+
+class ContCells(C.Structure):
+    """m3d_cont_cells_t."""
+
+    _fields_ = ([(k, C.c_void_p) for k in ("temp", "teta", "e_kT", "pe", "dxi", "ne", "nHI", "partHI", "nHeI",
+                                           "nH2")]
+                + [("HI_xion", C.c_double), ("helium_scattering", C.c_int), ("pad", C.c_int)])
+
+
+def set_table(xkap, ilogt: bool, ilogl: bool):
+    """bftrans_type%set_table (bftrans_mod.f90:77-91): the stored form of a table
+    xkap (ntt, nnu) as read -- divided by its maximum, logarithmic for a logarithmic
+    temperature interpolation (or, without temperature dependence, a logarithmic
+    wavelength one), ln of 1e-37 for non-positive entries.  Returns (xkap float32
+    (ntt, nnu), xkap_scale, log_table)."""
+    xkap = np.asarray(xkap, np.float64)
+    ntt = xkap.shape[0]
+    log_table = bool(ilogt if ntt > 1 else ilogl)
+    scale = float(xkap.max())
+    if scale <= 0:
+        scale = 1.0
+    if log_table:
+        stored = (np.log(np.where(xkap > 0, xkap, 1e-37)) - np.log(scale)).astype(np.float32)
+    else:
+        stored = (xkap / scale).astype(np.float32)
+    return np.ascontiguousarray(stored), scale, log_table
+
+
+def _cell_array(a, dev: bool):
+    if a is None:
+        return None
+    if dev:
+        return a.contiguous()
+    return np.ascontiguousarray(a, np.float64)
+
+
+def make_comps(comps: list, dev: bool = False):
+    """(array of BfComp, the arrays it points into)."""
+    n = len(comps)
+    arr = (BfComp * max(n, 1))()
+    keep = []
+    for s, c in zip(arr, comps):
+        lam = np.ascontiguousarray(c["lam"], np.float64)
+        tt = np.ascontiguousarray(c["tt"], np.float64)
+        xk = np.ascontiguousarray(c["xkap"], np.float32)
+        ld = np.ascontiguousarray(c.get("ldisk", np.zeros(lam.size, bool)), np.uint8)
+        lnlam = np.log(lam)
+        keep += [lam, tt, xk, ld, lnlam]
+        s.kind, s.istim, s.nnu, s.ntt = int(c["kind"]), int(c.get("istim", 0)), lam.size, tt.size
+        if xk.shape != (tt.size, lam.size):
+            raise M3DError(f"continuum: xkap must be (ntt, nnu) = ({tt.size}, {lam.size}), got {xk.shape}")
+        for k in _FLAGS:
+            setattr(s, k, int(bool(c.get(k, False))))
+        s.k = int(c.get("k", 0))
+        s.lam, s.lnlam, s.tt, s.xkap, s.ldisk = (a.ctypes.data for a in (lam, lnlam, tt, xk, ld))
+        for k in ("xkap_scale", "mint", "maxt", "minl", "maxl", "ion_xion", "level_g", "level_xion", "awgt"):
+            setattr(s, k, float(c.get(k, 0.0)))
+        for k in _CELL:
+            a = _cell_array(c.get(k), dev)
+            keep.append(a)
+            setattr(s, k, ptr(a).value if a is not None else None)
+    return arr, keep
+
+
+def make_cells(cells: dict, dev: bool = False):
+    s = ContCells()
+    keep = []
+    for k in ("temp", "teta", "e_kT", "pe", "dxi", "ne", "nHI", "partHI", "nHeI", "nH2"):
+        a = _cell_array(cells.get(k), dev)
+        keep.append(a)
+        setattr(s, k, ptr(a).value if a is not None else None)
+    s.HI_xion = float(cells.get("HI_xion", 13.598434))
+    s.helium_scattering = int(bool(cells.get("helium_scattering", True)))
+    return s, keep
+
+
+def continuum_opacities(comps: list, lam, nu, cells: dict, beta=None, sigma: bool = True):
+    """(xhat, sigma or None), each (ncell, nlam): numpy for host cells, CUDA tensors
+    for device cells (the cells dict's arrays all on one side)."""
+    init()
+    dev = not isinstance(cells["temp"], np.ndarray)
+    lam = np.ascontiguousarray(lam, np.float64)
+    nu = None if nu is None else np.ascontiguousarray(nu, np.float64)
+    ncell, nlam = int(cells["temp"].shape[0]), int(lam.size)
+    arr, keep = make_comps(comps, dev)
+    cs, keep2 = make_cells(cells, dev)
+    if dev:
+        import torch
+        xhat = torch.empty((ncell, nlam), dtype=torch.float32, device=cells["temp"].device)
+        sg = torch.empty_like(xhat) if sigma else None
+        beta = None if beta is None else beta.contiguous()
+        order_after_torch(cells["temp"])
+        flags = DEVICE_PTRS
+    else:
+        xhat = np.empty((ncell, nlam), np.float32)
+        sg = np.empty_like(xhat) if sigma else None
+        beta = None if beta is None else np.ascontiguousarray(beta, np.float32)
+        flags = 0
+    check(lib().m3d_continuum_opacities(C.c_int(len(comps)), arr, C.c_int(nlam), C.c_void_p(lam.ctypes.data),
+                                        None if nu is None else C.c_void_p(nu.ctypes.data), C.c_int(ncell),
+                                        C.byref(cs), ptr(beta), ptr(xhat), ptr(sg), C.c_uint(flags)),
+          "m3d_continuum_opacities")
+    del keep, keep2
+    return xhat, sg
+
+
+__all__ = ["continuum_opacities", "set_table", "BfComp", "ContCells", "HMINUS", "NPE", "H", "H_FF", "PAIR",
+           "H2PLUS", "PEDEP", "PEACH", "MOLECULAR", "REGULAR"]

@@ -25,6 +25,7 @@
 #include "m3d_aux.cuh"
 #include "m3d_columns.cuh"
 #include "m3d_colfused.cuh"
+#include "m3d_continuum.cuh"
 #include "m3d_optab.cuh"
 #include "m3d_hprof.cuh"
 #include "m3d_adjoint.cuh"
@@ -1476,6 +1477,7 @@ int m3d_lte_synthesis(const m3d_atmos_t *atm, int nf, const double *nu, const do
 
 #include "m3d_stateq_api.inc"
 #include "m3d_nlte_api.inc"
+#include "m3d_continuum_api.inc"
 #include "m3d_aux_api.inc"
 #include "m3d_columns_api.inc"
 #include "m3d_optab_api.inc"

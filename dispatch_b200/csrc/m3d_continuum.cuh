@@ -1,0 +1,283 @@
+// Continuum opacity of a window, HOP's composition_type%continuum_opacities
+// (HOP/composition_mod.f90:2893-2984):
+//   add_hrest                        :3807-3846
+//   the absdat components            bftrans_mod.f90: absorption_factor :476-531,
+//                                    interp_xkap :235-452 (their wavelength stencils,
+//                                    load_lam_interp_weights :100-198, on the host)
+//   components tabulated with stimulated emission, over 1 - beta   :2935-2970
+//   boltzmann_factor                 :2822-2852
+//   electron_scattering, rayleigh_scattering   :3851-3939
+// One warp per cell: the lanes first form each component's temperature stencil and
+// absorption factor for the cell (one component per lane), then run along the
+// window's wavelengths, each adding the components in their order.  Kinds follow the
+// Fortran: tables, xhat and sigma real(4); the EOS state, the absorption factors and
+// the wavelength cubes real(8); a real(4) value updated from a real(8) expression is
+// rounded once where the Fortran assigns it.
+#pragma once
+#include "m3d_math.cuh"
+
+namespace m3d {
+
+constexpr int kContWarps = 4;     // warps (cells) per block
+constexpr int kContMaxComp = 64;  // components of one call
+
+struct BfCompDev {
+  int kind, istim, nnu, ntt, ilogl, lam3, log_table, kvadt, minet, maxet, iteta, k, fs, fe, active, pad;
+  double xkap_scale, mint, maxt, ion_xion, level_g, level_xion, awgt;
+  const double *tt;
+  const float *xkap;      // (nnu, ntt)
+  const int *iw;          // (nlam) first stencil node, 0-based; -1 where none
+  const unsigned char *quad;
+  const float *lag;       // (3, nlam)
+  const double *n, *n2, *part, *level_n;
+};
+
+struct ContCellsDev {
+  const double *temp, *teta, *e_kT, *pe, *dxi, *ne, *nHI, *partHI, *nHeI, *nH2;
+  double HI_xion;
+  int helium_scattering;
+};
+
+// a component's state at one cell: the temperature stencil and the absorption factor
+struct BfCellDev {
+  float w0, w1, w2, fakt1;
+  int it, in_bounds, quadratic, edge;
+};
+
+// absorption_factor of one cell times xkap_scale, capped at the real(4) maximum
+__device__ __forceinline__ float cont_factor(const BfCompDev &c, const ContCellsDev &S, int x) {
+  const double ekt = S.e_kT[x], pe = S.pe[x], dxi = S.dxi[x];
+  double fk = DBL_MAX;
+  switch (c.kind) {
+    case 1: fk = c.n[x]; break;
+    case 2: fk = c.n[x] * pe; break;
+    case 3: {
+      int k5 = c.k * c.k;
+      k5 = k5 * k5 * c.k;
+      // the default-real literal over the integer 2 k^5: a real(4) quotient
+      fk = (double)__fdiv_rn(2.0898e-26f, (float)(2 * k5)) * c.level_n[x];
+      break;
+    }
+    case 4:
+      fk = exp(-ekt * (c.ion_xion - dxi) - c.part[x]);
+      fk = (double)2.0898e-26f / (2 * 13.598434 * ekt) * fk * c.n[x];
+      break;
+    case 5: fk = c.n[x] * c.n2[x]; break;
+    case 6: fk = 1e-40 * c.n[x] * c.n2[x]; break;
+    case 7: fk = pe * c.n[x]; break;
+    case 8: fk = pe * c.n[x]; fk = (1e-40 / 1.602189e-12) * ekt * fk; break;
+    case 9: fk = c.n[x] * c.awgt / 6.023e23; break;
+    case 10:
+      fk = c.level_g * exp(-ekt * c.level_xion - c.part[x]);
+      fk = fk * c.n[x];
+      break;
+  }
+  const double v = fk * c.xkap_scale;
+  return (float)(v < (double)FLT_MAX ? v : (double)FLT_MAX);
+}
+
+// interp_xkap's temperature stencil of one cell (:303-345)
+__device__ __forceinline__ BfCellDev cont_tstencil(const BfCompDev &c, double temp, double teta) {
+  BfCellDev r;
+  r.w0 = r.w1 = r.w2 = 0.0f;
+  r.it = 0;
+  r.quadratic = 0;
+  r.edge = 0;
+  bool inb = true;
+  if (!c.minet) inb = inb && (temp > c.mint);
+  if (!c.maxet) inb = inb && (temp < c.maxt);
+  r.in_bounds = inb;
+  if (!inb) return r;
+  const double t = c.iteta ? teta : temp;
+  const double *tt = c.tt;
+  const int ntt = c.ntt;
+  int it;
+  if (t < tt[0]) {
+    it = 1;
+    r.edge = 1;
+  } else if (t >= tt[ntt - 1]) {
+    it = ntt - 1;
+    r.edge = 2;
+  } else {
+    for (it = 1; it <= ntt - 1; it++)
+      if (tt[it] > t) break;
+    r.quadratic = c.kvadt;
+  }
+  if (r.quadratic) {
+    const int i = (it + 2 <= ntt) ? it : it - 1;
+    const double *t3 = tt + (i - 1);
+    const double dt1 = 1. / ((t3[0] - t3[1]) * (t3[0] - t3[2]));
+    const double dt2 = 1. / ((t3[1] - t3[0]) * (t3[1] - t3[2]));
+    const double dt3 = 1. / ((t3[2] - t3[0]) * (t3[2] - t3[1]));
+    const double d1 = t - t3[0], d2 = t - t3[1], d3 = t - t3[2];
+    r.w0 = (float)(d2 * d3 * dt1);
+    r.w1 = (float)(d1 * d3 * dt2);
+    r.w2 = (float)(d1 * d2 * dt3);
+    r.it = i;
+  } else {
+    const double dtdt1 = 1. / (tt[it] - tt[it - 1]);
+    r.w0 = (float)((t - tt[it - 1]) * dtdt1);
+    r.it = it;
+  }
+  return r;
+}
+
+// row j (1-based) of the table at the cell's temperature, converted to the form of
+// the wavelength interpolation (:332-357)
+__device__ __forceinline__ float cont_row(const BfCompDev &c, const BfCellDev &r, int j) {
+  const float *tab = c.xkap + (j - 1);
+  const size_t nnu = (size_t)c.nnu;
+  float y;
+  if (r.quadratic) {
+    const size_t i = (size_t)r.it;
+    y = __fadd_rn(__fadd_rn(__fmul_rn(tab[nnu * (i - 1)], r.w0), __fmul_rn(tab[nnu * i], r.w1)),
+                  __fmul_rn(tab[nnu * (i + 1)], r.w2));
+  } else {
+    const size_t it = (size_t)r.it;
+    const float a = tab[nnu * (it - 1)], b = tab[nnu * it];
+    y = __fadd_rn(__fmul_rn(__fsub_rn(b, a), r.w0), a);
+    if (r.edge == 1) y = fminf(y, tab[0]);
+    else if (r.edge == 2) y = fminf(y, tab[nnu * (c.ntt - 1)]);
+  }
+  if (c.log_table && !c.ilogl) y = exp4(y);
+  else if (c.ilogl && !c.log_table) y = logf(fmaxf(y, FLT_MIN));
+  return y;
+}
+
+// one component's contribution at wavelength f of the cell (interp_xkap :358-385 and
+// :386-426): returns false where it adds nothing
+__device__ __forceinline__ bool cont_comp(const BfCompDev &c, const BfCellDev &r, int f, double lam, float &add) {
+  if (!c.active || f < c.fs || f > c.fe) return false;
+  const int iw = c.iw[f];
+  float ab;
+  if (c.ntt > 1) {
+    if (!r.in_bounds) return false;
+    if (iw >= 0) {
+      const int i = iw + 1;
+      const float y1 = cont_row(c, r, i), y2 = cont_row(c, r, i + 1);
+      const float y3 = cont_row(c, r, i + 2 < c.nnu ? i + 2 : c.nnu);
+      const float *L = c.lag + 3 * (size_t)f;
+      ab = __fadd_rn(__fadd_rn(__fmul_rn(y1, L[0]), __fmul_rn(y2, L[1])), __fmul_rn(y3, L[2]));
+    } else {
+      ab = c.ilogl ? -FLT_MAX : 0.0f;
+    }
+    if (c.ilogl) ab = exp4(ab);
+    if (c.lam3) ab = __fmul_rn(ab, (float)(lam * lam * lam));
+    add = __fmul_rn(r.fakt1, ab);
+  } else {
+    if (iw < 0) {
+      ab = 0.0f;
+    } else {
+      const float *yy = c.xkap + iw;
+      const float *L = c.lag + 3 * (size_t)f;
+      ab = __fadd_rn(0.0f, __fmul_rn(yy[0], L[0]));
+      ab = __fadd_rn(ab, __fmul_rn(yy[1], L[1]));
+      if (c.quad[f]) ab = __fadd_rn(ab, __fmul_rn(yy[2], L[2]));
+      if (c.ilogl) ab = expf(ab);
+    }
+    if (c.lam3) ab = __fmul_rn(ab, (float)(lam * lam * lam));
+    add = __fmul_rn(ab, r.fakt1);
+  }
+  return true;
+}
+
+__global__ void __launch_bounds__(kContWarps * 32)
+k_continuum(int ncomp, const BfCompDev *__restrict__ comps, int any_istim, int nlam, const double *__restrict__ lam,
+            const double *__restrict__ nu, int ncell, ContCellsDev S, const float *__restrict__ beta,
+            float *__restrict__ xhat, float *__restrict__ sigma) {
+  __shared__ BfCellDev sc[kContWarps][kContMaxComp];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  BfCellDev *st = sc[wib];
+  const int nwarp = gridDim.x * kContWarps;
+  // thomson = 8./3.*PI*(EC**2/(EM*CC**2))**2 (composition_mod.f90:3856), a real(8)
+  // parameter whose 8./3. is a default-real quotient
+  const double rq = (4.80325e-10 * 4.80325e-10) / (9.109534e-28 * (2.99792458e10 * 2.99792458e10));
+  const double thomson = (double)(8.0f / 3.0f) * 3.14159265359 * (rq * rq);
+  for (int x = blockIdx.x * kContWarps + wib; x < ncell; x += nwarp) {
+    const double temp = S.temp[x], teta = S.teta[x];
+    for (int j = lane; j < ncomp; j += 32) {
+      const BfCompDev &c = comps[j];
+      BfCellDev r;
+      if (c.ntt > 1) {
+        r = cont_tstencil(c, temp, teta);
+      } else {
+        r.w0 = r.w1 = r.w2 = 0.0f;
+        r.it = 0;
+        r.in_bounds = 1;
+        r.quadratic = 0;
+        r.edge = 0;
+      }
+      r.fakt1 = (c.active && r.in_bounds) ? cont_factor(c, S, x) : 0.0f;
+      st[j] = r;
+    }
+    __syncwarp();
+    // add_hrest: the H I levels above n = 15, up to the lowered ionisation limit
+    const double ekt = S.e_kT[x], dxi = S.dxi[x];
+    const double nniv2 = (double)(15.5f * 15.5f);
+    bool hrest_on = false;
+    double hrest = 0.0;
+    if (S.nHI && 13.598434 >= nniv2 * dxi) {
+      double fakt = exp(-ekt * (S.HI_xion - dxi) - S.partHI[x]);
+      fakt = (double)2.0898e-26f / (2 * 13.598434 * ekt) * fakt * S.nHI[x];
+      hrest = exp(ekt * (13.598434 / nniv2 - dxi));
+      hrest = fakt * (hrest - 1);
+      hrest_on = true;
+    }
+    const double hk_T = (6.626176e-27 / 1.380662e-16) / temp;
+    const double nHIr = S.nHI ? S.nHI[x] : 0.0, nHE = S.nHeI ? S.nHeI[x] : 0.0, nH2 = S.nH2 ? S.nH2[x] : 0.0;
+    const double els = sigma ? thomson * S.ne[x] : 0.0;
+    for (int f = lane; f < nlam; f += 32) {
+      const double l = lam[f];
+      const size_t o = (size_t)f + (size_t)nlam * x;
+      float v = 0.0f;
+      if (hrest_on) v = (float)((double)v + hrest * (l * l * l));
+      for (int j = 0; j < ncomp; j++) {
+        const BfCompDev &c = comps[j];
+        if (c.istim) continue;
+        float add;
+        if (cont_comp(c, st[j], f, l, add)) v = __fadd_rn(v, add);
+      }
+      if (any_istim) {
+        float tmp = 0.0f;
+        for (int j = 0; j < ncomp; j++) {
+          const BfCompDev &c = comps[j];
+          if (!c.istim) continue;
+          float add;
+          if (cont_comp(c, st[j], f, l, add)) tmp = __fadd_rn(tmp, add);
+        }
+        float b;
+        if (beta) {
+          b = beta[o];
+        } else {
+          b = (float)exp(-nu[f] * hk_T);
+          b = b > FLT_MIN ? b : FLT_MIN;
+        }
+        v = __fadd_rn(v, __fdiv_rn(tmp, __fsub_rn(1.0f, b)));
+      }
+      xhat[o] = v;
+      if (sigma) {
+        float s = (float)(0.0 + els);
+        double xr = 0.0;
+        if (l > 1400.0) {
+          const double m = l > 1026.0 ? l : 1026.0;
+          xr = 1 / (m * m);
+        }
+        if (xr > 0.) {
+          const double rayh = ((double)5.799e-13f + xr * ((double)1.422e-6f + xr * (double)2.784f)) * nHIr;
+          const double rayh2 = ((double)8.14e-13f + xr * ((double)1.28e-6f + xr * (double)1.61f)) * nH2;
+          s = (float)((double)s + (rayh + rayh2) * xr * xr);
+        }
+        double he = 0.0;
+        if (S.helium_scattering) {
+          const double q = (double)500.f / l;
+          const double q2 = q * q;
+          he = (double)(0.66520e-24f * 4.f) * (q2 * q2);
+        }
+        sigma[o] = (float)((double)s + he * nHE);
+      }
+    }
+    __syncwarp();
+  }
+}
+
+}  // namespace m3d

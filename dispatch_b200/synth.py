@@ -851,3 +851,73 @@ def window_tables(seed, temp, ne, vproj, nf=256, lam0=5040.0, R=1e5, pad_guard=2
     bg = sample_table(seed, temp, ne, kind="background", lam_nodes=lam_q)
     ll = sample_table(seed + 1, temp, ne, kind="linelist", lam_nodes=plam, nline=nline)
     return lam_q, bg, ll
+
+
+def continuum_case(seed: int = 5, ncell: int = 2000, nlam: int = 256, lam_range=(3500.0, 12000.0)) -> tuple:
+    """(comps, lam, nu, cells) of a seeded continuum-opacity case: twelve absdat-like
+    components, one or more of every absorption-factor kind, their tables in the
+    stored form of set_table (dispatch_b200.continuum.set_table) with every
+    interpolation choice -- linear or quadratic in temperature (T or 5040/T nodes),
+    logarithmic tables, linear, quadratic or logarithmic in wavelength, nodes flagged
+    as discontinuities, extrapolation allowed or not at each end, lam^3 scaling, no
+    temperature dependence -- two tabulated with stimulated emission; tables that
+    cover the window only in part; cells below, inside and above the temperature
+    nodes; the EOS state drawn from a grey-atmosphere-like range (T 3500-12000 K,
+    ne 1e10-1e15 cm^-3).  The tables are synthetic (smooth positive cross sections
+    of realistic size), not HOP's absdat data."""
+    from .continuum import (H, H2PLUS, H_FF, HMINUS, MOLECULAR, NPE, PAIR, PEACH, PEDEP, REGULAR, set_table)
+    rng = np.random.default_rng(seed + 7000)
+    lam = np.geomspace(lam_range[0], lam_range[1], nlam)
+    nu = HZ_TO_AA / lam
+    temp = rng.uniform(3500.0, 12000.0, ncell)
+    e_kT = EE / (BK * temp)
+    ne = 10.0 ** rng.uniform(10.0, 15.0, ncell)
+    cells = {"temp": temp, "teta": 5040.0 / temp, "e_kT": e_kT, "pe": ne * BK * temp,
+             "dxi": rng.uniform(0.0, 0.06, ncell), "ne": ne, "nHI": 10.0 ** rng.uniform(14.0, 17.0, ncell),
+             "partHI": np.log(2.0) + rng.uniform(0.0, 1e-3, ncell), "nHeI": 10.0 ** rng.uniform(13.0, 16.0, ncell),
+             "nH2": 10.0 ** rng.uniform(6.0, 12.0, ncell), "HI_xion": 13.598434, "helium_scattering": True}
+    dens = lambda lo, hi: 10.0 ** rng.uniform(lo, hi, ncell)
+
+    def table(kind, nnu, lrange, tnodes, shape, ilogt=False, ilogl=False, **kw):
+        tl = np.geomspace(lrange[0], lrange[1], nnu)
+        tt = np.asarray(tnodes, np.float64)
+        raw = np.array([[shape(l, t) for l in tl] for t in tt]) if tt.size > 1 else np.array([[shape(l, 6000.0)
+                                                                                               for l in tl]])
+        xk, scale, logt = set_table(raw, ilogt, ilogl)
+        ld = np.zeros(nnu, bool)
+        ld[rng.choice(nnu - 2, size=max(1, nnu // 12), replace=False) + 1] = True
+        c = {"kind": kind, "lam": tl, "tt": tt, "xkap": xk, "xkap_scale": scale, "log_table": logt, "ldisk": ld,
+             "ilogl": ilogl, "minl": tl[0], "maxl": tl[-1], "mint": 0.0, "maxt": 1e9}
+        c.update(kw)
+        return c
+
+    tnod = np.linspace(4000.0, 10000.0, 7)
+    teta_nod = np.sort(5040.0 / np.linspace(4500.0, 11000.0, 8))
+    sig = lambda a, p: (lambda l, t: a * (l / 5000.0) ** p * (1.0 + 0.3 * np.sin(l / 700.0)) * (t / 6000.0) ** 0.5)
+    comps = [
+        table(HMINUS, 40, (2500.0, 16000.0), teta_nod, sig(4e-17, 0.8), ilogt=True, iteta=True, kvadl=True,
+              n=dens(8.0, 10.5)),
+        table(NPE, 30, (3000.0, 20000.0), tnod, sig(2e-26, 2.0), ilogt=True, kvadt=True, maxex=True,
+              n=dens(14.0, 17.0)),
+        table(H, 50, (3000.0, 8205.0), [6000.0], lambda l, t: 1e-17 * (l / 8205.0) ** 3, ilogl=True, lam3=True,
+              kvadl=True, k=3, level_n=dens(2.0, 7.0)),
+        table(H_FF, 20, (2000.0, 25000.0), tnod[:5], sig(1e-12, 1.0), lam3=True, ion_xion=13.598434,
+              n=dens(9.0, 13.0), part=np.log(rng.uniform(1.0, 1.5, ncell))),
+        table(PAIR, 25, (4000.0, 30000.0), [3000.0, 5000.0, 7000.0, 9000.0], sig(1e-45, 1.5), ilogt=True,
+              ilogl=True, loglam=True, n=dens(14.0, 17.0), n2=dens(13.0, 16.0)),
+        table(H2PLUS, 18, (3800.0, 9000.0), [4500.0, 6000.0, 7500.0], sig(1e-5, 0.5), kvadt=True,
+              mint=4600.0, maxt=9000.0, n=dens(10.0, 14.0), n2=dens(8.0, 12.0)),
+        table(PEDEP, 45, (3500.0, 11000.0), [5000.0], sig(3e-27, 1.2), kvadl=True, minex=True, maxex=True,
+              n=dens(8.0, 12.0)),
+        table(PEACH, 35, (3200.0, 13000.0), teta_nod[:7], sig(5e-3, 0.7), ilogt=True, iteta=True, kvadt=True,
+              kvadl=True, n=dens(6.0, 11.0)),
+        table(MOLECULAR, 22, (5000.0, 15000.0), tnod[1:], sig(2e-3, 1.0), ilogl=True, kvadt=True, minex=True,
+              awgt=28.0, n=dens(6.0, 10.0)),
+        table(REGULAR, 28, (3500.0, 7000.0), [6000.0], sig(2e-18, 3.0), lam3=True, level_g=9.0, level_xion=3.2,
+              n=dens(10.0, 13.0), part=np.log(rng.uniform(5.0, 30.0, ncell))),
+        table(HMINUS, 32, (4000.0, 14000.0), tnod, sig(3e-17, 0.6), istim=True, kvadt=True, kvadl=True,
+              loglam=True, n=dens(8.0, 10.5)),
+        table(REGULAR, 26, (3000.0, 9000.0), tnod[::2], sig(1e-18, 2.0), istim=True, ilogt=True, lam3=True,
+              level_g=2.0, level_xion=1.1, minex=True, n=dens(10.0, 13.0), part=np.log(rng.uniform(2.0, 9.0, ncell))),
+    ]
+    return comps, lam, nu, cells

@@ -472,6 +472,67 @@ int m3d_lte_synthesis_adjoint(const m3d_atmos_t *atm, int nf, const double *nu, 
                               const double *vec, const double *wmu, const float *g_flux, const m3d_lte_grad_t *grad,
                               unsigned flags);
 
+/* ---- continuum opacity of a window: composition_type%continuum_opacities
+ * (HOP/composition_mod.f90:2893-2984) -- the H I levels above n = 15 (add_hrest,
+ * :3807-3846), every absdat component (bftrans_mod.f90: load_lam_interp_weights
+ * :100-198, absorption_factor :476-531, interp_xkap :235-452), the components tabulated
+ * with stimulated emission over 1 - beta, and the scattering opacity: electrons
+ * (:3851-3872) and Rayleigh by H I, H2 and He I (:3878-3939).  The EOS state and the
+ * components' tables are inputs. */
+#define M3D_BF_HMINUS 1    /* 'H- BF': n */
+#define M3D_BF_NPE 2       /* 'H- FF', 'H2-', 'HE-': n Pe */
+#define M3D_BF_H 3         /* 'H BF' without occupation probabilities: 2.0898e-26/(2 k^5) n_k */
+#define M3D_BF_H_FF 4      /* 'H FF': 2.0898e-26 kT/(2 Ryd) n exp(-(xion - dxi)/kT) / U */
+#define M3D_BF_PAIR 5      /* 'H+H', 'H+HE', 'H2+H', 'H2+H2', 'H2+HE': n n2 */
+#define M3D_BF_H2PLUS 6    /* 'H2+': 1e-40 n n2 */
+#define M3D_BF_PEDEP 7     /* a Pe-dependent table: n Pe */
+#define M3D_BF_PEACH 8     /* a Pe-dependent Peach table: 1e-40/e e_kT n Pe */
+#define M3D_BF_MOLECULAR 9 /* n awgt / N_A, the mass density */
+#define M3D_BF_REGULAR 10  /* a level's bound-free: g exp(-xion/kT) n / U */
+
+/* One absdat component (bftrans_type).  Tables are host memory: lam (nnu) [AA],
+ * lnlam (nnu, with loglam), tt (ntt) the temperature nodes (T [K], or 5040/T with
+ * iteta), xkap (nnu x ntt, wavelength fastest) as set_table stores it (divided by
+ * xkap_scale, logarithmic when log_table), ldisk (nnu).  The per-cell arrays (ncell,
+ * float64) follow the call's flags: n the particle's number density [cm^-3]; n2 the
+ * second particle's (pairs, H2+); part the particle's ln partition function (H FF,
+ * regular); level_n the population of H I level k (M3D_BF_H). */
+typedef struct m3d_bf_comp {
+  int kind, istim, nnu, ntt;
+  int ilogl, kvadl, minex, maxex, loglam;
+  int kvadt, minet, maxet, iteta, lam3, log_table;
+  int k;
+  const double *lam, *lnlam, *tt;
+  const float *xkap;
+  const unsigned char *ldisk;
+  double xkap_scale, mint, maxt, minl, maxl;
+  double ion_xion, level_g, level_xion, awgt;
+  const double *n, *n2, *part, *level_n;
+} m3d_bf_comp_t;
+
+/* The EOS state of the cells (ncell, float64, per the call's flags): temp [K], teta
+ * = 5040/T, e_kT = 1 eV/kT, pe [dyn cm^-2], dxi the ionisation-energy lowering [eV],
+ * ne [cm^-3]; H I's number density and ln partition function (the H rest; NULL: no
+ * H rest, no H I Rayleigh), He I and H2 densities (Rayleigh; may be NULL), H I's
+ * ionisation energy [eV], and helium_scattering (the reference's switch, default on). */
+typedef struct m3d_cont_cells {
+  const double *temp, *teta, *e_kT, *pe, *dxi, *ne;
+  const double *nHI, *partHI, *nHeI, *nH2;
+  double HI_xion;
+  int helium_scattering, pad;
+} m3d_cont_cells_t;
+
+/* xhat (nlam, ncell) = the continuum's true absorption in the working form (the
+ * components in order; those with istim summed apart and divided by 1 - beta);
+ * sigma (nlam, ncell, may be NULL) = electron + Rayleigh scattering [1/cm].  lam and
+ * nu (nlam, host) are the window's wavelengths [AA] and frequencies [Hz]; beta
+ * (nlam, ncell) or NULL, then boltzmann_factor from nu.  An 'H BF' component with
+ * occupation probabilities (wcalc2) is the EOS's and not accepted (M3D_EINVAL for
+ * an unknown kind). */
+int m3d_continuum_opacities(int ncomp, const m3d_bf_comp_t *comps, int nlam, const double *lam, const double *nu,
+                            int ncell, const m3d_cont_cells_t *cells, const float *beta, float *xhat, float *sigma,
+                            unsigned flags);
+
 /* ---- statistical equilibrium (FP64) ----
  * Level and transition indices are 0-based (the reference's minus one).  Per-cell
  * arrays keep the cell index fastest: b(cell, level) at b[cell + ncell*level], as

@@ -1,0 +1,145 @@
+"""The continuum-opacity oracle (oracle/or_continuum.c) against what the reference
+states and against independent restatements:
+
+* load_lam_interp_weights' stencils bracket each wavelength, the weights sum to one,
+  and wavelengths outside a table that may not be extrapolated get none;
+* a table constant in wavelength and temperature is reproduced, one linear in
+  wavelength too, to the rounding of the real(4) weights, in every interpolation form;
+* set_table's stored form (dispatch_b200.continuum.set_table) against its formula;
+* the Thomson constant against const_mod's sigma_th, electron and Rayleigh
+  scattering and the H rest against direct numpy forms;
+* components tabulated with stimulated emission end up divided by 1 - beta.
+"""
+import numpy as np
+import pytest
+
+from dispatch_b200 import synth
+from dispatch_b200.continuum import HMINUS, set_table
+
+
+@pytest.fixture(scope="module")
+def oc(oracle):
+    from oracle import continuum
+    return continuum
+
+
+def _flat(value, lam_lo, lam_hi, nnu=12, tnodes=(4000.0, 7000.0, 10000.0), **kw):
+    tl = np.geomspace(lam_lo, lam_hi, nnu)
+    raw = np.full((len(tnodes), nnu), value)
+    xk, scale, logt = set_table(raw, kw.pop("ilogt", False), kw.get("ilogl", False))
+    c = {"kind": HMINUS, "lam": tl, "tt": np.asarray(tnodes), "xkap": xk, "xkap_scale": scale, "log_table": logt,
+         "minl": tl[0], "maxl": tl[-1], "mint": 0.0, "maxt": 1e9}
+    c.update(kw)
+    return c
+
+
+def _cells(ncell=40, seed=1):
+    rng = np.random.default_rng(seed)
+    t = rng.uniform(3000.0, 11000.0, ncell)
+    ne = 10.0 ** rng.uniform(10, 14, ncell)
+    return {"temp": t, "teta": 5040.0 / t, "e_kT": synth.EE / (synth.BK * t), "pe": ne * synth.BK * t,
+            "dxi": np.zeros(ncell), "ne": ne, "helium_scattering": True}
+
+
+def test_weights_bracket_and_sum(oc):
+    comps, lam, nu, cells = synth.continuum_case(ncell=8, nlam=300, lam_range=(2000.0, 20000.0))
+    for c in comps:
+        act, iw, quad, lag, fs, fe = oc.bf_weights(c, lam)
+        tl = c["lam"]
+        inside = (lam >= tl[0]) & (lam <= tl[-1])
+        allowed = inside | ((lam > tl[-1]) & bool(c.get("maxex"))) | ((lam < tl[0]) & bool(c.get("minex")))
+        assert act == bool(allowed.any())
+        assert np.array_equal(iw >= 0, allowed)
+        if not act:
+            continue
+        idx = np.flatnonzero(allowed)
+        assert fs == idx[0] and fe == idx[-1]
+        for f in idx:
+            w = lag[f, :3 if quad[f] else 2].astype(np.float64)
+            assert w.sum() == pytest.approx(1.0, abs=2e-7 * np.abs(w).sum())   # real(4) weights
+            if inside[f] and not quad[f]:
+                j = iw[f]
+                assert tl[j] <= lam[f] <= tl[j + 1]
+            if quad[f]:
+                assert not c["ldisk"][iw[f]]
+
+
+def test_constant_table_reproduced(oc):
+    cells = _cells()
+    lam = np.geomspace(4000.0, 9000.0, 50)
+    n = 10.0 ** np.random.default_rng(2).uniform(8, 11, 40)
+    forms = ({}, {"kvadt": True}, {"kvadl": True}, {"ilogt": True}, {"ilogl": True}, {"ilogl": True, "ilogt": True})
+    for kw in forms:
+        c = _flat(3e-17, 3000.0, 10000.0, n=n, **kw)
+        xhat, _ = oc.continuum_opacities([c], lam, None, cells, sigma=False)
+        want = (n * c["xkap_scale"]).astype(np.float32)
+        # the stored table is 1 (or ln 1 = 0) everywhere: the interpolation returns it,
+        # to the rounding of its real(4) weights, whose sum is 1 only to an ulp or two
+        np.testing.assert_allclose(xhat, np.repeat(want[:, None], lam.size, axis=1), rtol=4e-7, err_msg=str(kw))
+
+
+def test_linear_table_to_rounding(oc):
+    cells = _cells()
+    lam = np.geomspace(4100.0, 8900.0, 77)
+    tl = np.linspace(4000.0, 9000.0, 21)
+    raw = np.tile(1.0 + (tl - 4000.0) / 5000.0, (3, 1))
+    xk, scale, logt = set_table(raw, False, False)
+    c = {"kind": HMINUS, "lam": tl, "tt": np.array([4000.0, 7000.0, 10000.0]), "xkap": xk, "xkap_scale": scale,
+         "log_table": logt, "minl": tl[0], "maxl": tl[-1], "mint": 0.0, "maxt": 1e9, "kvadl": True,
+         "n": np.ones(40)}
+    xhat, _ = oc.continuum_opacities([c], lam, None, cells, sigma=False)
+    np.testing.assert_allclose(xhat, np.tile(1.0 + (lam - 4000.0) / 5000.0, (40, 1)), rtol=2e-6)
+
+
+def test_set_table_form():
+    raw = np.array([[1e-30, 2e-30, 0.0], [4e-30, 8e-30, 1e-30]])
+    xk, scale, logt = set_table(raw, True, False)
+    assert logt and scale == 8e-30
+    np.testing.assert_array_equal(xk, (np.log(np.where(raw > 0, raw, 1e-37)) - np.log(8e-30)).astype(np.float32))
+    xk, scale, logt = set_table(raw[:1], True, False)   # no temperature dependence: ilogl decides
+    assert not logt and scale == 2e-30
+    np.testing.assert_array_equal(xk, (raw[:1] / 2e-30).astype(np.float32))
+
+
+def test_scattering_and_hrest(oc):
+    cells = _cells()
+    cells.update(nHI=10.0 ** np.linspace(14, 17, 40), partHI=np.full(40, np.log(2.0)), nHeI=np.full(40, 1e15),
+                 nH2=np.full(40, 1e10), HI_xion=13.598434, dxi=np.linspace(0, 0.05, 40))
+    lam = np.concatenate([np.geomspace(1000.0, 1399.0, 20), np.geomspace(1401.0, 12000.0, 60)])
+    xhat, sg = oc.continuum_opacities([], lam, None, cells)
+    # Thomson: const_mod's sigma_th = 8/3 pi e^4/(m^2 c^4) = 6.6524e-25 cm^2
+    thomson = float(8.0 / 3.0 * 3.14159265359) * (4.80325e-10**2 / (9.109534e-28 * 2.99792458e10**2))**2
+    assert thomson == pytest.approx(6.6524e-25, rel=1e-4)
+    xr = np.where(lam > 1400.0, 1.0 / np.maximum(1026.0, lam) ** 2, 0.0)
+    rayh = (5.799e-13 + xr * (1.422e-6 + xr * 2.784))[None, :] * cells["nHI"][:, None]
+    rayh2 = (8.14e-13 + xr * (1.28e-6 + xr * 1.61))[None, :] * 1e10
+    he = 0.66520e-24 * 4.0 * (500.0 / lam) ** 4
+    want = thomson * cells["ne"][:, None] + (rayh + rayh2) * xr**2 + he[None, :] * 1e15
+    np.testing.assert_allclose(sg, want, rtol=3e-7)
+    # the H rest: the hydrogenic levels above n = 15 up to the lowered limit
+    ekt, dxi = cells["e_kT"], cells["dxi"]
+    fakt = np.exp(-ekt * (13.598434 - dxi) - np.log(2.0)) * 2.0898e-26 / (2 * 13.598434 * ekt) * cells["nHI"]
+    hr = fakt * (np.exp(ekt * (13.598434 / 240.25 - dxi)) - 1)
+    hr = np.where(13.598434 >= 240.25 * dxi, hr, 0.0)
+    np.testing.assert_allclose(xhat, hr[:, None] * lam[None, :] ** 3, rtol=3e-7)
+
+
+def test_stimulated_components_over_one_minus_beta(oc):
+    comps, lam, nu, cells = synth.continuum_case(ncell=30, nlam=40)
+    cells = {k: v for k, v in cells.items() if k not in ("nHI", "partHI")}   # no H rest: the component alone
+    c = dict(comps[0])
+    beta = np.random.default_rng(4).uniform(1e-6, 0.7, (30, 40)).astype(np.float32)
+    plain, _ = oc.continuum_opacities([c], lam, nu, cells, sigma=False)
+    c["istim"] = True
+    stim, _ = oc.continuum_opacities([c], lam, nu, cells, beta=beta, sigma=False)
+    np.testing.assert_array_equal(stim, plain / (np.float32(1.0) - beta))
+
+
+def test_full_case_finite(oc):
+    comps, lam, nu, cells = synth.continuum_case(ncell=200, nlam=128)
+    xhat, sg = oc.continuum_opacities(comps, lam, nu, cells)
+    assert np.all(np.isfinite(xhat)) and np.all(xhat > 0) and np.all(sg > 0)
+    # each kind contributes somewhere
+    for k, c in enumerate(comps):
+        x1, _ = oc.continuum_opacities([c], lam, nu, cells, sigma=False)
+        assert x1.max() > 0, k
