@@ -49,10 +49,11 @@ def _args():
     p.add_argument("--no-c4", action="store_true", help="skip the differentiable (adjoint) measurement")
     p.add_argument("--cube", type=int, default=240, help="cube edge (240 = the configuration; smaller for profiling)")
     # single cases for timing and profiling one kernel family (no JSON line)
-    p.add_argument("--case", default="c1", choices=["c1", "ali-window", "ali-columns", "optab", "c2", "batched"],
+    p.add_argument("--case", default="c1",
+                   choices=["c1", "ali-window", "ali-columns", "optab", "c2", "batched", "continuum"],
                    help="c1: the headline (default); the others run one seeded NLTE or table case and print "
                         "per-iteration times")
-    p.add_argument("--n", type=int, default=64, help="ali-window / optab: cube edge")
+    p.add_argument("--n", type=int, default=64, help="ali-window / optab / continuum: cube edge")
     p.add_argument("--ncol", type=int, default=1024, help="ali-columns: columns")
     p.add_argument("--nbound", type=int, default=20, help="ali-*: bound levels of the model atom")
     p.add_argument("--nline", type=int, default=60, help="ali-*: bound-bound transitions of the model atom")
@@ -409,6 +410,58 @@ def _nlte_batched(steps=2):
     del plans
     torch.cuda.empty_cache()
     return out
+
+
+def _continuum(steps=5, warmup=3, n=120):
+    """The continuum opacity of one window (HOP's continuum_opacities): the 120^3
+    cube's 1.73 M cells, 250 frequencies in 3500-12000 A, twelve absdat-like
+    components of every kind (synth.continuum_case), the H rest, electron and
+    Rayleigh scattering; inputs resident on the device, CUDA events on torch's
+    stream.  Beside it the C restatement on one core over 2000 cells of the same
+    case."""
+    import torch
+
+    from dispatch_b200 import synth
+    from dispatch_b200.continuum import continuum_opacities
+    ncell, nlam = n**3, 250
+    comps, lam, nu, cells = synth.continuum_case(ncell=ncell, nlam=nlam)
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    dc = {k: (dev(v) if isinstance(v, np.ndarray) else v) for k, v in cells.items()}
+    dcomps = [{k: (dev(v) if k in ("n", "n2", "part", "level_n") else v) for k, v in c.items()} for c in comps]
+    cur = torch.cuda.current_stream()
+    for _ in range(warmup):
+        continuum_opacities(dcomps, lam, nu, dc)
+    ts = []
+    for _ in range(steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(cur)
+        xh, sg = continuum_opacities(dcomps, lam, nu, dc)
+        e1.record(cur)
+        torch.cuda.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    ms = float(np.median(ts))
+    # algorithmic bytes: xhat and sigma written, the cells' EOS state and densities read
+    ncarr = 10 + sum(sum(1 for k in ("n", "n2", "part", "level_n") if c.get(k) is not None) for c in comps)
+    nbytes = 8.0 * nlam * ncell + 8.0 * ncarr * ncell
+    peaks = _peaks() or {}
+    peak = peaks.get("hbm_gbs", 6650.0)
+    from oracle import continuum as oc
+    sub = 2000
+    sc = {k: (v[:sub] if isinstance(v, np.ndarray) else v) for k, v in cells.items()}
+    scomps = [{k: (v[:sub] if k in ("n", "n2", "part", "level_n") else v) for k, v in c.items()} for c in comps]
+    t0 = time.perf_counter()
+    oc.continuum_opacities(scomps, lam, nu, sc)
+    dt = time.perf_counter() - t0
+    del xh, sg, dc, dcomps
+    torch.cuda.empty_cache()
+    return {"workload": f"continuum opacity of one window: {ncell / 1e6:.2f} M cells ({n}^3), {nlam} frequencies "
+                        "3500-12000 A, 12 absdat-like components of every kind, H rest, electron + Rayleigh scattering",
+            "unit": "Gpt*nu/s", "ms": ms, "value": ncell * nlam / (ms / 1e3) / 1e9,
+            "achieved_gbs": nbytes / (ms / 1e3) / 1e9, "peak_gbs": peak, "frac": nbytes / (ms / 1e3) / 1e9 / peak,
+            "cpu_baseline": {"value": sub * nlam / dt / 1e9, "unit": "Gpt*nu/s", "cores": 1, "kind": "port",
+                             "sample": f"{sub} cells of the same case, the C restatement on one core, {dt:.2f} s"},
+            "data": "synthetic (seeded EOS state and tables)"}
 
 
 def _optab(steps=5, warmup=3):
@@ -776,12 +829,13 @@ def run_b200(a):
                 "path": "FP64 end to end: line opacity and QLG-bot (fp64 tables, exp, log), transfer units, "
                         "rotate_array and long_char_quadratic, one launch per ray and slab"}
 
-    nlte = batched = optab = None
+    nlte = batched = optab = continuum = None
     if rank == 0 and not a.no_ali:
         nlte = _nlte_ali()
         batched = _nlte_batched()
     if rank == 0 and not a.no_optab:
         optab = _optab()
+        continuum = _continuum()
 
     c0 = c4 = None
     if rank == 0 and not a.no_c0:
@@ -813,7 +867,7 @@ def run_b200(a):
             "config": {**_workload(nf, a.cube), "windows_timed_rank0": wins[a.warmup:]},
             "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline, "roofline_sweep": roofline_sweep,
             "cpu_baseline": cpu, "clocks": clocks, "stages": stages, "fp64_plain": fp64, "c0_1d": c0, "c4_adjoint": c4,
-            "nlte_ali": nlte, "nlte_batched": batched, "optab": optab}
+            "nlte_ali": nlte, "nlte_batched": batched, "optab": optab, "continuum": continuum}
     print(json.dumps(line), flush=True)
 
 
@@ -959,6 +1013,10 @@ def main():
         import dispatch_b200 as m
         m.init(0)
         print(json.dumps(_c2_full(a.iters if a.iters != 2 else 30)), flush=True)
+    elif a.case == "continuum":
+        import dispatch_b200 as m
+        m.init(0)
+        print(json.dumps(_continuum(n=a.n)), flush=True)
     elif a.case == "batched":
         import dispatch_b200 as m
         m.init(0)

@@ -20,9 +20,15 @@ namespace m3d {
 
 constexpr int kContWarps = 4;     // warps (cells) per block
 constexpr int kContMaxComp = 64;  // components of one call
+constexpr int kContMaxRows = 1024;  // table rows a window reads, over all components (per cell, in shared memory)
+constexpr int kContMaxTab = 8192;   // their table entries at every temperature node (per block, in shared memory)
 
 struct BfCompDev {
-  int kind, istim, nnu, ntt, ilogl, lam3, log_table, kvadt, minet, maxet, iteta, k, fs, fe, active, pad;
+  int kind, istim, nnu, ntt, ilogl, lam3, log_table, kvadt, minet, maxet, iteta, k, fs, fe, active;
+  // the table rows the window's stencils read (0-based r0 .. r0 + nrow - 1), their
+  // place in the cell's shared row buffer and that of their entries at every
+  // temperature node in the block's shared table (-1: read from global memory)
+  int r0, nrow, soff, toff;
   double xkap_scale, mint, maxt, ion_xion, level_g, level_xion, awgt;
   const double *tt;
   const float *xkap;      // (nnu, ntt)
@@ -144,9 +150,32 @@ __device__ __forceinline__ float cont_row(const BfCompDev &c, const BfCellDev &r
   return y;
 }
 
+// the same row from the block's staged table: entry (row, node) at
+// stab[toff + node nrow + row - r0]
+__device__ __forceinline__ float cont_row_s(const BfCompDev &c, const BfCellDev &r, const float *stab, int j) {
+  const float *tab = stab + c.toff + (j - 1 - c.r0);
+  const size_t nr = (size_t)c.nrow;
+  float y;
+  if (r.quadratic) {
+    const size_t i = (size_t)r.it;
+    y = __fadd_rn(__fadd_rn(__fmul_rn(tab[nr * (i - 1)], r.w0), __fmul_rn(tab[nr * i], r.w1)),
+                  __fmul_rn(tab[nr * (i + 1)], r.w2));
+  } else {
+    const size_t it = (size_t)r.it;
+    const float a = tab[nr * (it - 1)], b = tab[nr * it];
+    y = __fadd_rn(__fmul_rn(__fsub_rn(b, a), r.w0), a);
+    if (r.edge == 1) y = fminf(y, tab[0]);
+    else if (r.edge == 2) y = fminf(y, tab[nr * (c.ntt - 1)]);
+  }
+  if (c.log_table && !c.ilogl) y = exp4(y);
+  else if (c.ilogl && !c.log_table) y = logf(fmaxf(y, FLT_MIN));
+  return y;
+}
+
 // one component's contribution at wavelength f of the cell (interp_xkap :358-385 and
 // :386-426): returns false where it adds nothing
-__device__ __forceinline__ bool cont_comp(const BfCompDev &c, const BfCellDev &r, int f, double lam, float &add) {
+__device__ __forceinline__ bool cont_comp(const BfCompDev &c, const BfCellDev &r, const float *rows, int f, double lam,
+                                          float &add) {
   if (!c.active || f < c.fs || f > c.fe) return false;
   const int iw = c.iw[f];
   float ab;
@@ -154,8 +183,17 @@ __device__ __forceinline__ bool cont_comp(const BfCompDev &c, const BfCellDev &r
     if (!r.in_bounds) return false;
     if (iw >= 0) {
       const int i = iw + 1;
-      const float y1 = cont_row(c, r, i), y2 = cont_row(c, r, i + 1);
-      const float y3 = cont_row(c, r, i + 2 < c.nnu ? i + 2 : c.nnu);
+      float y1, y2, y3;
+      if (c.soff >= 0) {
+        const float *yy = rows + c.soff - c.r0;   // yy[row], 0-based table rows
+        y1 = yy[iw];
+        y2 = yy[iw + 1];
+        y3 = yy[i + 2 < c.nnu ? iw + 2 : c.nnu - 1];
+      } else {
+        y1 = cont_row(c, r, i);
+        y2 = cont_row(c, r, i + 1);
+        y3 = cont_row(c, r, i + 2 < c.nnu ? i + 2 : c.nnu);
+      }
       const float *L = c.lag + 3 * (size_t)f;
       ab = __fadd_rn(__fadd_rn(__fmul_rn(y1, L[0]), __fmul_rn(y2, L[1])), __fmul_rn(y3, L[2]));
     } else {
@@ -184,10 +222,24 @@ __device__ __forceinline__ bool cont_comp(const BfCompDev &c, const BfCellDev &r
 __global__ void __launch_bounds__(kContWarps * 32)
 k_continuum(int ncomp, const BfCompDev *__restrict__ comps, int any_istim, int nlam, const double *__restrict__ lam,
             const double *__restrict__ nu, int ncell, ContCellsDev S, const float *__restrict__ beta,
-            float *__restrict__ xhat, float *__restrict__ sigma) {
+            float *__restrict__ xhat, float *__restrict__ sigma, int rows_used, int tab_used) {
   __shared__ BfCellDev sc[kContWarps][kContMaxComp];
+  extern __shared__ float cont_dyn[];
+  float *stab = cont_dyn;                                        // (tab_used) the staged table entries
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   BfCellDev *st = sc[wib];
+  float *rows = cont_dyn + tab_used + (size_t)wib * rows_used;   // (rows_used) this cell's rows
+  // the window's table rows at every temperature node, once per block
+  for (int j = 0; j < ncomp; j++) {
+    const BfCompDev &c = comps[j];
+    if (c.toff < 0) continue;
+    const int m = c.nrow * c.ntt;
+    for (int q = threadIdx.x; q < m; q += blockDim.x) {
+      const int node = q / c.nrow, row = q - node * c.nrow;
+      stab[c.toff + q] = c.xkap[(size_t)(c.r0 + row) + (size_t)c.nnu * node];
+    }
+  }
+  __syncthreads();
   const int nwarp = gridDim.x * kContWarps;
   // thomson = 8./3.*PI*(EC**2/(EM*CC**2))**2 (composition_mod.f90:3856), a real(8)
   // parameter whose 8./3. is a default-real quotient
@@ -209,6 +261,13 @@ k_continuum(int ncomp, const BfCompDev *__restrict__ comps, int any_istim, int n
       }
       r.fakt1 = (c.active && r.in_bounds) ? cont_factor(c, S, x) : 0.0f;
       st[j] = r;
+    }
+    __syncwarp();
+    // the table rows at the cell's temperature, each formed once (interp_xkap's yy)
+    for (int j = 0; j < ncomp; j++) {
+      const BfCompDev &c = comps[j];
+      if (c.soff < 0 || !c.active || !st[j].in_bounds) continue;
+      for (int q = lane; q < c.nrow; q += 32) rows[c.soff + q] = cont_row_s(c, st[j], stab, c.r0 + q + 1);
     }
     __syncwarp();
     // add_hrest: the H I levels above n = 15, up to the lowered ionisation limit
@@ -235,7 +294,7 @@ k_continuum(int ncomp, const BfCompDev *__restrict__ comps, int any_istim, int n
         const BfCompDev &c = comps[j];
         if (c.istim) continue;
         float add;
-        if (cont_comp(c, st[j], f, l, add)) v = __fadd_rn(v, add);
+        if (cont_comp(c, st[j], rows, f, l, add)) v = __fadd_rn(v, add);
       }
       if (any_istim) {
         float tmp = 0.0f;
@@ -243,7 +302,7 @@ k_continuum(int ncomp, const BfCompDev *__restrict__ comps, int any_istim, int n
           const BfCompDev &c = comps[j];
           if (!c.istim) continue;
           float add;
-          if (cont_comp(c, st[j], f, l, add)) tmp = __fadd_rn(tmp, add);
+          if (cont_comp(c, st[j], rows, f, l, add)) tmp = __fadd_rn(tmp, add);
         }
         float b;
         if (beta) {
