@@ -22,6 +22,7 @@ constexpr int kContWarps = 4;     // warps (cells) per block
 constexpr int kContMaxComp = 64;  // components of one call
 constexpr int kContMaxRows = 1024;  // table rows a window reads, over all components (per cell, in shared memory)
 constexpr int kContMaxTab = 8192;   // their table entries at every temperature node (per block, in shared memory)
+constexpr int kContKF = 8;          // wavelengths a lane holds in one pass over the components
 
 struct BfCompDev {
   int kind, istim, nnu, ntt, ilogl, lam3, log_table, kvadt, minet, maxet, iteta, k, fs, fe, active;
@@ -32,9 +33,10 @@ struct BfCompDev {
   double xkap_scale, mint, maxt, ion_xion, level_g, level_xion, awgt;
   const double *tt;
   const float *xkap;      // (nnu, ntt)
-  const int *iw;          // (nlam) first stencil node, 0-based; -1 where none
+  // (nlam) the wavelength stencil: the first node, 0-based (-1 where none), as int
+  // bits in x, and the three Lagrange weights in y, z, w
+  const float4 *wt;
   const unsigned char *quad;
-  const float *lag;       // (3, nlam)
   const double *n, *n2, *part, *level_n;
 };
 
@@ -172,51 +174,71 @@ __device__ __forceinline__ float cont_row_s(const BfCompDev &c, const BfCellDev 
   return y;
 }
 
-// one component's contribution at wavelength f of the cell (interp_xkap :358-385 and
-// :386-426): returns false where it adds nothing
-__device__ __forceinline__ bool cont_comp(const BfCompDev &c, const BfCellDev &r, const float *rows, int f, double lam,
-                                          float &add) {
-  if (!c.active || f < c.fs || f > c.fe) return false;
-  const int iw = c.iw[f];
-  float ab;
+// one component's contributions at the lane's wavelengths f0 + 32 k (interp_xkap
+// :358-385 and :386-426), each added to v[k] where the component reaches f; l3[k]
+// is real(lambda^3) there.  The component's fields are read once for all of them.
+template <int KF>
+__device__ __forceinline__ void cont_comp(const BfCompDev &c, const BfCellDev &r, const float *rows, int f0,
+                                          const float (&l3)[KF], float (&v)[KF]) {
+  if (!c.active) return;
+  const int fs = c.fs, fe = c.fe, nnu = c.nnu, ilogl = c.ilogl, lam3 = c.lam3;
+  const float4 *wt = c.wt;
   if (c.ntt > 1) {
-    if (!r.in_bounds) return false;
-    if (iw >= 0) {
-      const int i = iw + 1;
-      float y1, y2, y3;
-      if (c.soff >= 0) {
-        const float *yy = rows + c.soff - c.r0;   // yy[row], 0-based table rows
-        y1 = yy[iw];
-        y2 = yy[iw + 1];
-        y3 = yy[i + 2 < c.nnu ? iw + 2 : c.nnu - 1];
+    if (!r.in_bounds) return;
+    const float fakt1 = r.fakt1;
+    const int soff = c.soff;
+    const float *yy = rows + soff - c.r0;   // yy[row], 0-based table rows
+#pragma unroll
+    for (int k = 0; k < KF; k++) {
+      const int f = f0 + 32 * k;
+      if (f < fs || f > fe) continue;
+      const float4 w = __ldg(wt + f);
+      const int iw = __float_as_int(w.x);
+      float ab;
+      if (iw >= 0) {
+        float y1, y2, y3;
+        if (soff >= 0) {
+          y1 = yy[iw];
+          y2 = yy[iw + 1];
+          y3 = yy[iw + 3 < nnu ? iw + 2 : nnu - 1];
+        } else {
+          const int i = iw + 1;
+          y1 = cont_row(c, r, i);
+          y2 = cont_row(c, r, i + 1);
+          y3 = cont_row(c, r, i + 2 < nnu ? i + 2 : nnu);
+        }
+        ab = __fadd_rn(__fadd_rn(__fmul_rn(y1, w.y), __fmul_rn(y2, w.z)), __fmul_rn(y3, w.w));
       } else {
-        y1 = cont_row(c, r, i);
-        y2 = cont_row(c, r, i + 1);
-        y3 = cont_row(c, r, i + 2 < c.nnu ? i + 2 : c.nnu);
+        ab = ilogl ? -FLT_MAX : 0.0f;
       }
-      const float *L = c.lag + 3 * (size_t)f;
-      ab = __fadd_rn(__fadd_rn(__fmul_rn(y1, L[0]), __fmul_rn(y2, L[1])), __fmul_rn(y3, L[2]));
-    } else {
-      ab = c.ilogl ? -FLT_MAX : 0.0f;
+      if (ilogl) ab = exp4(ab);
+      if (lam3) ab = __fmul_rn(ab, l3[k]);
+      v[k] = __fadd_rn(v[k], __fmul_rn(fakt1, ab));
     }
-    if (c.ilogl) ab = exp4(ab);
-    if (c.lam3) ab = __fmul_rn(ab, (float)(lam * lam * lam));
-    add = __fmul_rn(r.fakt1, ab);
   } else {
-    if (iw < 0) {
-      ab = 0.0f;
-    } else {
-      const float *yy = c.xkap + iw;
-      const float *L = c.lag + 3 * (size_t)f;
-      ab = __fadd_rn(0.0f, __fmul_rn(yy[0], L[0]));
-      ab = __fadd_rn(ab, __fmul_rn(yy[1], L[1]));
-      if (c.quad[f]) ab = __fadd_rn(ab, __fmul_rn(yy[2], L[2]));
-      if (c.ilogl) ab = expf(ab);
+    const float fakt1 = r.fakt1;
+    const float *xk = c.xkap;
+    const unsigned char *quad = c.quad;
+#pragma unroll
+    for (int k = 0; k < KF; k++) {
+      const int f = f0 + 32 * k;
+      if (f < fs || f > fe) continue;
+      const float4 w = __ldg(wt + f);
+      const int iw = __float_as_int(w.x);
+      float ab;
+      if (iw < 0) {
+        ab = 0.0f;
+      } else {
+        const float *yy = xk + iw;
+        ab = __fadd_rn(0.0f, __fmul_rn(yy[0], w.y));
+        ab = __fadd_rn(ab, __fmul_rn(yy[1], w.z));
+        if (quad[f]) ab = __fadd_rn(ab, __fmul_rn(yy[2], w.w));
+        if (ilogl) ab = expf(ab);
+      }
+      if (lam3) ab = __fmul_rn(ab, l3[k]);
+      v[k] = __fadd_rn(v[k], __fmul_rn(ab, fakt1));
     }
-    if (c.lam3) ab = __fmul_rn(ab, (float)(lam * lam * lam));
-    add = __fmul_rn(ab, r.fakt1);
   }
-  return true;
 }
 
 __global__ void __launch_bounds__(kContWarps * 32)
@@ -285,54 +307,69 @@ k_continuum(int ncomp, const BfCompDev *__restrict__ comps, int any_istim, int n
     const double hk_T = (6.626176e-27 / 1.380662e-16) / temp;
     const double nHIr = S.nHI ? S.nHI[x] : 0.0, nHE = S.nHeI ? S.nHeI[x] : 0.0, nH2 = S.nH2 ? S.nH2[x] : 0.0;
     const double els = sigma ? thomson * S.ne[x] : 0.0;
-    for (int f = lane; f < nlam; f += 32) {
-      const double l = lam[f];
-      const size_t o = (size_t)f + (size_t)nlam * x;
-      float v = 0.0f;
-      if (hrest_on) v = (float)((double)v + hrest * (l * l * l));
+    for (int f0 = lane; f0 - lane < nlam; f0 += 32 * kContKF) {
+      float v[kContKF], l3[kContKF];
+#pragma unroll
+      for (int k = 0; k < kContKF; k++) {
+        const int f = f0 + 32 * k;
+        const double l = f < nlam ? lam[f] : 0.0;
+        const double cube = l * l * l;
+        l3[k] = (float)cube;
+        v[k] = hrest_on ? (float)((double)0.0f + hrest * cube) : 0.0f;
+      }
       for (int j = 0; j < ncomp; j++) {
         const BfCompDev &c = comps[j];
-        if (c.istim) continue;
-        float add;
-        if (cont_comp(c, st[j], rows, f, l, add)) v = __fadd_rn(v, add);
+        if (!c.istim) cont_comp<kContKF>(c, st[j], rows, f0, l3, v);
       }
       if (any_istim) {
-        float tmp = 0.0f;
+        float tmp[kContKF];
+#pragma unroll
+        for (int k = 0; k < kContKF; k++) tmp[k] = 0.0f;
         for (int j = 0; j < ncomp; j++) {
           const BfCompDev &c = comps[j];
-          if (!c.istim) continue;
-          float add;
-          if (cont_comp(c, st[j], rows, f, l, add)) tmp = __fadd_rn(tmp, add);
+          if (c.istim) cont_comp<kContKF>(c, st[j], rows, f0, l3, tmp);
         }
-        float b;
-        if (beta) {
-          b = beta[o];
-        } else {
-          b = (float)exp(-nu[f] * hk_T);
-          b = b > FLT_MIN ? b : FLT_MIN;
+#pragma unroll
+        for (int k = 0; k < kContKF; k++) {
+          const int f = f0 + 32 * k;
+          if (f >= nlam) break;
+          float b;
+          if (beta) {
+            b = beta[(size_t)f + (size_t)nlam * x];
+          } else {
+            b = (float)exp(-nu[f] * hk_T);
+            b = b > FLT_MIN ? b : FLT_MIN;
+          }
+          v[k] = __fadd_rn(v[k], __fdiv_rn(tmp[k], __fsub_rn(1.0f, b)));
         }
-        v = __fadd_rn(v, __fdiv_rn(tmp, __fsub_rn(1.0f, b)));
       }
-      xhat[o] = v;
-      if (sigma) {
-        float s = (float)(0.0 + els);
-        double xr = 0.0;
-        if (l > 1400.0) {
-          const double m = l > 1026.0 ? l : 1026.0;
-          xr = 1 / (m * m);
+#pragma unroll
+      for (int k = 0; k < kContKF; k++) {
+        const int f = f0 + 32 * k;
+        if (f >= nlam) break;
+        const size_t o = (size_t)f + (size_t)nlam * x;
+        xhat[o] = v[k];
+        if (sigma) {
+          const double l = lam[f];
+          float s = (float)(0.0 + els);
+          double xr = 0.0;
+          if (l > 1400.0) {
+            const double m = l > 1026.0 ? l : 1026.0;
+            xr = 1 / (m * m);
+          }
+          if (xr > 0.) {
+            const double rayh = ((double)5.799e-13f + xr * ((double)1.422e-6f + xr * (double)2.784f)) * nHIr;
+            const double rayh2 = ((double)8.14e-13f + xr * ((double)1.28e-6f + xr * (double)1.61f)) * nH2;
+            s = (float)((double)s + (rayh + rayh2) * xr * xr);
+          }
+          double he = 0.0;
+          if (S.helium_scattering) {
+            const double q = (double)500.f / l;
+            const double q2 = q * q;
+            he = (double)(0.66520e-24f * 4.f) * (q2 * q2);
+          }
+          sigma[o] = (float)((double)s + he * nHE);
         }
-        if (xr > 0.) {
-          const double rayh = ((double)5.799e-13f + xr * ((double)1.422e-6f + xr * (double)2.784f)) * nHIr;
-          const double rayh2 = ((double)8.14e-13f + xr * ((double)1.28e-6f + xr * (double)1.61f)) * nH2;
-          s = (float)((double)s + (rayh + rayh2) * xr * xr);
-        }
-        double he = 0.0;
-        if (S.helium_scattering) {
-          const double q = (double)500.f / l;
-          const double q2 = q * q;
-          he = (double)(0.66520e-24f * 4.f) * (q2 * q2);
-        }
-        sigma[o] = (float)((double)s + he * nHE);
       }
     }
     __syncwarp();
