@@ -46,6 +46,16 @@ struct ContCellsDev {
   int helium_scattering;
 };
 
+// the wavelength terms every cell shares, formed once per call (k_continuum_lam)
+// with the operations the per-cell expressions use: lambda^3 in real(8) and its
+// real(4) rounding, rayleigh_scattering's xr and its two polynomials, the
+// helium term's (500/lambda)^4 times the cross section (0 without helium
+// scattering)
+struct ContLamDev {
+  const double *cube, *xr, *rayh, *rayh2, *he;
+  const float *l3;
+};
+
 // a component's state at one cell: the temperature stencil and the absorption factor
 struct BfCellDev {
   float w0, w1, w2, fakt1;
@@ -175,11 +185,11 @@ __device__ __forceinline__ float cont_row_s(const BfCompDev &c, const BfCellDev 
 }
 
 // one component's contributions at the lane's wavelengths f0 + 32 k (interp_xkap
-// :358-385 and :386-426), each added to v[k] where the component reaches f; l3[k]
-// is real(lambda^3) there.  The component's fields are read once for all of them.
+// :358-385 and :386-426), each added to v[k] where the component reaches f; l3[f]
+// is real(lambda^3).  The component's fields are read once for all of them.
 template <int KF>
 __device__ __forceinline__ void cont_comp(const BfCompDev &c, const BfCellDev &r, const float *rows, int f0,
-                                          const float (&l3)[KF], float (&v)[KF]) {
+                                          const float *__restrict__ l3, float (&v)[KF]) {
   if (!c.active) return;
   const int fs = c.fs, fe = c.fe, nnu = c.nnu, ilogl = c.ilogl, lam3 = c.lam3;
   const float4 *wt = c.wt;
@@ -212,7 +222,7 @@ __device__ __forceinline__ void cont_comp(const BfCompDev &c, const BfCellDev &r
         ab = ilogl ? -FLT_MAX : 0.0f;
       }
       if (ilogl) ab = exp4(ab);
-      if (lam3) ab = __fmul_rn(ab, l3[k]);
+      if (lam3) ab = __fmul_rn(ab, __ldg(l3 + f));
       v[k] = __fadd_rn(v[k], __fmul_rn(fakt1, ab));
     }
   } else {
@@ -235,14 +245,52 @@ __device__ __forceinline__ void cont_comp(const BfCompDev &c, const BfCellDev &r
         if (quad[f]) ab = __fadd_rn(ab, __fmul_rn(yy[2], w.w));
         if (ilogl) ab = expf(ab);
       }
-      if (lam3) ab = __fmul_rn(ab, l3[k]);
+      if (lam3) ab = __fmul_rn(ab, __ldg(l3 + f));
       v[k] = __fadd_rn(v[k], __fmul_rn(ab, fakt1));
     }
   }
 }
 
-__global__ void __launch_bounds__(kContWarps * 32)
-k_continuum(int ncomp, const BfCompDev *__restrict__ comps, int any_istim, int nlam, const double *__restrict__ lam,
+// thomson = 8./3.*PI*(EC**2/(EM*CC**2))**2 (composition_mod.f90:3856), a real(8)
+// parameter whose 8./3. is a default-real quotient
+__device__ __forceinline__ double cont_thomson() {
+  const double rq = (4.80325e-10 * 4.80325e-10) / (9.109534e-28 * (2.99792458e10 * 2.99792458e10));
+  return (double)(8.0f / 3.0f) * 3.14159265359 * (rq * rq);
+}
+
+// the shared wavelength terms: rayleigh_scattering's per-wavelength xray2 and HeIscat
+// (composition_mod.f90:3903-3911) and the H I and H2 polynomials in xr it forms per cell
+__global__ void k_continuum_lam(int nlam, const double *__restrict__ lam, int helium, double *__restrict__ cube,
+                                float *__restrict__ l3, double *__restrict__ xr_o, double *__restrict__ rayh_o,
+                                double *__restrict__ rayh2_o, double *__restrict__ he_o) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= nlam) return;
+  const double l = lam[f];
+  const double c3 = l * l * l;
+  cube[f] = c3;
+  l3[f] = (float)c3;
+  double xr = 0.0;
+  if (l > 1400.0) {
+    const double m = l > 1026.0 ? l : 1026.0;
+    xr = 1 / (m * m);
+  }
+  xr_o[f] = xr;
+  rayh_o[f] = (double)5.799e-13f + xr * ((double)1.422e-6f + xr * (double)2.784f);
+  rayh2_o[f] = (double)8.14e-13f + xr * ((double)1.28e-6f + xr * (double)1.61f);
+  double he = 0.0;
+  if (helium) {
+    const double q = (double)500.f / l;
+    const double q2 = q * q;
+    he = (double)(0.66520e-24f * 4.f) * (q2 * q2);
+  }
+  he_o[f] = he;
+}
+
+// eight blocks per SM (64 registers): the latency of the stencil loads is hidden by
+// occupancy, measured faster than 80 registers at six blocks and than 56 or 48 at
+// nine or ten
+__global__ void __launch_bounds__(kContWarps * 32, 8)
+k_continuum(int ncomp, const BfCompDev *__restrict__ comps, int any_istim, int nlam, ContLamDev LW,
             const double *__restrict__ nu, int ncell, ContCellsDev S, const float *__restrict__ beta,
             float *__restrict__ xhat, float *__restrict__ sigma, int rows_used, int tab_used) {
   __shared__ BfCellDev sc[kContWarps][kContMaxComp];
@@ -263,10 +311,7 @@ k_continuum(int ncomp, const BfCompDev *__restrict__ comps, int any_istim, int n
   }
   __syncthreads();
   const int nwarp = gridDim.x * kContWarps;
-  // thomson = 8./3.*PI*(EC**2/(EM*CC**2))**2 (composition_mod.f90:3856), a real(8)
-  // parameter whose 8./3. is a default-real quotient
-  const double rq = (4.80325e-10 * 4.80325e-10) / (9.109534e-28 * (2.99792458e10 * 2.99792458e10));
-  const double thomson = (double)(8.0f / 3.0f) * 3.14159265359 * (rq * rq);
+  const double thomson = cont_thomson();
   for (int x = blockIdx.x * kContWarps + wib; x < ncell; x += nwarp) {
     const double temp = S.temp[x], teta = S.teta[x];
     for (int j = lane; j < ncomp; j += 32) {
@@ -308,18 +353,15 @@ k_continuum(int ncomp, const BfCompDev *__restrict__ comps, int any_istim, int n
     const double nHIr = S.nHI ? S.nHI[x] : 0.0, nHE = S.nHeI ? S.nHeI[x] : 0.0, nH2 = S.nH2 ? S.nH2[x] : 0.0;
     const double els = sigma ? thomson * S.ne[x] : 0.0;
     for (int f0 = lane; f0 - lane < nlam; f0 += 32 * kContKF) {
-      float v[kContKF], l3[kContKF];
+      float v[kContKF];
 #pragma unroll
       for (int k = 0; k < kContKF; k++) {
         const int f = f0 + 32 * k;
-        const double l = f < nlam ? lam[f] : 0.0;
-        const double cube = l * l * l;
-        l3[k] = (float)cube;
-        v[k] = hrest_on ? (float)((double)0.0f + hrest * cube) : 0.0f;
+        v[k] = (hrest_on && f < nlam) ? (float)((double)0.0f + hrest * __ldg(LW.cube + f)) : 0.0f;
       }
       for (int j = 0; j < ncomp; j++) {
         const BfCompDev &c = comps[j];
-        if (!c.istim) cont_comp<kContKF>(c, st[j], rows, f0, l3, v);
+        if (!c.istim) cont_comp<kContKF>(c, st[j], rows, f0, LW.l3, v);
       }
       if (any_istim) {
         float tmp[kContKF];
@@ -327,7 +369,7 @@ k_continuum(int ncomp, const BfCompDev *__restrict__ comps, int any_istim, int n
         for (int k = 0; k < kContKF; k++) tmp[k] = 0.0f;
         for (int j = 0; j < ncomp; j++) {
           const BfCompDev &c = comps[j];
-          if (c.istim) cont_comp<kContKF>(c, st[j], rows, f0, l3, tmp);
+          if (c.istim) cont_comp<kContKF>(c, st[j], rows, f0, LW.l3, tmp);
         }
 #pragma unroll
         for (int k = 0; k < kContKF; k++) {
@@ -350,25 +392,14 @@ k_continuum(int ncomp, const BfCompDev *__restrict__ comps, int any_istim, int n
         const size_t o = (size_t)f + (size_t)nlam * x;
         xhat[o] = v[k];
         if (sigma) {
-          const double l = lam[f];
           float s = (float)(0.0 + els);
-          double xr = 0.0;
-          if (l > 1400.0) {
-            const double m = l > 1026.0 ? l : 1026.0;
-            xr = 1 / (m * m);
-          }
+          const double xr = __ldg(LW.xr + f);
           if (xr > 0.) {
-            const double rayh = ((double)5.799e-13f + xr * ((double)1.422e-6f + xr * (double)2.784f)) * nHIr;
-            const double rayh2 = ((double)8.14e-13f + xr * ((double)1.28e-6f + xr * (double)1.61f)) * nH2;
+            const double rayh = __ldg(LW.rayh + f) * nHIr;
+            const double rayh2 = __ldg(LW.rayh2 + f) * nH2;
             s = (float)((double)s + (rayh + rayh2) * xr * xr);
           }
-          double he = 0.0;
-          if (S.helium_scattering) {
-            const double q = (double)500.f / l;
-            const double q2 = q * q;
-            he = (double)(0.66520e-24f * 4.f) * (q2 * q2);
-          }
-          sigma[o] = (float)((double)s + he * nHE);
+          sigma[o] = (float)((double)s + __ldg(LW.he + f) * nHE);
         }
       }
     }
