@@ -24,7 +24,7 @@ constexpr int kContMaxRows = 1024;  // table rows a window reads, over all compo
 constexpr int kContMaxTab = 8192;   // their table entries at every temperature node (per block, in shared memory)
 constexpr int kContKF = 8;          // wavelengths a lane holds in one pass over the components
 
-struct BfCompDev {
+struct __align__(16) BfCompDev {
   int kind, istim, nnu, ntt, ilogl, lam3, log_table, kvadt, minet, maxet, iteta, k, fs, fe, active;
   // the table rows the window's stencils read (0-based r0 .. r0 + nrow - 1), their
   // place in the cell's shared row buffer and that of their entries at every
@@ -39,6 +39,8 @@ struct BfCompDev {
   const unsigned char *quad;
   const double *n, *n2, *part, *level_n;
 };
+
+static_assert(sizeof(BfCompDev) % 16 == 0, "descriptors staged in shared memory ahead of the tables");
 
 struct ContCellsDev {
   const double *temp, *teta, *e_kT, *pe, *dxi, *ne, *nHI, *partHI, *nHeI, *nH2;
@@ -290,15 +292,25 @@ __global__ void k_continuum_lam(int nlam, const double *__restrict__ lam, int he
 // occupancy, measured faster than 80 registers at six blocks and than 56 or 48 at
 // nine or ten
 __global__ void __launch_bounds__(kContWarps * 32, 8)
-k_continuum(int ncomp, const BfCompDev *__restrict__ comps, int any_istim, int nlam, ContLamDev LW,
+k_continuum(int ncomp, const BfCompDev *__restrict__ comps_g, int any_istim, int nlam, ContLamDev LW,
             const double *__restrict__ nu, int ncell, ContCellsDev S, const float *__restrict__ beta,
             float *__restrict__ xhat, float *__restrict__ sigma, int rows_used, int tab_used) {
   __shared__ BfCellDev sc[kContWarps][kContMaxComp];
-  extern __shared__ float cont_dyn[];
+  extern __shared__ __align__(16) float cont_sh[];
+  BfCompDev *scomp = reinterpret_cast<BfCompDev *>(cont_sh);   // (ncomp) the components' descriptors
+  float *cont_dyn = cont_sh + ncomp * (sizeof(BfCompDev) / sizeof(float));
   float *stab = cont_dyn;                                        // (tab_used) the staged table entries
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   BfCellDev *st = sc[wib];
   float *rows = cont_dyn + tab_used + (size_t)wib * rows_used;   // (rows_used) this cell's rows
+  {
+    const int nw = ncomp * (int)(sizeof(BfCompDev) / sizeof(int));
+    const int *src = reinterpret_cast<const int *>(comps_g);
+    int *dst = reinterpret_cast<int *>(scomp);
+    for (int q = threadIdx.x; q < nw; q += blockDim.x) dst[q] = src[q];
+  }
+  __syncthreads();
+  const BfCompDev *comps = scomp;
   // the window's table rows at every temperature node, once per block
   for (int j = 0; j < ncomp; j++) {
     const BfCompDev &c = comps[j];
