@@ -169,6 +169,9 @@ def _peaks():
 NCU_SWEEP_DRAM_BYTES_PER_CELL_FREQ = 8.013
 NCU_OPACITY_WARP_INST_PER_CELL_LINE = 751598136 / (110592 * 500)
 NCU_OPACITY_DRAM_READ_BYTES_PER_CELL = 5516032 / 110592
+#  k_continuum: warp instructions per cell of a launch of the continuum case (250
+#    frequencies, twelve components; 826,256,950 for 110,592 cells)
+NCU_CONTINUUM_WARP_INST_PER_CELL = 826256950 / 110592
 
 
 def _subcube(atm, n):
@@ -412,9 +415,9 @@ def _nlte_batched(steps=2):
     return out
 
 
-def _continuum(steps=5, warmup=3, n=120):
+def _continuum(steps=5, warmup=3, n=120, sm_mhz=None):
     """The continuum opacity of one window (HOP's continuum_opacities): the 120^3
-    cube's 1.73 M cells, 250 frequencies in 3500-12000 A, twelve absdat-like
+    cube's 1.73 M cells, 250 frequencies in 3500-12000 A, fourteen absdat-like
     components of every kind (synth.continuum_case), the H rest, electron and
     Rayleigh scattering; inputs resident on the device, CUDA events on torch's
     stream.  Beside it the C restatement on one core over 2000 cells of the same
@@ -427,7 +430,8 @@ def _continuum(steps=5, warmup=3, n=120):
     comps, lam, nu, cells = synth.continuum_case(ncell=ncell, nlam=nlam)
     dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
     dc = {k: (dev(v) if isinstance(v, np.ndarray) else v) for k, v in cells.items()}
-    dcomps = [{k: (dev(v) if k in ("n", "n2", "part", "level_n") else v) for k, v in c.items()} for c in comps]
+    dcomps = [{k: (dev(v) if k in ("n", "n2", "part", "level_n", "level_w") else v) for k, v in c.items()}
+              for c in comps]
     cur = torch.cuda.current_stream()
     for _ in range(warmup):
         continuum_opacities(dcomps, lam, nu, dc)
@@ -442,23 +446,35 @@ def _continuum(steps=5, warmup=3, n=120):
         ts.append(e0.elapsed_time(e1))
     ms = float(np.median(ts))
     # algorithmic bytes: xhat and sigma written, the cells' EOS state and densities read
-    ncarr = 10 + sum(sum(1 for k in ("n", "n2", "part", "level_n") if c.get(k) is not None) for c in comps)
+    ncarr = 11 + sum(sum(1 for k in ("n", "n2", "part", "level_n", "level_w") if c.get(k) is not None) for c in comps)
     nbytes = 8.0 * nlam * ncell + 8.0 * ncarr * ncell
     peaks = _peaks() or {}
     peak = peaks.get("hbm_gbs", 6650.0)
     from oracle import continuum as oc
     sub = 2000
     sc = {k: (v[:sub] if isinstance(v, np.ndarray) else v) for k, v in cells.items()}
-    scomps = [{k: (v[:sub] if k in ("n", "n2", "part", "level_n") else v) for k, v in c.items()} for c in comps]
+    scomps = [{k: (v[:sub] if k in ("n", "n2", "part", "level_n", "level_w") else v) for k, v in c.items()}
+              for c in comps]
     t0 = time.perf_counter()
     oc.continuum_opacities(scomps, lam, nu, sc)
     dt = time.perf_counter() - t0
     del xh, sg, dc, dcomps
     torch.cuda.empty_cache()
+    # bound by instruction issue like the line opacity: 148 SMs x 4 schedulers x one
+    # warp instruction per cycle, the instructions per launch scaled from the ncu count
+    # of the 48^3 case by cells
+    issue_peak = 148 * 4 * (sm_mhz or 1965.0) / 1e3
+    inst = NCU_CONTINUUM_WARP_INST_PER_CELL * ncell
+    issue = {"kernel": "k_continuum", "bound": "issue", "achieved": inst / (ms / 1e3) / 1e9, "peak": issue_peak,
+             "unit": "G warp-instructions/s", "frac": inst / (ms / 1e3) / 1e9 / issue_peak,
+             "warp_instructions_per_launch": inst,
+             "peak_source": "148 SMs x 4 issue slots x " + ("sampled SM clock" if sm_mhz else "max SM clock")}
     return {"workload": f"continuum opacity of one window: {ncell / 1e6:.2f} M cells ({n}^3), {nlam} frequencies "
-                        "3500-12000 A, 12 absdat-like components of every kind, H rest, electron + Rayleigh scattering",
+                        "3500-12000 A, 14 absdat-like components of every kind (2 H BF levels under occupation "
+                        "probabilities), H rest, electron + Rayleigh scattering",
             "unit": "Gpt*nu/s", "ms": ms, "value": ncell * nlam / (ms / 1e3) / 1e9,
             "achieved_gbs": nbytes / (ms / 1e3) / 1e9, "peak_gbs": peak, "frac": nbytes / (ms / 1e3) / 1e9 / peak,
+            "roofline_issue": issue,
             "cpu_baseline": {"value": sub * nlam / dt / 1e9, "unit": "Gpt*nu/s", "cores": 1, "kind": "port",
                              "sample": f"{sub} cells of the same case, the C restatement on one core, {dt:.2f} s"},
             "data": "synthetic (seeded EOS state and tables)"}
@@ -835,7 +851,7 @@ def run_b200(a):
         batched = _nlte_batched()
     if rank == 0 and not a.no_optab:
         optab = _optab()
-        continuum = _continuum()
+        continuum = _continuum(sm_mhz=clocks.get("sm_mhz"))
 
     c0 = c4 = None
     if rank == 0 and not a.no_c0:

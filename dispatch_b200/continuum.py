@@ -4,7 +4,12 @@ m3d_continuum_opacities.
 
 A component is a dict holding an absdat component's table and flags (bftrans_type,
 HOP/bftrans_mod.f90:19-52) and the number densities its absorption factor reads;
-the cells dict holds the EOS state.  Cell arrays are numpy (host) or CUDA tensors
+the cells dict holds the EOS state.  An 'H BF' level under occupation
+probabilities (the reference's default H_occupation_probability) sets
+occupation=True, level_i (principal quantum number), level_xion (its excitation
+energy [eV]), level_n and level_w (its population and occupation probability per
+cell), n (H I's density), and optionally dissolved_only; its cells need ne, nHeI and
+shield ((1+a)^3.15/ne of composition_type%compute_shield).  Cell arrays are numpy (host) or CUDA tensors
 (device, then the outputs are CUDA tensors too); tables are numpy.
 
     xhat, sigma = continuum_opacities(comps, lam, nu, cells)
@@ -24,7 +29,7 @@ from . import DEVICE_PTRS, M3DError, check, init, lib, order_after_torch, ptr
 HMINUS, NPE, H, H_FF, PAIR, H2PLUS, PEDEP, PEACH, MOLECULAR, REGULAR = range(1, 11)
 
 _FLAGS = ("ilogl", "kvadl", "minex", "maxex", "loglam", "kvadt", "minet", "maxet", "iteta", "lam3", "log_table")
-_CELL = ("n", "n2", "part", "level_n")
+_CELL = ("n", "n2", "part", "level_n", "level_w")
 
 
 class BfComp(C.Structure):
@@ -36,7 +41,9 @@ class BfComp(C.Structure):
                    ("ldisk", C.c_void_p)]
                 + [(k, C.c_double) for k in ("xkap_scale", "mint", "maxt", "minl", "maxl", "ion_xion", "level_g",
                                              "level_xion", "awgt")]
-                + [(k, C.c_void_p) for k in _CELL])
+                + [(k, C.c_void_p) for k in _CELL[:4]]
+                + [(k, C.c_int) for k in ("occupation", "dissolved_only", "level_i", "pad2")]
+                + [("level_w", C.c_void_p)])
 
 
 class ContCells(C.Structure):
@@ -44,7 +51,8 @@ class ContCells(C.Structure):
 
     _fields_ = ([(k, C.c_void_p) for k in ("temp", "teta", "e_kT", "pe", "dxi", "ne", "nHI", "partHI", "nHeI",
                                            "nH2")]
-                + [("HI_xion", C.c_double), ("helium_scattering", C.c_int), ("pad", C.c_int)])
+                + [("HI_xion", C.c_double), ("helium_scattering", C.c_int), ("pad", C.c_int),
+                   ("shield", C.c_void_p)])
 
 
 def set_table(xkap, ilogt: bool, ilogl: bool):
@@ -95,6 +103,8 @@ def make_comps(comps: list, dev: bool = False):
         s.lam, s.lnlam, s.tt, s.xkap, s.ldisk = (a.ctypes.data for a in (lam, lnlam, tt, xk, ld))
         for k in ("xkap_scale", "mint", "maxt", "minl", "maxl", "ion_xion", "level_g", "level_xion", "awgt"):
             setattr(s, k, float(c.get(k, 0.0)))
+        s.occupation, s.dissolved_only = int(bool(c.get("occupation", False))), int(bool(c.get("dissolved_only", False)))
+        s.level_i = int(c.get("level_i", 0))
         for k in _CELL:
             a = _cell_array(c.get(k), dev)
             keep.append(a)
@@ -105,7 +115,7 @@ def make_comps(comps: list, dev: bool = False):
 def make_cells(cells: dict, dev: bool = False):
     s = ContCells()
     keep = []
-    for k in ("temp", "teta", "e_kT", "pe", "dxi", "ne", "nHI", "partHI", "nHeI", "nH2"):
+    for k in ("temp", "teta", "e_kT", "pe", "dxi", "ne", "nHI", "partHI", "nHeI", "nH2", "shield"):
         a = _cell_array(cells.get(k), dev)
         keep.append(a)
         setattr(s, k, ptr(a).value if a is not None else None)

@@ -7,6 +7,8 @@
 //   components tabulated with stimulated emission, over 1 - beta   :2935-2970
 //   boltzmann_factor                 :2822-2852
 //   electron_scattering, rayleigh_scattering   :3851-3939
+//   'H BF' under occupation probabilities: wcalc2   level_mod.f90:149-279 (its
+//                                    per-wavelength set-up, calc_x_and_k :77-94, on the host)
 // One warp per cell: the lanes first form each component's temperature stencil and
 // absorption factor for the cell (one component per lane), then run along the
 // window's wavelengths, each adding the components in their order.  Kinds follow the
@@ -24,6 +26,15 @@ constexpr int kContMaxRows = 1024;  // table rows a window reads, over all compo
 constexpr int kContMaxTab = 8192;   // their table entries at every temperature node (per block, in shared memory)
 constexpr int kContKF = 8;          // wavelengths a lane holds in one pass over the components
 
+// wcalc2's per-wavelength set-up of an 'H BF' level (level_mod.f90:186-218): cls 0
+// none, 1 beyond the series limit, 2 below it (a dissolved upper level); cutfac the
+// cut beyond the alpha line; x1, x2, kk = calc_x_and_k of the state, kd its kk in real(8)
+struct OccFDev {
+  double cutfac, kd;
+  float x1, x2, kk;
+  int cls;
+};
+
 struct __align__(16) BfCompDev {
   int kind, istim, nnu, ntt, ilogl, lam3, log_table, kvadt, minet, maxet, iteta, k, fs, fe, active;
   // the table rows the window's stencils read (0-based r0 .. r0 + nrow - 1), their
@@ -38,12 +49,18 @@ struct __align__(16) BfCompDev {
   const float4 *wt;
   const unsigned char *quad;
   const double *n, *n2, *part, *level_n;
+  // an 'H BF' level under occupation probabilities: occ, q = 2.0898e-26/(2 i^5) in
+  // real(4), its occupation probability per cell and the per-wavelength set-up
+  int occ;
+  float occ_q;
+  const double *level_w;
+  const OccFDev *occf;
 };
 
 static_assert(sizeof(BfCompDev) % 16 == 0, "descriptors staged in shared memory ahead of the tables");
 
 struct ContCellsDev {
-  const double *temp, *teta, *e_kT, *pe, *dxi, *ne, *nHI, *partHI, *nHeI, *nH2;
+  const double *temp, *teta, *e_kT, *pe, *dxi, *ne, *nHI, *partHI, *nHeI, *nH2, *shield;
   double HI_xion;
   int helium_scattering;
 };
@@ -72,6 +89,7 @@ __device__ __forceinline__ float cont_factor(const BfCompDev &c, const ContCells
     case 1: fk = c.n[x]; break;
     case 2: fk = c.n[x] * pe; break;
     case 3: {
+      if (c.occ) break;   // absorption_factor leaves huge(1d0): interp_xkap does not use it
       int k5 = c.k * c.k;
       k5 = k5 * k5 * c.k;
       // the default-real literal over the integer 2 k^5: a real(4) quotient
@@ -191,7 +209,8 @@ __device__ __forceinline__ float cont_row_s(const BfCompDev &c, const BfCellDev 
 // is real(lambda^3).  The component's fields are read once for all of them.
 template <int KF>
 __device__ __forceinline__ void cont_comp(const BfCompDev &c, const BfCellDev &r, const float *rows, int f0,
-                                          const float *__restrict__ l3, float (&v)[KF]) {
+                                          const float *__restrict__ l3, const ContCellsDev &S, int x,
+                                          float (&v)[KF]) {
   if (!c.active) return;
   const int fs = c.fs, fe = c.fe, nnu = c.nnu, ilogl = c.ilogl, lam3 = c.lam3;
   const float4 *wt = c.wt;
@@ -226,6 +245,61 @@ __device__ __forceinline__ void cont_comp(const BfCompDev &c, const BfCellDev &r
       if (ilogl) ab = exp4(ab);
       if (lam3) ab = __fmul_rn(ab, __ldg(l3 + f));
       v[k] = __fadd_rn(v[k], __fmul_rn(fakt1, ab));
+    }
+  } else if (c.occ) {
+    // interp_xkap_2's table at the window, then wcalc2 for the cell (bftrans_mod.f90
+    // :398-428, level_mod.f90:220-277): w, 1 - w, the level's population and
+    // 4 pi/3 n_H of the cell are in r; shield, ne and 4 pi/3 n_He are the cell's
+    const float w = r.w0, omw = r.w1, n = r.w2, nh43 = r.fakt1;
+    const double xd = S.shield[x];
+    const float xs = (float)xd, ne1 = (float)S.ne[x], nhe43 = (float)(4.18879 * S.nHeI[x]);
+    const float *xk = c.xkap;
+    const unsigned char *quad = c.quad;
+    const OccFDev *occf = c.occf;
+    const float scale = (float)c.xkap_scale;
+    const double q = (double)c.occ_q;
+#pragma unroll
+    for (int k = 0; k < KF; k++) {
+      const int f = f0 + 32 * k;
+      if (f < fs || f > fe) continue;
+      const OccFDev o = occf[f];
+      if (o.cls == 0) continue;
+      const float4 wv = __ldg(wt + f);
+      const int iw = __float_as_int(wv.x);
+      float ab;
+      if (iw < 0) {
+        ab = 0.0f;
+      } else {
+        const float *yy = xk + iw;
+        ab = __fadd_rn(0.0f, __fmul_rn(yy[0], wv.y));
+        ab = __fadd_rn(ab, __fmul_rn(yy[1], wv.z));
+        if (quad[f]) ab = __fadd_rn(ab, __fmul_rn(yy[2], wv.w));
+        if (ilogl) ab = expf(ab);
+      }
+      if (lam3) ab = __fmul_rn(ab, __ldg(l3 + f));
+      // g = real(2.0898E-26/(2 i^5) * cutfac * ab, 4), ab times real(xkap_scale, 4)
+      const float g = (float)((q * o.cutfac) * (double)__fmul_rn(ab, scale));
+      float d;
+      if (o.cls == 1) {
+        d = w;
+      } else {
+        // neutral perturbers E = exp(-a); charged ones C = frac/(1+frac), tested on
+        // the real(8) product; w - wstar formed as (1 - wstar) - (1 - w) near w = 1
+        const float a = __fadd_rn(__fmul_rn(nh43, o.x1), __fmul_rn(nhe43, o.x2));
+        float E, omE;
+        exp_neg0(a, E, omE);
+        const float k1 = o.kk;
+        const float xkk = __fmul_rn(xs, k1);
+        float C = 1.0f, omC = 0.0f;
+        if (xd * o.kd < 1e4) {
+          const float den = __fadd_rn(1.0f, __fmul_rn(0.1285f, xkk));
+          const float frac = __fdiv_rn(__fmul_rn(__fmul_rn(0.1402f, xkk), k1), __fmul_rn(ne1, den));
+          C = __fdiv_rn(frac, __fadd_rn(1.0f, frac));
+          omC = __fdiv_rn(1.0f, __fadd_rn(1.0f, frac));
+        }
+        d = (w > 0.5f) ? __fsub_rn(__fadd_rn(omE, __fmul_rn(E, omC)), omw) : __fsub_rn(w, __fmul_rn(E, C));
+      }
+      v[k] = __fadd_rn(v[k], __fmul_rn(__fmul_rn(d, n), g));
     }
   } else {
     const float fakt1 = r.fakt1;
@@ -338,7 +412,16 @@ k_continuum(int ncomp, const BfCompDev *__restrict__ comps_g, int any_istim, int
         r.quadratic = 0;
         r.edge = 0;
       }
-      r.fakt1 = (c.active && r.in_bounds) ? cont_factor(c, S, x) : 0.0f;
+      if (c.occ && c.ntt == 1) {
+        // wcalc2's per-cell terms (level_mod.f90:222-229)
+        const double wo = c.active ? c.level_w[x] : 0.0;
+        r.w0 = (float)wo;
+        r.w1 = (float)(1.0 - wo);
+        r.w2 = c.active ? (float)c.level_n[x] : 0.0f;
+        r.fakt1 = c.active ? (float)(4.18879 * c.n[x]) : 0.0f;
+      } else {
+        r.fakt1 = (c.active && r.in_bounds) ? cont_factor(c, S, x) : 0.0f;
+      }
       st[j] = r;
     }
     __syncwarp();
@@ -373,7 +456,7 @@ k_continuum(int ncomp, const BfCompDev *__restrict__ comps_g, int any_istim, int
       }
       for (int j = 0; j < ncomp; j++) {
         const BfCompDev &c = comps[j];
-        if (!c.istim) cont_comp<kContKF>(c, st[j], rows, f0, LW.l3, v);
+        if (!c.istim) cont_comp<kContKF>(c, st[j], rows, f0, LW.l3, S, x, v);
       }
       if (any_istim) {
         float tmp[kContKF];
@@ -381,7 +464,7 @@ k_continuum(int ncomp, const BfCompDev *__restrict__ comps_g, int any_istim, int
         for (int k = 0; k < kContKF; k++) tmp[k] = 0.0f;
         for (int j = 0; j < ncomp; j++) {
           const BfCompDev &c = comps[j];
-          if (c.istim) cont_comp<kContKF>(c, st[j], rows, f0, LW.l3, tmp);
+          if (c.istim) cont_comp<kContKF>(c, st[j], rows, f0, LW.l3, S, x, tmp);
         }
 #pragma unroll
         for (int k = 0; k < kContKF; k++) {

@@ -34,6 +34,12 @@ __device__ __forceinline__ void exp_neg(float t, float &E, float &u0) {
   u0 = fmaf(s, m, 1.0f - s);
 }
 
+// exp_neg0: E = 0 above t = 87 (and for a NaN t), t clamped at -87 below (exp_neg.inc:41-51)
+__device__ __forceinline__ void exp_neg0(float t, float &E, float &u0) {
+  exp_neg(fmaxf(t, -87.0f), E, u0);
+  if (!(t <= 87.0f)) E = 0.0f;
+}
+
 // exp4(x) = exp_neg0(-x): 0 below x = -87, saturating at exp(87) (exp_neg.inc:45-62)
 __device__ __forceinline__ float exp4(float x) {
   const float t = -x;

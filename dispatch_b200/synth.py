@@ -854,8 +854,9 @@ def window_tables(seed, temp, ne, vproj, nf=256, lam0=5040.0, R=1e5, pad_guard=2
 
 
 def continuum_case(seed: int = 5, ncell: int = 2000, nlam: int = 256, lam_range=(3500.0, 12000.0)) -> tuple:
-    """(comps, lam, nu, cells) of a seeded continuum-opacity case: twelve absdat-like
-    components, one or more of every absorption-factor kind, their tables in the
+    """(comps, lam, nu, cells) of a seeded continuum-opacity case: fourteen absdat-like
+    components, one or more of every absorption-factor kind (two 'H BF' levels under
+    occupation probabilities among them), their tables in the
     stored form of set_table (dispatch_b200.continuum.set_table) with every
     interpolation choice -- linear or quadratic in temperature (T or 5040/T nodes),
     logarithmic tables, linear, quadratic or logarithmic in wavelength, nodes flagged
@@ -920,4 +921,48 @@ def continuum_case(seed: int = 5, ncell: int = 2000, nlam: int = 256, lam_range=
         table(REGULAR, 26, (3000.0, 9000.0), tnod[::2], sig(1e-18, 2.0), istim=True, ilogt=True, lam3=True,
               level_g=2.0, level_xion=1.1, minex=True, n=dens(10.0, 13.0), part=np.log(rng.uniform(2.0, 9.0, ncell))),
     ]
+    # two 'H BF' levels under occupation probabilities (the reference's default),
+    # n = 2 and 3: Gaunt-factor-like tables (2.0898e-26/(2 n^5) lam^3 is Kramers'
+    # cross section) up to the series limit, extrapolated beyond it (maxex, as
+    # the reference sets for these levels); the window then holds wavelengths beyond
+    # each limit, dissolved upper states below it (both perturber branches of wcalc2,
+    # w near 1), and the cut past the alpha line
+    cells["shield"] = h_shield(temp, ne)
+    for i, dissolved in ((2, False), (3, True)):
+        edge = 911.267 * i * i
+        xion = 13.598434 * float(np.float32(1.0) - np.float32(1.0) / np.float32(i * i))
+        g = 2.0 * i * i
+        lvl_n = g * np.exp(-e_kT * xion) * cells["nHI"] / 2.0
+        w = h_occupation(cells["nHI"], cells["nHeI"], ne, cells["shield"], float(i))
+        c = table(H, 16 + 2 * i, (600.0, edge), [6000.0], lambda l, t: 0.95 * (l / edge) ** 0.1, lam3=True,
+                  kvadl=True, maxex=True, occupation=True, level_i=i, level_xion=xion, k=i, n=cells["nHI"],
+                  level_n=lvl_n, level_w=w, dissolved_only=dissolved)
+        comps.append(c)
     return comps, lam, nu, cells
+
+
+def h_shield(temp, ne):
+    """composition_type%compute_shield (HOP/composition_mod.f90:2604-2613): the
+    charged-perturber shielding (1 + a)^3.15 / ne, a = 0.08989 ne^(1/6) / sqrt(T)."""
+    a = 0.08989 * np.asarray(ne) ** 0.16667 / np.sqrt(np.asarray(temp))
+    return (1.0 + a) ** 3.15 / np.asarray(ne)
+
+
+def h_occupation(nh, nhe, ne, shield, ns):
+    """wcalc (HOP/level_mod.f90:108-142): the occupation probability of an H I state
+    of effective quantum number ns -- hard-sphere neutral H and He perturbers
+    (Hummer & Mihalas 1988) times the charged-perturber fit of Hubeny, Hummer & Lanz
+    (1994) where k x < 1e4.  A numpy stand-in for the EOS's level set-up."""
+    ns2 = ns * ns
+    rih = ns * np.sqrt(2.5 * ns2 + 0.5)
+    x1 = (5.29177349e-9 * (rih + 1.73)) ** 3
+    x2 = (5.29177349e-9 * (rih + 1.02)) ** 3
+    k = 8.3e14 / (ns2 * ns2)
+    if ns > 3.0:
+        k = k * 5.33333333 * ns / (ns + 1.0) ** 2
+    k = k * np.sqrt(k)
+    res = np.exp(-4.18879 * (np.asarray(nh) * x1 + np.asarray(nhe) * x2))
+    x = np.asarray(shield)
+    charged = k * x < 1e4
+    frac = 0.1402 * x * k * k / (np.asarray(ne) * (1.0 + 0.1285 * x * k))
+    return np.where(charged, res * frac / (1.0 + frac), res)

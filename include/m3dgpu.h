@@ -481,7 +481,7 @@ int m3d_lte_synthesis_adjoint(const m3d_atmos_t *atm, int nf, const double *nu, 
  * components' tables are inputs. */
 #define M3D_BF_HMINUS 1    /* 'H- BF': n */
 #define M3D_BF_NPE 2       /* 'H- FF', 'H2-', 'HE-': n Pe */
-#define M3D_BF_H 3         /* 'H BF' without occupation probabilities: 2.0898e-26/(2 k^5) n_k */
+#define M3D_BF_H 3         /* 'H BF': 2.0898e-26/(2 k^5) n_k, or wcalc2 under occupation probabilities */
 #define M3D_BF_H_FF 4      /* 'H FF': 2.0898e-26 kT/(2 Ryd) n exp(-(xion - dxi)/kT) / U */
 #define M3D_BF_PAIR 5      /* 'H+H', 'H+HE', 'H2+H', 'H2+H2', 'H2+HE': n n2 */
 #define M3D_BF_H2PLUS 6    /* 'H2+': 1e-40 n n2 */
@@ -496,7 +496,15 @@ int m3d_lte_synthesis_adjoint(const m3d_atmos_t *atm, int nf, const double *nu, 
  * xkap_scale, logarithmic when log_table), ldisk (nnu).  The per-cell arrays (ncell,
  * float64) follow the call's flags: n the particle's number density [cm^-3]; n2 the
  * second particle's (pairs, H2+); part the particle's ln partition function (H FF,
- * regular); level_n the population of H I level k (M3D_BF_H). */
+ * regular); level_n the population of H I level k (M3D_BF_H).
+ * occupation: an 'H BF' level under H_occupation_probability (the reference's
+ * default): a table without temperature dependence goes through wcalc2
+ * (level_mod.f90:149-279) with level_i the level's principal quantum number,
+ * level_xion its excitation energy [eV], level_n its population, level_w its
+ * occupation probability (per cell), n H I's number density, and the cells' ne, nHeI
+ * and shield; dissolved_only leaves out the wavelengths beyond the series limit.
+ * With temperature nodes the level keeps absorption_factor's huge(1d0) factor, as
+ * the reference does. */
 typedef struct m3d_bf_comp {
   int kind, istim, nnu, ntt;
   int ilogl, kvadl, minex, maxex, loglam;
@@ -508,27 +516,30 @@ typedef struct m3d_bf_comp {
   double xkap_scale, mint, maxt, minl, maxl;
   double ion_xion, level_g, level_xion, awgt;
   const double *n, *n2, *part, *level_n;
+  int occupation, dissolved_only, level_i, pad2;
+  const double *level_w;
 } m3d_bf_comp_t;
 
 /* The EOS state of the cells (ncell, float64, per the call's flags): temp [K], teta
  * = 5040/T, e_kT = 1 eV/kT, pe [dyn cm^-2], dxi the ionisation-energy lowering [eV],
  * ne [cm^-3]; H I's number density and ln partition function (the H rest; NULL: no
  * H rest, no H I Rayleigh), He I and H2 densities (Rayleigh; may be NULL), H I's
- * ionisation energy [eV], and helium_scattering (the reference's switch, default on). */
+ * ionisation energy [eV], and helium_scattering (the reference's switch, default on);
+ * shield = (1+a)^3.15/ne of compute_shield (composition_mod.f90:2604-2613) [cm^3],
+ * for the H BF levels under occupation probabilities (else may be NULL). */
 typedef struct m3d_cont_cells {
   const double *temp, *teta, *e_kT, *pe, *dxi, *ne;
   const double *nHI, *partHI, *nHeI, *nH2;
   double HI_xion;
   int helium_scattering, pad;
+  const double *shield;
 } m3d_cont_cells_t;
 
 /* xhat (nlam, ncell) = the continuum's true absorption in the working form (the
  * components in order; those with istim summed apart and divided by 1 - beta);
  * sigma (nlam, ncell, may be NULL) = electron + Rayleigh scattering [1/cm].  lam and
  * nu (nlam, host) are the window's wavelengths [AA] and frequencies [Hz]; beta
- * (nlam, ncell) or NULL, then boltzmann_factor from nu.  An 'H BF' component with
- * occupation probabilities (wcalc2) is the EOS's and not accepted (M3D_EINVAL for
- * an unknown kind). */
+ * (nlam, ncell) or NULL, then boltzmann_factor from nu. */
 int m3d_continuum_opacities(int ncomp, const m3d_bf_comp_t *comps, int nlam, const double *lam, const double *nu,
                             int ncell, const m3d_cont_cells_t *cells, const float *beta, float *xhat, float *sigma,
                             unsigned flags);

@@ -14,7 +14,7 @@ import numpy as np
 from .oracle import lib
 
 _FLAGS = ("ilogl", "kvadl", "minex", "maxex", "loglam", "kvadt", "minet", "maxet", "iteta", "lam3", "log_table")
-_CELL = ("n", "n2", "part", "level_n")
+_CELL = ("n", "n2", "part", "level_n", "level_w")
 
 
 class _Comp(C.Structure):
@@ -23,13 +23,16 @@ class _Comp(C.Structure):
                 + [(k, C.c_void_p) for k in ("lam", "lnlam", "tt", "xkap", "ldisk")]
                 + [(k, C.c_double) for k in ("xkap_scale", "mint", "maxt", "minl", "maxl", "ion_xion", "level_g",
                                              "level_xion", "awgt")]
-                + [(k, C.c_void_p) for k in _CELL])
+                + [(k, C.c_void_p) for k in _CELL[:4]]
+                + [(k, C.c_int) for k in ("occupation", "dissolved_only", "level_i", "pad2")]
+                + [("level_w", C.c_void_p)])
 
 
 class _Cells(C.Structure):
     _fields_ = ([(k, C.c_void_p) for k in ("temp", "teta", "e_kT", "pe", "dxi", "ne", "nHI", "partHI", "nHeI",
                                            "nH2")]
-                + [("HI_xion", C.c_double), ("helium_scattering", C.c_int), ("pad", C.c_int)])
+                + [("HI_xion", C.c_double), ("helium_scattering", C.c_int), ("pad", C.c_int),
+                   ("shield", C.c_void_p)])
 
 
 def _pack(comps, keep):
@@ -47,6 +50,8 @@ def _pack(comps, keep):
         s.lam, s.lnlam, s.tt, s.xkap, s.ldisk = (a.ctypes.data for a in (lam, lnlam, tt, xk, ld))
         for k in ("xkap_scale", "mint", "maxt", "minl", "maxl", "ion_xion", "level_g", "level_xion", "awgt"):
             setattr(s, k, float(c.get(k, 0.0)))
+        s.occupation, s.dissolved_only = int(bool(c.get("occupation", False))), int(bool(c.get("dissolved_only", False)))
+        s.level_i = int(c.get("level_i", 0))
         for k in _CELL:
             a = c.get(k)
             if a is not None:
@@ -79,7 +84,7 @@ def continuum_opacities(comps: list, lam, nu, cells: dict, beta=None, sigma: boo
     keep = []
     arr = _pack(comps, keep)
     s = _Cells()
-    for k in ("temp", "teta", "e_kT", "pe", "dxi", "ne", "nHI", "partHI", "nHeI", "nH2"):
+    for k in ("temp", "teta", "e_kT", "pe", "dxi", "ne", "nHI", "partHI", "nHeI", "nH2", "shield"):
         a = cells.get(k)
         if a is not None:
             a = np.ascontiguousarray(a, np.float64)

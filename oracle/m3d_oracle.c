@@ -103,6 +103,10 @@ void or_exp_neg_f32(int n, const float *t, float *E, float *u0)
 {
   for (int i = 0; i < n; i++) or_exp_neg1(t[i], &E[i], &u0[i]);
 }
+void or_exp_neg0_f32(int n, const float *t, float *E, float *u0)
+{
+  for (int i = 0; i < n; i++) or_exp_neg0(t[i], &E[i], &u0[i]);
+}
 void or_exp4_f32(int n, const float *x, float *y)
 {
   for (int i = 0; i < n; i++) y[i] = or_exp4(x[i]);

@@ -27,6 +27,9 @@ static float exp4_1(float x)
 
 static const double OR_RYD = 13.598434, OR_EE = 1.602189e-12, OR_HH = 6.626176e-27, OR_BK = 1.380662e-16;
 static const double OR_CC = 2.99792458e10, OR_EM = 9.109534e-28, OR_EC = 4.80325e-10, OR_PI = 3.14159265359;
+static const double OR_RBOHR = 5.29177349e-9;
+
+void or_exp_neg0_f32(int n, const float *t, float *E, float *u0);
 
 /* the fits_in test of load_lam_interp_weights: x in [lam(idx), lam(idx+1)), idx
  * 1-based within 1 .. nnu-1 */
@@ -117,6 +120,7 @@ static float bf_factor(const or_bf_comp_t *c, const or_cont_cells_t *s, int x)
     case OR_BF_HMINUS: fk = c->n[x]; break;
     case OR_BF_NPE: fk = c->n[x] * pe; break;
     case OR_BF_H: {
+      if (c->occupation) break;   /* fakt left at huge(1d0): interp_xkap does not use it */
       int k5 = c->k * c->k;
       k5 = k5 * k5 * c->k;
       const double scalar = (double)(2.0898e-26f / (float)(2 * k5));
@@ -213,6 +217,96 @@ static float t_row(const or_bf_comp_t *c, const tinterp_t *r, int j)
   return y;
 }
 
+/* calc_x_and_k (level_mod.f90:77-94): the hard-sphere volumes of H and He
+ * perturbers and the charged-perturber factor of a state of effective quantum
+ * number ns.  x**3 is (x*x)*x as gfortran expands a constant integer power; the
+ * literals 1.73, 1.02, 8.3e14 and 5.33333333 are default reals. */
+static void calc_x_and_k(double ns, double *x1, double *x2, double *k)
+{
+  const double ns2 = ns * ns;
+  const double rih = ns * sqrt(2.5 * ns2 + 0.5);
+  const double t1 = OR_RBOHR * (rih + (double)1.73f), t2 = OR_RBOHR * (rih + (double)1.02f);
+  *x1 = t1 * t1 * t1;
+  *x2 = t2 * t2 * t2;
+  double kk = (double)8.3e14f / (ns2 * ns2);
+  if (ns > 3.) kk = kk * (double)5.33333333f * ns / ((ns + 1.0) * (ns + 1.0));
+  *k = kk * sqrt(kk);
+}
+
+/* wcalc2 (level_mod.f90:149-279) for the cells: ab (nlam) is the level's table
+ * interpolated to the window (lam^3 included) for fs..fe, times real(xkap_scale) */
+static void wcalc2(const or_bf_comp_t *c, int nlam, const double *lam, const float *ab, int fs, int fe, int ncell,
+                   const or_cont_cells_t *s, float *chi)
+{
+  const int li = c->level_i;
+  const double hc_e = OR_HH * OR_CC / OR_EE, h_e = OR_HH / OR_EE;
+  const double redcut = hc_e / ((pow((double)li, -2.0) - pow((double)(li + 1), -2.0)) * OR_RYD) * 1e8;
+  int i5 = li * li;
+  i5 = i5 * i5 * li;
+  const float q = 2.0898e-26f / (float)(2 * i5);
+  /* per wavelength: 0 none, 1 beyond the series limit, 2 below it */
+  int *cls = calloc((size_t)nlam, sizeof(int));
+  float *g = calloc((size_t)nlam, sizeof(float)), *x1 = calloc((size_t)nlam, sizeof(float));
+  float *x2 = calloc((size_t)nlam, sizeof(float)), *kk = calloc((size_t)nlam, sizeof(float));
+  double *kd = calloc((size_t)nlam, sizeof(double));
+  for (int f = fs; f <= fe; f++) {
+    const double cutfac = lam[f] > redcut ? exp((redcut - lam[f]) * 1e-2) : 1.0;
+    if (!(cutfac > 1e-1)) continue;
+    g[f] = (float)((double)q * cutfac * (double)ab[f]);
+    const double nu = OR_CC / lam[f] * (double)1e8f;
+    double ns = 1. - (c->level_xion + h_e * nu) / OR_RYD;
+    if (ns > 0) {
+      ns = 1.0 / sqrt(ns);
+      double x1d, x2d, kkd;
+      calc_x_and_k(ns, &x1d, &x2d, &kkd);
+      cls[f] = 2;
+      x1[f] = (float)x1d;
+      x2[f] = (float)x2d;
+      kk[f] = (float)kkd;
+      kd[f] = kkd;
+    } else if (!c->dissolved_only) {
+      cls[f] = 1;
+    }
+  }
+  const double pi43 = 4.18879;
+  for (int x = 0; x < ncell; x++) {
+    const float w = (float)c->level_w[x];
+    const float omw = (float)(1.0 - c->level_w[x]);
+    const double xd = s->shield[x];
+    const float xs = (float)xd;
+    const float n = (float)c->level_n[x];
+    const float ne1 = (float)s->ne[x];
+    const float nh43 = (float)(pi43 * c->n[x]);
+    const float nhe43 = (float)(pi43 * s->nHeI[x]);
+    float *ch = chi + (size_t)nlam * x;
+    for (int f = fs; f <= fe; f++) {
+      if (cls[f] == 1) {
+        ch[f] = ch[f] + w * n * g[f];
+      } else if (cls[f] == 2) {
+        const float a = nh43 * x1[f] + nhe43 * x2[f];
+        float E, omE;
+        or_exp_neg0_f32(1, &a, &E, &omE);
+        const float k1 = kk[f];
+        const float xk = xs * k1;
+        float C = 1.0f, omC = 0.0f;
+        if (xd * kd[f] < 1e4) {
+          const float frac = 0.1402f * xk * k1 / (ne1 * (1.0f + 0.1285f * xk));
+          C = frac / (1.0f + frac);
+          omC = 1.0f / (1.0f + frac);
+        }
+        const float d = w > 0.5f ? (omE + E * omC) - omw : w - E * C;
+        ch[f] = ch[f] + d * n * g[f];
+      }
+    }
+  }
+  free(cls);
+  free(g);
+  free(x1);
+  free(x2);
+  free(kk);
+  free(kd);
+}
+
 /* add_absorption of one component to chi (nlam, ncell) */
 static void bf_add(const or_bf_comp_t *c, int nlam, const double *lam, int ncell, const or_cont_cells_t *s, float *chi)
 {
@@ -220,7 +314,25 @@ static void bf_add(const or_bf_comp_t *c, int nlam, const double *lam, int ncell
   unsigned char *quad = malloc((size_t)nlam);
   float *lag = malloc(sizeof(float) * 3 * nlam);
   int fs = 0, fe = -1;
-  if (or_bf_weights(c, nlam, lam, iw, quad, lag, &fs, &fe)) {
+  if (or_bf_weights(c, nlam, lam, iw, quad, lag, &fs, &fe) && c->ntt == 1 && c->kind == OR_BF_H && c->occupation) {
+    /* interp_xkap_2 with H_occupation_probability: the table at the window, then
+     * wcalc2 for every cell (bftrans_mod.f90:398-428) */
+    float *ab = calloc((size_t)nlam, sizeof(float));
+    for (int f = fs; f <= fe; f++) {
+      float v = 0.0f;
+      if (iw[f] >= 0) {
+        const float *yy = c->xkap + iw[f];
+        v = 0.0f + yy[0] * lag[3 * f];
+        v = v + yy[1] * lag[3 * f + 1];
+        if (quad[f]) v = v + yy[2] * lag[3 * f + 2];
+        if (c->ilogl) v = expf(v);
+      }
+      if (c->lam3) v = v * (float)(lam[f] * lam[f] * lam[f]);
+      ab[f] = v * (float)c->xkap_scale;
+    }
+    wcalc2(c, nlam, lam, ab, fs, fe, ncell, s, chi);
+    free(ab);
+  } else if (fe >= fs) {
     for (int x = 0; x < ncell; x++) {
       float *ch = chi + (size_t)nlam * x;
       if (c->ntt > 1) {

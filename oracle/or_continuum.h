@@ -4,8 +4,10 @@
  * add_hrest (:3807-3846), electron_scattering (:3851-3872), rayleigh_scattering
  * (:3878-3939), boltzmann_factor (:2822-2852), and the absdat components of
  * bftrans_mod.f90 (load_lam_interp_weights :100-198, interp_xkap :235-452,
- * absorption_factor :476-531, add_absorption :537-594).  TEST INFRASTRUCTURE
- * ONLY: the checker of the continuum kernels, never the product.
+ * absorption_factor :476-531, add_absorption :537-594), with the 'H BF' levels
+ * under occupation probabilities through wcalc2 and calc_x_and_k
+ * (HOP/level_mod.f90:77-94, 149-279).  TEST INFRASTRUCTURE ONLY: the checker of
+ * the continuum kernels, never the product.
  *
  * The EOS state (temperatures, electron pressure, the particles' number densities
  * and partition functions) and the components' tables are inputs.  Layouts: cell
@@ -24,7 +26,7 @@ extern "C" {
 enum {
   OR_BF_HMINUS = 1,   /* 'H- BF': n */
   OR_BF_NPE = 2,      /* 'H- FF', 'H2-', 'HE-': n Pe */
-  OR_BF_H = 3,        /* 'H BF' without occupation probabilities: 2.0898e-26/(2 k^5) n_k */
+  OR_BF_H = 3,        /* 'H BF': 2.0898e-26/(2 k^5) n_k, or wcalc2 with occupation */
   OR_BF_H_FF = 4,     /* 'H FF' */
   OR_BF_PAIR = 5,     /* 'H+H', 'H+HE', 'H2+H', 'H2+H2', 'H2+HE': n n2 */
   OR_BF_H2PLUS = 6,   /* 'H2+': 1e-40 n n2 */
@@ -45,6 +47,11 @@ typedef struct or_bf_comp {
   double xkap_scale, mint, maxt, minl, maxl;
   double ion_xion, level_g, level_xion, awgt;
   const double *n, *n2, *part, *level_n;
+  /* 'H BF' with H_occupation_probability: the level's principal quantum number
+   * (level_xion is its excitation energy), dissolved_only, its occupation
+   * probability per cell */
+  int occupation, dissolved_only, level_i, pad2;
+  const double *level_w;
 } or_bf_comp_t;
 
 typedef struct or_cont_cells {
@@ -52,6 +59,7 @@ typedef struct or_cont_cells {
   const double *nHI, *partHI, *nHeI, *nH2;
   double HI_xion;
   int helium_scattering, pad;
+  const double *shield;  /* (1+a)^3.15/ne of compute_shield, for the H BF occupation levels */
 } or_cont_cells_t;
 
 /* load_lam_interp_weights: the stencils of one component on the wavelengths lam

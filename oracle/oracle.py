@@ -83,6 +83,10 @@ def exp_neg(t):
     return _vec1("or_exp_neg_f32", t, np.float32, 2)
 
 
+def exp_neg0(t):
+    return _vec1("or_exp_neg0_f32", t, np.float32, 2)
+
+
 def exp4(x):
     return _vec1("or_exp4_f32", x, np.float32, 1)
 

@@ -8,7 +8,10 @@ states and against independent restatements:
 * set_table's stored form (dispatch_b200.continuum.set_table) against its formula;
 * the Thomson constant against const_mod's sigma_th, electron and Rayleigh
   scattering and the H rest against direct numpy forms;
-* components tabulated with stimulated emission end up divided by 1 - beta.
+* components tabulated with stimulated emission end up divided by 1 - beta;
+* an 'H BF' level under occupation probabilities (wcalc2, level_mod.f90:149-279)
+  against an independent float32 restatement, and in the limit without perturbers
+  (w = wstar = 1) against the same level without occupation probabilities.
 """
 import numpy as np
 import pytest
@@ -143,3 +146,99 @@ def test_full_case_finite(oc):
     for k, c in enumerate(comps):
         x1, _ = oc.continuum_opacities([c], lam, nu, cells, sigma=False)
         assert x1.max() > 0, k
+
+
+def _wcalc2_numpy(c, lam, cells, fs, fe, ab):
+    """wcalc2 restated with numpy scalars in the kinds of level_mod.f90:149-279:
+    real(8) set-up per wavelength, real(4) arithmetic per cell; exp_neg0 is the
+    oracle's K0 function (pinned by tests/test_oracle_contracts.py)."""
+    from oracle.oracle import exp_neg0
+    f32 = np.float32
+    hh, ee, cc, ryd = 6.626176e-27, 1.602189e-12, 2.99792458e10, 13.598434
+    li = int(c["level_i"])
+    redcut = (hh * cc / ee) / ((float(li) ** -2.0 - float(li + 1) ** -2.0) * ryd) * 1e8
+    q = f32(2.0898e-26) / f32(2 * li ** 5)
+    ncell = cells["ne"].size
+    out = np.zeros((ncell, lam.size), np.float32)
+    for f in range(fs, fe + 1):
+        cutfac = np.exp((redcut - lam[f]) * 1e-2) if lam[f] > redcut else 1.0
+        if not cutfac > 0.1:
+            continue
+        g = f32(float(q) * cutfac * float(ab[f]))
+        nu = cc / lam[f] * float(f32(1e8))
+        ns = 1.0 - (c["level_xion"] + (hh / ee) * nu) / ryd
+        w = c["level_w"].astype(np.float32)
+        n = c["level_n"].astype(np.float32)
+        if ns > 0:
+            ns = 1.0 / np.sqrt(ns)
+            ns2 = ns * ns
+            rih = ns * np.sqrt(2.5 * ns2 + 0.5)
+            t1 = 5.29177349e-9 * (rih + float(f32(1.73)))
+            t2 = 5.29177349e-9 * (rih + float(f32(1.02)))
+            k = float(f32(8.3e14)) / (ns2 * ns2)
+            if ns > 3.0:
+                k = k * float(f32(5.33333333)) * ns / ((ns + 1.0) * (ns + 1.0))
+            kd = k * np.sqrt(k)
+            x1, x2, kk = f32(t1 * t1 * t1), f32(t2 * t2 * t2), f32(kd)
+            nh43 = (4.18879 * c["n"]).astype(np.float32)
+            nhe43 = (4.18879 * cells["nHeI"]).astype(np.float32)
+            a = nh43 * x1 + nhe43 * x2
+            E, omE = exp_neg0(a)
+            xs = cells["shield"].astype(np.float32)
+            xk = xs * kk
+            ne1 = cells["ne"].astype(np.float32)
+            frac = f32(0.1402) * xk * kk / (ne1 * (f32(1.0) + f32(0.1285) * xk))
+            charged = cells["shield"] * kd < 1e4
+            C = np.where(charged, frac / (f32(1.0) + frac), f32(1.0)).astype(np.float32)
+            omC = np.where(charged, f32(1.0) / (f32(1.0) + frac), f32(0.0)).astype(np.float32)
+            omw = (1.0 - c["level_w"]).astype(np.float32)
+            d = np.where(w > f32(0.5), (omE + E * omC) - omw, w - E * C).astype(np.float32)
+            out[:, f] = d * n * g
+        elif not c.get("dissolved_only"):
+            out[:, f] = w * n * g
+    return out
+
+
+def test_h_occupation_level_against_numpy(oc):
+    comps, lam, nu, cells = synth.continuum_case(ncell=60, nlam=120)
+    cells = {k: v for k, v in cells.items() if k not in ("nHI", "partHI")}
+    for c in comps[12:]:
+        assert c["occupation"] and c["tt"].size == 1
+        act, iw, quad, lag, fs, fe = oc.bf_weights(c, lam)
+        assert act
+        # interp_xkap_2's table at the window, lam^3, times real(xkap_scale, 4)
+        ab = np.zeros(lam.size, np.float32)
+        xk = c["xkap"][0]
+        for f in range(fs, fe + 1):
+            if iw[f] < 0:
+                continue
+            v = np.float32(0.0) + xk[iw[f]] * lag[f, 0]
+            v = v + xk[iw[f] + 1] * lag[f, 1]
+            if quad[f]:
+                v = v + xk[iw[f] + 2] * lag[f, 2]
+            ab[f] = v * np.float32(lam[f] ** 3) * np.float32(c["xkap_scale"])
+        want = _wcalc2_numpy(c, lam, cells, fs, fe, ab)
+        got, _ = oc.continuum_opacities([c], lam, nu, cells, sigma=False)
+        assert (want > 0).mean() > 0.2
+        np.testing.assert_array_equal(got, want)
+
+
+def test_h_occupation_without_perturbers(oc):
+    """No neutral perturbers and the charged term out of reach: wstar = 1 and w = 1,
+    so the dissolved states add nothing and beyond the limit the level adds its plain
+    bound-free opacity (to the rounding of the two products' orders)."""
+    comps, lam, nu, cells = synth.continuum_case(ncell=40, nlam=200)
+    cells = {k: v for k, v in cells.items() if k not in ("nHI", "partHI")}
+    cells["nHeI"] = np.zeros(40)
+    cells["shield"] = np.full(40, 1e10)
+    c = dict(comps[12])
+    c["n"] = np.zeros(40)
+    c["level_w"] = np.ones(40)
+    occ, _ = oc.continuum_opacities([c], lam, nu, cells, sigma=False)
+    plain = dict(c)
+    plain["occupation"] = False
+    ref, _ = oc.continuum_opacities([plain], lam, nu, cells, sigma=False)
+    edge = 911.267 * 4
+    below, beyond = lam > edge * 1.001, lam < edge * 0.999
+    assert np.all(occ[:, below] == 0)
+    np.testing.assert_allclose(occ[:, beyond], ref[:, beyond], rtol=1e-6)

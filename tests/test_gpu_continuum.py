@@ -1,6 +1,7 @@
 """The continuum opacity on the B200 (m3d_continuum_opacities) against the oracle
-(oracle/or_continuum.c) on the seeded case of synth.continuum_case: twelve
-components of every absorption-factor kind and interpolation form, a visible and an
+(oracle/or_continuum.c) on the seeded case of synth.continuum_case: fourteen
+components of every absorption-factor kind and interpolation form, two 'H BF'
+levels under occupation probabilities (wcalc2) among them, a visible and an
 ultraviolet window (the Rayleigh cut at 1400 A, tables covering the window in part).
 
 Bit-exact wherever both sides do the same IEEE operations: the interpolations, the
@@ -75,8 +76,8 @@ def test_continuum_each_component_bit_exact_or_to_the_ulp(m3d, oc):
         xo, _ = oc.continuum_opacities([c], lam, nu, cells, sigma=False)
         xg, _ = continuum_opacities([c], lam, nu, cells, sigma=False)
         assert xo.max() > 0, j
-        plain = c["kind"] in exact_kinds and not c.get("istim") and not (c["ilogl"] and not c["log_table"]) \
-            and not (c["tt"].size == 1 and c["ilogl"])
+        plain = (c["kind"] in exact_kinds or c.get("occupation")) and not c.get("istim") \
+            and not (c["ilogl"] and not c["log_table"]) and not (c["tt"].size == 1 and c["ilogl"])
         if plain:
             np.testing.assert_array_equal(xg, xo, err_msg=f"component {j}")
         else:
@@ -93,7 +94,8 @@ def test_continuum_device_pointers(m3d, oc):
     xh, sh = continuum_opacities(comps, lam, nu, cells)
     dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
     dc = {k: (dev(v) if isinstance(v, np.ndarray) else v) for k, v in cells.items()}
-    dcomps = [{k: (dev(v) if k in ("n", "n2", "part", "level_n") else v) for k, v in c.items()} for c in comps]
+    dcomps = [{k: (dev(v) if k in ("n", "n2", "part", "level_n", "level_w") else v) for k, v in c.items()}
+              for c in comps]
     xd, sd = continuum_opacities(dcomps, lam, nu, dc)
     torch.cuda.synchronize()
     np.testing.assert_array_equal(xd.cpu().numpy(), xh)
@@ -113,3 +115,30 @@ def test_continuum_rejects(m3d):
         continuum_opacities([bad], lam, nu, cells)
     with pytest.raises(m3d.M3DError, match="beta or nu"):
         continuum_opacities([comps[10]], lam, None, cells)
+    nosh = {k: v for k, v in cells.items() if k != "shield"}
+    with pytest.raises(m3d.M3DError, match="occupation"):
+        continuum_opacities([comps[12]], lam, nu, nosh)
+    bad = dict(comps[12])
+    bad.pop("level_w")
+    with pytest.raises(m3d.M3DError, match="NULL density"):
+        continuum_opacities([bad], lam, nu, cells)
+
+
+def test_continuum_h_occupation_levels(m3d, oc):
+    """The 'H BF' levels under occupation probabilities alone (no H rest), both
+    wavelength classes of wcalc2 and dissolved_only, bit for bit; and the same level
+    with its table given temperature nodes keeps absorption_factor's huge(1d0)."""
+    from dispatch_b200.continuum import continuum_opacities
+    comps, lam, nu, cells = synth.continuum_case(ncell=2000, nlam=256)
+    cells = {k: v for k, v in cells.items() if k not in ("nHI", "partHI")}
+    for c in comps[12:]:
+        xo, _ = oc.continuum_opacities([c], lam, nu, cells, sigma=False)
+        xg, _ = continuum_opacities([c], lam, nu, cells, sigma=False)
+        assert (xo > 0).mean() > 0.2
+        np.testing.assert_array_equal(xg, xo)
+    c = dict(comps[12])
+    c["tt"] = np.array([5000.0, 8000.0])
+    c["xkap"] = np.vstack([c["xkap"], c["xkap"]])
+    xo, _ = oc.continuum_opacities([c], lam, nu, cells, sigma=False)
+    xg, _ = continuum_opacities([c], lam, nu, cells, sigma=False)
+    np.testing.assert_array_equal(xg, xo)
