@@ -170,8 +170,8 @@ NCU_SWEEP_DRAM_BYTES_PER_CELL_FREQ = 8.013
 NCU_OPACITY_WARP_INST_PER_CELL_LINE = 751598136 / (110592 * 500)
 NCU_OPACITY_DRAM_READ_BYTES_PER_CELL = 5516032 / 110592
 #  k_continuum: warp instructions per cell of a launch of the continuum case (250
-#    frequencies, twelve components; 826,256,950 for 110,592 cells)
-NCU_CONTINUUM_WARP_INST_PER_CELL = 826256950 / 110592
+#    frequencies, fourteen components; 904,826,466 for 110,592 cells)
+NCU_CONTINUUM_WARP_INST_PER_CELL = 904826466 / 110592
 
 
 def _subcube(atm, n):
