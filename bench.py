@@ -50,7 +50,7 @@ def _args():
     p.add_argument("--cube", type=int, default=240, help="cube edge (240 = the configuration; smaller for profiling)")
     # single cases for timing and profiling one kernel family (no JSON line)
     p.add_argument("--case", default="c1",
-                   choices=["c1", "ali-window", "ali-columns", "optab", "c2", "batched", "continuum"],
+                   choices=["c1", "ali-window", "ali-columns", "optab", "c2", "batched", "continuum", "c0"],
                    help="c1: the headline (default); the others run one seeded NLTE or table case and print "
                         "per-iteration times")
     p.add_argument("--n", type=int, default=64, help="ali-window / optab / continuum: cube edge")
@@ -622,8 +622,9 @@ def _c0(m, a):
     """The 1D plane-parallel LTE synthesis configuration, measured beside the headline:
     80 depths, 2000 lines in 5000-5100 A, all 20000 frequencies in 625 windows of 32,
     5 Gauss-Legendre rays, long_char_quadratic, FP32 and the plain FP64 path; the CPU
-    restatement on a bounded sample of the windows.  Host-side window loop over the
-    device-resident column."""
+    restatement on a bounded sample of the windows.  All 625 windows in one
+    m3d_lte_synthesis_windows call over the device-resident column (one opacity
+    launch per ray for every window); beside it the same windows one call each."""
     import torch
     from dispatch_b200 import synth
     atm, _, _, vec, wmu = synth.lte_config("c0", nf=32, window=0)
@@ -633,25 +634,41 @@ def _c0(m, a):
     datm = {k: (dev(v) if isinstance(v, np.ndarray) else v) for k, v in atm.items()}
     datm["species"] = [{k: dev(v) for k, v in sp.items()} for sp in atm["species"]]
     wins = [tuple(dev(x) for x in _window(llam_all, nu_all, 32, w)) for w in range(nwin)]
+    nu_b, llam_b = dev(nu_all[:nwin * 32].reshape(nwin, 32)), dev(llam_all[:nwin * 32].reshape(nwin, 32))
     cur = torch.cuda.current_stream()
     out = {"workload": "c0 1D LTE synthesis: 80 depths, 2000 lines 5000-5100 A, 20000 frequencies (625 windows "
                        "of 32), 5 Gauss rays, long_char_quadratic", "unit": UNIT,
            "ray_pt_nu": 5 * 80 * 20000, "data": "synthetic (grey column, random line list)"}
     flux = {}
     for fp64 in (False, True):
-        for nu_d, llam_d in wins[:3]:
-            m.lte_synthesis(datm, nu_d, llam_d, vec, wmu, device=True, fp64=fp64)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        torch.cuda.synchronize()
-        e0.record(cur)
-        fl = [m.lte_synthesis(datm, nu_d, llam_d, vec, wmu, device=True, fp64=fp64)[1] for nu_d, llam_d in wins]
-        e1.record(cur)
-        torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1)
-        flux[fp64] = torch.cat(fl).double()
+        for _ in range(3):
+            m.lte_synthesis_windows(datm, nu_b, llam_b, vec, wmu, device=True, fp64=fp64)
+        ts = []
+        for _ in range(3):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(cur)
+            fl = m.lte_synthesis_windows(datm, nu_b, llam_b, vec, wmu, device=True, fp64=fp64)[1]
+            e1.record(cur)
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        ms = float(np.median(ts))
+        flux[fp64] = fl.double()
         out["fp64" if fp64 else "fp32"] = {"ms": ms, "value": out["ray_pt_nu"] / (ms / 1e3) / 1e9}
     out["fp32_over_fp64"] = out["fp32"]["value"] / out["fp64"]["value"]
     out["max_rel_flux_err_fp32_vs_fp64"] = float((torch.abs(flux[False] - flux[True]) / flux[True]).max().item())
+    # the same windows one m3d_lte_synthesis call each (FP32), and their flux against the batch's
+    for nu_d, llam_d in wins[:3]:
+        m.lte_synthesis(datm, nu_d, llam_d, vec, wmu, device=True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(cur)
+    fl = [m.lte_synthesis(datm, nu_d, llam_d, vec, wmu, device=True)[1] for nu_d, llam_d in wins]
+    e1.record(cur)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    out["fp32_one_call_per_window"] = {"ms": ms, "value": out["ray_pt_nu"] / (ms / 1e3) / 1e9,
+                                       "flux_equals_batch": bool(torch.equal(torch.cat(fl).double(), flux[False]))}
     # the CPU restatement: every 25th window, one process per window over all cores
     import multiprocessing as mp
     sample = list(range(0, nwin, 25))
@@ -1033,6 +1050,10 @@ def main():
         import dispatch_b200 as m
         m.init(0)
         print(json.dumps(_continuum(n=a.n)), flush=True)
+    elif a.case == "c0":
+        import dispatch_b200 as m
+        m.init(0)
+        print(json.dumps(_c0(m, a)), flush=True)
     elif a.case == "batched":
         import dispatch_b200 as m
         m.init(0)

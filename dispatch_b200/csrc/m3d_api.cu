@@ -1153,6 +1153,9 @@ struct SynthIn {
   const double *dnu = nullptr, *dllam = nullptr;
   int nf = 0;
   size_t ncell = 0;
+  // a batch of nwin windows of nf frequencies (nu, llam of nwin nf), each with its grid
+  int nwin = 1;
+  const GridArgs *d_Gw = nullptr;
 };
 
 int stage_synthesis(Staging &st, const m3d_atmos_t *atm, int nf, const double *nu, const double *llam, bool fp64,
@@ -1220,15 +1223,19 @@ int launch_opacity(SynthIn &in, const double *v, bool fp64, void *dchi, void *dS
   const int nf = in.nf;
   const size_t ncell = in.ncell;
   const int block = 256, warps = block / 32;
+  const bool batch = in.nwin > 1;
   if (fp64) {
-    int grid = (int)((ncell + block - 1) / block);
+    int grid = (int)((ncell * in.nwin + block - 1) / block);
     if (grid > 148 * 8) grid = 148 * 8;
-    if (nf == 32)
+    if (batch)
+      LAUNCH_S(M3D_STAGE_OPACITY, (k_lte_opacity_units_f64<32, true>), grid, block, 0, in.A, in.G, in.dnu, v[0], v[1],
+               v[2], (double *)dchi, (double *)dS, (const double2 *)g_ctx.d_tab64, in.d_Gw, in.nwin);
+    else if (nf == 32)
       LAUNCH_S(M3D_STAGE_OPACITY, k_lte_opacity_units_f64<32>, grid, block, 0, in.A, in.G, in.dnu, v[0], v[1], v[2],
-               (double *)dchi, (double *)dS, (const double2 *)g_ctx.d_tab64);
+               (double *)dchi, (double *)dS, (const double2 *)g_ctx.d_tab64, (const GridArgs *)nullptr, 1);
     else
       LAUNCH_S(M3D_STAGE_OPACITY, k_lte_opacity_units_f64<0>, grid, block, 0, in.A, in.G, in.dnu, v[0], v[1], v[2],
-               (double *)dchi, (double *)dS, (const double2 *)g_ctx.d_tab64);
+               (double *)dchi, (double *)dS, (const double2 *)g_ctx.d_tab64, (const GridArgs *)nullptr, 1);
     return M3D_OK;
   }
   const bool lane32 = nf == 32;
@@ -1242,6 +1249,8 @@ int launch_opacity(SynthIn &in, const double *v, bool fp64, void *dchi, void *dS
         CUDA_TRY(cudaFuncSetAttribute((const void *)k_lte_opacity_units_lane<32, float, false>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_op));
         CUDA_TRY(cudaFuncSetAttribute((const void *)k_lte_opacity_units_lane<32, float, true>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_op));
+        CUDA_TRY(cudaFuncSetAttribute((const void *)k_lte_opacity_units_lane<32, float, false, false, true>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_op));
       } else {
         CUDA_TRY(cudaFuncSetAttribute((const void *)k_lte_opacity_units<float>,
@@ -1258,15 +1267,19 @@ int launch_opacity(SynthIn &in, const double *v, bool fp64, void *dchi, void *dS
              in.d_nsel[k]);
   }
   if (lane32) {
-    // lane kernel: one warp per 32 cells, grid-stride over warps
-    int lgrid = (int)((ncell + block - 1) / block);
+    // lane kernel: one warp per 32 cells (of one window), grid-stride over warps
+    const size_t nvc = (ncell + 31) / 32 * 32 * (size_t)in.nwin;
+    int lgrid = (int)((nvc + block - 1) / block);
     if (lgrid > 148 * 3 * 8) lgrid = 148 * 3 * 8;
-    if (in.reach)
+    if (batch)
+      LAUNCH_S(M3D_STAGE_OPACITY, (k_lte_opacity_units_lane<32, float, false, false, true>), lgrid, block, smem_op,
+               in.A, in.G, in.dnu, v[0], v[1], v[2], (float *)dchi, (float *)dS, g_ctx.d_tab, in.d_Gw, in.nwin);
+    else if (in.reach)
       LAUNCH_S(M3D_STAGE_OPACITY, (k_lte_opacity_units_lane<32, float, true>), lgrid, block, smem_op, in.A, in.G,
-               in.dnu, v[0], v[1], v[2], (float *)dchi, (float *)dS, g_ctx.d_tab);
+               in.dnu, v[0], v[1], v[2], (float *)dchi, (float *)dS, g_ctx.d_tab, (const GridArgs *)nullptr, 1);
     else
       LAUNCH_S(M3D_STAGE_OPACITY, (k_lte_opacity_units_lane<32, float, false>), lgrid, block, smem_op, in.A, in.G,
-               in.dnu, v[0], v[1], v[2], (float *)dchi, (float *)dS, g_ctx.d_tab);
+               in.dnu, v[0], v[1], v[2], (float *)dchi, (float *)dS, g_ctx.d_tab, (const GridArgs *)nullptr, 1);
   } else {
     int ogrid = (int)((ncell + warps - 1) / warps);
     if (ogrid > 148 * 16) ogrid = 148 * 16;
@@ -1282,6 +1295,10 @@ int check_synthesis_args(const m3d_atmos_t *atm, int nf, const char *who) {
   if (atm->nx < 1 || atm->ny < 1 || atm->nz < 1) return fail(M3D_EINVAL, "%s: bad atmosphere shape", who);
   return M3D_OK;
 }
+
+int lte_synthesis_impl(const m3d_atmos_t *atm, int nwin, int nf_win, const double *nu, const double *llam, int nray,
+                       const double *vec, const double *wmu, void *i_top, float *ie, float *flux, unsigned flags,
+                       const char *who);
 
 }  // namespace
 
@@ -1315,10 +1332,35 @@ int m3d_lte_transfer_units(const m3d_atmos_t *atm, int nf, const double *nu, con
 
 int m3d_lte_synthesis(const m3d_atmos_t *atm, int nf, const double *nu, const double *llam, int nray,
                       const double *vec, const double *wmu, void *i_top, float *ie, float *flux, unsigned flags) {
+  return lte_synthesis_impl(atm, 1, nf, nu, llam, nray, vec, wmu, i_top, ie, flux, flags, "m3d_lte_synthesis");
+}
+
+int m3d_lte_synthesis_windows(const m3d_atmos_t *atm, int nwin, int nf, const double *nu, const double *llam,
+                              int nray, const double *vec, const double *wmu, void *i_top, float *ie, float *flux,
+                              unsigned flags) {
+  return lte_synthesis_impl(atm, nwin, nf, nu, llam, nray, vec, wmu, i_top, ie, flux, flags,
+                            "m3d_lte_synthesis_windows");
+}
+
+}  // extern "C"
+
+namespace {
+
+// m3d_lte_synthesis for nwin consecutive windows of nf frequencies at once (nwin = 1:
+// one window).  The windows' transfer units are laid out as the rows of one window
+// of nwin nf frequencies, which the sweep, the reduction and the flux take as such:
+// each frequency's arithmetic is the single window's.
+int lte_synthesis_impl(const m3d_atmos_t *atm, int nwin, int nf_win, const double *nu, const double *llam, int nray,
+                       const double *vec, const double *wmu, void *i_top, float *ie, float *flux, unsigned flags,
+                       const char *who) {
   TRY(need_init());
-  if (!atm || !nu || !llam || !vec || !wmu || !ie || !flux) return fail(M3D_EINVAL, "m3d_lte_synthesis: NULL argument");
-  if (nray < 1) return fail(M3D_EINVAL, "m3d_lte_synthesis: need nray >= 1");
-  TRY(check_synthesis_args(atm, nf, "m3d_lte_synthesis"));
+  if (!atm || !nu || !llam || !vec || !wmu || !ie || !flux) return fail(M3D_EINVAL, "%s: NULL argument", who);
+  if (nray < 1) return fail(M3D_EINVAL, "%s: need nray >= 1", who);
+  if (nwin < 1) return fail(M3D_EINVAL, "%s: need nwin >= 1", who);
+  TRY(check_synthesis_args(atm, nf_win, who));
+  if (nwin > 1 && nf_win != 32) return fail(M3D_EUNSUPPORTED, "%s: window batches of nf = 32 only", who);
+  if ((size_t)nwin * nf_win > (size_t)INT_MAX / 2) return fail(M3D_EUNSUPPORTED, "%s: %d windows", who, nwin);
+  const int nf = nwin * nf_win;   // the frequencies of all windows, one after the other
   const int nx = atm->nx, ny = atm->ny, nz = atm->nz;
   if (nz < 2 || atm->nslab < 1 || !atm->slab_nz) return fail(M3D_EINVAL, "m3d_lte_synthesis: bad atmosphere shape");
   std::vector<int> z0(atm->nslab + 1, 0);
@@ -1335,8 +1377,33 @@ int m3d_lte_synthesis(const m3d_atmos_t *atm, int nf, const double *nu, const do
 
   Staging st(flags);
   SynthIn in;
-  TRY(stage_synthesis(st, atm, nf, nu, llam, fp64, "m3d_lte_synthesis", &in));
+  TRY(stage_synthesis(st, atm, nf, nu, llam, fp64, who, &in));
   const double *dnu = in.dnu;
+  if (nwin > 1) {
+    // every window's grid, as a call for that window alone forms it
+    if (in.reach) return fail(M3D_EUNSUPPORTED, "%s: reach_in with window batches", who);
+    if ((in.ncell + 31) / 32 * 32 * (size_t)nwin > (size_t)INT_MAX)
+      return fail(M3D_EUNSUPPORTED, "%s: %zu cells x %d windows", who, in.ncell, nwin);
+    std::vector<double> hl((size_t)nf);
+    if (st.device()) {
+      CUDA_TRY(cudaMemcpyAsync(hl.data(), llam, sizeof(double) * hl.size(), cudaMemcpyDeviceToHost, g_ctx.stream));
+      CUDA_TRY(cudaStreamSynchronize(g_ctx.stream));
+    } else {
+      memcpy(hl.data(), llam, sizeof(double) * hl.size());
+    }
+    std::vector<GridArgs> gw(nwin);
+    for (int w = 0; w < nwin; w++) {
+      gw[w] = grid_args(nf_win, hl.data() + (size_t)nf_win * w, in.dllam + (size_t)nf_win * w, false,
+                        (float)atm->tol, 0.0f);
+      if (!(gw[w].dllam > 0)) return fail(M3D_EINVAL, "%s: window %d: log(lambda) must be ascending", who, w);
+    }
+    void *dgw;
+    TRY(scratch(25, sizeof(GridArgs) * gw.size(), &dgw));
+    CUDA_TRY(cudaMemcpyAsync(dgw, gw.data(), sizeof(GridArgs) * gw.size(), cudaMemcpyHostToDevice, g_ctx.stream));
+    in.nf = nf_win;
+    in.nwin = nwin;
+    in.d_Gw = (const GridArgs *)dgw;
+  }
 
   // rotation table of every global plane, per ray; slab starts
   // A single column is a plane-parallel atmosphere: radiative_transfer applies no
@@ -1473,7 +1540,7 @@ int m3d_lte_synthesis(const m3d_atmos_t *atm, int nf, const double *nu, const do
   return M3D_OK;
 }
 
-}  // extern "C"
+}  // namespace
 
 #include "m3d_stateq_api.inc"
 #include "m3d_nlte_api.inc"

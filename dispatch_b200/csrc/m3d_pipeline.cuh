@@ -318,19 +318,30 @@ __device__ __forceinline__ float pick(const float (&a)[NF], int i) {
 // end, no peak test and a window capped by their reach (linelist_mod.f90:844-854, 914-921)
 // CHIL: write the line opacity chi_l of the window itself to chi_out (S_out unused):
 // the input of the adjoint's transfer units
-template <int NF, typename TO, bool REACH, bool CHIL = false>
-__global__ void __launch_bounds__(256, 3) k_lte_opacity_units_lane(AtmosDev A, GridArgs G, const double *nu, double v0,
+// BATCH: nwin windows of NF frequencies in one launch, each with its own grid Gw[w]
+// and frequencies nu + w NF; the warps run over (window, cell) with the cells of a
+// window padded to whole warps, so a warp holds one window, and a cell's row of
+// every window goes to chi_out + nwin NF cell + w NF: the rows of one window of
+// nwin NF frequencies, which the column solvers take as they are
+template <int NF, typename TO, bool REACH, bool CHIL = false, bool BATCH = false>
+__global__ void __launch_bounds__(256, 3) k_lte_opacity_units_lane(AtmosDev A, GridArgs G0, const double *nu0, double v0,
                                                                    double v1, double v2, TO *chi_out, TO *S_out,
-                                                                   const float2 *tab) {
+                                                                   const float2 *tab, const GridArgs *Gw, int nwin) {
   extern __shared__ float smem[];
   float2 *s_tab = reinterpret_cast<float2 *>(smem);
   stage_tables(s_tab, tab);
   const float ex_cutoff = -85.0f, voigt_peak = 0.5641895835f, sqrt_pi = 1.7724538509f;
-  const float lt = logf_m3d(G.tol / voigt_peak);
+  const float lt = logf_m3d(G0.tol / voigt_peak);
   const int ncell = A.ncell;
   const int nthreads = gridDim.x * blockDim.x;
   const int ncell_pad = (ncell + 31) / 32 * 32;
-  for (int cell = blockIdx.x * blockDim.x + threadIdx.x; cell < ncell_pad; cell += nthreads) {
+  const int nvc = BATCH ? ncell_pad * nwin : ncell_pad;
+  for (int vc = blockIdx.x * blockDim.x + threadIdx.x; vc < nvc; vc += nthreads) {
+    const int w = BATCH ? vc / ncell_pad : 0;
+    const int cell = BATCH ? vc - w * ncell_pad : vc;
+    const GridArgs G = BATCH ? Gw[w] : G0;
+    const double *nu = BATCH ? nu0 + (size_t)NF * w : nu0;
+    const size_t row = BATCH ? (size_t)NF * nwin * cell + (size_t)NF * w : (size_t)NF * cell;
     const bool live = cell < ncell;
     const int cs = live ? cell : ncell - 1;
     const float T = A.temp[cs], chi_c = A.chi_c[cs];
@@ -429,7 +440,7 @@ __global__ void __launch_bounds__(256, 3) k_lte_opacity_units_lane(AtmosDev A, G
     }
     if (CHIL) {
       if (live) {
-        float *co = reinterpret_cast<float *>(chi_out) + (size_t)NF * cell;
+        float *co = reinterpret_cast<float *>(chi_out) + row;
 #pragma unroll
         for (int f = 0; f < NF; f += 4)
           *reinterpret_cast<float4 *>(co + f) = make_float4(chl[f], chl[f + 1], chl[f + 2], chl[f + 3]);
@@ -438,7 +449,7 @@ __global__ void __launch_bounds__(256, 3) k_lte_opacity_units_lane(AtmosDev A, G
     }
     // epilogue: transfer units, written as 16-byte stores of this cell's row
     if (live) {
-      TO *co = chi_out + (size_t)NF * cell, *so = S_out + (size_t)NF * cell;
+      TO *co = chi_out + row, *so = S_out + row;
 #pragma unroll
       for (int f = 0; f < NF; f += 4) {
         TO c4[4], s4[4];
@@ -537,18 +548,27 @@ struct ChlF64<0> {
   __device__ __forceinline__ double &operator[](int i) { return p[i]; }
 };
 
-template <int NF>
-__global__ void __launch_bounds__(256) k_lte_opacity_units_f64(AtmosDev A, GridArgs G, const double *nu, double v0,
+// BATCH: nwin windows in one launch, as k_lte_opacity_units_lane<..., BATCH> (NF > 0)
+template <int NF, bool BATCH = false>
+__global__ void __launch_bounds__(256) k_lte_opacity_units_f64(AtmosDev A, GridArgs G0, const double *nu0, double v0,
                                                                double v1, double v2, double *chi_out, double *S_out,
-                                                               const double2 *tab) {
+                                                               const double2 *tab, const GridArgs *Gw, int nwin) {
+  static_assert(!BATCH || NF > 0, "window batches of a fixed window size");
   const double ex_cutoff = -85.0, voigt_peak = 0.56418958354775628, sqrt_pi = 1.7724538509055160;
-  const double tol = (double)G.tol, sdl = G.inv_dllam, flo_scale = (double)G.flo_scale;
+  const double tol = (double)G0.tol, flo_scale = (double)G0.flo_scale;
   const double lt = log(tol / voigt_peak);
   const int ncell = A.ncell;
-  const int nf = NF > 0 ? NF : G.nf;
-  for (int cell = blockIdx.x * blockDim.x + threadIdx.x; cell < ncell; cell += gridDim.x * blockDim.x) {
+  const int nf = NF > 0 ? NF : G0.nf;
+  const int nvc = BATCH ? ncell * nwin : ncell;
+  for (int vc = blockIdx.x * blockDim.x + threadIdx.x; vc < nvc; vc += gridDim.x * blockDim.x) {
+    const int w = BATCH ? vc / ncell : 0;
+    const int cell = BATCH ? vc - w * ncell : vc;
+    const GridArgs G = BATCH ? Gw[w] : G0;
+    const double *nu = BATCH ? nu0 + (size_t)nf * w : nu0;
+    const double sdl = G.inv_dllam;
     const double T = A.temp[cell], chi_c = A.chi_c[cell];
-    double *co = chi_out + (size_t)nf * cell, *so = S_out + (size_t)nf * cell;
+    const size_t row = BATCH ? (size_t)nf * nwin * cell + (size_t)nf * w : (size_t)nf * cell;
+    double *co = chi_out + row, *so = S_out + row;
     ChlF64<NF> chl(co);
 #pragma unroll
     for (int f = 0; f < nf; f++) chl[f] = 0.0;

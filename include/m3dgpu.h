@@ -424,6 +424,19 @@ int m3d_lte_synthesis(const m3d_atmos_t *atm, int nf, const double *nu, const do
                       int nray, const double *vec, const double *wmu, void *i_top, float *ie,
                       float *flux, unsigned flags);
 
+/* m3d_lte_synthesis over nwin windows of nf = 32 frequencies in one call, the
+ * reference's n_windows loop (ray_patch_mod.f90:97-127) with its windows on the
+ * device at once: nu and llam (nwin x nf) hold the windows one after the other, each
+ * window's grid formed from its own frequencies; ie (nray, nwin nf), flux (nwin nf),
+ * i_top (nray, ny, nx, nwin nf).  Equal bit for bit to one m3d_lte_synthesis call per
+ * window.  For atmospheres too small to fill the GPU with one window (a 1D column of
+ * 80 depths is three warps per window), where it runs every window's opacity in one
+ * launch per ray; the transfer units of all windows are held at once (8 B per cell
+ * and frequency of the batch).  No reach_in. */
+int m3d_lte_synthesis_windows(const m3d_atmos_t *atm, int nwin, int nf, const double *nu, const double *llam,
+                              int nray, const double *vec, const double *wmu, void *i_top, float *ie,
+                              float *flux, unsigned flags);
+
 /* ---- libhop's opacity call ----
  * m3d_hop_set_state loads a state for m3d_hop_opacity (host copies; the calling
  * thread's; velocities, slabs and geometry are ignored): the cells' e_kT, ne, tothi,
