@@ -259,6 +259,10 @@ __device__ __forceinline__ void rate_chunk_sum(float (*T)[33], int lane, int cnt
 // a cell at a time with all 32 lanes along f (one 128-byte load per array), written
 // to shared memory, and lane k adds cell k's terms in ascending f -- the
 // reference's order.  A line window of up to 32 points takes a single chunk.
+// The tiles run cell-major: the lines of 16 cells are neighbouring warps, so the
+// sectors their windows share (and those a window straddles) are read from DRAM
+// once and from L2 after.  Each (line, cell) has one writer, so the order changes
+// no sum.
 constexpr int kBbWarps = 4, kBbCells = 16;
 
 __global__ void __launch_bounds__(kBbWarps * 32)
@@ -278,7 +282,7 @@ k_bb_rates(NlWinDev W, NlRateOpts O, int ncell, const double *__restrict__ b,
   const size_t ntile = (size_t)ctiles * W.nline;
   const size_t stride = (size_t)gridDim.x * kBbWarps;
   for (size_t tt = (size_t)blockIdx.x * kBbWarps + wib; tt < ntile; tt += stride) {
-    const int i = (int)(tt / ctiles), c0 = (int)(tt % ctiles) * kBbCells;
+    const int i = (int)(tt % W.nline), c0 = (int)(tt / W.nline) * kBbCells;
     if (W.lactive && !W.lactive[i]) continue;
     const int li = W.li[i], lj = W.lj[i], fs = W.lblue[i], fe = W.lred[i], off = W.loff[i];
     const bool own_norm = O.per_direction && !W.lsums[i];
