@@ -167,6 +167,9 @@ def _peaks():
 #    Snu it writes, 8 B per frequency (the small case's 28 MB of output stayed in L2,
 #    a full launch's 3.5 GB cannot).
 NCU_SWEEP_DRAM_BYTES_PER_CELL_FREQ = 8.013
+#  k_quad_rot_column2: warp instructions per (cell, frequency) of a launch
+#    (21,865,784 for 110,592 cells x 32 frequencies)
+NCU_SWEEP_WARP_INST_PER_CELL_FREQ = 21865784 / (110592 * 32)
 NCU_OPACITY_WARP_INST_PER_CELL_LINE = 751598136 / (110592 * 500)
 NCU_OPACITY_DRAM_READ_BYTES_PER_CELL = 5516032 / 110592
 #  k_continuum: warp instructions per cell of a launch of the continuum case (250
@@ -789,6 +792,15 @@ def run_b200(a):
                       "frac": achieved / peak if achieved else None,
                       "traffic": NCU_SWEEP_DRAM_BYTES_PER_CELL_FREQ * ncell * nf, "peak_source": peak_kind,
                       "algorithmic_bytes_per_launch": bytes_launch}
+    # the same launch against instruction issue, the bound its arithmetic sets: the
+    # quadratic step's real(4) operations are the reference's
+    sv_inst = NCU_SWEEP_WARP_INST_PER_CELL_FREQ * ncell * nf
+    sv_launch_s = sv_ms / sv_n / 1e3 if sv_n else None
+    roofline_sweep["issue_view"] = {"warp_instructions_per_launch": sv_inst,
+                                    "achieved": sv_inst / sv_launch_s / 1e9 if sv_launch_s else None,
+                                    "peak": issue_peak, "unit": "G warp-instructions/s",
+                                    "frac": sv_inst / sv_launch_s / 1e9 / issue_peak if sv_launch_s else None,
+                                    "hbm_frac_at_full_issue": 8.0 * ncell * nf / (sv_inst / issue_peak) / peak}
     stages = {"opacity_ms_per_step": op_ms, "opacity_launches": op_n, "solve_ms_per_step": sv_ms,
               "solve_launches": sv_n, "reduce_ms_per_step": rd_ms,
               "solve_gpt_per_s": work_per_step / (sv_ms / 1e3) / 1e9 if sv_ms else None}
