@@ -146,11 +146,14 @@ __device__ __forceinline__ float optab_collapse_node(const float4 *t, size_t bas
 }
 
 constexpr int kOptabWarps = 8;
+// both samplers are latency-bound: at most 64 registers give 4 blocks (32 warps) per
+// SM, measured faster than 66-77 registers at 3 blocks and than 48 or 40 with spills
+constexpr int kOptabMinBlocks = 4;
 constexpr int kOptabUnroll = 2;   // frequencies per lane per pass of sample_interpolate_ll
 
 // sample_interpolate (optab_mod.f90:181-287): one warp per cell, lanes over the
 // frequencies; back = (kappa + kappa_scat) chi500, scat = kappa_scat chi500
-__global__ void __launch_bounds__(32 * kOptabWarps) k_optab_sample(OptabDev T, int nf, long long ncell,
+__global__ void __launch_bounds__(32 * kOptabWarps, kOptabMinBlocks) k_optab_sample(OptabDev T, int nf, long long ncell,
                                                                    const double *temp, const double *ne,
                                                                    const float *chi500, const OptabFreq *fc,
                                                                    float *back, float *scat) {
@@ -188,7 +191,7 @@ __global__ void __launch_bounds__(32 * kOptabWarps) k_optab_sample(OptabDev T, i
 // A lane takes kOptabUnroll frequencies per pass: their work slots are read and
 // their brackets found before the table lookups, so the slow reads of the slots
 // and of the wavelength nodes are in flight together.
-__global__ void __launch_bounds__(32 * kOptabWarps) k_optab_sample_ll(OptabDev T, int nf, long long ncell,
+__global__ void __launch_bounds__(32 * kOptabWarps, kOptabMinBlocks) k_optab_sample_ll(OptabDev T, int nf, long long ncell,
                                                                       const double *temp, const double *ne,
                                                                       const float *chi500, const float *vproj,
                                                                       const double *lam_q, const OptabFreq *fc,
