@@ -154,5 +154,30 @@ def continuum_opacities(comps: list, lam, nu, cells: dict, beta=None, sigma: boo
     return xhat, sg
 
 
-__all__ = ["continuum_opacities", "set_table", "BfComp", "ContCells", "HMINUS", "NPE", "H", "H_FF", "PAIR",
+def opacity(comps: list, lam, nu, cells: dict, beta=None, include_llist: bool = True, line_margin: float = 100.0,
+            disjoint: bool = False):
+    """composition_type%opacity (HOP/composition_mod.f90:3122-3260) through
+    m3d_opacity: the continuum of comps and cells, the line list of the state loaded
+    with hop_set_state (same cells) against it, and the conversion to physical
+    extinction.  Returns (chi, scat), each (ncell, nlam) float32: chi the total
+    extinction (the true absorption alone with disjoint), scat electron + Rayleigh
+    scattering.  Host arrays."""
+    init()
+    lam = np.ascontiguousarray(lam, np.float64)
+    nu = np.ascontiguousarray(nu, np.float64)
+    ncell, nlam = int(np.asarray(cells["temp"]).shape[0]), int(lam.size)
+    arr, keep = make_comps(comps, False)
+    cs, keep2 = make_cells(cells, False)
+    chi = np.empty((ncell, nlam), np.float32)
+    scat = np.empty_like(chi)
+    beta = None if beta is None else np.ascontiguousarray(beta, np.float32)
+    check(lib().m3d_opacity(C.c_int(nlam), C.c_void_p(lam.ctypes.data), C.c_void_p(nu.ctypes.data),
+                            C.c_int(len(comps)), arr, C.byref(cs), ptr(beta), ptr(chi), ptr(scat),
+                            C.c_int(int(bool(include_llist))), C.c_double(line_margin), C.c_int(int(bool(disjoint)))),
+          "m3d_opacity")
+    del keep, keep2
+    return chi, scat
+
+
+__all__ = ["continuum_opacities", "opacity", "set_table", "BfComp", "ContCells", "HMINUS", "NPE", "H", "H_FF", "PAIR",
            "H2PLUS", "PEDEP", "PEACH", "MOLECULAR", "REGULAR"]

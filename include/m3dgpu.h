@@ -557,6 +557,22 @@ int m3d_continuum_opacities(int ncomp, const m3d_bf_comp_t *comps, int nlam, con
                             int ncell, const m3d_cont_cells_t *cells, const float *beta, float *xhat, float *sigma,
                             unsigned flags);
 
+/* composition_type%opacity (composition_mod.f90:3122-3260), the whole pipeline that
+ * hop.opacity() and chi500 call, over the cells of the loaded state: beta (the
+ * caller's (nlam, n), or NULL: boltzmann_factor from nu and cells->temp);
+ * continuum_opacities of the components and cells (m3d_continuum_opacities) into the
+ * working xhat and the scattering opacity; with include_llist the line list of the
+ * state, the lines within line_margin [AA], against that xhat as the tolerance
+ * reference (as m3d_hop_opacity adds it, no velocities); then the one conversion to
+ * physical extinction, chi = xhat - ehat beta (the continuum alone: xhat (1 - beta)),
+ * plus the scattering opacity unless disjoint.  scat = electron + Rayleigh scattering.
+ * lam (nlam) [AA] ascending (uniform in ln(lambda) with the line list), nu (nlam)
+ * [Hz]; chi, scat (nlam, n); host buffers.  No absmet, no line scattering split (the
+ * reference's include_absmet and line_scat off). */
+int m3d_opacity(int nlam, const double *lam, const double *nu, int ncomp, const m3d_bf_comp_t *comps,
+                const m3d_cont_cells_t *cells, const float *beta, float *chi, float *scat, int include_llist,
+                double line_margin, int disjoint);
+
 /* ---- statistical equilibrium (FP64) ----
  * Level and transition indices are 0-based (the reference's minus one).  Per-cell
  * arrays keep the cell index fastest: b(cell, level) at b[cell + ncell*level], as
