@@ -171,7 +171,7 @@ def opacity(comps: list, lam, nu, cells: dict, beta=None, include_llist: bool = 
     chi = np.empty((ncell, nlam), np.float32)
     scat = np.empty_like(chi)
     beta = None if beta is None else np.ascontiguousarray(beta, np.float32)
-    check(lib().m3d_opacity(C.c_int(nlam), C.c_void_p(lam.ctypes.data), C.c_void_p(nu.ctypes.data),
+    check(lib().m3d_opacity(C.c_int(nlam), C.c_void_p(lam.ctypes.data), C.c_void_p(nu.ctypes.data), C.c_int(ncell),
                             C.c_int(len(comps)), arr, C.byref(cs), ptr(beta), ptr(chi), ptr(scat),
                             C.c_int(int(bool(include_llist))), C.c_double(line_margin), C.c_int(int(bool(disjoint)))),
           "m3d_opacity")
@@ -179,5 +179,31 @@ def opacity(comps: list, lam, nu, cells: dict, beta=None, include_llist: bool = 
     return chi, scat
 
 
-__all__ = ["continuum_opacities", "opacity", "set_table", "BfComp", "ContCells", "HMINUS", "NPE", "H", "H_FF", "PAIR",
+def airvac_corr(lam):
+    """The refractive index of air at wavelength lam [AA] (HOP/handyfuncs_mod.f90:437-445),
+    the published formula VALD uses (Piskunov, after Ciddor 1996)."""
+    s2 = (1e4 / np.asarray(lam, np.float64)) ** 2
+    return 1.00008336624212083 + 0.02408926869968 / (130.1065924522 - s2) + 0.0001599740894897 / (38.92568793293 - s2)
+
+
+def air2vac(air):
+    """Vacuum wavelength [AA] of the air wavelength air [AA]: the index evaluated at the
+    vacuum wavelength by three substitutions (HOP/handyfuncs_mod.f90:424-431)."""
+    air = np.asarray(air, np.float64)
+    w = air * airvac_corr(air)
+    w = air * airvac_corr(w)
+    return air * airvac_corr(w)
+
+
+def chi500(comps: list, cells: dict, ref_lam: float = 5000.0):
+    """load_state_variables' reference opacity (HOP/composition_mod.f90:2169-2176): the
+    total extinction at the vacuum wavelength of ref_lam [AA] air, continuum and
+    scattering without the line list (ncell,), float32."""
+    lam = np.atleast_1d(air2vac(ref_lam))
+    nu = (2.99792458e10 / 1e-8) / lam       # HZ_TO_AA / lambda (const_mod.f90:57)
+    chi, _ = opacity(comps, lam, nu, cells, include_llist=False)
+    return chi[:, 0]
+
+
+__all__ = ["continuum_opacities", "opacity", "chi500", "air2vac", "set_table", "BfComp", "ContCells", "HMINUS", "NPE", "H", "H_FF", "PAIR",
            "H2PLUS", "PEDEP", "PEACH", "MOLECULAR", "REGULAR"]

@@ -558,18 +558,21 @@ int m3d_continuum_opacities(int ncomp, const m3d_bf_comp_t *comps, int nlam, con
                             unsigned flags);
 
 /* composition_type%opacity (composition_mod.f90:3122-3260), the whole pipeline that
- * hop.opacity() and chi500 call, over the cells of the loaded state: beta (the
- * caller's (nlam, n), or NULL: boltzmann_factor from nu and cells->temp);
+ * hop.opacity() and chi500 call, over ncell cells (those of the loaded state with
+ * include_llist): beta (the caller's (nlam, ncell), or NULL: boltzmann_factor from nu
+ * and cells->temp);
  * continuum_opacities of the components and cells (m3d_continuum_opacities) into the
  * working xhat and the scattering opacity; with include_llist the line list of the
  * state, the lines within line_margin [AA], against that xhat as the tolerance
  * reference (as m3d_hop_opacity adds it, no velocities); then the one conversion to
  * physical extinction, chi = xhat - ehat beta (the continuum alone: xhat (1 - beta)),
- * plus the scattering opacity unless disjoint.  scat = electron + Rayleigh scattering.
- * lam (nlam) [AA] ascending (uniform in ln(lambda) with the line list), nu (nlam)
- * [Hz]; chi, scat (nlam, n); host buffers.  No absmet, no line scattering split (the
- * reference's include_absmet and line_scat off). */
-int m3d_opacity(int nlam, const double *lam, const double *nu, int ncomp, const m3d_bf_comp_t *comps,
+ * plus the scattering opacity unless disjoint.  scat (or NULL) = electron + Rayleigh
+ * scattering.  lam (nlam) [AA] ascending (uniform in ln(lambda) with the line list,
+ * nlam >= 2 then), nu (nlam) [Hz]; chi, scat (nlam, ncell); host buffers.  No absmet,
+ * no line scattering split (the reference's include_absmet and line_scat off).
+ * chi500, load_state_variables' reference opacity (composition_mod.f90:2169-2176), is
+ * this call at the one vacuum wavelength of 5000 A air without the line list. */
+int m3d_opacity(int nlam, const double *lam, const double *nu, int ncell, int ncomp, const m3d_bf_comp_t *comps,
                 const m3d_cont_cells_t *cells, const float *beta, float *chi, float *scat, int include_llist,
                 double line_margin, int disjoint);
 

@@ -82,3 +82,20 @@ def test_opacity_full_case_beta_from_nu(m3d, oracle):
     np.testing.assert_allclose(chi, want, rtol=1e-5)
     with pytest.raises(m3d.M3DError, match="uniform in ln"):
         opacity(comps, np.linspace(lam[0], lam[-1] * 1.01, lam.size), nu, cells)
+
+
+def test_chi500(m3d):
+    """load_state_variables' chi500: the pipeline at one wavelength without the line
+    list, needing no loaded state; equal to the continuum's xhat (1 - beta) + sigma."""
+    from dispatch_b200.continuum import air2vac, chi500, continuum_opacities
+    m3d.lib().m3d_hop_free_state()   # chi500 needs no line list
+    comps, _, _, cells = synth.continuum_case(ncell=700, nlam=8)
+    c5 = chi500(comps, cells)
+    assert c5.shape == (700,) and np.all(np.isfinite(c5)) and np.all(c5 > 0)
+    lam = np.atleast_1d(air2vac(5000.0))
+    assert 5001.0 < lam[0] < 5002.0              # 5000 A air is 5001.40 A vacuum
+    nu = (2.99792458e10 / 1e-8) / lam
+    xh, sg = continuum_opacities(comps, lam, nu, cells)
+    hk = 6.626176e-27 / 1.380662e-16
+    beta = np.maximum(np.exp(-nu[0] * (hk / cells["temp"])), np.finfo(np.float32).tiny).astype(np.float32)
+    np.testing.assert_allclose(c5, xh[:, 0] * (np.float32(1) - beta) + sg[:, 0], rtol=1e-5)
