@@ -1153,9 +1153,12 @@ struct SynthIn {
   const double *dnu = nullptr, *dllam = nullptr;
   int nf = 0;
   size_t ncell = 0;
-  // a batch of nwin windows of nf frequencies (nu, llam of nwin nf), each with its grid
+  // a batch of nwin windows of nf frequencies (nu, llam of nwin nf), each with its grid,
+  // for nray directions d_vr (3 each) in one launch
   int nwin = 1;
   const GridArgs *d_Gw = nullptr;
+  int nray = 1;
+  const double *d_vr = nullptr;
 };
 
 int stage_synthesis(Staging &st, const m3d_atmos_t *atm, int nf, const double *nu, const double *llam, bool fp64,
@@ -1225,17 +1228,19 @@ int launch_opacity(SynthIn &in, const double *v, bool fp64, void *dchi, void *dS
   const int block = 256, warps = block / 32;
   const bool batch = in.nwin > 1;
   if (fp64) {
-    int grid = (int)((ncell * in.nwin + block - 1) / block);
+    int grid = (int)((ncell * in.nwin * (batch ? in.nray : 1) + block - 1) / block);
     if (grid > 148 * 8) grid = 148 * 8;
     if (batch)
-      LAUNCH_S(M3D_STAGE_OPACITY, (k_lte_opacity_units_f64<32, true>), grid, block, 0, in.A, in.G, in.dnu, v[0], v[1],
-               v[2], (double *)dchi, (double *)dS, (const double2 *)g_ctx.d_tab64, in.d_Gw, in.nwin);
+      LAUNCH_S(M3D_STAGE_OPACITY, (k_lte_opacity_units_f64<32, true>), grid, block, 0, in.A, in.G, in.dnu, 0.0, 0.0,
+               0.0, (double *)dchi, (double *)dS, (const double2 *)g_ctx.d_tab64, in.d_Gw, in.nwin, in.d_vr, in.nray);
     else if (nf == 32)
       LAUNCH_S(M3D_STAGE_OPACITY, k_lte_opacity_units_f64<32>, grid, block, 0, in.A, in.G, in.dnu, v[0], v[1], v[2],
-               (double *)dchi, (double *)dS, (const double2 *)g_ctx.d_tab64, (const GridArgs *)nullptr, 1);
+               (double *)dchi, (double *)dS, (const double2 *)g_ctx.d_tab64, (const GridArgs *)nullptr, 1,
+               (const double *)nullptr, 1);
     else
       LAUNCH_S(M3D_STAGE_OPACITY, k_lte_opacity_units_f64<0>, grid, block, 0, in.A, in.G, in.dnu, v[0], v[1], v[2],
-               (double *)dchi, (double *)dS, (const double2 *)g_ctx.d_tab64, (const GridArgs *)nullptr, 1);
+               (double *)dchi, (double *)dS, (const double2 *)g_ctx.d_tab64, (const GridArgs *)nullptr, 1,
+               (const double *)nullptr, 1);
     return M3D_OK;
   }
   const bool lane32 = nf == 32;
@@ -1268,18 +1273,21 @@ int launch_opacity(SynthIn &in, const double *v, bool fp64, void *dchi, void *dS
   }
   if (lane32) {
     // lane kernel: one warp per 32 cells (of one window), grid-stride over warps
-    const size_t nvc = (ncell + 31) / 32 * 32 * (size_t)in.nwin;
+    const size_t nvc = (ncell + 31) / 32 * 32 * (size_t)in.nwin * (batch ? in.nray : 1);
     int lgrid = (int)((nvc + block - 1) / block);
     if (lgrid > 148 * 3 * 8) lgrid = 148 * 3 * 8;
     if (batch)
       LAUNCH_S(M3D_STAGE_OPACITY, (k_lte_opacity_units_lane<32, float, false, false, true>), lgrid, block, smem_op,
-               in.A, in.G, in.dnu, v[0], v[1], v[2], (float *)dchi, (float *)dS, g_ctx.d_tab, in.d_Gw, in.nwin);
+               in.A, in.G, in.dnu, 0.0, 0.0, 0.0, (float *)dchi, (float *)dS, g_ctx.d_tab, in.d_Gw, in.nwin, in.d_vr,
+               in.nray);
     else if (in.reach)
       LAUNCH_S(M3D_STAGE_OPACITY, (k_lte_opacity_units_lane<32, float, true>), lgrid, block, smem_op, in.A, in.G,
-               in.dnu, v[0], v[1], v[2], (float *)dchi, (float *)dS, g_ctx.d_tab, (const GridArgs *)nullptr, 1);
+               in.dnu, v[0], v[1], v[2], (float *)dchi, (float *)dS, g_ctx.d_tab, (const GridArgs *)nullptr, 1,
+               (const double *)nullptr, 1);
     else
       LAUNCH_S(M3D_STAGE_OPACITY, (k_lte_opacity_units_lane<32, float, false>), lgrid, block, smem_op, in.A, in.G,
-               in.dnu, v[0], v[1], v[2], (float *)dchi, (float *)dS, g_ctx.d_tab, (const GridArgs *)nullptr, 1);
+               in.dnu, v[0], v[1], v[2], (float *)dchi, (float *)dS, g_ctx.d_tab, (const GridArgs *)nullptr, 1,
+               (const double *)nullptr, 1);
   } else {
     int ogrid = (int)((ncell + warps - 1) / warps);
     if (ogrid > 148 * 16) ogrid = 148 * 16;
@@ -1397,13 +1405,20 @@ int lte_synthesis_impl(const m3d_atmos_t *atm, int nwin, int nf_win, const doubl
                         (float)atm->tol, 0.0f);
       if (!(gw[w].dllam > 0)) return fail(M3D_EINVAL, "%s: window %d: log(lambda) must be ascending", who, w);
     }
-    void *dgw;
+    void *dgw, *dvr;
     TRY(scratch(25, sizeof(GridArgs) * gw.size(), &dgw));
     CUDA_TRY(cudaMemcpyAsync(dgw, gw.data(), sizeof(GridArgs) * gw.size(), cudaMemcpyHostToDevice, g_ctx.stream));
+    TRY(scratch(26, sizeof(double) * 3 * nray, &dvr));
+    CUDA_TRY(cudaMemcpyAsync(dvr, vec, sizeof(double) * 3 * nray, cudaMemcpyHostToDevice, g_ctx.stream));
     in.nf = nf_win;
     in.nwin = nwin;
     in.d_Gw = (const GridArgs *)dgw;
+    in.nray = nray;
+    in.d_vr = (const double *)dvr;
   }
+  // a batch holds every ray's transfer units at once (the opacity of all of them is
+  // one launch); a single window one ray's
+  const size_t nray_units = nwin > 1 ? (size_t)nray : 1;
 
   // rotation table of every global plane, per ray; slab starts
   // A single column is a plane-parallel atmosphere: radiative_transfer applies no
@@ -1436,8 +1451,8 @@ int lte_synthesis_impl(const m3d_atmos_t *atm, int nwin, int nf_win, const doubl
   // transfer units of the whole column (one ray at a time) and the emergent planes
   const size_t esz = fp64 ? sizeof(double) : sizeof(float);
   void *dchi, *dS, *dtop;
-  TRY(scratch(7, esz * plane * nz, &dchi));
-  TRY(scratch(8, esz * plane * nz, &dS));
+  TRY(scratch(7, esz * plane * nz * nray_units, &dchi));
+  TRY(scratch(8, esz * plane * nz * nray_units, &dS));
   void *dtop_user = nullptr;
   if (i_top) {
     if (fp64) { double *p; TRY(st.map((double *)i_top, plane * nray, false, true, &p)); dtop_user = p; }
@@ -1466,20 +1481,25 @@ int lte_synthesis_impl(const m3d_atmos_t *atm, int nwin, int nf_win, const doubl
     TRY(scratch(11, sizeof(double) * plane * 3, &dmem));
   }
 
+  // a batch's opacity: every ray and window in one launch
+  if (nwin > 1) TRY(launch_opacity(in, vec, fp64, dchi, dS));
   for (int r = 0; r < nray; r++) {
     const double *v = vec + 3 * r;
-    TRY(launch_opacity(in, v, fp64, dchi, dS));
+    if (nwin == 1) TRY(launch_opacity(in, v, fp64, dchi, dS));
+    // this ray's transfer units
+    const size_t ru = nwin > 1 ? plane * nz * (size_t)r : 0;
+    const void *rchi = (const char *)dchi + esz * ru, *rS = (const char *)dS + esz * ru;
     if (!fp64) {
       const QuadConst qc = quad_const(atm->ds_cm[2], v[2]);
       if (nf % 2 == 0) {
         // frequency pairs: 8-byte taps, the ray's rotation weights in shared memory
         const size_t pairs = plane / 2;
         LAUNCH_S(M3D_STAGE_SOLVE, k_quad_rot_column2, (int)((pairs + 255) / 256), 256, sizeof(RotCol) * nz, nf, nx, ny,
-                 nz, (const float *)dchi, (const float *)dS, (const RotCol *)drot + (size_t)r * nz, (const int *)dz0,
+                 nz, (const float *)rchi, (const float *)rS, (const RotCol *)drot + (size_t)r * nz, (const int *)dz0,
                  atm->nslab, qc, pc, dtmax, Imax, (float *)dtop + plane * r);
       } else {
         LAUNCH_S(M3D_STAGE_SOLVE, k_quad_rot_column, (int)((plane + 255) / 256), 256, 0, nf, nx, ny, nz,
-                 (const float *)dchi, (const float *)dS, (const RotCol *)drot + (size_t)r * nz, (const int *)dz0,
+                 (const float *)rchi, (const float *)rS, (const RotCol *)drot + (size_t)r * nz, (const int *)dz0,
                  atm->nslab, qc, pc, dtmax, Imax, (float *)dtop + plane * r);
       }
       LAUNCH_S(M3D_STAGE_REDUCE, k_save_partial<float>, dim3((nf + 31) / 32, kParts), dim3(32, 8), 0, nf, (int)ncol,
@@ -1496,8 +1516,8 @@ int lte_synthesis_impl(const m3d_atmos_t *atm, int nwin, int nf_win, const doubl
         sl.maser_dtau_max = atm->maser_dtau_max;
         sl.maser_Inu_max = atm->maser_Inu_max;
         double *w = (double *)dwork;
-        LAUNCH(k_slab_in, grid_for(plane * n), 256, 0, plane, n, (const double *)dchi + plane * z0[s],
-               (const double *)dS + plane * z0[s], w, n);
+        LAUNCH(k_slab_in, grid_for(plane * n), 256, 0, plane, n, (const double *)rchi + plane * z0[s],
+               (const double *)rS + plane * z0[s], w, n);
         LAUNCH(k_upstream_boundary<double>, grid_for(plane), 256, 0, nf, nx, ny, n, 1, w, s == 0 ? M3D_BND_PCHIP : M3D_BND_MEM,
                (const double *)dmem, pc, (const float *)nullptr, (const float *)nullptr, (const double *)nullptr);
         const float bottom = (float)((double)z0[s] * atm->ds_code[2]);

@@ -318,15 +318,17 @@ __device__ __forceinline__ float pick(const float (&a)[NF], int i) {
 // end, no peak test and a window capped by their reach (linelist_mod.f90:844-854, 914-921)
 // CHIL: write the line opacity chi_l of the window itself to chi_out (S_out unused):
 // the input of the adjoint's transfer units
-// BATCH: nwin windows of NF frequencies in one launch, each with its own grid Gw[w]
-// and frequencies nu + w NF; the warps run over (window, cell) with the cells of a
-// window padded to whole warps, so a warp holds one window, and a cell's row of
-// every window goes to chi_out + nwin NF cell + w NF: the rows of one window of
-// nwin NF frequencies, which the column solvers take as they are
+// BATCH: nray directions (vr, 3 each) and nwin windows of NF frequencies in one
+// launch, each window with its own grid Gw[w] and frequencies nu + w NF; the warps run
+// over (ray, window, cell) with the cells of a window padded to whole warps, so a warp
+// holds one ray and window, and a cell's row of every window goes to chi_out +
+// ray ncell nwin NF + nwin NF cell + w NF: per ray the rows of one window of nwin NF
+// frequencies, which the column solvers take as they are
 template <int NF, typename TO, bool REACH, bool CHIL = false, bool BATCH = false>
-__global__ void __launch_bounds__(256, 3) k_lte_opacity_units_lane(AtmosDev A, GridArgs G0, const double *nu0, double v0,
-                                                                   double v1, double v2, TO *chi_out, TO *S_out,
-                                                                   const float2 *tab, const GridArgs *Gw, int nwin) {
+__global__ void __launch_bounds__(256, 3) k_lte_opacity_units_lane(AtmosDev A, GridArgs G0, const double *nu0,
+                                                                   double v0_, double v1_, double v2_, TO *chi_out,
+                                                                   TO *S_out, const float2 *tab, const GridArgs *Gw,
+                                                                   int nwin, const double *vr, int nray) {
   extern __shared__ float smem[];
   float2 *s_tab = reinterpret_cast<float2 *>(smem);
   stage_tables(s_tab, tab);
@@ -335,13 +337,17 @@ __global__ void __launch_bounds__(256, 3) k_lte_opacity_units_lane(AtmosDev A, G
   const int ncell = A.ncell;
   const int nthreads = gridDim.x * blockDim.x;
   const int ncell_pad = (ncell + 31) / 32 * 32;
-  const int nvc = BATCH ? ncell_pad * nwin : ncell_pad;
+  const int nvc = BATCH ? ncell_pad * nwin * nray : ncell_pad;
   for (int vc = blockIdx.x * blockDim.x + threadIdx.x; vc < nvc; vc += nthreads) {
-    const int w = BATCH ? vc / ncell_pad : 0;
-    const int cell = BATCH ? vc - w * ncell_pad : vc;
+    const int ray = BATCH ? vc / (ncell_pad * nwin) : 0;
+    const int wc = BATCH ? vc - ray * (ncell_pad * nwin) : vc;
+    const int w = BATCH ? wc / ncell_pad : 0;
+    const int cell = BATCH ? wc - w * ncell_pad : wc;
     const GridArgs G = BATCH ? Gw[w] : G0;
     const double *nu = BATCH ? nu0 + (size_t)NF * w : nu0;
-    const size_t row = BATCH ? (size_t)NF * nwin * cell + (size_t)NF * w : (size_t)NF * cell;
+    const double v0 = BATCH ? vr[3 * ray] : v0_, v1 = BATCH ? vr[3 * ray + 1] : v1_, v2 = BATCH ? vr[3 * ray + 2] : v2_;
+    const size_t row = BATCH ? (size_t)ray * ncell * nwin * NF + (size_t)NF * nwin * cell + (size_t)NF * w
+                             : (size_t)NF * cell;
     const bool live = cell < ncell;
     const int cs = live ? cell : ncell - 1;
     const float T = A.temp[cs], chi_c = A.chi_c[cs];
@@ -548,26 +554,32 @@ struct ChlF64<0> {
   __device__ __forceinline__ double &operator[](int i) { return p[i]; }
 };
 
-// BATCH: nwin windows in one launch, as k_lte_opacity_units_lane<..., BATCH> (NF > 0)
+// BATCH: nray directions and nwin windows in one launch, as
+// k_lte_opacity_units_lane<..., BATCH> (NF > 0)
 template <int NF, bool BATCH = false>
-__global__ void __launch_bounds__(256) k_lte_opacity_units_f64(AtmosDev A, GridArgs G0, const double *nu0, double v0,
-                                                               double v1, double v2, double *chi_out, double *S_out,
-                                                               const double2 *tab, const GridArgs *Gw, int nwin) {
+__global__ void __launch_bounds__(256) k_lte_opacity_units_f64(AtmosDev A, GridArgs G0, const double *nu0,
+                                                               double v0_, double v1_, double v2_, double *chi_out,
+                                                               double *S_out, const double2 *tab, const GridArgs *Gw,
+                                                               int nwin, const double *vr, int nray) {
   static_assert(!BATCH || NF > 0, "window batches of a fixed window size");
   const double ex_cutoff = -85.0, voigt_peak = 0.56418958354775628, sqrt_pi = 1.7724538509055160;
   const double tol = (double)G0.tol, flo_scale = (double)G0.flo_scale;
   const double lt = log(tol / voigt_peak);
   const int ncell = A.ncell;
   const int nf = NF > 0 ? NF : G0.nf;
-  const int nvc = BATCH ? ncell * nwin : ncell;
+  const int nvc = BATCH ? ncell * nwin * nray : ncell;
   for (int vc = blockIdx.x * blockDim.x + threadIdx.x; vc < nvc; vc += gridDim.x * blockDim.x) {
-    const int w = BATCH ? vc / ncell : 0;
-    const int cell = BATCH ? vc - w * ncell : vc;
+    const int ray = BATCH ? vc / (ncell * nwin) : 0;
+    const int wc = BATCH ? vc - ray * (ncell * nwin) : vc;
+    const int w = BATCH ? wc / ncell : 0;
+    const int cell = BATCH ? wc - w * ncell : wc;
     const GridArgs G = BATCH ? Gw[w] : G0;
     const double *nu = BATCH ? nu0 + (size_t)nf * w : nu0;
+    const double v0 = BATCH ? vr[3 * ray] : v0_, v1 = BATCH ? vr[3 * ray + 1] : v1_, v2 = BATCH ? vr[3 * ray + 2] : v2_;
     const double sdl = G.inv_dllam;
     const double T = A.temp[cell], chi_c = A.chi_c[cell];
-    const size_t row = BATCH ? (size_t)nf * nwin * cell + (size_t)nf * w : (size_t)nf * cell;
+    const size_t row = BATCH ? (size_t)ray * ncell * nwin * nf + (size_t)nf * nwin * cell + (size_t)nf * w
+                             : (size_t)nf * cell;
     double *co = chi_out + row, *so = S_out + row;
     ChlF64<NF> chl(co);
 #pragma unroll

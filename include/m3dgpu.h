@@ -430,9 +430,9 @@ int m3d_lte_synthesis(const m3d_atmos_t *atm, int nf, const double *nu, const do
  * window's grid formed from its own frequencies; ie (nray, nwin nf), flux (nwin nf),
  * i_top (nray, ny, nx, nwin nf).  Equal bit for bit to one m3d_lte_synthesis call per
  * window.  For atmospheres too small to fill the GPU with one window (a 1D column of
- * 80 depths is three warps per window), where it runs every window's opacity in one
- * launch per ray; the transfer units of all windows are held at once (8 B per cell
- * and frequency of the batch).  No reach_in. */
+ * 80 depths is three warps per window), where it runs the opacity of every ray and
+ * window in one launch; the transfer units of all rays and windows are held at once
+ * (8 B per ray, cell and frequency of the batch; 16 B with M3D_FP64).  No reach_in. */
 int m3d_lte_synthesis_windows(const m3d_atmos_t *atm, int nwin, int nf, const double *nu, const double *llam,
                               int nray, const double *vec, const double *wmu, void *i_top, float *ie,
                               float *flux, unsigned flags);
