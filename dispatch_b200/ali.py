@@ -286,15 +286,18 @@ class AliWindow(_AtomIteration):
             self.gw_ji.zero_()
             for d in dirs:
                 slab, wmu, vp = self.slabs[d], float(self.wmu[d]), self.vproj[d]
-                self.w1.copy_(self.xhat)
-                self.w2.copy_(self.ehat)
-                nlte.bb_opacity(win, self.b, self.nstar, self.pop_ratio, self.e_kT, self.inv_df, vp, self.adamp,
-                                self.w1, self.w2, lte=False, wmu=wmu, split=self.split if p.split_rates else None,
-                                wphi=self.wphi if first else None)
                 if p.split_rates:
-                    nlte.transfer_units_split(self.w1, self.w2, self.beta, self.split,
-                                              maser_chi_floor=p.maser_chi_floor)
+                    # add_bound_bound_opacities and work_to_transfer_units in one pass
+                    # from the background to (chi, S)
+                    nlte.bb_opacity_units(win, self.b, self.nstar, self.pop_ratio, self.e_kT, self.inv_df, vp,
+                                          self.adamp, self.xhat, self.ehat, self.beta, self.w1, self.w2, self.split,
+                                          wmu=wmu, wphi=self.wphi if first else None,
+                                          maser_chi_floor=p.maser_chi_floor)
                 else:
+                    self.w1.copy_(self.xhat)
+                    self.w2.copy_(self.ehat)
+                    nlte.bb_opacity(win, self.b, self.nstar, self.pop_ratio, self.e_kT, self.inv_df, vp, self.adamp,
+                                    self.w1, self.w2, lte=False, wmu=wmu, wphi=self.wphi if first else None)
                     rt.work_to_transfer_units(self.w1, self.w2, self.beta, maser_chi_floor=p.maser_chi_floor)
                 mode = p.bottom if slab.dir > 0 else BND_ZERO
                 rt.upstream_boundary(slab, self.work, mode)

@@ -140,11 +140,13 @@ __global__ void k_bb_opacity(NlWinDev W, int ncell, const double *__restrict__ b
                              const float *__restrict__ inv_df, const float *__restrict__ vproj,
                              const float *__restrict__ adamp, const float2 *__restrict__ tab, int lte,
                              float *__restrict__ xhat, float *__restrict__ ehat, NlSplit S,
-                             const float *__restrict__ units_beta = nullptr, float units_floor = 0.0f) {
+                             const float *__restrict__ units_beta = nullptr, float units_floor = 0.0f,
+                             const float *__restrict__ xin = nullptr, const float *__restrict__ ein = nullptr) {
   const size_t nf = (size_t)W.nf, n = nf * ncell;
   for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
     const int f = (int)(k % nf), c = (int)(k / nf);
-    float xh = xhat[k], eh = ehat[k];
+    // the background from xin/ein where given (xhat/ehat then only receive the result)
+    float xh = xin ? xin[k] : xhat[k], eh = ein ? ein[k] : ehat[k];
     float oL = eh, oR = 0.0f, cL = xh, cR = 0.0f;
     int oid = 0, cid = 0;
     const int p0 = W.lf_ptr[f], p1 = W.lf_ptr[f + 1];

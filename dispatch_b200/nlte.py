@@ -135,6 +135,26 @@ def bb_opacity(win, b, nstar, pop_ratio, e_kT, inv_df, vproj, adamp, xhat, ehat,
                                *[ptr(a) for a in s], ptr(wphi), C.c_uint(_flags(nstar, xhat))), "m3d_bb_opacity")
 
 
+def bb_opacity_units(win, b, nstar, pop_ratio, e_kT, inv_df, vproj, adamp, xhat, ehat, beta, chi, S, split,
+                     wmu=0.0, wphi=None, maser_chi_floor=1e-4):
+    """bb_opacity (non-LTE, split tracking into split) and transfer_units_split of one
+    direction in one pass (m3d_bb_opacity_units): the background xhat, ehat is read,
+    chi and S receive the transfer units."""
+    init()
+    st, keep = make_window(win)
+    b, nstar, pop_ratio, e_kT = (_c(x, np.float64) for x in (b, nstar, pop_ratio, e_kT))
+    inv_df, vproj, adamp, xhat, ehat, beta = (_c(x, np.float32) for x in (inv_df, vproj, adamp, xhat, ehat, beta))
+    _inplace(chi, np.float32, "chi")
+    _inplace(S, np.float32, "S")
+    s = [split[k] for k in ("opac_L", "opac_R", "id", "chi_L", "chi_R", "chi_id")]
+    n = _ncell(pop_ratio)
+    check(lib().m3d_bb_opacity_units(C.byref(st), C.c_int(n), ptr(b), ptr(nstar), ptr(pop_ratio), ptr(e_kT),
+                                     ptr(inv_df), ptr(vproj), ptr(adamp), C.c_float(wmu), ptr(xhat), ptr(ehat),
+                                     ptr(beta), C.c_double(maser_chi_floor), ptr(chi), ptr(S),
+                                     *[ptr(a) for a in s], ptr(wphi), C.c_uint(_flags(nstar, chi))),
+          "m3d_bb_opacity_units")
+
+
 def new_split(ncell: int, nf: int) -> dict:
     z = lambda dt: np.zeros((ncell, nf), dt)
     return {"opac_L": z(np.float32), "opac_R": z(np.float32), "id": z(np.int32),

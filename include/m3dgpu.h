@@ -777,6 +777,19 @@ int m3d_bb_opacity(const m3d_atom_window_t *w, int ncell, const double *b, const
                    float *split_chi_L, float *split_chi_R, int *split_chi_id, float *wphi,
                    unsigned flags);
 
+/* m3d_bb_opacity (non-LTE, with the split tracking) and
+ * m3d_work_to_transfer_units_split (no scattering term, masers floored) of one
+ * direction in one pass, as rt_patch_t%execute runs them back to back: the
+ * background xhat, ehat (nf, ncell) is read, the lines added, and every point leaves as
+ * chi, S (nf, ncell) with its split arrays.  Equal bit for bit to the two calls on a
+ * copy of the background; no count of the floored points. */
+int m3d_bb_opacity_units(const m3d_atom_window_t *w, int ncell, const double *b, const double *nstar,
+                         const double *pop_ratio, const double *e_kT, const float *inv_df, const float *vproj,
+                         const float *adamp, float wmu, const float *xhat, const float *ehat, const float *beta,
+                         double maser_chi_floor, float *chi, float *S, float *split_opac_L, float *split_opac_R,
+                         int *split_id, float *split_chi_L, float *split_chi_R, int *split_chi_id, float *wphi,
+                         unsigned flags);
+
 /* work_to_transfer_units with split rates (rt_patch_mod.f90:3591-3604, 3614-3632):
  * scat = chi_scat*dJnu (nf, ncell) or NULL */
 int m3d_work_to_transfer_units_split(int nf, int ncell, float *w1, float *w2, const float *beta,

@@ -100,6 +100,32 @@ def test_transfer_units_split(nl, gn, base):
             assert np.array_equal(r[0][0], r[1][0]) and np.array_equal(r[0][1], r[1][1]) and r[0][2] == r[1][2]
 
 
+def test_bb_opacity_units_fused(nl, gn, base):
+    """m3d_bb_opacity_units: the opacity and the split transfer units in one pass from
+    the background, against the oracle's bb_opacity then transfer_units_split on a
+    copy of it."""
+    atom, inp, win, c, field = base
+    n, nf = c["pop_ratio"].size, win["nf"]
+    adamp = nl.bb_damping(win, c["ne"], c["tothi"], c["vbar2"], c["stark_pe"], c["unsold"], c["inv_df"])
+    xh, eh = field["xhat"].copy(), field["ehat"].copy()
+    nl.bf_opacity(win, c["b"], c["nstar"], c["pop_ratio"], c["e_kT"], xh, eh)
+    w1, w2 = xh.copy(), eh.copy()
+    so = _split(n, nf)
+    wo = np.zeros((atom["nline"], n), np.float32)
+    nl.bb_opacity(win, c["b"], c["nstar"], c["pop_ratio"], c["e_kT"], c["inv_df"], c["vproj"], adamp, w1, w2,
+                  wmu=0.3, split=so, wphi=wo)
+    nl.transfer_units_split(w1, w2, field["beta"], so)
+    chi, S = np.zeros_like(w1), np.zeros_like(w2)
+    sg = _split(n, nf)
+    wg = np.zeros((atom["nline"], n), np.float32)
+    gn.bb_opacity_units(win, c["b"], c["nstar"], c["pop_ratio"], c["e_kT"], c["inv_df"], c["vproj"], adamp, xh, eh,
+                        field["beta"], chi, S, sg, wmu=0.3, wphi=wg)
+    assert np.array_equal(chi, w1) and np.array_equal(S, w2)
+    for k in so:
+        assert np.array_equal(sg[k], so[k]), k
+    assert np.array_equal(wg, wo)
+
+
 @pytest.mark.parametrize("split_rates,precond", [(True, True), (True, False), (False, True), (False, False)])
 def test_bb_rates(nl, gn, base, split_rates, precond):
     atom, inp, win, c, field = base
