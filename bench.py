@@ -754,13 +754,21 @@ def run_b200(a):
     value = ws * a.steps * work_per_step / (ms / 1e3) / 1e9
     clocks = clk.summary()
 
-    # stage times and the sweep kernel's roofline (library CUDA events on its stream)
+    # stage times and the kernels' rooflines (library CUDA events on its stream): the
+    # first timed window alone (the FP64 pass's window), then every timed window again,
+    # so the per-step stage times average the windows the timed steps ran
     m.profile_enable(True)
     step(a.warmup)
-    op_ms, op_n = m.profile_read(m.STAGE_OPACITY)
-    sv_ms, sv_n = m.profile_read(m.STAGE_SOLVE)
-    rd_ms, rd_n = m.profile_read(m.STAGE_REDUCE)
+    op1_ms, _ = m.profile_read(m.STAGE_OPACITY)
+    sv1_ms, _ = m.profile_read(m.STAGE_SOLVE)
+    m.profile_enable(True)
+    for i in range(a.warmup, steps_total):
+        step(i)
+    op_tot, op_n = m.profile_read(m.STAGE_OPACITY)
+    sv_tot, sv_n = m.profile_read(m.STAGE_SOLVE)
+    rd_tot, rd_n = m.profile_read(m.STAGE_REDUCE)
     m.profile_enable(False)
+    op_ms, sv_ms, rd_ms = op_tot / a.steps, sv_tot / a.steps, rd_tot / a.steps
     peaks = _peaks()
     peak = peaks["hbm_gbs"] if peaks else 6650.0
     peak_kind = "measured" if peaks else "fallback"
@@ -772,7 +780,7 @@ def run_b200(a):
     nline = sum(len(sp["llam0"]) for sp in atm["species"])
     sm_hz = (clocks.get("sm_mhz") or 1965.0) * 1e6
     issue_peak = 148 * 4 * sm_hz / 1e9
-    op_launch_s = op_ms / op_n / 1e3 if op_n else None
+    op_launch_s = op_tot / op_n / 1e3 if op_n else None
     inst = (NCU_OPACITY_WARP_INST_PER_CELL_LINE * ncell * nline) if NCU_OPACITY_WARP_INST_PER_CELL_LINE else None
     op_achieved = inst / op_launch_s / 1e9 if (inst and op_launch_s) else None
     roofline = {"kernel": "k_lte_opacity_units_lane<32> (line opacity + transfer units, one ray)", "bound": "issue",
@@ -786,7 +794,7 @@ def run_b200(a):
                              "peak_gbs": peak, "peak_source": peak_kind}}
     # the formal-solver sweep: HBM roofline, chi and Snu read once per ray point frequency
     bytes_launch = 8.0 * ncell * nf
-    achieved = bytes_launch / (sv_ms / sv_n / 1e3) / 1e9 if sv_n else None
+    achieved = bytes_launch / (sv_tot / sv_n / 1e3) / 1e9 if sv_n else None
     roofline_sweep = {"kernel": "k_quad_rot_column2 (rotate_array + long_char_quadratic, all slabs, one ray)",
                       "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                       "frac": achieved / peak if achieved else None,
@@ -795,14 +803,16 @@ def run_b200(a):
     # the same launch against instruction issue, the bound its arithmetic sets: the
     # quadratic step's real(4) operations are the reference's
     sv_inst = NCU_SWEEP_WARP_INST_PER_CELL_FREQ * ncell * nf
-    sv_launch_s = sv_ms / sv_n / 1e3 if sv_n else None
+    sv_launch_s = sv_tot / sv_n / 1e3 if sv_n else None
     roofline_sweep["issue_view"] = {"warp_instructions_per_launch": sv_inst,
                                     "achieved": sv_inst / sv_launch_s / 1e9 if sv_launch_s else None,
                                     "peak": issue_peak, "unit": "G warp-instructions/s",
                                     "frac": sv_inst / sv_launch_s / 1e9 / issue_peak if sv_launch_s else None,
                                     "hbm_frac_at_full_issue": 8.0 * ncell * nf / (sv_inst / issue_peak) / peak}
     stages = {"opacity_ms_per_step": op_ms, "opacity_launches": op_n, "solve_ms_per_step": sv_ms,
-              "solve_launches": sv_n, "reduce_ms_per_step": rd_ms,
+              "solve_launches": sv_n, "reduce_ms_per_step": rd_ms, "windows": a.steps,
+              "kernel_ms_per_step": op_ms + sv_ms + rd_ms,
+              "outside_kernels_ms_per_step": ms / a.steps - (op_ms + sv_ms + rd_ms),
               "solve_gpt_per_s": work_per_step / (sv_ms / 1e3) / 1e9 if sv_ms else None}
 
     # end to end through the C ABI with pinned host buffers (copies inside the timed region)
@@ -836,6 +846,13 @@ def run_b200(a):
         nu_d, llam_d = dwin[a.warmup]
         ie32, f32, it32 = m.lte_synthesis(datm, nu_d, llam_d, vec, wmu, device=True, return_itop=True)
         torch.cuda.synchronize()
+        # the FP32 pass timed on this same window, the ratio's numerator
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        m.lte_synthesis(datm, nu_d, llam_d, vec, wmu, device=True)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t32 = e0.elapsed_time(e1)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         ie64, f64, it64 = m.lte_synthesis(datm, nu_d, llam_d, vec, wmu, device=True, fp64=True, return_itop=True)
@@ -863,14 +880,15 @@ def run_b200(a):
         sv64_ms, sv64_n = m.profile_read(m.STAGE_SOLVE)
         m.profile_enable(False)
         fp64 = {"value": work_per_step / (t64 / 1e3) / 1e9, "unit": UNIT, "ms_per_step": t64,
-                "fp32_over_fp64": value / ws / (work_per_step / (t64 / 1e3) / 1e9),
+                "fp32_over_fp64": t64 / t32, "fp32_ms_same_window": t32,
+                "window": int(wins[a.warmup]),
                 "fp32_error_vs_fp64": errors,
                 "error_note": "relative; chi and S of ray 7 (mu 0.45), I_top every column and ray, ie and flux of "
                               "the window; single points of chi/S/I_top can differ by a QLG table node (FP32 and "
                               "FP64 snap a point to neighbouring nodes)",
                 "opacity_ms_per_step": op64_ms, "solve_ms_per_step": sv64_ms, "solve_launches": sv64_n,
-                "opacity_fp32_over_fp64": op64_ms / op_ms if op_ms else None,
-                "solve_fp32_over_fp64": sv64_ms / sv_ms if sv_ms else None,
+                "opacity_fp32_over_fp64": op64_ms / op1_ms if op1_ms else None,
+                "solve_fp32_over_fp64": sv64_ms / sv1_ms if sv1_ms else None,
                 "path": "FP64 end to end: line opacity and QLG-bot (fp64 tables, exp, log), transfer units, "
                         "rotate_array and long_char_quadratic, one launch per ray and slab"}
 
