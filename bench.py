@@ -161,16 +161,18 @@ def _peaks():
 # each kernel; the command is in the summaries under profiles/).
 #  k_quad_rot_column2: DRAM bytes per cell and frequency of a launch (28,360,192 B read
 #    for 110,592 cells x 32 frequencies), against 8 B algorithmic (chi and Snu once).
-#  k_lte_opacity_units_lane<32>: warp instructions per (cell, line) of a launch
-#    (751,598,136 for 110,592 cells x 500 lines), which scales a full launch's count by
-#    its cells and lines; DRAM bytes per cell: 49.9 B read (measured) plus the chi and
+#  k_lte_opacity_units_lane<32>: warp instructions per (cell, line), the mean over the
+#    104 launches of the 8 timed windows x 13 rays (79,401,861,582 for 110,592 cells x
+#    500 lines each; 13.0-14.8 per launch as the windows' line loads differ), which
+#    scales a full launch's count by its cells and lines; DRAM bytes per cell: 49.9 B
+#    read (measured, window 0) plus the chi and
 #    Snu it writes, 8 B per frequency (the small case's 28 MB of output stayed in L2,
 #    a full launch's 3.5 GB cannot).
 NCU_SWEEP_DRAM_BYTES_PER_CELL_FREQ = 8.013
 #  k_quad_rot_column2: warp instructions per (cell, frequency) of a launch
 #    (21,865,784 for 110,592 cells x 32 frequencies)
 NCU_SWEEP_WARP_INST_PER_CELL_FREQ = 21865784 / (110592 * 32)
-NCU_OPACITY_WARP_INST_PER_CELL_LINE = 751598136 / (110592 * 500)
+NCU_OPACITY_WARP_INST_PER_CELL_LINE = 79401861582 / (104 * 110592 * 500)
 NCU_OPACITY_DRAM_READ_BYTES_PER_CELL = 5516032 / 110592
 #  k_continuum: warp instructions per cell of a launch of the continuum case (250
 #    frequencies, fourteen components; 904,826,466 for 110,592 cells)
