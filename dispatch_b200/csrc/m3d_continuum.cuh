@@ -27,10 +27,11 @@ constexpr int kContMaxTab = 8192;   // their table entries at every temperature 
 constexpr int kContKF = 8;          // wavelengths a lane holds in one pass over the components
 
 // wcalc2's per-wavelength set-up of an 'H BF' level (level_mod.f90:186-218): cls 0
-// none, 1 beyond the series limit, 2 below it (a dissolved upper level); cutfac the
-// cut beyond the alpha line; x1, x2, kk = calc_x_and_k of the state, kd its kk in real(8)
+// none, 1 beyond the series limit, 2 below it (a dissolved upper level); qcut =
+// 2.0898E-26/(2 i^5) (real(4)) times the cut beyond the alpha line, the real(8) product
+// g(f) starts from; x1, x2, kk = calc_x_and_k of the state, kd its kk in real(8)
 struct OccFDev {
-  double cutfac, kd;
+  double qcut, kd;
   float x1, x2, kk;
   int cls;
 };
@@ -49,10 +50,9 @@ struct __align__(16) BfCompDev {
   const float4 *wt;
   const unsigned char *quad;
   const double *n, *n2, *part, *level_n;
-  // an 'H BF' level under occupation probabilities: occ, q = 2.0898e-26/(2 i^5) in
-  // real(4), its occupation probability per cell and the per-wavelength set-up
+  // an 'H BF' level under occupation probabilities: occ, its occupation probability
+  // per cell and the per-wavelength set-up
   int occ;
-  float occ_q;
   const double *level_w;
   const OccFDev *occf;
 };
@@ -257,7 +257,6 @@ __device__ __forceinline__ void cont_comp(const BfCompDev &c, const BfCellDev &r
     const unsigned char *quad = c.quad;
     const OccFDev *occf = c.occf;
     const float scale = (float)c.xkap_scale;
-    const double q = (double)c.occ_q;
 #pragma unroll
     for (int k = 0; k < KF; k++) {
       const int f = f0 + 32 * k;
@@ -278,7 +277,7 @@ __device__ __forceinline__ void cont_comp(const BfCompDev &c, const BfCellDev &r
       }
       if (lam3) ab = __fmul_rn(ab, __ldg(l3 + f));
       // g = real(2.0898E-26/(2 i^5) * cutfac * ab, 4), ab times real(xkap_scale, 4)
-      const float g = (float)((q * o.cutfac) * (double)__fmul_rn(ab, scale));
+      const float g = (float)(o.qcut * (double)__fmul_rn(ab, scale));
       float d;
       if (o.cls == 1) {
         d = w;
