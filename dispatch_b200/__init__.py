@@ -34,7 +34,7 @@ BND_MEM, BND_ZERO, BND_PCHIP, BND_LTE = range(4)
 EXPORTS = ("m3d_init", "m3d_free", "m3d_last_error", "m3d_version", "m3d_set_stream", "m3d_synchronize",
            "m3d_launch_count", "m3d_alloc_stats", "m3d_weights", "m3d_qlg_init", "m3d_qlg_tables", "m3d_qlg_bot_profile",
            "m3d_line_opacity", "m3d_lte_background", "m3d_work_to_transfer_units", "m3d_formal_solve",
-           "m3d_rotate_array", "m3d_upstream_boundary", "m3d_integrate_intensity", "m3d_lte_synthesis", "m3d_lte_synthesis_windows", "m3d_lte_transfer_units", "m3d_lte_synthesis_adjoint", "m3d_hop_set_state", "m3d_hop_free_state", "m3d_hop_opacity", "m3d_opacity", "m3d_bb_opacity_units",
+           "m3d_rotate_array", "m3d_upstream_boundary", "m3d_integrate_intensity", "m3d_lte_synthesis", "m3d_lte_synthesis_windows", "m3d_lte_transfer_units", "m3d_lte_synthesis_adjoint", "m3d_hop_set_state", "m3d_hop_free_state", "m3d_hop_opacity", "m3d_opacity", "m3d_bb_opacity_units", "m3d_h_levels",
            "m3d_profile_enable", "m3d_profile_read", "m3d_rotate_array_noalloc", "m3d_collision_nrows",
            "m3d_collision_rates",
            "m3d_stateq_update", "m3d_ng_accumulate", "m3d_ng_extrapolate", "m3d_bb_damping", "m3d_bf_opacity",

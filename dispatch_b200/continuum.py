@@ -179,6 +179,34 @@ def opacity(comps: list, lam, nu, cells: dict, beta=None, include_llist: bool = 
     return chi, scat
 
 
+def h_levels(cells: dict, nk: int, occupation: bool = True):
+    """The H I level set-up the 'H BF' components read (init_H_levels with
+    compute_shield, HOP/composition_mod.f90:2604-2613, 2708-2768) through m3d_h_levels:
+    (shield (ncell,), level_n (nk, ncell), level_w (nk, ncell) or None), numpy for host
+    cells, CUDA tensors for device cells.  cells needs temp, e_kT, ne, dxi, nHI, and
+    nHeI (with occupation) or partHI (without)."""
+    init()
+    dev = not isinstance(cells["temp"], np.ndarray)
+    arr = {k: _cell_array(cells.get(k), dev) for k in ("temp", "e_kT", "ne", "dxi", "nHI", "nHeI", "partHI")}
+    n = int(cells["temp"].shape[0])
+    if dev:
+        import torch
+        dv = cells["temp"].device
+        sh = torch.empty(n, dtype=torch.float64, device=dv)
+        ln = torch.empty((nk, n), dtype=torch.float64, device=dv)
+        lw = torch.empty((nk, n), dtype=torch.float64, device=dv) if occupation else None
+        order_after_torch(cells["temp"])
+        flags = DEVICE_PTRS
+    else:
+        sh, ln = np.empty(n), np.empty((nk, n))
+        lw = np.empty((nk, n)) if occupation else None
+        flags = 0
+    check(lib().m3d_h_levels(C.c_int(n), C.c_int(nk), C.c_int(int(occupation)),
+                             *[ptr(arr[k]) for k in ("temp", "e_kT", "ne", "dxi", "nHI", "nHeI", "partHI")],
+                             ptr(sh), ptr(ln), ptr(lw), C.c_uint(flags)), "m3d_h_levels")
+    return sh, ln, lw
+
+
 def airvac_corr(lam):
     """The refractive index of air at wavelength lam [AA] (HOP/handyfuncs_mod.f90:437-445),
     the published formula VALD uses (Piskunov, after Ciddor 1996)."""
@@ -205,5 +233,5 @@ def chi500(comps: list, cells: dict, ref_lam: float = 5000.0):
     return chi[:, 0]
 
 
-__all__ = ["continuum_opacities", "opacity", "chi500", "air2vac", "set_table", "BfComp", "ContCells", "HMINUS", "NPE", "H", "H_FF", "PAIR",
+__all__ = ["continuum_opacities", "opacity", "chi500", "air2vac", "h_levels", "set_table", "BfComp", "ContCells", "HMINUS", "NPE", "H", "H_FF", "PAIR",
            "H2PLUS", "PEDEP", "PEACH", "MOLECULAR", "REGULAR"]

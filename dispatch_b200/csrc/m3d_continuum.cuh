@@ -501,4 +501,80 @@ k_continuum(int ncomp, const BfCompDev *__restrict__ comps_g, int any_istim, int
   }
 }
 
+// calc_x_and_k (level_mod.f90:77-94) in real(8), as the host forms it for wcalc2
+__device__ __forceinline__ void h_calc_x_and_k(double ns, double &x1, double &x2, double &k) {
+  const double rbohr = 5.29177349e-9;
+  const double ns2 = ns * ns;
+  const double rih = ns * sqrt(2.5 * ns2 + 0.5);
+  const double t1 = rbohr * (rih + (double)1.73f), t2 = rbohr * (rih + (double)1.02f);
+  x1 = t1 * t1 * t1;
+  x2 = t2 * t2 * t2;
+  double kk = (double)8.3e14f / (ns2 * ns2);
+  if (ns > 3.) kk = kk * (double)5.33333333f * ns / ((ns + 1.0) * (ns + 1.0));
+  k = kk * sqrt(kk);
+}
+
+// init_H_levels with compute_shield (composition_mod.f90:2604-2613, 2708-2768), one
+// thread per cell: the shielding (1 + 0.08989 ne^0.16667/sqrt(T))^3.15/ne; the
+// hydrogenic levels i = 1..nk, xion = Ryd (1 - 1/i^2) (a real(4) bracket), g = 2 i^2,
+// n_i = g exp(-e_kT xion); with occupation probabilities w_i = wcalc (level_mod.f90:
+// 108-142) and the partition function 1 / sum w_i n_i, else exp(-ln U) with the levels
+// above n = sqrt(Ryd/dxi) dissolved where the first cell's dxi > 0 (the reference tests
+// dxi(1,1,1)); then n_i = nHI n_i part
+__global__ void k_h_levels(int ncell, int nk, int occupation, int dissolve, const double *__restrict__ temp,
+                           const double *__restrict__ e_kT, const double *__restrict__ ne,
+                           const double *__restrict__ dxi, const double *__restrict__ nHI,
+                           const double *__restrict__ nHeI, const double *__restrict__ partHI,
+                           double *__restrict__ shield, double *__restrict__ level_n, double *__restrict__ level_w) {
+  const double ryd = 13.598434, pi43 = 4.18879;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += gridDim.x * blockDim.x) {
+    const double nec = ne[c];
+    double sh = (double)0.08989f * pow(nec, 0.16667) / sqrt(temp[c]);
+    sh = pow(1.0 + sh, 3.15) / nec;
+    shield[c] = sh;
+    const double ekt = e_kT[c];
+    double part = 0.0;
+    if (occupation) {
+      const double nh = nHI[c], nhe = nHeI[c];
+      for (int i = 1; i <= nk; i++) {
+        const float xi = 1.0f - 1.0f / (float)(i * i);
+        const double n = (double)(2 * i * i) * exp(-ekt * (ryd * (double)xi));
+        double x1, x2, k1;
+        h_calc_x_and_k((double)i, x1, x2, k1);
+        const double k2 = k1 * k1;
+        double res = exp(-(pi43 * (nh * x1 + nhe * x2)));
+        if (k1 * sh < 1e4) {
+          const double frac = 0.1402 * sh * k2 / (nec * (1.0 + (double)0.1285f * sh * k1));
+          res = res * (frac / (1.0 + frac));
+        }
+        level_w[c + (size_t)ncell * (i - 1)] = res;
+        level_n[c + (size_t)ncell * (i - 1)] = n;
+        part = part + res * n;
+      }
+      part = 1.0 / part;
+    } else {
+      part = exp(-partHI[c]);
+      // a cell without lowering (dxi <= 0) keeps every level (int(sqrt(Ryd/0)) is
+      // undefined in the reference)
+      const bool cut = dissolve && dxi[c] > 0.0;
+      const double h1 = cut ? sqrt(ryd / dxi[c]) : 0.0;
+      const int nniv = cut && h1 < 2147483647.0 ? (int)h1 : 2147483647;
+      for (int i = 1; i <= nk; i++) {
+        const float xi = 1.0f - 1.0f / (float)(i * i);
+        double n = (double)(2 * i * i) * exp(-ekt * (ryd * (double)xi));
+        if (cut) {
+          if (nniv < i) n = 0.0;
+          else if (nniv == i) n = n * (h1 - (double)nniv);
+        }
+        level_n[c + (size_t)ncell * (i - 1)] = n;
+      }
+    }
+    const double nh = nHI[c];
+    for (int i = 1; i <= nk; i++) {
+      double &n = level_n[c + (size_t)ncell * (i - 1)];
+      n = nh * n * part;
+    }
+  }
+}
+
 }  // namespace m3d

@@ -557,6 +557,20 @@ int m3d_continuum_opacities(int ncomp, const m3d_bf_comp_t *comps, int nlam, con
                             int ncell, const m3d_cont_cells_t *cells, const float *beta, float *xhat, float *sigma,
                             unsigned flags);
 
+/* The H I level set-up the continuum's 'H BF' components read, init_H_levels with
+ * compute_shield (composition_mod.f90:2604-2613, 2708-2768) over ncell cells (float64,
+ * per the flags): shield (ncell) = (1 + 0.08989 ne^0.16667/sqrt(T))^3.15 / ne; for the
+ * hydrogenic levels i = 1..nk (nk <= 100) level_n (nk x ncell, level-major: level_n[c +
+ * ncell (i-1)]) = nHI g_i exp(-e_kT Ryd (1 - 1/i^2)) part.  With occupation (the
+ * reference's H_occupation_probability) level_w (same layout) = wcalc's occupation
+ * probability of each level (level_mod.f90:108-142, from nHI, nHeI, ne and shield) and
+ * part = 1/sum_i w_i g_i exp(..); without, part = exp(-partHI) and, when the first cell
+ * has dxi > 0 (as the reference decides), the levels above n = sqrt(Ryd/dxi) of each
+ * cell dissolved (a cell with dxi <= 0 keeps them all); level_w and nHeI may be NULL. */
+int m3d_h_levels(int ncell, int nk, int occupation, const double *temp, const double *e_kT, const double *ne,
+                 const double *dxi, const double *nHI, const double *nHeI, const double *partHI, double *shield,
+                 double *level_n, double *level_w, unsigned flags);
+
 /* composition_type%opacity (composition_mod.f90:3122-3260), the whole pipeline that
  * hop.opacity() and chi500 call, over ncell cells (those of the loaded state with
  * include_llist): beta (the caller's (nlam, ncell), or NULL: boltzmann_factor from nu

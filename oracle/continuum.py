@@ -107,3 +107,18 @@ def continuum_opacities(comps: list, lam, nu, cells: dict, beta=None, sigma: boo
     if rc != 0:
         raise ValueError("or_continuum_opacities: unsupported component")
     return xhat, sg
+
+
+def h_levels(cells: dict, nk: int, occupation: bool = True):
+    """init_H_levels with compute_shield: (shield (ncell,), level_n (nk, ncell),
+    level_w (nk, ncell) or None)."""
+    arr = {k: (None if cells.get(k) is None else np.ascontiguousarray(cells[k], np.float64))
+           for k in ("temp", "e_kT", "ne", "dxi", "nHI", "nHeI", "partHI")}
+    n = arr["temp"].size
+    sh = np.empty(n)
+    ln = np.empty((nk, n))
+    lw = np.empty((nk, n)) if occupation else None
+    p = lambda a: None if a is None else C.c_void_p(a.ctypes.data)
+    lib().or_h_levels(C.c_int(n), C.c_int(nk), C.c_int(int(occupation)), p(arr["temp"]), p(arr["e_kT"]),
+                      p(arr["ne"]), p(arr["dxi"]), p(arr["nHI"]), p(arr["nHeI"]), p(arr["partHI"]), p(sh), p(ln), p(lw))
+    return sh, ln, lw

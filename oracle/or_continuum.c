@@ -460,3 +460,63 @@ int or_continuum_opacities(int ncomp, const or_bf_comp_t *comps, int nlam, const
   }
   return 0;
 }
+
+/* init_H_levels with compute_shield (composition_mod.f90:2604-2613, 2708-2768) and
+ * wcalc (level_mod.f90:108-142), cell by cell as the reference's array statements
+ * evaluate them: the shielding, the hydrogenic levels' g exp(-e_kT xion) with xion =
+ * RYD (1. - 1./i**2) (a default-real bracket), the occupation probabilities and the
+ * partition function 1/sum w n, or exp(-ln U) with the levels above sqrt(RYD/dxi)
+ * dissolved when the first cell's dxi > 0; a cell with dxi <= 0 keeps every level
+ * (int(sqrt(RYD/0)) has no defined value in the reference). */
+void or_h_levels(int ncell, int nk, int occupation, const double *temp, const double *e_kT, const double *ne,
+                 const double *dxi, const double *nHI, const double *nHeI, const double *partHI, double *shield,
+                 double *level_n, double *level_w)
+{
+  const double pi43 = 4.18879;
+  const int dissolve = !occupation && dxi[0] > 0.0;
+  for (int c = 0; c < ncell; c++) {
+    double sh = (double)0.08989f * pow(ne[c], 0.16667) / sqrt(temp[c]);
+    sh = pow(1.0 + sh, 3.15) / ne[c];
+    shield[c] = sh;
+  }
+  for (int i = 1; i <= nk; i++) {
+    const float xi = 1.0f - 1.0f / (float)(i * i);
+    const double xion = OR_RYD * (double)xi, g = (double)(2 * i * i);
+    for (int c = 0; c < ncell; c++) level_n[c + (size_t)ncell * (i - 1)] = g * exp(-e_kT[c] * xion);
+  }
+  for (int c = 0; c < ncell; c++) {
+    double part;
+    if (occupation) {
+      part = 0.0;
+      for (int i = 1; i <= nk; i++) {
+        double x1, x2, k1;
+        calc_x_and_k((double)i, &x1, &x2, &k1);
+        const double k2 = k1 * k1;
+        const double x = shield[c];
+        double res = exp(-(pi43 * (nHI[c] * x1 + nHeI[c] * x2)));
+        if (k1 * x < 1e4) {
+          const double frac = 0.1402 * x * k2 / (ne[c] * (1.0 + (double)0.1285f * x * k1));
+          res = res * (frac / (1.0 + frac));
+        }
+        level_w[c + (size_t)ncell * (i - 1)] = res;
+        part = part + res * level_n[c + (size_t)ncell * (i - 1)];
+      }
+      part = 1.0 / part;
+    } else {
+      part = exp(-partHI[c]);
+      if (dissolve && dxi[c] > 0.0) {
+        const double h1 = sqrt(OR_RYD / dxi[c]);
+        const int nniv = h1 < 2147483647.0 ? (int)h1 : 2147483647;
+        for (int i = 1; i <= nk; i++) {
+          double *n = &level_n[c + (size_t)ncell * (i - 1)];
+          if (nniv < i) *n = 0.0;
+          else if (nniv == i) *n = *n * (h1 - (double)nniv);
+        }
+      }
+    }
+    for (int i = 1; i <= nk; i++) {
+      double *n = &level_n[c + (size_t)ncell * (i - 1)];
+      *n = nHI[c] * *n * part;
+    }
+  }
+}

@@ -75,6 +75,13 @@ int or_bf_weights(const or_bf_comp_t *c, int nlam, const double *lam, int *iw, u
 int or_continuum_opacities(int ncomp, const or_bf_comp_t *comps, int nlam, const double *lam, const double *nu,
                            int ncell, const or_cont_cells_t *cells, const float *beta, float *xhat, float *sigma);
 
+/* init_H_levels with compute_shield (composition_mod.f90:2604-2613, 2708-2768):
+ * shield (ncell), level_n and (with occupation) level_w (nk x ncell, level-major);
+ * dissolve: the first cell's dxi > 0 without occupation probabilities */
+void or_h_levels(int ncell, int nk, int occupation, const double *temp, const double *e_kT, const double *ne,
+                 const double *dxi, const double *nHI, const double *nHeI, const double *partHI, double *shield,
+                 double *level_n, double *level_w);
+
 #ifdef __cplusplus
 }
 #endif

@@ -242,3 +242,28 @@ def test_h_occupation_without_perturbers(oc):
     below, beyond = lam > edge * 1.001, lam < edge * 0.999
     assert np.all(occ[:, below] == 0)
     np.testing.assert_allclose(occ[:, beyond], ref[:, beyond], rtol=1e-6)
+
+
+def test_h_levels(oc):
+    """init_H_levels: with occupation probabilities the populations are nHI g exp(..)/Z
+    with Z = sum w g exp(..), so sum_i w_i n_i = nHI; without, nHI g exp(..) exp(-ln U)
+    and the levels above n = sqrt(RYD/dxi) dissolved; the shielding as stated."""
+    _, _, _, cells = synth.continuum_case(ncell=200, nlam=8)
+    sh, ln, lw = oc.h_levels(cells, 12, occupation=True)
+    want = (np.float64(np.float32(0.08989)) * cells["ne"] ** 0.16667 / np.sqrt(cells["temp"]))
+    np.testing.assert_allclose(sh, (1.0 + want) ** 3.15 / cells["ne"], rtol=1e-14)
+    np.testing.assert_allclose((lw * ln).sum(axis=0), cells["nHI"], rtol=1e-13)
+    assert np.all((lw > 0) & (lw <= 1)) and np.all(np.diff(lw, axis=0) <= 0)   # higher levels dissolve more
+    cells2 = dict(cells)
+    cells2["dxi"] = np.where(np.arange(200) % 5 == 0, 0.0, 0.02 + 0.1 * np.random.default_rng(1).random(200))
+    cells2["dxi"][0] = 0.05
+    sh2, ln2, lw2 = oc.h_levels(cells2, 12, occupation=False)
+    assert lw2 is None
+    i = np.arange(1, 13)[:, None]
+    xion = 13.598434 * (np.float32(1) - np.float32(1) / (i * i).astype(np.float32)).astype(np.float64)
+    full = cells["nHI"] * (2.0 * i * i * np.exp(-cells["e_kT"] * xion)) * np.exp(-cells["partHI"])
+    nniv = np.where(cells2["dxi"] > 0, np.floor(np.sqrt(13.598434 / np.where(cells2["dxi"] > 0, cells2["dxi"], 1))), 99)
+    assert np.all(ln2[i[:, 0][:, None] > nniv[None, :]] == 0)
+    keep = i <= nniv[None, :] - 1
+    np.testing.assert_allclose(ln2[keep], full[keep], rtol=1e-13)
+    np.testing.assert_allclose(ln2[:, cells2["dxi"] == 0], full[:, cells2["dxi"] == 0], rtol=1e-13)
