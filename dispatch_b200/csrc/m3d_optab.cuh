@@ -149,7 +149,8 @@ constexpr int kOptabWarps = 8;
 // both samplers are latency-bound: at most 64 registers give 4 blocks (32 warps) per
 // SM, measured faster than 66-77 registers at 3 blocks and than 48 or 40 with spills
 constexpr int kOptabMinBlocks = 4;
-constexpr int kOptabUnroll = 2;   // frequencies per lane per pass of sample_interpolate_ll
+constexpr int kOptabUnroll = 1;   // frequencies per lane per pass of sample_interpolate_ll
+constexpr int kOptabLLMinBlocks = 4;   // 5 or 6 spill and are slower
 
 // sample_interpolate (optab_mod.f90:181-287): one warp per cell, lanes over the
 // frequencies; back = (kappa + kappa_scat) chi500, scat = kappa_scat chi500
@@ -189,9 +190,10 @@ __global__ void __launch_bounds__(32 * kOptabWarps, kOptabMinBlocks) k_optab_sam
 // cell is lam_q (1 + vproj), bracketed by walking from the unshifted count;
 // xhat, ehat += kappa chi500, and chi_scat += kappa_scat chi500 when given.
 // A lane takes kOptabUnroll frequencies per pass: their work slots are read and
-// their brackets found before the table lookups, so the slow reads of the slots
-// and of the wavelength nodes are in flight together.
-__global__ void __launch_bounds__(32 * kOptabWarps, kOptabMinBlocks) k_optab_sample_ll(OptabDev T, int nf, long long ncell,
+// their brackets found before the table lookups.  One frequency at 4 blocks per SM
+// measured faster (8.7 ms at 2.1 M cells x 256) than two (10.6 ms), which held the
+// reads of two in flight at the cost of registers.
+__global__ void __launch_bounds__(32 * kOptabWarps, kOptabLLMinBlocks) k_optab_sample_ll(OptabDev T, int nf, long long ncell,
                                                                       const double *temp, const double *ne,
                                                                       const float *chi500, const float *vproj,
                                                                       const double *lam_q, const OptabFreq *fc,
