@@ -256,18 +256,21 @@ __device__ __forceinline__ void rate_chunk_sum(float (*T)[33], int lane, int cnt
   __syncwarp();
 }
 
-// bound_bound_rates: one warp per (line, 16 consecutive cells).  Lanes 0..15 form
-// their cell's per-line constants; the terms of every (cell, f) are then evaluated
+// bound_bound_rates: one warp per (line, kBbCells consecutive cells).  The first
+// kBbCells lanes form their cell's per-line constants; the terms of every (cell, f) are then evaluated
 // a cell at a time with all 32 lanes along f (one 128-byte load per array), written
 // to shared memory, and lane k adds cell k's terms in ascending f -- the
 // reference's order.  A line window of up to 32 points takes a single chunk.
-// The tiles run cell-major: the lines of 16 cells are neighbouring warps, so the
+// The tiles run cell-major: the lines of a tile's cells are neighbouring warps, so the
 // sectors their windows share (and those a window straddles) are read from DRAM
 // once and from L2 after.  Each (line, cell) has one writer, so the order changes
 // no sum.
-constexpr int kBbWarps = 4, kBbCells = 16;
+// 8 cells a tile (17 KB of shared terms a block) and 64 registers give 8 blocks (32
+// warps) per SM, which hides the loads' latency better than 16-cell tiles at 6 blocks:
+// the 120^3 window's sweep 748 -> 711 ms
+constexpr int kBbWarps = 4, kBbCells = 8;
 
-__global__ void __launch_bounds__(kBbWarps * 32)
+__global__ void __launch_bounds__(kBbWarps * 32, 8)
 k_bb_rates(NlWinDev W, NlRateOpts O, int ncell, const double *__restrict__ b,
            const double *__restrict__ nstar, const double *__restrict__ pop_ratio,
            const double *__restrict__ e_kT, const float *__restrict__ inv_df,
