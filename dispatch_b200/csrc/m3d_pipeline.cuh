@@ -325,7 +325,7 @@ __device__ __forceinline__ float pick(const float (&a)[NF], int i) {
 // ray ncell nwin NF + nwin NF cell + w NF: per ray the rows of one window of nwin NF
 // frequencies, which the column solvers take as they are
 template <int NF, typename TO, bool REACH, bool CHIL = false, bool BATCH = false>
-__global__ void __launch_bounds__(256, 3) k_lte_opacity_units_lane(AtmosDev A, GridArgs G0, const double *nu0,
+__global__ void __launch_bounds__(768, 1) k_lte_opacity_units_lane(AtmosDev A, GridArgs G0, const double *nu0,
                                                                    double v0_, double v1_, double v2_, TO *chi_out,
                                                                    TO *S_out, const float2 *tab, const GridArgs *Gw,
                                                                    int nwin, const double *vr, int nray) {
