@@ -489,7 +489,7 @@ __device__ __forceinline__ void deposit_adj_mk(float (&chl)[NF], const float (&g
 // reduced over the warp's cells and then the block, dL/dgpref of the line.
 // Shared memory: the QLG tables (float2), the table differences dW, and the block's
 // per-line sums (nline floats).
-__global__ void __launch_bounds__(256, 2) k_opacity_adj(AtmosDev A, GridArgs G, const double *nu, double v0,
+__global__ void __launch_bounds__(512, 1) k_opacity_adj(AtmosDev A, GridArgs G, const double *nu, double v0,
                                                         double v1, double v2, const float2 *tab, const float *dWg,
                                                         const float *g_chil, float *g_lnbase, float *g_ekt,
                                                         float *g_idf, float *const *g_gpref, int nline_max) {
